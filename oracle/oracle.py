@@ -1,0 +1,387 @@
+"""CPU oracle: Python bindings over the C restatement (``oracle/libpdoracle.so``)
+and over the reference's own LPS kernels compiled from its sources
+(``oracle/_ref/libpdref.so``).
+
+TEST INFRASTRUCTURE ONLY. tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` use it as the checker; the product package
+``peridigm_b200`` never imports it.
+
+Parity of the restatement is pinned by tests/test_oracle_golden.py (known
+answers of src/materials/unit_test/utPeridigm_ElasticMaterial.cpp, the gold
+Exodus files of the reference's verification/regression tests kept as
+fixtures in tests/golden/) and by tests/test_oracle_vs_ref.py (the compiled
+reference kernels).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpdoracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libpdref.so")
+
+INFLUENCE = {"One": 0, "Parabolic Decay": 1, "Gaussian": 2}
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class Plane(C.Structure):
+    """Rectangular_Plane bond filter (Peridigm_Discretization.cpp:158-175)."""
+
+    _fields_ = [
+        ("normal", C.c_double * 3),
+        ("lower_left", C.c_double * 3),
+        ("bottom_unit", C.c_double * 3),
+        ("bottom_length", C.c_double),
+        ("side_length", C.c_double),
+    ]
+
+
+class Explicit(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("x", _dp),
+        ("vol", _dp),
+        ("rho", _dp),
+        ("K", _dp),
+        ("mu", _dp),
+        ("row", _i64p),
+        ("col", _i32p),
+        ("influence", C.c_int),
+        ("horizon", C.c_double),
+        ("damage_on", C.c_int),
+        ("s_c", _dp),
+        ("contact_on", C.c_int),
+        ("r_search", C.c_double),
+        ("search_freq", C.c_int),
+        ("r_contact", C.c_double),
+        ("k_spring", C.c_double),
+        ("friction", C.c_double),
+        ("contact_horizon", _dp),
+        ("bc_mask", _u8p),
+        ("bc_a", _dp),
+        ("bc_b", _dp),
+        ("dt", C.c_double),
+        ("t0", C.c_double),
+        ("nsteps", C.c_int),
+    ]
+
+
+_lib = None
+_ref = None
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the oracle (and oracle/_ref when the reference tree exists)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.pdo_influence.restype = C.c_double
+        L.pdo_influence.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.pdo_plane_cuts_bond.argtypes = [C.POINTER(Plane), _dp, _dp]
+        L.pdo_neighbor_count.restype = C.c_int64
+        L.pdo_neighbor_count.argtypes = [C.c_int64, _dp, _dp, C.POINTER(Plane), C.c_int, _i32p]
+        L.pdo_neighbor_fill.argtypes = [C.c_int64, _dp, _dp, C.POINTER(Plane), C.c_int, _i64p, _i32p]
+        L.pdo_weighted_volume.argtypes = [C.c_int64, _dp, _dp, _i64p, _i32p, C.c_int, C.c_double, _dp]
+        L.pdo_damage_critical_stretch.argtypes = [C.c_int64, _dp, _dp, _i64p, _i32p, _dp, _dp, _dp, _dp]
+        L.pdo_dilatation.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, C.c_int, C.c_double, _dp]
+        L.pdo_force_lps.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp, _dp,
+                                    C.c_int, C.c_double, _dp]
+        L.pdo_critical_time_step.restype = C.c_double
+        L.pdo_critical_time_step.argtypes = [C.c_int64, _dp, _dp, _i64p, _i32p, _dp, _dp, C.c_double]
+        L.pdo_contact_count.restype = C.c_int64
+        L.pdo_contact_count.argtypes = [C.c_int64, _dp, C.c_double, _i64p, _i32p, _i32p]
+        L.pdo_contact_fill.argtypes = [C.c_int64, _dp, C.c_double, _i64p, _i32p, _i64p, _i32p]
+        L.pdo_contact_force.argtypes = [C.c_int64, _dp, _dp, _dp, _i64p, _i32p, C.c_double, C.c_double,
+                                        C.c_double, _dp, _dp]
+        L.pdo_explicit_run.argtypes = [C.POINTER(Explicit), _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own compiled LPS kernels, or None when not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_PATH):
+            return None
+        L = C.CDLL(REF_PATH)
+        L.pdref_set_influence.argtypes = [C.c_char_p]
+        L.pdref_weighted_volume.argtypes = [_dp, _dp, _dp, C.c_int, _i32p, C.c_double]
+        L.pdref_dilatation.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_int, C.c_double]
+        L.pdref_force_linear_elastic.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_int,
+                                                 C.c_double, C.c_double, C.c_double]
+        _ref = L
+    return _ref
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i64(a):
+    return a.ctypes.data_as(_i64p)
+
+
+def _i32(a):
+    return a.ctypes.data_as(_i32p)
+
+
+def _f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None:
+        assert a.size == n, (a.size, n)
+    return a
+
+
+def _per_point(v, n):
+    a = np.asarray(v, dtype=np.float64)
+    if a.ndim == 0:
+        a = np.full(n, float(a))
+    return np.ascontiguousarray(a)
+
+
+# ---------------------------------------------------------------------------
+# Neighbor-list formats
+# ---------------------------------------------------------------------------
+def csr_to_nl(row, col):
+    """CSR -> Peridigm's flattened list [n_0, j.., n_1, j..] (NeighborhoodData.hpp:56)."""
+    n = len(row) - 1
+    counts = np.diff(row)
+    out = np.empty(n + len(col), dtype=np.int32)
+    pos = np.arange(n) + row[:-1]
+    out[pos] = counts
+    mask = np.ones(len(out), dtype=bool)
+    mask[pos] = False
+    out[mask] = col
+    return out
+
+
+def nl_to_csr(nl, n):
+    nl = np.asarray(nl, dtype=np.int64)
+    row = np.zeros(n + 1, dtype=np.int64)
+    cols = []
+    k = 0
+    for i in range(n):
+        c = int(nl[k])
+        cols.append(nl[k + 1:k + 1 + c])
+        row[i + 1] = row[i] + c
+        k += c + 1
+    col = np.concatenate(cols).astype(np.int32) if cols else np.zeros(0, np.int32)
+    return row, col
+
+
+def planes_array(planes):
+    if not planes:
+        return None, 0
+    arr = (Plane * len(planes))()
+    for k, p in enumerate(planes):
+        arr[k].normal[:] = list(p["normal"])
+        arr[k].lower_left[:] = list(p["lower_left"])
+        arr[k].bottom_unit[:] = list(p["bottom_unit"])
+        arr[k].bottom_length = float(p["bottom_length"])
+        arr[k].side_length = float(p["side_length"])
+    return arr, len(planes)
+
+
+# ---------------------------------------------------------------------------
+# Wrappers
+# ---------------------------------------------------------------------------
+def neighbor_search(x, horizon, planes=None):
+    x = _f64(x)
+    n = x.size // 3
+    h = _per_point(horizon, n)
+    parr, npl = planes_array(planes)
+    counts = np.zeros(n, dtype=np.int32)
+    L = lib()
+    L.pdo_neighbor_count(n, _d(x), _d(h), parr, npl, _i32(counts))
+    row = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(counts, out=row[1:])
+    col = np.zeros(int(row[-1]), dtype=np.int32)
+    L.pdo_neighbor_fill(n, _d(x), _d(h), parr, npl, _i64(row), _i32(col))
+    return row, col
+
+
+def weighted_volume(x, vol, row, col, horizon, influence=0):
+    x, vol = _f64(x), _f64(vol)
+    n = vol.size
+    m = np.zeros(n)
+    lib().pdo_weighted_volume(n, _d(x), _d(vol), _i64(row), _i32(col), influence, horizon, _d(m))
+    return m
+
+
+def damage_critical_stretch(x, y, row, col, s_c, dmg_n):
+    x, y = _f64(x), _f64(y)
+    n = x.size // 3
+    sc = _per_point(s_c, n)
+    dn = _f64(dmg_n)
+    dnp1 = dn.copy()
+    nd = np.zeros(n)
+    lib().pdo_damage_critical_stretch(n, _d(x), _d(y), _i64(row), _i32(col), _d(sc), _d(dn), _d(dnp1), _d(nd))
+    return dnp1, nd
+
+
+def dilatation(x, y, m, vol, dmg, row, col, horizon, influence=0):
+    x, y, m, vol, dmg = _f64(x), _f64(y), _f64(m), _f64(vol), _f64(dmg)
+    n = vol.size
+    th = np.zeros(n)
+    lib().pdo_dilatation(n, _d(x), _d(y), _d(m), _d(vol), _d(dmg), _i64(row), _i32(col), influence, horizon, _d(th))
+    return th
+
+
+def force_lps(x, y, m, vol, theta, dmg, row, col, K, mu, horizon, influence=0):
+    x, y, m, vol, theta, dmg = map(_f64, (x, y, m, vol, theta, dmg))
+    n = vol.size
+    Kp, mup = _per_point(K, n), _per_point(mu, n)
+    f = np.zeros(3 * n)
+    lib().pdo_force_lps(n, _d(x), _d(y), _d(m), _d(vol), _d(theta), _d(dmg), _i64(row), _i32(col),
+                        _d(Kp), _d(mup), influence, horizon, _d(f))
+    return f
+
+
+def eval_model(x, y, vol, row, col, K, mu, horizon, s_c=None, dmg_n=None, influence=0, m=None):
+    """ModelEvaluator::evalModel order (Peridigm_ModelEvaluator.cpp:57-131): damage -> dilatation -> force."""
+    n = len(vol)
+    if m is None:
+        m = weighted_volume(x, vol, row, col, horizon, influence)
+    if dmg_n is None:
+        dmg_n = np.zeros(len(col))
+    if s_c is not None:
+        dmg, nd = damage_critical_stretch(x, y, row, col, s_c, dmg_n)
+    else:
+        dmg, nd = np.asarray(dmg_n, dtype=np.float64).copy(), None
+    th = dilatation(x, y, m, vol, dmg, row, col, horizon, influence)
+    f = force_lps(x, y, m, vol, th, dmg, row, col, K, mu, horizon, influence)
+    return {"m": m, "theta": th, "force": f, "bond_damage": dmg, "damage": nd}
+
+
+def critical_time_step(x, vol, row, col, K, rho, horizon):
+    x, vol = _f64(x), _f64(vol)
+    n = vol.size
+    return lib().pdo_critical_time_step(n, _d(x), _d(vol), _i64(row), _i32(col), _d(_per_point(K, n)),
+                                        _d(_per_point(rho, n)), horizon)
+
+
+def contact_search(y, r_search, brow, bcol):
+    y = _f64(y)
+    n = y.size // 3
+    counts = np.zeros(n, dtype=np.int32)
+    L = lib()
+    L.pdo_contact_count(n, _d(y), r_search, _i64(brow), _i32(bcol), _i32(counts))
+    crow = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(counts, out=crow[1:])
+    ccol = np.zeros(int(crow[-1]), dtype=np.int32)
+    L.pdo_contact_fill(n, _d(y), r_search, _i64(brow), _i32(bcol), _i64(crow), _i32(ccol))
+    return crow, ccol
+
+
+def contact_force(y, v, vol, crow, ccol, r_contact, k_spring, horizon, friction=0.0):
+    y, v, vol = _f64(y), _f64(v), _f64(vol)
+    n = vol.size
+    fc = np.zeros(3 * n)
+    lib().pdo_contact_force(n, _d(y), _d(v), _d(vol), _i64(crow), _i32(ccol), r_contact, k_spring, friction,
+                            _d(_per_point(horizon, n)), _d(fc))
+    return fc
+
+
+def explicit_run(prob, u, v, bond_damage=None):
+    """Peridigm::executeExplicit restated (Peridigm.cpp:1290-1593).
+
+    ``prob`` keys: x, vol, rho, K, mu, row, col, horizon, dt, nsteps; optional
+    influence, s_c (enables damage), contact dict {r_search, freq, r_contact,
+    k_spring, friction, horizon}, bc_mask/bc_a/bc_b, t0.
+    """
+    x = _f64(prob["x"])
+    n = x.size // 3
+    keep = []
+
+    def arr(a):
+        a = np.ascontiguousarray(a)
+        keep.append(a)
+        return a
+
+    vol = arr(_f64(prob["vol"]))
+    row = arr(np.asarray(prob["row"], np.int64))
+    col = arr(np.asarray(prob["col"], np.int32))
+    P = Explicit()
+    P.n = n
+    P.x = _d(arr(x))
+    P.vol = _d(vol)
+    P.rho = _d(arr(_per_point(prob["rho"], n)))
+    P.K = _d(arr(_per_point(prob["K"], n)))
+    P.mu = _d(arr(_per_point(prob["mu"], n)))
+    P.row = _i64(row)
+    P.col = _i32(col)
+    P.influence = int(prob.get("influence", 0))
+    P.horizon = float(prob["horizon"])
+    sc = prob.get("s_c")
+    P.damage_on = 1 if sc is not None else 0
+    P.s_c = _d(arr(_per_point(sc if sc is not None else 0.0, n)))
+    ct = prob.get("contact")
+    P.contact_on = 1 if ct else 0
+    if ct:
+        P.r_search = ct["r_search"]
+        P.search_freq = int(ct["freq"])
+        P.r_contact = ct["r_contact"]
+        P.k_spring = ct["k_spring"]
+        P.friction = ct.get("friction", 0.0)
+        P.contact_horizon = _d(arr(_per_point(ct["horizon"], n)))
+    if prob.get("bc_mask") is not None:
+        P.bc_mask = arr(np.asarray(prob["bc_mask"], np.uint8)).ctypes.data_as(_u8p)
+        P.bc_a = _d(arr(_f64(prob["bc_a"])))
+        P.bc_b = _d(arr(_f64(prob["bc_b"])))
+    P.dt = float(prob["dt"])
+    P.t0 = float(prob.get("t0", 0.0))
+    P.nsteps = int(prob["nsteps"])
+    u = _f64(u).copy()
+    v = _f64(v).copy()
+    a = np.zeros(3 * n)
+    f = np.zeros(3 * n)
+    fc = np.zeros(3 * n)
+    th = np.zeros(n)
+    nd = np.zeros(n)
+    bd = np.zeros(len(col)) if bond_damage is None else _f64(bond_damage).copy()
+    lib().pdo_explicit_run(C.byref(P), _d(u), _d(v), _d(a), _d(f), _d(fc), _d(th), _d(nd), _d(bd))
+    return {"u": u, "v": v, "a": a, "force": f, "contact_force": fc, "theta": th, "damage": nd,
+            "bond_damage": bd}
+
+
+# ---------------------------------------------------------------------------
+# Reference kernels (compiled from the reference's sources)
+# ---------------------------------------------------------------------------
+def ref_eval(x, y, vol, nl, n, K, mu, horizon, bond_damage=None):
+    """computeWeightedVolume + computeDilatation + computeInternalForceLinearElastic
+    exactly as ElasticMaterial::initialize/computeForce call them
+    (Peridigm_ElasticMaterial.cpp:137, :170-171)."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libpdref.so is not built")
+    x, y, vol = _f64(x), _f64(y), _f64(vol)
+    nl = np.ascontiguousarray(nl, dtype=np.int32)
+    nb = len(nl) - n
+    dmg = np.zeros(nb) if bond_damage is None else _f64(bond_damage)
+    m = np.zeros(n)
+    th = np.zeros(n)
+    f = np.zeros(3 * n)
+    L.pdref_weighted_volume(_d(x), _d(vol), _d(m), n, _i32(nl), horizon)
+    L.pdref_dilatation(_d(x), _d(y), _d(m), _d(vol), _d(dmg), _d(th), _i32(nl), n, horizon)
+    L.pdref_force_linear_elastic(_d(x), _d(y), _d(m), _d(vol), _d(th), _d(dmg), _d(f), _i32(nl), n, K, mu,
+                                 horizon)
+    return {"m": m, "theta": th, "force": f}

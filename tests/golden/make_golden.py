@@ -1,0 +1,247 @@
+"""Generate the golden fixtures in tests/golden/ from the reference tree.
+
+Run in a container that holds the reference source tree (default
+/root/reference, override with PERIDIGM_REF):
+
+    python tests/golden/make_golden.py
+
+It reads the reference's unit-test known answers and the gold Exodus (netCDF
+classic) files of its verification/regression tests, and writes small .npz /
+.json fixtures. Nothing at test time reads the reference tree; the fixtures
+are committed.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+from scipy.io import netcdf_file
+
+REF = os.environ.get("PERIDIGM_REF", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def _names(nc, key):
+    if key not in nc.variables:
+        return []
+    return [b"".join(r).decode().strip() for r in nc.variables[key][:]]
+
+
+def read_exodus_results(path):
+    nc = netcdf_file(path, "r", mmap=False)
+    res = {"time": np.array(nc.variables["time_whole"][:], dtype=np.float64)}
+    res["x"] = np.stack([nc.variables["coordx"][:], nc.variables["coordy"][:], nc.variables["coordz"][:]], 1)
+    for k, nm in enumerate(_names(nc, "name_nod_var")):
+        res[nm] = np.array(nc.variables["vals_nod_var%d" % (k + 1)][:], dtype=np.float64)
+    for k, nm in enumerate(_names(nc, "name_elem_var")):
+        res[nm] = np.array(nc.variables["vals_elem_var%deb1" % (k + 1)][:], dtype=np.float64)
+    nc.close()
+    return res
+
+
+# ---------------------------------------------------------------------------
+# 1. ElasticMaterial unit tests (src/materials/unit_test/utPeridigm_ElasticMaterial.cpp)
+# ---------------------------------------------------------------------------
+def unit_elastic():
+    cases = {}
+    # testTwoPts :78-187
+    cases["two_pts"] = {
+        "x": [0.0, 0.0, 0.0, 1.0, 0.0, 0.0],
+        "y": [0.0, 0.0, 0.0, 2.0, 0.0, 0.0],
+        "vol": [1.0, 1.0],
+        "nl": [1, 1, 1, 0],
+        "K": 130.0e9, "mu": 78.0e9, "horizon": 10.0,
+        "m": [1.0, 1.0], "m_tol": 1e-15,
+        "theta": [3.0, 3.0], "theta_tol": 1e-15,
+        "force": [2.34e12, 0, 0, -2.34e12, 0, 0], "force_tol": 1e-2,
+    }
+    # testEightPts :189-454: unit cube corners, z compressed to 0.98.
+    x8 = [0, 0, 0, 0, 0, 1, 0, 1, 0, 0, 1, 1, 1, 0, 0, 1, 0, 1, 1, 1, 0, 1, 1, 1]
+    y8 = [0, 0, 0, 0, 0, .98, 0, 1, 0, 0, 1, .98, 1, 0, 0, 1, 0, .98, 1, 1, 0, 1, 1, .98]
+    nl8 = []
+    for i in range(8):
+        nl8.append(7)
+        nl8.extend(j for j in range(8) if j != i)
+    # hand solution on cell 0 (:355-405): t = (|y|-|x|)*9.75e10, factor 2
+    f = [0.0, 0.0, 0.0]
+    for (t, uvec) in [
+        ((0.98 - 1.0) * 9.75e10, (0.0, 0.0, 1.0)),
+        ((math.sqrt(1.0 + 0.98 * 0.98) - math.sqrt(2.0)) * 9.75e10,
+         (0.0, 1.0 / math.sqrt(1.0 + 0.98 * 0.98), 0.98 / math.sqrt(1.0 + 0.98 * 0.98))),
+        ((math.sqrt(1.0 + 0.98 * 0.98) - math.sqrt(2.0)) * 9.75e10,
+         (1.0 / math.sqrt(1.0 + 0.98 * 0.98), 0.0, 0.98 / math.sqrt(1.0 + 0.98 * 0.98))),
+        ((math.sqrt(2.0 + 0.98 * 0.98) - math.sqrt(3.0)) * 9.75e10,
+         (1.0 / math.sqrt(2.0 + 0.98 * 0.98), 1.0 / math.sqrt(2.0 + 0.98 * 0.98),
+          0.98 / math.sqrt(2.0 + 0.98 * 0.98))),
+    ]:
+        for k in range(3):
+            f[k] += 2.0 * uvec[k] * t
+    # signs per cell (:409-449)
+    signs = [(1, 1, 1), (1, 1, -1), (1, -1, 1), (1, -1, -1), (-1, 1, 1), (-1, 1, -1), (-1, -1, 1), (-1, -1, -1)]
+    f8 = []
+    for s in signs:
+        f8.extend(s[k] * f[k] for k in range(3))
+    cases["eight_pts"] = {
+        "x": x8, "y": y8, "vol": [1.0] * 8, "nl": nl8,
+        "K": 130.0e9, "mu": 78.0e9, "horizon": 10.0,
+        "m": [12.0] * 8, "m_tol": 1e-12,
+        "theta": [-0.01991593994643333] * 8, "theta_tol": 1e-12,
+        "force": f8, "force_tol": 1e-11,
+    }
+    # testThreePts :456-664
+    V = [0.9, 1.1, 0.8]
+    t01 = (-2753550531.144094, -1510011581.595148, -621769474.7744727)
+    t10 = (3398655528.6806289, 1863778838.308732, 767438345.18594845)
+    t02 = (7736514797.0571524, 15402697641.41379, -11956431959.088315)
+    t20 = (-8687228655.850972, -17295482505.73966, 13425717013.587864)
+    t12 = (5110873051.7924152, -1252163897.689138, 6133047662.15088)
+    t21 = (-4649613866.523322, 1139155397.2982139, -5579536639.827986)
+    f3 = []
+    f3 += [t01[k] * V[1] - t10[k] * V[1] + t02[k] * V[2] - t20[k] * V[2] for k in range(3)]
+    f3 += [t10[k] * V[0] - t01[k] * V[0] + t12[k] * V[2] - t21[k] * V[2] for k in range(3)]
+    f3 += [t20[k] * V[0] - t02[k] * V[0] + t21[k] * V[1] - t12[k] * V[1] for k in range(3)]
+    cases["three_pts"] = {
+        "x": [1.1, 2.6, -0.1, -2.0, 0.9, -0.3, 0.0, 0.01, 1.8],
+        "y": [1.2, 2.4, -0.1, -1.9, 0.7, -0.8, 0.1, 0.21, 1.6],
+        "vol": V, "nl": [2, 1, 2, 2, 0, 2, 2, 0, 1],
+        "K": 130.0e9, "mu": 78.0e9, "horizon": 10.0,
+        "m": [23.016479999999931, 18.64767999999997, 20.497599999999963], "m_tol": 1e-12,
+        "theta": [-0.114127034572639, 0.08257537372985, -0.12166177890553], "theta_tol": 1e-11,
+        "force": f3, "force_tol": 1e-10,
+    }
+    with open(os.path.join(OUT, "unit_elastic.json"), "w") as fh:
+        json.dump(cases, fh, indent=1)
+
+
+# ---------------------------------------------------------------------------
+# 2. QuickGrid decks (PdQuickGrid discretization, QuickGrid.cxx:160-169,394-409,596-611)
+# ---------------------------------------------------------------------------
+def _cell_nbhd(cell, horizon, ncells):
+    d = horizon / cell
+    n = int(d)
+    if abs(d - n) >= 0.5:
+        n += 1
+    return min(n, ncells)
+
+
+def quickgrid(origin, length, npts, horizon, spherical):
+    """Cell centres, cell volumes and the neighbor list of a PdQuickGrid
+    tensor-product mesh: box neighborhood (NoOpNormFunction) by default,
+    strict d^2 < r^2 for "Spherical"."""
+    cells = [length[k] / npts[k] for k in range(3)]
+    axes = [[origin[k] + cells[k] / 2 + i * cells[k] for i in range(npts[k])] for k in range(3)]
+    nC = [_cell_nbhd(cells[k], horizon, npts[k]) for k in range(3)]
+    nx, ny, nz = npts
+    x, nl = [], []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                x.append((axes[0][i], axes[1][j], axes[2][k]))
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                nb = []
+                p = (axes[0][i], axes[1][j], axes[2][k])
+                for kk in range(max(0, k - nC[2]), min(nz, k + nC[2] + 1)):
+                    for jj in range(max(0, j - nC[1]), min(ny, j + nC[1] + 1)):
+                        for ii in range(max(0, i - nC[0]), min(nx, i + nC[0] + 1)):
+                            if (ii, jj, kk) == (i, j, k):
+                                continue
+                            q = (axes[0][ii], axes[1][jj], axes[2][kk])
+                            if spherical:
+                                dx, dy, dz = q[0] - p[0], q[1] - p[1], q[2] - p[2]
+                                if not (dx * dx + dy * dy + dz * dz - horizon * horizon < 0.0):
+                                    continue
+                            nb.append(ii + jj * nx + kk * nx * ny)
+                nl.append(len(nb))
+                nl.extend(nb)
+    vol = cells[0] * cells[1] * cells[2]
+    return np.array(x), np.full(len(x), vol), np.array(nl, dtype=np.int32)
+
+
+def bond_breaking():
+    d = os.path.join(REF, "test/verification/BondBreakingInitialVelocity")
+    g = read_exodus_results(os.path.join(d, "BondBreakingInitialVelocity_gold.e"))
+    x, vol, nl = quickgrid((0.0, 0.0, 0.0), (2.1, 2.0, 1.0), (2, 2, 1), 0.51, spherical=False)
+    assert np.allclose(x, g["x"])
+    v0 = np.zeros(12)
+    # Node Set k = "k+1" (1-based point ids); y velocities from the deck.
+    for pid, val in [(0, -244.939), (1, -244.959), (2, 244.939), (3, 244.959)]:
+        v0[3 * pid + 1] = val
+    np.savez_compressed(
+        os.path.join(OUT, "bond_breaking.npz"), x=x, vol=vol, nl=nl, v0=v0,
+        params=np.array([7800.0, 130.0e9, 60.0e9, 0.51, 0.02, 1.0e-8, 8.0e-5]),
+        time=g["time"], disp_y=g["DisplacementY"], vel_y=g["VelocityY"], damage=g["Damage"],
+        weighted_volume=g["Weighted_Volume"], dilatation=g["Dilatation"])
+
+
+def contact_2x1x1():
+    d = os.path.join(REF, "test/verification/Contact_2x1x1")
+    g = read_exodus_results(os.path.join(d, "Contact_2x1x1_gold.e"))
+    x, vol, nl = quickgrid((-2.0, -0.5, -0.5), (4.0, 1.0, 1.0), (2, 1, 1), 1.0, spherical=True)
+    assert np.allclose(x, g["x"])
+    v0 = np.array([1.0, 0, 0, -1.0, 0, 0])
+    np.savez_compressed(
+        os.path.join(OUT, "contact_2x1x1.npz"), x=x, vol=vol, nl=nl, v0=v0,
+        # density, K, mu, horizon, search radius, freq, contact radius, spring, dt, final time
+        params=np.array([7.8e-3, 130.0e3, 78.0e3, 1.0, 5.0, 100, 2.0, 1950.0e3, 4.150386640644e-8,
+                         4.150386640644e-5]),
+        time=g["time"], disp_x=g["DisplacementX"], vel_x=g["VelocityX"])
+
+
+# ---------------------------------------------------------------------------
+# 3. WaveInBar (Exodus hex mesh -> centroid/volume points, Peridigm_GeometryUtils.cpp:69-)
+# ---------------------------------------------------------------------------
+def _tet_volume(a, b, c, d):
+    return abs(np.dot(b - a, np.cross(c - a, d - a))) / 6.0
+
+
+def hex_volume(P):
+    """Volume of a hexahedron from 24 tetrahedra on face barycentres and the
+    body barycentre (the decomposition Peridigm_GeometryUtils.cpp:69-380 uses)."""
+    faces = [(0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (0, 4, 7, 3), (0, 3, 2, 1), (4, 5, 6, 7)]
+    fc = [P[list(f)].mean(0) for f in faces]
+    c = 0.5 * (fc[4] + fc[5])
+    v = 0.0
+    for f, cf in zip(faces, fc):
+        for k in range(4):
+            v += _tet_volume(P[f[k]], P[f[(k + 1) % 4]], cf, c)
+    return v
+
+
+def wave_in_bar():
+    d = os.path.join(REF, "test/regression/WaveInBar")
+    g = netcdf_file(os.path.join(d, "WaveInBar.g"), "r", mmap=False)
+    X = np.stack([g.variables["coordx"][:], g.variables["coordy"][:], g.variables["coordz"][:]], 1).astype(np.float64)
+    conn = np.array(g.variables["connect1"][:]) - 1
+    ns = np.array(g.variables["node_ns1"][:]) - 1
+    g.close()
+    vol = np.array([hex_volume(X[c]) for c in conn])
+    in_set = set(ns.tolist())
+    # Exodus node sets become the elements that contain one of their nodes
+    # (Peridigm_ExodusDiscretization.cpp:557-566).
+    elems = np.array([e for e, c in enumerate(conn) if any(int(k) in in_set for k in c)], dtype=np.int32)
+    r = read_exodus_results(os.path.join(d, "WaveInBar_gold.e"))
+    keep = [0, 1, 6, 11]
+    out = dict(x=r["x"], vol=vol, initial_velocity_points=elems,
+               # density, K, mu, horizon, dt, final time, output frequency
+               params=np.array([2200.0, 14.90e9, 8.94e9, 0.00601, 9.0659e-08, 0.00002, 20]),
+               time=r["time"][keep], keep=np.array(keep))
+    for nm in ["DisplacementX", "DisplacementY", "DisplacementZ", "VelocityX", "VelocityY", "VelocityZ",
+               "Force_DensityX", "Force_DensityY", "Force_DensityZ", "Dilatation", "Weighted_Volume"]:
+        out[nm] = r[nm][keep]
+    np.savez_compressed(os.path.join(OUT, "wave_in_bar.npz"), **out)
+
+
+def main():
+    unit_elastic()
+    bond_breaking()
+    contact_2x1x1()
+    wave_in_bar()
+    print("fixtures written to", OUT)
+
+
+if __name__ == "__main__":
+    main()
