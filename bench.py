@@ -1,0 +1,293 @@
+"""Benchmark: bond evaluations per second of the explicit LPS + critical-stretch
+step on the notched-plate workload (400x200x4 = 320,000 points, h = 0.5 mm,
+jitter +-0.05h seed 1, delta = 3.015h, s_c = 5e-4, +-2 m/s prescribed pulls).
+
+One bench step = one velocity-Verlet step: damage + dilatation pass, force
+pass with the Verlet epilogue, over every bond. value = bonds x steps /
+device time (CUDA events on the library's stream, max over ranks, summed over
+ranks for N > 1: each rank runs its own plate, weak scaling).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bond evals/s per explicit step, split-FP32 vs FP64 (1 B200); QS time to 1e-8 res"
+UNIT = "bond evals/s"
+
+
+def algorithmic_bytes(nb, n, precision="split"):
+    """Bytes each bond pass must move at minimum with this layout (one launch).
+
+    Per bond, both passes: col (4 B) + bond damage (1 B).
+    Per point, dilatation pass: row 8, xv 32, state 24, m 8, owner coefficients 8,
+    s_c 8, horizon 8, writes A/B 8, theta 8, node damage 8  -> 120 B.
+    Per point, force pass: row 8, xv 32, state 32, rho 8, horizon 8, v read+write 48,
+    next state 24, acceleration 24, BC mask 1 -> 185 B.
+    FP64 path: the gathered owner terms are FP64 (ab64, 32 B/point read in the
+    force pass, written in the dilatation pass)."""
+    if precision == "split":
+        return {"dilatation": 5 * nb + 120 * n, "force": 5 * nb + 185 * n}
+    return {"dilatation": 5 * nb + 144 * n, "force": 5 * nb + 217 * n}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [q.strip() for q in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    """The reference's own CPU implementation of the step (oracle/_ref: its
+    computeDilatation + computeInternalForceLinearElastic compiled from source,
+    with the restated critical-stretch damage and Verlet loops) on all host
+    cores, over a bounded sample of the workload: the left 100 columns of the
+    notched plate (80,000 points, the notch included)."""
+    if rank != 0:
+        return
+    from oracle import cpu_baseline
+    from oracle import oracle as O
+    from peridigm_b200 import workloads
+
+    O.build()
+    w = workloads.notched_plate(nx=100)
+    row, col = O.neighbor_search(w["x"], w["horizon"], w["planes"])
+    r = cpu_baseline.run(w, row, col, steps=args.steps, warmup=args.warmup)
+    value = r["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "notched_plate_100x200x4 (sample of notched_plate_400x200x4)",
+                       "points": int(len(w["vol"])), "bonds": int(len(col)), "precision": "fp64"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": f"{args.steps} explicit steps of a 100x200x4 slab of the plate "
+                                       f"({len(col)} bonds), {r['cores']} processes"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_setup(args.gpus)
+
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+
+    # CPU baseline processes are spawned before any CUDA call in this process.
+    from peridigm_b200 import Context, workloads
+
+    w = workloads.notched_plate()
+    n = int(len(w["vol"]))
+
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    def max_over_ranks(v):
+        if pg is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    ctx = Context(device=local, precision="split")
+    workloads.setup_context(ctx, w)
+    nb = ctx.num_bonds()
+    dt = 0.7 * ctx.critical_time_step()
+
+    # ---- value: split-FP32 explicit steps, state resident in HBM -----------
+    ctx.verlet_run(dt, args.warmup)
+    t_done = args.warmup * dt
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    st = ctx.verlet_run(dt, args.steps, t0=t_done)
+    barrier()
+    clk = clocks.stop()
+    t_done += args.steps * dt
+    ms = max_over_ranks(st["device_ms"])
+    value = world * nb * args.steps / (ms / 1e3)
+
+    # ---- per-kernel launch durations (CUDA events around each launch) -------
+    ksteps = min(args.steps, 500)
+    ctx.kernel_timing(True)
+    ctx.verlet_run(dt, ksteps, t0=t_done)
+    kt = ctx.kernel_times()
+    ctx.kernel_timing(False)
+    t_done += ksteps * dt
+    per = {"dilatation": kt["dilatation_ms"] / kt["evaluations"], "force": kt["force_ms"] / kt["evaluations"]}
+    dom = max(per, key=per.get)
+    algo = algorithmic_bytes(nb, n, "split")
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        hbm, peak_src = 6650.0, "fallback"
+    achieved = algo[dom] / (per[dom] / 1e3) / 1e9
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = tr.get("split", {}).get(dom)
+    except (OSError, ValueError):
+        pass
+    roofline = {"bound": "hbm", "kernel": f"k_{dom}_split", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic,
+                "algorithmic_bytes": algo[dom], "launch_ms": per[dom],
+                "per_kernel_ms": per}
+
+    # ---- plain FP64 path, same workload --------------------------------------
+    fsteps = min(args.steps, 1000)
+    c64 = Context(device=local, precision="fp64")
+    workloads.setup_context(c64, w)
+    c64.verlet_run(dt, args.warmup)
+    barrier()
+    st64 = c64.verlet_run(dt, fsteps, t0=args.warmup * dt)
+    barrier()
+    ms64 = max_over_ranks(st64["device_ms"])
+    value64 = world * nb * fsteps / (ms64 / 1e3)
+    c64.close()
+
+    # ---- e2e: the drop-in computeForce call with host buffers ---------------
+    # Each step: H2D of the current coordinates from pinned memory, damage +
+    # dilatation + force on the device, D2H of the force density.
+    esteps = min(args.steps, 500)
+    y = torch.from_numpy(ctx.field("Coordinates")).pin_memory()
+    f = torch.zeros(3 * n, dtype=torch.float64).pin_memory()
+    import ctypes as C
+
+    yp = C.cast(y.data_ptr(), C.POINTER(C.c_double))
+    fp = C.cast(f.data_ptr(), C.POINTER(C.c_double))
+    for _ in range(3):
+        ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(esteps):
+        ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": world * nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+           "d2h_bytes_per_step": 24 * n, "steps": esteps, "api": "pd_compute_force (host y in, host force out)"}
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import cpu_baseline
+        from oracle import oracle as O
+
+        row, col = ctx.bonds_csr()
+        O.build()
+        r = cpu_baseline.run(w, row, col, steps=40, dt=dt)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+               "sample": f"{r['steps']} explicit steps of the full 400x200x4 plate on {r['cores']} processes "
+                         f"(slabs with ghost layers, reference LPS kernels compiled from source)"}
+    ctx.close()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
+            "config": {"workload": "notched_plate_400x200x4", "points": n, "bonds": nb, "horizon_over_h": 3.015,
+                       "critical_stretch": 5e-4, "dt": dt, "precision": "split_fp32",
+                       "l2": "inputs larger than L2 (about 220 MB touched per step vs 126 MB L2)",
+                       "parallelism": f"replicas x{world}"},
+            "fp64": {"value": value64, "unit": UNIT, "steps": fsteps, "ms_per_step": ms64 / fsteps,
+                     "split_over_fp64": value / value64},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 2 * args.steps}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

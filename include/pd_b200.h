@@ -1,0 +1,197 @@
+/*
+ * pd_b200.h -- C ABI of the B200-native Peridigm hot path.
+ *
+ * The library replaces, behind plain C entry points, the per-bond force and
+ * damage path of Peridigm: the "Elastic" (LPS) material, the "Critical
+ * Stretch" damage model, the "Short Range Force" contact model, the
+ * velocity-Verlet explicit integrator and the quasi-static Newton/CG solve.
+ * All compute runs in hand-written sm_100a CUDA kernels; there is no CPU path.
+ *
+ * Conventions
+ *  - Every function returns an int status (PD_OK == 0). No exception crosses
+ *    the ABI; pd_last_error() gives a one-line message for the last failure.
+ *  - Point arrays are in the caller's order and interleaved xyz (3*i+k), as
+ *    Peridigm's Epetra vectors are. Host pointers are copied in/out; the
+ *    *_device variants take device pointers on the context's device.
+ *  - Bond families: Peridigm's flattened neighbor list [n_0, j.., n_1, j..]
+ *    (src/core/Peridigm_NeighborhoodData.hpp:56-140) or a search done here.
+ *    Bond-ordered data (bond damage) follows that list's order.
+ *  - Force outputs are force densities, as Material::computeForce produces
+ *    (multiply by volume for forces, src/core/Peridigm.cpp:1881-1884).
+ *  - The context owns its device memory. One context per host thread at a
+ *    time; contexts are independent.
+ */
+#ifndef PD_B200_H
+#define PD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PD_OK 0
+#define PD_ERR_ARG 1         /* bad argument (Teuchos TEST_FOR_EXCEPT in the reference) */
+#define PD_ERR_CUDA 2        /* CUDA runtime error */
+#define PD_ERR_NONFINITE 3   /* NaN/Inf in a force (Peridigm.cpp:1551-1566 terminate) */
+#define PD_ERR_TIMEOUT 4     /* a bounded device wait ran out */
+#define PD_ERR_STATE 5       /* call out of order (e.g. force before bonds) */
+#define PD_ERR_UNSUPPORTED 6 /* input outside what this build handles */
+#define PD_ERR_NOMEM 7       /* device allocation failed */
+#define PD_ERR_NOT_CONVERGED 8 /* solver stopped before its tolerance */
+
+/* ---- enums ------------------------------------------------------------- */
+/* Bond-kernel arithmetic. PD_FP64: every per-bond quantity in FP64, the
+ * reference's formulas in the reference's operation order. PD_SPLIT_FP32:
+ * per-bond math in FP32 with bond vectors and displacement differences formed
+ * in FP64 and rounded once; stretch as (2X.du+du.du)/(|Y|+|X|); FP64 kept for
+ * displacement/velocity state, weighted volume and reductions. */
+#define PD_FP64 0
+#define PD_SPLIT_FP32 1
+
+/* Influence functions (src/core/Peridigm_InfluenceFunction.hpp:69-87). */
+#define PD_INFLUENCE_ONE 0
+#define PD_INFLUENCE_PARABOLIC_DECAY 1
+#define PD_INFLUENCE_GAUSSIAN 2
+
+/* Output fields for pd_get_field (names of Peridigm fields). */
+#define PD_FIELD_DISPLACEMENT 0     /* "Displacement"       [3n] double */
+#define PD_FIELD_VELOCITY 1         /* "Velocity"           [3n] double */
+#define PD_FIELD_ACCELERATION 2     /* "Acceleration"       [3n] double */
+#define PD_FIELD_FORCE_DENSITY 3    /* "Force_Density" (internal + contact) [3n] double */
+#define PD_FIELD_CONTACT_FORCE 4    /* "Contact_Force_Density" [3n] double */
+#define PD_FIELD_DILATATION 5       /* "Dilatation"         [n] double */
+#define PD_FIELD_WEIGHTED_VOLUME 6  /* "Weighted_Volume"    [n] double */
+#define PD_FIELD_DAMAGE 7           /* "Damage"             [n] double */
+#define PD_FIELD_BOND_DAMAGE 8      /* "Bond_Damage"        [nb] double, neighbor-list order */
+#define PD_FIELD_COORDINATES 9      /* "Coordinates" x+u    [3n] double */
+#define PD_FIELD_NUM_NEIGHBORS 10   /* "Number_Of_Neighbors" [n] double */
+
+typedef struct pd_ctx pd_ctx;
+
+typedef struct {
+  int device;     /* CUDA device ordinal */
+  int precision;  /* PD_FP64 or PD_SPLIT_FP32 */
+  int influence;  /* PD_INFLUENCE_* */
+  int threads_per_point; /* lanes cooperating on one point's bond family: 0 = auto, else 4/8/16/32 */
+} pd_config;
+
+/* Rectangular_Plane bond filter (src/io/pdneigh/BondFilter.h:59-93 FinitePlane;
+ * parameters as parsed in src/io/discretization/Peridigm_Discretization.cpp:158-175). */
+typedef struct {
+  double normal[3];
+  double lower_left[3];
+  double bottom_unit[3];
+  double bottom_length;
+  double side_length;
+} pd_plane_filter;
+
+/* Run statistics of pd_verlet_run / pd_qs_solve. */
+typedef struct {
+  int64_t steps;          /* explicit steps taken */
+  int64_t bonds;          /* directed bonds in the family */
+  int64_t broken_bonds;   /* bonds with damage 1 at the end */
+  int64_t contact_pairs;  /* directed pairs in the last contact list */
+  double device_ms;       /* device time of the step loop (CUDA events) */
+  int64_t newton_iterations;
+  int64_t cg_iterations;
+  double final_residual;  /* relative FP64 residual of the last linear solve */
+} pd_stats;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+/* Replaces the construction done by PeridigmNS::Peridigm (src/core/Peridigm.cpp:105-792). */
+int pd_create(const pd_config* cfg, pd_ctx** out);
+int pd_destroy(pd_ctx* ctx);
+/* Message of the last failure on ctx (never NULL). */
+const char* pd_last_error(const pd_ctx* ctx);
+/* Library version string. */
+const char* pd_version(void);
+
+/* ---- discretization ----------------------------------------------------- */
+/* Points: model coordinates x[3n], cell volumes vol[n] and an optional block
+ * id per point (NULL = all block 0). Mirrors the "Model_Coordinates"/"Volume"
+ * fields a discretization hands Peridigm (Peridigm.cpp:811-930). */
+int pd_set_points(pd_ctx* ctx, int64_t n, const double* x, const double* vol, const int32_t* block);
+/* Per-block horizon (Blocks/"Horizon", one constant per block). */
+int pd_set_block_horizons(pd_ctx* ctx, int32_t n_blocks, const double* horizon);
+
+/* Bond family by search on the device: j in H(i) iff j != i, FP64
+ * dx*dx+dy*dy+dz*dz <= h_i*h_i and no plane filter cuts the bond.
+ * Replaces NeighborhoodList::buildNeighborhoodList (src/io/pdneigh/NeighborhoodList.cxx:621-761)
+ * with ZoltanSearchTree::FindPointsWithinRadius (src/io/Peridigm_ZoltanSearchTree.cpp:214-247)
+ * and FinitePlaneFilter (src/io/pdneigh/BondFilter.cxx:123-150). */
+int pd_build_bonds(pd_ctx* ctx, const pd_plane_filter* filters, int32_t n_filters);
+/* Bond family from a Peridigm neighbor list of length len (accepted verbatim). */
+int pd_set_bonds(pd_ctx* ctx, const int32_t* neighborhood_list, int64_t len);
+int pd_num_bonds(const pd_ctx* ctx, int64_t* nb);
+/* Neighbor list in Peridigm format; *len receives the length (cap may be 0 to query). */
+int pd_get_bonds(pd_ctx* ctx, int32_t* neighborhood_list, int64_t cap, int64_t* len);
+
+/* ---- material / damage -------------------------------------------------- */
+/* "Elastic" material (PeridigmNS::ElasticMaterial ctor, src/materials/Peridigm_ElasticMaterial.cpp:59-118):
+ * bulk modulus, shear modulus, density of one block. */
+int pd_material_lps(pd_ctx* ctx, int32_t block, double bulk_modulus, double shear_modulus, double density);
+/* Per-point moduli (an extension for heterogeneous bodies; the owner's values
+ * take the place of the block constants at src/materials/elastic.cxx:99,119). */
+int pd_material_lps_field(pd_ctx* ctx, const double* bulk_modulus, const double* shear_modulus);
+/* "Critical Stretch" damage (CriticalStretchDamageModel ctor, src/damage/Peridigm_CriticalStretchDamageModel.cpp:52-77)
+ * for one block; s_c < 0 disables damage on that block. */
+int pd_damage_critical_stretch(pd_ctx* ctx, int32_t block, double critical_stretch);
+/* Per-point critical stretch of the bond's owner (extension). */
+int pd_damage_critical_stretch_field(pd_ctx* ctx, const double* critical_stretch);
+
+/* ElasticMaterial::initialize -> computeWeightedVolume
+ * (Peridigm_ElasticMaterial.cpp:124-139, material_utilities.cxx:161-188,501-520).
+ * m_out may be NULL. */
+int pd_weighted_volume(pd_ctx* ctx, double* m_out);
+
+/* ModelEvaluator::evalModel for one configuration (src/core/Peridigm_ModelEvaluator.cpp:57-131):
+ * CriticalStretchDamageModel::computeDamage (Peridigm_CriticalStretchDamageModel.cpp:108-184),
+ * then ElasticMaterial::computeForce (Peridigm_ElasticMaterial.cpp:141-172:
+ * computeDilatation + computeInternalForceLinearElastic). y = current
+ * coordinates [3n] (host). Damage is trial damage (NP1) on top of the
+ * committed state (N); pd_update_state commits it. force_density_out [3n]
+ * may be NULL. */
+int pd_compute_force(pd_ctx* ctx, const double* y, double* force_density_out);
+/* Same with device pointers. */
+int pd_compute_force_device(pd_ctx* ctx, const double* y_dev, double* force_density_dev);
+/* DamageModel::computeDamage alone (Peridigm_DamageModel.hpp:107-112). */
+int pd_compute_damage(pd_ctx* ctx, const double* y);
+/* DataManager::updateState (Peridigm_DataManager.hpp:159): commit NP1 damage. */
+int pd_update_state(pd_ctx* ctx);
+/* Bond damage in neighbor-list order (doubles 0/1), in and out. */
+int pd_set_bond_damage(pd_ctx* ctx, const double* bond_damage);
+
+/* ---- explicit integration ----------------------------------------------- */
+/* ComputeCriticalTimeStep (src/core/Peridigm_CriticalTimeStep.cpp:52-130), min over points. */
+int pd_critical_time_step(pd_ctx* ctx, double* dt_out);
+/* Initial displacement / velocity (DirichletBC "Initial Displacement"/"Initial Velocity",
+ * src/core/Peridigm_BoundaryCondition.cpp:157-187). NULL leaves the field unchanged. */
+int pd_set_state(pd_ctx* ctx, const double* u, const double* v);
+/* Prescribed displacement u_c(t) = a*t + b on coordinate c of the listed points
+ * (DirichletIncrementBC, Peridigm_BoundaryCondition.cpp:202-241: each step sets
+ * v_c = (u_c(t) - u_c(t_prev)) / (t - t_prev)). */
+int pd_add_prescribed_displacement(pd_ctx* ctx, int64_t n_points, const int64_t* points, int32_t coordinate,
+                                   double a, double b);
+int pd_clear_boundary_conditions(pd_ctx* ctx);
+/* Velocity-Verlet loop of Peridigm::executeExplicit (src/core/Peridigm.cpp:1290-1593):
+ * initial evaluation at t0, then nsteps steps of size dt. State stays on the
+ * device; read it with pd_get_field. stats may be NULL. */
+int pd_verlet_run(pd_ctx* ctx, double dt, double t0, int64_t nsteps, pd_stats* stats);
+/* Reads a field (PD_FIELD_*) into host memory in the caller's order. */
+int pd_get_field(pd_ctx* ctx, int32_t field, double* out);
+
+/* ---- instrumentation ----------------------------------------------------- */
+/* Named stopwatches around the hot calls are the reference's Timer
+ * (src/core/Peridigm_Timer.hpp:77-86); here CUDA events bracket every launch
+ * of the two bond passes while enabled. ms_out[0]/[1] receive the summed
+ * device time of the dilatation (+damage) pass and of the force (+Verlet)
+ * pass since the last reset; launches_out the number of evaluations. */
+int pd_set_kernel_timing(pd_ctx* ctx, int enable);
+int pd_get_kernel_timing(pd_ctx* ctx, double* ms_out, int64_t* launches_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PD_B200_H */

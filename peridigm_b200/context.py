@@ -1,0 +1,214 @@
+"""Thin Python owner of one ``pd_ctx`` (include/pd_b200.h).
+
+Every method maps to one C entry point, converts numpy arrays to pointers and
+raises :class:`PDError` on a non-zero status, the way the reference raises
+(TEUCHOS_TEST_FOR_EXCEPT) or terminates (TEUCHOS_TEST_FOR_TERMINATION).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import PDError
+
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _f64(a, size=None, name="array"):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if size is not None and a.size != size:
+        raise ValueError(f"{name}: expected {size} values, got {a.size}")
+    return a
+
+
+class Context:
+    """One device-resident discretization (points, bond family, material, state)."""
+
+    def __init__(self, device=0, precision="split", influence="One", threads_per_point=0):
+        self.L = _lib.load()
+        cfg = _lib.Config()
+        cfg.device = int(device)
+        cfg.precision = _lib.PD_SPLIT_FP32 if precision in ("split", "split_fp32", _lib.PD_SPLIT_FP32) else _lib.PD_FP64
+        cfg.influence = {"One": 0, "Parabolic Decay": 1, "Gaussian": 2}[influence]
+        cfg.threads_per_point = int(threads_per_point)
+        h = C.c_void_p()
+        rc = self.L.pd_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise PDError(rc, "pd_create failed (no CUDA device or bad configuration)")
+        self.h = h
+        self.precision = cfg.precision
+        self.n = 0
+
+    # -- plumbing -----------------------------------------------------------
+    def _ok(self, rc):
+        if rc != 0:
+            raise PDError(rc, self.L.pd_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- discretization -----------------------------------------------------
+    def set_points(self, x, vol, block=None):
+        vol = _f64(vol, name="vol")
+        n = vol.size
+        x = _f64(x, 3 * n, "x")
+        self._keep_x = x
+        blk = None
+        if block is not None:
+            blk = np.ascontiguousarray(block, dtype=np.int32)
+            if blk.size != n:
+                raise ValueError("block: one id per point")
+        self._ok(self.L.pd_set_points(self.h, n, _d(x), _d(vol), blk.ctypes.data_as(_i32p) if blk is not None else None))
+        self.n = n
+
+    def set_horizons(self, horizons):
+        h = _f64(np.atleast_1d(horizons))
+        self._ok(self.L.pd_set_block_horizons(self.h, h.size, _d(h)))
+
+    def build_bonds(self, planes=()):
+        arr = None
+        if planes:
+            arr = (_lib.PlaneFilter * len(planes))()
+            for k, p in enumerate(planes):
+                arr[k].normal[:] = [float(v) for v in p["normal"]]
+                arr[k].lower_left[:] = [float(v) for v in p["lower_left"]]
+                arr[k].bottom_unit[:] = [float(v) for v in p["bottom_unit"]]
+                arr[k].bottom_length = float(p["bottom_length"])
+                arr[k].side_length = float(p["side_length"])
+        self._ok(self.L.pd_build_bonds(self.h, arr, len(planes)))
+
+    def set_bonds(self, neighborhood_list):
+        nl = np.ascontiguousarray(neighborhood_list, dtype=np.int32)
+        self._ok(self.L.pd_set_bonds(self.h, nl.ctypes.data_as(_i32p), nl.size))
+
+    def num_bonds(self):
+        nb = C.c_int64()
+        self._ok(self.L.pd_num_bonds(self.h, C.byref(nb)))
+        return nb.value
+
+    def get_bonds(self):
+        ln = C.c_int64()
+        self._ok(self.L.pd_get_bonds(self.h, None, 0, C.byref(ln)))
+        out = np.zeros(ln.value, dtype=np.int32)
+        self._ok(self.L.pd_get_bonds(self.h, out.ctypes.data_as(_i32p), out.size, C.byref(ln)))
+        return out
+
+    def bonds_csr(self):
+        nl = self.get_bonds()
+        n = self.n
+        counts = np.zeros(n, dtype=np.int64)
+        k = 0
+        keep = np.ones(nl.size, dtype=bool)
+        for i in range(n):
+            c = int(nl[k])
+            counts[i] = c
+            keep[k] = False
+            k += c + 1
+        row = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(counts, out=row[1:])
+        return row, nl[keep].astype(np.int32)
+
+    # -- material / damage --------------------------------------------------
+    def material(self, K, mu, rho, block=0):
+        self._ok(self.L.pd_material_lps(self.h, int(block), float(K), float(mu), float(rho)))
+
+    def material_field(self, K, mu):
+        K, mu = _f64(K, self.n, "K"), _f64(mu, self.n, "mu")
+        self._ok(self.L.pd_material_lps_field(self.h, _d(K), _d(mu)))
+
+    def critical_stretch(self, s_c, block=0):
+        self._ok(self.L.pd_damage_critical_stretch(self.h, int(block), float(s_c)))
+
+    def critical_stretch_field(self, s_c):
+        s = _f64(s_c, self.n, "s_c")
+        self._ok(self.L.pd_damage_critical_stretch_field(self.h, _d(s)))
+
+    def weighted_volume(self):
+        m = np.zeros(self.n)
+        self._ok(self.L.pd_weighted_volume(self.h, _d(m)))
+        return m
+
+    # -- evaluation -----------------------------------------------------------
+    def compute_force(self, y):
+        y = _f64(y, 3 * self.n, "y")
+        f = np.zeros(3 * self.n)
+        self._ok(self.L.pd_compute_force(self.h, _d(y), _d(f)))
+        return f
+
+    def compute_force_device(self, y_ptr, f_ptr):
+        self._ok(self.L.pd_compute_force_device(self.h, C.c_void_p(y_ptr), C.c_void_p(f_ptr)))
+
+    def compute_damage(self, y):
+        y = _f64(y, 3 * self.n, "y")
+        self._ok(self.L.pd_compute_damage(self.h, _d(y)))
+
+    def update_state(self):
+        self._ok(self.L.pd_update_state(self.h))
+
+    def set_bond_damage(self, bd):
+        bd = _f64(bd, self.num_bonds(), "bond damage")
+        self._ok(self.L.pd_set_bond_damage(self.h, _d(bd)))
+
+    # -- integration ----------------------------------------------------------
+    def critical_time_step(self):
+        dt = C.c_double()
+        self._ok(self.L.pd_critical_time_step(self.h, C.byref(dt)))
+        return dt.value
+
+    def set_state(self, u=None, v=None):
+        uu = _f64(u, 3 * self.n, "u") if u is not None else None
+        vv = _f64(v, 3 * self.n, "v") if v is not None else None
+        self._ok(self.L.pd_set_state(self.h, _d(uu) if uu is not None else None, _d(vv) if vv is not None else None))
+
+    def prescribed_displacement(self, points, coordinate, a, b=0.0):
+        p = np.ascontiguousarray(points, dtype=np.int64)
+        self._ok(self.L.pd_add_prescribed_displacement(self.h, p.size, p.ctypes.data_as(_i64p), int(coordinate),
+                                                       float(a), float(b)))
+
+    def clear_boundary_conditions(self):
+        self._ok(self.L.pd_clear_boundary_conditions(self.h))
+
+    def verlet_run(self, dt, nsteps, t0=0.0):
+        st = _lib.Stats()
+        self._ok(self.L.pd_verlet_run(self.h, float(dt), float(t0), int(nsteps), C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
+
+    def kernel_timing(self, enable=True):
+        self._ok(self.L.pd_set_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_times(self):
+        ms = np.zeros(2)
+        cnt = C.c_int64()
+        self._ok(self.L.pd_get_kernel_timing(self.h, _d(ms), C.byref(cnt)))
+        return {"dilatation_ms": ms[0], "force_ms": ms[1], "evaluations": cnt.value}
+
+    def field(self, name):
+        fid = _lib.FIELDS[name]
+        size = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 9: 3}.get(fid, 1) * self.n
+        if fid == _lib.FIELDS["Bond_Damage"]:
+            size = self.num_bonds()
+        out = np.zeros(size)
+        self._ok(self.L.pd_get_field(self.h, fid, _d(out)))
+        return out

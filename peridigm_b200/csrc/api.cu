@@ -1,0 +1,629 @@
+// C ABI of the B200 Peridigm hot path (declarations and reference citations in
+// include/pd_b200.h). Host-side orchestration only: argument checks, uploads,
+// kernel sequencing on the context's stream, status and error reporting.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pd_internal.cuh"
+
+using namespace pdb;
+
+namespace {
+
+const char* kVersion = "pd_b200 0.1 (sm_100a)";
+
+int fail(pd_ctx* c, int code, const std::string& msg) {
+  c->err = msg;
+  return code;
+}
+
+#define CHECK_CTX(c) \
+  if (!(c)) return PD_ERR_ARG
+
+#define TRY(expr)                 \
+  do {                            \
+    int rc_ = (expr);             \
+    if (rc_ != PD_OK) return rc_; \
+  } while (0)
+
+int ensure_device(pd_ctx* c) {
+  PD_CUDA_TRY(c, cudaSetDevice(c->device));
+  return PD_OK;
+}
+
+// Per-point material arrays from block tables and per-point overrides.
+int upload_material(pd_ctx* c) {
+  const int64_t n = c->n;
+  std::vector<double4> pt(n);
+  std::vector<double> sc(n), hp(n);
+  c->any_damage = false;
+  for (int64_t i = 0; i < n; ++i) {
+    const int b = c->hblock.empty() ? 0 : c->hblock[i];
+    const double K = c->field_K.empty() ? c->block_K[b] : c->field_K[i];
+    const double mu = c->field_mu.empty() ? c->block_mu[b] : c->field_mu[i];
+    pt[i] = make_double4(0.0, K, mu, c->block_rho[b]);
+    sc[i] = c->field_sc.empty() ? c->block_sc[b] : c->field_sc[i];
+    if (sc[i] >= 0.0) c->any_damage = true;
+    hp[i] = c->block_h[b];
+  }
+  PD_CUDA_TRY(c, c->pt.alloc(n));
+  PD_CUDA_TRY(c, c->sc.alloc(n));
+  PD_CUDA_TRY(c, c->coef.alloc(n));
+  PD_CUDA_TRY(c, cudaMemcpy(c->pt.p, pt.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, cudaMemcpy(c->sc.p, sc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, cudaMemcpy(c->hp.p, hp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  return PD_OK;
+}
+
+int upload_horizons(pd_ctx* c) {
+  std::vector<double> hp(c->n);
+  for (int64_t i = 0; i < c->n; ++i) hp[i] = c->block_h[c->hblock.empty() ? 0 : c->hblock[i]];
+  PD_CUDA_TRY(c, c->hp.alloc(c->n));
+  PD_CUDA_TRY(c, cudaMemcpy(c->hp.p, hp.data(), c->n * sizeof(double), cudaMemcpyHostToDevice));
+  return PD_OK;
+}
+
+int alloc_state(pd_ctx* c) {
+  if (c->st[0].count >= (size_t)c->n && c->u.count >= (size_t)(3 * c->n) && c->n > 0) return PD_OK;
+  const int64_t n = c->n;
+  for (int k = 0; k < 2; ++k) {
+    PD_CUDA_TRY(c, c->st[k].alloc(n));
+    PD_CUDA_TRY(c, cudaMemset(c->st[k].p, 0, c->st[k].bytes()));
+  }
+  PD_CUDA_TRY(c, c->ab64.alloc(c->precision == PD_FP64 ? n : 1));
+  PD_CUDA_TRY(c, c->u.alloc(3 * n));
+  PD_CUDA_TRY(c, c->v.alloc(3 * n));
+  PD_CUDA_TRY(c, c->a.alloc(3 * n));
+  PD_CUDA_TRY(c, c->f.alloc(3 * n));
+  PD_CUDA_TRY(c, c->fc.alloc(3 * n));
+  PD_CUDA_TRY(c, c->theta.alloc(n));
+  PD_CUDA_TRY(c, c->node_damage.alloc(n));
+  for (auto* b : {&c->u, &c->v, &c->a, &c->f, &c->fc, &c->theta, &c->node_damage})
+    PD_CUDA_TRY(c, cudaMemset(b->p, 0, b->bytes()));
+  c->cur = 0;
+  c->state_init = false;
+  return PD_OK;
+}
+
+// Everything a model evaluation needs: bonds, material, weighted volume, state buffers.
+int ensure_ready(pd_ctx* c) {
+  TRY(ensure_device(c));
+  if (c->n == 0 || !c->row.p) return fail(c, PD_ERR_STATE, "points and bonds must be set first");
+  if (!c->have_material) return fail(c, PD_ERR_STATE, "no material: call pd_material_lps first");
+  if (!c->symmetric)
+    return fail(c, PD_ERR_UNSUPPORTED,
+                "bond families are not symmetric (j in H(i) without i in H(j)); the gather force pass needs "
+                "symmetric families");
+  TRY(alloc_state(c));
+  if (!c->wv_done) {
+    TRY(upload_material(c));
+    PD_CUDA_TRY(c, launch_weighted_volume(c));
+    PD_CUDA_TRY(c, launch_pack_owner(c));
+    PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->wv_done = true;
+  }
+  if (c->bc_dirty) {
+    const int64_t n = c->n;
+    c->has_bc = false;
+    for (uint8_t m : c->h_bc_mask) c->has_bc |= (m != 0);
+    if (c->has_bc) {
+      PD_CUDA_TRY(c, c->bc_mask.alloc(n));
+      PD_CUDA_TRY(c, c->bc_a.alloc(3 * n));
+      PD_CUDA_TRY(c, c->bc_b.alloc(3 * n));
+      PD_CUDA_TRY(c, cudaMemcpy(c->bc_mask.p, c->h_bc_mask.data(), n, cudaMemcpyHostToDevice));
+      PD_CUDA_TRY(c, cudaMemcpy(c->bc_a.p, c->h_bc_a.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+      PD_CUDA_TRY(c, cudaMemcpy(c->bc_b.p, c->h_bc_b.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    c->bc_dirty = false;
+  }
+  return PD_OK;
+}
+
+int check_status(pd_ctx* c) {
+  int st = 0;
+  PD_CUDA_TRY(c, cudaMemcpyAsync(&st, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (st) PD_CUDA_TRY(c, cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  if (st & ST_NONFINITE_FORCE) return fail(c, PD_ERR_NONFINITE, "NaN returned by force evaluation");
+  if (st & ST_NONFINITE_CONTACT) return fail(c, PD_ERR_NONFINITE, "NaN returned by contact force evaluation");
+  if (st & ST_TIMEOUT) return fail(c, PD_ERR_TIMEOUT, "a bounded device wait ran out");
+  return PD_OK;
+}
+
+// evalModel on the configuration already in st[cur]; trial damage on dmg_trial.
+int eval_trial(pd_ctx* c, double* f_dev) {
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+  StepParams sp{};
+  sp.mode = EVAL_ONLY;
+  sp.damage_on = c->any_damage ? 1 : 0;
+  sp.f_out = f_dev;
+  PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg_trial.p));
+  c->trial_valid = true;
+  return check_status(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pd_version(void) { return kVersion; }
+
+const char* pd_last_error(const pd_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pd_create(const pd_config* cfg, pd_ctx** out) {
+  if (!out) return PD_ERR_ARG;
+  *out = nullptr;
+  pd_ctx* c = new pd_ctx();
+  if (cfg) {
+    c->device = cfg->device;
+    c->precision = cfg->precision;
+    c->influence = cfg->influence;
+    if (cfg->threads_per_point) c->tpo = cfg->threads_per_point;
+  }
+  if (c->precision != PD_FP64 && c->precision != PD_SPLIT_FP32) {
+    delete c;
+    return PD_ERR_ARG;
+  }
+  if (c->influence < 0 || c->influence > 2 || !(c->tpo == 4 || c->tpo == 8 || c->tpo == 16 || c->tpo == 32)) {
+    delete c;
+    return PD_ERR_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || c->device < 0 || c->device >= ndev) {
+    delete c;
+    return PD_ERR_CUDA;
+  }
+  if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      c->status.alloc(1) != cudaSuccess || cudaMemset(c->status.p, 0, sizeof(int)) != cudaSuccess) {
+    delete c;
+    return PD_ERR_CUDA;
+  }
+  c->block_h.assign(1, 0.0);
+  c->block_K.assign(1, 0.0);
+  c->block_mu.assign(1, 0.0);
+  c->block_rho.assign(1, 0.0);
+  c->block_sc.assign(1, -1.0);
+  *out = c;
+  return PD_OK;
+}
+
+int pd_destroy(pd_ctx* c) {
+  if (!c) return PD_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  contact_release(c);
+  qs_release(c);
+  cudaStream_t s = c->stream;
+  delete c;
+  if (s) cudaStreamDestroy(s);
+  return PD_OK;
+}
+
+int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, const int32_t* block) {
+  CHECK_CTX(c);
+  if (n <= 0 || n >= (int64_t(1) << 31) || !x || !vol) return fail(c, PD_ERR_ARG, "pd_set_points: bad arguments");
+  TRY(ensure_device(c));
+  c->n = n;
+  c->hx.assign(x, x + 3 * n);
+  c->hvol.assign(vol, vol + n);
+  int32_t nblk = 1;
+  if (block) {
+    c->hblock.assign(block, block + n);
+    for (int64_t i = 0; i < n; ++i) {
+      if (block[i] < 0) return fail(c, PD_ERR_ARG, "pd_set_points: negative block id");
+      nblk = std::max(nblk, block[i] + 1);
+    }
+  } else {
+    c->hblock.clear();
+  }
+  c->n_blocks = nblk;
+  c->block_h.resize(nblk, c->block_h.empty() ? 0.0 : c->block_h[0]);
+  c->block_K.resize(nblk, 0.0);
+  c->block_mu.resize(nblk, 0.0);
+  c->block_rho.resize(nblk, 0.0);
+  c->block_sc.resize(nblk, -1.0);
+  std::vector<double4> xv(n);
+  for (int64_t i = 0; i < n; ++i) xv[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], vol[i]);
+  PD_CUDA_TRY(c, c->xv.alloc(n));
+  PD_CUDA_TRY(c, cudaMemcpy(c->xv.p, xv.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  c->row.release();
+  c->col.release();
+  c->nb = 0;
+  c->wv_done = false;
+  c->h_bc_mask.assign(n, 0);
+  c->h_bc_a.assign(3 * n, 0.0);
+  c->h_bc_b.assign(3 * n, 0.0);
+  c->bc_dirty = true;
+  c->field_K.clear();
+  c->field_mu.clear();
+  c->field_sc.clear();
+  for (int k = 0; k < 2; ++k) c->st[k].release();
+  c->u.release();
+  c->state_init = false;
+  return PD_OK;
+}
+
+int pd_set_block_horizons(pd_ctx* c, int32_t n_blocks, const double* horizon) {
+  CHECK_CTX(c);
+  if (n_blocks <= 0 || !horizon) return fail(c, PD_ERR_ARG, "pd_set_block_horizons: bad arguments");
+  if (n_blocks > (int32_t)c->block_h.size()) {
+    c->block_h.resize(n_blocks, 0.0);
+    c->block_K.resize(n_blocks, 0.0);
+    c->block_mu.resize(n_blocks, 0.0);
+    c->block_rho.resize(n_blocks, 0.0);
+    c->block_sc.resize(n_blocks, -1.0);
+  }
+  for (int b = 0; b < n_blocks; ++b) {
+    if (!(horizon[b] > 0.0)) return fail(c, PD_ERR_ARG, "horizon must be positive");
+    c->block_h[b] = horizon[b];
+  }
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_build_bonds(pd_ctx* c, const pd_plane_filter* filters, int32_t n_filters) {
+  CHECK_CTX(c);
+  if (c->n == 0) return fail(c, PD_ERR_STATE, "pd_build_bonds: points not set");
+  if (n_filters > 0 && !filters) return fail(c, PD_ERR_ARG, "pd_build_bonds: null filters");
+  for (int32_t b = 0; b < c->n_blocks; ++b)
+    if (!(c->block_h[b] > 0.0)) return fail(c, PD_ERR_STATE, "pd_build_bonds: horizon of every block must be set");
+  TRY(ensure_device(c));
+  TRY(upload_horizons(c));
+  TRY(build_bonds_device(c, filters, n_filters));
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_set_bonds(pd_ctx* c, const int32_t* nl, int64_t len) {
+  CHECK_CTX(c);
+  if (c->n == 0) return fail(c, PD_ERR_STATE, "pd_set_bonds: points not set");
+  if (!nl || len < c->n) return fail(c, PD_ERR_ARG, "pd_set_bonds: neighbor list too short");
+  TRY(ensure_device(c));
+  std::vector<int64_t> row(c->n + 1);
+  std::vector<int32_t> col;
+  col.reserve(len - c->n);
+  int64_t k = 0;
+  for (int64_t i = 0; i < c->n; ++i) {
+    if (k >= len) return fail(c, PD_ERR_ARG, "pd_set_bonds: neighbor list ends early");
+    const int32_t cnt = nl[k++];
+    if (cnt < 0 || k + cnt > len) return fail(c, PD_ERR_ARG, "pd_set_bonds: bad neighbor count");
+    row[i] = (int64_t)col.size();
+    for (int32_t q = 0; q < cnt; ++q) {
+      const int32_t j = nl[k++];
+      if (j < 0 || j >= c->n || j == i) return fail(c, PD_ERR_ARG, "pd_set_bonds: neighbor id out of range or self");
+      col.push_back(j);
+    }
+  }
+  if (k != len) return fail(c, PD_ERR_ARG, "pd_set_bonds: trailing entries in neighbor list");
+  row[c->n] = (int64_t)col.size();
+  c->nb = (int64_t)col.size();
+  PD_CUDA_TRY(c, c->row.alloc(c->n + 1));
+  PD_CUDA_TRY(c, c->col.alloc(std::max<int64_t>(c->nb, 1)));
+  PD_CUDA_TRY(c, cudaMemcpy(c->row.p, row.data(), (c->n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+  if (c->nb) PD_CUDA_TRY(c, cudaMemcpy(c->col.p, col.data(), c->nb * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (c->hp.count < (size_t)c->n) TRY(upload_horizons(c));
+  TRY(finalize_bonds(c, false));
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_num_bonds(const pd_ctx* c, int64_t* nb) {
+  if (!c || !nb) return PD_ERR_ARG;
+  *nb = c->nb;
+  return PD_OK;
+}
+
+int pd_get_bonds(pd_ctx* c, int32_t* nl, int64_t cap, int64_t* len) {
+  CHECK_CTX(c);
+  if (!len) return fail(c, PD_ERR_ARG, "pd_get_bonds: null len");
+  *len = c->n + c->nb;
+  if (cap == 0) return PD_OK;
+  if (!nl || cap < *len) return fail(c, PD_ERR_ARG, "pd_get_bonds: buffer too small");
+  TRY(ensure_device(c));
+  std::vector<int64_t> row(c->n + 1);
+  std::vector<int32_t> col(std::max<int64_t>(c->nb, 1));
+  PD_CUDA_TRY(c, cudaMemcpy(row.data(), c->row.p, (c->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  if (c->nb) PD_CUDA_TRY(c, cudaMemcpy(col.data(), c->col.p, c->nb * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  int64_t k = 0;
+  for (int64_t i = 0; i < c->n; ++i) {
+    nl[k++] = (int32_t)(row[i + 1] - row[i]);
+    for (int64_t b = row[i]; b < row[i + 1]; ++b) nl[k++] = col[b];
+  }
+  return PD_OK;
+}
+
+int pd_material_lps(pd_ctx* c, int32_t block, double K, double mu, double rho) {
+  CHECK_CTX(c);
+  if (block < 0 || block >= (int32_t)c->block_K.size()) return fail(c, PD_ERR_ARG, "pd_material_lps: bad block");
+  if (!(K > 0.0) || !(mu > 0.0) || !(rho > 0.0)) return fail(c, PD_ERR_ARG, "pd_material_lps: moduli and density must be positive");
+  c->block_K[block] = K;
+  c->block_mu[block] = mu;
+  c->block_rho[block] = rho;
+  c->have_material = true;
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_material_lps_field(pd_ctx* c, const double* K, const double* mu) {
+  CHECK_CTX(c);
+  if (c->n == 0 || !K || !mu) return fail(c, PD_ERR_ARG, "pd_material_lps_field: bad arguments");
+  for (int64_t i = 0; i < c->n; ++i)
+    if (!(K[i] > 0.0) || !(mu[i] > 0.0)) return fail(c, PD_ERR_ARG, "pd_material_lps_field: moduli must be positive");
+  c->field_K.assign(K, K + c->n);
+  c->field_mu.assign(mu, mu + c->n);
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_damage_critical_stretch(pd_ctx* c, int32_t block, double s_c) {
+  CHECK_CTX(c);
+  if (block < 0 || block >= (int32_t)c->block_sc.size()) return fail(c, PD_ERR_ARG, "pd_damage_critical_stretch: bad block");
+  c->block_sc[block] = s_c;
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_damage_critical_stretch_field(pd_ctx* c, const double* s_c) {
+  CHECK_CTX(c);
+  if (c->n == 0 || !s_c) return fail(c, PD_ERR_ARG, "pd_damage_critical_stretch_field: bad arguments");
+  c->field_sc.assign(s_c, s_c + c->n);
+  c->wv_done = false;
+  return PD_OK;
+}
+
+int pd_weighted_volume(pd_ctx* c, double* m_out) {
+  CHECK_CTX(c);
+  TRY(ensure_ready(c));
+  if (m_out) {
+    std::vector<double4> pt(c->n);
+    PD_CUDA_TRY(c, cudaMemcpy(pt.data(), c->pt.p, c->n * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < c->n; ++i) m_out[i] = pt[i].x;
+  }
+  return PD_OK;
+}
+
+int pd_compute_force_device(pd_ctx* c, const double* y_dev, double* f_dev) {
+  CHECK_CTX(c);
+  if (!y_dev) return fail(c, PD_ERR_ARG, "pd_compute_force_device: null coordinates");
+  TRY(ensure_ready(c));
+  PD_CUDA_TRY(c, launch_state_from_y(c, y_dev));
+  return eval_trial(c, f_dev);
+}
+
+int pd_compute_force(pd_ctx* c, const double* y, double* f_out) {
+  CHECK_CTX(c);
+  if (!y) return fail(c, PD_ERR_ARG, "pd_compute_force: null coordinates");
+  TRY(ensure_ready(c));
+  const size_t bytes = 3 * (size_t)c->n * sizeof(double);
+  // y is staged through the force buffer, then f is written there
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->f.p, y, bytes, cudaMemcpyHostToDevice, c->stream));
+  PD_CUDA_TRY(c, launch_state_from_y(c, c->f.p));
+  TRY(eval_trial(c, c->f.p));
+  if (f_out) {
+    PD_CUDA_TRY(c, cudaMemcpyAsync(f_out, c->f.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  return PD_OK;
+}
+
+int pd_compute_damage(pd_ctx* c, const double* y) { return pd_compute_force(c, y, nullptr); }
+
+int pd_update_state(pd_ctx* c) {
+  CHECK_CTX(c);
+  TRY(ensure_device(c));
+  if (c->trial_valid) {
+    PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg.p, c->dmg_trial.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+    PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->trial_valid = false;
+  }
+  return PD_OK;
+}
+
+int pd_set_bond_damage(pd_ctx* c, const double* bd) {
+  CHECK_CTX(c);
+  if (!bd || !c->dmg.p) return fail(c, PD_ERR_STATE, "pd_set_bond_damage: bonds not set");
+  std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
+  for (int64_t b = 0; b < c->nb; ++b) {
+    if (bd[b] == 0.0) h[b] = 0;
+    else if (bd[b] == 1.0) h[b] = 1;
+    else return fail(c, PD_ERR_UNSUPPORTED, "bond damage must be 0 or 1 (critical-stretch values)");
+  }
+  TRY(ensure_device(c));
+  PD_CUDA_TRY(c, cudaMemcpy(c->dmg.p, h.data(), (size_t)c->nb, cudaMemcpyHostToDevice));
+  c->trial_valid = false;
+  return PD_OK;
+}
+
+int pd_critical_time_step(pd_ctx* c, double* dt_out) {
+  CHECK_CTX(c);
+  if (!dt_out) return fail(c, PD_ERR_ARG, "pd_critical_time_step: null output");
+  TRY(ensure_ready(c));
+  DBuf<double> d;
+  PD_CUDA_TRY(c, d.alloc(1));
+  PD_CUDA_TRY(c, launch_critical_dt(c, d.p));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(dt_out, d.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return PD_OK;
+}
+
+int pd_set_state(pd_ctx* c, const double* u, const double* v) {
+  CHECK_CTX(c);
+  TRY(ensure_ready(c));
+  const size_t bytes = 3 * (size_t)c->n * sizeof(double);
+  if (u) PD_CUDA_TRY(c, cudaMemcpy(c->u.p, u, bytes, cudaMemcpyHostToDevice));
+  else if (!c->state_init) PD_CUDA_TRY(c, cudaMemset(c->u.p, 0, bytes));
+  if (v) PD_CUDA_TRY(c, cudaMemcpy(c->v.p, v, bytes, cudaMemcpyHostToDevice));
+  else if (!c->state_init) PD_CUDA_TRY(c, cudaMemset(c->v.p, 0, bytes));
+  if (u || !c->state_init) {
+    c->cur = 0;
+    PD_CUDA_TRY(c, launch_sync_state(c));
+    PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  c->state_init = true;
+  return PD_OK;
+}
+
+int pd_add_prescribed_displacement(pd_ctx* c, int64_t np, const int64_t* pts, int32_t coord, double a, double b) {
+  CHECK_CTX(c);
+  if (c->n == 0) return fail(c, PD_ERR_STATE, "points not set");
+  if (coord < 0 || coord > 2 || np < 0 || (np > 0 && !pts)) return fail(c, PD_ERR_ARG, "bad boundary condition");
+  for (int64_t k = 0; k < np; ++k) {
+    const int64_t i = pts[k];
+    if (i < 0 || i >= c->n) return fail(c, PD_ERR_ARG, "boundary-condition point out of range");
+    c->h_bc_mask[i] |= (uint8_t)(1u << coord);
+    c->h_bc_a[3 * i + coord] = a;
+    c->h_bc_b[3 * i + coord] = b;
+  }
+  c->bc_dirty = true;
+  return PD_OK;
+}
+
+int pd_clear_boundary_conditions(pd_ctx* c) {
+  CHECK_CTX(c);
+  std::fill(c->h_bc_mask.begin(), c->h_bc_mask.end(), 0);
+  c->bc_dirty = true;
+  return PD_OK;
+}
+
+int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* stats) {
+  CHECK_CTX(c);
+  if (!(dt > 0.0) || nsteps < 0) return fail(c, PD_ERR_ARG, "pd_verlet_run: dt must be positive and nsteps >= 0");
+  TRY(ensure_ready(c));
+  if (!c->state_init) TRY(pd_set_state(c, nullptr, nullptr));
+  const bool contact = c->contact != nullptr;
+  cudaEvent_t e0, e1;
+  PD_CUDA_TRY(c, cudaEventCreate(&e0));
+  PD_CUDA_TRY(c, cudaEventCreate(&e1));
+  StepParams sp{};
+  sp.dt = dt;
+  sp.t0 = t0;
+  sp.damage_on = c->any_damage ? 1 : 0;
+  sp.has_bc = c->has_bc ? 1 : 0;
+  sp.has_contact = contact ? 1 : 0;
+  // initial evaluation (Peridigm.cpp:1393-1423): its damage is not committed
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (contact) {
+    TRY(contact_prepare(c, 0));
+    TRY(contact_eval(c));
+  }
+  sp.step = 0;
+  sp.mode = nsteps == 0 ? EVAL_LAST : EVAL_ADVANCE;
+  sp.f_out = nsteps == 0 ? c->f.p : nullptr;
+  PD_CUDA_TRY(c, cudaEventRecord(e0, c->stream));
+  PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg_trial.p));
+  if (nsteps > 0) c->cur ^= 1;
+  for (int64_t s = 1; s <= nsteps; ++s) {
+    sp.step = s;
+    const bool last = s == nsteps;
+    sp.mode = last ? EVAL_LAST : EVAL_ADVANCE;
+    sp.f_out = last ? c->f.p : nullptr;
+    if (contact) {
+      TRY(contact_prepare(c, s));
+      TRY(contact_eval(c));
+    }
+    PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg.p));
+    if (!last) c->cur ^= 1;
+  }
+  PD_CUDA_TRY(c, cudaEventRecord(e1, c->stream));
+  PD_CUDA_TRY(c, cudaEventSynchronize(e1));
+  if (c->ktime) PD_CUDA_TRY(c, collect_kernel_times(c));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->trial_valid = false;
+  int rc = check_status(c);
+  if (stats) {
+    stats->steps = nsteps;
+    stats->bonds = c->nb;
+    stats->device_ms = ms;
+    std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
+    PD_CUDA_TRY(c, cudaMemcpy(h.data(), c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToHost));
+    int64_t br = 0;
+    for (int64_t b = 0; b < c->nb; ++b) br += h[b];
+    stats->broken_bonds = br;
+    stats->contact_pairs = contact_pairs(c);
+  }
+  return rc;
+}
+
+int pd_set_kernel_timing(pd_ctx* c, int enable) {
+  CHECK_CTX(c);
+  TRY(ensure_device(c));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (c->ktime) PD_CUDA_TRY(c, collect_kernel_times(c));
+  c->ktime = enable != 0;
+  c->kms[0] = c->kms[1] = 0.0;
+  c->klaunches = 0;
+  return PD_OK;
+}
+
+int pd_get_kernel_timing(pd_ctx* c, double* ms_out, int64_t* launches_out) {
+  CHECK_CTX(c);
+  TRY(ensure_device(c));
+  PD_CUDA_TRY(c, collect_kernel_times(c));
+  if (ms_out) {
+    ms_out[0] = c->kms[0];
+    ms_out[1] = c->kms[1];
+  }
+  if (launches_out) *launches_out = c->klaunches;
+  return PD_OK;
+}
+
+int pd_get_field(pd_ctx* c, int32_t field, double* out) {
+  CHECK_CTX(c);
+  if (!out) return fail(c, PD_ERR_ARG, "pd_get_field: null output");
+  TRY(ensure_ready(c));
+  const int64_t n = c->n;
+  const size_t b3 = 3 * (size_t)n * sizeof(double);
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  switch (field) {
+    case PD_FIELD_DISPLACEMENT:
+    case PD_FIELD_COORDINATES: {
+      if (c->precision == PD_SPLIT_FP32) {
+        DBuf<double> tmp;
+        PD_CUDA_TRY(c, tmp.alloc(3 * n));
+        PD_CUDA_TRY(c, launch_state_to_u(c, tmp.p));
+        PD_CUDA_TRY(c, cudaMemcpyAsync(out, tmp.p, b3, cudaMemcpyDeviceToHost, c->stream));
+        PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      } else {
+        PD_CUDA_TRY(c, cudaMemcpy(out, c->u.p, b3, cudaMemcpyDeviceToHost));
+      }
+      if (field == PD_FIELD_COORDINATES)
+        for (int64_t k = 0; k < 3 * n; ++k) out[k] = c->hx[k] + out[k];
+      return PD_OK;
+    }
+    case PD_FIELD_VELOCITY: PD_CUDA_TRY(c, cudaMemcpy(out, c->v.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
+    case PD_FIELD_ACCELERATION: PD_CUDA_TRY(c, cudaMemcpy(out, c->a.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
+    case PD_FIELD_FORCE_DENSITY: PD_CUDA_TRY(c, cudaMemcpy(out, c->f.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
+    case PD_FIELD_CONTACT_FORCE: PD_CUDA_TRY(c, cudaMemcpy(out, c->fc.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
+    case PD_FIELD_DILATATION:
+      PD_CUDA_TRY(c, cudaMemcpy(out, c->theta.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+      return PD_OK;
+    case PD_FIELD_DAMAGE:
+      PD_CUDA_TRY(c, cudaMemcpy(out, c->node_damage.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+      return PD_OK;
+    case PD_FIELD_WEIGHTED_VOLUME: return pd_weighted_volume(c, out);
+    case PD_FIELD_BOND_DAMAGE: {
+      std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
+      const uint8_t* src = c->trial_valid ? c->dmg_trial.p : c->dmg.p;
+      PD_CUDA_TRY(c, cudaMemcpy(h.data(), src, (size_t)c->nb, cudaMemcpyDeviceToHost));
+      for (int64_t b = 0; b < c->nb; ++b) out[b] = (double)h[b];
+      return PD_OK;
+    }
+    case PD_FIELD_NUM_NEIGHBORS: {
+      std::vector<int64_t> row(n + 1);
+      PD_CUDA_TRY(c, cudaMemcpy(row.data(), c->row.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+      for (int64_t i = 0; i < n; ++i) out[i] = (double)(row[i + 1] - row[i]);
+      return PD_OK;
+    }
+    default: return fail(c, PD_ERR_ARG, "pd_get_field: unknown field");
+  }
+}
+
+}  // extern "C"

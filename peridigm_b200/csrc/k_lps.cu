@@ -1,0 +1,681 @@
+// LPS elastic + critical-stretch damage + velocity-Verlet kernels (sm_100a).
+//
+// Two bond passes per evaluation, both gathers, no atomics:
+//   pass 1 (k_damage_dilatation): per bond, critical-stretch test and the
+//     dilatation term; per point theta, node damage and the owner force-state
+//     coefficients (A, B) the second pass gathers.
+//   pass 2 (k_force): per bond f_i += (t_ij + t_ji) * Y/|Y| * V_j, the gather
+//     form of the reference's scatter (elastic.cxx:125-130: the owner adds
+//     t_ij*Y*V_j, the neighbor's own loop subtracts t_ji*(-Y)*V_j), followed
+//     by the Verlet epilogue of Peridigm::executeExplicit (Peridigm.cpp:1480-1577).
+// A group of TPO consecutive lanes owns one point's bond family; lanes stride
+// through the row (coalesced col/damage loads), partial sums are combined by
+// a fixed xor-shuffle tree, so results are deterministic.
+#include <math.h>
+
+#include "pd_internal.cuh"
+
+namespace pdb {
+
+constexpr int kBlock = 256;
+
+// ---------------------------------------------------------------------------
+// Influence functions (src/core/Peridigm_InfluenceFunction.hpp:69-87)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double omega_d(int kind, double zeta, double h) {
+  if (kind == PD_INFLUENCE_ONE) return 1.0;
+  if (kind == PD_INFLUENCE_PARABOLIC_DECAY) {
+    if (zeta > h) return 0.0;
+    double s = __ddiv_rn(zeta, h);
+    return s < 0.5 ? 1.0 : __dadd_rn(__dmul_rn(__dmul_rn(-4.0, s), s), __dmul_rn(4.0, s));
+  }
+  double h2 = __dmul_rn(__dmul_rn(__dmul_rn(h, h), 0.4), 0.4);
+  return exp(-__ddiv_rn(__dmul_rn(zeta, zeta), h2));
+}
+
+__device__ __forceinline__ float omega_f(int kind, float zeta, float h) {
+  if (kind == PD_INFLUENCE_ONE) return 1.0f;
+  if (kind == PD_INFLUENCE_PARABOLIC_DECAY) {
+    if (zeta > h) return 0.0f;
+    float s = zeta / h;
+    return s < 0.5f ? 1.0f : -4.0f * s * s + 4.0f * s;
+  }
+  float h2 = h * h * 0.16f;
+  return expf(-(zeta * zeta) / h2);
+}
+
+// Squared distance exactly as the reference computes it (dx*dx+dy*dy)+dz*dz,
+// with no fused multiply-add, so FP64 distances round like the reference's.
+__device__ __forceinline__ double sq3_rn(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+template <int TPO>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+  for (int o = TPO / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int TPO>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = TPO / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <int TPO>
+__device__ __forceinline__ int group_sum(int v) {
+#pragma unroll
+  for (int o = TPO / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double pack_ab(float A, float B) {
+  return __hiloint2double(__float_as_int(B), __float_as_int(A));
+}
+__device__ __forceinline__ float2 unpack_ab(double w) {
+  return make_float2(__int_as_float(__double2loint(w)), __int_as_float(__double2hiint(w)));
+}
+
+// ---------------------------------------------------------------------------
+// K1: weighted volume m_i = sum_j omega*|xi|^2*V_j (material_utilities.cxx:161-188)
+// ---------------------------------------------------------------------------
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_weighted_volume(int64_t n, const int64_t* __restrict__ row,
+                                                            const int32_t* __restrict__ col,
+                                                            const double4* __restrict__ xv,
+                                                            const double* __restrict__ hp, int influence,
+                                                            double4* __restrict__ pt) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double acc = 0.0;
+  if (valid) {
+    const double4 xi = xv[i];
+    const double h = hp[i];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
+      const double4 xj = xv[col[b]];
+      const double z2 = sq3_rn(__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z));
+      const double om = omega_d(influence, __dsqrt_rn(z2), h);
+      acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(om, z2), xj.w));
+    }
+  }
+  acc = group_sum<TPO>(acc);
+  if (valid && lane == 0) pt[i].x = acc;
+}
+
+// Split-path owner coefficients: A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m.
+__global__ void k_pack_owner(int64_t n, const double4* __restrict__ pt, float2* __restrict__ coef) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = pt[i];  // (m, K, mu, rho)
+  const double m = p.x;
+  coef[i] = make_float2((float)((3.0 * p.y - 5.0 * p.z) / m), (float)(15.0 * p.z / m));
+}
+
+// ---------------------------------------------------------------------------
+// K2: damage + dilatation, split-FP32.
+//   X = fp32(x_j - x_i), du = fp32(u_j - u_i) (differences in FP64, one rounding)
+//   e = (2 X.du + du.du) / (|Y| + |X|)          (= |Y| - |X| without cancellation)
+//   break when e/|X| > s_c (CriticalStretchDamageModel.cpp:155-158)
+//   theta_i = 3/m_i * sum omega*(1-d)*|X|*e*V_j  (material_utilities.cxx:284)
+// ---------------------------------------------------------------------------
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_dilatation_split(
+    int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+    const double4* __restrict__ xv, double4* __restrict__ st, const double4* __restrict__ pt,
+    const float2* __restrict__ coef, const double* __restrict__ sc, const double* __restrict__ hp,
+    int influence, int damage_on, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  float th = 0.0f;
+  int broken = 0;
+  int64_t b0 = 0, b1 = 0;
+  if (valid) {
+    b0 = row[i];
+    b1 = row[i + 1];
+    const double4 xi = xv[i];
+    const double4 ui = st[i];
+    const float s_c = damage_on ? (float)sc[i] : -1.0f;
+    const float h = (float)hp[i];
+    for (int64_t b = b0 + lane; b < b1; b += TPO) {
+      if (dmg[b]) {
+        broken++;
+        continue;
+      }
+      const int32_t j = col[b];
+      const double4 xj = xv[j];
+      const double4 uj = st[j];
+      const float Xx = (float)(xj.x - xi.x), Xy = (float)(xj.y - xi.y), Xz = (float)(xj.z - xi.z);
+      const float Ux = (float)(uj.x - ui.x), Uy = (float)(uj.y - ui.y), Uz = (float)(uj.z - ui.z);
+      const float zeta = sqrtf(Xx * Xx + Xy * Xy + Xz * Xz);
+      const float Yx = Xx + Ux, Yy = Xy + Uy, Yz = Xz + Uz;
+      const float dY = sqrtf(Yx * Yx + Yy * Yy + Yz * Yz);
+      const float e = (2.0f * (Xx * Ux + Xy * Uy + Xz * Uz) + (Ux * Ux + Uy * Uy + Uz * Uz)) / (dY + zeta);
+      if (s_c >= 0.0f && e / zeta > s_c) {
+        dmg[b] = 1;
+        broken++;
+        continue;
+      }
+      th += omega_f(influence, zeta, h) * zeta * e * (float)xj.w;
+    }
+  }
+  th = group_sum<TPO>(th);
+  broken = group_sum<TPO>(broken);
+  if (valid && lane == 0) {
+    const double theta = 3.0 * (double)th / pt[i].x;
+    const float2 cf = coef[i];
+    st[i].w = pack_ab((float)theta * cf.x, cf.y);
+    theta_out[i] = theta;
+    node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K2: damage + dilatation, FP64, the reference's operation order:
+//   rel = (|Y|-|X|)/|X| > s_c                     (CriticalStretchDamageModel.cpp:147-158)
+//   theta += 3*omega*(1-d)*|X|*e*V_j/m_i           (material_utilities.cxx:284)
+// Writes ab64[i] = (theta, 3K/m - alpha/3, alpha) (elastic.cxx:99,119).
+// ---------------------------------------------------------------------------
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_dilatation_fp64(
+    int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+    const double4* __restrict__ xv, const double4* __restrict__ st, const double4* __restrict__ pt,
+    const double* __restrict__ sc, const double* __restrict__ hp, int influence, int damage_on,
+    double4* __restrict__ ab64, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double th = 0.0;
+  int broken = 0;
+  int64_t b0 = 0, b1 = 0;
+  double m = 1.0;
+  if (valid) {
+    b0 = row[i];
+    b1 = row[i + 1];
+    const double4 xi = xv[i];
+    const double4 yi = st[i];
+    m = pt[i].x;
+    const double s_c = damage_on ? sc[i] : -1.0;
+    const double h = hp[i];
+    for (int64_t b = b0 + lane; b < b1; b += TPO) {
+      if (dmg[b]) {
+        broken++;
+        continue;
+      }
+      const int32_t j = col[b];
+      const double4 xj = xv[j];
+      const double4 yj = st[j];
+      const double zeta = __dsqrt_rn(sq3_rn(__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z)));
+      const double dY = __dsqrt_rn(sq3_rn(__dsub_rn(yj.x, yi.x), __dsub_rn(yj.y, yi.y), __dsub_rn(yj.z, yi.z)));
+      if (s_c >= 0.0 && __ddiv_rn(__dsub_rn(dY, zeta), zeta) > s_c) {
+        dmg[b] = 1;
+        broken++;
+        continue;
+      }
+      const double e = __dsub_rn(dY, zeta);
+      const double om = omega_d(influence, zeta, h);
+      // 3.0*omega*(1.0-d)*d*e*cellVolume/m with d = 0
+      double t = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(3.0, om), zeta), e), xj.w);
+      th = __dadd_rn(th, __ddiv_rn(t, m));
+    }
+  }
+  th = group_sum<TPO>(th);
+  broken = group_sum<TPO>(broken);
+  if (valid && lane == 0) {
+    const double4 p = pt[i];
+    const double alpha = __ddiv_rn(__dmul_rn(15.0, p.z), p.x);
+    const double q = __dsub_rn(__ddiv_rn(__dmul_rn(3.0, p.y), p.x), __ddiv_rn(alpha, 3.0));
+    ab64[i] = make_double4(th, q, alpha, 0.0);
+    theta_out[i] = th;
+    node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Verlet epilogue shared by both precisions. Lane c (< 3) of the group handles
+// component c of point i; f is the internal force density of that component.
+// Order of Peridigm::executeExplicit: f += f_contact (Peridigm.cpp:1567),
+// a = (f + f_ext)/rho (:1569-1573), v += dt/2*a (:1577); then the next step's
+// v += dt/2*a (:1480), kinematic BC (:1486, DirichletIncrementBC
+// Peridigm_BoundaryCondition.cpp:232-237), y = x+u+dt*v (:1497), u += dt*v (:1501).
+// FP64 operations use explicit round-to-nearest intrinsics (no contraction)
+// so the state rounds like the reference's scalar build.
+// ---------------------------------------------------------------------------
+struct EpiArgs {
+  double dt, t0;
+  int64_t step;  // evaluation index: 0 = initial evaluation at t0, s = step s
+  int mode;
+  int has_contact, has_bc, split;
+  const double* fc;
+  double* f_out;
+  double* u;  // FP64-path displacement [3n]
+  double* v;
+  double* a;
+  const uint8_t* bc_mask;
+  const double* bc_a;
+  const double* bc_b;
+  const double4* st_cur;
+  double4* st_next;
+  int* status;
+};
+
+__device__ __forceinline__ double comp3(const double4& q, int c) { return c == 0 ? q.x : (c == 1 ? q.y : q.z); }
+__device__ __forceinline__ double* comp_ptr(double4* q, int c) {
+  return c == 0 ? &q->x : (c == 1 ? &q->y : &q->z);
+}
+
+__device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int c, double f, const double4& xi,
+                                                double rho) {
+  const int64_t k = 3 * i + c;
+  double ftot = f;
+  if (E.has_contact) ftot = __dadd_rn(ftot, E.fc[k]);
+  if (!isfinite(ftot)) atomicOr(E.status, ST_NONFINITE_FORCE);
+  if (E.f_out) E.f_out[k] = ftot;
+  if (E.mode == EVAL_ONLY) return;
+  const double dt = E.dt, dt2 = E.dt / 2.0;
+  const double acc = __ddiv_rn(__dadd_rn(ftot, 0.0), rho);
+  double v = E.v[k];
+  if (E.step > 0) v = __dadd_rn(v, __dmul_rn(dt2, acc));  // end of step (none after the initial evaluation)
+  if (E.mode == EVAL_LAST) {
+    E.v[k] = v;
+    E.a[k] = acc;
+    return;
+  }
+  // first half of step s+1
+  double vh = __dadd_rn(v, __dmul_rn(dt2, acc));
+  if (E.has_bc && ((E.bc_mask[i] >> c) & 1)) {
+    const double tc = __dadd_rn(E.t0, __dmul_rn((double)(E.step + 1), dt));
+    const double tp = E.step == 0 ? E.t0 : __dadd_rn(E.t0, __dmul_rn((double)E.step, dt));
+    if (tc != tp) {
+      const double cur = __dadd_rn(__dmul_rn(E.bc_a[k], tc), E.bc_b[k]);
+      const double prev = __dadd_rn(__dmul_rn(E.bc_a[k], tp), E.bc_b[k]);
+      const double d = __dsub_rn(cur, prev);
+      vh = __dadd_rn(__dmul_rn(0.0, d), __dmul_rn(__dmul_rn(1.0, d), __ddiv_rn(1.0, __dsub_rn(tc, tp))));
+    }
+  }
+  E.v[k] = vh;
+  E.a[k] = acc;
+  const double step_dx = __dmul_rn(dt, vh);
+  if (E.split) {
+    const double u = comp3(E.st_cur[i], c);
+    *comp_ptr(&E.st_next[i], c) = __dadd_rn(u, step_dx);
+  } else {
+    const double u = E.u[k];
+    const double x = comp3(xi, c);
+    *comp_ptr(&E.st_next[i], c) = __dadd_rn(__dadd_rn(x, u), step_dx);  // y = x+u+dt*v
+    E.u[k] = __dadd_rn(u, step_dx);                                      // u += dt*v
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3: force gather, split-FP32. Recomputes X, du, |X|, |Y|, e with the same
+// FP32 operations as pass 1 (identical values), then
+//   t_ij + t_ji = omega*(|X|*(A_i + A_j) + e*(B_i + B_j))   (bond intact)
+//   f_i += (t_ij + t_ji) * V_j * Y/|Y|
+// Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
+// ---------------------------------------------------------------------------
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_force_split(int64_t n, const int64_t* __restrict__ row,
+                                                        const int32_t* __restrict__ col,
+                                                        const uint8_t* __restrict__ dmg,
+                                                        const double4* __restrict__ xv,
+                                                        const double4* __restrict__ st,
+                                                        const double4* __restrict__ pt,
+                                                        const double* __restrict__ hp, int influence,
+                                                        EpiArgs E) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  double4 xi = make_double4(0, 0, 0, 0);
+  if (valid) {
+    xi = xv[i];
+    const double4 ui = st[i];
+    const float2 abi = unpack_ab(ui.w);
+    const float h = (float)hp[i];
+    const int64_t b1 = row[i + 1];
+    for (int64_t b = row[i] + lane; b < b1; b += TPO) {
+      if (dmg[b]) continue;
+      const int32_t j = col[b];
+      const double4 xj = xv[j];
+      const double4 uj = st[j];
+      const float Xx = (float)(xj.x - xi.x), Xy = (float)(xj.y - xi.y), Xz = (float)(xj.z - xi.z);
+      const float Ux = (float)(uj.x - ui.x), Uy = (float)(uj.y - ui.y), Uz = (float)(uj.z - ui.z);
+      const float zeta = sqrtf(Xx * Xx + Xy * Xy + Xz * Xz);
+      const float Yx = Xx + Ux, Yy = Xy + Uy, Yz = Xz + Uz;
+      const float dY = sqrtf(Yx * Yx + Yy * Yy + Yz * Yz);
+      const float e = (2.0f * (Xx * Ux + Xy * Uy + Xz * Uz) + (Ux * Ux + Uy * Uy + Uz * Uz)) / (dY + zeta);
+      const float2 abj = unpack_ab(uj.w);
+      const float T = omega_f(influence, zeta, h) * (zeta * (abi.x + abj.x) + e * (abi.y + abj.y));
+      const float s = T * (float)xj.w / dY;
+      fx += s * Yx;
+      fy += s * Yy;
+      fz += s * Yz;
+    }
+  }
+  fx = group_sum<TPO>(fx);
+  fy = group_sum<TPO>(fy);
+  fz = group_sum<TPO>(fz);
+  if (valid && lane < 3) {
+    const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
+    verlet_epilogue(E, i, lane, f, xi, pt[i].w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// K3: force gather, FP64, each term in the reference's operation order:
+//   c1 = omega*theta*(3K/m - alpha/3); t = c1*|X| + omega*alpha*e   (elastic.cxx:119-120)
+//   own term  +  (t_ij*Y)/|Y| * V_j      (elastic.cxx:121-127)
+//   neighbor  -  (t_ji*(-Y))/|Y| * V_j   (elastic.cxx:128-130 from j's loop)
+// ---------------------------------------------------------------------------
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t* __restrict__ row,
+                                                       const int32_t* __restrict__ col,
+                                                       const uint8_t* __restrict__ dmg,
+                                                       const double4* __restrict__ xv,
+                                                       const double4* __restrict__ st,
+                                                       const double4* __restrict__ ab64,
+                                                       const double4* __restrict__ pt,
+                                                       const double* __restrict__ hp, int influence,
+                                                       EpiArgs E) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  double4 xi = make_double4(0, 0, 0, 0);
+  if (valid) {
+    xi = xv[i];
+    const double4 yi = st[i];
+    const double4 ai = ab64[i];  // (theta, q, alpha)
+    const double hi = hp[i];
+    const int64_t b1 = row[i + 1];
+    for (int64_t b = row[i] + lane; b < b1; b += TPO) {
+      if (dmg[b]) continue;
+      const int32_t j = col[b];
+      const double4 xj = xv[j];
+      const double4 yj = st[j];
+      const double4 aj = ab64[j];
+      const double zeta = __dsqrt_rn(sq3_rn(__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z)));
+      const double Yx = __dsub_rn(yj.x, yi.x), Yy = __dsub_rn(yj.y, yi.y), Yz = __dsub_rn(yj.z, yi.z);
+      const double dY = __dsqrt_rn(sq3_rn(Yx, Yy, Yz));
+      const double e = __dsub_rn(dY, zeta);
+      const double om_i = omega_d(influence, zeta, hi);
+      const double om_j = influence == PD_INFLUENCE_ONE ? 1.0 : omega_d(influence, zeta, hp[j]);
+      const double ti = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(om_i, ai.x), ai.y), zeta),
+                                  __dmul_rn(__dmul_rn(om_i, ai.z), e));
+      const double tj = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(om_j, aj.x), aj.y), zeta),
+                                  __dmul_rn(__dmul_rn(om_j, aj.z), e));
+      const double V = xj.w;
+      fx = __dadd_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yx), dY), V));
+      fy = __dadd_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yy), dY), V));
+      fz = __dadd_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yz), dY), V));
+      fx = __dsub_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yx), dY), V));
+      fy = __dsub_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yy), dY), V));
+      fz = __dsub_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yz), dY), V));
+    }
+  }
+  fx = group_sum<TPO>(fx);
+  fy = group_sum<TPO>(fy);
+  fz = group_sum<TPO>(fz);
+  if (valid && lane < 3) {
+    const double f = lane == 0 ? fx : (lane == 1 ? fy : fz);
+    verlet_epilogue(E, i, lane, f, xi, pt[i].w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// State conversions and the stable time step
+// ---------------------------------------------------------------------------
+// Gathered state from current coordinates y [3n]: split -> u = y - x, FP64 -> y.
+__global__ void k_state_from_y(int64_t n, const double* __restrict__ y, const double4* __restrict__ xv,
+                               double4* __restrict__ st, double* __restrict__ u, int split) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 x = xv[i];
+  const double y0 = y[3 * i], y1 = y[3 * i + 1], y2 = y[3 * i + 2];
+  double4 s = st[i];
+  if (split) {
+    s.x = y0 - x.x;
+    s.y = y1 - x.y;
+    s.z = y2 - x.z;
+  } else {
+    s.x = y0;
+    s.y = y1;
+    s.z = y2;
+    if (u) {
+      u[3 * i] = y0 - x.x;
+      u[3 * i + 1] = y1 - x.y;
+      u[3 * i + 2] = y2 - x.z;
+    }
+  }
+  st[i] = s;
+}
+
+// Gathered state from the displacement u [3n] (after pd_set_state): split -> u,
+// FP64 -> y = x + u (Peridigm.cpp:1497 with v = 0 contribution already in u).
+__global__ void k_state_from_u(int64_t n, const double* __restrict__ u, const double4* __restrict__ xv,
+                               double4* __restrict__ st, int split) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 x = xv[i];
+  double4 s = st[i];
+  if (split) {
+    s.x = u[3 * i];
+    s.y = u[3 * i + 1];
+    s.z = u[3 * i + 2];
+  } else {
+    s.x = __dadd_rn(x.x, u[3 * i]);
+    s.y = __dadd_rn(x.y, u[3 * i + 1]);
+    s.z = __dadd_rn(x.z, u[3 * i + 2]);
+  }
+  st[i] = s;
+}
+
+// Displacement [3n] out of the state (split path keeps u only in st).
+__global__ void k_state_to_u(int64_t n, const double4* __restrict__ st, double* __restrict__ u) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 s = st[i];
+  u[3 * i] = s.x;
+  u[3 * i + 1] = s.y;
+  u[3 * i + 2] = s.z;
+}
+
+// ComputeCriticalTimeStep (Peridigm_CriticalTimeStep.cpp:52-130): per point
+// dt_i = sqrt(2 rho / sum_j V_j*k/|xi|), k = 18K/(pi h^4); block minima go to
+// partial[] and k_min_reduce takes the minimum (order-independent, exact).
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_critical_dt(int64_t n, const int64_t* __restrict__ row,
+                                                        const int32_t* __restrict__ col,
+                                                        const double4* __restrict__ xv,
+                                                        const double4* __restrict__ pt,
+                                                        const double* __restrict__ hp, double* __restrict__ partial) {
+  __shared__ double smin[kBlock / TPO];
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double den = 0.0;
+  int64_t nn = 0;
+  if (valid) {
+    const double4 xi = xv[i];
+    const double4 p = pt[i];
+    const double h = hp[i];
+    const double spring =
+        __ddiv_rn(__dmul_rn(18.0, p.y), __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(3.14159265358979323846, h), h), h), h));
+    nn = row[i + 1] - row[i];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
+      const double4 xj = xv[col[b]];
+      const double d = __dsqrt_rn(sq3_rn(__dsub_rn(xi.x, xj.x), __dsub_rn(xi.y, xj.y), __dsub_rn(xi.z, xj.z)));
+      den = __dadd_rn(den, __ddiv_rn(__dmul_rn(xj.w, spring), d));
+    }
+  }
+  den = group_sum<TPO>(den);
+  double cts = 1.0e50;
+  if (valid && nn > 0) cts = __dsqrt_rn(__ddiv_rn(__dmul_rn(2.0, pt[i].w), den));
+  if (lane == 0) smin[threadIdx.x / TPO] = cts;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mn = 1.0e50;
+    for (int k = 0; k < kBlock / TPO; ++k) mn = fmin(mn, smin[k]);
+    partial[blockIdx.x] = mn;
+  }
+}
+
+__global__ void k_min_reduce(int64_t m, const double* __restrict__ partial, double* __restrict__ out) {
+  __shared__ double s[kBlock];
+  double mn = 1.0e50;
+  for (int64_t k = threadIdx.x; k < m; k += blockDim.x) mn = fmin(mn, partial[k]);
+  s[threadIdx.x] = mn;
+  __syncthreads();
+  for (int o = kBlock / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) s[threadIdx.x] = fmin(s[threadIdx.x], s[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0];
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+static inline unsigned grid_for(int64_t n, int tpo) { return (unsigned)((n * tpo + kBlock - 1) / kBlock); }
+static inline unsigned grid1(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+#define PD_DISPATCH_TPO(tpo, KERNEL, GRID, ...)                                      \
+  switch (tpo) {                                                                     \
+    case 4: KERNEL<4><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;           \
+    case 8: KERNEL<8><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;           \
+    case 16: KERNEL<16><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;         \
+    default: KERNEL<32><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;         \
+  }
+
+cudaError_t launch_weighted_volume(const pd_ctx* c) {
+  if (c->n == 0) return cudaSuccess;
+  PD_DISPATCH_TPO(c->tpo, k_weighted_volume, grid_for(c->n, c->tpo), c->n, c->row.p, c->col.p, c->xv.p, c->hp.p,
+                  c->influence, c->pt.p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_owner(pd_ctx* c) {
+  if (c->n == 0) return cudaSuccess;
+  k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->coef.p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev) {
+  if (c->n == 0) return cudaSuccess;
+  k_state_from_y<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, y_dev, c->xv.p, c->st[c->cur].p, c->u.p,
+                                                        c->precision == PD_SPLIT_FP32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sync_state(pd_ctx* c) {
+  if (c->n == 0) return cudaSuccess;
+  k_state_from_u<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->u.p, c->xv.p, c->st[c->cur].p,
+                                                        c->precision == PD_SPLIT_FP32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_state_to_u(pd_ctx* c, double* u_out_dev) {
+  if (c->n == 0) return cudaSuccess;
+  k_state_to_u<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->st[c->cur].p, u_out_dev);
+  return cudaGetLastError();
+}
+
+// One model evaluation (damage -> dilatation -> force [-> Verlet epilogue]) on
+// the gathered state st[cur], with bond damage dmg updated in place.
+cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
+  if (c->n == 0) return cudaSuccess;
+  const unsigned grid = grid_for(c->n, c->tpo);
+  const bool split = c->precision == PD_SPLIT_FP32;
+  double4* st = c->st[c->cur].p;
+  cudaEvent_t* ev = nullptr;
+  if (c->ktime) {
+    if (c->kev_used + 3 > c->kev.size()) {
+      for (int k = 0; k < 3 * 256; ++k) {
+        cudaEvent_t e;
+        cudaError_t err = cudaEventCreate(&e);
+        if (err != cudaSuccess) return err;
+        c->kev.push_back(e);
+      }
+    }
+    ev = &c->kev[c->kev_used];
+    c->kev_used += 3;
+    cudaEventRecord(ev[0], c->stream);
+  }
+  if (split) {
+    PD_DISPATCH_TPO(c->tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->pt.p,
+                    c->coef.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->theta.p, c->node_damage.p);
+  } else {
+    PD_DISPATCH_TPO(c->tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->pt.p, c->sc.p,
+                    c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (ev) cudaEventRecord(ev[1], c->stream);
+  EpiArgs E;
+  E.dt = sp.dt;
+  E.t0 = sp.t0;
+  E.step = sp.step;
+  E.mode = sp.mode;
+  E.has_contact = sp.has_contact;
+  E.has_bc = sp.has_bc;
+  E.split = split;
+  E.fc = c->fc.p;
+  E.f_out = sp.f_out;
+  E.u = c->u.p;
+  E.v = c->v.p;
+  E.a = c->a.p;
+  E.bc_mask = c->bc_mask.p;
+  E.bc_a = c->bc_a.p;
+  E.bc_b = c->bc_b.p;
+  E.st_cur = st;
+  E.st_next = c->st[c->cur ^ 1].p;
+  E.status = c->status.p;
+  if (split) {
+    PD_DISPATCH_TPO(c->tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->pt.p, c->hp.p,
+                    c->influence, E);
+  } else {
+    PD_DISPATCH_TPO(c->tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->ab64.p, c->pt.p,
+                    c->hp.p, c->influence, E);
+  }
+  if (ev) cudaEventRecord(ev[2], c->stream);
+  return cudaGetLastError();
+}
+
+// Folds the recorded bond-pass events into c->kms (synchronizes on the last one).
+cudaError_t collect_kernel_times(pd_ctx* c) {
+  if (c->kev_used == 0) return cudaSuccess;
+  cudaError_t e = cudaEventSynchronize(c->kev[c->kev_used - 1]);
+  if (e != cudaSuccess) return e;
+  for (size_t k = 0; k + 3 <= c->kev_used; k += 3) {
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, c->kev[k], c->kev[k + 1]);
+    cudaEventElapsedTime(&b, c->kev[k + 1], c->kev[k + 2]);
+    c->kms[0] += a;
+    c->kms[1] += b;
+    c->klaunches += 1;
+  }
+  c->kev_used = 0;
+  return cudaSuccess;
+}
+
+cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out_dev) {
+  const unsigned grid = grid_for(c->n, c->tpo);
+  if (c->scratch.count < (size_t)grid + 1) {
+    cudaError_t e = c->scratch.alloc((size_t)grid + 1);
+    if (e != cudaSuccess) return e;
+  }
+  PD_DISPATCH_TPO(c->tpo, k_critical_dt, grid, c->n, c->row.p, c->col.p, c->xv.p, c->pt.p, c->hp.p, c->scratch.p);
+  k_min_reduce<<<1, kBlock, 0, c->stream>>>((int64_t)grid, c->scratch.p, dt_out_dev);
+  return cudaGetLastError();
+}
+
+}  // namespace pdb

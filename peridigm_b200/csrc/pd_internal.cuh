@@ -1,0 +1,196 @@
+// Internal declarations of the B200 Peridigm hot path: the device-side data
+// layout of a context and the kernels' launch helpers.
+//
+// HBM layout (n points, nb directed bonds, all in the caller's point order):
+//   xv[n]        double4 (x, y, z, V)             constant, 32 B, one sector per gather
+//   st[2][n]     double4 gathered state, double buffered across steps:
+//                  split-FP32 : (u_x, u_y, u_z, packed float2 {A, B})
+//                  FP64       : (y_x, y_y, y_z, 0)   y = current coordinates
+//   ab64[n]      double4 (theta, 3K/m - alpha/3, alpha, 0)  FP64 path only
+//   row[n+1]     int64 bond row pointers          col[nb] int32 neighbor ids
+//   dmg[nb]      uint8 bond damage (0/1), monotone, updated in place
+//   pt[n]        double4 (m, K, mu, rho) per-point material, sc[n] critical stretch
+//   coef[n]      float2 split-path owner coefficients ((3K-5mu)/m, 15mu/m)
+//   u[3n], v[3n], a[3n], f[3n], fc[3n] FP64 integration state (interleaved xyz)
+// A = theta*(3K-5mu)/m and B = 15mu/m are the owner terms of the LPS force
+// state t = (1-d)[A*omega*|xi| + (1-d)*B*omega*e] (elastic.cxx:99,119-120).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pd_b200.h"
+
+namespace pdb {
+
+// ---------------------------------------------------------------------------
+// Kernel parameter blocks
+// ---------------------------------------------------------------------------
+struct BondView {
+  const int64_t* row;
+  const int32_t* col;
+  uint8_t* dmg;
+  int64_t n;
+};
+
+struct StepParams {
+  // integration
+  double dt;
+  double t0;
+  int64_t step;     // step index n being completed by this evaluation (0 = initial)
+  int mode;         // EvalMode
+  int influence;
+  int damage_on;
+  int has_contact;
+  int has_bc;
+  // outputs
+  double* f_out;    // force density [3n] (may be null)
+};
+
+// EVAL_ONLY: evaluation (force out) with no integration; EVAL_ADVANCE: finish
+// evaluation `step` and advance the state to step+1; EVAL_LAST: finish the
+// last step (v, a final, no advance).
+enum EvalMode { EVAL_ONLY = 0, EVAL_ADVANCE = 2, EVAL_LAST = 3 };
+
+// ---------------------------------------------------------------------------
+// Device buffer
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t count = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  cudaError_t alloc(size_t n) {
+    release();
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void**)&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    count = n;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    count = 0;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+struct ContactState;
+struct QsState;
+
+}  // namespace pdb
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct pd_ctx {
+  int device = 0;
+  int precision = PD_SPLIT_FP32;
+  int influence = PD_INFLUENCE_ONE;
+  int tpo = 16;  // lanes per point
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // points
+  int64_t n = 0;
+  std::vector<double> hx, hvol;
+  std::vector<int32_t> hblock;
+  int32_t n_blocks = 1;
+  std::vector<double> block_h, block_K, block_mu, block_rho, block_sc;
+  bool have_material = false;
+  std::vector<double> field_K, field_mu, field_sc;  // per-point overrides (empty = none)
+  pdb::DBuf<double4> xv;
+  pdb::DBuf<double> hp;  // horizon per point
+
+  // bonds
+  int64_t nb = 0;
+  int max_row = 0;
+  bool symmetric = true;
+  pdb::DBuf<int64_t> row;
+  pdb::DBuf<int32_t> col;
+  pdb::DBuf<uint8_t> dmg;        // committed (N) bond damage
+  pdb::DBuf<uint8_t> dmg_trial;  // NP1 scratch for non-committing evaluations
+  bool trial_valid = false;
+
+  // material
+  bool wv_done = false;
+  pdb::DBuf<double4> pt;     // (m, K, mu, rho)
+  pdb::DBuf<double> sc;      // critical stretch (<0: off)
+  pdb::DBuf<float2> coef;    // split-path owner coefficients
+  bool any_damage = false;
+
+  // state
+  pdb::DBuf<double4> st[2];
+  int cur = 0;
+  pdb::DBuf<double4> ab64;
+  pdb::DBuf<double> u, v, a, f, fc, theta, node_damage;
+  bool state_init = false;
+
+  // boundary conditions
+  std::vector<uint8_t> h_bc_mask;
+  std::vector<double> h_bc_a, h_bc_b;
+  bool bc_dirty = true;
+  bool has_bc = false;
+  pdb::DBuf<uint8_t> bc_mask;
+  pdb::DBuf<double> bc_a, bc_b;
+
+  // misc
+  pdb::DBuf<int> status;      // device status word (non-finite etc.)
+  pdb::DBuf<double> scratch;  // reduction partials
+  bool ktime = false;                 // bracket bond-pass launches with events
+  std::vector<cudaEvent_t> kev;        // 3 per evaluation while ktime
+  size_t kev_used = 0;
+  double kms[2] = {0.0, 0.0};
+  int64_t klaunches = 0;
+  pdb::ContactState* contact = nullptr;
+  pdb::QsState* qs = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// Launch helpers (implemented in the .cu files)
+// ---------------------------------------------------------------------------
+namespace pdb {
+
+cudaError_t launch_weighted_volume(const pd_ctx* c);
+cudaError_t launch_pack_owner(pd_ctx* c);
+cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg);
+cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev);
+cudaError_t launch_sync_state(pd_ctx* c);
+cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out);
+cudaError_t launch_state_to_u(pd_ctx* c, double* u_out_dev);
+cudaError_t collect_kernel_times(pd_ctx* c);
+
+// bonds
+int build_bonds_device(pd_ctx* c, const pd_plane_filter* filters, int nf);
+int finalize_bonds(pd_ctx* c, bool sort_rows);
+
+// contact (k_contact.cu) and quasi-static state hooks
+void contact_release(pd_ctx* c);
+int contact_prepare(pd_ctx* c, int64_t step);  // search when due at this step
+int contact_eval(pd_ctx* c);                   // contact force density into c->fc
+int64_t contact_pairs(const pd_ctx* c);
+void qs_release(pd_ctx* c);
+
+// status bits
+enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4 };
+
+}  // namespace pdb
+
+#define PD_CUDA_TRY(ctx, expr)                                                   \
+  do {                                                                           \
+    cudaError_t e_ = (expr);                                                     \
+    if (e_ != cudaSuccess) {                                                     \
+      (ctx)->err = std::string(#expr) + ": " + cudaGetErrorString(e_);           \
+      return e_ == cudaErrorMemoryAllocation ? PD_ERR_NOMEM : PD_ERR_CUDA;       \
+    }                                                                            \
+  } while (0)

@@ -235,8 +235,46 @@ def wave_in_bar():
     np.savez_compressed(os.path.join(OUT, "wave_in_bar.npz"), **out)
 
 
+# ---------------------------------------------------------------------------
+# 4. FinitePlane filter known answers (src/io/pdneigh/unit_test/utFinitePlaneFilter.cxx)
+# ---------------------------------------------------------------------------
+def finite_plane():
+    """Planes of getCase_1a..3a (:118-161) and the expected exclusion flags of
+    each point over the 8 corner points of a unit cube (:200-209, :310-319,
+    :420-429, :528-537, :638-647), parsed from the reference test file."""
+    import re
+
+    path = os.path.join(REF, "src/io/pdneigh/unit_test/utFinitePlaneFilter.cxx")
+    src = open(path).read()
+    s2 = math.sqrt(2.0)
+    env = {"sqrt2": s2, "sqrt": math.sqrt}
+    cases = {}
+    for name in ["1a", "1b", "2a", "2b", "3a"]:
+        body = re.search(r"FinitePlane getCase_%s\(\)\{(.*?)\n\}" % name, src, re.S).group(1)
+        vals = {}
+        for var in ["n", "r0", "ub"]:
+            comps = []
+            for k in range(3):
+                expr = re.search(r"%s\[%d\]\s*=\s*([^;]+);" % (var, k), body).group(1)
+                comps.append(eval(expr, {}, env))
+            vals[var] = comps
+        for var in ["a", "b"]:
+            vals[var] = eval(re.search(r"\b%s\s*=\s*([^,;]+)[,;]" % var, body).group(1), {}, env)
+        test = src[src.index("FinitePlane plane = getCase_%s();" % name):]
+        flags = []
+        for k in range(8):
+            arr = re.search(r"bool n%d\[\]\s*=\s*\{([^}]*)\}" % k, test).group(1)
+            flags.append([int(t) for t in arr.split(",")])
+        cases[name] = {"normal": vals["n"], "lower_left": vals["r0"], "bottom_unit": vals["ub"],
+                       "bottom_length": vals["b"], "side_length": vals["a"], "exclude": flags}
+    pts = [0, 0, 0, 1, 0, 0, 0, 1, 0, 1, 1, 0, 0, 0, 1, 1, 0, 1, 0, 1, 1, 1, 1, 1]
+    with open(os.path.join(OUT, "finite_plane.json"), "w") as fh:
+        json.dump({"points": pts, "horizon": 1.1 * math.sqrt(3.0), "cases": cases}, fh, indent=1)
+
+
 def main():
     unit_elastic()
+    finite_plane()
     bond_breaking()
     contact_2x1x1()
     wave_in_bar()

@@ -1,0 +1,179 @@
+"""GPU velocity-Verlet runs against the reference's gold files and the oracle.
+
+* BondBreakingInitialVelocity gold (Disp/Vel 1e-9, Damage 1e-3, .comp file):
+  both precisions; final node damage [0,1,0,1] exactly.
+* WaveInBar gold (.comp tolerances) on the FP64 path; the split path within
+  stated looser bounds (1e-6 of the field's max).
+* Notched plate vs the oracle explicit run: FP64 u relative error <= 1e-9.
+* Determinism (no atomics): two runs are bit-identical.
+* Full-size (320,000-point notched plate) size-independent properties.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from peridigm_b200 import Context, workloads
+
+pytestmark = pytest.mark.gpu
+G = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_bond_breaking_gold(precision):
+    z = np.load(os.path.join(G, "bond_breaking.npz"))
+    rho, K, mu, h, sc, dt, T = z["params"]
+    with Context(precision=precision) as ctx:
+        ctx.set_points(z["x"].ravel(), z["vol"])
+        ctx.set_horizons([h])
+        ctx.set_bonds(z["nl"])
+        ctx.material(K, mu, rho)
+        ctx.critical_stretch(sc)
+        ctx.set_state(np.zeros(12), z["v0"])
+        # one run of 8000 steps, read at the end; and checkpoints via chained runs
+        for k in range(8):
+            ctx.verlet_run(dt, 1000, t0=k * 1000 * dt)
+            u, v, d = ctx.field("Displacement"), ctx.field("Velocity"), ctx.field("Damage")
+            gu, gv = z["disp_y"][k + 1], z["vel_y"][k + 1]
+            if precision == "fp64":  # .comp tolerances
+                assert np.abs(u[1::3] - gu).max() < 1e-9
+                assert np.abs(v[1::3] - gv).max() < 1e-9
+            else:  # split-FP32 bond arithmetic: 1e-6 of the field's magnitude
+                assert np.abs(u[1::3] - gu).max() < 1e-6 * np.abs(gu).max()
+                assert np.abs(v[1::3] - gv).max() < 1e-6 * np.abs(gv).max()
+            assert np.abs(d - z["damage"][k + 1]).max() < 1e-3
+    assert list(d) == [0.0, 1.0, 0.0, 1.0]
+
+
+def _wave_setup(ctx, z):
+    rho, K, mu, h, dt, T, fq = z["params"]
+    n = len(z["vol"])
+    ctx.set_points(z["x"].ravel(), z["vol"])
+    ctx.set_horizons([h])
+    ctx.build_bonds()
+    ctx.material(K, mu, rho)
+    v = np.zeros(3 * n)
+    v[3 * z["initial_velocity_points"]] = -100.0
+    ctx.set_state(np.zeros(3 * n), v)
+    return dt, int(fq)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_wave_in_bar_gold(precision):
+    z = np.load(os.path.join(G, "wave_in_bar.npz"))
+    with Context(precision=precision) as ctx:
+        dt, fq = _wave_setup(ctx, z)
+        assert np.abs(ctx.weighted_volume() - z["Weighted_Volume"][0]).max() < 1e-15
+        prev = 0
+        for k, kk in enumerate(z["keep"]):
+            s = int(kk) * fq
+            if s > prev:
+                ctx.verlet_run(dt, s - prev, t0=prev * dt)
+                prev = s
+            else:
+                ctx.verlet_run(dt, 0)
+            u, v, f, th = (ctx.field(nm) for nm in ("Displacement", "Velocity", "Force_Density", "Dilatation"))
+            for c, ax in enumerate("XYZ"):
+                gu, gv, gf = z["Displacement" + ax][k], z["Velocity" + ax][k], z["Force_Density" + ax][k]
+                if precision == "fp64":
+                    assert np.abs(u[c::3] - gu).max() < 5e-14
+                    assert np.abs(v[c::3] - gv).max() < 1e-8
+                    assert np.abs(f[c::3] - gf).max() < 5.0
+                else:
+                    assert np.abs(u[c::3] - gu).max() <= 1e-6 * max(np.abs(gu).max(), 1e-9)
+                    assert np.abs(v[c::3] - gv).max() <= 1e-6 * max(np.abs(gv).max(), 1.0)
+                    assert np.abs(f[c::3] - gf).max() <= 1e-6 * max(np.abs(gf).max(), 1.0)
+            if precision == "fp64":
+                assert np.abs(th - z["Dilatation"][k]).max() < 5e-13
+            else:
+                assert np.abs(th - z["Dilatation"][k]).max() < 1e-6 * max(np.abs(z["Dilatation"][k]).max(), 1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_notched_plate_matches_oracle(precision):
+    w = workloads.notched_plate(nx=48, ny=30, nz=4, h=0.5e-3, notch_cells=12, s_c=2.0e-4, pull=5.0)
+    nsteps = 150
+    with Context(precision=precision) as ctx:
+        workloads.setup_context(ctx, w)
+        dt = 0.7 * ctx.critical_time_step()
+        row, col = ctx.bonds_csr()
+        st = ctx.verlet_run(dt, nsteps)
+        u, v, bd = ctx.field("Displacement"), ctx.field("Velocity"), ctx.field("Bond_Damage")
+    ref = O.explicit_run(workloads.oracle_problem(w, row, col, dt, nsteps), np.zeros_like(w["x"]), w["v0"])
+    assert st["broken_bonds"] > 0, "the case should break bonds"
+    if precision == "fp64":
+        assert np.array_equal(bd, ref["bond_damage"])
+        assert np.abs(u - ref["u"]).max() <= 1e-9 * np.abs(ref["u"]).max()
+        assert np.abs(v - ref["v"]).max() <= 1e-9 * np.abs(ref["v"]).max()
+    else:
+        # one-step shadow: the same state through both evaluators gives the same breaks
+        diff = np.sum(bd != ref["bond_damage"])
+        assert diff <= 0.01 * max(st["broken_bonds"], 1)
+        assert np.abs(u - ref["u"]).max() <= 2e-3 * np.abs(ref["u"]).max()
+
+
+def test_split_one_step_shadow_force_and_breaks():
+    """Same state through FP64 oracle and split kernels: forces <= 1e-6 (L2) and the
+    break sets identical except bonds within 1e-6*s_c of s_c."""
+    w = workloads.notched_plate(nx=48, ny=30, nz=4, h=0.5e-3, notch_cells=12, s_c=2.0e-4, pull=5.0)
+    with Context(precision="fp64") as ctx:
+        workloads.setup_context(ctx, w)
+        dt = 0.7 * ctx.critical_time_step()
+        ctx.verlet_run(dt, 120)
+        y = ctx.field("Coordinates")
+        bd0 = ctx.field("Bond_Damage")
+        row, col = ctx.bonds_csr()
+    s_c = w["s_c"]
+    ref = O.eval_model(w["x"], y, w["vol"], row, col, w["K"], w["mu"], w["horizon"], s_c=s_c, dmg_n=bd0)
+    with Context(precision="split") as ctx:
+        workloads.setup_context(ctx, w)
+        ctx.set_bond_damage(bd0)
+        f = ctx.compute_force(y)
+        bd = ctx.field("Bond_Damage")
+    owner = np.repeat(np.arange(len(w["vol"])), np.diff(row))
+    P, Y = w["x"].reshape(-1, 3), y.reshape(-1, 3)
+    L0 = np.linalg.norm(P[col] - P[owner], axis=1)
+    s = (np.linalg.norm(Y[col] - Y[owner], axis=1) - L0) / L0
+    near = np.abs(s - s_c) <= 1e-6 * s_c
+    assert np.array_equal(bd[~near], ref["bond_damage"][~near])
+    assert np.linalg.norm(f - ref["force"]) / np.linalg.norm(ref["force"]) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_deterministic(precision):
+    w = workloads.notched_plate(nx=40, ny=24, nz=3, h=0.5e-3, notch_cells=10, s_c=2.0e-4, pull=5.0)
+    out = []
+    for _ in range(2):
+        with Context(precision=precision) as ctx:
+            workloads.setup_context(ctx, w)
+            dt = 0.7 * ctx.critical_time_step()
+            ctx.verlet_run(dt, 100)
+            out.append((ctx.field("Displacement"), ctx.field("Bond_Damage")))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_full_size_notched_plate_properties():
+    """320,000 points (400x200x4, jitter seed 1): the bond family equals the
+    oracle's, families are symmetric, internal forces conserve momentum
+    (sum_i V_i f_i = 0), and split vs FP64 forces agree to 1e-6 (L2)."""
+    w = workloads.notched_plate()
+    row, col = O.neighbor_search(w["x"], w["horizon"], w["planes"])
+    with Context(precision="split") as cs, Context(precision="fp64") as cd:
+        for ctx in (cs, cd):
+            workloads.setup_context(ctx, w)
+        r2, c2 = cs.bonds_csr()
+        assert np.array_equal(r2, row) and np.array_equal(c2, col)
+        dt = 0.7 * cd.critical_time_step()
+        cd.verlet_run(dt, 200)
+        y = cd.field("Coordinates")
+        bd = cd.field("Bond_Damage")
+        cs.set_bond_damage(bd)
+        cd.set_bond_damage(bd)
+        fs = cs.compute_force(y)
+        fd = cd.compute_force(y)
+    V = np.repeat(w["vol"], 3)
+    for f in (fs, fd):
+        mom = (V * f).reshape(-1, 3).sum(0)
+        assert np.all(np.abs(mom) <= 1e-5 * np.abs(V * f).reshape(-1, 3).sum(0))
+    assert np.linalg.norm(fs - fd) / np.linalg.norm(fd) < 1e-6

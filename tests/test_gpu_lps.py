@@ -1,0 +1,183 @@
+"""GPU parity of the LPS / damage / search kernels against the CPU oracle.
+
+Tolerances (stated per test):
+* FP64 path: the reference's own unit-test tolerances on the known answers;
+  relative L2 force error <= 1e-11 against the oracle on the same inputs.
+* split-FP32 path: relative L2 force error <= 1e-6, per-point force error
+  <= 1e-5 of max|f|, bond-break sets identical except bonds whose FP64
+  stretch lies within 1e-6*s_c of s_c.
+* bond families and neighbor lists: bit-exact.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from peridigm_b200 import Context, PDError, plugins, workloads
+
+pytestmark = pytest.mark.gpu
+G = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def make_cloud(nx=10, ny=9, nz=7, h=1.0e-3, seed=0, strain=2e-3):
+    x, vol = workloads.lattice(nx, ny, nz, h, jitter=0.05, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    P = x.reshape(-1, 3)
+    u = np.zeros_like(P)
+    u[:, 0] = strain * P[:, 0] + 0.3 * strain * np.sin(P[:, 1] / (3 * h))
+    u[:, 1] = -0.3 * strain * P[:, 1] + 0.5 * strain * P[:, 2]
+    u[:, 2] = 0.2 * strain * np.cos(P[:, 0] / (4 * h)) * h
+    u += rng.normal(0, 1e-3 * strain * h, size=u.shape)
+    return x, vol, (P + u).ravel(), 3.015 * h
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+@pytest.mark.parametrize("case", ["two_pts", "eight_pts", "three_pts"])
+def test_unit_elastic_known_answers(case, precision):
+    """testTwoPts / testEightPts / testThreePts through the ElasticMaterial mirror."""
+    c = json.load(open(os.path.join(G, "unit_elastic.json")))[case]
+    n = len(c["vol"])
+    nl = np.array(c["nl"], np.int32)
+    dm = plugins.DataManager(n, len(nl) - n)
+    dm.getData("Model_Coordinates")[:] = c["x"]
+    dm.getData("Volume")[:] = c["vol"]
+    dm.getData("Coordinates", "NP1")[:] = c["y"]
+    mat = plugins.ElasticMaterial({"Density": 7800.0, "Bulk Modulus": c["K"], "Shear Modulus": c["mu"],
+                                   "Horizon": c["horizon"]}, precision=precision)
+    mat.initialize(1.0, n, np.arange(n), nl, dm)
+    mat.computeForce(1.0, n, np.arange(n), nl, dm)
+    m, th, f = dm.getData("Weighted_Volume"), dm.getData("Dilatation", "NP1"), dm.getData("Force_Density", "NP1")
+    tol = (lambda t: t) if precision == "fp64" else (lambda t: max(t, 2e-6))
+    np.testing.assert_allclose(m, c["m"], rtol=c["m_tol"], atol=0)
+    np.testing.assert_allclose(th, c["theta"], rtol=tol(c["theta_tol"]), atol=0)
+    fe = np.array(c["force"])
+    big = np.abs(fe) > 1e-3 * np.abs(fe).max()
+    np.testing.assert_allclose(f[big], fe[big], rtol=tol(c["force_tol"]))
+    assert np.all(np.abs(f[~big]) <= 1e-3 * np.abs(fe).max())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_eval_model_matches_oracle(precision):
+    """Weighted volume, dilatation, force and damage on a jittered lattice with a
+    smooth non-uniform deformation and some bonds already broken."""
+    x, vol, y, h = make_cloud()
+    row, col = O.neighbor_search(x, h)
+    rng = np.random.default_rng(7)
+    # symmetric pre-broken bonds
+    bd = np.zeros(len(col))
+    n = len(vol)
+    owner = np.repeat(np.arange(n), np.diff(row))
+    pick = rng.random(len(col)) < 0.05
+    pairs = {(min(i, j), max(i, j)) for i, j, p in zip(owner, col, pick) if p}
+    for b, (i, j) in enumerate(zip(owner, col)):
+        if (min(i, j), max(i, j)) in pairs:
+            bd[b] = 1.0
+    K, mu = 130e9, 78e9
+    ref = O.eval_model(x, y, vol, row, col, K, mu, h, s_c=1.5e-3, dmg_n=bd)
+    with Context(precision=precision) as ctx:
+        ctx.set_points(x, vol)
+        ctx.set_horizons([h])
+        ctx.build_bonds()
+        r2, c2 = ctx.bonds_csr()
+        assert np.array_equal(r2, row) and np.array_equal(c2, col)
+        ctx.material(K, mu, 7800.0)
+        ctx.critical_stretch(1.5e-3)
+        ctx.set_bond_damage(bd)
+        f = ctx.compute_force(y)
+        m = ctx.weighted_volume()
+        th = ctx.field("Dilatation")
+        bdn = ctx.field("Bond_Damage")
+        nd = ctx.field("Damage")
+    np.testing.assert_allclose(m, ref["m"], rtol=1e-14)
+    if precision == "fp64":
+        assert np.array_equal(bdn, ref["bond_damage"])
+        np.testing.assert_allclose(nd, ref["damage"], rtol=0, atol=1e-15)
+        assert rel_l2(th, ref["theta"]) < 1e-12
+        assert rel_l2(f, ref["force"]) < 1e-11
+    else:
+        # stretch of every bond in FP64 decides which breaks may differ
+        P, Y = x.reshape(-1, 3), y.reshape(-1, 3)
+        s = (np.linalg.norm(Y[col] - Y[owner], axis=1) - np.linalg.norm(P[col] - P[owner], axis=1)) / \
+            np.linalg.norm(P[col] - P[owner], axis=1)
+        near = np.abs(s - 1.5e-3) <= 1e-6 * 1.5e-3
+        assert np.array_equal(bdn[~near], ref["bond_damage"][~near])
+        if not near.any():
+            assert rel_l2(th, ref["theta"]) < 1e-6
+            assert rel_l2(f, ref["force"]) < 1e-6
+            assert np.abs(f - ref["force"]).max() < 1e-5 * np.abs(ref["force"]).max()
+
+
+@pytest.mark.parametrize("case", ["1a", "1b", "2a", "2b", "3a"])
+def test_finite_plane_known_answers(case):
+    d = json.load(open(os.path.join(G, "finite_plane.json")))
+    c = d["cases"][case]
+    with Context() as ctx:
+        ctx.set_points(d["points"], np.ones(8))
+        ctx.set_horizons([d["horizon"]])
+        ctx.build_bonds([c])
+        row, col = ctx.bonds_csr()
+    for i in range(8):
+        assert set(col[row[i]:row[i + 1]].tolist()) == {j for j in range(8) if not c["exclude"][i][j]}
+
+
+def test_bond_family_bit_exact_with_notch():
+    w = workloads.notched_plate(nx=60, ny=40, nz=4, h=0.5e-3, notch_cells=15)
+    row, col = O.neighbor_search(w["x"], w["horizon"], w["planes"])
+    with Context() as ctx:
+        ctx.set_points(w["x"], w["vol"])
+        ctx.set_horizons([w["horizon"]])
+        ctx.build_bonds(w["planes"])
+        r2, c2 = ctx.bonds_csr()
+        nl = ctx.get_bonds()
+    assert np.array_equal(r2, row) and np.array_equal(c2, col)
+    assert np.array_equal(nl, O.csr_to_nl(row, col))
+
+
+def test_critical_time_step_matches_oracle():
+    x, vol, y, h = make_cloud()
+    row, col = O.neighbor_search(x, h)
+    with Context(precision="fp64") as ctx:
+        ctx.set_points(x, vol)
+        ctx.set_horizons([h])
+        ctx.set_bonds(O.csr_to_nl(row, col))
+        ctx.material(130e9, 78e9, 7800.0)
+        dt = ctx.critical_time_step()
+    assert dt == O.critical_time_step(x, vol, row, col, 130e9, 7800.0, h)
+
+
+def test_device_pointer_entry():
+    """pd_compute_force_device on torch-owned device buffers equals the host entry."""
+    torch = pytest.importorskip("torch")
+    x, vol, y, h = make_cloud(seed=4)
+    with Context(precision="split") as ctx:
+        ctx.set_points(x, vol)
+        ctx.set_horizons([h])
+        ctx.build_bonds()
+        ctx.material(130e9, 78e9, 7800.0)
+        f_host = ctx.compute_force(y)
+        yd = torch.tensor(y, dtype=torch.float64, device="cuda")
+        fd = torch.zeros_like(yd)
+        torch.cuda.synchronize()
+        ctx.compute_force_device(yd.data_ptr(), fd.data_ptr())
+        assert np.array_equal(fd.cpu().numpy(), f_host)
+
+
+def test_errors_are_reported():
+    with Context() as ctx:
+        with pytest.raises(PDError):
+            ctx.compute_force(np.zeros(3))  # no points
+        ctx.set_points(np.zeros(6) + np.array([0, 0, 0, 1, 0, 0.0]), np.ones(2))
+        with pytest.raises(PDError):
+            ctx.set_bonds(np.array([1, 5, 0], np.int32))  # neighbor id out of range
+        ctx.set_bonds(np.array([1, 1, 0], np.int32))  # 0->1 without 1->0
+        ctx.set_horizons([2.0])
+        ctx.material(1.0, 1.0, 1.0)
+        with pytest.raises(PDError) as e:
+            ctx.compute_force(np.zeros(6))
+        assert e.value.code == 6
