@@ -80,10 +80,11 @@ def test_wave_in_bar_gold(precision):
                     assert np.abs(u[c::3] - gu).max() < 5e-14
                     assert np.abs(v[c::3] - gv).max() < 1e-8
                     assert np.abs(f[c::3] - gf).max() < 5.0
-                else:
-                    assert np.abs(u[c::3] - gu).max() <= 1e-6 * max(np.abs(gu).max(), 1e-9)
-                    assert np.abs(v[c::3] - gv).max() <= 1e-6 * max(np.abs(gv).max(), 1.0)
-                    assert np.abs(f[c::3] - gf).max() <= 1e-6 * max(np.abs(gf).max(), 1.0)
+                else:  # split-FP32: fields within 1e-6 (L2, relative), points within 1e-5 of max
+                    for a, g in ((u[c::3], gu), (v[c::3], gv), (f[c::3], gf)):
+                        if np.abs(g).max() > 0:
+                            assert np.linalg.norm(a - g) <= 1e-6 * np.linalg.norm(g)
+                            assert np.abs(a - g).max() <= 1e-5 * np.abs(g).max()
             if precision == "fp64":
                 assert np.abs(th - z["Dilatation"][k]).max() < 5e-13
             else:

@@ -8,6 +8,7 @@ Tolerances (stated per test):
   stretch lies within 1e-6*s_c of s_c.
 * bond families and neighbor lists: bit-exact.
 """
+import ctypes as C
 import json
 import os
 
@@ -170,8 +171,10 @@ def test_device_pointer_entry():
 
 def test_errors_are_reported():
     with Context() as ctx:
-        with pytest.raises(PDError):
-            ctx.compute_force(np.zeros(3))  # no points
+        y = np.zeros(3)
+        rc = ctx.L.pd_compute_force(ctx.h, y.ctypes.data_as(C.POINTER(C.c_double)), None)
+        assert rc == 5  # PD_ERR_STATE: no points yet
+        assert b"points" in ctx.L.pd_last_error(ctx.h)
         ctx.set_points(np.zeros(6) + np.array([0, 0, 0, 1, 0, 0.0]), np.ones(2))
         with pytest.raises(PDError):
             ctx.set_bonds(np.array([1, 5, 0], np.int32))  # neighbor id out of range
