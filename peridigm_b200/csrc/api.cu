@@ -53,7 +53,10 @@ int upload_material(pd_ctx* c) {
   }
   PD_CUDA_TRY(c, c->pt.alloc(n));
   PD_CUDA_TRY(c, c->sc.alloc(n));
-  PD_CUDA_TRY(c, c->coef.alloc(n));
+  if (c->precision == PD_SPLIT_FP32) {
+    PD_CUDA_TRY(c, c->xr.alloc(n));
+    PD_CUDA_TRY(c, c->own.alloc(n));
+  }
   PD_CUDA_TRY(c, cudaMemcpy(c->pt.p, pt.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
   PD_CUDA_TRY(c, cudaMemcpy(c->sc.p, sc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
   PD_CUDA_TRY(c, cudaMemcpy(c->hp.p, hp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
@@ -69,11 +72,16 @@ int upload_horizons(pd_ctx* c) {
 }
 
 int alloc_state(pd_ctx* c) {
-  if (c->st[0].count >= (size_t)c->n && c->u.count >= (size_t)(3 * c->n) && c->n > 0) return PD_OK;
+  if (c->u.count >= (size_t)(3 * c->n) && c->n > 0) return PD_OK;
   const int64_t n = c->n;
   for (int k = 0; k < 2; ++k) {
-    PD_CUDA_TRY(c, c->st[k].alloc(n));
-    PD_CUDA_TRY(c, cudaMemset(c->st[k].p, 0, c->st[k].bytes()));
+    if (c->precision == PD_SPLIT_FP32) {
+      PD_CUDA_TRY(c, c->ur[k].alloc(n));
+      PD_CUDA_TRY(c, cudaMemset(c->ur[k].p, 0, c->ur[k].bytes()));
+    } else {
+      PD_CUDA_TRY(c, c->st[k].alloc(n));
+      PD_CUDA_TRY(c, cudaMemset(c->st[k].p, 0, c->st[k].bytes()));
+    }
   }
   PD_CUDA_TRY(c, c->ab64.alloc(c->precision == PD_FP64 ? n : 1));
   PD_CUDA_TRY(c, c->u.alloc(3 * n));
@@ -163,7 +171,7 @@ int pd_create(const pd_config* cfg, pd_ctx** out) {
     c->device = cfg->device;
     c->precision = cfg->precision;
     c->influence = cfg->influence;
-    if (cfg->threads_per_point) c->tpo = cfg->threads_per_point;
+    if (cfg->threads_per_point) c->tpo = c->tpo_split = cfg->threads_per_point;
   }
   if (c->precision != PD_FP64 && c->precision != PD_SPLIT_FP32) {
     delete c;
@@ -242,7 +250,10 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   c->field_K.clear();
   c->field_mu.clear();
   c->field_sc.clear();
-  for (int k = 0; k < 2; ++k) c->st[k].release();
+  for (int k = 0; k < 2; ++k) {
+    c->st[k].release();
+    c->ur[k].release();
+  }
   c->u.release();
   c->state_init = false;
   return PD_OK;
@@ -585,15 +596,7 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
   switch (field) {
     case PD_FIELD_DISPLACEMENT:
     case PD_FIELD_COORDINATES: {
-      if (c->precision == PD_SPLIT_FP32) {
-        DBuf<double> tmp;
-        PD_CUDA_TRY(c, tmp.alloc(3 * n));
-        PD_CUDA_TRY(c, launch_state_to_u(c, tmp.p));
-        PD_CUDA_TRY(c, cudaMemcpyAsync(out, tmp.p, b3, cudaMemcpyDeviceToHost, c->stream));
-        PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-      } else {
-        PD_CUDA_TRY(c, cudaMemcpy(out, c->u.p, b3, cudaMemcpyDeviceToHost));
-      }
+      PD_CUDA_TRY(c, cudaMemcpy(out, c->u.p, b3, cudaMemcpyDeviceToHost));
       if (field == PD_FIELD_COORDINATES)
         for (int64_t k = 0; k < 3 * n; ++k) out[k] = c->hx[k] + out[k];
       return PD_OK;

@@ -1,16 +1,24 @@
 // LPS elastic + critical-stretch damage + velocity-Verlet kernels (sm_100a).
 //
 // Two bond passes per evaluation, both gathers, no atomics:
-//   pass 1 (k_damage_dilatation): per bond, critical-stretch test and the
+//   pass 1 (k_dilatation_*): per bond, critical-stretch test and the
 //     dilatation term; per point theta, node damage and the owner force-state
-//     coefficients (A, B) the second pass gathers.
-//   pass 2 (k_force): per bond f_i += (t_ij + t_ji) * Y/|Y| * V_j, the gather
+//     terms the second pass gathers.
+//   pass 2 (k_force_*): per bond f_i += (t_ij + t_ji) * Y/|Y| * V_j, the gather
 //     form of the reference's scatter (elastic.cxx:125-130: the owner adds
 //     t_ij*Y*V_j, the neighbor's own loop subtracts t_ji*(-Y)*V_j), followed
 //     by the Verlet epilogue of Peridigm::executeExplicit (Peridigm.cpp:1480-1577).
 // A group of TPO consecutive lanes owns one point's bond family; lanes stride
 // through the row (coalesced col/damage loads), partial sums are combined by
 // a fixed xor-shuffle tree, so results are deterministic.
+//
+// Split-FP32 path data (one 32-byte record per point, fetched with one
+// 256-bit load per neighbor):
+//   xr[j] = (x_hi[3], x_lo[3], V, h)   x_hi = fp32(x), x_lo = fp32(x - x_hi)
+//   ur[j] = (u_hi[3], u_lo[3], A, B)   same split of the FP64 displacement
+// X = (x_hi_j - x_hi_i) + (x_lo_j - x_lo_i) is the bond vector to within one
+// FP32 ulp, with no FP64 instruction in the bond loop; likewise du. The FP64
+// displacement u[3n] stays the integration state.
 #include <math.h>
 
 #include "pd_internal.cuh"
@@ -50,30 +58,67 @@ __device__ __forceinline__ double sq3_rn(double dx, double dy, double dz) {
   return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-template <int TPO>
-__device__ __forceinline__ float group_sum(float v) {
-#pragma unroll
-  for (int o = TPO / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-template <int TPO>
-__device__ __forceinline__ double group_sum(double v) {
-#pragma unroll
-  for (int o = TPO / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-template <int TPO>
-__device__ __forceinline__ int group_sum(int v) {
+template <int TPO, typename T>
+__device__ __forceinline__ T group_sum(T v) {
 #pragma unroll
   for (int o = TPO / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
-__device__ __forceinline__ double pack_ab(float A, float B) {
-  return __hiloint2double(__float_as_int(B), __float_as_int(A));
+// 256-bit record loads. nc: read-only path, for data no thread writes during
+// the kernel. The coherent form is used where another lane of the same kernel
+// writes other bytes of the same records.
+__device__ __forceinline__ Rec8 ld_rec_nc(const Rec8* p) {
+  Rec8 r;
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]),
+        "=f"(r.v[7])
+      : "l"(p));
+  return r;
 }
-__device__ __forceinline__ float2 unpack_ab(double w) {
-  return make_float2(__int_as_float(__double2loint(w)), __int_as_float(__double2hiint(w)));
+__device__ __forceinline__ Rec8 ld_rec(const Rec8* p) {
+  Rec8 r;
+  asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]),
+                 "=f"(r.v[6]), "=f"(r.v[7])
+               : "l"(p)
+               : "memory");
+  return r;
+}
+
+__device__ __forceinline__ void split_hi_lo(double v, float* hi, float* lo) {
+  const float h = __double2float_rn(v);
+  *hi = h;
+  *lo = __double2float_rn(v - (double)h);
+}
+
+// Bond geometry of the split path (identical operations in both passes and,
+// with both endpoints swapped, exactly negated X, du, Y: bond damage stays
+// symmetric).
+struct SplitBond {
+  float Yx, Yy, Yz, zeta, ry, e;
+};
+__device__ __forceinline__ SplitBond split_bond(const Rec8& xi, const Rec8& ui, const Rec8& xj, const Rec8& uj) {
+  SplitBond s;
+  const float Xx = (xj.v[0] - xi.v[0]) + (xj.v[3] - xi.v[3]);
+  const float Xy = (xj.v[1] - xi.v[1]) + (xj.v[4] - xi.v[4]);
+  const float Xz = (xj.v[2] - xi.v[2]) + (xj.v[5] - xi.v[5]);
+  const float Ux = (uj.v[0] - ui.v[0]) + (uj.v[3] - ui.v[3]);
+  const float Uy = (uj.v[1] - ui.v[1]) + (uj.v[4] - ui.v[4]);
+  const float Uz = (uj.v[2] - ui.v[2]) + (uj.v[5] - ui.v[5]);
+  const float xx = fmaf(Xz, Xz, fmaf(Xy, Xy, Xx * Xx));
+  s.Yx = Xx + Ux;
+  s.Yy = Xy + Uy;
+  s.Yz = Xz + Uz;
+  const float yy = fmaf(s.Yz, s.Yz, fmaf(s.Yy, s.Yy, s.Yx * s.Yx));
+  const float rx = rsqrtf(xx);
+  s.ry = rsqrtf(yy);
+  s.zeta = xx * rx;
+  const float dY = yy * s.ry;
+  const float xu = fmaf(Xz, Uz, fmaf(Xy, Uy, Xx * Ux));
+  const float uu = fmaf(Uz, Uz, fmaf(Uy, Uy, Ux * Ux));
+  s.e = __fdividef(fmaf(2.0f, xu, uu), dY + s.zeta);  // |Y| - |X| without cancellation
+  return s;
 }
 
 // ---------------------------------------------------------------------------
@@ -104,28 +149,37 @@ __global__ void __launch_bounds__(kBlock) k_weighted_volume(int64_t n, const int
   if (valid && lane == 0) pt[i].x = acc;
 }
 
-// Split-path owner coefficients: A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m.
-__global__ void k_pack_owner(int64_t n, const double4* __restrict__ pt, float2* __restrict__ coef) {
+// Split-path constant records: xr = (x_hi, x_lo, V, h) and owner terms
+// own = (3/m, (3K-5mu)/m, 15mu/m, s_c).
+__global__ void k_pack_owner(int64_t n, const double4* __restrict__ xv, const double4* __restrict__ pt,
+                             const double* __restrict__ sc, const double* __restrict__ hp, Rec8* __restrict__ xr,
+                             float4* __restrict__ own) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const double4 x = xv[i];
+  Rec8 r;
+  split_hi_lo(x.x, &r.v[0], &r.v[3]);
+  split_hi_lo(x.y, &r.v[1], &r.v[4]);
+  split_hi_lo(x.z, &r.v[2], &r.v[5]);
+  r.v[6] = (float)x.w;
+  r.v[7] = (float)hp[i];
+  xr[i] = r;
   const double4 p = pt[i];  // (m, K, mu, rho)
-  const double m = p.x;
-  coef[i] = make_float2((float)((3.0 * p.y - 5.0 * p.z) / m), (float)(15.0 * p.z / m));
+  own[i] = make_float4((float)(3.0 / p.x), (float)((3.0 * p.y - 5.0 * p.z) / p.x), (float)(15.0 * p.z / p.x),
+                       (float)sc[i]);
 }
 
 // ---------------------------------------------------------------------------
 // K2: damage + dilatation, split-FP32.
-//   X = fp32(x_j - x_i), du = fp32(u_j - u_i) (differences in FP64, one rounding)
-//   e = (2 X.du + du.du) / (|Y| + |X|)          (= |Y| - |X| without cancellation)
-//   break when e/|X| > s_c (CriticalStretchDamageModel.cpp:155-158)
+//   break when e > s_c*|X|, i.e. (|Y|-|X|)/|X| > s_c (CriticalStretchDamageModel.cpp:155-158)
 //   theta_i = 3/m_i * sum omega*(1-d)*|X|*e*V_j  (material_utilities.cxx:284)
+// Writes the owner terms A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m into ur[i].
 // ---------------------------------------------------------------------------
 template <int TPO>
-__global__ void __launch_bounds__(kBlock) k_dilatation_split(
+__global__ void __launch_bounds__(kBlock, 4) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
-    const double4* __restrict__ xv, double4* __restrict__ st, const double4* __restrict__ pt,
-    const float2* __restrict__ coef, const double* __restrict__ sc, const double* __restrict__ hp,
-    int influence, int damage_on, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+    const Rec8* __restrict__ xr, Rec8* __restrict__ ur, const float4* __restrict__ own, int influence,
+    int damage_on, double* __restrict__ theta_out, double* __restrict__ node_damage) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -133,42 +187,38 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_split(
   float th = 0.0f;
   int broken = 0;
   int64_t b0 = 0, b1 = 0;
+  float4 ow = make_float4(0.f, 0.f, 0.f, -1.f);
   if (valid) {
     b0 = row[i];
     b1 = row[i + 1];
-    const double4 xi = xv[i];
-    const double4 ui = st[i];
-    const float s_c = damage_on ? (float)sc[i] : -1.0f;
-    const float h = (float)hp[i];
+    ow = own[i];
+    const Rec8 xi = ld_rec_nc(xr + i);
+    const Rec8 ui = ld_rec(ur + i);
+    const float s_c = damage_on ? ow.w : -1.0f;
+#pragma unroll 2
     for (int64_t b = b0 + lane; b < b1; b += TPO) {
       if (dmg[b]) {
         broken++;
-        continue;
+      } else {
+        const int32_t j = col[b];
+        const Rec8 xj = ld_rec_nc(xr + j);
+        const Rec8 uj = ld_rec(ur + j);
+        const SplitBond s = split_bond(xi, ui, xj, uj);
+        if (s_c >= 0.0f && s.e > s_c * s.zeta) {
+          dmg[b] = 1;
+          broken++;
+        } else {
+          th = fmaf(omega_f(influence, s.zeta, xi.v[7]) * s.zeta * s.e, xj.v[6], th);
+        }
       }
-      const int32_t j = col[b];
-      const double4 xj = xv[j];
-      const double4 uj = st[j];
-      const float Xx = (float)(xj.x - xi.x), Xy = (float)(xj.y - xi.y), Xz = (float)(xj.z - xi.z);
-      const float Ux = (float)(uj.x - ui.x), Uy = (float)(uj.y - ui.y), Uz = (float)(uj.z - ui.z);
-      const float zeta = sqrtf(Xx * Xx + Xy * Xy + Xz * Xz);
-      const float Yx = Xx + Ux, Yy = Xy + Uy, Yz = Xz + Uz;
-      const float dY = sqrtf(Yx * Yx + Yy * Yy + Yz * Yz);
-      const float e = (2.0f * (Xx * Ux + Xy * Uy + Xz * Uz) + (Ux * Ux + Uy * Uy + Uz * Uz)) / (dY + zeta);
-      if (s_c >= 0.0f && e / zeta > s_c) {
-        dmg[b] = 1;
-        broken++;
-        continue;
-      }
-      th += omega_f(influence, zeta, h) * zeta * e * (float)xj.w;
     }
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
   if (valid && lane == 0) {
-    const double theta = 3.0 * (double)th / pt[i].x;
-    const float2 cf = coef[i];
-    st[i].w = pack_ab((float)theta * cf.x, cf.y);
-    theta_out[i] = theta;
+    const float theta = th * ow.x;
+    *reinterpret_cast<float2*>(&ur[i].v[6]) = make_float2(theta * ow.y, ow.z);
+    theta_out[i] = (double)theta;
     node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
   }
 }
@@ -235,7 +285,6 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_fp64(
   }
 }
 
-
 // ---------------------------------------------------------------------------
 // Verlet epilogue shared by both precisions. Lane c (< 3) of the group handles
 // component c of point i; f is the internal force density of that component.
@@ -253,14 +302,14 @@ struct EpiArgs {
   int has_contact, has_bc, split;
   const double* fc;
   double* f_out;
-  double* u;  // FP64-path displacement [3n]
+  double* u;  // FP64 displacement [3n]
   double* v;
   double* a;
   const uint8_t* bc_mask;
   const double* bc_a;
   const double* bc_b;
-  const double4* st_cur;
-  double4* st_next;
+  double4* st_next;  // FP64 path: next coordinates
+  Rec8* ur_next;     // split path: next displacement record
   int* status;
 };
 
@@ -269,7 +318,7 @@ __device__ __forceinline__ double* comp_ptr(double4* q, int c) {
   return c == 0 ? &q->x : (c == 1 ? &q->y : &q->z);
 }
 
-__device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int c, double f, const double4& xi,
+__device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int c, double f, double xc,
                                                 double rho) {
   const int64_t k = 3 * i + c;
   double ftot = f;
@@ -301,62 +350,55 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
   E.v[k] = vh;
   E.a[k] = acc;
   const double step_dx = __dmul_rn(dt, vh);
+  const double u = E.u[k];
+  const double un = __dadd_rn(u, step_dx);  // u += dt*v
+  E.u[k] = un;
   if (E.split) {
-    const double u = comp3(E.st_cur[i], c);
-    *comp_ptr(&E.st_next[i], c) = __dadd_rn(u, step_dx);
+    float hi, lo;
+    split_hi_lo(un, &hi, &lo);
+    E.ur_next[i].v[c] = hi;
+    E.ur_next[i].v[c + 3] = lo;
   } else {
-    const double u = E.u[k];
-    const double x = comp3(xi, c);
-    *comp_ptr(&E.st_next[i], c) = __dadd_rn(__dadd_rn(x, u), step_dx);  // y = x+u+dt*v
-    E.u[k] = __dadd_rn(u, step_dx);                                      // u += dt*v
+    *comp_ptr(&E.st_next[i], c) = __dadd_rn(__dadd_rn(xc, u), step_dx);  // y = x+u+dt*v
   }
 }
 
 // ---------------------------------------------------------------------------
-// K3: force gather, split-FP32. Recomputes X, du, |X|, |Y|, e with the same
-// FP32 operations as pass 1 (identical values), then
+// K3: force gather, split-FP32:
 //   t_ij + t_ji = omega*(|X|*(A_i + A_j) + e*(B_i + B_j))   (bond intact)
 //   f_i += (t_ij + t_ji) * V_j * Y/|Y|
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
 template <int TPO>
-__global__ void __launch_bounds__(kBlock) k_force_split(int64_t n, const int64_t* __restrict__ row,
-                                                        const int32_t* __restrict__ col,
-                                                        const uint8_t* __restrict__ dmg,
-                                                        const double4* __restrict__ xv,
-                                                        const double4* __restrict__ st,
-                                                        const double4* __restrict__ pt,
-                                                        const double* __restrict__ hp, int influence,
-                                                        EpiArgs E) {
+__global__ void __launch_bounds__(kBlock, 4) k_force_split(int64_t n, const int64_t* __restrict__ row,
+                                                           const int32_t* __restrict__ col,
+                                                           const uint8_t* __restrict__ dmg,
+                                                           const Rec8* __restrict__ xr, const Rec8* __restrict__ ur,
+                                                           const double4* __restrict__ pt, int influence,
+                                                           EpiArgs E) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
   const bool valid = i < n;
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  double4 xi = make_double4(0, 0, 0, 0);
   if (valid) {
-    xi = xv[i];
-    const double4 ui = st[i];
-    const float2 abi = unpack_ab(ui.w);
-    const float h = (float)hp[i];
+    const Rec8 xi = ld_rec_nc(xr + i);
+    const Rec8 ui = ld_rec_nc(ur + i);
     const int64_t b1 = row[i + 1];
+#pragma unroll 2
     for (int64_t b = row[i] + lane; b < b1; b += TPO) {
-      if (dmg[b]) continue;
-      const int32_t j = col[b];
-      const double4 xj = xv[j];
-      const double4 uj = st[j];
-      const float Xx = (float)(xj.x - xi.x), Xy = (float)(xj.y - xi.y), Xz = (float)(xj.z - xi.z);
-      const float Ux = (float)(uj.x - ui.x), Uy = (float)(uj.y - ui.y), Uz = (float)(uj.z - ui.z);
-      const float zeta = sqrtf(Xx * Xx + Xy * Xy + Xz * Xz);
-      const float Yx = Xx + Ux, Yy = Xy + Uy, Yz = Xz + Uz;
-      const float dY = sqrtf(Yx * Yx + Yy * Yy + Yz * Yz);
-      const float e = (2.0f * (Xx * Ux + Xy * Uy + Xz * Uz) + (Ux * Ux + Uy * Uy + Uz * Uz)) / (dY + zeta);
-      const float2 abj = unpack_ab(uj.w);
-      const float T = omega_f(influence, zeta, h) * (zeta * (abi.x + abj.x) + e * (abi.y + abj.y));
-      const float s = T * (float)xj.w / dY;
-      fx += s * Yx;
-      fy += s * Yy;
-      fz += s * Yz;
+      if (!dmg[b]) {
+        const int32_t j = col[b];
+        const Rec8 xj = ld_rec_nc(xr + j);
+        const Rec8 uj = ld_rec_nc(ur + j);
+        const SplitBond s = split_bond(xi, ui, xj, uj);
+        const float T =
+            omega_f(influence, s.zeta, xi.v[7]) * fmaf(s.zeta, ui.v[6] + uj.v[6], s.e * (ui.v[7] + uj.v[7]));
+        const float w = T * xj.v[6] * s.ry;
+        fx = fmaf(w, s.Yx, fx);
+        fy = fmaf(w, s.Yy, fy);
+        fz = fmaf(w, s.Yz, fz);
+      }
     }
   }
   fx = group_sum<TPO>(fx);
@@ -364,7 +406,7 @@ __global__ void __launch_bounds__(kBlock) k_force_split(int64_t n, const int64_t
   fz = group_sum<TPO>(fz);
   if (valid && lane < 3) {
     const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
-    verlet_epilogue(E, i, lane, f, xi, pt[i].w);
+    verlet_epilogue(E, i, lane, f, 0.0, pt[i].w);
   }
 }
 
@@ -426,66 +468,48 @@ __global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t*
   fz = group_sum<TPO>(fz);
   if (valid && lane < 3) {
     const double f = lane == 0 ? fx : (lane == 1 ? fy : fz);
-    verlet_epilogue(E, i, lane, f, xi, pt[i].w);
+    verlet_epilogue(E, i, lane, f, comp3(xi, lane), pt[i].w);
   }
 }
 
 // ---------------------------------------------------------------------------
 // State conversions and the stable time step
 // ---------------------------------------------------------------------------
-// Gathered state from current coordinates y [3n]: split -> u = y - x, FP64 -> y.
+// State from current coordinates y [3n]: u = y - x (FP64), then the gathered
+// copy (split: hi/lo record, FP64: y itself).
 __global__ void k_state_from_y(int64_t n, const double* __restrict__ y, const double4* __restrict__ xv,
-                               double4* __restrict__ st, double* __restrict__ u, int split) {
+                               double* __restrict__ u, double4* __restrict__ st, Rec8* __restrict__ ur) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 x = xv[i];
   const double y0 = y[3 * i], y1 = y[3 * i + 1], y2 = y[3 * i + 2];
-  double4 s = st[i];
-  if (split) {
-    s.x = y0 - x.x;
-    s.y = y1 - x.y;
-    s.z = y2 - x.z;
+  const double u0 = y0 - x.x, u1 = y1 - x.y, u2 = y2 - x.z;
+  u[3 * i] = u0;
+  u[3 * i + 1] = u1;
+  u[3 * i + 2] = u2;
+  if (ur) {
+    split_hi_lo(u0, &ur[i].v[0], &ur[i].v[3]);
+    split_hi_lo(u1, &ur[i].v[1], &ur[i].v[4]);
+    split_hi_lo(u2, &ur[i].v[2], &ur[i].v[5]);
   } else {
-    s.x = y0;
-    s.y = y1;
-    s.z = y2;
-    if (u) {
-      u[3 * i] = y0 - x.x;
-      u[3 * i + 1] = y1 - x.y;
-      u[3 * i + 2] = y2 - x.z;
-    }
+    st[i] = make_double4(y0, y1, y2, 0.0);
   }
-  st[i] = s;
 }
 
-// Gathered state from the displacement u [3n] (after pd_set_state): split -> u,
-// FP64 -> y = x + u (Peridigm.cpp:1497 with v = 0 contribution already in u).
+// Gathered state from the displacement u [3n] (after pd_set_state): split ->
+// hi/lo record, FP64 -> y = x + u.
 __global__ void k_state_from_u(int64_t n, const double* __restrict__ u, const double4* __restrict__ xv,
-                               double4* __restrict__ st, int split) {
+                               double4* __restrict__ st, Rec8* __restrict__ ur) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 x = xv[i];
-  double4 s = st[i];
-  if (split) {
-    s.x = u[3 * i];
-    s.y = u[3 * i + 1];
-    s.z = u[3 * i + 2];
+  if (ur) {
+    split_hi_lo(u[3 * i], &ur[i].v[0], &ur[i].v[3]);
+    split_hi_lo(u[3 * i + 1], &ur[i].v[1], &ur[i].v[4]);
+    split_hi_lo(u[3 * i + 2], &ur[i].v[2], &ur[i].v[5]);
   } else {
-    s.x = __dadd_rn(x.x, u[3 * i]);
-    s.y = __dadd_rn(x.y, u[3 * i + 1]);
-    s.z = __dadd_rn(x.z, u[3 * i + 2]);
+    st[i] = make_double4(__dadd_rn(x.x, u[3 * i]), __dadd_rn(x.y, u[3 * i + 1]), __dadd_rn(x.z, u[3 * i + 2]), 0.0);
   }
-  st[i] = s;
-}
-
-// Displacement [3n] out of the state (split path keeps u only in st).
-__global__ void k_state_to_u(int64_t n, const double4* __restrict__ st, double* __restrict__ u) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double4 s = st[i];
-  u[3 * i] = s.x;
-  u[3 * i + 1] = s.y;
-  u[3 * i + 2] = s.z;
 }
 
 // ComputeCriticalTimeStep (Peridigm_CriticalTimeStep.cpp:52-130): per point
@@ -564,38 +588,34 @@ cudaError_t launch_weighted_volume(const pd_ctx* c) {
 }
 
 cudaError_t launch_pack_owner(pd_ctx* c) {
-  if (c->n == 0) return cudaSuccess;
-  k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->coef.p);
+  if (c->n == 0 || c->precision != PD_SPLIT_FP32) return cudaSuccess;
+  k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->xv.p, c->pt.p, c->sc.p, c->hp.p, c->xr.p, c->own.p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev) {
   if (c->n == 0) return cudaSuccess;
-  k_state_from_y<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, y_dev, c->xv.p, c->st[c->cur].p, c->u.p,
-                                                        c->precision == PD_SPLIT_FP32);
+  const bool split = c->precision == PD_SPLIT_FP32;
+  k_state_from_y<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, y_dev, c->xv.p, c->u.p, split ? nullptr : c->st[c->cur].p,
+                                                        split ? c->ur[c->cur].p : nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sync_state(pd_ctx* c) {
   if (c->n == 0) return cudaSuccess;
-  k_state_from_u<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->u.p, c->xv.p, c->st[c->cur].p,
-                                                        c->precision == PD_SPLIT_FP32);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_state_to_u(pd_ctx* c, double* u_out_dev) {
-  if (c->n == 0) return cudaSuccess;
-  k_state_to_u<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->st[c->cur].p, u_out_dev);
+  const bool split = c->precision == PD_SPLIT_FP32;
+  k_state_from_u<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->u.p, c->xv.p, split ? nullptr : c->st[c->cur].p,
+                                                        split ? c->ur[c->cur].p : nullptr);
   return cudaGetLastError();
 }
 
 // One model evaluation (damage -> dilatation -> force [-> Verlet epilogue]) on
-// the gathered state st[cur], with bond damage dmg updated in place.
+// the gathered state of parity c->cur, with bond damage dmg updated in place.
 cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   if (c->n == 0) return cudaSuccess;
-  const unsigned grid = grid_for(c->n, c->tpo);
   const bool split = c->precision == PD_SPLIT_FP32;
-  double4* st = c->st[c->cur].p;
+  const int tpo = split ? c->tpo_split : c->tpo;
+  const unsigned grid = grid_for(c->n, tpo);
   cudaEvent_t* ev = nullptr;
   if (c->ktime) {
     if (c->kev_used + 3 > c->kev.size()) {
@@ -611,11 +631,11 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
     cudaEventRecord(ev[0], c->stream);
   }
   if (split) {
-    PD_DISPATCH_TPO(c->tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->pt.p,
-                    c->coef.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->theta.p, c->node_damage.p);
+    PD_DISPATCH_TPO(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->xr.p, c->ur[c->cur].p,
+                    c->own.p, c->influence, sp.damage_on, c->theta.p, c->node_damage.p);
   } else {
-    PD_DISPATCH_TPO(c->tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->pt.p, c->sc.p,
-                    c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
+    PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
+                    c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -636,15 +656,15 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   E.bc_mask = c->bc_mask.p;
   E.bc_a = c->bc_a.p;
   E.bc_b = c->bc_b.p;
-  E.st_cur = st;
-  E.st_next = c->st[c->cur ^ 1].p;
+  E.st_next = split ? nullptr : c->st[c->cur ^ 1].p;
+  E.ur_next = split ? c->ur[c->cur ^ 1].p : nullptr;
   E.status = c->status.p;
   if (split) {
-    PD_DISPATCH_TPO(c->tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->pt.p, c->hp.p,
+    PD_DISPATCH_TPO(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->xr.p, c->ur[c->cur].p, c->pt.p,
                     c->influence, E);
   } else {
-    PD_DISPATCH_TPO(c->tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, st, c->ab64.p, c->pt.p,
-                    c->hp.p, c->influence, E);
+    PD_DISPATCH_TPO(tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
+                    c->pt.p, c->hp.p, c->influence, E);
   }
   if (ev) cudaEventRecord(ev[2], c->stream);
   return cudaGetLastError();

@@ -2,16 +2,18 @@
 // layout of a context and the kernels' launch helpers.
 //
 // HBM layout (n points, nb directed bonds, all in the caller's point order):
-//   xv[n]        double4 (x, y, z, V)             constant, 32 B, one sector per gather
-//   st[2][n]     double4 gathered state, double buffered across steps:
-//                  split-FP32 : (u_x, u_y, u_z, packed float2 {A, B})
-//                  FP64       : (y_x, y_y, y_z, 0)   y = current coordinates
-//   ab64[n]      double4 (theta, 3K/m - alpha/3, alpha, 0)  FP64 path only
+//   xv[n]        double4 (x, y, z, V) FP64 model coordinates and volume
 //   row[n+1]     int64 bond row pointers          col[nb] int32 neighbor ids
 //   dmg[nb]      uint8 bond damage (0/1), monotone, updated in place
-//   pt[n]        double4 (m, K, mu, rho) per-point material, sc[n] critical stretch
-//   coef[n]      float2 split-path owner coefficients ((3K-5mu)/m, 15mu/m)
+//   pt[n]        double4 (m, K, mu, rho) per-point material, sc[n] critical stretch, hp[n] horizon
 //   u[3n], v[3n], a[3n], f[3n], fc[3n] FP64 integration state (interleaved xyz)
+// Split-FP32 path, gathered per neighbor with one 256-bit load each:
+//   xr[n]        Rec8 (x_hi[3], x_lo[3], V, h)          constant
+//   ur[2][n]     Rec8 (u_hi[3], u_lo[3], A, B)          double buffered across steps
+//   own[n]       float4 (3/m, (3K-5mu)/m, 15mu/m, s_c)  owner terms
+// FP64 path:
+//   st[2][n]     double4 (y_x, y_y, y_z, 0) current coordinates, double buffered
+//   ab64[n]      double4 (theta, 3K/m - alpha/3, alpha, 0)
 // A = theta*(3K-5mu)/m and B = 15mu/m are the owner terms of the LPS force
 // state t = (1-d)[A*omega*|xi| + (1-d)*B*omega*e] (elastic.cxx:99,119-120).
 #pragma once
@@ -25,6 +27,11 @@
 #include "../../include/pd_b200.h"
 
 namespace pdb {
+
+// One 32-byte record per point, fetched with a single 256-bit load.
+struct __align__(32) Rec8 {
+  float v[8];
+};
 
 // ---------------------------------------------------------------------------
 // Kernel parameter blocks
@@ -97,7 +104,8 @@ struct pd_ctx {
   int device = 0;
   int precision = PD_SPLIT_FP32;
   int influence = PD_INFLUENCE_ONE;
-  int tpo = 16;  // lanes per point
+  int tpo = 16;       // lanes per point (FP64 path and setup kernels)
+  int tpo_split = 4;  // lanes per point of the split-FP32 bond passes
   cudaStream_t stream = nullptr;
   std::string err;
 
@@ -126,11 +134,13 @@ struct pd_ctx {
   bool wv_done = false;
   pdb::DBuf<double4> pt;     // (m, K, mu, rho)
   pdb::DBuf<double> sc;      // critical stretch (<0: off)
-  pdb::DBuf<float2> coef;    // split-path owner coefficients
+  pdb::DBuf<pdb::Rec8> xr;   // split path: (x_hi, x_lo, V, h)
+  pdb::DBuf<float4> own;     // split path: (3/m, (3K-5mu)/m, 15mu/m, s_c)
   bool any_damage = false;
 
   // state
-  pdb::DBuf<double4> st[2];
+  pdb::DBuf<double4> st[2];   // FP64 path gathered coordinates
+  pdb::DBuf<pdb::Rec8> ur[2]; // split path gathered displacement records
   int cur = 0;
   pdb::DBuf<double4> ab64;
   pdb::DBuf<double> u, v, a, f, fc, theta, node_damage;
@@ -167,7 +177,6 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg);
 cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev);
 cudaError_t launch_sync_state(pd_ctx* c);
 cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out);
-cudaError_t launch_state_to_u(pd_ctx* c, double* u_out_dev);
 cudaError_t collect_kernel_times(pd_ctx* c);
 
 // bonds
