@@ -163,6 +163,22 @@ int pd_update_state(pd_ctx* ctx);
 /* Bond damage in neighbor-list order (doubles 0/1), in and out. */
 int pd_set_bond_damage(pd_ctx* ctx, const double* bond_damage);
 
+/* ---- contact -------------------------------------------------------------- */
+/* "Short Range Force" contact: ShortRangeForceContactModel
+ * (src/contact/Peridigm_ShortRangeForceContactModel.cpp:50-87) with the
+ * ContactManager's "Search Radius" / "Search Frequency"
+ * (src/core/Peridigm_ContactManager.cpp:79-84). The horizon of the spring
+ * coefficient is each point's block horizon (Peridigm_ContactManager.cpp:241-249).
+ * contact_radius <= 0 disables contact. Once set, pd_verlet_run searches at
+ * setup and every search_frequency steps and adds the contact force. */
+int pd_contact_short_range(pd_ctx* ctx, double search_radius, int32_t search_frequency, double contact_radius,
+                           double spring_constant, double friction_coefficient);
+/* ContactManager::contactSearch + ShortRangeForceContactModel::computeForce
+ * (Peridigm_ContactManager.cpp:696-748, Peridigm_ShortRangeForceContactModel.cpp:98-261)
+ * on host coordinates y[3n] and velocities v[3n]; fc_out[3n] receives the
+ * contact force density. */
+int pd_contact_force(pd_ctx* ctx, const double* y, const double* v, double* fc_out);
+
 /* ---- explicit integration ----------------------------------------------- */
 /* ComputeCriticalTimeStep (src/core/Peridigm_CriticalTimeStep.cpp:52-130), min over points. */
 int pd_critical_time_step(pd_ctx* ctx, double* dt_out);

@@ -89,6 +89,8 @@ SIGNATURES = {
     "pd_clear_boundary_conditions": (C.c_int, [_vp]),
     "pd_verlet_run": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int64, C.POINTER(Stats)]),
     "pd_get_field": (C.c_int, [_vp, C.c_int32, _dp]),
+    "pd_contact_short_range": (C.c_int, [_vp, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double]),
+    "pd_contact_force": (C.c_int, [_vp, _dp, _dp, _dp]),
     "pd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "pd_get_kernel_timing": (C.c_int, [_vp, _dp, _i64p]),
 }

@@ -171,6 +171,17 @@ class Context:
         bd = _f64(bd, self.num_bonds(), "bond damage")
         self._ok(self.L.pd_set_bond_damage(self.h, _d(bd)))
 
+    # -- contact ---------------------------------------------------------------
+    def contact(self, search_radius, search_frequency, contact_radius, spring_constant, friction=0.0):
+        self._ok(self.L.pd_contact_short_range(self.h, float(search_radius), int(search_frequency),
+                                               float(contact_radius), float(spring_constant), float(friction)))
+
+    def contact_force(self, y, v):
+        y, v = _f64(y, 3 * self.n, "y"), _f64(v, 3 * self.n, "v")
+        fc = np.zeros(3 * self.n)
+        self._ok(self.L.pd_contact_force(self.h, _d(y), _d(v), _d(fc)))
+        return fc
+
     # -- integration ----------------------------------------------------------
     def critical_time_step(self):
         dt = C.c_double()

@@ -563,6 +563,32 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
   return rc;
 }
 
+int pd_contact_short_range(pd_ctx* c, double r_search, int32_t freq, double r_contact, double k_spring,
+                           double friction) {
+  CHECK_CTX(c);
+  if (c->n == 0 || !c->row.p) return fail(c, PD_ERR_STATE, "contact: points and bonds must be set first");
+  TRY(ensure_device(c));
+  return contact_configure(c, r_search, freq, r_contact, k_spring, friction);
+}
+
+int pd_contact_force(pd_ctx* c, const double* y, const double* v, double* fc_out) {
+  CHECK_CTX(c);
+  if (!y || !v || !fc_out) return fail(c, PD_ERR_ARG, "pd_contact_force: null argument");
+  if (!c->contact) return fail(c, PD_ERR_STATE, "pd_contact_force: contact not configured");
+  TRY(ensure_ready(c));
+  const size_t bytes = 3 * (size_t)c->n * sizeof(double);
+  DBuf<double> yd, vd, fd;
+  PD_CUDA_TRY(c, yd.alloc(3 * c->n));
+  PD_CUDA_TRY(c, vd.alloc(3 * c->n));
+  PD_CUDA_TRY(c, fd.alloc(3 * c->n));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(yd.p, y, bytes, cudaMemcpyHostToDevice, c->stream));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(vd.p, v, bytes, cudaMemcpyHostToDevice, c->stream));
+  TRY(contact_force_from(c, yd.p, vd.p, fd.p));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(fc_out, fd.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  TRY(check_status(c));
+  return PD_OK;
+}
+
 int pd_set_kernel_timing(pd_ctx* c, int enable) {
   CHECK_CTX(c);
   TRY(ensure_device(c));

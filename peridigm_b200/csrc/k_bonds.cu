@@ -20,15 +20,10 @@
 #include <cfloat>
 #include <cmath>
 
+#include "cells.cuh"
 #include "pd_internal.cuh"
 
 namespace pdb {
-
-struct Grid {
-  double lo[3];
-  double cell;
-  int dims[3];
-};
 
 struct PlaneDev {
   double n[3], r0[3], ub[3], ua[3];
@@ -39,14 +34,6 @@ struct Planes {
   PlaneDev p[kMaxPlanes];
   int count;
 };
-
-__device__ __forceinline__ int cell_coord(const Grid& g, double v, int k) {
-  double q = floor((v - g.lo[k]) / g.cell);
-  int c = (int)q;
-  if (q < 0) c = 0;
-  if (q >= g.dims[k]) c = g.dims[k] - 1;
-  return c;
-}
 
 __global__ void k_cell_ids(int64_t n, const double4* __restrict__ xv, Grid g, int32_t* __restrict__ cid,
                            int32_t* __restrict__ idx) {
@@ -308,6 +295,49 @@ int finalize_bonds(pd_ctx* c, bool sort_rows) {
   return PD_OK;
 }
 
+Grid make_grid(int64_t n, const double lo[3], const double hi[3], double reach) {
+  Grid g;
+  double cell = reach * 1.0001;
+  if (!(cell > 0.0)) cell = 1.0;
+  for (;;) {
+    double tot = 1.0;
+    for (int k = 0; k < 3; ++k) {
+      g.dims[k] = (int)std::floor((hi[k] - lo[k]) / cell) + 1;
+      tot *= g.dims[k];
+    }
+    if (tot <= 4.0 * (double)n + 64.0 && tot < 2.0e9) break;
+    cell *= 1.5;
+  }
+  for (int k = 0; k < 3; ++k) g.lo[k] = lo[k];
+  g.cell = cell;
+  return g;
+}
+
+int bin_points(pd_ctx* c, const double4* pos, int64_t n, const Grid& g, DBuf<int32_t>& idx_s,
+               DBuf<int64_t>& cell_start) {
+  const int64_t ncell = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+  DBuf<int32_t> cid, idx, cid_s;
+  PD_CUDA_TRY(c, cid.alloc(n));
+  PD_CUDA_TRY(c, idx.alloc(n));
+  PD_CUDA_TRY(c, cid_s.alloc(n));
+  PD_CUDA_TRY(c, idx_s.alloc(n));
+  PD_CUDA_TRY(c, cell_start.alloc(ncell + 1));
+  const unsigned g1 = (unsigned)((n + 255) / 256);
+  k_cell_ids<<<g1, 256, 0, c->stream>>>(n, pos, g, cid.p, idx.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  int end_bit = 1;
+  while (end_bit < 31 && (int64_t(1) << end_bit) <= ncell) ++end_bit;
+  size_t tmp_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, cid.p, cid_s.p, idx.p, idx_s.p, (int)n, 0, end_bit, c->stream);
+  DBuf<unsigned char> tmp;
+  PD_CUDA_TRY(c, tmp.alloc(tmp_bytes));
+  PD_CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, cid.p, cid_s.p, idx.p, idx_s.p, (int)n, 0, end_bit,
+                                                 c->stream));
+  k_cell_bounds<<<(unsigned)((n + 1 + 255) / 256), 256, 0, c->stream>>>(n, ncell, cid_s.p, cell_start.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
 int build_bonds_device(pd_ctx* c, const pd_plane_filter* filters, int nf) {
   const int64_t n = c->n;
   if (nf < 0 || nf > kMaxPlanes) {
@@ -343,42 +373,14 @@ int build_bonds_device(pd_ctx* c, const pd_plane_filter* filters, int nf) {
     c->err = "horizon must be positive";
     return PD_ERR_ARG;
   }
-  Grid g;
-  double cell = hmax * 1.0001;
-  for (;;) {
-    double tot = 1.0;
-    for (int k = 0; k < 3; ++k) {
-      g.dims[k] = (int)std::floor((hi[k] - lo[k]) / cell) + 1;
-      tot *= g.dims[k];
-    }
-    if (tot <= 4.0 * (double)n + 64.0 && tot < 2.0e9) break;
-    cell *= 1.5;
-  }
-  for (int k = 0; k < 3; ++k) g.lo[k] = lo[k];
-  g.cell = cell;
-  const int64_t ncell = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
-
-  DBuf<int32_t> cid, idx, cid_s, idx_s;
+  const Grid g = make_grid(n, lo, hi, hmax);
+  DBuf<int32_t> idx_s;
   DBuf<int64_t> cell_start, counts;
-  PD_CUDA_TRY(c, cid.alloc(n));
-  PD_CUDA_TRY(c, idx.alloc(n));
-  PD_CUDA_TRY(c, cid_s.alloc(n));
-  PD_CUDA_TRY(c, idx_s.alloc(n));
-  PD_CUDA_TRY(c, cell_start.alloc(ncell + 1));
+  {
+    int rc = bin_points(c, c->xv.p, n, g, idx_s, cell_start);
+    if (rc != PD_OK) return rc;
+  }
   PD_CUDA_TRY(c, counts.alloc(n + 1));
-  const unsigned g1 = (unsigned)((n + 255) / 256);
-  k_cell_ids<<<g1, 256, 0, c->stream>>>(n, c->xv.p, g, cid.p, idx.p);
-  PD_CUDA_TRY(c, cudaGetLastError());
-  int end_bit = 1;
-  while (end_bit < 31 && (int64_t(1) << end_bit) <= ncell) ++end_bit;
-  size_t tmp_bytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, cid.p, cid_s.p, idx.p, idx_s.p, (int)n, 0, end_bit, c->stream);
-  DBuf<unsigned char> tmp;
-  PD_CUDA_TRY(c, tmp.alloc(tmp_bytes));
-  PD_CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, cid.p, cid_s.p, idx.p, idx_s.p, (int)n, 0, end_bit,
-                                                 c->stream));
-  k_cell_bounds<<<(unsigned)((n + 1 + 255) / 256), 256, 0, c->stream>>>(n, ncell, cid_s.p, cell_start.p);
-  PD_CUDA_TRY(c, cudaGetLastError());
   const unsigned gw = (unsigned)((n * 32 + 255) / 256);
   k_neighbors<false><<<gw, 256, 0, c->stream>>>(n, c->xv.p, c->hp.p, g, cell_start.p, idx_s.p, pl, counts.p, nullptr,
                                                 nullptr);

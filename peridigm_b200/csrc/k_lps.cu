@@ -699,3 +699,21 @@ cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out_dev) {
 }
 
 }  // namespace pdb
+
+namespace pdb {
+
+__global__ void k_u_from_record(int64_t n, const Rec8* __restrict__ ur, double* __restrict__ u) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Rec8 r = ur[i];
+  for (int c = 0; c < 3; ++c) u[3 * i + c] = (double)r.v[c] + (double)r.v[c + 3];
+}
+
+// Displacement held by the split-path record of the given parity.
+cudaError_t launch_u_from_record(pd_ctx* c, int parity, double* u_out) {
+  if (c->n == 0) return cudaSuccess;
+  k_u_from_record<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->ur[parity].p, u_out);
+  return cudaGetLastError();
+}
+
+}  // namespace pdb

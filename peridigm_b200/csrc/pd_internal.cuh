@@ -188,6 +188,9 @@ void contact_release(pd_ctx* c);
 int contact_prepare(pd_ctx* c, int64_t step);  // search when due at this step
 int contact_eval(pd_ctx* c);                   // contact force density into c->fc
 int64_t contact_pairs(const pd_ctx* c);
+int contact_configure(pd_ctx* c, double r_search, int freq, double r_contact, double k_spring, double friction);
+int contact_force_from(pd_ctx* c, const double* y_dev, const double* v_dev, double* fc_dev);
+cudaError_t launch_u_from_record(pd_ctx* c, int parity, double* u_out);  // split path: hi + lo
 void qs_release(pd_ctx* c);
 
 // status bits

@@ -112,3 +112,63 @@ def oracle_problem(w, row, col, dt, nsteps):
 def bonds_per_point_estimate(horizon_over_h):
     r = horizon_over_h
     return 4.0 / 3.0 * math.pi * r ** 3
+
+
+def plate_sphere(nx=400, ny=400, nz=40, h=0.25e-3, radius_cells=25, s_c=3.0e-4, speed=20.0, gap_cells=0.5,
+                 search_extra=0.6, freq=100, nsteps=2000):
+    """Brittle plate (block 0, critical stretch s_c) and a dropped sphere (block 1,
+    elastic only) on the same lattice spacing, short-range contact.
+
+    Sphere: lattice points within radius_cells*h of its centre, centred above the
+    plate middle with its lowest point gap_cells*h above the plate's top layer;
+    initial velocity -speed in z. Contact radius 0.9h, spring constant = plate
+    bulk modulus, search radius 0.9h + search_extra*h (a pair outside it at a
+    search cannot close the extra gap within freq steps at these speeds),
+    search frequency freq."""
+    xp, vp = lattice(nx, ny, nz, h)
+    r = radius_cells
+    k = np.arange(-r, r + 1)
+    Z, Y, X = np.meshgrid(k, k, k, indexing="ij")
+    keep = X ** 2 + Y ** 2 + Z ** 2 <= r * r
+    c = np.array([nx * h / 2.0, ny * h / 2.0, nz * h - 0.5 * h + (r + gap_cells + 1.0) * h])
+    xs = (np.stack([X[keep], Y[keep], Z[keep]], 1) * h + c).ravel()
+    x = np.concatenate([xp, xs])
+    vol = np.full(x.size // 3, h ** 3)
+    block = np.concatenate([np.zeros(xp.size // 3, np.int32), np.ones(xs.size // 3, np.int32)])
+    v0 = np.zeros_like(x)
+    v0[xp.size + 2::3] = -speed
+    return dict(name=f"plate_sphere_{nx}x{ny}x{nz}_r{r}", x=x, vol=vol, block=block, horizon=3.015 * h,
+                K=130.0e9, mu=78.0e9, rho=7800.0, s_c=s_c, s_c_blocks=[s_c, -1.0], planes=[], v0=v0, bcs=[],
+                safety=0.7, nsteps=nsteps, h=h,
+                contact=dict(r_search=0.9 * h + search_extra * h, freq=freq, r_contact=0.9 * h, k_spring=130.0e9,
+                             friction=0.0))
+
+
+def setup_context_blocks(ctx, w):
+    """Multi-block variant of setup_context (one material, per-block damage, contact)."""
+    ctx.set_points(w["x"], w["vol"], w.get("block"))
+    nblk = int(np.max(w["block"])) + 1 if w.get("block") is not None else 1
+    ctx.set_horizons([w["horizon"]] * nblk)
+    ctx.build_bonds(w["planes"])
+    for b in range(nblk):
+        ctx.material(w["K"], w["mu"], w["rho"], block=b)
+        ctx.critical_stretch(w["s_c_blocks"][b], block=b)
+    ct = w.get("contact")
+    if ct:
+        ctx.contact(ct["r_search"], ct["freq"], ct["r_contact"], ct["k_spring"], ct.get("friction", 0.0))
+    for bc in w["bcs"]:
+        ctx.prescribed_displacement(bc["points"], bc["coordinate"], bc["a"], bc["b"])
+    ctx.set_state(np.zeros_like(w["x"]), w["v0"])
+    return ctx
+
+
+def oracle_problem_blocks(w, row, col, dt, nsteps):
+    p = oracle_problem(w, row, col, dt, nsteps)
+    blk = w["block"]
+    p["s_c"] = np.where(np.asarray(w["s_c_blocks"])[blk] >= 0, np.asarray(w["s_c_blocks"])[blk], 1e300)
+    ct = w.get("contact")
+    if ct:
+        p["contact"] = dict(r_search=ct["r_search"], freq=ct["freq"], r_contact=ct["r_contact"],
+                            k_spring=ct["k_spring"], friction=ct.get("friction", 0.0),
+                            horizon=np.full(len(w["vol"]), w["horizon"]))
+    return p
