@@ -198,6 +198,40 @@ int pd_verlet_run(pd_ctx* ctx, double dt, double t0, int64_t nsteps, pd_stats* s
 /* Reads a field (PD_FIELD_*) into host memory in the caller's order. */
 int pd_get_field(pd_ctx* ctx, int32_t field, double* out);
 
+/* ---- quasi-static ---------------------------------------------------------- */
+#define PD_PRECOND_NONE 0         /* plain CG (the reference's default, usePreconditioner=false, Peridigm.cpp:2740) */
+#define PD_PRECOND_BLOCK_JACOBI 1 /* inverse 3x3 diagonal blocks ("Block 3x3", Peridigm.cpp:1603-1646) */
+#define PD_PRECOND_MPNN 2         /* learned message-passing preconditioner + block Jacobi (no reference counterpart) */
+
+typedef struct {
+  double newton_tolerance;      /* absolute, on ||r||_2 + 20 ||r||_inf ("Absolute Tolerance", Peridigm.cpp:4316) */
+  double cg_relative_tolerance; /* ||r_cg|| / ||r_cg,0|| of each linear solve (Belos "Relative Tolerance", :2556) */
+  int32_t max_newton_iterations;/* "Maximum Solver Iterations" */
+  int32_t max_cg_iterations;
+  int32_t preconditioner;       /* PD_PRECOND_* */
+  int32_t use_predictor;        /* start the free dofs from the previous step's increment (Peridigm.cpp:2764-2769) */
+} pd_qs_options;
+
+/* One quasi-static load step t_prev -> t_cur of Peridigm::executeQuasiStatic
+ * (src/core/Peridigm.cpp:2651-3043): prescribed-displacement increments on
+ * their dofs, then Newton on r = V (f_int + f_ext) (computeQuasiStaticResidual,
+ * :4176-4317) with CG on the matrix-free tangent -dr/du. Updates the
+ * displacement (u += du) and velocity (v = du / (t_cur - t_prev)). Bond damage
+ * is held fixed. stats (may be NULL) accumulates steps, Newton and CG
+ * iterations and device time. */
+int pd_qs_load_step(pd_ctx* ctx, double t_prev, double t_cur, const pd_qs_options* options, pd_stats* stats);
+
+/* Material::computeJacobian (src/materials/Peridigm_Material.hpp:174-180,
+ * FULL_MATRIX) in matrix-free form: kw = K w with K = -d(V f)/du at
+ * displacement u (V-weighted, Scale(-1): Peridigm_ElasticMaterial.cpp:366-370,
+ * Peridigm.cpp:2800); rows and columns of prescribed dofs are identity
+ * (applyKinematicBC_InsertZerosAndSetDiagonal, Peridigm.cpp:2799). Host arrays [3n]. */
+int pd_jacobian_apply(pd_ctx* ctx, const double* u, const double* w, double* kw);
+/* BLOCK_DIAGONAL Jacobian (SerialMatrix::addBlockDiagonalValues,
+ * src/core/Peridigm_SerialMatrix.cpp:110-170): the 3x3 diagonal blocks of K
+ * at displacement u, row-major, 9 per point. */
+int pd_jacobian_block_diagonal(pd_ctx* ctx, const double* u, double* blocks);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Named stopwatches around the hot calls are the reference's Timer
  * (src/core/Peridigm_Timer.hpp:77-86); here CUDA events bracket every launch

@@ -111,6 +111,8 @@ def lib():
         L.pdo_contact_fill.argtypes = [C.c_int64, _dp, C.c_double, _i64p, _i32p, _i64p, _i32p]
         L.pdo_contact_force.argtypes = [C.c_int64, _dp, _dp, _dp, _i64p, _i32p, C.c_double, C.c_double,
                                         C.c_double, _dp, _dp]
+        L.pdo_lps_jv.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp, _dp, C.c_int, C.c_double,
+                                 _dp, _dp]
         L.pdo_explicit_run.argtypes = [C.POINTER(Explicit), _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
@@ -270,6 +272,72 @@ def eval_model(x, y, vol, row, col, K, mu, horizon, s_c=None, dmg_n=None, influe
     th = dilatation(x, y, m, vol, dmg, row, col, horizon, influence)
     f = force_lps(x, y, m, vol, th, dmg, row, col, K, mu, horizon, influence)
     return {"m": m, "theta": th, "force": f, "bond_damage": dmg, "damage": nd}
+
+
+def lps_jv(x, y, vol, row, col, K, mu, horizon, w, bond_damage=None, influence=0):
+    """(d f / d u) w at configuration y (force density linearization)."""
+    x, y, vol, w = map(_f64, (x, y, vol, w))
+    n = vol.size
+    dmg = np.zeros(len(col)) if bond_damage is None else _f64(bond_damage)
+    m = weighted_volume(x, vol, row, col, horizon, influence)
+    th = dilatation(x, y, m, vol, dmg, row, col, horizon, influence)
+    df = np.zeros(3 * n)
+    lib().pdo_lps_jv(n, _d(x), _d(y), _d(m), _d(vol), _d(th), _d(dmg), _i64(row), _i32(col),
+                     _d(_per_point(K, n)), _d(_per_point(mu, n)), influence, horizon, _d(w), _d(df))
+    return df
+
+
+def tangent_dense(x, y, vol, row, col, K, mu, horizon, bc_dofs=(), bond_damage=None):
+    """Dense quasi-static tangent -d(V f)/du (Peridigm.cpp:2793-2800: V-weighted
+    Jacobian, Scale(-1)), BC rows/columns replaced by identity (small n only)."""
+    n = len(vol)
+    T = np.zeros((3 * n, 3 * n))
+    for k in range(3 * n):
+        e = np.zeros(3 * n)
+        e[k] = 1.0
+        T[:, k] = -np.repeat(np.asarray(vol, float), 3) * lps_jv(x, y, vol, row, col, K, mu, horizon, e, bond_damage)
+    for k in bc_dofs:
+        T[k, :] = 0.0
+        T[:, k] = 0.0
+        T[k, k] = 1.0
+    return T
+
+
+def qs_residual(x, u, vol, row, col, K, mu, horizon, bc_dofs=(), bond_damage=None):
+    """Peridigm::computeQuasiStaticResidual (Peridigm.cpp:4176-4317): r = V (f_int + f_ext),
+    BC rows zeroed; returns (r, ||r||_2 + 20 ||r||_inf)."""
+    y = _f64(x) + _f64(u)
+    f = eval_model(x, y, vol, row, col, K, mu, horizon, dmg_n=bond_damage)["force"]
+    r = np.repeat(np.asarray(vol, float), 3) * f
+    r[list(bc_dofs)] = 0.0
+    return r, float(np.linalg.norm(r) + 20.0 * np.abs(r).max())
+
+
+def qs_solve(x, vol, row, col, K, mu, horizon, bc, times, tol, max_iter=50, u0=None):
+    """Quasi-static load steps restated from Peridigm::executeQuasiStatic
+    (Peridigm.cpp:2651-3043) with a dense linear solve in place of Belos CG and
+    full Newton steps: per step, prescribed increments on the BC dofs, then
+    Newton on the free dofs until ||r||_2 + 20||r||_inf <= tol.
+    bc: list of (dof, a, b) with u_dof(t) = a t + b. Returns u per time."""
+    n = len(vol)
+    u = np.zeros(3 * n) if u0 is None else _f64(u0).copy()
+    dofs = [d for d, a, b in bc]
+    out = [u.copy()]
+    for s in range(1, len(times)):
+        tp, tc = times[s - 1], times[s]
+        for d, a, b in bc:
+            u[d] += (a * tc + b) - (a * tp + b)
+        r, nrm = qs_residual(x, u, vol, row, col, K, mu, horizon, dofs)
+        it = 0
+        while nrm > tol and it < max_iter:
+            T = tangent_dense(x, _f64(x) + u, vol, row, col, K, mu, horizon, dofs)
+            du = np.linalg.solve(T, r)
+            du[dofs] = 0.0
+            u += du
+            r, nrm = qs_residual(x, u, vol, row, col, K, mu, horizon, dofs)
+            it += 1
+        out.append(u.copy())
+    return out
 
 
 def critical_time_step(x, vol, row, col, K, rho, horizon):

@@ -580,3 +580,67 @@ int pdo_explicit_run(const pdo_explicit* p, double* u, double* v, double* a, dou
   free(cl.ccol);
   return 0;
 }
+
+/* ---------------------------------------------------------------------------
+ * Linearized LPS force (directional derivative of pdo_force_lps along w).
+ * With de = Yhat.(w_j - w_p) and dYhat = ((w_j - w_p) - Yhat de)/|Y|:
+ *   dtheta_p = sum 3 omega (1-d) zeta de V_j / m_p
+ *   dt = (1-d) (omega dtheta_p (3K/m - alpha/3) zeta + (1-d) omega alpha de)
+ *   f_p += (dt Yhat + t dYhat) V_j,  f_j -= (dt Yhat + t dYhat) V_p
+ * (the scatter of elastic.cxx:119-130 differentiated term by term).
+ * ------------------------------------------------------------------------- */
+void pdo_lps_jv(int64_t n, const double* x, const double* y, const double* m, const double* vol,
+                const double* theta, const double* dmg, const int64_t* row, const int32_t* col,
+                const double* K, const double* mu, int influence, double horizon, const double* w,
+                double* df) {
+  double* dth = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  for (int64_t p = 0; p < n; ++p) {
+    double acc = 0.0;
+    for (int64_t b = row[p]; b < row[p + 1]; ++b) {
+      int64_t j = col[b];
+      double X[3], Y[3], dw[3];
+      for (int k = 0; k < 3; ++k) {
+        X[k] = x[3 * j + k] - x[3 * p + k];
+        Y[k] = y[3 * j + k] - y[3 * p + k];
+        dw[k] = w[3 * j + k] - w[3 * p + k];
+      }
+      double zeta = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+      double dY = sqrt(Y[0] * Y[0] + Y[1] * Y[1] + Y[2] * Y[2]);
+      double de = (Y[0] * dw[0] + Y[1] * dw[1] + Y[2] * dw[2]) / dY;
+      double omega = pdo_influence(influence, zeta, horizon);
+      acc += 3.0 * omega * (1.0 - dmg[b]) * zeta * de * vol[j] / m[p];
+    }
+    dth[p] = acc;
+  }
+  memset(df, 0, sizeof(double) * 3 * (size_t)n);
+  for (int64_t p = 0; p < n; ++p) {
+    double alpha = 15.0 * mu[p] / m[p];
+    double q = 3.0 * K[p] / m[p] - alpha / 3.0;
+    for (int64_t b = row[p]; b < row[p + 1]; ++b) {
+      int64_t j = col[b];
+      double X[3], Y[3], dw[3];
+      for (int k = 0; k < 3; ++k) {
+        X[k] = x[3 * j + k] - x[3 * p + k];
+        Y[k] = y[3 * j + k] - y[3 * p + k];
+        dw[k] = w[3 * j + k] - w[3 * p + k];
+      }
+      double zeta = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+      double dY = sqrt(Y[0] * Y[0] + Y[1] * Y[1] + Y[2] * Y[2]);
+      double e = dY - zeta;
+      double de = (Y[0] * dw[0] + Y[1] * dw[1] + Y[2] * dw[2]) / dY;
+      double omega = pdo_influence(influence, zeta, horizon);
+      double d1 = 1.0 - dmg[b];
+      double c1 = omega * theta[p] * q;
+      double t = d1 * (c1 * zeta + d1 * omega * alpha * e);
+      double dt = d1 * (omega * dth[p] * q * zeta + d1 * omega * alpha * de);
+      for (int k = 0; k < 3; ++k) {
+        double yh = Y[k] / dY;
+        double dyh = (dw[k] - yh * de) / dY;
+        double g = dt * yh + t * dyh;
+        df[3 * p + k] += g * vol[j];
+        df[3 * j + k] -= g * vol[p];
+      }
+    }
+  }
+  free(dth);
+}

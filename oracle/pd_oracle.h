@@ -72,6 +72,15 @@ void pdo_contact_force(int64_t n, const double* y, const double* v, const double
                        const int64_t* crow, const int32_t* ccol, double r_contact,
                        double k_spring, double friction, const double* horizon_pt, double* fc);
 
+/* Directional derivative of the LPS force density (the linearization the
+ * reference's tangent assembles by automatic differentiation,
+ * Peridigm_ElasticMaterial.cpp:258-383): df = (d f / d u) w, scatter form
+ * mirroring elastic.cxx. theta, m at the configuration y. */
+void pdo_lps_jv(int64_t n, const double* x, const double* y, const double* m, const double* vol,
+                const double* theta, const double* dmg, const int64_t* row, const int32_t* col,
+                const double* K, const double* mu, int influence, double horizon, const double* w,
+                double* df);
+
 /* Whole explicit run (Peridigm::executeExplicit). */
 typedef struct {
   int64_t n;

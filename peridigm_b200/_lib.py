@@ -61,6 +61,17 @@ class Stats(C.Structure):
                 ("cg_iterations", C.c_int64), ("final_residual", C.c_double)]
 
 
+PD_PRECOND_NONE = 0
+PD_PRECOND_BLOCK_JACOBI = 1
+PD_PRECOND_MPNN = 2
+
+
+class QsOptions(C.Structure):
+    _fields_ = [("newton_tolerance", C.c_double), ("cg_relative_tolerance", C.c_double),
+                ("max_newton_iterations", C.c_int32), ("max_cg_iterations", C.c_int32),
+                ("preconditioner", C.c_int32), ("use_predictor", C.c_int32)]
+
+
 # name -> (restype, argtypes); every symbol include/pd_b200.h declares.
 SIGNATURES = {
     "pd_create": (C.c_int, [C.POINTER(Config), C.POINTER(_vp)]),
@@ -91,6 +102,9 @@ SIGNATURES = {
     "pd_get_field": (C.c_int, [_vp, C.c_int32, _dp]),
     "pd_contact_short_range": (C.c_int, [_vp, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "pd_contact_force": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "pd_qs_load_step": (C.c_int, [_vp, C.c_double, C.c_double, C.c_void_p, C.POINTER(Stats)]),
+    "pd_jacobian_apply": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "pd_jacobian_block_diagonal": (C.c_int, [_vp, _dp, _dp]),
     "pd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "pd_get_kernel_timing": (C.c_int, [_vp, _dp, _i64p]),
 }

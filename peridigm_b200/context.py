@@ -206,6 +206,34 @@ class Context:
         self._ok(self.L.pd_verlet_run(self.h, float(dt), float(t0), int(nsteps), C.byref(st)))
         return {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
 
+    # -- quasi-static --------------------------------------------------------
+    def qs_load_step(self, t_prev, t_cur, newton_tolerance, cg_relative_tolerance=1e-8, max_newton=20,
+                     max_cg=20000, preconditioner="block_jacobi", use_predictor=True, stats=None):
+        o = _lib.QsOptions()
+        o.newton_tolerance = float(newton_tolerance)
+        o.cg_relative_tolerance = float(cg_relative_tolerance)
+        o.max_newton_iterations = int(max_newton)
+        o.max_cg_iterations = int(max_cg)
+        o.preconditioner = {"none": _lib.PD_PRECOND_NONE, "block_jacobi": _lib.PD_PRECOND_BLOCK_JACOBI,
+                            "mpnn": _lib.PD_PRECOND_MPNN}[preconditioner]
+        o.use_predictor = 1 if use_predictor else 0
+        st = stats if stats is not None else _lib.Stats()
+        self._ok(self.L.pd_qs_load_step(self.h, float(t_prev), float(t_cur), C.cast(C.byref(o), C.c_void_p),
+                                        C.byref(st)))
+        return st
+
+    def jacobian_apply(self, u, w):
+        u, w = _f64(u, 3 * self.n, "u"), _f64(w, 3 * self.n, "w")
+        kw = np.zeros(3 * self.n)
+        self._ok(self.L.pd_jacobian_apply(self.h, _d(u), _d(w), _d(kw)))
+        return kw
+
+    def jacobian_blocks(self, u):
+        u = _f64(u, 3 * self.n, "u")
+        b = np.zeros(9 * self.n)
+        self._ok(self.L.pd_jacobian_block_diagonal(self.h, _d(u), _d(b)))
+        return b.reshape(self.n, 3, 3)
+
     def kernel_timing(self, enable=True):
         self._ok(self.L.pd_set_kernel_timing(self.h, 1 if enable else 0))
 

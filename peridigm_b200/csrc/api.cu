@@ -157,6 +157,10 @@ int eval_trial(pd_ctx* c, double* f_dev) {
 
 }  // namespace
 
+namespace pdb {
+int ensure_ready_internal(pd_ctx* c) { return ensure_ready(c); }
+}  // namespace pdb
+
 extern "C" {
 
 const char* pd_version(void) { return kVersion; }
@@ -561,6 +565,45 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
     stats->contact_pairs = contact_pairs(c);
   }
   return rc;
+}
+
+int pd_qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {
+  CHECK_CTX(c);
+  if (!o) return fail(c, PD_ERR_ARG, "pd_qs_load_step: null options");
+  if (!(t_cur > t_prev) || o->preconditioner < 0 || o->preconditioner > 2 || o->max_cg_iterations <= 0 ||
+      o->max_newton_iterations < 0 || !(o->cg_relative_tolerance > 0.0))
+    return fail(c, PD_ERR_ARG, "pd_qs_load_step: bad options");
+  if (!c->state_init) TRY(pd_set_state(c, nullptr, nullptr));
+  return qs_load_step(c, t_prev, t_cur, o, st);
+}
+
+int pd_jacobian_apply(pd_ctx* c, const double* u, const double* w, double* kw) {
+  CHECK_CTX(c);
+  if (!u || !w || !kw) return fail(c, PD_ERR_ARG, "pd_jacobian_apply: null argument");
+  TRY(ensure_ready(c));
+  const size_t b3 = 3 * (size_t)c->n * sizeof(double);
+  DBuf<double> ud, wd, kd;
+  PD_CUDA_TRY(c, ud.alloc(3 * c->n));
+  PD_CUDA_TRY(c, wd.alloc(3 * c->n));
+  PD_CUDA_TRY(c, kd.alloc(3 * c->n));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(ud.p, u, b3, cudaMemcpyHostToDevice, c->stream));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(wd.p, w, b3, cudaMemcpyHostToDevice, c->stream));
+  TRY(qs_tangent_apply(c, ud.p, wd.p, kd.p));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(kw, kd.p, b3, cudaMemcpyDeviceToHost, c->stream));
+  return check_status(c);
+}
+
+int pd_jacobian_block_diagonal(pd_ctx* c, const double* u, double* blocks) {
+  CHECK_CTX(c);
+  if (!u || !blocks) return fail(c, PD_ERR_ARG, "pd_jacobian_block_diagonal: null argument");
+  TRY(ensure_ready(c));
+  DBuf<double> ud, bd;
+  PD_CUDA_TRY(c, ud.alloc(3 * c->n));
+  PD_CUDA_TRY(c, bd.alloc(9 * c->n));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(ud.p, u, 3 * c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  TRY(qs_tangent_blocks(c, ud.p, bd.p));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(blocks, bd.p, 9 * c->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return check_status(c);
 }
 
 int pd_contact_short_range(pd_ctx* c, double r_search, int32_t freq, double r_contact, double k_spring,

@@ -363,6 +363,6 @@ int contact_force_from(pd_ctx* c, const double* y_dev, const double* v_dev, doub
   return PD_OK;
 }
 
-void qs_release(pd_ctx*) {}
+
 
 }  // namespace pdb

@@ -687,6 +687,26 @@ cudaError_t collect_kernel_times(pd_ctx* c) {
   return cudaSuccess;
 }
 
+// FP64 model evaluation at caller coordinates y4 (x, y, z, -): dilatation
+// pass into ab (theta, 3K/m - alpha/3, alpha) and force density into f_out.
+// No damage update; the committed bond damage is used as is.
+cudaError_t launch_fp64_eval_at(pd_ctx* c, const double4* y4, double4* ab, double* theta, double* nd,
+                                double* f_out) {
+  if (c->n == 0) return cudaSuccess;
+  const unsigned grid = grid_for(c->n, c->tpo);
+  PD_DISPATCH_TPO(c->tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, c->dmg.p, c->xv.p, y4, c->pt.p,
+                  c->sc.p, c->hp.p, c->influence, 0, ab, theta, nd);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  EpiArgs E{};
+  E.mode = EVAL_ONLY;
+  E.f_out = f_out;
+  E.status = c->status.p;
+  PD_DISPATCH_TPO(c->tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, c->dmg.p, c->xv.p, y4, ab, c->pt.p, c->hp.p,
+                  c->influence, E);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out_dev) {
   const unsigned grid = grid_for(c->n, c->tpo);
   if (c->scratch.count < (size_t)grid + 1) {

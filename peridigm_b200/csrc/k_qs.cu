@@ -1,0 +1,696 @@
+// Quasi-static Newton / CG (sm_100a), FP64.
+//
+// Replaces Peridigm::executeQuasiStatic (src/core/Peridigm.cpp:2470-3043) with
+// its residual (computeQuasiStaticResidual, :4176-4317), tangent
+// (ElasticMaterial::computeAutomaticDifferentiationJacobian,
+// src/materials/Peridigm_ElasticMaterial.cpp:258-383, Scale(-1) at
+// Peridigm.cpp:2800) and Belos CG (:2551-2573, :3321-3362):
+//  * residual r = V (f_int + f_ext), rows of prescribed dofs zeroed;
+//  * tangent K = -d r / d u applied matrix-free: the exact linearization of
+//    the LPS force in two bond passes (d theta, then d f), rows and columns of
+//    prescribed dofs replaced by identity (applyKinematicBC_InsertZerosAndSetDiagonal);
+//  * preconditioned CG with deterministic FP64 dot products; block-Jacobi
+//    preconditioner = inverses of the analytic 3x3 diagonal blocks of K
+//    (the reference's "Block 3x3" preconditioner, Peridigm.cpp:1603-1646);
+//    the learned preconditioner plugs in through mpnn_apply;
+//  * Newton with a backtracking step on the reference's convergence metric
+//    ||r||_2 + 20 ||r||_inf (Peridigm.cpp:4316).
+// For a bond (i,j) with Y = y_j - y_i, e = |Y| - |X|, de = Yhat.(w_j - w_i):
+//   d theta_i = sum 3 omega zeta de V_j / m_i
+//   t_ij = omega (zeta theta_i q_i + alpha_i e),  q = 3K/m - alpha/3, alpha = 15mu/m
+//   dt_ij = omega (zeta dtheta_i q_i + alpha_i de)
+//   d f_i = sum V_j [ (dt_ij + dt_ji) Yhat + (t_ij + t_ji) (dw - Yhat de)/|Y| ]
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "pd_internal.cuh"
+
+namespace pdb {
+
+constexpr int kQsBlock = 256;
+constexpr int kQsTpo = 8;
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs: fixed, so reductions are deterministic
+
+struct QsState {
+  DBuf<double4> yq;    // coordinates x + u + du
+  DBuf<double4> abq;   // (theta, q, alpha, q/m)
+  DBuf<double4> w;     // CG direction (p, dtheta)
+  DBuf<double> th, nd, f, r, du, x, z, q, pred, dinv, partial, scal;
+  DBuf<uint8_t> fixed;  // bit c: dof c prescribed
+  int64_t n = 0;
+};
+
+__device__ __forceinline__ double qs_omega(int kind, double zeta, double h) {
+  if (kind == PD_INFLUENCE_ONE) return 1.0;
+  if (kind == PD_INFLUENCE_PARABOLIC_DECAY) {
+    if (zeta > h) return 0.0;
+    const double s = zeta / h;
+    return s < 0.5 ? 1.0 : -4.0 * s * s + 4.0 * s;
+  }
+  return exp(-(zeta * zeta) / (h * h * 0.16));
+}
+
+template <typename T>
+__device__ __forceinline__ T qs_group_sum(T v) {
+#pragma unroll
+  for (int o = kQsTpo / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// y = (x + u) + du (Peridigm.cpp:2684-2687 operation order)
+__global__ void k_qs_positions(int64_t n, const double4* __restrict__ xv, const double* __restrict__ u,
+                               const double* __restrict__ du, double4* __restrict__ y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 x = xv[i];
+  y[i] = make_double4((x.x + u[3 * i]) + du[3 * i], (x.y + u[3 * i + 1]) + du[3 * i + 1],
+                      (x.z + u[3 * i + 2]) + du[3 * i + 2], 0.0);
+}
+
+// abq.w = q/m for the block-diagonal term
+__global__ void k_qs_qm(int64_t n, const double4* __restrict__ pt, double4* __restrict__ ab) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ab[i].w = ab[i].y / pt[i].x;
+}
+
+// r = V f with prescribed rows zeroed; block partials of sum r^2 and max |r|.
+__global__ void k_qs_residual(int64_t n, const double* __restrict__ f, const double4* __restrict__ xv,
+                              const uint8_t* __restrict__ fixed, double* __restrict__ r,
+                              double* __restrict__ partial) {
+  __shared__ double s2[kQsBlock], sm[kQsBlock];
+  double a2 = 0.0, am = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k / 3;
+    const int c = (int)(k - 3 * i);
+    double v = f[k] * xv[i].w;
+    if ((fixed[i] >> c) & 1) v = 0.0;
+    r[k] = v;
+    a2 += v * v;
+    am = fmax(am, fabs(v));
+  }
+  s2[threadIdx.x] = a2;
+  sm[threadIdx.x] = am;
+  __syncthreads();
+  for (int o = kQsBlock / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s2[threadIdx.x] += s2[threadIdx.x + o];
+      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s2[0];
+    partial[2 * blockIdx.x + 1] = sm[0];
+  }
+}
+
+// Sums (even slots) and maxima (odd slots) of kRedBlocks partial pairs, or
+// plain sums of `width` interleaved partials; fixed order.
+__global__ void k_qs_reduce(const double* __restrict__ partial, int width, int mode, double* __restrict__ out) {
+  __shared__ double s[kQsBlock];
+  for (int c = 0; c < width; ++c) {
+    double a = (mode == 1 && c == 1) ? 0.0 : 0.0;
+    for (int b = threadIdx.x; b < kRedBlocks; b += blockDim.x) {
+      const double v = partial[width * b + c];
+      a = (mode == 1 && c == 1) ? fmax(a, v) : a + v;
+    }
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = kQsBlock / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) s[threadIdx.x] = (mode == 1 && c == 1) ? fmax(s[threadIdx.x], s[threadIdx.x + o])
+                                                                   : s[threadIdx.x] + s[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[c] = s[0];
+    __syncthreads();
+  }
+}
+
+// Tangent pass 1: d theta_i into w[i].w
+__global__ void __launch_bounds__(kQsBlock) k_qs_dtheta(int64_t n, const int64_t* __restrict__ row,
+                                                        const int32_t* __restrict__ col,
+                                                        const uint8_t* __restrict__ dmg,
+                                                        const double4* __restrict__ xv,
+                                                        const double4* __restrict__ y,
+                                                        const double4* __restrict__ pt,
+                                                        const double* __restrict__ hp, int influence,
+                                                        double4* __restrict__ w) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
+  const int lane = threadIdx.x & (kQsTpo - 1);
+  const bool valid = i < n;
+  double acc = 0.0;
+  if (valid) {
+    const double4 xi = xv[i], yi = y[i], wi = w[i];
+    const double h = hp[i];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+      if (dmg[b]) continue;
+      const int32_t j = col[b];
+      const double4 xj = xv[j], yj = y[j], wj = w[j];
+      const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
+      const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
+      const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
+      const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
+      const double de = (Y0 * (wj.x - wi.x) + Y1 * (wj.y - wi.y) + Y2 * (wj.z - wi.z)) / dY;
+      acc += 3.0 * qs_omega(influence, zeta, h) * zeta * de * xj.w;
+    }
+  }
+  acc = qs_group_sum(acc);
+  if (valid && lane == 0) w[i].w = acc / pt[i].x;
+}
+
+// Tangent pass 2: q = K p = -V d f (prescribed rows: q = p); block partials of p.q
+__global__ void __launch_bounds__(kQsBlock) k_qs_df(int64_t n, const int64_t* __restrict__ row,
+                                                    const int32_t* __restrict__ col,
+                                                    const uint8_t* __restrict__ dmg,
+                                                    const double4* __restrict__ xv,
+                                                    const double4* __restrict__ y,
+                                                    const double4* __restrict__ ab,
+                                                    const double* __restrict__ hp, int influence,
+                                                    const double4* __restrict__ w, const uint8_t* __restrict__ fixed,
+                                                    double* __restrict__ q, double* __restrict__ partial) {
+  __shared__ double spq[kQsBlock];
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
+  const int lane = threadIdx.x & (kQsTpo - 1);
+  const bool valid = i < n;
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  double4 wi = make_double4(0, 0, 0, 0), xi = make_double4(0, 0, 0, 1);
+  if (valid) {
+    xi = xv[i];
+    const double4 yi = y[i], ai = ab[i];
+    wi = w[i];
+    const double h = hp[i];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+      if (dmg[b]) continue;
+      const int32_t j = col[b];
+      const double4 xj = xv[j], yj = y[j], wj = w[j], aj = ab[j];
+      const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
+      const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
+      const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
+      const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
+      const double e = dY - zeta;
+      const double w0 = wj.x - wi.x, w1 = wj.y - wi.y, w2 = wj.z - wi.z;
+      const double de = (Y0 * w0 + Y1 * w1 + Y2 * w2) / dY;
+      const double om = qs_omega(influence, zeta, h);
+      const double T = om * (zeta * (ai.x * ai.y + aj.x * aj.y) + (ai.z + aj.z) * e);
+      const double dT = om * (zeta * (wi.w * ai.y + wj.w * aj.y) + (ai.z + aj.z) * de);
+      const double V = xj.w, inv = 1.0 / dY;
+      const double y0 = Y0 * inv, y1 = Y1 * inv, y2 = Y2 * inv;
+      d0 += V * (dT * y0 + T * (w0 - y0 * de) * inv);
+      d1 += V * (dT * y1 + T * (w1 - y1 * de) * inv);
+      d2 += V * (dT * y2 + T * (w2 - y2 * de) * inv);
+    }
+  }
+  d0 = qs_group_sum(d0);
+  d1 = qs_group_sum(d1);
+  d2 = qs_group_sum(d2);
+  double pq = 0.0;
+  if (valid && lane < 3) {
+    const double d = lane == 0 ? d0 : (lane == 1 ? d1 : d2);
+    const double p = lane == 0 ? wi.x : (lane == 1 ? wi.y : wi.z);
+    const double out = ((fixed[i] >> lane) & 1) ? p : -xi.w * d;
+    q[3 * i + lane] = out;
+    pq = p * out;
+  }
+  spq[threadIdx.x] = pq;
+  __syncthreads();
+  for (int o = kQsBlock / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) spq[threadIdx.x] += spq[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = spq[0];
+}
+
+// Inverse 3x3 diagonal blocks of K (prescribed rows/columns set to identity).
+__global__ void __launch_bounds__(kQsBlock) k_qs_block_diag(int64_t n, const int64_t* __restrict__ row,
+                                                            const int32_t* __restrict__ col,
+                                                            const uint8_t* __restrict__ dmg,
+                                                            const double4* __restrict__ xv,
+                                                            const double4* __restrict__ y,
+                                                            const double4* __restrict__ ab,
+                                                            const double4* __restrict__ pt,
+                                                            const double* __restrict__ hp, int influence,
+                                                            const uint8_t* __restrict__ fixed,
+                                                            double* __restrict__ dinv, int invert) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
+  const int lane = threadIdx.x & (kQsTpo - 1);
+  const bool valid = i < n;
+  double D[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double hv[3] = {0, 0, 0};
+  double4 xi = make_double4(0, 0, 0, 1), ai = make_double4(0, 0, 0, 0);
+  double mi = 1.0;
+  if (valid) {
+    xi = xv[i];
+    const double4 yi = y[i];
+    ai = ab[i];
+    mi = pt[i].x;
+    const double h = hp[i];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+      if (dmg[b]) continue;
+      const int32_t j = col[b];
+      const double4 xj = xv[j], yj = y[j], aj = ab[j];
+      const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
+      const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
+      const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
+      const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
+      const double e = dY - zeta;
+      const double om = qs_omega(influence, zeta, h);
+      const double T = om * (zeta * (ai.x * ai.y + aj.x * aj.y) + (ai.z + aj.z) * e);
+      const double V = xj.w;
+      const double yh[3] = {Y0 / dY, Y1 / dY, Y2 / dY};
+      const double a = -V * om * ((ai.z + aj.z) + 3.0 * om * zeta * zeta * aj.w * xi.w);
+      const double g = -V * T / dY;
+      for (int r = 0; r < 3; ++r) {
+        hv[r] += V * om * zeta * yh[r];
+        for (int c = 0; c < 3; ++c) D[3 * r + c] += (a - g) * yh[r] * yh[c] + (r == c ? g : 0.0);
+      }
+    }
+  }
+  for (int k = 0; k < 9; ++k) D[k] = qs_group_sum(D[k]);
+  for (int k = 0; k < 3; ++k) hv[k] = qs_group_sum(hv[k]);
+  if (valid && lane == 0) {
+    const double s = 3.0 * ai.y / mi;
+    double A[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) A[3 * r + c] = -xi.w * (D[3 * r + c] - s * hv[r] * hv[c]);  // K_ii = -V_i D_i
+    const uint8_t fx = fixed[i];
+    for (int c = 0; c < 3; ++c)
+      if ((fx >> c) & 1)
+        for (int k = 0; k < 3; ++k) {
+          A[3 * c + k] = (k == c) ? 1.0 : 0.0;
+          A[3 * k + c] = (k == c) ? 1.0 : 0.0;
+        }
+    if (!invert) {
+      for (int k = 0; k < 9; ++k) dinv[9 * i + k] = A[k];
+      return;
+    }
+    const double c00 = A[4] * A[8] - A[5] * A[7], c01 = A[5] * A[6] - A[3] * A[8], c02 = A[3] * A[7] - A[4] * A[6];
+    const double det = A[0] * c00 + A[1] * c01 + A[2] * c02;
+    const double id = 1.0 / det;
+    double* o = dinv + 9 * i;
+    o[0] = c00 * id;
+    o[1] = (A[2] * A[7] - A[1] * A[8]) * id;
+    o[2] = (A[1] * A[5] - A[2] * A[4]) * id;
+    o[3] = c01 * id;
+    o[4] = (A[0] * A[8] - A[2] * A[6]) * id;
+    o[5] = (A[2] * A[3] - A[0] * A[5]) * id;
+    o[6] = c02 * id;
+    o[7] = (A[1] * A[6] - A[0] * A[7]) * id;
+    o[8] = (A[0] * A[4] - A[1] * A[3]) * id;
+  }
+}
+
+// z = P r (block Jacobi or identity); optional partial sums of r.z and r.r.
+__global__ void k_qs_precond(int64_t n, const double* __restrict__ dinv, const double* __restrict__ r,
+                             double* __restrict__ z, int use_bj) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double r0 = r[3 * i], r1 = r[3 * i + 1], r2 = r[3 * i + 2];
+  if (!use_bj) {
+    z[3 * i] = r0, z[3 * i + 1] = r1, z[3 * i + 2] = r2;
+    return;
+  }
+  const double* d = dinv + 9 * i;
+  z[3 * i] = d[0] * r0 + d[1] * r1 + d[2] * r2;
+  z[3 * i + 1] = d[3] * r0 + d[4] * r1 + d[5] * r2;
+  z[3 * i + 2] = d[6] * r0 + d[7] * r1 + d[8] * r2;
+}
+
+// Partial dot products: out[3b] = a.b, out[3b+1] = a.c, out[3b+2] = a.a (c may equal b)
+__global__ void k_qs_dots(int64_t m, const double* __restrict__ a, const double* __restrict__ b,
+                          const double* __restrict__ c, double* __restrict__ partial) {
+  __shared__ double s[3][kQsBlock];
+  double ab = 0.0, ac = 0.0, aa = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+    const double va = a[k];
+    ab += va * b[k];
+    ac += va * c[k];
+    aa += va * va;
+  }
+  s[0][threadIdx.x] = ab;
+  s[1][threadIdx.x] = ac;
+  s[2][threadIdx.x] = aa;
+  __syncthreads();
+  for (int o = kQsBlock / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partial[3 * blockIdx.x + k] = s[k][0];
+}
+
+// x += alpha p ; r -= alpha q   (alpha = scal[0]/scal[1])
+__global__ void k_qs_axpy2(int64_t m, const double* __restrict__ scal, const double4* __restrict__ w,
+                           const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const double alpha = scal[0] / scal[1];
+  const double4 p = w[k / 3];
+  const int c = (int)(k % 3);
+  const double pk = c == 0 ? p.x : (c == 1 ? p.y : p.z);
+  x[k] += alpha * pk;
+  r[k] -= alpha * q[k];
+}
+
+// p = z + beta p  with beta = scal[2]/scal[0] (flexible: (z.r - z.r_old)/rz_old folded by the host)
+__global__ void k_qs_update_p(int64_t n, const double* __restrict__ scal, const double* __restrict__ z,
+                              double4* __restrict__ w, int first) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double beta = first ? 0.0 : scal[3];
+  double4 p = w[i];
+  p.x = z[3 * i] + beta * p.x;
+  p.y = z[3 * i + 1] + beta * p.y;
+  p.z = z[3 * i + 2] + beta * p.z;
+  w[i] = p;
+}
+
+__global__ void k_qs_set_scalars(double* scal, const double* red, int what) {
+  // what 0: scal[1] = p.q ; what 1: rz_new -> beta
+  if (threadIdx.x != 0) return;
+  if (what == 0) {
+    scal[1] = red[0];
+  } else {
+    const double rz_new = red[0];
+    scal[3] = rz_new / scal[0];  // beta (Fletcher-Reeves on the preconditioned residual)
+    scal[0] = rz_new;
+    scal[4] = red[2];  // r.r
+  }
+}
+
+__global__ void k_qs_axpy(int64_t m, double a, const double* __restrict__ x, double* __restrict__ y) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) y[k] += a * x[k];
+}
+
+__global__ void k_qs_apply_bc(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ a,
+                              const double* __restrict__ b, double tc, double tp, double* __restrict__ du) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int c = 0; c < 3; ++c)
+    if ((mask[i] >> c) & 1) {
+      const int64_t k = 3 * i + c;
+      du[k] = (a[k] * tc + b[k]) - (a[k] * tp + b[k]);  // DirichletIncrementBC coeff 1 (Peridigm_BoundaryCondition.cpp:235)
+    }
+}
+
+__global__ void k_qs_finish(int64_t m, double inv_dt, const double* __restrict__ du, double* __restrict__ u,
+                            double* __restrict__ v) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  u[k] += du[k];
+  v[k] = du[k] * inv_dt;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static unsigned g1(int64_t m) { return (unsigned)((m + kQsBlock - 1) / kQsBlock); }
+static unsigned gt(int64_t n) { return (unsigned)((n * kQsTpo + kQsBlock - 1) / kQsBlock); }
+
+static int qs_alloc(pd_ctx* c) {
+  if (!c->qs) c->qs = new QsState();
+  QsState* s = c->qs;
+  if (s->n == c->n) return PD_OK;
+  const int64_t n = c->n;
+  PD_CUDA_TRY(c, s->yq.alloc(n));
+  PD_CUDA_TRY(c, s->abq.alloc(n));
+  PD_CUDA_TRY(c, s->w.alloc(n));
+  PD_CUDA_TRY(c, s->th.alloc(n));
+  PD_CUDA_TRY(c, s->nd.alloc(n));
+  for (auto* b : {&s->f, &s->r, &s->du, &s->x, &s->z, &s->q, &s->pred}) PD_CUDA_TRY(c, b->alloc(3 * n));
+  PD_CUDA_TRY(c, s->dinv.alloc(9 * n));
+  PD_CUDA_TRY(c, s->partial.alloc(3 * (size_t)std::max<int64_t>(kRedBlocks, gt(n)) + 8));
+  PD_CUDA_TRY(c, s->scal.alloc(16));
+  PD_CUDA_TRY(c, s->fixed.alloc(n));
+  PD_CUDA_TRY(c, cudaMemset(s->pred.p, 0, s->pred.bytes()));
+  s->n = n;
+  return PD_OK;
+}
+
+void qs_release(pd_ctx* c) {
+  delete c->qs;
+  c->qs = nullptr;
+}
+
+// Residual at y = x + u + du; returns ||r||_2 and ||r||_inf.
+static int qs_residual(pd_ctx* c, double* l2, double* linf) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, c->u.p, s->du.p, s->yq.p);
+  PD_CUDA_TRY(c, launch_fp64_eval_at(c, s->yq.p, s->abq.p, s->th.p, s->nd.p, s->f.p));
+  k_qs_residual<<<kRedBlocks, kQsBlock, 0, c->stream>>>(n, s->f.p, c->xv.p, s->fixed.p, s->r.p, s->partial.p);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 2, 1, s->scal.p + 8);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  double h[2];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  *l2 = std::sqrt(h[0]);
+  *linf = h[1];
+  if (!std::isfinite(*l2)) {
+    c->err = "NaN returned by force evaluation";
+    return PD_ERR_NONFINITE;
+  }
+  return PD_OK;
+}
+
+static int qs_apply_precond(pd_ctx* c, int precond, const double* r, double* z) {
+  QsState* s = c->qs;
+  if (precond == PD_PRECOND_MPNN) return mpnn_apply(c, r, z, s->dinv.p);
+  k_qs_precond<<<g1(c->n), kQsBlock, 0, c->stream>>>(c->n, s->dinv.p, r, z, precond == PD_PRECOND_BLOCK_JACOBI);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+// Tangent-vector product q = K w.xyz (w.w receives d theta).
+static int qs_tangent(pd_ctx* c) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_dtheta<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, c->pt.p,
+                                                 c->hp.p, c->influence, s->w.p);
+  k_qs_df<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p, c->hp.p,
+                                             c->influence, s->w.p, s->fixed.p, s->q.p, s->partial.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+// Preconditioned CG on K x = r (Belos BlockCG in the reference). Flexible
+// (Polak-Ribiere) beta when the preconditioner is not a fixed linear operator.
+static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out) {
+  QsState* s = c->qs;
+  const int64_t n = c->n, m = 3 * n;
+  const bool flexible = precond == PD_PRECOND_MPNN;
+  PD_CUDA_TRY(c, cudaMemsetAsync(s->x.p, 0, s->x.bytes(), c->stream));
+  TRY_RC(qs_apply_precond(c, precond, s->r.p, s->z.p));
+  // scal: [0] rz, [1] pq, [3] beta, [4] rr
+  k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 8);
+  double h[3];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const double r0 = std::sqrt(h[2]);
+  double rz = h[0];
+  *iters = 0;
+  *rel_out = 0.0;
+  if (r0 == 0.0) return PD_OK;
+  PD_CUDA_TRY(c, cudaMemcpyAsync(s->scal.p, &rz, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  k_qs_update_p<<<g1(n), kQsBlock, 0, c->stream>>>(n, s->scal.p, s->z.p, s->w.p, 1);
+  DBuf<double> zold;
+  if (flexible) PD_CUDA_TRY(c, zold.alloc(m));
+  double rel = 1.0;
+  int it = 0;
+  while (it < max_it) {
+    TRY_RC(qs_tangent(c));
+    k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 1, 0, s->scal.p + 8);
+    k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 0);
+    if (flexible) PD_CUDA_TRY(c, cudaMemcpyAsync(zold.p, s->z.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    k_qs_axpy2<<<g1(m), kQsBlock, 0, c->stream>>>(m, s->scal.p, s->w.p, s->q.p, s->x.p, s->r.p);
+    TRY_RC(qs_apply_precond(c, precond, s->r.p, s->z.p));
+    if (flexible) {
+      // beta = z_new.(r_new - r_old)/rz_old = (z_new.r_new - z_new.r_old)/rz_old with r_old = r_new + alpha q
+      k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
+      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 8);
+      double hz[3], sc[2];
+      PD_CUDA_TRY(c, cudaMemcpyAsync(hz, s->scal.p + 8, sizeof(hz), cudaMemcpyDeviceToHost, c->stream));
+      PD_CUDA_TRY(c, cudaMemcpyAsync(sc, s->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+      k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->z.p, s->q.p, s->q.p, s->partial.p);
+      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 12);
+      double hq[3];
+      PD_CUDA_TRY(c, cudaMemcpyAsync(hq, s->scal.p + 12, sizeof(hq), cudaMemcpyDeviceToHost, c->stream));
+      PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      const double alpha = sc[0] / sc[1];
+      const double zr_new = hz[0];
+      const double zr_old = zr_new + alpha * hq[0];  // z_new.r_old
+      const double beta = std::max(0.0, (zr_new - zr_old) / rz);
+      rz = zr_new;
+      const double hs[5] = {rz, sc[1], 0.0, beta, hz[2]};
+      PD_CUDA_TRY(c, cudaMemcpyAsync(s->scal.p, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
+      rel = std::sqrt(hz[2]) / r0;
+    } else {
+      k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
+      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 8);
+      k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 1);
+      double rr;
+      PD_CUDA_TRY(c, cudaMemcpyAsync(&rr, s->scal.p + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+      rel = std::sqrt(rr) / r0;
+    }
+    ++it;
+    if (!std::isfinite(rel)) {
+      c->err = "CG diverged (non-finite residual)";
+      return PD_ERR_NONFINITE;
+    }
+    if (rel <= rel_tol) break;
+    k_qs_update_p<<<g1(n), kQsBlock, 0, c->stream>>>(n, s->scal.p, s->z.p, s->w.p, 0);
+  }
+  PD_CUDA_TRY(c, cudaGetLastError());
+  *iters = it;
+  *rel_out = rel;
+  return rel <= rel_tol ? PD_OK : PD_ERR_NOT_CONVERGED;
+}
+
+__global__ void k_qs_pack_w(int64_t n, const double* __restrict__ w, const uint8_t* __restrict__ fixed,
+                            double4* __restrict__ w4) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t f = fixed[i];
+  w4[i] = make_double4((f & 1) ? 0.0 : w[3 * i], (f & 2) ? 0.0 : w[3 * i + 1], (f & 4) ? 0.0 : w[3 * i + 2], 0.0);
+}
+
+__global__ void k_qs_fixed_rows(int64_t n, const double* __restrict__ w, const uint8_t* __restrict__ fixed,
+                                double* __restrict__ q) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int c = 0; c < 3; ++c)
+    if ((fixed[i] >> c) & 1) q[3 * i + c] = w[3 * i + c];
+}
+
+static int qs_prepare_at(pd_ctx* c, const double* u_dev) {
+  TRY_RC(ensure_ready_internal(c));
+  TRY_RC(qs_alloc(c));
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  std::vector<uint8_t> fx(n, 0);
+  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
+  PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, 3 * n * sizeof(double), c->stream));
+  k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, u_dev, s->du.p, s->yq.p);
+  PD_CUDA_TRY(c, launch_fp64_eval_at(c, s->yq.p, s->abq.p, s->th.p, s->nd.p, s->f.p));
+  k_qs_qm<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->pt.p, s->abq.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+// Matrix-free tangent K w at displacement u (prescribed rows/columns identity).
+int qs_tangent_apply(pd_ctx* c, const double* u_dev, const double* w_dev, double* kw_dev) {
+  TRY_RC(qs_prepare_at(c, u_dev));
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_pack_w<<<g1(n), kQsBlock, 0, c->stream>>>(n, w_dev, s->fixed.p, s->w.p);
+  TRY_RC(qs_tangent(c));
+  k_qs_fixed_rows<<<g1(n), kQsBlock, 0, c->stream>>>(n, w_dev, s->fixed.p, s->q.p);
+  PD_CUDA_TRY(c, cudaMemcpyAsync(kw_dev, s->q.p, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  return PD_OK;
+}
+
+// 3x3 diagonal blocks of K at displacement u (row-major, 9 per point).
+int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev) {
+  TRY_RC(qs_prepare_at(c, u_dev));
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_block_diag<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p,
+                                                     c->pt.p, c->hp.p, c->influence, s->fixed.p, blocks_dev, 0);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {
+  TRY_RC(ensure_ready_internal(c));
+  TRY_RC(qs_alloc(c));
+  QsState* s = c->qs;
+  const int64_t n = c->n, m = 3 * n;
+  const int precond = o->preconditioner;
+  if (precond == PD_PRECOND_MPNN && !mpnn_ready(c)) {
+    c->err = "the learned preconditioner is not trained (pd_mpnn_train) or loaded";
+    return PD_ERR_STATE;
+  }
+  // prescribed dofs and their increments (DirichletIncrementBC on deltaU)
+  std::vector<uint8_t> fx(n, 0);
+  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
+  const double dt = t_cur - t_prev;
+  if (o->use_predictor && st && st->steps > 0) {
+    PD_CUDA_TRY(c, cudaMemcpyAsync(s->du.p, s->pred.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
+  }
+  if (c->has_bc)
+    k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, s->du.p);
+  double l2, linf;
+  TRY_RC(qs_residual(c, &l2, &linf));
+  double metric = l2 + 20.0 * linf;
+  int newton = 0, cg_total = 0;
+  double last_rel = 0.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c->stream);
+  while (metric > o->newton_tolerance && newton < o->max_newton_iterations) {
+    if (precond != PD_PRECOND_NONE) {
+      k_qs_qm<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->pt.p, s->abq.p);
+      k_qs_block_diag<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p,
+                                                         c->pt.p, c->hp.p, c->influence, s->fixed.p, s->dinv.p, 1);
+      PD_CUDA_TRY(c, cudaGetLastError());
+    }
+    int its = 0;
+    double rel = 0.0;
+    int rc = qs_cg(c, precond, o->cg_relative_tolerance, o->max_cg_iterations, &its, &rel);
+    cg_total += its;
+    last_rel = rel;
+    if (rc != PD_OK && rc != PD_ERR_NOT_CONVERGED) return rc;
+    // du += alpha * x, backtracking on the convergence metric
+    double alpha = 1.0, prev = metric;
+    k_qs_axpy<<<g1(m), kQsBlock, 0, c->stream>>>(m, alpha, s->x.p, s->du.p);
+    TRY_RC(qs_residual(c, &l2, &linf));
+    metric = l2 + 20.0 * linf;
+    for (int k = 0; k < 8 && !(metric < prev); ++k) {
+      k_qs_axpy<<<g1(m), kQsBlock, 0, c->stream>>>(m, -0.5 * alpha, s->x.p, s->du.p);
+      alpha *= 0.5;
+      TRY_RC(qs_residual(c, &l2, &linf));
+      metric = l2 + 20.0 * linf;
+    }
+    ++newton;
+  }
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // commit: u += du, v = du/dt (Peridigm.cpp:2858-2862); predictor for the next step
+  k_qs_finish<<<g1(m), kQsBlock, 0, c->stream>>>(m, dt != 0.0 ? 1.0 / dt : 0.0, s->du.p, c->u.p, c->v.p);
+  PD_CUDA_TRY(c, cudaMemcpyAsync(s->pred.p, s->du.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  if (c->has_bc) PD_CUDA_TRY(c, cudaMemsetAsync(s->pred.p, 0, 0, c->stream));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->f.p, s->f.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->theta.p, s->th.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  c->cur = 0;
+  PD_CUDA_TRY(c, launch_sync_state(c));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (st) {
+    st->steps += 1;
+    st->newton_iterations += newton;
+    st->cg_iterations += cg_total;
+    st->final_residual = last_rel;
+    st->device_ms += ms;
+    st->bonds = c->nb;
+  }
+  if (metric > o->newton_tolerance) {
+    c->err = "quasi-static Newton iteration did not reach its tolerance";
+    return PD_ERR_NOT_CONVERGED;
+  }
+  return PD_OK;
+}
+
+}  // namespace pdb

@@ -178,6 +178,16 @@ cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev);
 cudaError_t launch_sync_state(pd_ctx* c);
 cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out);
 cudaError_t collect_kernel_times(pd_ctx* c);
+cudaError_t launch_fp64_eval_at(pd_ctx* c, const double4* y4, double4* ab, double* theta, double* nd, double* f_out);
+int ensure_ready_internal(pd_ctx* c);
+
+// quasi-static (k_qs.cu) and the learned preconditioner (k_mpnn.cu)
+int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st);
+int qs_tangent_apply(pd_ctx* c, const double* u_dev, const double* w_dev, double* kw_dev);
+int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev);
+bool mpnn_ready(const pd_ctx* c);
+int mpnn_apply(pd_ctx* c, const double* r, double* z, const double* dinv);
+void mpnn_release(pd_ctx* c);
 
 // bonds
 int build_bonds_device(pd_ctx* c, const pd_plane_filter* filters, int nf);
@@ -197,6 +207,12 @@ void qs_release(pd_ctx* c);
 enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4 };
 
 }  // namespace pdb
+
+#define TRY_RC(expr)              \
+  do {                            \
+    int rc_ = (expr);             \
+    if (rc_ != PD_OK) return rc_; \
+  } while (0)
 
 #define PD_CUDA_TRY(ctx, expr)                                                   \
   do {                                                                           \

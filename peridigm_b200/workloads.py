@@ -114,23 +114,23 @@ def bonds_per_point_estimate(horizon_over_h):
     return 4.0 / 3.0 * math.pi * r ** 3
 
 
-def plate_sphere(nx=400, ny=400, nz=40, h=0.25e-3, radius_cells=25, s_c=3.0e-4, speed=20.0, gap_cells=0.5,
+def plate_sphere(nx=400, ny=400, nz=40, h=0.25e-3, radius_cells=25, s_c=3.0e-4, speed=20.0, gap_cells=3.5,
                  search_extra=0.6, freq=100, nsteps=2000):
     """Brittle plate (block 0, critical stretch s_c) and a dropped sphere (block 1,
     elastic only) on the same lattice spacing, short-range contact.
 
     Sphere: lattice points within radius_cells*h of its centre, centred above the
-    plate middle with its lowest point gap_cells*h above the plate's top layer;
-    initial velocity -speed in z. Contact radius 0.9h, spring constant = plate
-    bulk modulus, search radius 0.9h + search_extra*h (a pair outside it at a
-    search cannot close the extra gap within freq steps at these speeds),
-    search frequency freq."""
+    plate middle, its lowest point gap_cells*h above the plate's top layer (more
+    than a horizon, so no bond joins the bodies); initial velocity -speed in z.
+    Contact radius 0.9h, spring constant = plate bulk modulus, search radius
+    0.9h + search_extra*h (a pair outside it at a search cannot close the extra
+    gap within freq steps at these speeds), search frequency freq."""
     xp, vp = lattice(nx, ny, nz, h)
     r = radius_cells
     k = np.arange(-r, r + 1)
     Z, Y, X = np.meshgrid(k, k, k, indexing="ij")
     keep = X ** 2 + Y ** 2 + Z ** 2 <= r * r
-    c = np.array([nx * h / 2.0, ny * h / 2.0, nz * h - 0.5 * h + (r + gap_cells + 1.0) * h])
+    c = np.array([nx * h / 2.0, ny * h / 2.0, nz * h - 0.5 * h + (r + gap_cells) * h])
     xs = (np.stack([X[keep], Y[keep], Z[keep]], 1) * h + c).ravel()
     x = np.concatenate([xp, xs])
     vol = np.full(x.size // 3, h ** 3)
@@ -172,3 +172,21 @@ def oracle_problem_blocks(w, row, col, dt, nsteps):
                             k_spring=ct["k_spring"], friction=ct.get("friction", 0.0),
                             horizon=np.full(len(w["vol"]), w["horizon"]))
     return p
+
+
+def qs_cube(n=60, h=1.0e-3, seed=0, displacement=1.0e-4, load_steps=20, jitter=0.0):
+    """Quasi-static tensile cube: n^3 lattice, delta = 3.015h, bulk modulus drawn
+    log-uniform in [50, 200] GPa from the seed, shear modulus 0.6K; the x = min
+    face (3 layers) clamped in all components, the x = max face (3 layers)
+    displaced u_x = displacement * t for load parameter t in [0, 1], reached in
+    load_steps equal steps."""
+    x, vol = lattice(n, n, n, h, jitter=jitter, seed=seed)
+    rng = np.random.default_rng(seed)
+    K = float(np.exp(rng.uniform(np.log(50.0e9), np.log(200.0e9))))
+    col_id = np.arange(n ** 3) % n
+    left = np.nonzero(col_id < 3)[0]
+    right = np.nonzero(col_id >= n - 3)[0]
+    bcs = [dict(points=left, coordinate=c, a=0.0, b=0.0) for c in range(3)]
+    bcs.append(dict(points=right, coordinate=0, a=displacement, b=0.0))
+    return dict(name=f"qs_cube_{n}", x=x, vol=vol, horizon=3.015 * h, K=K, mu=0.6 * K, rho=7800.0, s_c=None,
+                planes=[], v0=np.zeros_like(x), bcs=bcs, h=h, times=np.linspace(0.0, 1.0, load_steps + 1))

@@ -272,9 +272,29 @@ def finite_plane():
         json.dump({"points": pts, "horizon": 1.1 * math.sqrt(3.0), "cases": cases}, fh, indent=1)
 
 
+def compression_qs():
+    """Compression_QS_3x2x2 (test/regression/Compression_QS_3x2x2): 12-point
+    PdQuickGrid, spherical neighborhood, 20 quasi-static load steps."""
+    d = os.path.join(REF, "test/regression/Compression_QS_3x2x2")
+    g = read_exodus_results(os.path.join(d, "Compression_QS_3x2x2_gold.e"))
+    x, vol, nl = quickgrid((-1.5, -1.0, -1.0), (3.0, 2.0, 2.0), (3, 2, 2), 1.75, spherical=True)
+    assert np.allclose(x, g["x"])
+    # node sets (1-based ids in the deck) -> (points, coordinate, a, b) with u(t) = a t + b
+    bcs = [([0, 3, 6, 9], 0, 0.0, 0.0), ([2, 5, 8, 11], 0, -0.1 / 0.00005, 0.0), ([0, 3], 2, 0.0, 0.0),
+           ([0, 6], 1, 0.0, 0.0)]
+    bc = np.array([(p, c, a, b) for pts, c, a, b in bcs for p in pts], dtype=np.float64)
+    out = dict(x=x, vol=vol, nl=nl, bc=bc, params=np.array([7800.0, 130.0e9, 78.0e9, 1.75, 0.0, 0.00005, 20, 1.0e-2]),
+               time=g["time"])
+    for nm in ["DisplacementX", "DisplacementY", "DisplacementZ", "VelocityX", "VelocityY", "VelocityZ",
+               "Force_DensityX", "Force_DensityY", "Force_DensityZ", "Weighted_Volume", "Dilatation"]:
+        out[nm] = g[nm]
+    np.savez_compressed(os.path.join(OUT, "compression_qs.npz"), **out)
+
+
 def main():
     unit_elastic()
     finite_plane()
+    compression_qs()
     bond_breaking()
     contact_2x1x1()
     wave_in_bar()

