@@ -232,6 +232,25 @@ int pd_jacobian_apply(pd_ctx* ctx, const double* u, const double* w, double* kw)
  * at displacement u, row-major, 9 per point. */
 int pd_jacobian_block_diagonal(pd_ctx* ctx, const double* u, double* blocks);
 
+/* ---- learned preconditioner (no counterpart in the reference) -------------
+ * A message-passing network on the subgraph of bonds shorter than `radius`
+ * (3 layers, hidden 64, BF16 weights and activations, FP32 accumulation)
+ * that corrects block Jacobi: z = P_bj r + rms(P_bj r) * N(P_bj r / rms, r / rms).
+ * Used with PD_PRECOND_MPNN in flexible CG; a stall, or a true FP64 residual
+ * above the tolerance, falls back to block-Jacobi CG. */
+int pd_mpnn_init(pd_ctx* ctx, uint64_t seed, double radius);
+/* While every > 0, block-Jacobi CG solves of pd_qs_load_step store training
+ * pairs (r_k, x* - x_k) from every every-th iterate (K (x* - x_k) = r_k). */
+int pd_mpnn_collect(pd_ctx* ctx, int32_t every);
+int pd_mpnn_num_pairs(pd_ctx* ctx, int64_t* count);
+/* Adam on the stored pairs, loss |z - e|^2 / |e|^2, on the device. */
+int pd_mpnn_train(pd_ctx* ctx, int32_t epochs, double learning_rate, int32_t batch, double* loss);
+int pd_mpnn_num_params(int64_t* count);
+int pd_mpnn_get_weights(pd_ctx* ctx, float* weights);
+int pd_mpnn_set_weights(pd_ctx* ctx, const float* weights);
+/* Loss and parameter gradient of one pair (a = P_bj r, r, e; 9n floats), for checks. */
+int pd_mpnn_loss_grad(pd_ctx* ctx, const float* pair, double* loss, float* grad);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Named stopwatches around the hot calls are the reference's Timer
  * (src/core/Peridigm_Timer.hpp:77-86); here CUDA events bracket every launch

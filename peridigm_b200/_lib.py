@@ -105,6 +105,14 @@ SIGNATURES = {
     "pd_qs_load_step": (C.c_int, [_vp, C.c_double, C.c_double, C.c_void_p, C.POINTER(Stats)]),
     "pd_jacobian_apply": (C.c_int, [_vp, _dp, _dp, _dp]),
     "pd_jacobian_block_diagonal": (C.c_int, [_vp, _dp, _dp]),
+    "pd_mpnn_init": (C.c_int, [_vp, C.c_uint64, C.c_double]),
+    "pd_mpnn_collect": (C.c_int, [_vp, C.c_int32]),
+    "pd_mpnn_num_pairs": (C.c_int, [_vp, _i64p]),
+    "pd_mpnn_train": (C.c_int, [_vp, C.c_int32, C.c_double, C.c_int32, _dp]),
+    "pd_mpnn_num_params": (C.c_int, [_i64p]),
+    "pd_mpnn_get_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "pd_mpnn_set_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "pd_mpnn_loss_grad": (C.c_int, [_vp, C.POINTER(C.c_float), _dp, C.POINTER(C.c_float)]),
     "pd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "pd_get_kernel_timing": (C.c_int, [_vp, _dp, _i64p]),
 }

@@ -234,6 +234,47 @@ class Context:
         self._ok(self.L.pd_jacobian_block_diagonal(self.h, _d(u), _d(b)))
         return b.reshape(self.n, 3, 3)
 
+    # -- learned preconditioner ----------------------------------------------
+    def mpnn_init(self, seed=0, radius=None):
+        """Initialise the network on the subgraph of bonds shorter than radius."""
+        self._ok(self.L.pd_mpnn_init(self.h, int(seed), float(radius)))
+
+    def mpnn_collect(self, every):
+        self._ok(self.L.pd_mpnn_collect(self.h, int(every)))
+
+    def mpnn_num_pairs(self):
+        k = C.c_int64()
+        self._ok(self.L.pd_mpnn_num_pairs(self.h, C.byref(k)))
+        return k.value
+
+    def mpnn_train(self, epochs, learning_rate=1e-3, batch=8):
+        loss = C.c_double()
+        self._ok(self.L.pd_mpnn_train(self.h, int(epochs), float(learning_rate), int(batch), C.byref(loss)))
+        return loss.value
+
+    @staticmethod
+    def mpnn_num_params():
+        k = C.c_int64()
+        _lib.load().pd_mpnn_num_params(C.byref(k))
+        return k.value
+
+    def mpnn_weights(self):
+        w = np.zeros(self.mpnn_num_params(), dtype=np.float32)
+        self._ok(self.L.pd_mpnn_get_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
+        return w
+
+    def mpnn_set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._ok(self.L.pd_mpnn_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def mpnn_loss_grad(self, a, r, e):
+        pair = np.ascontiguousarray(np.concatenate([a, r, e]), dtype=np.float32)
+        loss = C.c_double()
+        g = np.zeros(self.mpnn_num_params(), dtype=np.float32)
+        self._ok(self.L.pd_mpnn_loss_grad(self.h, pair.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss),
+                                          g.ctypes.data_as(C.POINTER(C.c_float))))
+        return loss.value, g
+
     def kernel_timing(self, enable=True):
         self._ok(self.L.pd_set_kernel_timing(self.h, 1 if enable else 0))
 

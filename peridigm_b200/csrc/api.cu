@@ -210,6 +210,7 @@ int pd_destroy(pd_ctx* c) {
   cudaStreamSynchronize(c->stream);
   contact_release(c);
   qs_release(c);
+  mpnn_release(c);
   cudaStream_t s = c->stream;
   delete c;
   if (s) cudaStreamDestroy(s);
@@ -575,6 +576,60 @@ int pd_qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options*
     return fail(c, PD_ERR_ARG, "pd_qs_load_step: bad options");
   if (!c->state_init) TRY(pd_set_state(c, nullptr, nullptr));
   return qs_load_step(c, t_prev, t_cur, o, st);
+}
+
+int pd_mpnn_init(pd_ctx* c, uint64_t seed, double radius) {
+  CHECK_CTX(c);
+  if (!(radius > 0.0)) return fail(c, PD_ERR_ARG, "pd_mpnn_init: radius must be positive");
+  TRY(ensure_ready(c));
+  return mpnn_init(c, seed, radius);
+}
+
+int pd_mpnn_collect(pd_ctx* c, int32_t every) {
+  CHECK_CTX(c);
+  if (every < 0) return fail(c, PD_ERR_ARG, "pd_mpnn_collect: every must be >= 0");
+  return mpnn_set_capture(c, every);
+}
+
+int pd_mpnn_num_pairs(pd_ctx* c, int64_t* count) {
+  CHECK_CTX(c);
+  if (!count) return fail(c, PD_ERR_ARG, "null count");
+  *count = mpnn_num_pairs(c);
+  return PD_OK;
+}
+
+int pd_mpnn_train(pd_ctx* c, int32_t epochs, double learning_rate, int32_t batch, double* loss) {
+  CHECK_CTX(c);
+  if (epochs < 0 || !(learning_rate > 0.0) || batch <= 0) return fail(c, PD_ERR_ARG, "pd_mpnn_train: bad arguments");
+  TRY(ensure_device(c));
+  return mpnn_train(c, epochs, learning_rate, batch, loss);
+}
+
+int pd_mpnn_num_params(int64_t* count) {
+  if (!count) return PD_ERR_ARG;
+  *count = mpnn_num_params();
+  return PD_OK;
+}
+
+int pd_mpnn_get_weights(pd_ctx* c, float* w) {
+  CHECK_CTX(c);
+  if (!w) return fail(c, PD_ERR_ARG, "null weights");
+  TRY(ensure_device(c));
+  return mpnn_get_weights(c, w);
+}
+
+int pd_mpnn_set_weights(pd_ctx* c, const float* w) {
+  CHECK_CTX(c);
+  if (!w) return fail(c, PD_ERR_ARG, "null weights");
+  TRY(ensure_device(c));
+  return mpnn_set_weights(c, w);
+}
+
+int pd_mpnn_loss_grad(pd_ctx* c, const float* pair, double* loss, float* grad) {
+  CHECK_CTX(c);
+  if (!pair || !loss) return fail(c, PD_ERR_ARG, "null argument");
+  TRY(ensure_device(c));
+  return mpnn_loss_grad(c, pair, loss, grad);
 }
 
 int pd_jacobian_apply(pd_ctx* c, const double* u, const double* w, double* kw) {

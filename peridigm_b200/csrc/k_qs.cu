@@ -108,11 +108,12 @@ __global__ void k_qs_residual(int64_t n, const double* __restrict__ f, const dou
 
 // Sums (even slots) and maxima (odd slots) of kRedBlocks partial pairs, or
 // plain sums of `width` interleaved partials; fixed order.
-__global__ void k_qs_reduce(const double* __restrict__ partial, int width, int mode, double* __restrict__ out) {
+__global__ void k_qs_reduce(const double* __restrict__ partial, int nblk, int width, int mode,
+                            double* __restrict__ out) {
   __shared__ double s[kQsBlock];
   for (int c = 0; c < width; ++c) {
-    double a = (mode == 1 && c == 1) ? 0.0 : 0.0;
-    for (int b = threadIdx.x; b < kRedBlocks; b += blockDim.x) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
       const double v = partial[width * b + c];
       a = (mode == 1 && c == 1) ? fmax(a, v) : a + v;
     }
@@ -430,6 +431,8 @@ static int qs_alloc(pd_ctx* c) {
   return PD_OK;
 }
 
+const uint8_t* qs_fixed_mask(const pd_ctx* c) { return c->qs ? c->qs->fixed.p : nullptr; }
+
 void qs_release(pd_ctx* c) {
   delete c->qs;
   c->qs = nullptr;
@@ -442,7 +445,7 @@ static int qs_residual(pd_ctx* c, double* l2, double* linf) {
   k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, c->u.p, s->du.p, s->yq.p);
   PD_CUDA_TRY(c, launch_fp64_eval_at(c, s->yq.p, s->abq.p, s->th.p, s->nd.p, s->f.p));
   k_qs_residual<<<kRedBlocks, kQsBlock, 0, c->stream>>>(n, s->f.p, c->xv.p, s->fixed.p, s->r.p, s->partial.p);
-  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 2, 1, s->scal.p + 8);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 2, 1, s->scal.p + 8);
   PD_CUDA_TRY(c, cudaGetLastError());
   double h[2];
   PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -478,15 +481,99 @@ static int qs_tangent(pd_ctx* c) {
 
 // Preconditioned CG on K x = r (Belos BlockCG in the reference). Flexible
 // (Polak-Ribiere) beta when the preconditioner is not a fixed linear operator.
+__global__ void k_qs_true_residual(int64_t m, const double* __restrict__ b, const double* __restrict__ q,
+                                   double* __restrict__ r) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) r[k] = b[k] - q[k];
+}
+
+__global__ void k_qs_x_to_w(int64_t n, const double* __restrict__ x, double4* __restrict__ w) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  w[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0);
+}
+
+static void k_qs_pack_x(int64_t n, QsState* s, pd_ctx* c) {
+  k_qs_x_to_w<<<g1(n), kQsBlock, 0, c->stream>>>(n, s->x.p, s->w.p);
+}
+
+static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out,
+                     bool* stalled);
+
+// CG with the learned preconditioner first and block Jacobi as the fallback:
+// when the flexible iteration stalls, or when the true FP64 residual |b - K x|
+// (recomputed, not the recursive one) misses the tolerance, the solve restarts
+// from the current x with block Jacobi. The true residual is the judge.
 static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out) {
+  QsState* s = c->qs;
+  const int64_t m = 3 * c->n;
+  if (precond != PD_PRECOND_MPNN) {
+    bool stalled = false;
+    return qs_cg_run(c, precond, rel_tol, max_it, iters, rel_out, &stalled);
+  }
+  DBuf<double> b, x0;
+  PD_CUDA_TRY(c, b.alloc(m));
+  PD_CUDA_TRY(c, x0.alloc(m));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(b.p, s->r.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  bool stalled = false;
+  int its = 0;
+  double rel = 0.0;
+  int rc = qs_cg_run(c, PD_PRECOND_MPNN, rel_tol, max_it, &its, &rel, &stalled);
+  if (rc != PD_OK && rc != PD_ERR_NOT_CONVERGED && rc != PD_ERR_NONFINITE) return rc;
+  // true residual r = b - K x
+  const int64_t n = c->n;
+  k_qs_pack_x(n, s, c);
+  TRY_RC(qs_tangent(c));
+  k_qs_true_residual<<<g1(m), kQsBlock, 0, c->stream>>>(m, b.p, s->q.p, s->r.p);
+  k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->r.p, b.p, s->partial.p);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
+  double h[3];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, b.p, b.p, b.p, s->partial.p);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 12);
+  double hb[3];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(hb, s->scal.p + 12, sizeof(hb), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const double true_rel = hb[0] > 0 ? std::sqrt(h[0] / hb[0]) : 0.0;
+
+  if (std::isfinite(true_rel) && true_rel <= rel_tol && !stalled) {
+    *iters = its;
+    *rel_out = true_rel;
+    return PD_OK;
+  }
+  // fall back: block Jacobi on the remaining system K dx = b - K x (x kept when finite)
+  c->qs_fallbacks += 1;
+  if (!std::isfinite(true_rel)) {
+    PD_CUDA_TRY(c, cudaMemsetAsync(s->x.p, 0, m * sizeof(double), c->stream));
+    PD_CUDA_TRY(c, cudaMemcpyAsync(s->r.p, b.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  }
+  PD_CUDA_TRY(c, cudaMemcpyAsync(x0.p, s->x.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  // the remaining system is solved to the tolerance relative to |b|
+  const double tol2 = (std::isfinite(true_rel) && true_rel > 0) ? std::min(1.0, rel_tol / true_rel) : rel_tol;
+  int its2 = 0;
+  double rel2 = 0.0;
+  rc = qs_cg_run(c, PD_PRECOND_BLOCK_JACOBI, tol2, max_it, &its2, &rel2, &stalled);
+  k_qs_axpy<<<g1(m), kQsBlock, 0, c->stream>>>(m, 1.0, x0.p, s->x.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  *iters = its + its2;
+  *rel_out = rel2 * (std::isfinite(true_rel) && true_rel > 0 ? true_rel : 1.0);
+  return rc;
+}
+
+static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out,
+                     bool* stalled) {
   QsState* s = c->qs;
   const int64_t n = c->n, m = 3 * n;
   const bool flexible = precond == PD_PRECOND_MPNN;
+  const int every = (precond == PD_PRECOND_BLOCK_JACOBI) ? mpnn_capture_every(c) : 0;
+  double best = 1.0;
+  int best_it = 0;
+  *stalled = false;
   PD_CUDA_TRY(c, cudaMemsetAsync(s->x.p, 0, s->x.bytes(), c->stream));
   TRY_RC(qs_apply_precond(c, precond, s->r.p, s->z.p));
   // scal: [0] rz, [1] pq, [3] beta, [4] rr
   k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
-  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 8);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
   double h[3];
   PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -501,9 +588,10 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
   if (flexible) PD_CUDA_TRY(c, zold.alloc(m));
   double rel = 1.0;
   int it = 0;
+  if (every > 0) TRY_RC(mpnn_snapshot(c, s->r.p, s->x.p));
   while (it < max_it) {
     TRY_RC(qs_tangent(c));
-    k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 1, 0, s->scal.p + 8);
+    k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, (int)gt(n), 1, 0, s->scal.p + 8);
     k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 0);
     if (flexible) PD_CUDA_TRY(c, cudaMemcpyAsync(zold.p, s->z.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     k_qs_axpy2<<<g1(m), kQsBlock, 0, c->stream>>>(m, s->scal.p, s->w.p, s->q.p, s->x.p, s->r.p);
@@ -511,12 +599,12 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
     if (flexible) {
       // beta = z_new.(r_new - r_old)/rz_old = (z_new.r_new - z_new.r_old)/rz_old with r_old = r_new + alpha q
       k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
-      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 8);
+      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
       double hz[3], sc[2];
       PD_CUDA_TRY(c, cudaMemcpyAsync(hz, s->scal.p + 8, sizeof(hz), cudaMemcpyDeviceToHost, c->stream));
       PD_CUDA_TRY(c, cudaMemcpyAsync(sc, s->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
       k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->z.p, s->q.p, s->q.p, s->partial.p);
-      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 12);
+      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 12);
       double hq[3];
       PD_CUDA_TRY(c, cudaMemcpyAsync(hq, s->scal.p + 12, sizeof(hq), cudaMemcpyDeviceToHost, c->stream));
       PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -530,7 +618,7 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
       rel = std::sqrt(hz[2]) / r0;
     } else {
       k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
-      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, 3, 0, s->scal.p + 8);
+      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
       k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 1);
       double rr;
       PD_CUDA_TRY(c, cudaMemcpyAsync(&rr, s->scal.p + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -539,13 +627,26 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
     }
     ++it;
     if (!std::isfinite(rel)) {
+      if (every > 0) mpnn_drop_snapshots(c);
       c->err = "CG diverged (non-finite residual)";
       return PD_ERR_NONFINITE;
     }
     if (rel <= rel_tol) break;
+    if (every > 0 && it % every == 0) TRY_RC(mpnn_snapshot(c, s->r.p, s->x.p));
+    if (flexible) {  // stall: no 10x decrease of the residual over 60 iterations
+      if (rel < 0.1 * best) best = rel, best_it = it;
+      if (it - best_it > 60) {
+        *stalled = true;
+        break;
+      }
+    }
     k_qs_update_p<<<g1(n), kQsBlock, 0, c->stream>>>(n, s->scal.p, s->z.p, s->w.p, 0);
   }
   PD_CUDA_TRY(c, cudaGetLastError());
+  if (every > 0) {
+    if (rel <= rel_tol) TRY_RC(mpnn_commit_snapshots(c, s->x.p, s->dinv.p));
+    else mpnn_drop_snapshots(c);
+  }
   *iters = it;
   *rel_out = rel;
   return rel <= rel_tol ? PD_OK : PD_ERR_NOT_CONVERGED;
@@ -672,7 +773,6 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   // commit: u += du, v = du/dt (Peridigm.cpp:2858-2862); predictor for the next step
   k_qs_finish<<<g1(m), kQsBlock, 0, c->stream>>>(m, dt != 0.0 ? 1.0 / dt : 0.0, s->du.p, c->u.p, c->v.p);
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->pred.p, s->du.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  if (c->has_bc) PD_CUDA_TRY(c, cudaMemsetAsync(s->pred.p, 0, 0, c->stream));
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->f.p, s->f.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->theta.p, s->th.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   c->cur = 0;

@@ -164,6 +164,8 @@ struct pd_ctx {
   int64_t klaunches = 0;
   pdb::ContactState* contact = nullptr;
   pdb::QsState* qs = nullptr;
+  void* mpnn = nullptr;        // learned preconditioner state (k_mpnn.cu)
+  int64_t qs_fallbacks = 0;    // learned-preconditioner solves that fell back to block Jacobi
 };
 
 // ---------------------------------------------------------------------------
@@ -188,6 +190,19 @@ int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev);
 bool mpnn_ready(const pd_ctx* c);
 int mpnn_apply(pd_ctx* c, const double* r, double* z, const double* dinv);
 void mpnn_release(pd_ctx* c);
+int mpnn_init(pd_ctx* c, uint64_t seed, double radius);
+int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out);
+int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_host);
+int mpnn_set_capture(pd_ctx* c, int every);
+int mpnn_capture_every(const pd_ctx* c);
+int mpnn_snapshot(pd_ctx* c, const double* r, const double* x);
+int mpnn_commit_snapshots(pd_ctx* c, const double* x_final, const double* dinv);
+void mpnn_drop_snapshots(pd_ctx* c);
+int64_t mpnn_num_pairs(const pd_ctx* c);
+int mpnn_get_weights(pd_ctx* c, float* w);
+int mpnn_set_weights(pd_ctx* c, const float* w);
+int mpnn_num_params();
+const uint8_t* qs_fixed_mask(const pd_ctx* c);
 
 // bonds
 int build_bonds_device(pd_ctx* c, const pd_plane_filter* filters, int nf);
