@@ -732,13 +732,15 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   double l2, linf;
   TRY_RC(qs_residual(c, &l2, &linf));
   double metric = l2 + 20.0 * linf;
+  // negative tolerance: relative to this step's initial metric
+  const double newton_tol = o->newton_tolerance < 0.0 ? -o->newton_tolerance * metric : o->newton_tolerance;
   int newton = 0, cg_total = 0;
   double last_rel = 0.0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, c->stream);
-  while (metric > o->newton_tolerance && newton < o->max_newton_iterations) {
+  while (metric > newton_tol && newton < o->max_newton_iterations) {
     if (precond != PD_PRECOND_NONE) {
       k_qs_qm<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->pt.p, s->abq.p);
       k_qs_block_diag<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p,
@@ -786,7 +788,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
     st->device_ms += ms;
     st->bonds = c->nb;
   }
-  if (metric > o->newton_tolerance) {
+  if (metric > newton_tol) {
     c->err = "quasi-static Newton iteration did not reach its tolerance";
     return PD_ERR_NOT_CONVERGED;
   }

@@ -49,7 +49,7 @@ def test_mpnn_trains_and_helps_cg():
         tr.mpnn_collect(3)
         st = None
         for k in range(1, len(w["times"])):
-            st = tr.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=1e-9, cg_relative_tolerance=1e-8,
+            st = tr.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=-1e-8, cg_relative_tolerance=1e-8,
                                  preconditioner="block_jacobi", stats=st)
         assert tr.mpnn_num_pairs() > 20
         l1 = tr.mpnn_train(1, learning_rate=2e-3, batch=4)
@@ -67,7 +67,7 @@ def test_mpnn_trains_and_helps_cg():
                 ctx.mpnn_set_weights(weights)
             st = None
             for k in range(1, len(w2["times"])):
-                st = ctx.qs_load_step(w2["times"][k - 1], w2["times"][k], newton_tolerance=1e-9,
+                st = ctx.qs_load_step(w2["times"][k - 1], w2["times"][k], newton_tolerance=-1e-8,
                                       cg_relative_tolerance=1e-8, preconditioner=precond, stats=st)
             out[precond] = (ctx.field("Displacement"), st.cg_iterations)
     ub, ib = out["block_jacobi"]
