@@ -244,12 +244,14 @@ int pd_mpnn_init(pd_ctx* ctx, uint64_t seed, double radius);
  * pairs (r_k, x* - x_k) from every every-th iterate (K (x* - x_k) = r_k). */
 int pd_mpnn_collect(pd_ctx* ctx, int32_t every);
 int pd_mpnn_num_pairs(pd_ctx* ctx, int64_t* count);
-/* Adam on the stored pairs, loss |z - e|^2 / |e|^2, on the device. */
+/* Adam on the stored residuals, loss |K z - r|^2 / |r|^2 with K the tangent at
+ * the context's current displacement (rescaled to each residual's modulus). */
 int pd_mpnn_train(pd_ctx* ctx, int32_t epochs, double learning_rate, int32_t batch, double* loss);
 int pd_mpnn_num_params(int64_t* count);
 int pd_mpnn_get_weights(pd_ctx* ctx, float* weights);
 int pd_mpnn_set_weights(pd_ctx* ctx, const float* weights);
-/* Loss and parameter gradient of one pair (a = P_bj r, r, e; 9n floats), for checks. */
+/* Loss and parameter gradient for one residual (a = P_bj r, r; 6n floats) with
+ * the tangent at the current displacement, for gradient checks. */
 int pd_mpnn_loss_grad(pd_ctx* ctx, const float* pair, double* loss, float* grad);
 
 /* ---- instrumentation ----------------------------------------------------- */

@@ -267,8 +267,8 @@ class Context:
         w = np.ascontiguousarray(w, dtype=np.float32)
         self._ok(self.L.pd_mpnn_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
 
-    def mpnn_loss_grad(self, a, r, e):
-        pair = np.ascontiguousarray(np.concatenate([a, r, e]), dtype=np.float32)
+    def mpnn_loss_grad(self, a, r):
+        pair = np.ascontiguousarray(np.concatenate([a, r]), dtype=np.float32)
         loss = C.c_double()
         g = np.zeros(self.mpnn_num_params(), dtype=np.float32)
         self._ok(self.L.pd_mpnn_loss_grad(self.h, pair.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss),

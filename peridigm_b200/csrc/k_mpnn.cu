@@ -8,8 +8,9 @@
 //   h0 = relu(W0 f + b0)                         f = (a/s_a, r/s_r), 6 inputs
 //   h_l = h_{l-1} + relu(Ws_l h_{l-1} + Wn_l m_l + b_l),  m_l = mean_{j in N(i)} h_{l-1,j},  l = 1..3
 //   out = Wd h3 + bd                              3 outputs
-// Training: pairs (r_k, e_k) captured from block-Jacobi CG solves (e_k = x* - x_k
-// solves K e_k = r_k), loss |z - e|^2/|e|^2 per pair, Adam on FP32 master
+// Training: residuals r_k captured from block-Jacobi CG solves, loss
+// |K z - r|^2 / |r|^2 per residual (z approximates a local inverse of the
+// tangent, the part a 3-hop network can represent), Adam on FP32 master
 // weights; forward and backward are the kernels below, one warp per node,
 // gathers only (the transpose of the mean aggregation is a gather over the
 // symmetric subgraph), deterministic block reductions for weight gradients.
@@ -52,6 +53,7 @@ struct MpnnState {
   // training set: per pair a, r, e (float, 3n each)
   DBuf<float> pairs;
   int64_t npairs = 0, cap = 0;
+  std::vector<double> pair_k;  // bulk modulus at capture (the tangent scales with it)
   // capture from CG
   int every = 0;
   std::vector<DBuf<double>*> snap_r, snap_x;
@@ -248,37 +250,6 @@ __global__ void __launch_bounds__(256) k_mp_decode(int64_t n, const __nv_bfloat1
 // ---------------------------------------------------------------------------
 // Training: loss and backward
 // ---------------------------------------------------------------------------
-// out, z = a + s_a out, g = dL/dout = 2 s_a (z - e)/|e|^2 ; partial loss sums
-__global__ void __launch_bounds__(256) k_mp_loss(int64_t n, const __nv_bfloat16* __restrict__ h3,
-                                                 const __nv_bfloat16* __restrict__ wb, const float* __restrict__ a,
-                                                 const float* __restrict__ e, const double* __restrict__ dscal,
-                                                 double inv_e2, float* __restrict__ gout,
-                                                 double* __restrict__ partial) {
-  __shared__ double sl[8];
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  double l = 0.0;
-  if (i < n) {
-    const float2 hv = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(h3)[(int64_t)(H / 2) * i + lane]);
-    for (int c = 0; c < 3; ++c) {
-      float s = bf(wb[OFF_WD + c * H + 2 * lane]) * hv.x + bf(wb[OFF_WD + c * H + 2 * lane + 1]) * hv.y;
-      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-      const double out = (double)s + (double)bf(wb[OFF_BD + c]);
-      const double z = (double)a[3 * i + c] + dscal[0] * out;
-      const double d = z - (double)e[3 * i + c];
-      l += d * d * inv_e2;
-      if (lane == 0) gout[3 * i + c] = (float)(2.0 * dscal[0] * d * inv_e2);
-    }
-  }
-  if (lane == 0) sl[threadIdx.x >> 5] = l;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int k = 0; k < 8; ++k) s += sl[k];
-    partial[blockIdx.x] = s;
-  }
-}
-
 // dh3 = Wd^T g
 __global__ void __launch_bounds__(256) k_mp_decode_back(int64_t n, const __nv_bfloat16* __restrict__ wb,
                                                         const float* __restrict__ gout, float* __restrict__ dh) {
@@ -506,6 +477,17 @@ static int mp_alloc(pd_ctx* c, MpnnState* s, bool train) {
 
 static MpnnState* mp_state(pd_ctx* c) { return reinterpret_cast<MpnnState*>(c->mpnn); }
 
+// Bulk modulus of block 0 (or the median of a per-point field): the tangent of
+// a body with a fixed K/mu ratio scales with it.
+static double current_modulus(const pd_ctx* c) {
+  if (!c->field_K.empty()) {
+    std::vector<double> v(c->field_K);
+    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+    return v[v.size() / 2];
+  }
+  return c->block_K.empty() ? 1.0 : c->block_K[0];
+}
+
 int mpnn_init(pd_ctx* c, uint64_t seed, double radius) {
   if (!c->mpnn) c->mpnn = new MpnnState();
   MpnnState* s = mp_state(c);
@@ -586,44 +568,106 @@ int mpnn_apply(pd_ctx* c, const double* r, double* z, const double* dinv) {
   return PD_OK;
 }
 
-// One pair: forward with saved activations, loss, backward accumulating into s->g.
-static int mp_pair_grad(pd_ctx* c, MpnnState* s, const float* pair, double* loss) {
-  const int64_t n = c->n;
+// z = a + s_a (Wd h3 + bd) in FP64 from a float `a`; prescribed dofs zero.
+__global__ void __launch_bounds__(256) k_mp_zout(int64_t n, const __nv_bfloat16* __restrict__ h3,
+                                                 const __nv_bfloat16* __restrict__ wb, const float* __restrict__ a,
+                                                 double sa, const uint8_t* __restrict__ fixed,
+                                                 double* __restrict__ z) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const float2 hv = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(h3)[(int64_t)(H / 2) * i + lane]);
+  float o[3];
+  for (int c = 0; c < 3; ++c) {
+    float s = bf(wb[OFF_WD + c * H + 2 * lane]) * hv.x + bf(wb[OFF_WD + c * H + 2 * lane + 1]) * hv.y;
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    o[c] = s + bf(wb[OFF_BD + c]);
+  }
+  if (lane < 3) {
+    const uint8_t fx = fixed ? fixed[i] : 0;
+    z[3 * i + lane] = ((fx >> lane) & 1) ? 0.0 : (double)a[3 * i + lane] + sa * (double)o[lane];
+  }
+}
+
+// res = scale*q - r (prescribed dofs zero); partials of |res|^2 and |r|^2
+__global__ void k_mp_residual(int64_t m, double scale, const double* __restrict__ q, const float* __restrict__ r,
+                              const uint8_t* __restrict__ fixed, double* __restrict__ res,
+                              double* __restrict__ partial) {
+  __shared__ double s0[256], s1[256];
+  double a0 = 0.0, a1 = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+    const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
+    const double rk = fx ? 0.0 : (double)r[k];
+    const double v = fx ? 0.0 : scale * q[k] - rk;
+    res[k] = v;
+    a0 += v * v;
+    a1 += rk * rk;
+  }
+  s0[threadIdx.x] = a0;
+  s1[threadIdx.x] = a1;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) s0[threadIdx.x] += s0[threadIdx.x + o], s1[threadIdx.x] += s1[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[2 * blockIdx.x] = s0[0], partial[2 * blockIdx.x + 1] = s1[0];
+}
+
+// gout = coef * kres (prescribed dofs zero)
+__global__ void k_mp_gout(int64_t m, double coef, const double* __restrict__ kres, const uint8_t* __restrict__ fixed,
+                          float* __restrict__ gout) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
+  gout[k] = fx ? 0.f : (float)(coef * kres[k]);
+}
+
+// One pair (a = P_bj r, r as float [3n] each): forward with saved activations,
+// residual-space loss L = |kscale K z - r|^2 / |r|^2 with K the tangent prepared
+// by qs_prepare_current (kscale rescales it to the modulus of the pair), and
+// backward accumulating into s->g. dL/dz = 2 kscale K (kscale K z - r)/|r|^2.
+static int mp_pair_grad(pd_ctx* c, MpnnState* s, const float* pair, double kscale, double* loss) {
+  const int64_t n = c->n, m = 3 * n;
   const float* A = pair;
   const float* R = pair + 3 * n;
-  const float* E = pair + 6 * n;
-  DBuf<double> part, dscal;
-  PD_CUDA_TRY(c, part.alloc(2 * (size_t)std::max<unsigned>(kRed, gw(n))));
-  PD_CUDA_TRY(c, dscal.alloc(2));
-  // norms of a, r and e (FP64 host side for the loss scale)
-  std::vector<float> he(3 * n);
-  PD_CUDA_TRY(c, cudaMemcpyAsync(he.data(), E, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-  std::vector<float> ha(3 * n), hr(3 * n);
-  PD_CUDA_TRY(c, cudaMemcpyAsync(ha.data(), A, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-  PD_CUDA_TRY(c, cudaMemcpyAsync(hr.data(), R, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  const uint8_t* fixed = qs_fixed_mask(c);
+  DBuf<double> part, z, kz, res, kres;
+  PD_CUDA_TRY(c, part.alloc(2 * kRed));
+  PD_CUDA_TRY(c, z.alloc(m));
+  PD_CUDA_TRY(c, kz.alloc(m));
+  PD_CUDA_TRY(c, res.alloc(m));
+  PD_CUDA_TRY(c, kres.alloc(m));
+  std::vector<float> ha(m), hr(m);
+  PD_CUDA_TRY(c, cudaMemcpyAsync(ha.data(), A, m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(hr.data(), R, m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  double e2 = 0.0, a2 = 0.0, r2 = 0.0;
-  for (int64_t k = 0; k < 3 * n; ++k) e2 += (double)he[k] * he[k], a2 += (double)ha[k] * ha[k], r2 += (double)hr[k] * hr[k];
-  const double sa = std::sqrt(a2 / (3.0 * n)), sr = std::sqrt(r2 / (3.0 * n));
+  double a2 = 0.0, r2 = 0.0;
+  for (int64_t k = 0; k < m; ++k) a2 += (double)ha[k] * ha[k], r2 += (double)hr[k] * hr[k];
+  const double sa = std::sqrt(a2 / (double)m), sr = std::sqrt(r2 / (double)m);
   const float hs[2] = {(float)(sa > 0 ? 1.0 / sa : 0.0), (float)(sr > 0 ? 1.0 / sr : 0.0)};
-  const double hd[2] = {sa, sr};
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->scal.p, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
-  PD_CUDA_TRY(c, cudaMemcpyAsync(dscal.p, hd, sizeof(hd), cudaMemcpyHostToDevice, c->stream));
   k_mp_features<float><<<g1(n), 256, 0, c->stream>>>(n, A, R, s->scal.p, s->feat.p);
   k_mp_encode<<<gw(n), 256, 0, c->stream>>>(n, s->feat.p, s->wb.p, s->pre[0].p, s->h[0].p);
   TRY_RC(mp_forward_layers(c, s, true));
-  const unsigned gblk = gw(n);
-  k_mp_loss<<<gblk, 256, 0, c->stream>>>(n, s->h[NL].p, s->wb.p, A, E, dscal.p, e2 > 0 ? 1.0 / e2 : 0.0, s->gout.p,
-                                         part.p);
-  std::vector<double> hl(gblk);
-  PD_CUDA_TRY(c, cudaMemcpyAsync(hl.data(), part.p, gblk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  k_mp_zout<<<gw(n), 256, 0, c->stream>>>(n, s->h[NL].p, s->wb.p, A, sa, fixed, z.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  TRY_RC(qs_apply_K(c, z.p, kz.p));
+  k_mp_residual<<<kRed, 256, 0, c->stream>>>(m, kscale, kz.p, R, fixed, res.p, part.p);
+  TRY_RC(qs_apply_K(c, res.p, kres.p));
+  std::vector<double> hp(2 * kRed);
+  PD_CUDA_TRY(c, cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  double rs2 = 0.0, rr2 = 0.0;
+  for (int b = 0; b < kRed; ++b) rs2 += hp[2 * b], rr2 += hp[2 * b + 1];
+  const double inv_r2 = rr2 > 0 ? 1.0 / rr2 : 0.0;
+  // dL/dout = s_a dL/dz
+  k_mp_gout<<<g1(m), 256, 0, c->stream>>>(m, 2.0 * kscale * inv_r2 * sa, kres.p, fixed, s->gout.p);
   // backward
   k_mp_dec_wgrad<<<1, 3 * H + 3, 0, c->stream>>>(n, s->gout.p, s->h[NL].p, s->g.p);
   k_mp_decode_back<<<gw(n), 256, 0, c->stream>>>(n, s->wb.p, s->gout.p, s->dh.p);
   for (int l = NL - 1; l >= 0; --l) {
     const __nv_bfloat16* wl = s->wb.p + OFF_L + l * LSZ;
     k_mp_layer_back<<<gw(n), 256, 0, c->stream>>>(n, s->mrow.p, wl, s->pre[l + 1].p, s->dh.p, s->dhs.p, s->dm.p);
-    // weight gradients of layer l: dpre (in dh) x h_{l} and x m_l
     k_mp_wgrad<__nv_bfloat16><<<kRed, 256, 0, c->stream>>>(n, H, s->dh.p, s->h[l].p, s->gpart.p);
     k_mp_wgrad_reduce<<<17, 256, 0, c->stream>>>(kRed, H, s->gpart.p, s->g.p, OFF_L + l * LSZ, OFF_L + l * LSZ + 2 * H * H);
     k_mp_wgrad<float><<<kRed, 256, 0, c->stream>>>(n, H, s->dh.p, s->m[l].p, s->gpart.p);
@@ -636,9 +680,7 @@ static int mp_pair_grad(pd_ctx* c, MpnnState* s, const float* pair, double* loss
   k_mp_wgrad_reduce<<<2, 256, 0, c->stream>>>(kRed, F, s->gpart.p, s->g.p, OFF_W0, OFF_B0);
   PD_CUDA_TRY(c, cudaGetLastError());
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  double L = 0.0;
-  for (unsigned b = 0; b < gblk; ++b) L += hl[b];
-  *loss = L;
+  *loss = rs2 * inv_r2;
   return PD_OK;
 }
 
@@ -649,11 +691,12 @@ int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_
     return PD_ERR_STATE;
   }
   TRY_RC(mp_alloc(c, s, true));
+  TRY_RC(qs_prepare_current(c));
   DBuf<float> pair;
-  PD_CUDA_TRY(c, pair.alloc(9 * c->n));
-  PD_CUDA_TRY(c, cudaMemcpy(pair.p, pair_host, 9 * c->n * sizeof(float), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, pair.alloc(6 * c->n));
+  PD_CUDA_TRY(c, cudaMemcpy(pair.p, pair_host, 6 * c->n * sizeof(float), cudaMemcpyHostToDevice));
   PD_CUDA_TRY(c, cudaMemsetAsync(s->g.p, 0, NPARAM * sizeof(float), c->stream));
-  TRY_RC(mp_pair_grad(c, s, pair.p, loss));
+  TRY_RC(mp_pair_grad(c, s, pair.p, 1.0, loss));
   if (grad_host) PD_CUDA_TRY(c, cudaMemcpy(grad_host, s->g.p, NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
   return PD_OK;
 }
@@ -669,7 +712,9 @@ int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {
     return PD_ERR_STATE;
   }
   TRY_RC(mp_alloc(c, s, true));
+  TRY_RC(qs_prepare_current(c));
   const int64_t n = c->n;
+  const double k_now = current_modulus(c);
   std::mt19937_64 rng(12345 + s->adam_t);
   std::vector<int64_t> order(s->npairs);
   double last = 0.0;
@@ -683,7 +728,7 @@ int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {
       const int64_t b1 = std::min<int64_t>(s->npairs, b0 + batch);
       for (int64_t q = b0; q < b1; ++q) {
         double l = 0.0;
-        TRY_RC(mp_pair_grad(c, s, s->pairs.p + (size_t)order[q] * 9 * n, &l));
+        TRY_RC(mp_pair_grad(c, s, s->pairs.p + (size_t)order[q] * 9 * n, s->pair_k[order[q]] / k_now, &l));
         acc += l;
         ++cnt;
       }
@@ -754,6 +799,7 @@ int mpnn_commit_snapshots(pd_ctx* c, const double* x_final, const double* dinv) 
                                                  s->pairs.p + per * (s->npairs + k));
   }
   PD_CUDA_TRY(c, cudaGetLastError());
+  for (int k = 0; k < s->nsnap; ++k) s->pair_k.push_back(current_modulus(c));
   s->npairs += s->nsnap;
   s->nsnap = 0;
   return PD_OK;

@@ -707,6 +707,20 @@ int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev) {
   return PD_OK;
 }
 
+// Tangent at the context's current displacement, for repeated products.
+int qs_prepare_current(pd_ctx* c) { return qs_prepare_at(c, c->u.p); }
+
+// kw = K w with the tangent prepared by qs_prepare_current.
+int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_pack_w<<<g1(n), kQsBlock, 0, c->stream>>>(n, w_dev, s->fixed.p, s->w.p);
+  TRY_RC(qs_tangent(c));
+  k_qs_fixed_rows<<<g1(n), kQsBlock, 0, c->stream>>>(n, w_dev, s->fixed.p, s->q.p);
+  PD_CUDA_TRY(c, cudaMemcpyAsync(kw_dev, s->q.p, 3 * n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  return PD_OK;
+}
+
 int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {
   TRY_RC(ensure_ready_internal(c));
   TRY_RC(qs_alloc(c));

@@ -187,6 +187,8 @@ int ensure_ready_internal(pd_ctx* c);
 int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st);
 int qs_tangent_apply(pd_ctx* c, const double* u_dev, const double* w_dev, double* kw_dev);
 int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev);
+int qs_prepare_current(pd_ctx* c);
+int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev);
 bool mpnn_ready(const pd_ctx* c);
 int mpnn_apply(pd_ctx* c, const double* r, double* z, const double* dinv);
 void mpnn_release(pd_ctx* c);

@@ -1,7 +1,8 @@
 """GPU learned CG preconditioner: gradients against the CPU oracle, training on
 solver-generated pairs, and its effect inside the quasi-static CG.
 
-* pd_mpnn_loss_grad vs oracle/mpnn.py on the same BF16 weights: loss to 1e-4
+* pd_mpnn_loss_grad (residual-space loss |K z - r|^2/|r|^2) vs oracle/mpnn.py
+  with the oracle's dense tangent, on the same BF16 weights: loss to 1e-4
   relative, gradient to 2e-2 relative L2 (FP32 vs FP64 sums and BF16 rounding
   of stored activations);
 * block-Jacobi QS solves with capture produce pairs, training lowers the loss;
@@ -12,6 +13,7 @@ import numpy as np
 import pytest
 
 from oracle import mpnn as M
+from oracle import oracle as O
 from peridigm_b200 import Context, workloads
 
 pytestmark = pytest.mark.gpu
@@ -26,17 +28,22 @@ def _cube(n, seed):
 
 def test_mpnn_gradient_matches_oracle():
     w, ctx = _cube(5, 1)
+    dofs = sorted({3 * int(p) + b["coordinate"] for b in w["bcs"] for p in b["points"]})
     with ctx:
         ctx.mpnn_init(seed=3, radius=1.5e-3)
+        row, col = ctx.bonds_csr()
+        K = O.tangent_dense(w["x"], w["x"], w["vol"], row, col, w["K"], w["mu"], w["horizon"], dofs)
         rng = np.random.default_rng(0)
         wts = (rng.standard_normal(M.NPARAM) * 0.15).astype(np.float32)
         ctx.mpnn_set_weights(wts)
         n = len(w["vol"])
-        a, r, e = (rng.standard_normal(3 * n).astype(np.float32) for _ in range(3))
-        L, g = ctx.mpnn_loss_grad(a, r, e)
-        row, col = ctx.bonds_csr()
+        # a residual of the cube's own tangent and a first guess of its scale
+        e = rng.standard_normal(3 * n) * 1e-6
+        r = (K @ e).astype(np.float32)
+        a = (e * (1.0 + 0.3 * rng.standard_normal(3 * n))).astype(np.float32)
+        L, g = ctx.mpnn_loss_grad(a, r)
     mrow, mcol = M.subgraph(w["x"], row, col, 1.5e-3)
-    Lr, gr = M.loss_grad(wts, a, r, e, mrow, mcol)
+    Lr, gr = M.loss_grad_residual(wts, a, r, K, dofs, mrow, mcol)
     assert abs(L - Lr) <= 1e-4 * abs(Lr)
     assert np.linalg.norm(g - gr) <= 2e-2 * np.linalg.norm(gr)
 
