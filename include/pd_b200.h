@@ -97,6 +97,7 @@ typedef struct {
   int64_t newton_iterations;
   int64_t cg_iterations;
   double final_residual;  /* relative FP64 residual of the last linear solve */
+  int64_t preconditioner_fallbacks; /* learned-preconditioner solves finished by block Jacobi */
 } pd_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */

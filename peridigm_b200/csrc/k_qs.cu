@@ -750,6 +750,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   const double newton_tol = o->newton_tolerance < 0.0 ? -o->newton_tolerance * metric : o->newton_tolerance;
   int newton = 0, cg_total = 0;
   double last_rel = 0.0;
+  const int64_t fallbacks0 = c->qs_fallbacks;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -799,6 +800,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
     st->newton_iterations += newton;
     st->cg_iterations += cg_total;
     st->final_residual = last_rel;
+    st->preconditioner_fallbacks += c->qs_fallbacks - fallbacks0;
     st->device_ms += ms;
     st->bonds = c->nb;
   }
