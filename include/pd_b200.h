@@ -183,6 +183,25 @@ int pd_contact_force(pd_ctx* ctx, const double* y, const double* v, double* fc_o
 /* ---- explicit integration ----------------------------------------------- */
 /* ComputeCriticalTimeStep (src/core/Peridigm_CriticalTimeStep.cpp:52-130), min over points. */
 int pd_critical_time_step(pd_ctx* ctx, double* dt_out);
+/* The same critical time step, computed with no device allocation. No
+ * counterpart in the reference: it exists for callers that cannot allocate
+ * device memory around the call. pd_critical_time_step allocates and frees a
+ * small device buffer on each call; a host whose pool allocator has reserved
+ * the device's memory sees that allocation fail, and the free synchronises the
+ * whole device, stalling the host's other streams inside its time loop. Here
+ * the block minima live in a static 512 KiB device array (65,536 doubles) in
+ * the library, so:
+ *  - the context must already be set up (bonds, material, and one
+ *    pd_weighted_volume or evaluation done), else PD_ERR_STATE;
+ *  - at most 65,536 blocks of 256 threads: 1,048,576 points at the default 16
+ *    lanes per point; larger contexts get PD_ERR_ARG (use pd_critical_time_step);
+ *  - nothing needs to start at zero: each call writes every partial it reads;
+ *  - the array is shared by all contexts on a device, so calls that overlap on
+ *    one device (from two threads) race and must be serialised by the caller;
+ *  - the first call on each device resolves the array's address and may load
+ *    the library's module there: make it before any stream capture begins.
+ * The result is copied to the host double *dt_out after a stream synchronise. */
+int pd_critical_time_step_static(pd_ctx* ctx, double* dt_out);
 /* Initial displacement / velocity (DirichletBC "Initial Displacement"/"Initial Velocity",
  * src/core/Peridigm_BoundaryCondition.cpp:157-187). NULL leaves the field unchanged. */
 int pd_set_state(pd_ctx* ctx, const double* u, const double* v);

@@ -96,6 +96,7 @@ SIGNATURES = {
     "pd_update_state": (C.c_int, [_vp]),
     "pd_set_bond_damage": (C.c_int, [_vp, _dp]),
     "pd_critical_time_step": (C.c_int, [_vp, _dp]),
+    "pd_critical_time_step_static": (C.c_int, [_vp, _dp]),
     "pd_set_state": (C.c_int, [_vp, _dp, _dp]),
     "pd_add_prescribed_displacement": (C.c_int, [_vp, C.c_int64, _i64p, C.c_int32, C.c_double, C.c_double]),
     "pd_clear_boundary_conditions": (C.c_int, [_vp]),

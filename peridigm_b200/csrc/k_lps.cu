@@ -718,6 +718,15 @@ cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out_dev) {
   return cudaGetLastError();
 }
 
+int64_t critical_dt_partials(const pd_ctx* c) { return (int64_t)grid_for(c->n, c->tpo); }
+
+cudaError_t launch_critical_dt_into(pd_ctx* c, double* partial, double* dt_out_dev) {
+  const unsigned grid = grid_for(c->n, c->tpo);
+  PD_DISPATCH_TPO(c->tpo, k_critical_dt, grid, c->n, c->row.p, c->col.p, c->xv.p, c->pt.p, c->hp.p, partial);
+  k_min_reduce<<<1, kBlock, 0, c->stream>>>((int64_t)grid, partial, dt_out_dev);
+  return cudaGetLastError();
+}
+
 }  // namespace pdb
 
 namespace pdb {

@@ -179,6 +179,10 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg);
 cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev);
 cudaError_t launch_sync_state(pd_ctx* c);
 cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out);
+// The critical-dt kernels with the block partials in caller memory: partial
+// must hold critical_dt_partials(c) doubles; nothing is allocated.
+int64_t critical_dt_partials(const pd_ctx* c);
+cudaError_t launch_critical_dt_into(pd_ctx* c, double* partial, double* dt_out_dev);
 cudaError_t collect_kernel_times(pd_ctx* c);
 cudaError_t launch_fp64_eval_at(pd_ctx* c, const double4* y4, double4* ab, double* theta, double* nd, double* f_out);
 int ensure_ready_internal(pd_ctx* c);
