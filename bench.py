@@ -31,18 +31,27 @@ UNIT = "bond evals/s"
 
 
 def algorithmic_bytes(nb, n, precision="split"):
-    """Bytes each bond pass must move at minimum with this layout (one launch).
+    """Bytes each bond pass must move at minimum with this layout (one launch),
+    every per-point record counted once (ideal reuse of gathered neighbors).
 
-    Per bond, both passes: col (4 B) + bond damage (1 B).
-    Per point, dilatation pass: row 8, xv 32, state 24, m 8, owner coefficients 8,
-    s_c 8, horizon 8, writes A/B 8, theta 8, node damage 8  -> 120 B.
-    Per point, force pass: row 8, xv 32, state 32, rho 8, horizon 8, v read+write 48,
-    next state 24, acceleration 24, BC mask 1 -> 185 B.
-    FP64 path: the gathered owner terms are FP64 (ab64, 32 B/point read in the
-    force pass, written in the dilatation pass)."""
+    Split-FP32, per bond, both passes: col 4 + bond damage 1 + bond vector
+    record (X in FP32, omega*V_j) 16 = 21 B.
+    Per point, dilatation pass: row 8, owner terms 16, displacement record 32,
+    writes A/B 8, theta 8, node damage 8 -> 80 B.
+    Per point, force pass: row 8, displacement record 32, rho 8, v read+write 48,
+    acceleration 24, u read+write 48, next displacement record 24, BC mask 1 -> 193 B.
+    FP64 path (no bond records): per bond col 4 + damage 1; per point the
+    gathered FP64 coordinates, material and owner terms (144 B / 217 B)."""
     if precision == "split":
-        return {"dilatation": 5 * nb + 120 * n, "force": 5 * nb + 185 * n}
+        return {"dilatation": 21 * nb + 80 * n, "force": 21 * nb + 193 * n}
     return {"dilatation": 5 * nb + 144 * n, "force": 5 * nb + 217 * n}
+
+
+# DRAM bytes (read + write) per launch of the split bond passes on this
+# workload, from one ncu capture (--set full, step 1 of the notched plate):
+# k_dilatation_split<4> 566.3 MB read + 5.7 MB written, k_force_split<4>
+# 633.1 MB read + 8.3 MB written.
+NCU_TRAFFIC = {"dilatation": 572.0e6, "force": 641.4e6}
 
 
 class ClockSampler:
@@ -214,12 +223,7 @@ def main():
     except (OSError, KeyError, ValueError):
         hbm, peak_src = 6650.0, "fallback"
     achieved = algo[dom] / (per[dom] / 1e3) / 1e9
-    traffic = None
-    try:
-        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        traffic = tr.get("split", {}).get(dom)
-    except (OSError, ValueError):
-        pass
+    traffic = NCU_TRAFFIC[dom]
     roofline = {"bound": "hbm", "kernel": f"k_{dom}_split", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic,
                 "algorithmic_bytes": algo[dom], "launch_ms": per[dom],
@@ -277,7 +281,7 @@ def main():
             "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
             "config": {"workload": "notched_plate_400x200x4", "points": n, "bonds": nb, "horizon_over_h": 3.015,
                        "critical_stretch": 5e-4, "dt": dt, "precision": "split_fp32",
-                       "l2": "inputs larger than L2 (about 220 MB touched per step vs 126 MB L2)",
+                       "l2": "inputs larger than L2 (about 1.2 GB read per step vs 126 MB L2)",
                        "parallelism": f"replicas x{world}"},
             "fp64": {"value": value64, "unit": UNIT, "steps": fsteps, "ms_per_step": ms64 / fsteps,
                      "split_over_fp64": value / value64},

@@ -54,12 +54,12 @@ int upload_material(pd_ctx* c) {
   PD_CUDA_TRY(c, c->pt.alloc(n));
   PD_CUDA_TRY(c, c->sc.alloc(n));
   if (c->precision == PD_SPLIT_FP32) {
-    PD_CUDA_TRY(c, c->xr.alloc(n));
+    PD_CUDA_TRY(c, c->bx.alloc((size_t)c->nb));
     PD_CUDA_TRY(c, c->own.alloc(n));
   }
-  PD_CUDA_TRY(c, cudaMemcpy(c->pt.p, pt.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-  PD_CUDA_TRY(c, cudaMemcpy(c->sc.p, sc.data(), n * sizeof(double), cudaMemcpyHostToDevice));
-  PD_CUDA_TRY(c, cudaMemcpy(c->hp.p, hp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, c->pt.p, pt.data(), n * sizeof(double4)));
+  PD_CUDA_TRY(c, h2d(c, c->sc.p, sc.data(), n * sizeof(double)));
+  PD_CUDA_TRY(c, h2d(c, c->hp.p, hp.data(), n * sizeof(double)));
   return PD_OK;
 }
 
@@ -67,7 +67,7 @@ int upload_horizons(pd_ctx* c) {
   std::vector<double> hp(c->n);
   for (int64_t i = 0; i < c->n; ++i) hp[i] = c->block_h[c->hblock.empty() ? 0 : c->hblock[i]];
   PD_CUDA_TRY(c, c->hp.alloc(c->n));
-  PD_CUDA_TRY(c, cudaMemcpy(c->hp.p, hp.data(), c->n * sizeof(double), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, c->hp.p, hp.data(), c->n * sizeof(double)));
   return PD_OK;
 }
 
@@ -77,10 +77,10 @@ int alloc_state(pd_ctx* c) {
   for (int k = 0; k < 2; ++k) {
     if (c->precision == PD_SPLIT_FP32) {
       PD_CUDA_TRY(c, c->ur[k].alloc(n));
-      PD_CUDA_TRY(c, cudaMemset(c->ur[k].p, 0, c->ur[k].bytes()));
+      PD_CUDA_TRY(c, dzero(c, c->ur[k].p, c->ur[k].bytes()));
     } else {
       PD_CUDA_TRY(c, c->st[k].alloc(n));
-      PD_CUDA_TRY(c, cudaMemset(c->st[k].p, 0, c->st[k].bytes()));
+      PD_CUDA_TRY(c, dzero(c, c->st[k].p, c->st[k].bytes()));
     }
   }
   PD_CUDA_TRY(c, c->ab64.alloc(c->precision == PD_FP64 ? n : 1));
@@ -92,7 +92,7 @@ int alloc_state(pd_ctx* c) {
   PD_CUDA_TRY(c, c->theta.alloc(n));
   PD_CUDA_TRY(c, c->node_damage.alloc(n));
   for (auto* b : {&c->u, &c->v, &c->a, &c->f, &c->fc, &c->theta, &c->node_damage})
-    PD_CUDA_TRY(c, cudaMemset(b->p, 0, b->bytes()));
+    PD_CUDA_TRY(c, dzero(c, b->p, b->bytes()));
   c->cur = 0;
   c->state_init = false;
   return PD_OK;
@@ -123,9 +123,9 @@ int ensure_ready(pd_ctx* c) {
       PD_CUDA_TRY(c, c->bc_mask.alloc(n));
       PD_CUDA_TRY(c, c->bc_a.alloc(3 * n));
       PD_CUDA_TRY(c, c->bc_b.alloc(3 * n));
-      PD_CUDA_TRY(c, cudaMemcpy(c->bc_mask.p, c->h_bc_mask.data(), n, cudaMemcpyHostToDevice));
-      PD_CUDA_TRY(c, cudaMemcpy(c->bc_a.p, c->h_bc_a.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
-      PD_CUDA_TRY(c, cudaMemcpy(c->bc_b.p, c->h_bc_b.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+      PD_CUDA_TRY(c, h2d(c, c->bc_mask.p, c->h_bc_mask.data(), n));
+      PD_CUDA_TRY(c, h2d(c, c->bc_a.p, c->h_bc_a.data(), 3 * n * sizeof(double)));
+      PD_CUDA_TRY(c, h2d(c, c->bc_b.p, c->h_bc_b.data(), 3 * n * sizeof(double)));
     }
     c->bc_dirty = false;
   }
@@ -191,7 +191,7 @@ int pd_create(const pd_config* cfg, pd_ctx** out) {
     return PD_ERR_CUDA;
   }
   if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      c->status.alloc(1) != cudaSuccess || cudaMemset(c->status.p, 0, sizeof(int)) != cudaSuccess) {
+      c->status.alloc(1) != cudaSuccess || dzero(c, c->status.p, sizeof(int)) != cudaSuccess) {
     delete c;
     return PD_ERR_CUDA;
   }
@@ -243,7 +243,7 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   std::vector<double4> xv(n);
   for (int64_t i = 0; i < n; ++i) xv[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], vol[i]);
   PD_CUDA_TRY(c, c->xv.alloc(n));
-  PD_CUDA_TRY(c, cudaMemcpy(c->xv.p, xv.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, c->xv.p, xv.data(), n * sizeof(double4)));
   c->row.release();
   c->col.release();
   c->nb = 0;
@@ -320,8 +320,8 @@ int pd_set_bonds(pd_ctx* c, const int32_t* nl, int64_t len) {
   c->nb = (int64_t)col.size();
   PD_CUDA_TRY(c, c->row.alloc(c->n + 1));
   PD_CUDA_TRY(c, c->col.alloc(std::max<int64_t>(c->nb, 1)));
-  PD_CUDA_TRY(c, cudaMemcpy(c->row.p, row.data(), (c->n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
-  if (c->nb) PD_CUDA_TRY(c, cudaMemcpy(c->col.p, col.data(), c->nb * sizeof(int32_t), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, c->row.p, row.data(), (c->n + 1) * sizeof(int64_t)));
+  if (c->nb) PD_CUDA_TRY(c, h2d(c, c->col.p, col.data(), c->nb * sizeof(int32_t)));
   if (c->hp.count < (size_t)c->n) TRY(upload_horizons(c));
   TRY(finalize_bonds(c, false));
   c->wv_done = false;
@@ -343,8 +343,8 @@ int pd_get_bonds(pd_ctx* c, int32_t* nl, int64_t cap, int64_t* len) {
   TRY(ensure_device(c));
   std::vector<int64_t> row(c->n + 1);
   std::vector<int32_t> col(std::max<int64_t>(c->nb, 1));
-  PD_CUDA_TRY(c, cudaMemcpy(row.data(), c->row.p, (c->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
-  if (c->nb) PD_CUDA_TRY(c, cudaMemcpy(col.data(), c->col.p, c->nb * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (c->n + 1) * sizeof(int64_t)));
+  if (c->nb) PD_CUDA_TRY(c, d2h(c, col.data(), c->col.p, c->nb * sizeof(int32_t)));
   int64_t k = 0;
   for (int64_t i = 0; i < c->n; ++i) {
     nl[k++] = (int32_t)(row[i + 1] - row[i]);
@@ -397,7 +397,7 @@ int pd_weighted_volume(pd_ctx* c, double* m_out) {
   TRY(ensure_ready(c));
   if (m_out) {
     std::vector<double4> pt(c->n);
-    PD_CUDA_TRY(c, cudaMemcpy(pt.data(), c->pt.p, c->n * sizeof(double4), cudaMemcpyDeviceToHost));
+    PD_CUDA_TRY(c, d2h(c, pt.data(), c->pt.p, c->n * sizeof(double4)));
     for (int64_t i = 0; i < c->n; ++i) m_out[i] = pt[i].x;
   }
   return PD_OK;
@@ -450,7 +450,7 @@ int pd_set_bond_damage(pd_ctx* c, const double* bd) {
     else return fail(c, PD_ERR_UNSUPPORTED, "bond damage must be 0 or 1 (critical-stretch values)");
   }
   TRY(ensure_device(c));
-  PD_CUDA_TRY(c, cudaMemcpy(c->dmg.p, h.data(), (size_t)c->nb, cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, c->dmg.p, h.data(), (size_t)c->nb));
   c->trial_valid = false;
   return PD_OK;
 }
@@ -471,10 +471,10 @@ int pd_set_state(pd_ctx* c, const double* u, const double* v) {
   CHECK_CTX(c);
   TRY(ensure_ready(c));
   const size_t bytes = 3 * (size_t)c->n * sizeof(double);
-  if (u) PD_CUDA_TRY(c, cudaMemcpy(c->u.p, u, bytes, cudaMemcpyHostToDevice));
-  else if (!c->state_init) PD_CUDA_TRY(c, cudaMemset(c->u.p, 0, bytes));
-  if (v) PD_CUDA_TRY(c, cudaMemcpy(c->v.p, v, bytes, cudaMemcpyHostToDevice));
-  else if (!c->state_init) PD_CUDA_TRY(c, cudaMemset(c->v.p, 0, bytes));
+  if (u) PD_CUDA_TRY(c, h2d(c, c->u.p, u, bytes));
+  else if (!c->state_init) PD_CUDA_TRY(c, dzero(c, c->u.p, bytes));
+  if (v) PD_CUDA_TRY(c, h2d(c, c->v.p, v, bytes));
+  else if (!c->state_init) PD_CUDA_TRY(c, dzero(c, c->v.p, bytes));
   if (u || !c->state_init) {
     c->cur = 0;
     PD_CUDA_TRY(c, launch_sync_state(c));
@@ -559,7 +559,7 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
     stats->bonds = c->nb;
     stats->device_ms = ms;
     std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
-    PD_CUDA_TRY(c, cudaMemcpy(h.data(), c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToHost));
+    PD_CUDA_TRY(c, d2h(c, h.data(), c->dmg.p, (size_t)c->nb));
     int64_t br = 0;
     for (int64_t b = 0; b < c->nb; ++b) br += h[b];
     stats->broken_bonds = br;
@@ -720,32 +720,32 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
   switch (field) {
     case PD_FIELD_DISPLACEMENT:
     case PD_FIELD_COORDINATES: {
-      PD_CUDA_TRY(c, cudaMemcpy(out, c->u.p, b3, cudaMemcpyDeviceToHost));
+      PD_CUDA_TRY(c, d2h(c, out, c->u.p, b3));
       if (field == PD_FIELD_COORDINATES)
         for (int64_t k = 0; k < 3 * n; ++k) out[k] = c->hx[k] + out[k];
       return PD_OK;
     }
-    case PD_FIELD_VELOCITY: PD_CUDA_TRY(c, cudaMemcpy(out, c->v.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
-    case PD_FIELD_ACCELERATION: PD_CUDA_TRY(c, cudaMemcpy(out, c->a.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
-    case PD_FIELD_FORCE_DENSITY: PD_CUDA_TRY(c, cudaMemcpy(out, c->f.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
-    case PD_FIELD_CONTACT_FORCE: PD_CUDA_TRY(c, cudaMemcpy(out, c->fc.p, b3, cudaMemcpyDeviceToHost)); return PD_OK;
+    case PD_FIELD_VELOCITY: PD_CUDA_TRY(c, d2h(c, out, c->v.p, b3)); return PD_OK;
+    case PD_FIELD_ACCELERATION: PD_CUDA_TRY(c, d2h(c, out, c->a.p, b3)); return PD_OK;
+    case PD_FIELD_FORCE_DENSITY: PD_CUDA_TRY(c, d2h(c, out, c->f.p, b3)); return PD_OK;
+    case PD_FIELD_CONTACT_FORCE: PD_CUDA_TRY(c, d2h(c, out, c->fc.p, b3)); return PD_OK;
     case PD_FIELD_DILATATION:
-      PD_CUDA_TRY(c, cudaMemcpy(out, c->theta.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+      PD_CUDA_TRY(c, d2h(c, out, c->theta.p, n * sizeof(double)));
       return PD_OK;
     case PD_FIELD_DAMAGE:
-      PD_CUDA_TRY(c, cudaMemcpy(out, c->node_damage.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+      PD_CUDA_TRY(c, d2h(c, out, c->node_damage.p, n * sizeof(double)));
       return PD_OK;
     case PD_FIELD_WEIGHTED_VOLUME: return pd_weighted_volume(c, out);
     case PD_FIELD_BOND_DAMAGE: {
       std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
       const uint8_t* src = c->trial_valid ? c->dmg_trial.p : c->dmg.p;
-      PD_CUDA_TRY(c, cudaMemcpy(h.data(), src, (size_t)c->nb, cudaMemcpyDeviceToHost));
+      PD_CUDA_TRY(c, d2h(c, h.data(), src, (size_t)c->nb));
       for (int64_t b = 0; b < c->nb; ++b) out[b] = (double)h[b];
       return PD_OK;
     }
     case PD_FIELD_NUM_NEIGHBORS: {
       std::vector<int64_t> row(n + 1);
-      PD_CUDA_TRY(c, cudaMemcpy(row.data(), c->row.p, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+      PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (n + 1) * sizeof(int64_t)));
       for (int64_t i = 0; i < n; ++i) out[i] = (double)(row[i + 1] - row[i]);
       return PD_OK;
     }

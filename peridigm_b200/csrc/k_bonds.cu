@@ -259,13 +259,13 @@ static int sort_and_check_rows(pd_ctx* c, bool sort_rows) {
     }
     // long rows: block-wide sort over the list of long rows
     std::vector<int64_t> hrow(c->n + 1);
-    PD_CUDA_TRY(c, cudaMemcpy(hrow.data(), c->row.p, (c->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    PD_CUDA_TRY(c, d2h(c, hrow.data(), c->row.p, (c->n + 1) * sizeof(int64_t)));
     std::vector<int64_t> longs;
     for (int64_t i = 0; i < c->n; ++i)
       if (hrow[i + 1] - hrow[i] > 1024) longs.push_back(i);
     DBuf<int64_t> dl;
     PD_CUDA_TRY(c, dl.alloc(longs.size()));
-    PD_CUDA_TRY(c, cudaMemcpy(dl.p, longs.data(), longs.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    PD_CUDA_TRY(c, h2d(c, dl.p, longs.data(), longs.size() * sizeof(int64_t)));
     PD_CUDA_TRY(c, cudaFuncSetAttribute(k_sort_long_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4));
     k_sort_long_rows<<<(unsigned)std::min<size_t>(longs.size(), 1024), 512, 16384 * 4, c->stream>>>(
         dl.p, (int)longs.size(), c->row.p, c->col.p);

@@ -278,7 +278,7 @@ static int ensure_contact_buffers(pd_ctx* c) {
     const double h = c->block_h[c->hblock.empty() ? 0 : c->hblock[i]];
     kap[i] = (9.0 * cs->k_spring / (pi * h * h * h * h)) / h;
   }
-  PD_CUDA_TRY(c, cudaMemcpy(cs->kappa.p, kap.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, cs->kappa.p, kap.data(), n * sizeof(double)));
   return PD_OK;
 }
 

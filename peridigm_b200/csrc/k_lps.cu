@@ -12,12 +12,13 @@
 // through the row (coalesced col/damage loads), partial sums are combined by
 // a fixed xor-shuffle tree, so results are deterministic.
 //
-// Split-FP32 path data (one 32-byte record per point, fetched with one
-// 256-bit load per neighbor):
-//   xr[j] = (x_hi[3], x_lo[3], V, h)   x_hi = fp32(x), x_lo = fp32(x - x_hi)
-//   ur[j] = (u_hi[3], u_lo[3], A, B)   same split of the FP64 displacement
-// X = (x_hi_j - x_hi_i) + (x_lo_j - x_lo_i) is the bond vector to within one
-// FP32 ulp, with no FP64 instruction in the bond loop; likewise du. The FP64
+// Split-FP32 path data:
+//   bx[b] = (X, omega*V_j)             per bond, streamed: X = fp32(x_j - x_i)
+//                                      formed in FP64, rounded once
+//   ur[j] = (u_hi[3], u_lo[3], A, B)   per point, one 256-bit gather per bond;
+//                                      u_hi = fp32(u), u_lo = fp32(u - u_hi)
+// du = (u_hi_j - u_hi_i) + (u_lo_j - u_lo_i) is the displacement difference to
+// within one FP32 ulp, with no FP64 instruction in the bond loop. The FP64
 // displacement u[3n] stays the integration state.
 #include <math.h>
 
@@ -39,17 +40,6 @@ __device__ __forceinline__ double omega_d(int kind, double zeta, double h) {
   }
   double h2 = __dmul_rn(__dmul_rn(__dmul_rn(h, h), 0.4), 0.4);
   return exp(-__ddiv_rn(__dmul_rn(zeta, zeta), h2));
-}
-
-__device__ __forceinline__ float omega_f(int kind, float zeta, float h) {
-  if (kind == PD_INFLUENCE_ONE) return 1.0f;
-  if (kind == PD_INFLUENCE_PARABOLIC_DECAY) {
-    if (zeta > h) return 0.0f;
-    float s = zeta / h;
-    return s < 0.5f ? 1.0f : -4.0f * s * s + 4.0f * s;
-  }
-  float h2 = h * h * 0.16f;
-  return expf(-(zeta * zeta) / h2);
 }
 
 // Squared distance exactly as the reference computes it (dx*dx+dy*dy)+dz*dz,
@@ -78,11 +68,10 @@ __device__ __forceinline__ Rec8 ld_rec_nc(const Rec8* p) {
 }
 __device__ __forceinline__ Rec8 ld_rec(const Rec8* p) {
   Rec8 r;
-  asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]),
-                 "=f"(r.v[6]), "=f"(r.v[7])
-               : "l"(p)
-               : "memory");
+  asm("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]),
+        "=f"(r.v[7])
+      : "l"(p));
   return r;
 }
 
@@ -92,34 +81,53 @@ __device__ __forceinline__ void split_hi_lo(double v, float* hi, float* lo) {
   *lo = __double2float_rn(v - (double)h);
 }
 
-// Bond geometry of the split path (identical operations in both passes and,
-// with both endpoints swapped, exactly negated X, du, Y: bond damage stays
-// symmetric).
+// Bond geometry of the split path from the bond's stored X (FP32, q.xyz) and
+// the two endpoints' displacement records. Identical operations in both passes;
+// with both endpoints swapped X, du and Y are exactly negated (X_ji = -X_ij is
+// rounded from an exactly negated FP64 difference), so e and |X| are identical
+// and bond damage stays symmetric.
 struct SplitBond {
   float Yx, Yy, Yz, zeta, ry, e;
 };
-__device__ __forceinline__ SplitBond split_bond(const Rec8& xi, const Rec8& ui, const Rec8& xj, const Rec8& uj) {
+__device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui, const Rec8& uj) {
   SplitBond s;
-  const float Xx = (xj.v[0] - xi.v[0]) + (xj.v[3] - xi.v[3]);
-  const float Xy = (xj.v[1] - xi.v[1]) + (xj.v[4] - xi.v[4]);
-  const float Xz = (xj.v[2] - xi.v[2]) + (xj.v[5] - xi.v[5]);
   const float Ux = (uj.v[0] - ui.v[0]) + (uj.v[3] - ui.v[3]);
   const float Uy = (uj.v[1] - ui.v[1]) + (uj.v[4] - ui.v[4]);
   const float Uz = (uj.v[2] - ui.v[2]) + (uj.v[5] - ui.v[5]);
-  const float xx = fmaf(Xz, Xz, fmaf(Xy, Xy, Xx * Xx));
-  s.Yx = Xx + Ux;
-  s.Yy = Xy + Uy;
-  s.Yz = Xz + Uz;
+  const float xx = fmaf(q.z, q.z, fmaf(q.y, q.y, q.x * q.x));
+  s.Yx = q.x + Ux;
+  s.Yy = q.y + Uy;
+  s.Yz = q.z + Uz;
   const float yy = fmaf(s.Yz, s.Yz, fmaf(s.Yy, s.Yy, s.Yx * s.Yx));
-  const float rx = rsqrtf(xx);
   s.ry = rsqrtf(yy);
-  s.zeta = xx * rx;
+  s.zeta = xx * rsqrtf(xx);
   const float dY = yy * s.ry;
-  const float xu = fmaf(Xz, Uz, fmaf(Xy, Uy, Xx * Ux));
+  const float xu = fmaf(q.z, Uz, fmaf(q.y, Uy, q.x * Ux));
   const float uu = fmaf(Uz, Uz, fmaf(Uy, Uy, Ux * Ux));
   s.e = __fdividef(fmaf(2.0f, xu, uu), dY + s.zeta);  // |Y| - |X| without cancellation
   return s;
 }
+
+// Streaming loads of bond-ordered data (read once per pass; kept out of L1 so
+// the neighbor records stay resident there).
+//
+// The split passes walk a row kUnroll bonds per lane at a time: first the
+// bond-ordered loads of the batch (damage, neighbor id, X), all independent,
+// then the batch's neighbor-record gathers, then the arithmetic. Loads do not
+// wait on the damage byte, so each lane keeps 2*kUnroll loads in flight
+// instead of a damage -> id -> record chain per bond.
+// Batch depth and the launch bound were swept on the 320,000-point notched
+// plate (1, 2 or 4 bonds per batch; 4 or 2 resident blocks per SM): 4 and 2
+// are the fastest.
+#ifndef PD_BOND_UNROLL
+#define PD_BOND_UNROLL 4
+#endif
+#ifndef PD_BOND_MINB
+#define PD_BOND_MINB 2
+#endif
+constexpr int kUnroll = PD_BOND_UNROLL;
+__device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
+__device__ __forceinline__ int32_t ld_stream(const int32_t* p) { return __ldcs(p); }
 
 // ---------------------------------------------------------------------------
 // K1: weighted volume m_i = sum_j omega*|xi|^2*V_j (material_utilities.cxx:161-188)
@@ -149,24 +157,36 @@ __global__ void __launch_bounds__(kBlock) k_weighted_volume(int64_t n, const int
   if (valid && lane == 0) pt[i].x = acc;
 }
 
-// Split-path constant records: xr = (x_hi, x_lo, V, h) and owner terms
-// own = (3/m, (3K-5mu)/m, 15mu/m, s_c).
-__global__ void k_pack_owner(int64_t n, const double4* __restrict__ xv, const double4* __restrict__ pt,
-                             const double* __restrict__ sc, const double* __restrict__ hp, Rec8* __restrict__ xr,
+// Split-path owner terms own = (3/m, (3K-5mu)/m, 15mu/m, s_c).
+__global__ void k_pack_owner(int64_t n, const double4* __restrict__ pt, const double* __restrict__ sc,
                              float4* __restrict__ own) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double4 x = xv[i];
-  Rec8 r;
-  split_hi_lo(x.x, &r.v[0], &r.v[3]);
-  split_hi_lo(x.y, &r.v[1], &r.v[4]);
-  split_hi_lo(x.z, &r.v[2], &r.v[5]);
-  r.v[6] = (float)x.w;
-  r.v[7] = (float)hp[i];
-  xr[i] = r;
   const double4 p = pt[i];  // (m, K, mu, rho)
   own[i] = make_float4((float)(3.0 / p.x), (float)((3.0 * p.y - 5.0 * p.z) / p.x), (float)(15.0 * p.z / p.x),
                        (float)sc[i]);
+}
+
+// Split-path bond stream bx[b] = (X = x_j - x_i, omega(|X|, h_i) * V_j): the
+// difference and the influence weight in FP64, each rounded once to FP32.
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t* __restrict__ row,
+                                                       const int32_t* __restrict__ col,
+                                                       const double4* __restrict__ xv,
+                                                       const double* __restrict__ hp, int influence,
+                                                       float4* __restrict__ bx) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  if (i >= n) return;
+  const double4 xi = xv[i];
+  const double h = hp[i];
+  for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
+    const double4 xj = xv[col[b]];
+    const double dx = __dsub_rn(xj.x, xi.x), dy = __dsub_rn(xj.y, xi.y), dz = __dsub_rn(xj.z, xi.z);
+    const double om = omega_d(influence, __dsqrt_rn(sq3_rn(dx, dy, dz)), h);
+    bx[b] = make_float4((float)dx, (float)dy, (float)dz, (float)__dmul_rn(om, xj.w));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -176,10 +196,10 @@ __global__ void k_pack_owner(int64_t n, const double4* __restrict__ xv, const do
 // Writes the owner terms A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m into ur[i].
 // ---------------------------------------------------------------------------
 template <int TPO>
-__global__ void __launch_bounds__(kBlock, 4) k_dilatation_split(
+__global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
-    const Rec8* __restrict__ xr, Rec8* __restrict__ ur, const float4* __restrict__ own, int influence,
-    int damage_on, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+    const float4* __restrict__ bx, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
+    double* __restrict__ theta_out, double* __restrict__ node_damage) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -192,23 +212,36 @@ __global__ void __launch_bounds__(kBlock, 4) k_dilatation_split(
     b0 = row[i];
     b1 = row[i + 1];
     ow = own[i];
-    const Rec8 xi = ld_rec_nc(xr + i);
     const Rec8 ui = ld_rec(ur + i);
     const float s_c = damage_on ? ow.w : -1.0f;
-#pragma unroll 2
-    for (int64_t b = b0 + lane; b < b1; b += TPO) {
-      if (dmg[b]) {
-        broken++;
-      } else {
-        const int32_t j = col[b];
-        const Rec8 xj = ld_rec_nc(xr + j);
-        const Rec8 uj = ld_rec(ur + j);
-        const SplitBond s = split_bond(xi, ui, xj, uj);
-        if (s_c >= 0.0f && s.e > s_c * s.zeta) {
-          dmg[b] = 1;
+#pragma unroll 1
+    for (int64_t base = b0 + lane; base < b1; base += kUnroll * TPO) {
+      int dd[kUnroll];
+      int32_t jj[kUnroll];
+      float4 qq[kUnroll];
+      Rec8 uu[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        const int64_t b = base + (int64_t)k * TPO;
+        const bool in = b < b1;
+        dd[k] = in ? (int)dmg[b] : 2;  // 2: past the row end
+        jj[k] = in ? ld_stream(col + b) : (int32_t)i;
+        qq[k] = in ? ld_stream(bx + b) : make_float4(1.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + jj[k]);
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        if (dd[k] == 1) {
           broken++;
-        } else {
-          th = fmaf(omega_f(influence, s.zeta, xi.v[7]) * s.zeta * s.e, xj.v[6], th);
+        } else if (dd[k] == 0) {
+          const SplitBond s = split_bond(qq[k], ui, uu[k]);
+          if (s_c >= 0.0f && s.e > s_c * s.zeta) {
+            dmg[base + (int64_t)k * TPO] = 1;
+            broken++;
+          } else {
+            th = fmaf(qq[k].w * s.zeta, s.e, th);
+          }
         }
       }
     }
@@ -370,34 +403,46 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
 template <int TPO>
-__global__ void __launch_bounds__(kBlock, 4) k_force_split(int64_t n, const int64_t* __restrict__ row,
-                                                           const int32_t* __restrict__ col,
-                                                           const uint8_t* __restrict__ dmg,
-                                                           const Rec8* __restrict__ xr, const Rec8* __restrict__ ur,
-                                                           const double4* __restrict__ pt, int influence,
-                                                           EpiArgs E) {
+__global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
+                                                                      const int32_t* __restrict__ col,
+                                                                      const uint8_t* __restrict__ dmg,
+                                                                      const float4* __restrict__ bx,
+                                                                      const Rec8* __restrict__ ur,
+                                                                      const double4* __restrict__ pt, EpiArgs E) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
   const bool valid = i < n;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (valid) {
-    const Rec8 xi = ld_rec_nc(xr + i);
     const Rec8 ui = ld_rec_nc(ur + i);
     const int64_t b1 = row[i + 1];
-#pragma unroll 2
-    for (int64_t b = row[i] + lane; b < b1; b += TPO) {
-      if (!dmg[b]) {
-        const int32_t j = col[b];
-        const Rec8 xj = ld_rec_nc(xr + j);
-        const Rec8 uj = ld_rec_nc(ur + j);
-        const SplitBond s = split_bond(xi, ui, xj, uj);
-        const float T =
-            omega_f(influence, s.zeta, xi.v[7]) * fmaf(s.zeta, ui.v[6] + uj.v[6], s.e * (ui.v[7] + uj.v[7]));
-        const float w = T * xj.v[6] * s.ry;
-        fx = fmaf(w, s.Yx, fx);
-        fy = fmaf(w, s.Yy, fy);
-        fz = fmaf(w, s.Yz, fz);
+#pragma unroll 1
+    for (int64_t base = row[i] + lane; base < b1; base += kUnroll * TPO) {
+      bool live[kUnroll];
+      int32_t jj[kUnroll];
+      float4 qq[kUnroll];
+      Rec8 uu[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        const int64_t b = base + (int64_t)k * TPO;
+        const bool in = b < b1;
+        live[k] = in && !dmg[b];
+        jj[k] = in ? ld_stream(col + b) : (int32_t)i;
+        qq[k] = in ? ld_stream(bx + b) : make_float4(1.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        if (live[k]) {
+          const SplitBond s = split_bond(qq[k], ui, uu[k]);
+          const float T = fmaf(s.zeta, ui.v[6] + uu[k].v[6], s.e * (ui.v[7] + uu[k].v[7]));
+          const float w = T * qq[k].w * s.ry;
+          fx = fmaf(w, s.Yx, fx);
+          fy = fmaf(w, s.Yy, fy);
+          fz = fmaf(w, s.Yz, fz);
+        }
       }
     }
   }
@@ -589,7 +634,9 @@ cudaError_t launch_weighted_volume(const pd_ctx* c) {
 
 cudaError_t launch_pack_owner(pd_ctx* c) {
   if (c->n == 0 || c->precision != PD_SPLIT_FP32) return cudaSuccess;
-  k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->xv.p, c->pt.p, c->sc.p, c->hp.p, c->xr.p, c->own.p);
+  k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->sc.p, c->own.p);
+  PD_DISPATCH_TPO(c->tpo, k_pack_bonds, grid_for(c->n, c->tpo), c->n, c->row.p, c->col.p, c->xv.p, c->hp.p,
+                  c->influence, c->bx.p);
   return cudaGetLastError();
 }
 
@@ -631,8 +678,8 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
     cudaEventRecord(ev[0], c->stream);
   }
   if (split) {
-    PD_DISPATCH_TPO(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->xr.p, c->ur[c->cur].p,
-                    c->own.p, c->influence, sp.damage_on, c->theta.p, c->node_damage.p);
+    PD_DISPATCH_TPO(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
+                    c->own.p, sp.damage_on, c->theta.p, c->node_damage.p);
   } else {
     PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
                     c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
@@ -660,8 +707,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   E.ur_next = split ? c->ur[c->cur ^ 1].p : nullptr;
   E.status = c->status.p;
   if (split) {
-    PD_DISPATCH_TPO(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->xr.p, c->ur[c->cur].p, c->pt.p,
-                    c->influence, E);
+    PD_DISPATCH_TPO(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E);
   } else {
     PD_DISPATCH_TPO(tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
                     c->pt.p, c->hp.p, c->influence, E);

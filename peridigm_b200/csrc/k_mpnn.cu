@@ -520,9 +520,9 @@ int mpnn_init(pd_ctx* c, uint64_t seed, double radius) {
   PD_CUDA_TRY(c, s->g.alloc(NPARAM));
   PD_CUDA_TRY(c, s->am.alloc(NPARAM));
   PD_CUDA_TRY(c, s->av.alloc(NPARAM));
-  PD_CUDA_TRY(c, cudaMemcpy(s->w.p, w.data(), NPARAM * sizeof(float), cudaMemcpyHostToDevice));
-  PD_CUDA_TRY(c, cudaMemset(s->am.p, 0, NPARAM * sizeof(float)));
-  PD_CUDA_TRY(c, cudaMemset(s->av.p, 0, NPARAM * sizeof(float)));
+  PD_CUDA_TRY(c, h2d(c, s->w.p, w.data(), NPARAM * sizeof(float)));
+  PD_CUDA_TRY(c, dzero(c, s->am.p, NPARAM * sizeof(float)));
+  PD_CUDA_TRY(c, dzero(c, s->av.p, NPARAM * sizeof(float)));
   k_mp_cast<<<(NPARAM + 255) / 256, 256, 0, c->stream>>>(NPARAM, s->w.p, s->wb.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   s->adam_t = 0;
@@ -694,10 +694,10 @@ int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_
   TRY_RC(qs_prepare_current(c));
   DBuf<float> pair;
   PD_CUDA_TRY(c, pair.alloc(6 * c->n));
-  PD_CUDA_TRY(c, cudaMemcpy(pair.p, pair_host, 6 * c->n * sizeof(float), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, pair.p, pair_host, 6 * c->n * sizeof(float)));
   PD_CUDA_TRY(c, cudaMemsetAsync(s->g.p, 0, NPARAM * sizeof(float), c->stream));
   TRY_RC(mp_pair_grad(c, s, pair.p, 1.0, loss));
-  if (grad_host) PD_CUDA_TRY(c, cudaMemcpy(grad_host, s->g.p, NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+  if (grad_host) PD_CUDA_TRY(c, d2h(c, grad_host, s->g.p, NPARAM * sizeof(float)));
   return PD_OK;
 }
 
@@ -817,7 +817,7 @@ int mpnn_get_weights(pd_ctx* c, float* w) {
     c->err = "learned preconditioner not initialised";
     return PD_ERR_STATE;
   }
-  PD_CUDA_TRY(c, cudaMemcpy(w, s->w.p, NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+  PD_CUDA_TRY(c, d2h(c, w, s->w.p, NPARAM * sizeof(float)));
   return PD_OK;
 }
 
@@ -827,7 +827,7 @@ int mpnn_set_weights(pd_ctx* c, const float* w) {
     c->err = "call pd_mpnn_init before loading weights";
     return PD_ERR_STATE;
   }
-  PD_CUDA_TRY(c, cudaMemcpy(s->w.p, w, NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  PD_CUDA_TRY(c, h2d(c, s->w.p, w, NPARAM * sizeof(float)));
   k_mp_cast<<<(NPARAM + 255) / 256, 256, 0, c->stream>>>(NPARAM, s->w.p, s->wb.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   s->ready = true;

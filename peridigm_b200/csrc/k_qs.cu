@@ -360,11 +360,17 @@ __global__ void k_qs_update_p(int64_t n, const double* __restrict__ scal, const 
                               double4* __restrict__ w, int first) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double beta = first ? 0.0 : scal[3];
   double4 p = w[i];
-  p.x = z[3 * i] + beta * p.x;
-  p.y = z[3 * i + 1] + beta * p.y;
-  p.z = z[3 * i + 2] + beta * p.z;
+  if (first) {  // p = z; the previous direction is not read (it may be unset)
+    p.x = z[3 * i];
+    p.y = z[3 * i + 1];
+    p.z = z[3 * i + 2];
+  } else {
+    const double beta = scal[3];
+    p.x = z[3 * i] + beta * p.x;
+    p.y = z[3 * i + 1] + beta * p.y;
+    p.z = z[3 * i + 2] + beta * p.z;
+  }
   w[i] = p;
 }
 
@@ -426,7 +432,7 @@ static int qs_alloc(pd_ctx* c) {
   PD_CUDA_TRY(c, s->partial.alloc(3 * (size_t)std::max<int64_t>(kRedBlocks, gt(n)) + 8));
   PD_CUDA_TRY(c, s->scal.alloc(16));
   PD_CUDA_TRY(c, s->fixed.alloc(n));
-  PD_CUDA_TRY(c, cudaMemset(s->pred.p, 0, s->pred.bytes()));
+  PD_CUDA_TRY(c, dzero(c, s->pred.p, s->pred.bytes()));
   s->n = n;
   return PD_OK;
 }
@@ -584,8 +590,6 @@ static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* it
   if (r0 == 0.0) return PD_OK;
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->scal.p, &rz, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   k_qs_update_p<<<g1(n), kQsBlock, 0, c->stream>>>(n, s->scal.p, s->z.p, s->w.p, 1);
-  DBuf<double> zold;
-  if (flexible) PD_CUDA_TRY(c, zold.alloc(m));
   double rel = 1.0;
   int it = 0;
   if (every > 0) TRY_RC(mpnn_snapshot(c, s->r.p, s->x.p));
@@ -593,7 +597,6 @@ static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* it
     TRY_RC(qs_tangent(c));
     k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, (int)gt(n), 1, 0, s->scal.p + 8);
     k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 0);
-    if (flexible) PD_CUDA_TRY(c, cudaMemcpyAsync(zold.p, s->z.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     k_qs_axpy2<<<g1(m), kQsBlock, 0, c->stream>>>(m, s->scal.p, s->w.p, s->q.p, s->x.p, s->r.p);
     TRY_RC(qs_apply_precond(c, precond, s->r.p, s->z.p));
     if (flexible) {

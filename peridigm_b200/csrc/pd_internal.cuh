@@ -7,9 +7,11 @@
 //   dmg[nb]      uint8 bond damage (0/1), monotone, updated in place
 //   pt[n]        double4 (m, K, mu, rho) per-point material, sc[n] critical stretch, hp[n] horizon
 //   u[3n], v[3n], a[3n], f[3n], fc[3n] FP64 integration state (interleaved xyz)
-// Split-FP32 path, gathered per neighbor with one 256-bit load each:
-//   xr[n]        Rec8 (x_hi[3], x_lo[3], V, h)          constant
-//   ur[2][n]     Rec8 (u_hi[3], u_lo[3], A, B)          double buffered across steps
+// Split-FP32 path:
+//   bx[nb]       float4 (X in FP32, omega(|X|)*V_j) per bond, streamed in bond order;
+//                X = x_j - x_i formed in FP64 and rounded once, constant
+//   ur[2][n]     Rec8 (u_hi[3], u_lo[3], A, B) gathered per neighbor with one
+//                256-bit load; double buffered across steps
 //   own[n]       float4 (3/m, (3K-5mu)/m, 15mu/m, s_c)  owner terms
 // FP64 path:
 //   st[2][n]     double4 (y_x, y_y, y_z, 0) current coordinates, double buffered
@@ -134,7 +136,7 @@ struct pd_ctx {
   bool wv_done = false;
   pdb::DBuf<double4> pt;     // (m, K, mu, rho)
   pdb::DBuf<double> sc;      // critical stretch (<0: off)
-  pdb::DBuf<pdb::Rec8> xr;   // split path: (x_hi, x_lo, V, h)
+  pdb::DBuf<float4> bx;      // split path: per bond (X, omega*V_j)
   pdb::DBuf<float4> own;     // split path: (3/m, (3K-5mu)/m, 15mu/m, s_c)
   bool any_damage = false;
 
@@ -227,6 +229,22 @@ void qs_release(pd_ctx* c);
 // status bits
 enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4 };
 
+}  // namespace pdb
+
+namespace pdb {
+// Host <-> device transfers and fills in the context's stream order. The
+// context stream is non-blocking, so the legacy-stream cudaMemcpy/cudaMemset
+// would not be ordered with its kernels (a pageable cudaMemcpy may even return
+// before its DMA lands). The copies return once complete.
+inline cudaError_t h2d(const pd_ctx* c, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(c->stream);
+}
+inline cudaError_t d2h(const pd_ctx* c, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(c->stream);
+}
+inline cudaError_t dzero(const pd_ctx* c, void* dst, size_t bytes) { return cudaMemsetAsync(dst, 0, bytes, c->stream); }
 }  // namespace pdb
 
 #define TRY_RC(expr)              \
