@@ -143,6 +143,64 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def qs_leg(local, load_steps):
+    """Quasi-static time to 1e-8: the 60^3 tensile cube (216,000 points, h = 1 mm,
+    delta = 3.015h, K log-uniform in [50, 200] GPa from seed 1000, mu = 0.6K, x = 0
+    face clamped, x = max face pulled to 1e-4 m) over `load_steps` equal load
+    steps; Newton to 1e-8 of each load increment's residual, CG to 1e-8 relative.
+    Block-Jacobi CG against the learned preconditioner, trained here on
+    block-Jacobi solves of a 12^3 cube over six random moduli and load paths
+    (the network is local, so it transfers across sizes). Times are device time
+    of the Newton loops (CUDA events)."""
+    from peridigm_b200 import Context, workloads
+
+    t0 = time.perf_counter()
+    w = workloads.qs_cube(n=12, h=1.0e-3, seed=11, jitter=0.05, load_steps=4)
+    with Context(device=local, precision="fp64") as tr:
+        workloads.setup_context(tr, w)
+        tr.mpnn_init(seed=7, radius=1.5e-3)
+        tr.mpnn_collect(4)
+        rng = np.random.default_rng(5)
+        for _ in range(6):
+            K = float(np.exp(rng.uniform(np.log(50e9), np.log(200e9))))
+            tr.material(K, 0.6 * K, 7800.0)
+            tr.clear_boundary_conditions()
+            for bc in w["bcs"][:3]:
+                tr.prescribed_displacement(bc["points"], bc["coordinate"], 0.0, 0.0)
+            right = w["bcs"][3]["points"]
+            tr.prescribed_displacement(right, 0, float(rng.uniform(0.5e-4, 1.5e-4)), 0.0)
+            tr.prescribed_displacement(right, 1, float(rng.uniform(-0.5e-4, 0.5e-4)), 0.0)
+            tr.set_state(np.zeros_like(w["x"]), np.zeros_like(w["x"]))
+            st = None
+            for k in range(1, len(w["times"])):
+                st = tr.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=-1e-8,
+                                     cg_relative_tolerance=1e-8, preconditioner="block_jacobi", stats=st)
+        pairs = tr.mpnn_num_pairs()
+        loss = tr.mpnn_train(40, learning_rate=2e-3, batch=8)
+        weights = tr.mpnn_weights()
+    train_s = time.perf_counter() - t0
+    w2 = workloads.qs_cube(n=60, h=1.0e-3, seed=1000, load_steps=load_steps)
+    out = {"workload": f"qs_cube_60x60x60 (seed 1000, {load_steps} load steps)", "points": int(len(w2["vol"])),
+           "tolerance": 1e-8, "training": {"pairs": pairs, "epochs": 40, "final_loss": loss, "seconds": train_s}}
+    for precond in ("block_jacobi", "mpnn"):
+        with Context(device=local, precision="fp64") as ctx:
+            workloads.setup_context(ctx, w2)
+            if precond == "mpnn":
+                ctx.mpnn_init(seed=0, radius=1.5e-3)
+                ctx.mpnn_set_weights(weights)
+            st = None
+            t1 = time.perf_counter()
+            for k in range(1, len(w2["times"])):
+                st = ctx.qs_load_step(w2["times"][k - 1], w2["times"][k], newton_tolerance=-1e-8,
+                                      cg_relative_tolerance=1e-8, preconditioner=precond, stats=st)
+            wall = time.perf_counter() - t1
+            out[precond] = {"seconds": st.device_ms / 1e3, "wall_seconds": wall, "cg_iterations": st.cg_iterations,
+                            "newton_iterations": st.newton_iterations, "final_cg_residual": st.final_residual,
+                            "fallbacks": st.preconditioner_fallbacks}
+    out["mpnn_time_over_block_jacobi"] = out["mpnn"]["seconds"] / out["block_jacobi"]["seconds"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -150,6 +208,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-qs", action="store_true")
+    ap.add_argument("--qs-load-steps", type=int, default=20)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args.gpus)
@@ -262,6 +322,11 @@ def main():
     e2e = {"value": world * nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
            "d2h_bytes_per_step": 24 * n, "steps": esteps, "api": "pd_compute_force (host y in, host force out)"}
 
+    # ---- quasi-static time to 1e-8 (rank 0 only) -----------------------------
+    qs = None
+    if rank == 0 and not args.no_qs:
+        qs = qs_leg(local, args.qs_load_steps)
+
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -285,7 +350,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "fp64": {"value": value64, "unit": UNIT, "steps": fsteps, "ms_per_step": ms64 / fsteps,
                      "split_over_fp64": value / value64},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "qs": qs, "clocks": clk,
             "gpu_launches": 2 * args.steps}
     if rank == 0:
         print(json.dumps(line), flush=True)

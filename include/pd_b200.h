@@ -225,7 +225,8 @@ int pd_get_field(pd_ctx* ctx, int32_t field, double* out);
 
 typedef struct {
   double newton_tolerance;      /* on ||r||_2 + 20 ||r||_inf (Peridigm.cpp:4316): > 0 absolute ("Absolute
-                                 * Tolerance"), < 0 relative to the load step's initial value */
+                                 * Tolerance"), < 0 relative to the value at the load step's start with
+                                 * only the prescribed increments applied (before any predictor) */
   double cg_relative_tolerance; /* ||r_cg|| / ||r_cg,0|| of each linear solve (Belos "Relative Tolerance", :2556) */
   int32_t max_newton_iterations;/* "Maximum Solver Iterations" */
   int32_t max_cg_iterations;

@@ -739,18 +739,27 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
   const double dt = t_cur - t_prev;
-  if (o->use_predictor && st && st->steps > 0) {
-    PD_CUDA_TRY(c, cudaMemcpyAsync(s->du.p, s->pred.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  } else {
-    PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
-  }
-  if (c->has_bc)
-    k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, s->du.p);
+  const bool predict = o->use_predictor && st && st->steps > 0;
   double l2, linf;
-  TRY_RC(qs_residual(c, &l2, &linf));
+  // Negative tolerance: relative to the metric of this load step's start
+  // without the predictor (prescribed increments only), the scale of the load
+  // increment; the predicted start can sit close to the FP64 floor.
+  double ref_metric = 0.0;
+  if (o->newton_tolerance < 0.0 || !predict) {
+    PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
+    if (c->has_bc)
+      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, s->du.p);
+    TRY_RC(qs_residual(c, &l2, &linf));
+    ref_metric = l2 + 20.0 * linf;
+  }
+  if (predict) {
+    PD_CUDA_TRY(c, cudaMemcpyAsync(s->du.p, s->pred.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if (c->has_bc)
+      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, s->du.p);
+    TRY_RC(qs_residual(c, &l2, &linf));
+  }
   double metric = l2 + 20.0 * linf;
-  // negative tolerance: relative to this step's initial metric
-  const double newton_tol = o->newton_tolerance < 0.0 ? -o->newton_tolerance * metric : o->newton_tolerance;
+  const double newton_tol = o->newton_tolerance < 0.0 ? -o->newton_tolerance * ref_metric : o->newton_tolerance;
   int newton = 0, cg_total = 0;
   double last_rel = 0.0;
   const int64_t fallbacks0 = c->qs_fallbacks;
