@@ -215,6 +215,25 @@ int pd_clear_boundary_conditions(pd_ctx* ctx);
  * initial evaluation at t0, then nsteps steps of size dt. State stays on the
  * device; read it with pd_get_field. stats may be NULL. */
 int pd_verlet_run(pd_ctx* ctx, double dt, double t0, int64_t nsteps, pd_stats* stats);
+/* Stepping form of pd_verlet_run for hosts that act between steps, e.g. the
+ * halo exchange of a domain decomposition (no counterpart in the reference,
+ * whose step loop exchanges ghosts through Epetra imports inside
+ * executeExplicit, Peridigm.cpp:1497-1546). pd_verlet_begin does the initial
+ * evaluation at t0 and the first half of step 1; pd_verlet_step(k) completes k
+ * steps and starts the next; pd_verlet_finish completes the last one and fills
+ * stats (device_ms spans begin to finish, host time between calls included).
+ * begin + step(n - 1) + finish gives the same state as pd_verlet_run(n). */
+int pd_verlet_begin(pd_ctx* ctx, double dt, double t0);
+int pd_verlet_step(pd_ctx* ctx, int64_t nsteps);
+int pd_verlet_finish(pd_ctx* ctx, pd_stats* stats);
+/* Ghost-state exchange between pd_verlet_begin and pd_verlet_finish (device
+ * pointers on the context's device, ordered on its stream; both return after
+ * the copy). pack: out[6k..6k+5] = (u, y) of point idx[k], the displacement
+ * and current coordinates the next step's evaluation reads. unpack: makes
+ * points idx[k] hold in[6k..6k+5] exactly as the packing context held them.
+ * Indices outside [0, n) are skipped and reported as PD_ERR_ARG. */
+int pd_pack_state_device(pd_ctx* ctx, int64_t n_idx, const int32_t* idx, double* out);
+int pd_unpack_state_device(pd_ctx* ctx, int64_t n_idx, const int32_t* idx, const double* in);
 /* Reads a field (PD_FIELD_*) into host memory in the caller's order. */
 int pd_get_field(pd_ctx* ctx, int32_t field, double* out);
 

@@ -97,6 +97,11 @@ SIGNATURES = {
     "pd_set_bond_damage": (C.c_int, [_vp, _dp]),
     "pd_critical_time_step": (C.c_int, [_vp, _dp]),
     "pd_critical_time_step_static": (C.c_int, [_vp, _dp]),
+    "pd_verlet_begin": (C.c_int, [_vp, C.c_double, C.c_double]),
+    "pd_verlet_step": (C.c_int, [_vp, C.c_int64]),
+    "pd_verlet_finish": (C.c_int, [_vp, C.POINTER(Stats)]),
+    "pd_pack_state_device": (C.c_int, [_vp, C.c_int64, _vp, _vp]),
+    "pd_unpack_state_device": (C.c_int, [_vp, C.c_int64, _vp, _vp]),
     "pd_set_state": (C.c_int, [_vp, _dp, _dp]),
     "pd_add_prescribed_displacement": (C.c_int, [_vp, C.c_int64, _i64p, C.c_int32, C.c_double, C.c_double]),
     "pd_clear_boundary_conditions": (C.c_int, [_vp]),

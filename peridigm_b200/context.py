@@ -206,6 +206,34 @@ class Context:
         self._ok(self.L.pd_verlet_run(self.h, float(dt), float(t0), int(nsteps), C.byref(st)))
         return {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
 
+    def verlet_begin(self, dt, t0=0.0):
+        """Stepping form of verlet_run: begin + step(n - 1) + finish == verlet_run(n)."""
+        self._ok(self.L.pd_verlet_begin(self.h, float(dt), float(t0)))
+
+    def verlet_step(self, nsteps=1):
+        self._ok(self.L.pd_verlet_step(self.h, int(nsteps)))
+
+    def verlet_finish(self):
+        st = _lib.Stats()
+        self._ok(self.L.pd_verlet_finish(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.Stats._fields_}
+
+    def pack_state(self, idx, out):
+        """out[k] = (u, y) of point idx[k]; idx int32 and out float64 [len(idx), 6]
+        torch tensors on this context's device."""
+        import torch
+
+        torch.cuda.current_stream(idx.device).synchronize()
+        self._ok(self.L.pd_pack_state_device(self.h, int(idx.numel()), C.c_void_p(idx.data_ptr()),
+                                             C.c_void_p(out.data_ptr())))
+
+    def unpack_state(self, idx, vals):
+        import torch
+
+        torch.cuda.current_stream(idx.device).synchronize()
+        self._ok(self.L.pd_unpack_state_device(self.h, int(idx.numel()), C.c_void_p(idx.data_ptr()),
+                                               C.c_void_p(vals.data_ptr())))
+
     # -- quasi-static --------------------------------------------------------
     def qs_load_step(self, t_prev, t_cur, newton_tolerance, cg_relative_tolerance=1e-8, max_newton=20,
                      max_cg=20000, preconditioner="block_jacobi", use_predictor=True, stats=None):

@@ -140,6 +140,7 @@ int check_status(pd_ctx* c) {
   if (st & ST_NONFINITE_FORCE) return fail(c, PD_ERR_NONFINITE, "NaN returned by force evaluation");
   if (st & ST_NONFINITE_CONTACT) return fail(c, PD_ERR_NONFINITE, "NaN returned by contact force evaluation");
   if (st & ST_TIMEOUT) return fail(c, PD_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (st & ST_BAD_INDEX) return fail(c, PD_ERR_ARG, "a point index was outside the context (ignored)");
   return PD_OK;
 }
 
@@ -211,6 +212,8 @@ int pd_destroy(pd_ctx* c) {
   contact_release(c);
   qs_release(c);
   mpnn_release(c);
+  for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
+  if (c->vbeg) cudaEventDestroy(c->vbeg);
   cudaStream_t s = c->stream;
   delete c;
   if (s) cudaStreamDestroy(s);
@@ -558,14 +561,112 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
     stats->steps = nsteps;
     stats->bonds = c->nb;
     stats->device_ms = ms;
-    std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
-    PD_CUDA_TRY(c, d2h(c, h.data(), c->dmg.p, (size_t)c->nb));
-    int64_t br = 0;
-    for (int64_t b = 0; b < c->nb; ++b) br += h[b];
-    stats->broken_bonds = br;
+    TRY(count_broken(c, &stats->broken_bonds));
     stats->contact_pairs = contact_pairs(c);
   }
   return rc;
+}
+
+// ---- stepping form: begin + step(n - 1) + finish == pd_verlet_run(n) ------
+static StepParams verlet_params(const pd_ctx* c, double dt, double t0) {
+  StepParams sp{};
+  sp.dt = dt;
+  sp.t0 = t0;
+  sp.damage_on = c->any_damage ? 1 : 0;
+  sp.has_bc = c->has_bc ? 1 : 0;
+  sp.has_contact = c->contact != nullptr ? 1 : 0;
+  return sp;
+}
+
+int pd_verlet_begin(pd_ctx* c, double dt, double t0) {
+  CHECK_CTX(c);
+  if (!(dt > 0.0)) return fail(c, PD_ERR_ARG, "pd_verlet_begin: dt must be positive");
+  TRY(ensure_ready(c));
+  if (!c->state_init) TRY(pd_set_state(c, nullptr, nullptr));
+  StepParams sp = verlet_params(c, dt, t0);
+  if (!c->vbeg) PD_CUDA_TRY(c, cudaEventCreate(&c->vbeg));
+  PD_CUDA_TRY(c, cudaEventRecord(c->vbeg, c->stream));
+  // initial evaluation (Peridigm.cpp:1393-1423): its damage is not committed
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+  if (sp.has_contact) {
+    TRY(contact_prepare(c, 0));
+    TRY(contact_eval(c));
+  }
+  sp.step = 0;
+  sp.mode = EVAL_ADVANCE;
+  PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg_trial.p));
+  c->cur ^= 1;
+  c->vrun = true;
+  c->vdt = dt;
+  c->vt0 = t0;
+  c->vstep = 0;
+  c->trial_valid = false;
+  return check_status(c);
+}
+
+int pd_verlet_step(pd_ctx* c, int64_t nsteps) {
+  CHECK_CTX(c);
+  if (!c->vrun) return fail(c, PD_ERR_STATE, "pd_verlet_step: call pd_verlet_begin first");
+  if (nsteps < 0) return fail(c, PD_ERR_ARG, "pd_verlet_step: nsteps must be >= 0");
+  StepParams sp = verlet_params(c, c->vdt, c->vt0);
+  for (int64_t k = 0; k < nsteps; ++k) {
+    sp.step = ++c->vstep;
+    sp.mode = EVAL_ADVANCE;
+    if (sp.has_contact) {
+      TRY(contact_prepare(c, sp.step));
+      TRY(contact_eval(c));
+    }
+    PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg.p));
+    c->cur ^= 1;
+  }
+  return check_status(c);
+}
+
+int pd_verlet_finish(pd_ctx* c, pd_stats* stats) {
+  CHECK_CTX(c);
+  if (!c->vrun) return fail(c, PD_ERR_STATE, "pd_verlet_finish: call pd_verlet_begin first");
+  StepParams sp = verlet_params(c, c->vdt, c->vt0);
+  sp.step = ++c->vstep;
+  sp.mode = EVAL_LAST;
+  sp.f_out = c->f.p;
+  if (sp.has_contact) {
+    TRY(contact_prepare(c, sp.step));
+    TRY(contact_eval(c));
+  }
+  PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg.p));
+  cudaEvent_t e1;
+  PD_CUDA_TRY(c, cudaEventCreate(&e1));
+  PD_CUDA_TRY(c, cudaEventRecord(e1, c->stream));
+  PD_CUDA_TRY(c, cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->vbeg, e1);
+  cudaEventDestroy(e1);
+  c->vrun = false;
+  const int rc = check_status(c);
+  if (stats) {
+    stats->steps = c->vstep;
+    stats->bonds = c->nb;
+    stats->device_ms = ms;
+    TRY(count_broken(c, &stats->broken_bonds));
+    stats->contact_pairs = contact_pairs(c);
+  }
+  return rc;
+}
+
+int pd_pack_state_device(pd_ctx* c, int64_t n_idx, const int32_t* idx_dev, double* out_dev) {
+  CHECK_CTX(c);
+  if (n_idx < 0 || (n_idx > 0 && (!idx_dev || !out_dev))) return fail(c, PD_ERR_ARG, "pd_pack_state_device: bad arguments");
+  if (!c->vrun) return fail(c, PD_ERR_STATE, "pd_pack_state_device: only between pd_verlet_begin and pd_verlet_finish");
+  PD_CUDA_TRY(c, launch_pack_state(c, n_idx, idx_dev, out_dev));
+  return check_status(c);
+}
+
+int pd_unpack_state_device(pd_ctx* c, int64_t n_idx, const int32_t* idx_dev, const double* in_dev) {
+  CHECK_CTX(c);
+  if (n_idx < 0 || (n_idx > 0 && (!idx_dev || !in_dev))) return fail(c, PD_ERR_ARG, "pd_unpack_state_device: bad arguments");
+  if (!c->vrun) return fail(c, PD_ERR_STATE, "pd_unpack_state_device: only between pd_verlet_begin and pd_verlet_finish");
+  PD_CUDA_TRY(c, launch_unpack_state(c, n_idx, idx_dev, in_dev));
+  return check_status(c);
 }
 
 int pd_qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {

@@ -791,4 +791,88 @@ cudaError_t launch_u_from_record(pd_ctx* c, int parity, double* u_out) {
   return cudaGetLastError();
 }
 
+// out[6k..6k+5] = (u, y) of point idx[k]; y is the FP64 path's gathered
+// coordinate record (x + u on the split path, which gathers u itself).
+__global__ void k_pack_state(int64_t n, int64_t n_idx, const int32_t* __restrict__ idx, const double* __restrict__ u,
+                             const double4* __restrict__ xv, const double4* __restrict__ st, double* __restrict__ out,
+                             int* __restrict__ status) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_idx) return;
+  const int64_t i = idx[k];
+  if (i < 0 || i >= n) {  // index outside the context: reported, not accessed
+    atomicOr(status, ST_BAD_INDEX);
+    return;
+  }
+  const double u0 = u[3 * i], u1 = u[3 * i + 1], u2 = u[3 * i + 2];
+  double4 y;
+  if (st) {
+    y = st[i];
+  } else {
+    const double4 x = xv[i];
+    y = make_double4(x.x + u0, x.y + u1, x.z + u2, 0.0);
+  }
+  double* o = out + 6 * k;
+  o[0] = u0, o[1] = u1, o[2] = u2, o[3] = y.x, o[4] = y.y, o[5] = y.z;
+}
+
+// The receiving side: u and the record the next evaluation gathers (hi/lo
+// split of u on the split path, y on the FP64 path), both as the owner holds them.
+__global__ void k_unpack_state(int64_t n, int64_t n_idx, const int32_t* __restrict__ idx,
+                               const double* __restrict__ in, double* __restrict__ u, double4* __restrict__ st,
+                               Rec8* __restrict__ ur, int* __restrict__ status) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_idx) return;
+  const int64_t i = idx[k];
+  if (i < 0 || i >= n) {
+    atomicOr(status, ST_BAD_INDEX);
+    return;
+  }
+  const double* v = in + 6 * k;
+  for (int c = 0; c < 3; ++c) u[3 * i + c] = v[c];
+  if (ur) {
+    for (int c = 0; c < 3; ++c) split_hi_lo(v[c], &ur[i].v[c], &ur[i].v[c + 3]);
+  } else {
+    st[i] = make_double4(v[3], v[4], v[5], 0.0);
+  }
+}
+
+cudaError_t launch_pack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, double* out) {
+  if (n_idx == 0) return cudaSuccess;
+  const bool split = c->precision == PD_SPLIT_FP32;
+  k_pack_state<<<grid1(n_idx), kBlock, 0, c->stream>>>(c->n, n_idx, idx, c->u.p, c->xv.p,
+                                                        split ? nullptr : c->st[c->cur].p, out, c->status.p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, const double* in) {
+  if (n_idx == 0) return cudaSuccess;
+  const bool split = c->precision == PD_SPLIT_FP32;
+  k_unpack_state<<<grid1(n_idx), kBlock, 0, c->stream>>>(c->n, n_idx, idx, in, c->u.p,
+                                                          split ? nullptr : c->st[c->cur].p,
+                                                          split ? c->ur[c->cur].p : nullptr, c->status.p);
+  return cudaGetLastError();
+}
+
+__global__ void k_count_nonzero(int64_t m, const uint8_t* __restrict__ d, unsigned long long* __restrict__ out) {
+  unsigned long long cnt = 0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+    cnt += d[k] != 0;
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+int count_broken(pd_ctx* c, int64_t* out) {
+  *out = 0;
+  if (c->nb == 0) return PD_OK;
+  if (c->scratch.count < 1) PD_CUDA_TRY(c, c->scratch.alloc(1));
+  unsigned long long* dcount = reinterpret_cast<unsigned long long*>(c->scratch.p);
+  PD_CUDA_TRY(c, cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), c->stream));
+  k_count_nonzero<<<4 * 148, kBlock, 0, c->stream>>>(c->nb, c->dmg.p, dcount);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  unsigned long long h = 0;
+  PD_CUDA_TRY(c, d2h(c, &h, dcount, sizeof(h)));
+  *out = (int64_t)h;
+  return PD_OK;
+}
+
 }  // namespace pdb

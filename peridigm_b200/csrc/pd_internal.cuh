@@ -147,6 +147,11 @@ struct pd_ctx {
   pdb::DBuf<double4> ab64;
   pdb::DBuf<double> u, v, a, f, fc, theta, node_damage;
   bool state_init = false;
+  // stepping form of the Verlet loop (pd_verlet_begin / _step / _finish)
+  bool vrun = false;
+  double vdt = 0.0, vt0 = 0.0;
+  int64_t vstep = 0;
+  cudaEvent_t vbeg = nullptr;
 
   // boundary conditions
   std::vector<uint8_t> h_bc_mask;
@@ -224,10 +229,16 @@ int64_t contact_pairs(const pd_ctx* c);
 int contact_configure(pd_ctx* c, double r_search, int freq, double r_contact, double k_spring, double friction);
 int contact_force_from(pd_ctx* c, const double* y_dev, const double* v_dev, double* fc_dev);
 cudaError_t launch_u_from_record(pd_ctx* c, int parity, double* u_out);  // split path: hi + lo
+// Ghost-state exchange: (u, y) of the listed points in the state the next
+// evaluation reads, 6 doubles per point; unpack overwrites it.
+cudaError_t launch_pack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, double* out);
+cudaError_t launch_unpack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, const double* in);
+// Number of broken bonds (damage byte set) of the committed damage.
+int count_broken(pd_ctx* c, int64_t* out);
 void qs_release(pd_ctx* c);
 
 // status bits
-enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4 };
+enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4, ST_BAD_INDEX = 8 };
 
 }  // namespace pdb
 
