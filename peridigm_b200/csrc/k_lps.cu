@@ -117,15 +117,53 @@ __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui,
 // wait on the damage byte, so each lane keeps 2*kUnroll loads in flight
 // instead of a damage -> id -> record chain per bond.
 // Batch depth and the launch bound were swept on the 320,000-point notched
-// plate (1, 2 or 4 bonds per batch; 4 or 2 resident blocks per SM): 4 and 2
-// are the fastest.
+// plate (1, 2 or 4 bonds per batch; 2, 3 or 4 resident blocks per SM): with
+// the staged streams below, 4 bonds per batch and 4 blocks per SM (64
+// registers per thread, 40 KB of staging per block) are the fastest.
 #ifndef PD_BOND_UNROLL
 #define PD_BOND_UNROLL 4
 #endif
 #ifndef PD_BOND_MINB
-#define PD_BOND_MINB 2
+#define PD_BOND_MINB 4
 #endif
 constexpr int kUnroll = PD_BOND_UNROLL;
+
+// Bond streams staged through shared memory with cp.async: while a lane
+// gathers and computes batch t, its batch t+1 of bond records and neighbor ids
+// is already in flight into its own slots (two stages; each thread reads only
+// what it copied, so no block barrier is needed).
+#ifndef PD_BOND_STAGE
+#define PD_BOND_STAGE 1
+#endif
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Stages batch `base` (kUnroll bonds, stride TPO) of a lane into slot `st`.
+template <int TPO>
+__device__ __forceinline__ void stage_batch(float4 (*sq)[kUnroll][kBlock], int32_t (*sj)[kUnroll][kBlock], int st,
+                                            int64_t base, int64_t b1, const float4* __restrict__ bx,
+                                            const int32_t* __restrict__ col) {
+#pragma unroll
+  for (int k = 0; k < kUnroll; ++k) {
+    const int64_t b = base + (int64_t)k * TPO;
+    if (b < b1) {
+      cp_async16(&sq[st][k][threadIdx.x], bx + b);
+      cp_async4(&sj[st][k][threadIdx.x], col + b);
+    }
+  }
+  cp_commit();
+}
 __device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
 __device__ __forceinline__ int32_t ld_stream(const int32_t* p) { return __ldcs(p); }
 
@@ -214,6 +252,46 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     ow = own[i];
     const Rec8 ui = ld_rec(ur + i);
     const float s_c = damage_on ? ow.w : -1.0f;
+#if PD_BOND_STAGE
+    __shared__ float4 sq[2][kUnroll][kBlock];
+    __shared__ int32_t sj[2][kUnroll][kBlock];
+    int st = 0;
+    stage_batch<TPO>(sq, sj, 0, b0 + lane, b1, bx, col);
+#pragma unroll 1
+    for (int64_t base = b0 + lane; base < b1; base += kUnroll * TPO) {
+      stage_batch<TPO>(sq, sj, st ^ 1, base + kUnroll * TPO, b1, bx, col);  // next batch (maybe empty)
+      cp_wait<1>();                                                          // this batch has landed
+      int dd[kUnroll];
+      int32_t jj[kUnroll];
+      Rec8 uu[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        const int64_t b = base + (int64_t)k * TPO;
+        const bool in = b < b1;
+        dd[k] = in ? (int)dmg[b] : 2;  // 2: past the row end
+        jj[k] = in ? sj[st][k][threadIdx.x] : (int32_t)i;
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + jj[k]);
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        if (dd[k] == 1) {
+          broken++;
+        } else if (dd[k] == 0) {
+          const float4 q = sq[st][k][threadIdx.x];
+          const SplitBond s = split_bond(q, ui, uu[k]);
+          if (s_c >= 0.0f && s.e > s_c * s.zeta) {
+            dmg[base + (int64_t)k * TPO] = 1;
+            broken++;
+          } else {
+            th = fmaf(q.w * s.zeta, s.e, th);
+          }
+        }
+      }
+      st ^= 1;
+    }
+    cp_wait<0>();
+#else
 #pragma unroll 1
     for (int64_t base = b0 + lane; base < b1; base += kUnroll * TPO) {
       int dd[kUnroll];
@@ -245,6 +323,7 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
         }
       }
     }
+#endif
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
@@ -417,6 +496,44 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
   if (valid) {
     const Rec8 ui = ld_rec_nc(ur + i);
     const int64_t b1 = row[i + 1];
+#if PD_BOND_STAGE
+    __shared__ float4 sq[2][kUnroll][kBlock];
+    __shared__ int32_t sj[2][kUnroll][kBlock];
+    const int64_t bs = row[i] + lane;
+    int st = 0;
+    stage_batch<TPO>(sq, sj, 0, bs, b1, bx, col);
+#pragma unroll 1
+    for (int64_t base = bs; base < b1; base += kUnroll * TPO) {
+      stage_batch<TPO>(sq, sj, st ^ 1, base + kUnroll * TPO, b1, bx, col);
+      cp_wait<1>();
+      bool live[kUnroll];
+      int32_t jj[kUnroll];
+      Rec8 uu[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        const int64_t b = base + (int64_t)k * TPO;
+        const bool in = b < b1;
+        live[k] = in && !dmg[b];
+        jj[k] = in ? sj[st][k][threadIdx.x] : (int32_t)i;
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        if (live[k]) {
+          const float4 q = sq[st][k][threadIdx.x];
+          const SplitBond s = split_bond(q, ui, uu[k]);
+          const float T = fmaf(s.zeta, ui.v[6] + uu[k].v[6], s.e * (ui.v[7] + uu[k].v[7]));
+          const float w = T * q.w * s.ry;
+          fx = fmaf(w, s.Yx, fx);
+          fy = fmaf(w, s.Yy, fy);
+          fz = fmaf(w, s.Yz, fz);
+        }
+      }
+      st ^= 1;
+    }
+    cp_wait<0>();
+#else
 #pragma unroll 1
     for (int64_t base = row[i] + lane; base < b1; base += kUnroll * TPO) {
       bool live[kUnroll];
@@ -445,6 +562,7 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
         }
       }
     }
+#endif
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);

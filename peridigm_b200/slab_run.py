@@ -45,8 +45,7 @@ def main():
             dt_local = torch.tensor([0.7 * ctx.critical_time_step()], dtype=torch.float64, device="cuda")
             dist.all_reduce(dt_local, op=dist.ReduceOp.MIN)
             dt = float(dt_local.item())
-            row, _ = ctx.bonds_csr()
-            owned_bonds = int((row[plan.owned_local + 1] - row[plan.owned_local]).sum())
+            owned_bonds = int(ctx.field("Number_Of_Neighbors")[plan.owned_local].sum())
             halo = slabs.HaloExchange(plan, torch.device("cuda", local), dist)
             dist.barrier()
             torch.cuda.synchronize()
