@@ -240,7 +240,11 @@ int pd_get_field(pd_ctx* ctx, int32_t field, double* out);
 /* ---- quasi-static ---------------------------------------------------------- */
 #define PD_PRECOND_NONE 0         /* plain CG (the reference's default, usePreconditioner=false, Peridigm.cpp:2740) */
 #define PD_PRECOND_BLOCK_JACOBI 1 /* inverse 3x3 diagonal blocks ("Block 3x3", Peridigm.cpp:1603-1646) */
-#define PD_PRECOND_MPNN 2         /* learned message-passing preconditioner + block Jacobi (no reference counterpart) */
+#define PD_PRECOND_MPNN 2         /* learned message-passing correction on top of PD_PRECOND_TWO_LEVEL, or of block
+                                   * Jacobi alone after pd_mpnn_coarse(ctx, -1) (no reference counterpart) */
+#define PD_PRECOND_TWO_LEVEL 3    /* block Jacobi + exact Galerkin coarse correction on aggregate cells (no reference
+                                   * counterpart): z = P_bj r + P0 (P0^T K P0)^-1 P0^T r, P0 = piecewise-constant
+                                   * translations of the non-empty cells of a grid of side >= 2 * max horizon */
 
 typedef struct {
   double newton_tolerance;      /* on ||r||_2 + 20 ||r||_inf (Peridigm.cpp:4316): > 0 absolute ("Absolute
@@ -251,6 +255,9 @@ typedef struct {
   int32_t max_cg_iterations;
   int32_t preconditioner;       /* PD_PRECOND_* */
   int32_t use_predictor;        /* start the free dofs from the previous step's increment (Peridigm.cpp:2764-2769) */
+  double coarse_cell;           /* PD_PRECOND_TWO_LEVEL: aggregate cell side; the side used is max(coarse_cell,
+                                 * 2 * max horizon), grown 1.25x at a time until the coarse space has at most
+                                 * 6144 dofs (0: the default) */
 } pd_qs_options;
 
 /* One quasi-static load step t_prev -> t_cur of Peridigm::executeQuasiStatic
@@ -274,25 +281,47 @@ int pd_jacobian_apply(pd_ctx* ctx, const double* u, const double* w, double* kw)
 int pd_jacobian_block_diagonal(pd_ctx* ctx, const double* u, double* blocks);
 
 /* ---- learned preconditioner (no counterpart in the reference) -------------
- * A message-passing network on the subgraph of bonds shorter than `radius`
- * (3 layers, hidden 64, BF16 weights and activations, FP32 accumulation)
- * that corrects block Jacobi: z = P_bj r + rms(P_bj r) * N(P_bj r / rms, r / rms).
- * Used with PD_PRECOND_MPNN in flexible CG; a stall, or a true FP64 residual
- * above the tolerance, falls back to block-Jacobi CG. */
-int pd_mpnn_init(pd_ctx* ctx, uint64_t seed, double radius);
-/* While every > 0, block-Jacobi CG solves of pd_qs_load_step store training
- * pairs (r_k, x* - x_k) from every every-th iterate (K (x* - x_k) = r_k). */
+ * A learned middle level added to the two-level preconditioner:
+ *   z = P_bj r + P0 Ac^-1 P0^T r + Q S G^T G S Q^T r
+ * Q: piecewise-constant prolongation from patches (the non-empty cells of a
+ * grid of side `patch`, about two lattice spacings); S: per-patch scales from
+ * the block-Jacobi blocks; G: a linear message-passing network on the patch
+ * graph (3 layers, hidden 64, BF16 weights, FP32 activations and
+ * accumulation). M is symmetric positive definite, so PD_PRECOND_MPNN solves
+ * run plain CG; a stall, or a true FP64 residual above the tolerance, falls
+ * back to the same preconditioner without the network. */
+int pd_mpnn_init(pd_ctx* ctx, uint64_t seed, double patch);
+/* While every > 0, block-Jacobi and two-level CG solves of pd_qs_load_step
+ * store training pairs (r_k, x* - x_k) from every every-th iterate
+ * (K (x* - x_k) = r_k). */
 int pd_mpnn_collect(pd_ctx* ctx, int32_t every);
 int pd_mpnn_num_pairs(pd_ctx* ctx, int64_t* count);
-/* Adam on the stored residuals, loss |K z - r|^2 / |r|^2 with K the tangent at
- * the context's current displacement (rescaled to each residual's modulus). */
+/* Adam on the stored pairs, loss L = 1 - (r.z)^2 / ((z.K z)(e.r)) (the
+ * energy-norm error left by one optimally scaled preconditioned step) with K
+ * the tangent at the context's current displacement, rescaled to each pair's
+ * modulus. */
 int pd_mpnn_train(pd_ctx* ctx, int32_t epochs, double learning_rate, int32_t batch, double* loss);
 int pd_mpnn_num_params(int64_t* count);
 int pd_mpnn_get_weights(pd_ctx* ctx, float* weights);
 int pd_mpnn_set_weights(pd_ctx* ctx, const float* weights);
-/* Loss and parameter gradient for one residual (a = P_bj r, r; 6n floats) with
- * the tangent at the current displacement, for gradient checks. */
+/* Loss and parameter gradient for one pair (a = P_bj r, r = K e, e; 9n
+ * floats) with the tangent at the current displacement, for gradient checks.
+ * With the coarse level on, z includes P0 Ac^-1 P0^T r of the current
+ * displacement. */
 int pd_mpnn_loss_grad(pd_ctx* ctx, const float* pair, double* loss, float* grad);
+/* Coarse level under the network (training, loss and PD_PRECOND_MPNN solves):
+ * cell >= 0 puts the network on top of the two-level preconditioner with
+ * aggregate cells of side max(cell, 2 * max horizon) (the default after
+ * pd_mpnn_init, cell 0); cell < 0 puts it on block Jacobi alone. */
+int pd_mpnn_coarse(pd_ctx* ctx, double cell);
+/* The coarse space of PD_PRECOND_TWO_LEVEL at displacement u (host [3n]):
+ * n_coarse receives 3 x the number of aggregates; aggregate[n] the aggregate
+ * of each point, A the assembled P0^T K P0 and A_inv its inverse (row-major
+ * n_coarse^2, coarse dof 3I + c = component c of aggregate I). Call first with
+ * aggregate, A and A_inv NULL to get n_coarse; on the second call *n_coarse
+ * must hold at least that. */
+int pd_qs_coarse_operator(pd_ctx* ctx, const double* u, double cell, int64_t* n_coarse, int32_t* aggregate,
+                          double* A, double* A_inv);
 
 /* ---- instrumentation ----------------------------------------------------- */
 /* Named stopwatches around the hot calls are the reference's Timer

@@ -1,33 +1,34 @@
-"""CPU oracle of the learned CG preconditioner's network (numpy, FP64 sums).
+"""CPU oracle of the learned middle level of the QS CG preconditioner (numpy).
 
-TEST INFRASTRUCTURE ONLY: tests compare the CUDA forward/backward kernels of
-peridigm_b200/csrc/k_mpnn.cu against this restatement. The network has no
-counterpart in the reference; this file restates the network the CUDA code
-defines (hidden 64, 3 mean-aggregation message-passing layers with residual
-connections, BF16 weights and BF16 stored activations):
+TEST INFRASTRUCTURE ONLY: tests compare the CUDA kernels of
+peridigm_b200/csrc/k_mpnn.cu against this restatement. The preconditioner has
+no counterpart in the reference; this file restates the one the CUDA code
+defines:
 
-  f   = (a / s_a, r / s_r)                     s = rms over all 3n entries
-  h0  = bf16(relu(W0 f + b0))
-  h_l = bf16(h_{l-1} + relu(Ws_l h_{l-1} + Wn_l m_l + b_l)),  m_l = mean_{j in N(i)} h_{l-1, j}
-  out = Wd h3 + bd,   z = a + s_a out
+  z = a + z0 + Q S G^T G S Q^T r        a = P_bj r, z0 = the coarse correction
 
-Two training losses are restated: the error-space L = |z - e|^2 / |e|^2
-(loss_grad) and the residual-space L = |K z - r|^2 / |r|^2 with prescribed
-dofs zeroed (loss_grad_residual), the one the CUDA trainer minimises.
-Gradients treat the BF16 roundings as identity (straight-through), as the
-kernels do.
+  patches: the non-empty cells (cell order, x fastest) of a grid of side
+           `side` from the coordinate minimum, dims = floor(extent / side) + 1;
+           neighbors of a patch: the non-empty cells of its 3x3x3
+           neighborhood (itself excluded), z then y then x ascending
+  Q:       piecewise constant from patches to the free dofs of their points
+  S:       s_I = sqrt(sum_{i in I} sum_{c free} (D_i^-1)_cc / 3) / |I|
+  G:       h0 = W0 v,  h_l = h_{l-1} + Ws_l h_{l-1} + Wn_l mean_{J in N(I)} h_{l-1,J}
+
+with BF16 weights (activations and sums in FP64 here, FP32 on the device).
+Loss (pairs r = K e): the energy-norm error left by one optimally scaled
+step, L = 1 - (r.z)^2 / ((z.K z)(e.r)), prescribed dofs of z, r and e zeroed;
+the gradient of <g_c, G^T G v> is the sum of two backward passes of G.
 """
 from __future__ import annotations
 
 import numpy as np
 
-H, F, NL = 64, 6, 3
-OFF_W0, OFF_B0 = 0, H * F
-OFF_L = OFF_B0 + H
-LSZ = 2 * H * H + H
-OFF_WD = OFF_L + NL * LSZ
-OFF_BD = OFF_WD + 3 * H
-NPARAM = OFF_BD + 3
+H, NL = 64, 3
+OFF_W0 = 0
+OFF_L = 3 * H
+LSZ = 2 * H * H
+NPARAM = OFF_L + NL * LSZ
 
 
 def bf16(x):
@@ -41,167 +42,137 @@ def bf16(x):
 
 def unpack(w):
     w = np.asarray(w, dtype=np.float64)
-    W0 = w[OFF_W0:OFF_B0].reshape(H, F)
-    b0 = w[OFF_B0:OFF_L]
+    W0 = w[OFF_W0:OFF_L].reshape(H, 3)
     layers = []
     for l in range(NL):
         o = OFF_L + l * LSZ
-        layers.append((w[o:o + H * H].reshape(H, H), w[o + H * H:o + 2 * H * H].reshape(H, H),
-                       w[o + 2 * H * H:o + LSZ]))
-    Wd = w[OFF_WD:OFF_BD].reshape(3, H)
-    bd = w[OFF_BD:OFF_BD + 3]
-    return W0, b0, layers, Wd, bd
+        layers.append((w[o:o + H * H].reshape(H, H), w[o + H * H:o + 2 * H * H].reshape(H, H)))
+    return W0, layers
 
 
-def loss_grad(w, a, r, e, mrow, mcol, round_bf16=True):
-    """Loss and gradient (length NPARAM) of one pair; a, r, e are [3n] float32."""
-    rnd = bf16 if round_bf16 else (lambda v: np.asarray(v, dtype=np.float32))
-    wb = rnd(np.asarray(w, np.float32)).astype(np.float64)
-    W0, b0, layers, Wd, bd = unpack(wb)
-    n = len(mrow) - 1
-    a = np.asarray(a, np.float32).reshape(n, 3)
-    r = np.asarray(r, np.float32).reshape(n, 3)
-    e = np.asarray(e, np.float32).reshape(n, 3).astype(np.float64)
-    sa = np.sqrt(np.sum(a.astype(np.float64) ** 2) / (3 * n))
-    sr = np.sqrt(np.sum(r.astype(np.float64) ** 2) / (3 * n))
-    ia, ir = np.float32(1.0 / sa), np.float32(1.0 / sr)
-    f = np.concatenate([a * ia, r * ir], axis=1).astype(np.float64)
-    deg = np.diff(mrow).astype(np.float64)
-    owner = np.repeat(np.arange(n), np.diff(mrow))
+def patches(x, side):
+    """(patch of each point, neighbor lists) of the patch graph."""
+    x = np.asarray(x, np.float64).reshape(-1, 3)
+    lo, hi = x.min(0), x.max(0)
+    dims = np.floor((hi - lo) / side).astype(np.int64) + 1
+    c = np.clip(np.floor((x - lo) / side).astype(np.int64), 0, dims - 1)
+    cid = (c[:, 2] * dims[1] + c[:, 1]) * dims[0] + c[:, 0]
+    cells = np.unique(cid)
+    pid = np.searchsorted(cells, cid)
+    where = {int(q): k for k, q in enumerate(cells)}
+    nbrs = []
+    for q in cells:
+        cx, cy, cz = q % dims[0], (q // dims[0]) % dims[1], q // (dims[0] * dims[1])
+        out = []
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    if dx == 0 and dy == 0 and dz == 0:
+                        continue
+                    X, Y, Z = cx + dx, cy + dy, cz + dz
+                    if X < 0 or Y < 0 or Z < 0 or X >= dims[0] or Y >= dims[1] or Z >= dims[2]:
+                        continue
+                    k = where.get(int((Z * dims[1] + Y) * dims[0] + X))
+                    if k is not None:
+                        out.append(k)
+        nbrs.append(out)
+    return pid, nbrs
 
-    def mean_agg(h):
-        m = np.zeros_like(h)
-        np.add.at(m, owner, h[mcol])
-        return m / np.maximum(deg, 1.0)[:, None]
 
-    pre0 = f @ W0.T + b0
-    hs = [rnd(np.maximum(pre0, 0.0)).astype(np.float64)]
-    pres, ms = [], []
-    for (Ws, Wn, b) in layers:
-        h = hs[-1]
-        m = mean_agg(h)
-        pre = h @ Ws.T + m @ Wn.T + b
-        pres.append(pre)
-        ms.append(m)
-        hs.append(rnd(h + np.maximum(pre, 0.0)).astype(np.float64))
-    out = hs[-1] @ Wd.T + bd
-    z = a.astype(np.float64) + sa * out
-    e2 = np.sum(e * e)
-    L = float(np.sum((z - e) ** 2) / e2)
-    # backward
+def scales(dinv_blocks, pid, fixed_dofs=()):
+    """s_I from the block-Jacobi inverse blocks [n, 3, 3], prescribed dofs left
+    out (rounded to float32)."""
+    npatch = int(pid.max()) + 1
+    dg = np.einsum("nii->ni", np.asarray(dinv_blocks, np.float64)).copy()
+    dg.ravel()[list(fixed_dofs)] = 0.0
+    tr = dg.sum(1) / 3.0
+    s = np.bincount(pid, tr, npatch)
+    cnt = np.bincount(pid, minlength=npatch)
+    return (np.sqrt(s) / cnt).astype(np.float32).astype(np.float64)
+
+
+def _mean_matrix(nbrs):
+    n = len(nbrs)
+    A = np.zeros((n, n))
+    for i, js in enumerate(nbrs):
+        for j in js:
+            A[i, j] += 1.0 / len(js)
+    return A
+
+
+def _q(pid, fixed, npatch):
+    n = pid.size
+    Q = np.zeros((3 * n, 3 * npatch))
+    for i in range(n):
+        for c in range(3):
+            if not fixed[3 * i + c]:
+                Q[3 * i + c, 3 * pid[i] + c] = 1.0
+    return Q
+
+
+def forward(wb, v, Am):
+    """G v for v [np, 3]; returns the output and the saved (h_{l-1}, mean) pairs."""
+    W0, layers = unpack(wb)
+    h = v @ W0.T
+    saved = []
+    for Ws, Wn in layers:
+        m = Am @ h
+        saved.append((h, m))
+        h = h + h @ Ws.T + m @ Wn.T
+    return h, saved
+
+
+def transpose(wb, y, Am):
+    """G^T y for y [np, 64]; returns [np, 3]."""
+    W0, layers = unpack(wb)
+    x = y
+    for Ws, Wn in reversed(layers):
+        x = x + x @ Ws + Am.T @ (x @ Wn)
+    return x @ W0
+
+
+def backward(wb, v, saved, U, Am):
+    """Gradient of <U, G v> with respect to the weights (length NPARAM)."""
+    W0, layers = unpack(wb)
     g = np.zeros(NPARAM)
-    gout = 2.0 * sa * (z - e) / e2
-    g[OFF_WD:OFF_BD] = (gout.T @ hs[-1]).ravel()
-    g[OFF_BD:OFF_BD + 3] = gout.sum(0)
-    dh = gout @ Wd
+    cur = U
     for l in range(NL - 1, -1, -1):
-        Ws, Wn, b = layers[l]
-        dpre = dh * (pres[l] > 0)
+        Ws, Wn = layers[l]
+        h, m = saved[l]
         o = OFF_L + l * LSZ
-        g[o:o + H * H] = (dpre.T @ hs[l]).ravel()
-        g[o + H * H:o + 2 * H * H] = (dpre.T @ ms[l]).ravel()
-        g[o + 2 * H * H:o + LSZ] = dpre.sum(0)
-        dm = (dpre @ Wn) / np.maximum(deg, 1.0)[:, None]
-        dprev = dh + dpre @ Ws
-        np.add.at(dprev, mcol, dm[owner])
-        dh = dprev
-    dpre0 = dh * (pre0 > 0)
-    g[OFF_W0:OFF_B0] = (dpre0.T @ f).ravel()
-    g[OFF_B0:OFF_L] = dpre0.sum(0)
-    return L, g
-
-
-def loss_grad_residual(w, a, r, K, fixed_dofs, mrow, mcol, round_bf16=True):
-    """Residual-space loss L = |K z - r|^2 / |r|^2 (z = a + s_a out, prescribed
-    dofs of z and r zero) and its gradient; K is a dense tangent [3n, 3n]."""
-    wb = (bf16 if round_bf16 else (lambda v: np.asarray(v, np.float32)))(np.asarray(w, np.float32))
-    n = len(mrow) - 1
-    a32 = np.asarray(a, np.float32)
-    r32 = np.asarray(r, np.float32)
-    fixed = np.zeros(3 * n, bool)
-    fixed[list(fixed_dofs)] = True
-    # forward through the shared network body, with a target-free pass
-    L0, _, aux = _forward(wb, a32, r32, mrow, mcol, round_bf16)
-    z = a32.astype(np.float64) + aux["sa"] * aux["out"].ravel()
-    z[fixed] = 0.0
-    rr = r32.astype(np.float64).copy()
-    rr[fixed] = 0.0
-    res = K @ z - rr
-    res[fixed] = 0.0
-    r2 = float(rr @ rr)
-    L = float(res @ res) / r2
-    dz = 2.0 * (K.T @ res) / r2
-    dz[fixed] = 0.0
-    gout = (aux["sa"] * dz).reshape(n, 3)
-    return L, _backward(wb, gout, aux, mrow, mcol)
-
-
-def _forward(wb, a, r, mrow, mcol, round_bf16):
-    rnd = bf16 if round_bf16 else (lambda v: np.asarray(v, dtype=np.float32))
-    W0, b0, layers, Wd, bd = unpack(np.asarray(wb, np.float64))
-    n = len(mrow) - 1
-    a = a.reshape(n, 3)
-    r = r.reshape(n, 3)
-    sa = np.sqrt(np.sum(a.astype(np.float64) ** 2) / (3 * n))
-    sr = np.sqrt(np.sum(r.astype(np.float64) ** 2) / (3 * n))
-    ia, ir = np.float32(1.0 / sa), np.float32(1.0 / sr)
-    f = np.concatenate([a * ia, r * ir], axis=1).astype(np.float64)
-    deg = np.diff(mrow).astype(np.float64)
-    owner = np.repeat(np.arange(n), np.diff(mrow))
-
-    def mean_agg(h):
-        m = np.zeros_like(h)
-        np.add.at(m, owner, h[mcol])
-        return m / np.maximum(deg, 1.0)[:, None]
-
-    pre0 = f @ W0.T + b0
-    hs = [rnd(np.maximum(pre0, 0.0)).astype(np.float64)]
-    pres, ms = [], []
-    for (Ws, Wn, b) in layers:
-        h = hs[-1]
-        m = mean_agg(h)
-        pre = h @ Ws.T + m @ Wn.T + b
-        pres.append(pre)
-        ms.append(m)
-        hs.append(rnd(h + np.maximum(pre, 0.0)).astype(np.float64))
-    out = hs[-1] @ Wd.T + bd
-    aux = dict(sa=sa, f=f, pre0=pre0, hs=hs, pres=pres, ms=ms, out=out, deg=deg, owner=owner)
-    return 0.0, None, aux
-
-
-def _backward(wb, gout, aux, mrow, mcol):
-    W0, b0, layers, Wd, bd = unpack(np.asarray(wb, np.float64))
-    hs, pres, ms, deg, owner = aux["hs"], aux["pres"], aux["ms"], aux["deg"], aux["owner"]
-    g = np.zeros(NPARAM)
-    g[OFF_WD:OFF_BD] = (gout.T @ hs[-1]).ravel()
-    g[OFF_BD:OFF_BD + 3] = gout.sum(0)
-    dh = gout @ Wd
-    for l in range(NL - 1, -1, -1):
-        Ws, Wn, b = layers[l]
-        dpre = dh * (pres[l] > 0)
-        o = OFF_L + l * LSZ
-        g[o:o + H * H] = (dpre.T @ hs[l]).ravel()
-        g[o + H * H:o + 2 * H * H] = (dpre.T @ ms[l]).ravel()
-        g[o + 2 * H * H:o + LSZ] = dpre.sum(0)
-        dm = (dpre @ Wn) / np.maximum(deg, 1.0)[:, None]
-        dprev = dh + dpre @ Ws
-        np.add.at(dprev, mcol, dm[owner])
-        dh = dprev
-    dpre0 = dh * (aux["pre0"] > 0)
-    g[OFF_W0:OFF_B0] = (dpre0.T @ aux["f"]).ravel()
-    g[OFF_B0:OFF_L] = dpre0.sum(0)
+        g[o:o + H * H] += (cur.T @ h).ravel()
+        g[o + H * H:o + 2 * H * H] += (cur.T @ m).ravel()
+        cur = cur + cur @ Ws + Am.T @ (cur @ Wn)
+    g[OFF_W0:OFF_L] += (cur.T @ v).ravel()
     return g
 
 
-def subgraph(x, row, col, radius, bond_damage=None):
-    """Bonds shorter than radius, in bond-family order (the kernel's subgraph)."""
-    P = np.asarray(x, float).reshape(-1, 3)
-    n = len(P)
-    owner = np.repeat(np.arange(n), np.diff(row))
-    d = P[col] - P[owner]
-    keep = np.einsum("ij,ij->i", d, d) <= radius * radius
-    if bond_damage is not None:
-        keep &= np.asarray(bond_damage) == 0
-    mrow = np.zeros(n + 1, np.int64)
-    np.cumsum(np.bincount(owner[keep], minlength=n), out=mrow[1:])
-    return mrow, np.asarray(col)[keep].astype(np.int64)
+def loss_grad(w, a, r, e, K, fixed_dofs, pid, nbrs, scale, z0=None, round_bf16=True):
+    """L = 1 - (r.z)^2 / ((z.K z)(e.r)), z = a + z0 + Q S G^T G S Q^T r, and dL/dw."""
+    wb = (bf16(np.asarray(w, np.float32)) if round_bf16 else np.asarray(w, np.float32)).astype(np.float64)
+    n = pid.size
+    npatch = int(pid.max()) + 1
+    fixed = np.zeros(3 * n, bool)
+    fixed[list(fixed_dofs)] = True
+    Am = _mean_matrix(nbrs)
+    Q = _q(pid, fixed, npatch)
+    S = np.repeat(np.asarray(scale, np.float64), 3)
+    rr = np.asarray(r, np.float32).astype(np.float64)
+    rr[fixed] = 0.0
+    ee = np.asarray(e, np.float32).astype(np.float64)
+    ee[fixed] = 0.0
+    v0 = (S * (Q.T @ rr)).reshape(npatch, 3)
+    y0, sv0 = forward(wb, v0, Am)
+    z = np.asarray(a, np.float32).astype(np.float64) + Q @ (S * transpose(wb, y0, Am).ravel())
+    if z0 is not None:
+        z = z + np.asarray(z0, np.float64)
+    z[fixed] = 0.0
+    kz = K @ z
+    A, B, E = float(rr @ z), float(z @ kz), float(ee @ rr)
+    L = 1.0 - A * A / (B * E)
+    gz = -2.0 * A / (B * E) * rr + 2.0 * A * A / (B * B * E) * kz
+    gz[fixed] = 0.0
+    v1 = (S * (Q.T @ gz)).reshape(npatch, 3)
+    y1, sv1 = forward(wb, v1, Am)
+    g = backward(wb, v0, sv0, y1, Am) + backward(wb, v1, sv1, y0, Am)
+    return L, g

@@ -340,6 +340,48 @@ def qs_solve(x, vol, row, col, K, mu, horizon, bc, times, tol, max_iter=50, u0=N
     return out
 
 
+def coarse_aggregates(x, horizon_max, cell=0.0, max_coarse=6144):
+    """Aggregates of the two-level preconditioner (no reference counterpart):
+    the non-empty cells, numbered in cell order (x fastest), of a grid of side
+    max(cell, 2 * max horizon * (1 + 1e-6)) from the coordinate minimum, dims =
+    floor(extent / side) + 1 per axis, the side grown 1.25x until there are at
+    most max_coarse / 3 aggregates. Returns (aggregate of each point, side)."""
+    x = _f64(x).reshape(-1, 3)
+    lo, hi = x.min(axis=0), x.max(axis=0)
+    side = max(float(cell), 2.0 * float(horizon_max) * (1.0 + 1.0e-6))
+    while True:
+        dims = np.floor((hi - lo) / side).astype(np.int64) + 1
+        if 3 * min(int(np.prod(dims)), x.shape[0]) > 64 * max_coarse:  # far too fine: grow before binning
+            side *= 1.25
+            continue
+        c = np.clip(np.floor((x - lo) / side).astype(np.int64), 0, dims - 1)
+        cid = (c[:, 2] * dims[1] + c[:, 1]) * dims[0] + c[:, 0]
+        cells = np.unique(cid)
+        if 3 * cells.size <= max_coarse:
+            return np.searchsorted(cells, cid).astype(np.int32), side
+        side *= 1.25
+
+
+def coarse_operator(T, agg, fixed_dofs=()):
+    """Galerkin coarse matrix P0^T T P0 of the two-level preconditioner: P0 maps
+    coarse dof 3I + c to component c of the free dofs of the points of aggregate
+    I (piecewise-constant translations, prescribed dofs excluded); a coarse dof
+    with no free fine dof gets a unit diagonal. Returns (Ac, P0)."""
+    agg = np.asarray(agg, np.int64)
+    n = agg.size
+    nc = 3 * (int(agg.max()) + 1)
+    P = np.zeros((3 * n, nc))
+    for i in range(n):
+        for c in range(3):
+            P[3 * i + c, 3 * agg[i] + c] = 1.0
+    P[list(fixed_dofs), :] = 0.0
+    A = P.T @ T @ P
+    for k in range(nc):
+        if A[k, k] == 0.0:
+            A[k, k] = 1.0
+    return A, P
+
+
 def critical_time_step(x, vol, row, col, K, rho, horizon):
     x, vol = _f64(x), _f64(vol)
     n = vol.size

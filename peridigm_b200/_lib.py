@@ -65,12 +65,13 @@ class Stats(C.Structure):
 PD_PRECOND_NONE = 0
 PD_PRECOND_BLOCK_JACOBI = 1
 PD_PRECOND_MPNN = 2
+PD_PRECOND_TWO_LEVEL = 3
 
 
 class QsOptions(C.Structure):
     _fields_ = [("newton_tolerance", C.c_double), ("cg_relative_tolerance", C.c_double),
                 ("max_newton_iterations", C.c_int32), ("max_cg_iterations", C.c_int32),
-                ("preconditioner", C.c_int32), ("use_predictor", C.c_int32)]
+                ("preconditioner", C.c_int32), ("use_predictor", C.c_int32), ("coarse_cell", C.c_double)]
 
 
 # name -> (restype, argtypes); every symbol include/pd_b200.h declares.
@@ -120,6 +121,8 @@ SIGNATURES = {
     "pd_mpnn_get_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "pd_mpnn_set_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "pd_mpnn_loss_grad": (C.c_int, [_vp, C.POINTER(C.c_float), _dp, C.POINTER(C.c_float)]),
+    "pd_mpnn_coarse": (C.c_int, [_vp, C.c_double]),
+    "pd_qs_coarse_operator": (C.c_int, [_vp, _dp, C.c_double, _i64p, _i32p, _dp, _dp]),
     "pd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "pd_get_kernel_timing": (C.c_int, [_vp, _dp, _i64p]),
 }

@@ -236,15 +236,19 @@ class Context:
 
     # -- quasi-static --------------------------------------------------------
     def qs_load_step(self, t_prev, t_cur, newton_tolerance, cg_relative_tolerance=1e-8, max_newton=20,
-                     max_cg=20000, preconditioner="block_jacobi", use_predictor=True, stats=None):
+                     max_cg=20000, preconditioner="block_jacobi", use_predictor=True, stats=None, coarse_cell=0.0):
+        """One load step; preconditioner "none", "block_jacobi", "two_level" (block Jacobi + aggregate
+        coarse correction, cells of side max(coarse_cell, 2 * max horizon)) or "mpnn" (the learned
+        correction on the base set by mpnn_coarse)."""
         o = _lib.QsOptions()
         o.newton_tolerance = float(newton_tolerance)
         o.cg_relative_tolerance = float(cg_relative_tolerance)
         o.max_newton_iterations = int(max_newton)
         o.max_cg_iterations = int(max_cg)
         o.preconditioner = {"none": _lib.PD_PRECOND_NONE, "block_jacobi": _lib.PD_PRECOND_BLOCK_JACOBI,
-                            "mpnn": _lib.PD_PRECOND_MPNN}[preconditioner]
+                            "mpnn": _lib.PD_PRECOND_MPNN, "two_level": _lib.PD_PRECOND_TWO_LEVEL}[preconditioner]
         o.use_predictor = 1 if use_predictor else 0
+        o.coarse_cell = float(coarse_cell)
         st = stats if stats is not None else _lib.Stats()
         self._ok(self.L.pd_qs_load_step(self.h, float(t_prev), float(t_cur), C.cast(C.byref(o), C.c_void_p),
                                         C.byref(st)))
@@ -262,10 +266,27 @@ class Context:
         self._ok(self.L.pd_jacobian_block_diagonal(self.h, _d(u), _d(b)))
         return b.reshape(self.n, 3, 3)
 
+    def coarse_operator(self, u, cell=0.0):
+        """(aggregate of each point, assembled P0^T K P0, its inverse) of the two-level preconditioner
+        at displacement u."""
+        u = _f64(u, 3 * self.n, "u")
+        nc = C.c_int64(0)
+        self._ok(self.L.pd_qs_coarse_operator(self.h, _d(u), float(cell), C.byref(nc), None, None, None))
+        agg = np.zeros(self.n, dtype=np.int32)
+        A = np.zeros((nc.value, nc.value))
+        Ai = np.zeros((nc.value, nc.value))
+        self._ok(self.L.pd_qs_coarse_operator(self.h, _d(u), float(cell), C.byref(nc),
+                                              agg.ctypes.data_as(C.POINTER(C.c_int32)), _d(A), _d(Ai)))
+        return agg, A, Ai
+
     # -- learned preconditioner ----------------------------------------------
-    def mpnn_init(self, seed=0, radius=None):
-        """Initialise the network on the subgraph of bonds shorter than radius."""
-        self._ok(self.L.pd_mpnn_init(self.h, int(seed), float(radius)))
+    def mpnn_coarse(self, cell=0.0):
+        """cell >= 0: the network corrects the two-level preconditioner; < 0: block Jacobi alone."""
+        self._ok(self.L.pd_mpnn_coarse(self.h, float(cell)))
+
+    def mpnn_init(self, seed=0, patch=None):
+        """Initialise the learned middle level on patches (grid cells) of side `patch`."""
+        self._ok(self.L.pd_mpnn_init(self.h, int(seed), float(patch)))
 
     def mpnn_collect(self, every):
         self._ok(self.L.pd_mpnn_collect(self.h, int(every)))
@@ -295,8 +316,9 @@ class Context:
         w = np.ascontiguousarray(w, dtype=np.float32)
         self._ok(self.L.pd_mpnn_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
 
-    def mpnn_loss_grad(self, a, r):
-        pair = np.ascontiguousarray(np.concatenate([a, r]), dtype=np.float32)
+    def mpnn_loss_grad(self, a, r, e):
+        """Loss and weight gradient for one pair (a = P_bj r, r = K e, e)."""
+        pair = np.ascontiguousarray(np.concatenate([a, r, e]), dtype=np.float32)
         loss = C.c_double()
         g = np.zeros(self.mpnn_num_params(), dtype=np.float32)
         self._ok(self.L.pd_mpnn_loss_grad(self.h, pair.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss),

@@ -212,6 +212,7 @@ int pd_destroy(pd_ctx* c) {
   contact_release(c);
   qs_release(c);
   mpnn_release(c);
+  coarse_release(c);
   for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
   if (c->vbeg) cudaEventDestroy(c->vbeg);
   cudaStream_t s = c->stream;
@@ -224,6 +225,7 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   CHECK_CTX(c);
   if (n <= 0 || n >= (int64_t(1) << 31) || !x || !vol) return fail(c, PD_ERR_ARG, "pd_set_points: bad arguments");
   TRY(ensure_device(c));
+  coarse_release(c);
   c->n = n;
   c->hx.assign(x, x + 3 * n);
   c->hvol.assign(vol, vol + n);
@@ -251,10 +253,12 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   c->col.release();
   c->nb = 0;
   c->wv_done = false;
+  coarse_release(c);
   c->h_bc_mask.assign(n, 0);
   c->h_bc_a.assign(3 * n, 0.0);
   c->h_bc_b.assign(3 * n, 0.0);
   c->bc_dirty = true;
+  coarse_invalidate(c);
   c->field_K.clear();
   c->field_mu.clear();
   c->field_sc.clear();
@@ -282,6 +286,7 @@ int pd_set_block_horizons(pd_ctx* c, int32_t n_blocks, const double* horizon) {
     c->block_h[b] = horizon[b];
   }
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -295,6 +300,7 @@ int pd_build_bonds(pd_ctx* c, const pd_plane_filter* filters, int32_t n_filters)
   TRY(upload_horizons(c));
   TRY(build_bonds_device(c, filters, n_filters));
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -328,6 +334,7 @@ int pd_set_bonds(pd_ctx* c, const int32_t* nl, int64_t len) {
   if (c->hp.count < (size_t)c->n) TRY(upload_horizons(c));
   TRY(finalize_bonds(c, false));
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -365,6 +372,7 @@ int pd_material_lps(pd_ctx* c, int32_t block, double K, double mu, double rho) {
   c->block_rho[block] = rho;
   c->have_material = true;
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -376,6 +384,7 @@ int pd_material_lps_field(pd_ctx* c, const double* K, const double* mu) {
   c->field_K.assign(K, K + c->n);
   c->field_mu.assign(mu, mu + c->n);
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -384,6 +393,7 @@ int pd_damage_critical_stretch(pd_ctx* c, int32_t block, double s_c) {
   if (block < 0 || block >= (int32_t)c->block_sc.size()) return fail(c, PD_ERR_ARG, "pd_damage_critical_stretch: bad block");
   c->block_sc[block] = s_c;
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -392,6 +402,7 @@ int pd_damage_critical_stretch_field(pd_ctx* c, const double* s_c) {
   if (c->n == 0 || !s_c) return fail(c, PD_ERR_ARG, "pd_damage_critical_stretch_field: bad arguments");
   c->field_sc.assign(s_c, s_c + c->n);
   c->wv_done = false;
+  coarse_release(c);
   return PD_OK;
 }
 
@@ -455,6 +466,7 @@ int pd_set_bond_damage(pd_ctx* c, const double* bd) {
   TRY(ensure_device(c));
   PD_CUDA_TRY(c, h2d(c, c->dmg.p, h.data(), (size_t)c->nb));
   c->trial_valid = false;
+  coarse_invalidate(c);
   return PD_OK;
 }
 
@@ -499,6 +511,7 @@ int pd_add_prescribed_displacement(pd_ctx* c, int64_t np, const int64_t* pts, in
     c->h_bc_b[3 * i + coord] = b;
   }
   c->bc_dirty = true;
+  coarse_invalidate(c);
   return PD_OK;
 }
 
@@ -506,6 +519,7 @@ int pd_clear_boundary_conditions(pd_ctx* c) {
   CHECK_CTX(c);
   std::fill(c->h_bc_mask.begin(), c->h_bc_mask.end(), 0);
   c->bc_dirty = true;
+  coarse_invalidate(c);
   return PD_OK;
 }
 
@@ -672,18 +686,18 @@ int pd_unpack_state_device(pd_ctx* c, int64_t n_idx, const int32_t* idx_dev, con
 int pd_qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {
   CHECK_CTX(c);
   if (!o) return fail(c, PD_ERR_ARG, "pd_qs_load_step: null options");
-  if (!(t_cur > t_prev) || o->preconditioner < 0 || o->preconditioner > 2 || o->max_cg_iterations <= 0 ||
+  if (!(t_cur > t_prev) || o->preconditioner < 0 || o->preconditioner > 3 || o->max_cg_iterations <= 0 ||
       o->max_newton_iterations < 0 || !(o->cg_relative_tolerance > 0.0))
     return fail(c, PD_ERR_ARG, "pd_qs_load_step: bad options");
   if (!c->state_init) TRY(pd_set_state(c, nullptr, nullptr));
   return qs_load_step(c, t_prev, t_cur, o, st);
 }
 
-int pd_mpnn_init(pd_ctx* c, uint64_t seed, double radius) {
+int pd_mpnn_init(pd_ctx* c, uint64_t seed, double patch) {
   CHECK_CTX(c);
-  if (!(radius > 0.0)) return fail(c, PD_ERR_ARG, "pd_mpnn_init: radius must be positive");
+  if (!(patch > 0.0) || !std::isfinite(patch)) return fail(c, PD_ERR_ARG, "pd_mpnn_init: patch side must be positive");
   TRY(ensure_ready(c));
-  return mpnn_init(c, seed, radius);
+  return mpnn_init(c, seed, patch);
 }
 
 int pd_mpnn_collect(pd_ctx* c, int32_t every) {
@@ -724,6 +738,41 @@ int pd_mpnn_set_weights(pd_ctx* c, const float* w) {
   if (!w) return fail(c, PD_ERR_ARG, "null weights");
   TRY(ensure_device(c));
   return mpnn_set_weights(c, w);
+}
+
+int pd_mpnn_coarse(pd_ctx* c, double cell) {
+  CHECK_CTX(c);
+  if (!std::isfinite(cell)) return fail(c, PD_ERR_ARG, "pd_mpnn_coarse: cell must be finite");
+  return mpnn_set_coarse(c, cell);
+}
+
+int pd_qs_coarse_operator(pd_ctx* c, const double* u, double cell, int64_t* n_coarse, int32_t* aggregate, double* A,
+                          double* A_inv) {
+  CHECK_CTX(c);
+  if (!u || !n_coarse || !std::isfinite(cell)) return fail(c, PD_ERR_ARG, "pd_qs_coarse_operator: bad arguments");
+  TRY(ensure_ready(c));
+  DBuf<double> ud;
+  PD_CUDA_TRY(c, ud.alloc(3 * c->n));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(ud.p, u, 3 * c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int64_t nc = 0;
+  TRY(qs_coarse_operator(c, ud.p, cell, &nc, nullptr, nullptr, nullptr));
+  const bool want = aggregate || A || A_inv;
+  if (want && *n_coarse < nc) {
+    *n_coarse = nc;
+    return fail(c, PD_ERR_ARG, "pd_qs_coarse_operator: n_coarse on entry is smaller than the coarse space");
+  }
+  *n_coarse = nc;
+  if (!want) return check_status(c);
+  DBuf<int32_t> ag;
+  DBuf<double> ad, ai;
+  PD_CUDA_TRY(c, ag.alloc(c->n));
+  PD_CUDA_TRY(c, ad.alloc((size_t)nc * nc));
+  PD_CUDA_TRY(c, ai.alloc((size_t)nc * nc));
+  TRY(qs_coarse_operator(c, ud.p, cell, &nc, ag.p, ad.p, ai.p));
+  if (aggregate) PD_CUDA_TRY(c, d2h(c, aggregate, ag.p, c->n * sizeof(int32_t)));
+  if (A) PD_CUDA_TRY(c, d2h(c, A, ad.p, (size_t)nc * nc * sizeof(double)));
+  if (A_inv) PD_CUDA_TRY(c, d2h(c, A_inv, ai.p, (size_t)nc * nc * sizeof(double)));
+  return check_status(c);
 }
 
 int pd_mpnn_loss_grad(pd_ctx* c, const float* pair, double* loss, float* grad) {

@@ -1,0 +1,579 @@
+// Aggregate coarse space of the quasi-static CG preconditioners (sm_100a).
+// No counterpart in the reference (Peridigm's CG is unpreconditioned or block
+// Jacobi, src/core/Peridigm.cpp:2740, 1603-1646); it is the coarse level of the
+// two-level and learned preconditioners:
+//
+//   z = P_bj r + P0 Ac^-1 P0^T r  (+ the network's correction, k_mpnn.cu)
+//
+// P0: piecewise-constant translations on aggregates = the non-empty cells of a
+// grid of side >= 2 * max horizon (3 coarse dofs per aggregate, prescribed dofs
+// excluded). Ac = P0^T K P0 is the exact Galerkin product with the tangent K of
+// k_qs.cu, assembled from the bonds without forming K:
+//
+//   K w|_i = -V_i [ sum_j V_j B_ij (w_j - w_i) + q_i dth_i H_i + sum_j h_ij q_j dth_j ]
+//   B_ij = om (a_i + a_j) Yh Yh^T + (T_ij / |Y|) (I - Yh Yh^T)
+//   h_ij = V_j om zeta Yh,  H_i = sum_j h_ij,  dth_i = sum_j g_ij . (w_j - w_i),
+//   g_ij = 3 om zeta V_j Yh / m_i
+//
+// (om = omega(zeta, horizon of the bond's owner), a = alpha, q = 3K/m - alpha/3,
+// T_ij the force-state sum of k_qs_df). The pair term couples each point to its
+// bonds; the dilatation term is a sum of rank-one terms, one per point p,
+// (force response to dth_p) x (dth_p as a function of w). A family of radius
+// delta spans at most 2 cells per axis of a grid of side >= 2 delta, so every
+// point's contributions fall in 8 "slots" (the 2x2x2 cells from the cell of
+// x_p - delta); k_coarse_point sums them per slot, k_coarse_rows adds them into
+// the dense Ac one aggregate row per warp in a fixed order (deterministic, no
+// atomics). Ac is inverted in place by blocked Gauss-Jordan (SPD, no pivoting)
+// and applied as a dense matrix-vector product. Bond damage is taken as
+// symmetric (d_ij = d_ji), as the critical-stretch law produces it.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "cells.cuh"
+#include "pd_internal.cuh"
+
+namespace pdb {
+
+constexpr int kSlots = 8;
+constexpr int kSlotVals = 15;  // pair 3x3 (9), force response a (3), dtheta functional b (3)
+constexpr int kGjB = 64;       // Gauss-Jordan block
+constexpr int kMaxCoarse = 6144;
+
+struct CoarseState {
+  bool built = false;      // aggregates
+  bool have_op = false;    // Ac^-1 ready
+  double cell = 0.0;
+  Grid g;
+  int64_t n = 0, nagg = 0;
+  int nc = 0;
+  DBuf<int32_t> sorted, agg_of, cell_agg, agg_cell, clo;
+  DBuf<int64_t> cstart;
+  DBuf<double> slots;      // [n][8][15]
+  DBuf<double> A;          // nc x nc, the inverse after coarse_build
+  DBuf<double> P, R, C;    // Gauss-Jordan work
+  DBuf<double> rc, zc;
+  DBuf<int> status;
+};
+
+__device__ __forceinline__ double co_omega(int kind, double zeta, double h) {
+  if (kind == PD_INFLUENCE_ONE) return 1.0;
+  if (kind == PD_INFLUENCE_PARABOLIC_DECAY) {
+    if (zeta > h) return 0.0;
+    const double s = zeta / h;
+    return s < 0.5 ? 1.0 : -4.0 * s * s + 4.0 * s;
+  }
+  return exp(-(zeta * zeta) / (h * h * 0.16));
+}
+
+__device__ __forceinline__ int slot_of(const Grid& g, const int lo[3], const double4& x, int* bad) {
+  const int dx = cell_coord(g, x.x, 0) - lo[0], dy = cell_coord(g, x.y, 1) - lo[1], dz = cell_coord(g, x.z, 2) - lo[2];
+  if ((unsigned)dx > 1u || (unsigned)dy > 1u || (unsigned)dz > 1u) {
+    *bad = 1;
+    return -1;
+  }
+  return dx + 2 * dy + 4 * dz;
+}
+
+// Per point p: slot sums of the pair rows of p, and of p's dilatation
+// rank-one term (a: rows, b: columns), prescribed dofs masked.
+__global__ void __launch_bounds__(128) k_coarse_point(int64_t n, const int64_t* __restrict__ row,
+                                                      const int32_t* __restrict__ col,
+                                                      const uint8_t* __restrict__ dmg,
+                                                      const double4* __restrict__ xv, const double4* __restrict__ y,
+                                                      const double4* __restrict__ ab, const double4* __restrict__ pt,
+                                                      const double* __restrict__ hp, int influence,
+                                                      const uint8_t* __restrict__ fixed, Grid g,
+                                                      int32_t* __restrict__ clo_out, double* __restrict__ out,
+                                                      int* __restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc[kSlots][kSlotVals];
+#pragma unroll
+  for (int s = 0; s < kSlots; ++s)
+#pragma unroll
+    for (int k = 0; k < kSlotVals; ++k) acc[s][k] = 0.0;
+  const double4 xi = xv[i], yi = y[i], ai = ab[i];
+  const double hi = hp[i], mi = pt[i].x, Vi = xi.w, qi = ai.y;
+  const uint8_t fi = fixed[i];
+  // slots: cells lo .. lo+1 per axis from the cell of x_i - reach
+  const double reach = hi * (1.0 + 1.0e-9);
+  int lo[3] = {cell_coord(g, xi.x - reach, 0), cell_coord(g, xi.y - reach, 1), cell_coord(g, xi.z - reach, 2)};
+  int bad = 0;
+  const int si = slot_of(g, lo, xi, &bad);
+  for (int64_t b = row[i]; b < row[i + 1] && !bad; ++b) {
+    if (dmg[b]) continue;
+    const int32_t j = col[b];
+    const double4 xj = xv[j], yj = y[j], aj = ab[j];
+    const double hj = hp[j], Vj = xj.w;
+    const uint8_t fj = fixed[j];
+    const int sj = slot_of(g, lo, xj, &bad);
+    if (bad) break;
+    const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
+    const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
+    const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
+    const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
+    const double e = dY - zeta;
+    const double yh[3] = {Y0 / dY, Y1 / dY, Y2 / dY};
+    const double omi = co_omega(influence, zeta, hi), omj = co_omega(influence, zeta, hj);
+    const double T = omi * (zeta * (ai.x * ai.y + aj.x * aj.y) + (ai.z + aj.z) * e);
+    const double tg = T / dY, ax = omi * (ai.z + aj.z) - tg;
+    const double vv = Vi * Vj;
+    const double gs = 3.0 * omi * zeta * Vj / mi;            // g_ij = gs * yh
+    const double ri = -Vi * qi * Vj * omi * zeta;            // row i of the dth_i response
+    const double rj = Vj * Vi * omj * zeta * qi;             // row j of the dth_i response
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const bool ci = !((fi >> c) & 1), cj = !((fj >> c) & 1);
+      if (ci) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double w = vv * (ax * yh[c] * yh[d] + (c == d ? tg : 0.0));
+          if (!((fj >> d) & 1)) acc[sj][3 * c + d] -= w;
+          if (!((fi >> d) & 1)) acc[si][3 * c + d] += w;
+        }
+        acc[si][9 + c] += ri * yh[c];
+      }
+      if (cj) acc[sj][9 + c] += rj * yh[c];
+      if (cj) acc[sj][12 + c] += gs * yh[c];
+      if (ci) acc[si][12 + c] -= gs * yh[c];
+    }
+  }
+  if (bad) atomicOr(status, ST_BAD_INDEX);
+  clo_out[4 * i] = lo[0];
+  clo_out[4 * i + 1] = lo[1];
+  clo_out[4 * i + 2] = lo[2];
+  clo_out[4 * i + 3] = si;
+  double* o = out + (size_t)i * kSlots * kSlotVals;
+#pragma unroll
+  for (int s = 0; s < kSlots; ++s)
+#pragma unroll
+    for (int k = 0; k < kSlotVals; ++k) o[s * kSlotVals + k] = acc[s][k];
+}
+
+// One warp per aggregate row I: Ac[I, J] for the 5x5x5 cells J around I,
+// accumulated in shared memory over the points of the 3x3x3 cells around I in
+// cell order (each lane owns fixed (slot, entry) items: deterministic).
+constexpr int kRowWarps = 4;
+__global__ void __launch_bounds__(32 * kRowWarps) k_coarse_rows(int64_t nagg, int nc, Grid g,
+                                                                 const int32_t* __restrict__ agg_cell,
+                                                                 const int32_t* __restrict__ cell_agg,
+                                                                 const int64_t* __restrict__ cstart,
+                                                                 const int32_t* __restrict__ sorted,
+                                                                 const int32_t* __restrict__ clo,
+                                                                 const double* __restrict__ slots,
+                                                                 double* __restrict__ A) {
+  __shared__ double acc[kRowWarps][125 * 9];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t I = (int64_t)blockIdx.x * kRowWarps + w;
+  if (I >= nagg) return;
+  double* s = acc[w];
+  for (int k = lane; k < 125 * 9; k += 32) s[k] = 0.0;
+  __syncwarp();
+  const int cell = agg_cell[I];
+  const int cx = cell % g.dims[0], cy = (cell / g.dims[0]) % g.dims[1], cz = cell / (g.dims[0] * g.dims[1]);
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int qx = cx + dx, qy = cy + dy, qz = cz + dz;
+        if (qx < 0 || qy < 0 || qz < 0 || qx >= g.dims[0] || qy >= g.dims[1] || qz >= g.dims[2]) continue;
+        const int q = (qz * g.dims[1] + qy) * g.dims[0] + qx;
+        const bool own_cell = (dx == 0 && dy == 0 && dz == 0);
+        for (int64_t t = cstart[q]; t < cstart[q + 1]; ++t) {
+          const int32_t p = sorted[t];
+          const int lx = clo[4 * p], ly = clo[4 * p + 1], lz = clo[4 * p + 2];
+          const int ox = cx - lx, oy = cy - ly, oz = cz - lz;
+          if ((unsigned)ox > 1u || (unsigned)oy > 1u || (unsigned)oz > 1u) continue;
+          const double* sp = slots + (size_t)p * kSlots * kSlotVals;
+          const int srow = ox + 2 * oy + 4 * oz;
+          const double a0 = sp[srow * kSlotVals + 9], a1 = sp[srow * kSlotVals + 10], a2 = sp[srow * kSlotVals + 11];
+          for (int it = lane; it < kSlots * 9; it += 32) {
+            const int sl = it / 9, cd = it - 9 * sl, c = cd / 3, d = cd - 3 * c;
+            const int jx = lx + (sl & 1) - cx + 2, jy = ly + ((sl >> 1) & 1) - cy + 2, jz = lz + (sl >> 2) - cz + 2;
+            const double av = c == 0 ? a0 : (c == 1 ? a1 : a2);
+            double v = av * sp[sl * kSlotVals + 12 + d];
+            if (own_cell) v += sp[sl * kSlotVals + cd];
+            s[((jz * 5 + jy) * 5 + jx) * 9 + cd] += v;
+          }
+          __syncwarp();
+        }
+      }
+  // write the row block
+  for (int jl = lane; jl < 125; jl += 32) {
+    const int jx = cx + jl % 5 - 2, jy = cy + (jl / 5) % 5 - 2, jz = cz + jl / 25 - 2;
+    if (jx < 0 || jy < 0 || jz < 0 || jx >= g.dims[0] || jy >= g.dims[1] || jz >= g.dims[2]) continue;
+    const int J = cell_agg[(jz * g.dims[1] + jy) * g.dims[0] + jx];
+    if (J < 0) continue;
+    for (int cd = 0; cd < 9; ++cd)
+      A[(size_t)(3 * I + cd / 3) * nc + 3 * J + cd % 3] = s[jl * 9 + cd];
+  }
+}
+
+// Coarse dofs with no free fine dof: identity rows.
+__global__ void k_coarse_unit_diag(int nc, double* __restrict__ A) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nc && A[(size_t)k * nc + k] == 0.0) A[(size_t)k * nc + k] = 1.0;
+}
+
+// aggregate id per cell (-1: empty) and cell of each aggregate, in cell order
+__global__ void k_coarse_cells(int64_t ncell, const int64_t* __restrict__ cstart, int32_t* __restrict__ cell_agg,
+                               int32_t* __restrict__ agg_cell, int64_t* __restrict__ nagg_out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int32_t k = 0;
+  for (int64_t q = 0; q < ncell; ++q) {
+    if (cstart[q + 1] > cstart[q]) {
+      cell_agg[q] = k;
+      agg_cell[k] = (int32_t)q;
+      ++k;
+    } else {
+      cell_agg[q] = -1;
+    }
+  }
+  *nagg_out = k;
+}
+
+__global__ void k_coarse_agg_of(int64_t n, const double4* __restrict__ xv, Grid g, const int32_t* __restrict__ cell_agg,
+                                int32_t* __restrict__ agg_of) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 p = xv[i];
+  agg_of[i] = cell_agg[(cell_coord(g, p.z, 2) * g.dims[1] + cell_coord(g, p.y, 1)) * g.dims[0] + cell_coord(g, p.x, 0)];
+}
+
+// ---------------------------------------------------------------------------
+// Dense SPD inverse: blocked in-place Gauss-Jordan (no pivoting), 64-wide steps
+//   P = A_kk^-1; R = P A_k* (new block row); C = A_*k (old block column);
+//   A_ij -= C_i R_j (i, j outside block k); A_kj = R_j; A_ik = -C_i P; A_kk = P
+// ---------------------------------------------------------------------------
+// P = inverse of the bk x bk diagonal block at k0 (one block of 256 threads).
+__global__ void __launch_bounds__(256) k_gj_pivot(int nc, int k0, int bk, const double* __restrict__ A,
+                                                  double* __restrict__ P) {
+  __shared__ double S[kGjB][kGjB + 1];
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int r = t / kGjB, c = t % kGjB;
+    S[r][c] = (r < bk && c < bk) ? A[(size_t)(k0 + r) * nc + k0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int k = 0; k < bk; ++k) {
+    const double p = 1.0 / S[k][k];
+    __syncthreads();
+    for (int c = threadIdx.x; c < bk; c += blockDim.x) S[k][c] = (c == k) ? p : S[k][c] * p;
+    __syncthreads();
+    for (int t = threadIdx.x; t < bk * bk; t += blockDim.x) {
+      const int r = t / bk, c = t % bk;
+      if (r != k && c != k) S[r][c] -= S[r][k] * S[k][c];
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < bk; r += blockDim.x)
+      if (r != k) S[r][k] = -S[r][k] * p;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < bk * bk; t += blockDim.x) P[t] = S[t / bk][t % bk];
+}
+
+// R[r][j] = sum_t P[r][t] A[k0+t][j] (bk x nc); C[i][t] = A[i][k0+t] (nc x bk).
+// Block x: 64 columns j (R) or 64 rows i (C, blocks past the R range).
+__global__ void __launch_bounds__(256) k_gj_panel(int nc, int k0, int bk, const double* __restrict__ A,
+                                                  const double* __restrict__ P, double* __restrict__ R,
+                                                  double* __restrict__ C) {
+  const int ntile = (nc + kGjB - 1) / kGjB;
+  if ((int)blockIdx.x >= ntile) {  // copy the old block column
+    const int i0 = ((int)blockIdx.x - ntile) * kGjB;
+    for (int t = threadIdx.x; t < kGjB * bk; t += blockDim.x) {
+      const int i = i0 + t / bk, c = t % bk;
+      if (i < nc) C[(size_t)i * bk + c] = A[(size_t)i * nc + k0 + c];
+    }
+    return;
+  }
+  __shared__ double sP[kGjB][kGjB + 1];
+  const int j0 = blockIdx.x * kGjB;
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int r = t / kGjB, c = t % kGjB;
+    sP[r][c] = (r < bk && c < bk) ? P[r * bk + c] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int r = t / kGjB, c = t % kGjB;
+    if (r >= bk || j0 + c >= nc) continue;
+    const double* a = A + (size_t)k0 * nc + j0 + c;
+    double s = 0.0;
+    for (int k = 0; k < bk; ++k) s = fma(sP[r][k], a[(size_t)k * nc], s);
+    R[(size_t)r * nc + j0 + c] = s;
+  }
+}
+
+// 64x64 output tiles, 4x4 per thread, k in chunks of 16.
+__global__ void __launch_bounds__(256) k_gj_update(int nc, int k0, int bk, double* __restrict__ A,
+                                                   const double* __restrict__ P, const double* __restrict__ R,
+                                                   const double* __restrict__ C) {
+  const int i0 = blockIdx.y * kGjB, j0 = blockIdx.x * kGjB;
+  const bool rowk = (i0 == k0), colk = (j0 == k0);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  if (rowk) {  // new block row (and the pivot block)
+    for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+      const int r = t / kGjB, c = t % kGjB;
+      if (r < bk && j0 + c < nc) A[(size_t)(i0 + r) * nc + j0 + c] = colk ? P[r * bk + c] : R[(size_t)r * nc + j0 + c];
+    }
+    return;
+  }
+  __shared__ double sC[kGjB][17], sR[16][kGjB + 1];
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int kc = 0; kc < bk; kc += 16) {
+    for (int t = threadIdx.x; t < kGjB * 16; t += blockDim.x) {
+      const int r = t / 16, k = t % 16;
+      sC[r][k] = (i0 + r < nc && kc + k < bk) ? C[(size_t)(i0 + r) * bk + kc + k] : 0.0;
+      const int kk = t / kGjB, c = t % kGjB;
+      double v = 0.0;
+      if (kc + kk < bk && j0 + c < nc && (!colk || c < bk))
+        v = colk ? P[(kc + kk) * bk + c] : R[(size_t)(kc + kk) * nc + j0 + c];
+      sR[kk][c] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      double cv[4], rv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) cv[a] = sC[ty + 16 * a][k];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) rv[b] = sR[k][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(cv[a], rv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      if (i >= nc || j >= nc || (colk && j - k0 >= bk)) continue;
+      double* o = A + (size_t)i * nc + j;
+      *o = colk ? -acc[a][b] : *o - acc[a][b];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Application: rc = P0^T r (warp per aggregate), zc = Ac^-1 rc (warp per row),
+// z += P0 zc on free dofs
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_coarse_restrict(int64_t nagg, const int32_t* __restrict__ agg_cell,
+                                  const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
+                                  const T* __restrict__ r, double* __restrict__ rc) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= nagg) return;
+  const int q = agg_cell[I];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+    const int64_t p = sorted[t];
+    s0 += (double)r[3 * p];
+    s1 += (double)r[3 * p + 1];
+    s2 += (double)r[3 * p + 2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) rc[3 * I] = s0, rc[3 * I + 1] = s1, rc[3 * I + 2] = s2;
+}
+
+__global__ void k_coarse_gemv(int nc, const double* __restrict__ A, const double* __restrict__ x,
+                              double* __restrict__ y) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= nc) return;
+  const double* a = A + (size_t)i * nc;
+  double s = 0.0;
+  for (int k = lane; k < nc; k += 32) s = fma(a[k], x[k], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) y[i] = s;
+}
+
+__global__ void k_coarse_prolong(int64_t n, const int32_t* __restrict__ agg_of, const double* __restrict__ zc,
+                                 double scale, const uint8_t* __restrict__ fixed, double* __restrict__ z) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t I = agg_of[i];
+  const uint8_t f = fixed[i];
+  for (int c = 0; c < 3; ++c)
+    if (!((f >> c) & 1)) z[3 * i + c] += scale * zc[3 * I + c];
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static CoarseState* co_state(pd_ctx* c) {
+  if (!c->coarse) c->coarse = new CoarseState();
+  return c->coarse;
+}
+
+void coarse_release(pd_ctx* c) {
+  delete c->coarse;
+  c->coarse = nullptr;
+}
+
+void coarse_invalidate(pd_ctx* c) {
+  if (c->coarse) c->coarse->have_op = false;
+}
+
+bool coarse_valid(const pd_ctx* c) { return c->coarse && c->coarse->have_op; }
+
+int64_t coarse_size(const pd_ctx* c) { return c->coarse && c->coarse->have_op ? c->coarse->nc : 0; }
+
+// Aggregates: the non-empty cells of a grid of side max(cell, 2 * max
+// horizon) over the model coordinates, the side grown by 1.25x until the
+// coarse space has at most kMaxCoarse dofs.
+static int co_aggregates(pd_ctx* c, CoarseState* s, double cell) {
+  const int64_t n = c->n;
+  double hmax = 0.0;
+  for (double h : c->block_h) hmax = std::max(hmax, h);
+  double side = std::max(cell, 2.0 * hmax * (1.0 + 1.0e-6));
+  if (s->built && s->n == n && s->cell == side) return PD_OK;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], c->hx[3 * i + k]), hi[k] = std::max(hi[k], c->hx[3 * i + k]);
+  DBuf<int64_t> nagg_d;
+  PD_CUDA_TRY(c, nagg_d.alloc(1));
+  const double want = side;
+  for (;;) {
+    Grid g;
+    for (int k = 0; k < 3; ++k) {
+      g.lo[k] = lo[k];
+      g.dims[k] = (int)std::floor((hi[k] - lo[k]) / side) + 1;
+    }
+    g.cell = side;
+    const int64_t ncell = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+    if (3 * std::min<int64_t>(ncell, n) > 64 * (int64_t)kMaxCoarse) {  // far too fine: grow before binning
+      side *= 1.25;
+      continue;
+    }
+    TRY_RC(bin_points(c, c->xv.p, n, g, s->sorted, s->cstart));
+    PD_CUDA_TRY(c, s->cell_agg.alloc(ncell));
+    PD_CUDA_TRY(c, s->agg_cell.alloc(std::min<int64_t>(ncell, n)));
+    k_coarse_cells<<<1, 32, 0, c->stream>>>(ncell, s->cstart.p, s->cell_agg.p, s->agg_cell.p, nagg_d.p);
+    PD_CUDA_TRY(c, cudaGetLastError());
+    int64_t nagg = 0;
+    PD_CUDA_TRY(c, d2h(c, &nagg, nagg_d.p, sizeof(int64_t)));
+    if (3 * nagg > kMaxCoarse) {
+      side *= 1.25;
+      continue;
+    }
+    s->g = g;
+    s->nagg = nagg;
+    s->nc = (int)(3 * nagg);
+    break;
+  }
+  PD_CUDA_TRY(c, s->agg_of.alloc(n));
+  k_coarse_agg_of<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, c->xv.p, s->g, s->cell_agg.p, s->agg_of.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  const int nc = s->nc;
+  PD_CUDA_TRY(c, s->clo.alloc(4 * (size_t)n));
+  PD_CUDA_TRY(c, s->slots.alloc((size_t)n * kSlots * kSlotVals));
+  PD_CUDA_TRY(c, s->A.alloc((size_t)nc * nc));
+  PD_CUDA_TRY(c, s->P.alloc(kGjB * kGjB));
+  PD_CUDA_TRY(c, s->R.alloc((size_t)kGjB * nc));
+  PD_CUDA_TRY(c, s->C.alloc((size_t)kGjB * nc));
+  PD_CUDA_TRY(c, s->rc.alloc(nc));
+  PD_CUDA_TRY(c, s->zc.alloc(nc));
+  PD_CUDA_TRY(c, s->status.alloc(1));
+  s->n = n;
+  s->cell = want;
+  s->built = true;
+  s->have_op = false;
+  return PD_OK;
+}
+
+// Assembles Ac = P0^T K P0 at the tangent state (y, ab = (theta, q, alpha, .),
+// fixed) and inverts it in place. A copy of the assembled matrix goes to
+// `assembled` (device, nc*nc) when not null.
+int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* fixed, double cell,
+                 double* assembled) {
+  CoarseState* s = co_state(c);
+  TRY_RC(co_aggregates(c, s, cell));
+  const int64_t n = c->n;
+  const int nc = s->nc;
+  PD_CUDA_TRY(c, dzero(c, s->status.p, sizeof(int)));
+  k_coarse_point<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, y, ab,
+                                                                     c->pt.p, c->hp.p, c->influence, fixed, s->g,
+                                                                     s->clo.p, s->slots.p, s->status.p);
+  PD_CUDA_TRY(c, dzero(c, s->A.p, s->A.bytes()));
+  k_coarse_rows<<<(unsigned)((s->nagg + kRowWarps - 1) / kRowWarps), 32 * kRowWarps, 0, c->stream>>>(
+      s->nagg, nc, s->g, s->agg_cell.p, s->cell_agg.p, s->cstart.p, s->sorted.p, s->clo.p, s->slots.p, s->A.p);
+  k_coarse_unit_diag<<<(nc + 255) / 256, 256, 0, c->stream>>>(nc, s->A.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  int st = 0;
+  PD_CUDA_TRY(c, d2h(c, &st, s->status.p, sizeof(int)));
+  if (st) {
+    c->err = "coarse space: a bond reaches past its point's 2x2x2 aggregate cells";
+    return PD_ERR_STATE;
+  }
+  if (assembled)
+    PD_CUDA_TRY(c, cudaMemcpyAsync(assembled, s->A.p, s->A.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  const int ntile = (nc + kGjB - 1) / kGjB;
+  for (int k0 = 0; k0 < nc; k0 += kGjB) {
+    const int bk = std::min(kGjB, nc - k0);
+    k_gj_pivot<<<1, 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p);
+    k_gj_panel<<<2 * ntile, 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p, s->R.p, s->C.p);
+    k_gj_update<<<dim3(ntile, ntile), 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p, s->R.p, s->C.p);
+  }
+  PD_CUDA_TRY(c, cudaGetLastError());
+  s->have_op = true;
+  return PD_OK;
+}
+
+// z += scale P0 Ac^-1 P0^T r on the free dofs (r double or float).
+template <typename T>
+static int co_apply(pd_ctx* c, const T* r, double* z, const uint8_t* fixed, double scale) {
+  CoarseState* s = c->coarse;
+  if (!s || !s->have_op) {
+    c->err = "coarse operator not built";
+    return PD_ERR_STATE;
+  }
+  const int64_t n = c->n;
+  k_coarse_restrict<T><<<(unsigned)((s->nagg * 32 + 255) / 256), 256, 0, c->stream>>>(s->nagg, s->agg_cell.p,
+                                                                                      s->cstart.p, s->sorted.p, r,
+                                                                                      s->rc.p);
+  k_coarse_gemv<<<(unsigned)(((int64_t)s->nc * 32 + 255) / 256), 256, 0, c->stream>>>(s->nc, s->A.p, s->rc.p, s->zc.p);
+  k_coarse_prolong<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, s->agg_of.p, s->zc.p, scale, fixed, z);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+int coarse_apply_add(pd_ctx* c, const double* r, double* z, const uint8_t* fixed) {
+  return co_apply(c, r, z, fixed, 1.0);
+}
+int coarse_apply_add_f(pd_ctx* c, const float* r, double* z, const uint8_t* fixed, double scale) {
+  return co_apply(c, r, z, fixed, scale);
+}
+
+// Aggregate of every point (device, n) of the current coarse space.
+int coarse_aggregates(pd_ctx* c, int32_t* agg_dev) {
+  CoarseState* s = c->coarse;
+  if (!s || !s->built) {
+    c->err = "coarse space not built";
+    return PD_ERR_STATE;
+  }
+  PD_CUDA_TRY(c, cudaMemcpyAsync(agg_dev, s->agg_of.p, c->n * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+  return PD_OK;
+}
+
+int coarse_copy_inverse(pd_ctx* c, double* dst) {
+  CoarseState* s = c->coarse;
+  if (!s || !s->have_op) {
+    c->err = "coarse operator not built";
+    return PD_ERR_STATE;
+  }
+  PD_CUDA_TRY(c, cudaMemcpyAsync(dst, s->A.p, (size_t)s->nc * s->nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 c->stream));
+  return PD_OK;
+}
+
+}  // namespace pdb

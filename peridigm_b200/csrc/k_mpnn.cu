@@ -1,55 +1,78 @@
-// Learned message-passing preconditioner for the quasi-static CG (sm_100a).
-// No counterpart in the reference; it plugs into the block-Jacobi CG of
-// k_qs.cu as z = P_bj r + s_a * N(a/s_a, r/s_r), a = P_bj r, s_a = rms(a),
-// s_r = rms(r) (so z scales with r), on the subgraph of bonds shorter than a
-// radius (the nearest shells of the bond family).
+// Learned middle level of the quasi-static CG preconditioner (sm_100a).
+// No counterpart in the reference. The preconditioner is
 //
-// Network (hidden 64, BF16 weights and BF16 node activations, FP32 accumulate):
-//   h0 = relu(W0 f + b0)                         f = (a/s_a, r/s_r), 6 inputs
-//   h_l = h_{l-1} + relu(Ws_l h_{l-1} + Wn_l m_l + b_l),  m_l = mean_{j in N(i)} h_{l-1,j},  l = 1..3
-//   out = Wd h3 + bd                              3 outputs
-// Training: residuals r_k captured from block-Jacobi CG solves, loss
-// |K z - r|^2 / |r|^2 per residual (z approximates a local inverse of the
-// tangent, the part a 3-hop network can represent), Adam on FP32 master
-// weights; forward and backward are the kernels below, one warp per node,
-// gathers only (the transpose of the mean aggregation is a gather over the
-// symmetric subgraph), deterministic block reductions for weight gradients.
+//   z = P_bj r  +  P0 Ac^-1 P0^T r  +  Q S G^T G S Q^T r
+//       block      exact coarse        learned middle level
+//       Jacobi     (k_coarse.cu)       (this file)
+//
+// Q: piecewise-constant prolongation from "patches" (the non-empty cells of a
+// grid of side `patch`, about two lattice spacings) to the free dofs of their
+// points; S: one positive scale per patch, s_I = sqrt(sum_{i in I} tr'(D_i^-1)/3)
+// / |I| from the block-Jacobi inverse blocks D_i^-1 (tr': free dofs only; the
+// patch's Galerkin diagonal is about |I| / that sum); G: a linear message-passing network on
+// the patch graph (patches joined to the non-empty cells of their 3x3x3
+// neighborhood, whose points are bonded):
+//
+//   h0 = W0 v                                   v = S Q^T r, 3 -> 64 channels
+//   h_l = h_{l-1} + Ws_l h_{l-1} + Wn_l mean_{J in N(I)} h_{l-1,J},  l = 1..3
+//
+// with hidden 64, BF16 weights and FP32 activations and accumulation. G^T G is
+// symmetric positive semi-definite and S diagonal positive, so M stays
+// symmetric positive definite and plain CG keeps its optimality. The middle
+// level covers the band between block Jacobi (the nearest neighbors) and the
+// coarse cells (two horizons): an exact patch-level solve halves the two-level
+// CG iterations on a 24^3 cube; G^T G is trained to approximate it locally.
+//
+// Training: pairs (r_k, e_k = x* - x_k) captured from two-level CG solves
+// (K e_k = r_k); loss = the energy-norm error left by one optimally scaled
+// preconditioned step, L = min_alpha |e - alpha z|_K^2 / |e|_K^2
+// = 1 - (r.z)^2 / ((z.K z)(e.r)), with K the matrix-free tangent rescaled to
+// each pair's modulus. It is invariant to the scale of z (additive multilevel
+// preconditioners overshoot by design, which a residual-norm loss punishes)
+// and needs one tangent product per pair. With w = G^T G v the weight
+// gradient of g^T w is the gradient of <G g_c, G v> (g_c = S Q^T dL/dz): two
+// forward passes of G and two backward passes, each with the other's output
+// as its upstream gradient.
+// Adam on FP32 master weights, cast to BF16 after every step. All reductions
+// run in a fixed order (bit-reproducible).
 #include <cuda_bf16.h>
+#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <random>
 #include <vector>
 
+#include "cells.cuh"
 #include "pd_internal.cuh"
 
 namespace pdb {
 
 constexpr int H = 64;
-constexpr int F = 6;
 constexpr int NL = 3;
-constexpr int OFF_W0 = 0, OFF_B0 = H * F;
-constexpr int OFF_L = OFF_B0 + H;               // per layer: Ws (H*H), Wn (H*H), b (H)
-constexpr int LSZ = 2 * H * H + H;
-constexpr int OFF_WD = OFF_L + NL * LSZ, OFF_BD = OFF_WD + 3 * H;
-constexpr int NPARAM = OFF_BD + 3;
+constexpr int OFF_W0 = 0;       // W0 [H][3]
+constexpr int OFF_L = 3 * H;    // per layer: Ws [H][H], Wn [H][H]
+constexpr int LSZ = 2 * H * H;
+constexpr int NPARAM = OFF_L + NL * LSZ;
 constexpr int kRed = 148;
+constexpr int kTile = 32;       // patches per block tile of the layer kernels
 
 struct MpnnState {
   bool ready = false;    // weights initialised (trained or loaded)
   bool trained = false;
-  double radius = 0.0;
-  DBuf<int64_t> mrow;
-  DBuf<int32_t> mcol;
-  int64_t n = 0;
-  DBuf<float> w, g, am, av, gpart;
+  bool patches = false;  // patch graph built
+  double patch = 0.0;    // patch cell side
+  double coarse_cell = 0.0;  // >= 0: the coarse level sits under the network (aggregate cell side)
+  int64_t n = 0, np = 0;
+  Grid g;
+  DBuf<int32_t> sorted, pid, cell_patch, patch_cell, pcol;
+  DBuf<int64_t> cstart, prow;
+  DBuf<float> scale;     // s_I
+  DBuf<float> w, g_, am, av, gpart;
   DBuf<__nv_bfloat16> wb;
   int64_t adam_t = 0;
-  // activations
-  DBuf<float> feat, pre[NL + 1], m[NL], dh, dhs, dm, gout, scal;
-  DBuf<__nv_bfloat16> h[NL + 1];
-  DBuf<double> a;  // P_bj r of the current application
-  DBuf<double> bjpart, dscal;  // inference reduction partials and scales
+  // activations: two sets (v and the gradient input), FP32
+  DBuf<float> v[2], h[2][NL + 1], m[2][NL], d, s_buf, t_buf, out3;
   // training set: per pair a, r, e (float, 3n each)
   DBuf<float> pairs;
   int64_t npairs = 0, cap = 0;
@@ -65,347 +88,334 @@ struct MpnnState {
 };
 
 // ---------------------------------------------------------------------------
-// Subgraph of bonds shorter than the radius (symmetric when the bond family is)
+// Patch graph
 // ---------------------------------------------------------------------------
-template <bool FILL>
-__global__ void k_mp_subgraph(int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col,
-                              const uint8_t* __restrict__ dmg, const double4* __restrict__ xv, double r2,
-                              int64_t* __restrict__ cnt, const int64_t* __restrict__ mrow, int32_t* __restrict__ mcol) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double4 xi = xv[i];
-  int64_t k = FILL ? mrow[i] : 0;
-  for (int64_t b = row[i]; b < row[i + 1]; ++b) {
-    if (dmg[b]) continue;
-    const int32_t j = col[b];
-    const double4 xj = xv[j];
-    const double d0 = xj.x - xi.x, d1 = xj.y - xi.y, d2 = xj.z - xi.z;
-    if (d0 * d0 + d1 * d1 + d2 * d2 <= r2) {
-      if (FILL) mcol[k] = j;
+__global__ void k_pt_cells(int64_t ncell, const int64_t* __restrict__ cstart, int32_t* __restrict__ cell_patch,
+                           int32_t* __restrict__ patch_cell, int64_t* __restrict__ np_out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int32_t k = 0;
+  for (int64_t q = 0; q < ncell; ++q) {
+    if (cstart[q + 1] > cstart[q]) {
+      cell_patch[q] = k;
+      patch_cell[k] = (int32_t)q;
       ++k;
+    } else {
+      cell_patch[q] = -1;
     }
   }
-  if (!FILL) cnt[i] = k;
+  *np_out = k;
 }
 
-__global__ void k_mp_scan_small(int64_t n, const int64_t* __restrict__ cnt, int64_t* __restrict__ out) {
-  // single-thread exclusive scan (setup only, n up to a few million)
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int64_t s = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    out[i] = s;
-    s += cnt[i];
-  }
-  out[n] = s;
-}
-
-// ---------------------------------------------------------------------------
-// Inference / training forward
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
-
-// a = P_bj r (FP64) and block partials of sum a^2, sum r^2
-__global__ void k_mp_bj(int64_t n, const double* __restrict__ dinv, const double* __restrict__ r,
-                        double* __restrict__ a, float* __restrict__ feat, double* __restrict__ partial) {
-  __shared__ double s0[256], s1[256];
-  double aa = 0.0, rr = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double r0 = r[3 * i], r1 = r[3 * i + 1], r2 = r[3 * i + 2];
-    const double* d = dinv + 9 * i;
-    const double a0 = d[0] * r0 + d[1] * r1 + d[2] * r2;
-    const double a1 = d[3] * r0 + d[4] * r1 + d[5] * r2;
-    const double a2 = d[6] * r0 + d[7] * r1 + d[8] * r2;
-    a[3 * i] = a0, a[3 * i + 1] = a1, a[3 * i + 2] = a2;
-    aa += a0 * a0 + a1 * a1 + a2 * a2;
-    rr += r0 * r0 + r1 * r1 + r2 * r2;
-  }
-  s0[threadIdx.x] = aa;
-  s1[threadIdx.x] = rr;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) s0[threadIdx.x] += s0[threadIdx.x + o], s1[threadIdx.x] += s1[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) partial[2 * blockIdx.x] = s0[0], partial[2 * blockIdx.x + 1] = s1[0];
-}
-
-// scal[0] = s_a, scal[1] = s_r (rms, floored)
-__global__ void k_mp_scales(int nblk, const double* __restrict__ partial, int64_t n, float* __restrict__ scal,
-                            double* __restrict__ dscal) {
-  if (threadIdx.x != 0) return;
-  double sa = 0.0, sr = 0.0;
-  for (int b = 0; b < nblk; ++b) sa += partial[2 * b], sr += partial[2 * b + 1];
-  sa = sqrt(sa / (3.0 * (double)n));
-  sr = sqrt(sr / (3.0 * (double)n));
-  dscal[0] = sa;
-  dscal[1] = sr;
-  scal[0] = (float)(sa > 0 ? 1.0 / sa : 0.0);
-  scal[1] = (float)(sr > 0 ? 1.0 / sr : 0.0);
-}
-
-// features from FP64 a, r (inference) or FP32 stored pair arrays (training)
-template <typename T>
-__global__ void k_mp_features(int64_t n, const T* __restrict__ a, const T* __restrict__ r,
-                              const float* __restrict__ scal, float* __restrict__ feat) {
+__global__ void k_pt_pid(int64_t n, const double4* __restrict__ xv, Grid g, const int32_t* __restrict__ cell_patch,
+                         int32_t* __restrict__ pid) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float ia = scal[0], ir = scal[1];
-  for (int c = 0; c < 3; ++c) {
-    feat[F * i + c] = (float)a[3 * i + c] * ia;
-    feat[F * i + 3 + c] = (float)r[3 * i + c] * ir;
+  const double4 p = xv[i];
+  pid[i] = cell_patch[(cell_coord(g, p.z, 2) * g.dims[1] + cell_coord(g, p.y, 1)) * g.dims[0] + cell_coord(g, p.x, 0)];
+}
+
+// neighbors of patch I: the non-empty cells of its 3x3x3 neighborhood (itself excluded), in cell order
+template <bool FILL>
+__global__ void k_pt_adj(int64_t np, Grid g, const int32_t* __restrict__ patch_cell,
+                         const int32_t* __restrict__ cell_patch, int64_t* __restrict__ cnt,
+                         const int64_t* __restrict__ prow, int32_t* __restrict__ pcol) {
+  const int64_t I = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= np) return;
+  const int q = patch_cell[I];
+  const int cx = q % g.dims[0], cy = (q / g.dims[0]) % g.dims[1], cz = q / (g.dims[0] * g.dims[1]);
+  int64_t k = FILL ? prow[I] : 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        if (!dx && !dy && !dz) continue;
+        const int x = cx + dx, y = cy + dy, z = cz + dz;
+        if (x < 0 || y < 0 || z < 0 || x >= g.dims[0] || y >= g.dims[1] || z >= g.dims[2]) continue;
+        const int32_t J = cell_patch[(z * g.dims[1] + y) * g.dims[0] + x];
+        if (J < 0) continue;
+        if (FILL) pcol[k] = J;
+        ++k;
+      }
+  if (!FILL) cnt[I] = k;
+}
+
+// s_I = sqrt(sum_{i in I} sum_{c free} (D_i^-1)_cc / 3) / |I|  (warp per patch;
+// the identity rows of prescribed dofs are left out)
+__global__ void k_pt_scale(int64_t np, const int32_t* __restrict__ patch_cell, const int64_t* __restrict__ cstart,
+                           const int32_t* __restrict__ sorted, const double* __restrict__ dinv,
+                           const uint8_t* __restrict__ fixed, float* __restrict__ scale) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= np) return;
+  const int q = patch_cell[I];
+  double s = 0.0;
+  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+    const int64_t p = sorted[t];
+    const double* d = dinv + 9 * p;
+    const uint8_t f = fixed ? fixed[p] : 0;
+    s += ((f & 1 ? 0.0 : d[0]) + (f & 2 ? 0.0 : d[4]) + (f & 4 ? 0.0 : d[8])) / 3.0;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  const double cnt = (double)(cstart[q + 1] - cstart[q]);
+  if (lane == 0) scale[I] = (float)(s > 0.0 ? sqrt(s) / cnt : 0.0);
+}
+
+// v_I = mul * s_I * sum_{i in I, free} r_i  (warp per patch; fixed order)
+template <typename T>
+__global__ void k_pt_restrict(int64_t np, const int32_t* __restrict__ patch_cell, const int64_t* __restrict__ cstart,
+                              const int32_t* __restrict__ sorted, const T* __restrict__ r,
+                              const uint8_t* __restrict__ fixed, const float* __restrict__ scale, double mul,
+                              float* __restrict__ v) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= np) return;
+  const int q = patch_cell[I];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+    const int64_t p = sorted[t];
+    const uint8_t f = fixed ? fixed[p] : 0;
+    if (!(f & 1)) s0 += (double)r[3 * p];
+    if (!(f & 2)) s1 += (double)r[3 * p + 1];
+    if (!(f & 4)) s2 += (double)r[3 * p + 2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) {
+    const double sc = mul * (double)scale[I];
+    v[3 * I] = (float)(sc * s0), v[3 * I + 1] = (float)(sc * s1), v[3 * I + 2] = (float)(sc * s2);
   }
 }
 
-// h0 = relu(W0 f + b0); lane l owns outputs 2l, 2l+1
-__global__ void __launch_bounds__(256) k_mp_encode(int64_t n, const float* __restrict__ feat,
-                                                   const __nv_bfloat16* __restrict__ wb, float* __restrict__ pre0,
-                                                   __nv_bfloat16* __restrict__ h0) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+// z_i += mul * s_I * out_I on the free dofs of point i (I = patch of i)
+__global__ void k_pt_prolong(int64_t n, const int32_t* __restrict__ pid, const float* __restrict__ out,
+                             const float* __restrict__ scale, double mul, const uint8_t* __restrict__ fixed,
+                             double* __restrict__ z) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float f[F];
-  for (int k = 0; k < F; ++k) f[k] = feat[F * i + k];
-  for (int q = 0; q < 2; ++q) {
-    const int o = 2 * lane + q;
-    float s = bf(wb[OFF_B0 + o]);
-    for (int k = 0; k < F; ++k) s = fmaf(bf(wb[OFF_W0 + o * F + k]), f[k], s);
-    if (pre0) pre0[(int64_t)H * i + o] = s;
-    h0[(int64_t)H * i + o] = __float2bfloat16(fmaxf(s, 0.0f));
-  }
-}
-
-// one message-passing layer; weights staged in shared memory transposed
-// (wT[k][o]) so lane l reads the bf16 pair (2l, 2l+1) conflict-free.
-__global__ void __launch_bounds__(256) k_mp_layer(int64_t n, const int64_t* __restrict__ mrow,
-                                                  const int32_t* __restrict__ mcol,
-                                                  const __nv_bfloat16* __restrict__ wl,
-                                                  const __nv_bfloat16* __restrict__ hin, __nv_bfloat16* __restrict__ hout,
-                                                  float* __restrict__ pre_out, float* __restrict__ m_out) {
-  __shared__ __nv_bfloat162 sWs[H][H / 2], sWn[H][H / 2];
-  __shared__ float sb[H];
-  for (int t = threadIdx.x; t < H * H / 2; t += blockDim.x) {
-    const int k = t / (H / 2), op = t % (H / 2);
-    sWs[k][op] = __halves2bfloat162(wl[(2 * op) * H + k], wl[(2 * op + 1) * H + k]);
-    sWn[k][op] = __halves2bfloat162(wl[H * H + (2 * op) * H + k], wl[H * H + (2 * op + 1) * H + k]);
-  }
-  for (int t = threadIdx.x; t < H; t += blockDim.x) sb[t] = bf(wl[2 * H * H + t]);
-  __syncthreads();
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
-  const __nv_bfloat162* hin2 = reinterpret_cast<const __nv_bfloat162*>(hin);
-  const float2 hs = __bfloat1622float2(hin2[(int64_t)(H / 2) * i + lane]);
-  float2 mm = make_float2(0.f, 0.f);
-  const int64_t b0 = mrow[i], b1 = mrow[i + 1];
-  for (int64_t b = b0; b < b1; ++b) {
-    const float2 hj = __bfloat1622float2(hin2[(int64_t)(H / 2) * mcol[b] + lane]);
-    mm.x += hj.x;
-    mm.y += hj.y;
-  }
-  const float inv = b1 > b0 ? 1.0f / (float)(b1 - b0) : 0.0f;
-  mm.x *= inv;
-  mm.y *= inv;
-  float o0 = sb[2 * lane], o1 = sb[2 * lane + 1];
-#pragma unroll 8
-  for (int k = 0; k < H; ++k) {
-    const float hk = __shfl_sync(0xffffffffu, (k & 1) ? hs.y : hs.x, k >> 1);
-    const float mk = __shfl_sync(0xffffffffu, (k & 1) ? mm.y : mm.x, k >> 1);
-    const float2 ws = __bfloat1622float2(sWs[k][lane]);
-    const float2 wn = __bfloat1622float2(sWn[k][lane]);
-    o0 = fmaf(ws.x, hk, fmaf(wn.x, mk, o0));
-    o1 = fmaf(ws.y, hk, fmaf(wn.y, mk, o1));
-  }
-  if (pre_out) {
-    pre_out[(int64_t)H * i + 2 * lane] = o0;
-    pre_out[(int64_t)H * i + 2 * lane + 1] = o1;
-    m_out[(int64_t)H * i + 2 * lane] = mm.x;
-    m_out[(int64_t)H * i + 2 * lane + 1] = mm.y;
-  }
-  reinterpret_cast<__nv_bfloat162*>(hout)[(int64_t)(H / 2) * i + lane] =
-      __floats2bfloat162_rn(hs.x + fmaxf(o0, 0.0f), hs.y + fmaxf(o1, 0.0f));
-}
-
-// out = Wd h3 + bd ; z = a + s_a * out (inference, FP64 z)
-__global__ void __launch_bounds__(256) k_mp_decode(int64_t n, const __nv_bfloat16* __restrict__ h3,
-                                                   const __nv_bfloat16* __restrict__ wb,
-                                                   const double* __restrict__ a, const double* __restrict__ dscal,
-                                                   const uint8_t* __restrict__ fixed, double* __restrict__ z) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
-  const float2 hv = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(h3)[(int64_t)(H / 2) * i + lane]);
-  float o[3];
-  for (int c = 0; c < 3; ++c) {
-    float s = bf(wb[OFF_WD + c * H + 2 * lane]) * hv.x + bf(wb[OFF_WD + c * H + 2 * lane + 1]) * hv.y;
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    o[c] = s + bf(wb[OFF_BD + c]);
-  }
-  if (lane < 3) {
-    const uint8_t fx = fixed ? fixed[i] : 0;
-    const double v = ((fx >> lane) & 1) ? 0.0 : a[3 * i + lane] + dscal[0] * (double)o[lane];
-    z[3 * i + lane] = v;
-  }
+  const int64_t I = pid[i];
+  const uint8_t f = fixed ? fixed[i] : 0;
+  const double sc = mul * (double)scale[I];
+  for (int c = 0; c < 3; ++c)
+    if (!((f >> c) & 1)) z[3 * i + c] += sc * (double)out[3 * I + c];
 }
 
 // ---------------------------------------------------------------------------
-// Training: loss and backward
+// Network G and its transpose
 // ---------------------------------------------------------------------------
-// dh3 = Wd^T g
-__global__ void __launch_bounds__(256) k_mp_decode_back(int64_t n, const __nv_bfloat16* __restrict__ wb,
-                                                        const float* __restrict__ gout, float* __restrict__ dh) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
-  for (int q = 0; q < 2; ++q) {
-    const int k = 2 * lane + q;
-    float s = 0.0f;
-    for (int c = 0; c < 3; ++c) s = fmaf(bf(wb[OFF_WD + c * H + k]), gout[3 * i + c], s);
-    dh[(int64_t)H * i + k] = s;
-  }
-}
-
-// per node of layer l: dpre = dh * [pre > 0]; dhs = dh + Ws^T dpre ; dm = (Wn^T dpre)/deg
-__global__ void __launch_bounds__(256) k_mp_layer_back(int64_t n, const int64_t* __restrict__ mrow,
-                                                       const __nv_bfloat16* __restrict__ wl,
-                                                       const float* __restrict__ pre, float* __restrict__ dh,
-                                                       float* __restrict__ dhs, float* __restrict__ dm) {
-  __shared__ __nv_bfloat162 sWs[H][H / 2], sWn[H][H / 2];  // [o][k pair]
-  for (int t = threadIdx.x; t < H * H / 2; t += blockDim.x) {
-    const int o = t / (H / 2), kp = t % (H / 2);
-    sWs[o][kp] = __halves2bfloat162(wl[o * H + 2 * kp], wl[o * H + 2 * kp + 1]);
-    sWn[o][kp] = __halves2bfloat162(wl[H * H + o * H + 2 * kp], wl[H * H + o * H + 2 * kp + 1]);
-  }
-  __syncthreads();
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
-  const int64_t base = (int64_t)H * i;
-  float d0 = dh[base + 2 * lane], d1 = dh[base + 2 * lane + 1];
-  const float p0 = pre[base + 2 * lane] > 0.f ? d0 : 0.f;
-  const float p1 = pre[base + 2 * lane + 1] > 0.f ? d1 : 0.f;
-  // dpre written back into dh for the weight-gradient pass
-  dh[base + 2 * lane] = p0;
-  dh[base + 2 * lane + 1] = p1;
-  float s0 = d0, s1 = d1, m0 = 0.f, m1 = 0.f;
-#pragma unroll 8
-  for (int o = 0; o < H; ++o) {
-    const float po = __shfl_sync(0xffffffffu, (o & 1) ? p1 : p0, o >> 1);
-    const float2 ws = __bfloat1622float2(sWs[o][lane]);
-    const float2 wn = __bfloat1622float2(sWn[o][lane]);
-    s0 = fmaf(ws.x, po, s0);
-    s1 = fmaf(ws.y, po, s1);
-    m0 = fmaf(wn.x, po, m0);
-    m1 = fmaf(wn.y, po, m1);
-  }
-  const int64_t deg = mrow[i + 1] - mrow[i];
-  const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
-  dhs[base + 2 * lane] = s0;
-  dhs[base + 2 * lane + 1] = s1;
-  dm[base + 2 * lane] = m0 * inv;
-  dm[base + 2 * lane + 1] = m1 * inv;
-}
-
-// dh_prev[j] = dhs[j] + sum_{i in N(j)} dm[i]   (transpose of the mean over a symmetric graph)
-__global__ void __launch_bounds__(256) k_mp_gather_back(int64_t n, const int64_t* __restrict__ mrow,
-                                                        const int32_t* __restrict__ mcol,
-                                                        const float* __restrict__ dhs, const float* __restrict__ dm,
-                                                        float* __restrict__ dh_prev) {
-  const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (j >= n) return;
-  const float2* dm2 = reinterpret_cast<const float2*>(dm);
-  float2 s = reinterpret_cast<const float2*>(dhs)[(int64_t)(H / 2) * j + lane];
-  for (int64_t b = mrow[j]; b < mrow[j + 1]; ++b) {
-    const float2 v = dm2[(int64_t)(H / 2) * mcol[b] + lane];
-    s.x += v.x;
-    s.y += v.y;
-  }
-  reinterpret_cast<float2*>(dh_prev)[(int64_t)(H / 2) * j + lane] = s;
-}
-
-// encoder: dpre0 = dh0 * [pre0 > 0] (in place)
-__global__ void k_mp_relu_back(int64_t m, const float* __restrict__ pre, float* __restrict__ dh) {
+// h0[I][o] = sum_c W0[o][c] v[I][c]
+__global__ void k_pt_encode(int64_t np, const float* __restrict__ v, const __nv_bfloat16* __restrict__ wb,
+                            float* __restrict__ h0) {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < m && !(pre[k] > 0.f)) dh[k] = 0.f;
+  if (k >= np * H) return;
+  const int64_t I = k / H;
+  const int o = (int)(k - I * H);
+  float s = 0.f;
+  for (int c = 0; c < 3; ++c) s = fmaf(__bfloat162float(wb[OFF_W0 + 3 * o + c]), v[3 * I + c], s);
+  h0[k] = s;
 }
 
-// Weight gradient partials: G[o][k] += sum_i A[i][o] B[i][k]; A = dpre [n][H],
-// B [n][K] (bf16 activations, fp32 means or features); bias row: sum_i A[i][o].
-template <typename TB>
-__global__ void __launch_bounds__(256) k_mp_wgrad(int64_t n, int K, const float* __restrict__ A,
-                                                  const TB* __restrict__ B, float* __restrict__ part) {
+// out[I][c] = sum_o W0[o][c] x[I][o]  (warp per patch)
+__global__ void k_pt_encode_t(int64_t np, const float* __restrict__ x, const __nv_bfloat16* __restrict__ wb,
+                              float* __restrict__ out) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= np) return;
+  const float x0 = x[(int64_t)H * I + 2 * lane], x1 = x[(int64_t)H * I + 2 * lane + 1];
+  float s[3];
+  for (int c = 0; c < 3; ++c) {
+    s[c] = __bfloat162float(wb[OFF_W0 + 3 * (2 * lane) + c]) * x0 + __bfloat162float(wb[OFF_W0 + 3 * (2 * lane + 1) + c]) * x1;
+    for (int o = 16; o > 0; o >>= 1) s[c] += __shfl_xor_sync(0xffffffffu, s[c], o);
+  }
+  if (lane == 0) out[3 * I] = s[0], out[3 * I + 1] = s[1], out[3 * I + 2] = s[2];
+}
+
+// One layer: hout = hin + Ws hin + Wn mean_J hin_J (mout receives the mean).
+// Block tiles of 32 patches: phase 1 gathers [h | mean] rows into shared
+// memory (one warp per 4 patches, 2 features per lane), phase 2 multiplies by
+// [Ws | Wn] staged k-major in shared memory (8 outputs per thread, 16-byte
+// weight loads, FP32 accumulation).
+__global__ void __launch_bounds__(256) k_pt_layer(int64_t np, const int64_t* __restrict__ prow,
+                                                  const int32_t* __restrict__ pcol,
+                                                  const __nv_bfloat16* __restrict__ wl, const float* __restrict__ hin,
+                                                  float* __restrict__ hout, float* __restrict__ mout) {
+  __shared__ __align__(16) __nv_bfloat16 sW[2 * H][H + 8];  // sW[k][o] (rows padded: 144 B, 16-B aligned)
+  __shared__ float sX[kTile][2 * H + 1];
+  for (int t = threadIdx.x; t < 2 * H * H; t += blockDim.x) {  // coalesced read, transposed store
+    const int part = t / (H * H), o = (t % (H * H)) / H, k = t % H;
+    sW[part * H + k][o] = wl[t];
+  }
+  __syncthreads();
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nl = threadIdx.x >> 3, ob = (threadIdx.x & 7) * 8;
+  for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile) {
+    for (int q = 0; q < kTile / 8; ++q) {
+      const int r = wid * (kTile / 8) + q;
+      const int64_t I = i0 + r;
+      float2 hv = make_float2(0.f, 0.f), mv = make_float2(0.f, 0.f);
+      if (I < np) {
+        hv = reinterpret_cast<const float2*>(hin)[(int64_t)(H / 2) * I + lane];
+        const int64_t b0 = prow[I], b1 = prow[I + 1];
+        const float2* h2 = reinterpret_cast<const float2*>(hin);
+        int64_t b = b0;
+        for (; b + 4 <= b1; b += 4) {  // four independent neighbor loads in flight
+          const int32_t j0 = pcol[b], j1 = pcol[b + 1], j2 = pcol[b + 2], j3 = pcol[b + 3];
+          const float2 u0 = h2[(int64_t)(H / 2) * j0 + lane], u1 = h2[(int64_t)(H / 2) * j1 + lane];
+          const float2 u2 = h2[(int64_t)(H / 2) * j2 + lane], u3 = h2[(int64_t)(H / 2) * j3 + lane];
+          mv.x += (u0.x + u1.x) + (u2.x + u3.x);
+          mv.y += (u0.y + u1.y) + (u2.y + u3.y);
+        }
+        for (; b < b1; ++b) {
+          const float2 u = h2[(int64_t)(H / 2) * pcol[b] + lane];
+          mv.x += u.x;
+          mv.y += u.y;
+        }
+        const float inv = b1 > b0 ? 1.0f / (float)(b1 - b0) : 0.0f;
+        mv.x *= inv;
+        mv.y *= inv;
+        if (mout) reinterpret_cast<float2*>(mout)[(int64_t)(H / 2) * I + lane] = mv;
+      }
+      sX[r][2 * lane] = hv.x;
+      sX[r][2 * lane + 1] = hv.y;
+      sX[r][H + 2 * lane] = mv.x;
+      sX[r][H + 2 * lane + 1] = mv.y;
+    }
+    __syncthreads();
+    float acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < 2 * H; ++k) {
+      const float x = sX[nl][k];
+      const uint4 wv = *reinterpret_cast<const uint4*>(&sW[k][ob]);
+      const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float2 f = __bfloat1622float2(w2[j]);
+        acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
+        acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
+      }
+    }
+    const int64_t I = i0 + nl;
+    if (I < np) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) hout[(int64_t)H * I + ob + j] = sX[nl][ob + j] + acc[j];
+    }
+    __syncthreads();
+  }
+}
+
+// Transposed layer, per patch: s = d + Ws^T d, t = Wn^T d / deg (the gather
+// of t over the symmetric patch graph completes it, k_pt_gather_t).
+__global__ void __launch_bounds__(256) k_pt_layer_t(int64_t np, const int64_t* __restrict__ prow,
+                                                    const __nv_bfloat16* __restrict__ wl, const float* __restrict__ d,
+                                                    float* __restrict__ s_out, float* __restrict__ t_out) {
+  __shared__ __align__(16) __nv_bfloat16 sW[H][2 * H];  // sW[o][k']: k' < H: Ws[o][k'], else Wn[o][k'-H]
+  __shared__ float sX[kTile][H + 1];
+  for (int t = threadIdx.x; t < 2 * H * H; t += blockDim.x) {
+    const int o = t / (2 * H), k = t % (2 * H);
+    sW[o][k] = k < H ? wl[o * H + k] : wl[H * H + o * H + (k - H)];
+  }
+  __syncthreads();
+  const int nl = threadIdx.x >> 3, ob = (threadIdx.x & 7) * 16;
+  for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile) {
+    for (int t = threadIdx.x; t < kTile * H; t += blockDim.x) {
+      const int r = t / H, o = t % H;
+      const int64_t I = i0 + r;
+      sX[r][o] = I < np ? d[(int64_t)H * I + o] : 0.f;
+    }
+    __syncthreads();
+    float acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[j] = 0.f;
+#pragma unroll 4
+    for (int o = 0; o < H; ++o) {
+      const float x = sX[nl][o];
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        const uint4 wv = *reinterpret_cast<const uint4*>(&sW[o][ob + 8 * half]);
+        const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float2 f = __bfloat1622float2(w2[j]);
+          acc[8 * half + 2 * j] = fmaf(x, f.x, acc[8 * half + 2 * j]);
+          acc[8 * half + 2 * j + 1] = fmaf(x, f.y, acc[8 * half + 2 * j + 1]);
+        }
+      }
+    }
+    const int64_t I = i0 + nl;
+    if (I < np) {
+      const int64_t deg = prow[I + 1] - prow[I];
+      const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int k = ob + j;
+        if (k < H) s_out[(int64_t)H * I + k] = sX[nl][k] + acc[j];
+        else t_out[(int64_t)H * I + (k - H)] = acc[j] * inv;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// x_J = s_J + sum_{I in N(J)} t_I  (warp per patch, 2 features per lane)
+__global__ void __launch_bounds__(256) k_pt_gather_t(int64_t np, const int64_t* __restrict__ prow,
+                                                     const int32_t* __restrict__ pcol, const float* __restrict__ s,
+                                                     const float* __restrict__ t, float* __restrict__ x) {
+  const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (J >= np) return;
+  const float2* t2 = reinterpret_cast<const float2*>(t);
+  float2 a = reinterpret_cast<const float2*>(s)[(int64_t)(H / 2) * J + lane];
+  const int64_t b1 = prow[J + 1];
+  int64_t b = prow[J];
+  for (; b + 4 <= b1; b += 4) {
+    const int32_t j0 = pcol[b], j1 = pcol[b + 1], j2 = pcol[b + 2], j3 = pcol[b + 3];
+    const float2 u0 = t2[(int64_t)(H / 2) * j0 + lane], u1 = t2[(int64_t)(H / 2) * j1 + lane];
+    const float2 u2 = t2[(int64_t)(H / 2) * j2 + lane], u3 = t2[(int64_t)(H / 2) * j3 + lane];
+    a.x += (u0.x + u1.x) + (u2.x + u3.x);
+    a.y += (u0.y + u1.y) + (u2.y + u3.y);
+  }
+  for (; b < b1; ++b) {
+    const float2 u = t2[(int64_t)(H / 2) * pcol[b] + lane];
+    a.x += u.x;
+    a.y += u.y;
+  }
+  reinterpret_cast<float2*>(x)[(int64_t)(H / 2) * J + lane] = a;
+}
+
+// ---------------------------------------------------------------------------
+// Training kernels
+// ---------------------------------------------------------------------------
+// Weight-gradient partials: part[b][o*K+k] = sum_{i in block b's range} A[i][o] B[i][k]
+__global__ void __launch_bounds__(256) k_pt_wgrad(int64_t n, int K, const float* __restrict__ A,
+                                                  const float* __restrict__ B, float* __restrict__ part) {
   __shared__ float sa[H], sbv[H];
-  const int entries = H * K + H;
-  float acc[17];
-  for (int q = 0; q < 17; ++q) acc[q] = 0.f;
+  const int entries = H * K;
+  float acc[16];
+  for (int q = 0; q < 16; ++q) acc[q] = 0.f;
   const int64_t per = (n + gridDim.x - 1) / gridDim.x;
   const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(n, i0 + per);
   for (int64_t i = i0; i < i1; ++i) {
     if (threadIdx.x < H) sa[threadIdx.x] = A[(int64_t)H * i + threadIdx.x];
-    if (threadIdx.x < K) sbv[threadIdx.x] = (float)B[(int64_t)K * i + threadIdx.x];
+    if (threadIdx.x < K) sbv[threadIdx.x] = B[(int64_t)K * i + threadIdx.x];
     __syncthreads();
     int q = 0;
-    for (int e = threadIdx.x; e < entries; e += blockDim.x, ++q) {
-      if (e < H * K) acc[q] = fmaf(sa[e / K], sbv[e % K], acc[q]);
-      else acc[q] += sa[e - H * K];
-    }
+    for (int e = threadIdx.x; e < entries; e += blockDim.x, ++q) acc[q] = fmaf(sa[e / K], sbv[e % K], acc[q]);
     __syncthreads();
   }
   int q = 0;
   for (int e = threadIdx.x; e < entries; e += blockDim.x, ++q) part[(int64_t)blockIdx.x * entries + e] = acc[q];
 }
 
-template <>
-__global__ void __launch_bounds__(256) k_mp_wgrad<__nv_bfloat16>(int64_t n, int K, const float* __restrict__ A,
-                                                                 const __nv_bfloat16* __restrict__ B,
-                                                                 float* __restrict__ part) {
-  __shared__ float sa[H], sbv[H];
-  const int entries = H * K + H;
-  float acc[17];
-  for (int q = 0; q < 17; ++q) acc[q] = 0.f;
-  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
-  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(n, i0 + per);
-  for (int64_t i = i0; i < i1; ++i) {
-    if (threadIdx.x < H) sa[threadIdx.x] = A[(int64_t)H * i + threadIdx.x];
-    if (threadIdx.x < K) sbv[threadIdx.x] = __bfloat162float(B[(int64_t)K * i + threadIdx.x]);
-    __syncthreads();
-    int q = 0;
-    for (int e = threadIdx.x; e < entries; e += blockDim.x, ++q) {
-      if (e < H * K) acc[q] = fmaf(sa[e / K], sbv[e % K], acc[q]);
-      else acc[q] += sa[e - H * K];
-    }
-    __syncthreads();
-  }
-  int q = 0;
-  for (int e = threadIdx.x; e < entries; e += blockDim.x, ++q) part[(int64_t)blockIdx.x * entries + e] = acc[q];
-}
-
-// g[dst_w + o*K + k] += sum_b part[b][o*K+k]; g[dst_b + o] += sum_b part[b][H*K+o]
-__global__ void k_mp_wgrad_reduce(int nblk, int K, const float* __restrict__ part, float* __restrict__ g, int dst_w,
-                                  int dst_b) {
-  const int entries = H * K + H;
+// g[dst + e] += sum_b part[b][e]  (fixed order)
+__global__ void k_pt_wgrad_reduce(int nblk, int entries, const float* __restrict__ part, float* __restrict__ g,
+                                  int dst) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < entries; e += gridDim.x * blockDim.x) {
     float s = 0.f;
     for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * entries + e];
-    if (e < H * K) g[dst_w + e] += s;
-    else if (dst_b >= 0) g[dst_b + (e - H * K)] += s;  // dst_b < 0: no bias for this matrix
-  }
-}
-
-// decoder weight gradient: dWd[c][k] += sum_i g[i][c] h3[i][k]; dbd[c] += sum_i g[i][c]
-__global__ void k_mp_dec_wgrad(int64_t n, const float* __restrict__ gout, const __nv_bfloat16* __restrict__ h3,
-                               float* __restrict__ g) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;  // 0 .. 3*H+3
-  if (e >= 3 * H + 3) return;
-  double s = 0.0;
-  if (e < 3 * H) {
-    const int c = e / H, k = e % H;
-    for (int64_t i = 0; i < n; ++i) s += (double)gout[3 * i + c] * (double)__bfloat162float(h3[(int64_t)H * i + k]);
-    g[OFF_WD + e] += (float)s;
-  } else {
-    const int c = e - 3 * H;
-    for (int64_t i = 0; i < n; ++i) s += gout[3 * i + c];
-    g[OFF_BD + c] += (float)s;
+    g[dst + e] += s;
   }
 }
 
@@ -424,6 +434,67 @@ __global__ void k_mp_adam(int np, float* __restrict__ w, const float* __restrict
 __global__ void k_mp_cast(int np, const float* __restrict__ w, __nv_bfloat16* __restrict__ wb) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < np) wb[k] = __float2bfloat16(w[k]);
+}
+
+// z = a (FP64 from float), prescribed dofs zero
+__global__ void k_mp_base(int64_t m, const float* __restrict__ a, const uint8_t* __restrict__ fixed,
+                          double* __restrict__ z) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
+  z[k] = fx ? 0.0 : (double)a[k];
+}
+
+// partials of r.z, z.Kz, e.r over the free dofs (3 per block, fixed order)
+__global__ void k_mp_dots3(int64_t m, const float* __restrict__ r, const double* __restrict__ z,
+                           const double* __restrict__ kz, const float* __restrict__ e,
+                           const uint8_t* __restrict__ fixed, double* __restrict__ partial) {
+  __shared__ double s0[256], s1[256], s2[256];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+    if (fixed && ((fixed[k / 3] >> (k % 3)) & 1)) continue;
+    const double rk = (double)r[k], zk = z[k];
+    a0 += rk * zk;
+    a1 += zk * kz[k];
+    a2 += (double)e[k] * rk;
+  }
+  s0[threadIdx.x] = a0;
+  s1[threadIdx.x] = a1;
+  s2[threadIdx.x] = a2;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      s0[threadIdx.x] += s0[threadIdx.x + o], s1[threadIdx.x] += s1[threadIdx.x + o],
+          s2[threadIdx.x] += s2[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    partial[3 * blockIdx.x] = s0[0], partial[3 * blockIdx.x + 1] = s1[0], partial[3 * blockIdx.x + 2] = s2[0];
+}
+
+// gz = ca * r + cb * kz (prescribed dofs zero)
+__global__ void k_mp_gz(int64_t m, double ca, const float* __restrict__ r, double cb, const double* __restrict__ kz,
+                        const uint8_t* __restrict__ fixed, double* __restrict__ gz) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
+  gz[k] = fx ? 0.0 : ca * (double)r[k] + cb * kz[k];
+}
+
+// random probe e: uniform in [-1, 1) on the free dofs from a counter hash
+__global__ void k_mp_rand_e(int64_t m, uint64_t seed, const uint8_t* __restrict__ fixed, double* __restrict__ e,
+                            double* __restrict__ zero) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  uint64_t x = seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(k + 1));
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
+  e[k] = fx ? 0.0 : (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  zero[k] = 0.0;
 }
 
 // pair capture: a = P_bj r, r, e = x* - x_k, as float
@@ -450,30 +521,7 @@ __global__ void k_mp_make_pair(int64_t n, const double* __restrict__ dinv, const
 // ---------------------------------------------------------------------------
 static unsigned gw(int64_t n) { return (unsigned)((n * 32 + 255) / 256); }
 static unsigned g1(int64_t n) { return (unsigned)((n + 255) / 256); }
-
-static int mp_alloc(pd_ctx* c, MpnnState* s, bool train) {
-  const int64_t n = c->n;
-  if (s->n != n) {
-    for (int l = 0; l <= NL; ++l) PD_CUDA_TRY(c, s->h[l].alloc((size_t)H * n));
-    PD_CUDA_TRY(c, s->feat.alloc((size_t)F * n));
-    PD_CUDA_TRY(c, s->a.alloc(3 * n));
-    PD_CUDA_TRY(c, s->scal.alloc(8));
-    PD_CUDA_TRY(c, s->bjpart.alloc(2 * kRed));
-    PD_CUDA_TRY(c, s->dscal.alloc(2));
-    s->n = n;
-    for (int l = 0; l <= NL; ++l) s->pre[l].release();
-  }
-  if (train && s->pre[0].count < (size_t)H * n) {
-    for (int l = 0; l <= NL; ++l) PD_CUDA_TRY(c, s->pre[l].alloc((size_t)H * n));
-    for (int l = 0; l < NL; ++l) PD_CUDA_TRY(c, s->m[l].alloc((size_t)H * n));
-    PD_CUDA_TRY(c, s->dh.alloc((size_t)H * n));
-    PD_CUDA_TRY(c, s->dhs.alloc((size_t)H * n));
-    PD_CUDA_TRY(c, s->dm.alloc((size_t)H * n));
-    PD_CUDA_TRY(c, s->gout.alloc(3 * n));
-    PD_CUDA_TRY(c, s->gpart.alloc((size_t)kRed * (H * H + H) + 16));
-  }
-  return PD_OK;
-}
+static unsigned gtile(int64_t np) { return (unsigned)std::min<int64_t>((np + kTile - 1) / kTile, 148 * 8); }
 
 static MpnnState* mp_state(pd_ctx* c) { return reinterpret_cast<MpnnState*>(c->mpnn); }
 
@@ -488,38 +536,87 @@ static double current_modulus(const pd_ctx* c) {
   return c->block_K.empty() ? 1.0 : c->block_K[0];
 }
 
-int mpnn_init(pd_ctx* c, uint64_t seed, double radius) {
+// Patches: the non-empty cells of a grid of side `side` over the model coordinates.
+static int mp_patches(pd_ctx* c, MpnnState* s, double side) {
+  const int64_t n = c->n;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], c->hx[3 * i + k]), hi[k] = std::max(hi[k], c->hx[3 * i + k]);
+  Grid g;
+  double tot = 1.0;
+  for (int k = 0; k < 3; ++k) {
+    g.lo[k] = lo[k];
+    g.dims[k] = (int)std::floor((hi[k] - lo[k]) / side) + 1;
+    tot *= g.dims[k];
+  }
+  if (tot > 2.0e9) {
+    c->err = "pd_mpnn_init: the patch side is too small for the body";
+    return PD_ERR_ARG;
+  }
+  g.cell = side;
+  const int64_t ncell = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
+  TRY_RC(bin_points(c, c->xv.p, n, g, s->sorted, s->cstart));
+  DBuf<int64_t> npd, cnt;
+  PD_CUDA_TRY(c, npd.alloc(1));
+  PD_CUDA_TRY(c, s->cell_patch.alloc(ncell));
+  PD_CUDA_TRY(c, s->patch_cell.alloc(std::min<int64_t>(ncell, n)));
+  k_pt_cells<<<1, 32, 0, c->stream>>>(ncell, s->cstart.p, s->cell_patch.p, s->patch_cell.p, npd.p);
+  int64_t np = 0;
+  PD_CUDA_TRY(c, d2h(c, &np, npd.p, sizeof(int64_t)));
+  PD_CUDA_TRY(c, s->pid.alloc(n));
+  k_pt_pid<<<g1(n), 256, 0, c->stream>>>(n, c->xv.p, g, s->cell_patch.p, s->pid.p);
+  PD_CUDA_TRY(c, cnt.alloc(np + 1));
+  PD_CUDA_TRY(c, s->prow.alloc(np + 1));
+  k_pt_adj<false><<<g1(np), 256, 0, c->stream>>>(np, g, s->patch_cell.p, s->cell_patch.p, cnt.p, nullptr, nullptr);
+  PD_CUDA_TRY(c, cudaMemsetAsync(cnt.p + np, 0, sizeof(int64_t), c->stream));
+  size_t scan_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt.p, s->prow.p, (int)(np + 1), c->stream);
+  DBuf<unsigned char> stmp;
+  PD_CUDA_TRY(c, stmp.alloc(scan_bytes));
+  PD_CUDA_TRY(c, cub::DeviceScan::ExclusiveSum(stmp.p, scan_bytes, cnt.p, s->prow.p, (int)(np + 1), c->stream));
+  int64_t ne = 0;
+  PD_CUDA_TRY(c, d2h(c, &ne, s->prow.p + np, sizeof(int64_t)));
+  PD_CUDA_TRY(c, s->pcol.alloc(std::max<int64_t>(ne, 1)));
+  k_pt_adj<true><<<g1(np), 256, 0, c->stream>>>(np, g, s->patch_cell.p, s->cell_patch.p, nullptr, s->prow.p,
+                                                s->pcol.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  PD_CUDA_TRY(c, s->scale.alloc(np));
+  PD_CUDA_TRY(c, dzero(c, s->scale.p, np * sizeof(float)));
+  for (int k = 0; k < 2; ++k) {
+    PD_CUDA_TRY(c, s->v[k].alloc(3 * np));
+    for (int l = 0; l <= NL; ++l) PD_CUDA_TRY(c, s->h[k][l].alloc((size_t)H * np));
+    for (int l = 0; l < NL; ++l) PD_CUDA_TRY(c, s->m[k][l].alloc((size_t)H * np));
+  }
+  PD_CUDA_TRY(c, s->d.alloc((size_t)H * np));
+  PD_CUDA_TRY(c, s->s_buf.alloc((size_t)H * np));
+  PD_CUDA_TRY(c, s->t_buf.alloc((size_t)H * np));
+  PD_CUDA_TRY(c, s->out3.alloc(3 * np));
+  s->g = g;
+  s->np = np;
+  s->n = n;
+  s->patch = side;
+  s->patches = true;
+  return PD_OK;
+}
+
+int mpnn_init(pd_ctx* c, uint64_t seed, double patch) {
   if (!c->mpnn) c->mpnn = new MpnnState();
   MpnnState* s = mp_state(c);
-  const int64_t n = c->n;
-  s->radius = radius;
-  // subgraph
-  DBuf<int64_t> cnt;
-  PD_CUDA_TRY(c, cnt.alloc(n + 1));
-  PD_CUDA_TRY(c, s->mrow.alloc(n + 1));
-  const double r2 = radius * radius;
-  k_mp_subgraph<false><<<g1(n), 256, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, r2, cnt.p, nullptr,
-                                                     nullptr);
-  k_mp_scan_small<<<1, 32, 0, c->stream>>>(n, cnt.p, s->mrow.p);
-  int64_t nm = 0;
-  PD_CUDA_TRY(c, cudaMemcpyAsync(&nm, s->mrow.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
-  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  PD_CUDA_TRY(c, s->mcol.alloc(std::max<int64_t>(nm, 1)));
-  k_mp_subgraph<true><<<g1(n), 256, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, r2, nullptr, s->mrow.p,
-                                                    s->mcol.p);
-  PD_CUDA_TRY(c, cudaGetLastError());
-  // weights: He-style uniform init from the seed; zero decoder so z starts at P_bj r
+  TRY_RC(mp_patches(c, s, patch));
+  // weights: W0 = 0.5 [I3; 0] and near-zero layers plus small uniform noise
+  // from the seed, so G^T G starts near 0.25 I (a Jacobi-scaled middle level)
   std::vector<float> w(NPARAM, 0.f);
   std::mt19937_64 rng(seed);
   auto uni = [&](float lim) { return (float)((rng() >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0) * lim; };
-  for (int k = 0; k < H * F; ++k) w[OFF_W0 + k] = uni(std::sqrt(6.0f / F));
+  for (int k = 0; k < 3 * H; ++k) w[OFF_W0 + k] = uni(0.01f) + ((k % 4 == 0 && k < 12) ? 0.5f : 0.0f);
   for (int l = 0; l < NL; ++l)
-    for (int k = 0; k < 2 * H * H; ++k) w[OFF_L + l * LSZ + k] = uni(0.5f * std::sqrt(6.0f / (2 * H)));
+    for (int k = 0; k < LSZ; ++k) w[OFF_L + l * LSZ + k] = uni(0.01f);
   PD_CUDA_TRY(c, s->w.alloc(NPARAM));
   PD_CUDA_TRY(c, s->wb.alloc(NPARAM));
-  PD_CUDA_TRY(c, s->g.alloc(NPARAM));
+  PD_CUDA_TRY(c, s->g_.alloc(NPARAM));
   PD_CUDA_TRY(c, s->am.alloc(NPARAM));
   PD_CUDA_TRY(c, s->av.alloc(NPARAM));
+  PD_CUDA_TRY(c, s->gpart.alloc((size_t)kRed * H * H + 16));
   PD_CUDA_TRY(c, h2d(c, s->w.p, w.data(), NPARAM * sizeof(float)));
   PD_CUDA_TRY(c, dzero(c, s->am.p, NPARAM * sizeof(float)));
   PD_CUDA_TRY(c, dzero(c, s->av.p, NPARAM * sizeof(float)));
@@ -528,7 +625,7 @@ int mpnn_init(pd_ctx* c, uint64_t seed, double radius) {
   s->adam_t = 0;
   s->ready = true;
   s->trained = false;
-  return mp_alloc(c, s, false);
+  return PD_OK;
 }
 
 bool mpnn_ready(const pd_ctx* c) { return c->mpnn && reinterpret_cast<const MpnnState*>(c->mpnn)->ready; }
@@ -538,149 +635,139 @@ void mpnn_release(pd_ctx* c) {
   c->mpnn = nullptr;
 }
 
-// Layers 1..3 from h[0]; training saves pre-activations and means.
-static int mp_forward_layers(pd_ctx* c, MpnnState* s, bool save) {
-  const int64_t n = c->n;
-  for (int l = 0; l < NL; ++l) {
-    k_mp_layer<<<gw(n), 256, 0, c->stream>>>(n, s->mrow.p, s->mcol.p, s->wb.p + OFF_L + l * LSZ, s->h[l].p,
-                                             s->h[l + 1].p, save ? s->pre[l + 1].p : nullptr,
-                                             save ? s->m[l].p : nullptr);
+// Patch scales from the block-Jacobi inverse blocks of the current tangent.
+int mpnn_prepare(pd_ctx* c, const double* dinv) {
+  MpnnState* s = mp_state(c);
+  if (!s || !s->patches || s->n != c->n) {
+    c->err = "learned preconditioner not initialised for these points";
+    return PD_ERR_STATE;
   }
+  k_pt_scale<<<gw(s->np), 256, 0, c->stream>>>(s->np, s->patch_cell.p, s->cstart.p, s->sorted.p, dinv,
+                                               qs_fixed_mask(c), s->scale.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
 }
 
-int mpnn_apply(pd_ctx* c, const double* r, double* z, const double* dinv) {
+// h[k][0..NL] = G v[k] (means saved when `save`)
+static int mp_forward(pd_ctx* c, MpnnState* s, int k, bool save) {
+  const int64_t np = s->np;
+  k_pt_encode<<<g1(np * H), 256, 0, c->stream>>>(np, s->v[k].p, s->wb.p, s->h[k][0].p);
+  for (int l = 0; l < NL; ++l)
+    k_pt_layer<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->wb.p + OFF_L + l * LSZ, s->h[k][l].p,
+                                                 s->h[k][l + 1].p, save ? s->m[k][l].p : nullptr);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+// out3 = G^T y (y: 64 channels per patch, not modified)
+static int mp_transpose(pd_ctx* c, MpnnState* s, const float* y) {
+  const int64_t np = s->np;
+  const float* cur = y;
+  for (int l = NL - 1; l >= 0; --l) {
+    k_pt_layer_t<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->wb.p + OFF_L + l * LSZ, cur, s->s_buf.p,
+                                                   s->t_buf.p);
+    k_pt_gather_t<<<gw(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
+    cur = s->d.p;
+  }
+  k_pt_encode_t<<<gw(np), 256, 0, c->stream>>>(np, cur, s->wb.p, s->out3.p);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+static void mp_wgrad(pd_ctx* c, MpnnState* s, int K, const float* A, const float* B, int dst) {
+  k_pt_wgrad<<<kRed, 256, 0, c->stream>>>(s->np, K, A, B, s->gpart.p);
+  k_pt_wgrad_reduce<<<(H * K + 255) / 256, 256, 0, c->stream>>>(kRed, H * K, s->gpart.p, s->g_.p, dst);
+}
+
+// Weight gradients of <U, G v[k]> (activations of set k saved), added into g_.
+static int mp_backward(pd_ctx* c, MpnnState* s, int k, const float* U) {
+  const int64_t np = s->np;
+  const float* cur = U;
+  for (int l = NL - 1; l >= 0; --l) {
+    mp_wgrad(c, s, H, cur, s->h[k][l].p, OFF_L + l * LSZ);
+    mp_wgrad(c, s, H, cur, s->m[k][l].p, OFF_L + l * LSZ + H * H);
+    k_pt_layer_t<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->wb.p + OFF_L + l * LSZ, cur, s->s_buf.p,
+                                                   s->t_buf.p);
+    k_pt_gather_t<<<gw(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
+    cur = s->d.p;
+  }
+  mp_wgrad(c, s, 3, cur, s->v[k].p, OFF_W0);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+// z += Q S G^T G S Q^T r on the free dofs (inference).
+int mpnn_apply_add(pd_ctx* c, const double* r, double* z) {
   MpnnState* s = mp_state(c);
-  if (!s || !s->ready) {
+  if (!s || !s->ready || !s->patches || s->n != c->n) {
     c->err = "learned preconditioner not initialised";
     return PD_ERR_STATE;
   }
-  TRY_RC(mp_alloc(c, s, false));
-  const int64_t n = c->n;
-  k_mp_bj<<<kRed, 256, 0, c->stream>>>(n, dinv, r, s->a.p, s->feat.p, s->bjpart.p);
-  k_mp_scales<<<1, 32, 0, c->stream>>>(kRed, s->bjpart.p, n, s->scal.p, s->dscal.p);
-  k_mp_features<double><<<g1(n), 256, 0, c->stream>>>(n, s->a.p, r, s->scal.p, s->feat.p);
-  k_mp_encode<<<gw(n), 256, 0, c->stream>>>(n, s->feat.p, s->wb.p, nullptr, s->h[0].p);
-  TRY_RC(mp_forward_layers(c, s, false));
-  k_mp_decode<<<gw(n), 256, 0, c->stream>>>(n, s->h[NL].p, s->wb.p, s->a.p, s->dscal.p, qs_fixed_mask(c), z);
+  const uint8_t* fixed = qs_fixed_mask(c);
+  k_pt_restrict<double><<<gw(s->np), 256, 0, c->stream>>>(s->np, s->patch_cell.p, s->cstart.p, s->sorted.p, r, fixed,
+                                                          s->scale.p, 1.0, s->v[0].p);
+  TRY_RC(mp_forward(c, s, 0, false));
+  TRY_RC(mp_transpose(c, s, s->h[0][NL].p));
+  k_pt_prolong<<<g1(c->n), 256, 0, c->stream>>>(c->n, s->pid.p, s->out3.p, s->scale.p, 1.0, fixed, z);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
 }
 
-// z = a + s_a (Wd h3 + bd) in FP64 from a float `a`; prescribed dofs zero.
-__global__ void __launch_bounds__(256) k_mp_zout(int64_t n, const __nv_bfloat16* __restrict__ h3,
-                                                 const __nv_bfloat16* __restrict__ wb, const float* __restrict__ a,
-                                                 double sa, const uint8_t* __restrict__ fixed,
-                                                 double* __restrict__ z) {
-  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= n) return;
-  const float2 hv = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(h3)[(int64_t)(H / 2) * i + lane]);
-  float o[3];
-  for (int c = 0; c < 3; ++c) {
-    float s = bf(wb[OFF_WD + c * H + 2 * lane]) * hv.x + bf(wb[OFF_WD + c * H + 2 * lane + 1]) * hv.y;
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    o[c] = s + bf(wb[OFF_BD + c]);
-  }
-  if (lane < 3) {
-    const uint8_t fx = fixed ? fixed[i] : 0;
-    z[3 * i + lane] = ((fx >> lane) & 1) ? 0.0 : (double)a[3 * i + lane] + sa * (double)o[lane];
-  }
-}
-
-// res = scale*q - r (prescribed dofs zero); partials of |res|^2 and |r|^2
-__global__ void k_mp_residual(int64_t m, double scale, const double* __restrict__ q, const float* __restrict__ r,
-                              const uint8_t* __restrict__ fixed, double* __restrict__ res,
-                              double* __restrict__ partial) {
-  __shared__ double s0[256], s1[256];
-  double a0 = 0.0, a1 = 0.0;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
-    const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
-    const double rk = fx ? 0.0 : (double)r[k];
-    const double v = fx ? 0.0 : scale * q[k] - rk;
-    res[k] = v;
-    a0 += v * v;
-    a1 += rk * rk;
-  }
-  s0[threadIdx.x] = a0;
-  s1[threadIdx.x] = a1;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if (threadIdx.x < o) s0[threadIdx.x] += s0[threadIdx.x + o], s1[threadIdx.x] += s1[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) partial[2 * blockIdx.x] = s0[0], partial[2 * blockIdx.x + 1] = s1[0];
-}
-
-// gout = coef * kres (prescribed dofs zero)
-__global__ void k_mp_gout(int64_t m, double coef, const double* __restrict__ kres, const uint8_t* __restrict__ fixed,
-                          float* __restrict__ gout) {
-  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= m) return;
-  const bool fx = fixed && ((fixed[k / 3] >> (k % 3)) & 1);
-  gout[k] = fx ? 0.f : (float)(coef * kres[k]);
-}
-
-// One pair (a = P_bj r, r as float [3n] each): forward with saved activations,
-// residual-space loss L = |kscale K z - r|^2 / |r|^2 with K the tangent prepared
-// by qs_prepare_current (kscale rescales it to the modulus of the pair), and
-// backward accumulating into s->g. dL/dz = 2 kscale K (kscale K z - r)/|r|^2.
+// One pair (a = P_bj r, r, e as float [3n] each, captured at modulus kscale x
+// the current one): z = a + [coarse] + Q S G^T G S Q^T r (coarse and middle
+// terms at the pair's modulus, 1/kscale); L = 1 - (r.z)^2 / ((z.Kp z)(e.r)),
+// Kp = kscale K with K the tangent prepared by qs_prepare_current; the weight
+// gradient is added into g_.
 static int mp_pair_grad(pd_ctx* c, MpnnState* s, const float* pair, double kscale, double* loss) {
-  const int64_t n = c->n, m = 3 * n;
+  const int64_t n = c->n, m = 3 * n, np = s->np;
   const float* A = pair;
   const float* R = pair + 3 * n;
+  const float* E = pair + 6 * n;
   const uint8_t* fixed = qs_fixed_mask(c);
-  DBuf<double> part, z, kz, res, kres;
-  PD_CUDA_TRY(c, part.alloc(2 * kRed));
+  DBuf<double> part, z, kz;
+  PD_CUDA_TRY(c, part.alloc(3 * kRed));
   PD_CUDA_TRY(c, z.alloc(m));
   PD_CUDA_TRY(c, kz.alloc(m));
-  PD_CUDA_TRY(c, res.alloc(m));
-  PD_CUDA_TRY(c, kres.alloc(m));
-  std::vector<float> ha(m), hr(m);
-  PD_CUDA_TRY(c, cudaMemcpyAsync(ha.data(), A, m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-  PD_CUDA_TRY(c, cudaMemcpyAsync(hr.data(), R, m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  double a2 = 0.0, r2 = 0.0;
-  for (int64_t k = 0; k < m; ++k) a2 += (double)ha[k] * ha[k], r2 += (double)hr[k] * hr[k];
-  const double sa = std::sqrt(a2 / (double)m), sr = std::sqrt(r2 / (double)m);
-  const float hs[2] = {(float)(sa > 0 ? 1.0 / sa : 0.0), (float)(sr > 0 ? 1.0 / sr : 0.0)};
-  PD_CUDA_TRY(c, cudaMemcpyAsync(s->scal.p, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
-  k_mp_features<float><<<g1(n), 256, 0, c->stream>>>(n, A, R, s->scal.p, s->feat.p);
-  k_mp_encode<<<gw(n), 256, 0, c->stream>>>(n, s->feat.p, s->wb.p, s->pre[0].p, s->h[0].p);
-  TRY_RC(mp_forward_layers(c, s, true));
-  k_mp_zout<<<gw(n), 256, 0, c->stream>>>(n, s->h[NL].p, s->wb.p, A, sa, fixed, z.p);
+  k_mp_base<<<g1(m), 256, 0, c->stream>>>(m, A, fixed, z.p);
+  if (s->coarse_cell >= 0.0) TRY_RC(coarse_apply_add_f(c, R, z.p, fixed, 1.0 / kscale));
+  k_pt_restrict<float><<<gw(np), 256, 0, c->stream>>>(np, s->patch_cell.p, s->cstart.p, s->sorted.p, R, fixed,
+                                                      s->scale.p, 1.0, s->v[0].p);
+  TRY_RC(mp_forward(c, s, 0, true));
+  TRY_RC(mp_transpose(c, s, s->h[0][NL].p));
+  k_pt_prolong<<<g1(n), 256, 0, c->stream>>>(n, s->pid.p, s->out3.p, s->scale.p, 1.0 / kscale, fixed, z.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   TRY_RC(qs_apply_K(c, z.p, kz.p));
-  k_mp_residual<<<kRed, 256, 0, c->stream>>>(m, kscale, kz.p, R, fixed, res.p, part.p);
-  TRY_RC(qs_apply_K(c, res.p, kres.p));
-  std::vector<double> hp(2 * kRed);
-  PD_CUDA_TRY(c, cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  double rs2 = 0.0, rr2 = 0.0;
-  for (int b = 0; b < kRed; ++b) rs2 += hp[2 * b], rr2 += hp[2 * b + 1];
-  const double inv_r2 = rr2 > 0 ? 1.0 / rr2 : 0.0;
-  // dL/dout = s_a dL/dz
-  k_mp_gout<<<g1(m), 256, 0, c->stream>>>(m, 2.0 * kscale * inv_r2 * sa, kres.p, fixed, s->gout.p);
-  // backward
-  k_mp_dec_wgrad<<<1, 3 * H + 3, 0, c->stream>>>(n, s->gout.p, s->h[NL].p, s->g.p);
-  k_mp_decode_back<<<gw(n), 256, 0, c->stream>>>(n, s->wb.p, s->gout.p, s->dh.p);
-  for (int l = NL - 1; l >= 0; --l) {
-    const __nv_bfloat16* wl = s->wb.p + OFF_L + l * LSZ;
-    k_mp_layer_back<<<gw(n), 256, 0, c->stream>>>(n, s->mrow.p, wl, s->pre[l + 1].p, s->dh.p, s->dhs.p, s->dm.p);
-    k_mp_wgrad<__nv_bfloat16><<<kRed, 256, 0, c->stream>>>(n, H, s->dh.p, s->h[l].p, s->gpart.p);
-    k_mp_wgrad_reduce<<<17, 256, 0, c->stream>>>(kRed, H, s->gpart.p, s->g.p, OFF_L + l * LSZ, OFF_L + l * LSZ + 2 * H * H);
-    k_mp_wgrad<float><<<kRed, 256, 0, c->stream>>>(n, H, s->dh.p, s->m[l].p, s->gpart.p);
-    // Wn has no bias of its own: only the matrix part of this reduction is kept
-    k_mp_wgrad_reduce<<<17, 256, 0, c->stream>>>(kRed, H, s->gpart.p, s->g.p, OFF_L + l * LSZ + H * H, -1);
-    k_mp_gather_back<<<gw(n), 256, 0, c->stream>>>(n, s->mrow.p, s->mcol.p, s->dhs.p, s->dm.p, s->dh.p);
+  k_mp_dots3<<<kRed, 256, 0, c->stream>>>(m, R, z.p, kz.p, E, fixed, part.p);
+  std::vector<double> hp(3 * kRed);
+  PD_CUDA_TRY(c, d2h(c, hp.data(), part.p, hp.size() * sizeof(double)));
+  double a = 0.0, b = 0.0, e = 0.0;
+  for (int k = 0; k < kRed; ++k) a += hp[3 * k], b += hp[3 * k + 1], e += hp[3 * k + 2];
+  b *= kscale;
+  if (!(b > 0.0) || !(e > 0.0)) {
+    *loss = 1.0;  // z (or the pair) carries no energy: nothing to learn from it
+    return PD_OK;
   }
-  k_mp_relu_back<<<g1((int64_t)H * n), 256, 0, c->stream>>>((int64_t)H * n, s->pre[0].p, s->dh.p);
-  k_mp_wgrad<float><<<kRed, 256, 0, c->stream>>>(n, F, s->dh.p, s->feat.p, s->gpart.p);
-  k_mp_wgrad_reduce<<<2, 256, 0, c->stream>>>(kRed, F, s->gpart.p, s->g.p, OFF_W0, OFF_B0);
-  PD_CUDA_TRY(c, cudaGetLastError());
+  // dL/dz = -2a/(b e) r + 2a^2/(b^2 e) kscale K z (into z); dL/dw = (1/kscale) S Q^T dL/dz
+  k_mp_gz<<<g1(m), 256, 0, c->stream>>>(m, -2.0 * a / (b * e), R, 2.0 * a * a * kscale / (b * b * e), kz.p, fixed,
+                                        z.p);
+  k_pt_restrict<double><<<gw(np), 256, 0, c->stream>>>(np, s->patch_cell.p, s->cstart.p, s->sorted.p, z.p, fixed,
+                                                       s->scale.p, 1.0 / kscale, s->v[1].p);
+  TRY_RC(mp_forward(c, s, 1, true));
+  TRY_RC(mp_backward(c, s, 0, s->h[1][NL].p));
+  TRY_RC(mp_backward(c, s, 1, s->h[0][NL].p));
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  *loss = rs2 * inv_r2;
+  *loss = 1.0 - a * a / (b * e);
+  return PD_OK;
+}
+
+// Tangent, block Jacobi, patch scales and (when on) the coarse operator at
+// the context's current displacement.
+static int mp_prepare_training(pd_ctx* c, MpnnState* s) {
+  TRY_RC(qs_prepare_current(c));
+  const double* dinv = nullptr;
+  TRY_RC(qs_block_jacobi_current(c, &dinv));
+  TRY_RC(mpnn_prepare(c, dinv));
+  if (s->coarse_cell >= 0.0) TRY_RC(qs_build_coarse_current(c, s->coarse_cell));
   return PD_OK;
 }
 
@@ -690,14 +777,13 @@ int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_
     c->err = "learned preconditioner not initialised";
     return PD_ERR_STATE;
   }
-  TRY_RC(mp_alloc(c, s, true));
-  TRY_RC(qs_prepare_current(c));
+  TRY_RC(mp_prepare_training(c, s));
   DBuf<float> pair;
-  PD_CUDA_TRY(c, pair.alloc(6 * c->n));
-  PD_CUDA_TRY(c, h2d(c, pair.p, pair_host, 6 * c->n * sizeof(float)));
-  PD_CUDA_TRY(c, cudaMemsetAsync(s->g.p, 0, NPARAM * sizeof(float), c->stream));
+  PD_CUDA_TRY(c, pair.alloc(9 * c->n));
+  PD_CUDA_TRY(c, h2d(c, pair.p, pair_host, 9 * c->n * sizeof(float)));
+  PD_CUDA_TRY(c, cudaMemsetAsync(s->g_.p, 0, NPARAM * sizeof(float), c->stream));
   TRY_RC(mp_pair_grad(c, s, pair.p, 1.0, loss));
-  if (grad_host) PD_CUDA_TRY(c, d2h(c, grad_host, s->g.p, NPARAM * sizeof(float)));
+  if (grad_host) PD_CUDA_TRY(c, d2h(c, grad_host, s->g_.p, NPARAM * sizeof(float)));
   return PD_OK;
 }
 
@@ -711,11 +797,23 @@ int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {
     c->err = "no training pairs collected";
     return PD_ERR_STATE;
   }
-  TRY_RC(mp_alloc(c, s, true));
-  TRY_RC(qs_prepare_current(c));
+  TRY_RC(mp_prepare_training(c, s));
   const int64_t n = c->n;
   const double k_now = current_modulus(c);
   std::mt19937_64 rng(12345 + s->adam_t);
+  // Random probes (e uniform on the free dofs, r = K e) join every batch, one
+  // per four captured pairs: CG iterates' errors are smooth, and without the
+  // rough modes the network could amplify them unseen.
+  const double* dinv = nullptr;
+  TRY_RC(qs_block_jacobi_current(c, &dinv));
+  DBuf<double> pe, pz, pr;
+  DBuf<float> ppair;
+  PD_CUDA_TRY(c, pe.alloc(3 * n));
+  PD_CUDA_TRY(c, pz.alloc(3 * n));
+  PD_CUDA_TRY(c, pr.alloc(3 * n));
+  PD_CUDA_TRY(c, ppair.alloc(9 * n));
+  const int nprobe = std::max(1, batch / 4);
+  uint64_t probe_seed = 0x5DEECE66Dull + 7919ull * (uint64_t)s->adam_t;
   std::vector<int64_t> order(s->npairs);
   double last = 0.0;
   for (int ep = 0; ep < epochs; ++ep) {
@@ -724,7 +822,7 @@ int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {
     double acc = 0.0;
     int64_t cnt = 0;
     for (int64_t b0 = 0; b0 < s->npairs; b0 += batch) {
-      PD_CUDA_TRY(c, cudaMemsetAsync(s->g.p, 0, NPARAM * sizeof(float), c->stream));
+      PD_CUDA_TRY(c, cudaMemsetAsync(s->g_.p, 0, NPARAM * sizeof(float), c->stream));
       const int64_t b1 = std::min<int64_t>(s->npairs, b0 + batch);
       for (int64_t q = b0; q < b1; ++q) {
         double l = 0.0;
@@ -732,11 +830,18 @@ int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {
         acc += l;
         ++cnt;
       }
+      for (int q = 0; q < nprobe; ++q) {
+        k_mp_rand_e<<<g1(3 * n), 256, 0, c->stream>>>(3 * n, probe_seed++, qs_fixed_mask(c), pe.p, pz.p);
+        TRY_RC(qs_apply_K(c, pe.p, pr.p));
+        k_mp_make_pair<<<g1(n), 256, 0, c->stream>>>(n, dinv, pr.p, pe.p, pz.p, ppair.p);
+        double l = 0.0;
+        TRY_RC(mp_pair_grad(c, s, ppair.p, 1.0, &l));
+      }
       s->adam_t += 1;
       const float b1c = 0.9f, b2c = 0.999f;
       const float c1 = 1.f - std::pow(b1c, (float)s->adam_t), c2 = 1.f - std::pow(b2c, (float)s->adam_t);
-      k_mp_adam<<<(NPARAM + 255) / 256, 256, 0, c->stream>>>(NPARAM, s->w.p, s->g.p, s->am.p, s->av.p, (float)lr, b1c,
-                                                             b2c, c1, c2, 1.0f / (float)(b1 - b0), s->wb.p);
+      k_mp_adam<<<(NPARAM + 255) / 256, 256, 0, c->stream>>>(NPARAM, s->w.p, s->g_.p, s->am.p, s->av.p, (float)lr, b1c,
+                                                             b2c, c1, c2, 1.0f / (float)(b1 - b0 + nprobe), s->wb.p);
       PD_CUDA_TRY(c, cudaGetLastError());
     }
     last = cnt ? acc / cnt : 0.0;
@@ -747,7 +852,7 @@ int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {
   return PD_OK;
 }
 
-// ---- pair capture from the block-Jacobi CG ---------------------------------
+// ---- pair capture from the block-Jacobi / two-level CG ----------------------
 int mpnn_set_capture(pd_ctx* c, int every) {
   if (!c->mpnn) c->mpnn = new MpnnState();
   mp_state(c)->every = every;
@@ -823,7 +928,7 @@ int mpnn_get_weights(pd_ctx* c, float* w) {
 
 int mpnn_set_weights(pd_ctx* c, const float* w) {
   MpnnState* s = mp_state(c);
-  if (!s || !s->mrow.p) {
+  if (!s || !s->w.p) {
     c->err = "call pd_mpnn_init before loading weights";
     return PD_ERR_STATE;
   }
@@ -836,5 +941,15 @@ int mpnn_set_weights(pd_ctx* c, const float* w) {
 }
 
 int mpnn_num_params() { return NPARAM; }
+
+double mpnn_coarse_cell(const pd_ctx* c) {
+  return c->mpnn ? reinterpret_cast<const MpnnState*>(c->mpnn)->coarse_cell : -1.0;
+}
+
+int mpnn_set_coarse(pd_ctx* c, double cell) {
+  if (!c->mpnn) c->mpnn = new MpnnState();
+  mp_state(c)->coarse_cell = cell < 0.0 ? -1.0 : cell;
+  return PD_OK;
+}
 
 }  // namespace pdb

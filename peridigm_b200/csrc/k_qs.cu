@@ -12,7 +12,8 @@
 //  * preconditioned CG with deterministic FP64 dot products; block-Jacobi
 //    preconditioner = inverses of the analytic 3x3 diagonal blocks of K
 //    (the reference's "Block 3x3" preconditioner, Peridigm.cpp:1603-1646);
-//    the learned preconditioner plugs in through mpnn_apply;
+//    the two-level and learned preconditioners add k_coarse.cu's coarse
+//    correction and k_mpnn.cu's learned middle level to it;
 //  * Newton with a backtracking step on the reference's convergence metric
 //    ||r||_2 + 20 ||r||_inf (Peridigm.cpp:4316).
 // For a bond (i,j) with Y = y_j - y_i, e = |Y| - |X|, de = Yhat.(w_j - w_i):
@@ -39,6 +40,13 @@ struct QsState {
   DBuf<double> th, nd, f, r, du, x, z, q, pred, dinv, partial, scal;
   DBuf<uint8_t> fixed;  // bit c: dof c prescribed
   int64_t n = 0;
+  bool coarse_on = false;  // the preconditioner adds the aggregate coarse correction (k_coarse.cu)
+  // Coarse-operator reuse: the operator is rebuilt when the model changed, or
+  // when a solve needs more than 1.3x (+5) the CG iterations of the first solve
+  // after the last rebuild (the tangent drifted from the one it was built at).
+  double coarse_cell = -1.0;
+  int64_t coarse_ref_iters = -1;
+  bool coarse_rebuild = true;
 };
 
 __device__ __forceinline__ double qs_omega(int kind, double zeta, double h) {
@@ -465,11 +473,15 @@ static int qs_residual(pd_ctx* c, double* l2, double* linf) {
   return PD_OK;
 }
 
+// z = M r: block Jacobi, plus the coarse correction (two-level), plus the
+// network's correction (learned).
 static int qs_apply_precond(pd_ctx* c, int precond, const double* r, double* z) {
   QsState* s = c->qs;
-  if (precond == PD_PRECOND_MPNN) return mpnn_apply(c, r, z, s->dinv.p);
-  k_qs_precond<<<g1(c->n), kQsBlock, 0, c->stream>>>(c->n, s->dinv.p, r, z, precond == PD_PRECOND_BLOCK_JACOBI);
+  k_qs_precond<<<g1(c->n), kQsBlock, 0, c->stream>>>(c->n, s->dinv.p, r, z, precond != PD_PRECOND_NONE);
   PD_CUDA_TRY(c, cudaGetLastError());
+  if (precond == PD_PRECOND_MPNN) TRY_RC(mpnn_apply_add(c, r, z));
+  if (s->coarse_on && (precond == PD_PRECOND_MPNN || precond == PD_PRECOND_TWO_LEVEL))
+    TRY_RC(coarse_apply_add(c, r, z, s->fixed.p));
   return PD_OK;
 }
 
@@ -506,10 +518,12 @@ static void k_qs_pack_x(int64_t n, QsState* s, pd_ctx* c) {
 static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out,
                      bool* stalled);
 
-// CG with the learned preconditioner first and block Jacobi as the fallback:
-// when the flexible iteration stalls, or when the true FP64 residual |b - K x|
-// (recomputed, not the recursive one) misses the tolerance, the solve restarts
-// from the current x with block Jacobi. The true residual is the judge.
+// CG with the learned preconditioner first and its base without the network
+// (block Jacobi, with the coarse correction when the network sits on the
+// two-level preconditioner) as the fallback: when the flexible iteration
+// stalls, or when the true FP64 residual |b - K x| (recomputed, not the
+// recursive one) misses the tolerance, the solve restarts from the current x
+// with the base. The true residual is the judge.
 static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out) {
   QsState* s = c->qs;
   const int64_t m = 3 * c->n;
@@ -558,7 +572,8 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
   const double tol2 = (std::isfinite(true_rel) && true_rel > 0) ? std::min(1.0, rel_tol / true_rel) : rel_tol;
   int its2 = 0;
   double rel2 = 0.0;
-  rc = qs_cg_run(c, PD_PRECOND_BLOCK_JACOBI, tol2, max_it, &its2, &rel2, &stalled);
+  rc = qs_cg_run(c, s->coarse_on ? PD_PRECOND_TWO_LEVEL : PD_PRECOND_BLOCK_JACOBI, tol2, max_it, &its2, &rel2,
+                 &stalled);
   k_qs_axpy<<<g1(m), kQsBlock, 0, c->stream>>>(m, 1.0, x0.p, s->x.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   *iters = its + its2;
@@ -571,7 +586,8 @@ static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* it
   QsState* s = c->qs;
   const int64_t n = c->n, m = 3 * n;
   const bool flexible = precond == PD_PRECOND_MPNN;
-  const int every = (precond == PD_PRECOND_BLOCK_JACOBI) ? mpnn_capture_every(c) : 0;
+  const int every =
+      (precond == PD_PRECOND_BLOCK_JACOBI || precond == PD_PRECOND_TWO_LEVEL) ? mpnn_capture_every(c) : 0;
   double best = 1.0;
   int best_it = 0;
   *stalled = false;
@@ -713,6 +729,40 @@ int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev) {
 // Tangent at the context's current displacement, for repeated products.
 int qs_prepare_current(pd_ctx* c) { return qs_prepare_at(c, c->u.p); }
 
+// Block-Jacobi inverse blocks at the tangent prepared by qs_prepare_current.
+int qs_block_jacobi_current(pd_ctx* c, const double** dinv_out) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_block_diag<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p,
+                                                     c->pt.p, c->hp.p, c->influence, s->fixed.p, s->dinv.p, 1);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  *dinv_out = s->dinv.p;
+  return PD_OK;
+}
+
+// Coarse operator at the tangent prepared by qs_prepare_current.
+int qs_build_coarse_current(pd_ctx* c, double cell) {
+  QsState* s = c->qs;
+  TRY_RC(coarse_build(c, s->yq.p, s->abq.p, s->fixed.p, cell, nullptr));
+  s->coarse_on = true;
+  s->coarse_rebuild = true;  // the next load step builds its own
+  return PD_OK;
+}
+
+// Coarse space at displacement u: size, aggregates, assembled matrix and inverse (device buffers, may be null).
+int qs_coarse_operator(pd_ctx* c, const double* u_dev, double cell, int64_t* n_coarse, int32_t* agg_dev,
+                       double* A_dev, double* Ainv_dev) {
+  TRY_RC(qs_prepare_at(c, u_dev));
+  QsState* s = c->qs;
+  TRY_RC(coarse_build(c, s->yq.p, s->abq.p, s->fixed.p, cell, A_dev));
+  s->coarse_rebuild = true;
+  *n_coarse = coarse_size(c);
+  if (agg_dev) TRY_RC(coarse_aggregates(c, agg_dev));
+  if (Ainv_dev) TRY_RC(coarse_copy_inverse(c, Ainv_dev));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return PD_OK;
+}
+
 // kw = K w with the tangent prepared by qs_prepare_current.
 int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev) {
   QsState* s = c->qs;
@@ -767,18 +817,36 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, c->stream);
+  const bool two_level =
+      precond == PD_PRECOND_TWO_LEVEL || (precond == PD_PRECOND_MPNN && mpnn_coarse_cell(c) >= 0.0);
+  const double cell = precond == PD_PRECOND_MPNN ? mpnn_coarse_cell(c) : o->coarse_cell;
+  s->coarse_on = false;
   while (metric > newton_tol && newton < o->max_newton_iterations) {
     if (precond != PD_PRECOND_NONE) {
       k_qs_qm<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->pt.p, s->abq.p);
       k_qs_block_diag<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p,
                                                          c->pt.p, c->hp.p, c->influence, s->fixed.p, s->dinv.p, 1);
       PD_CUDA_TRY(c, cudaGetLastError());
+      if (precond == PD_PRECOND_MPNN) TRY_RC(mpnn_prepare(c, s->dinv.p));
+    }
+    if (two_level) {
+      if (s->coarse_rebuild || !coarse_valid(c) || s->coarse_cell != std::max(0.0, cell)) {
+        TRY_RC(coarse_build(c, s->yq.p, s->abq.p, s->fixed.p, std::max(0.0, cell), nullptr));
+        s->coarse_cell = std::max(0.0, cell);
+        s->coarse_ref_iters = -1;
+        s->coarse_rebuild = false;
+      }
+      s->coarse_on = true;
     }
     int its = 0;
     double rel = 0.0;
     int rc = qs_cg(c, precond, o->cg_relative_tolerance, o->max_cg_iterations, &its, &rel);
     cg_total += its;
     last_rel = rel;
+    if (two_level) {
+      if (s->coarse_ref_iters < 0) s->coarse_ref_iters = its;
+      else if (its > (13 * s->coarse_ref_iters) / 10 + 5) s->coarse_rebuild = true;
+    }
     if (rc != PD_OK && rc != PD_ERR_NOT_CONVERGED) return rc;
     // du += alpha * x, backtracking on the convergence metric
     double alpha = 1.0, prev = metric;

@@ -96,6 +96,7 @@ struct DBuf {
 
 struct ContactState;
 struct QsState;
+struct CoarseState;
 
 }  // namespace pdb
 
@@ -171,6 +172,7 @@ struct pd_ctx {
   int64_t klaunches = 0;
   pdb::ContactState* contact = nullptr;
   pdb::QsState* qs = nullptr;
+  pdb::CoarseState* coarse = nullptr;  // aggregate coarse level of the QS preconditioners (k_coarse.cu)
   void* mpnn = nullptr;        // learned preconditioner state (k_mpnn.cu)
   int64_t qs_fallbacks = 0;    // learned-preconditioner solves that fell back to block Jacobi
 };
@@ -201,9 +203,11 @@ int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev);
 int qs_prepare_current(pd_ctx* c);
 int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev);
 bool mpnn_ready(const pd_ctx* c);
-int mpnn_apply(pd_ctx* c, const double* r, double* z, const double* dinv);
+int mpnn_apply_add(pd_ctx* c, const double* r, double* z);
+int mpnn_prepare(pd_ctx* c, const double* dinv);
+int qs_block_jacobi_current(pd_ctx* c, const double** dinv_out);
 void mpnn_release(pd_ctx* c);
-int mpnn_init(pd_ctx* c, uint64_t seed, double radius);
+int mpnn_init(pd_ctx* c, uint64_t seed, double patch);
 int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out);
 int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_host);
 int mpnn_set_capture(pd_ctx* c, int every);
@@ -216,6 +220,23 @@ int mpnn_get_weights(pd_ctx* c, float* w);
 int mpnn_set_weights(pd_ctx* c, const float* w);
 int mpnn_num_params();
 const uint8_t* qs_fixed_mask(const pd_ctx* c);
+int qs_build_coarse_current(pd_ctx* c, double cell);
+double mpnn_coarse_cell(const pd_ctx* c);
+int mpnn_set_coarse(pd_ctx* c, double cell);
+
+// aggregate coarse level (k_coarse.cu)
+int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* fixed, double cell,
+                 double* assembled);
+int coarse_apply_add(pd_ctx* c, const double* r, double* z, const uint8_t* fixed);
+int coarse_apply_add_f(pd_ctx* c, const float* r, double* z, const uint8_t* fixed, double scale);
+int coarse_aggregates(pd_ctx* c, int32_t* agg_dev);
+int coarse_copy_inverse(pd_ctx* c, double* dst_dev);
+int64_t coarse_size(const pd_ctx* c);
+void coarse_release(pd_ctx* c);
+void coarse_invalidate(pd_ctx* c);  // the model changed: rebuild the operator before its next use
+bool coarse_valid(const pd_ctx* c);
+int qs_coarse_operator(pd_ctx* c, const double* u_dev, double cell, int64_t* n_coarse, int32_t* agg_dev,
+                       double* A_dev, double* Ainv_dev);
 
 // bonds
 int build_bonds_device(pd_ctx* c, const pd_plane_filter* filters, int nf);
