@@ -16,7 +16,7 @@
 //   g_ij = 3 om zeta V_j Yh / m_i
 //
 // (om = omega(zeta, horizon of the bond's owner), a = alpha, q = 3K/m - alpha/3,
-// T_ij the force-state sum of k_qs_df). The pair term couples each point to its
+// T_ij the force-state sum of k_qs_bond_geom). The pair term couples each point to its
 // bonds; the dilatation term is a sum of rank-one terms, one per point p,
 // (force response to dth_p) x (dth_p as a function of w). A family of radius
 // delta spans at most 2 cells per axis of a grid of side >= 2 delta, so every

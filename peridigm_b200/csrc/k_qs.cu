@@ -7,8 +7,10 @@
 // Peridigm.cpp:2800) and Belos CG (:2551-2573, :3321-3362):
 //  * residual r = V (f_int + f_ext), rows of prescribed dofs zeroed;
 //  * tangent K = -d r / d u applied matrix-free: the exact linearization of
-//    the LPS force in two bond passes (d theta, then d f), rows and columns of
-//    prescribed dofs replaced by identity (applyKinematicBC_InsertZerosAndSetDiagonal);
+//    the LPS force in two bond passes (d theta, then d f) over per-bond
+//    geometry built once per state (unit deformed bond, V_j om zeta,
+//    V_j T/|Y|, V_j om (alpha_i + alpha_j)), rows and columns of prescribed
+//    dofs replaced by identity (applyKinematicBC_InsertZerosAndSetDiagonal);
 //  * preconditioned CG with deterministic FP64 dot products; block-Jacobi
 //    preconditioner = inverses of the analytic 3x3 diagonal blocks of K
 //    (the reference's "Block 3x3" preconditioner, Peridigm.cpp:1603-1646);
@@ -41,6 +43,12 @@ struct QsState {
   DBuf<uint8_t> fixed;  // bit c: dof c prescribed
   int64_t n = 0;
   bool coarse_on = false;  // the preconditioner adds the aggregate coarse correction (k_coarse.cu)
+  // Per-bond tangent geometry at the current (y, theta, q, alpha), rebuilt
+  // after every change of the state (geo_dirty): g = (yh, V_j om zeta),
+  // gc = (V_j T / |Y|, V_j om (alpha_i + alpha_j)); zero for broken bonds.
+  DBuf<double4> geo;
+  DBuf<double2> gco;
+  bool geo_dirty = true;
   // Coarse-operator reuse: the operator is rebuilt when the model changed, or
   // when a solve needs more than 1.3x (+5) the CG iterations of the first solve
   // after the last rebuild (the tangent drifted from the one it was built at).
@@ -137,78 +145,91 @@ __global__ void k_qs_reduce(const double* __restrict__ partial, int nblk, int wi
   }
 }
 
-// Tangent pass 1: d theta_i into w[i].w
-__global__ void __launch_bounds__(kQsBlock) k_qs_dtheta(int64_t n, const int64_t* __restrict__ row,
-                                                        const int32_t* __restrict__ col,
-                                                        const uint8_t* __restrict__ dmg,
-                                                        const double4* __restrict__ xv,
-                                                        const double4* __restrict__ y,
-                                                        const double4* __restrict__ pt,
-                                                        const double* __restrict__ hp, int influence,
-                                                        double4* __restrict__ w) {
+// Per-bond tangent geometry (one lane group per owner, bonds strided over lanes).
+__global__ void __launch_bounds__(kQsBlock) k_qs_bond_geom(int64_t n, const int64_t* __restrict__ row,
+                                                           const int32_t* __restrict__ col,
+                                                           const uint8_t* __restrict__ dmg,
+                                                           const double4* __restrict__ xv,
+                                                           const double4* __restrict__ y,
+                                                           const double4* __restrict__ ab,
+                                                           const double* __restrict__ hp, int influence,
+                                                           double4* __restrict__ g, double2* __restrict__ gc) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
+  const int lane = threadIdx.x & (kQsTpo - 1);
+  if (i >= n) return;
+  const double4 xi = xv[i], yi = y[i], ai = ab[i];
+  const double h = hp[i];
+  for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+    if (dmg[b]) {
+      g[b] = make_double4(0.0, 0.0, 0.0, 0.0);
+      gc[b] = make_double2(0.0, 0.0);
+      continue;
+    }
+    const int32_t j = col[b];
+    const double4 xj = xv[j], yj = y[j], aj = ab[j];
+    const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
+    const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
+    const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
+    const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
+    const double e = dY - zeta;
+    const double om = qs_omega(influence, zeta, h);
+    const double T = om * (zeta * (ai.x * ai.y + aj.x * aj.y) + (ai.z + aj.z) * e);
+    const double V = xj.w;
+    g[b] = make_double4(Y0 / dY, Y1 / dY, Y2 / dY, V * om * zeta);
+    gc[b] = make_double2(V * T / dY, V * om * (ai.z + aj.z));
+  }
+}
+
+// Tangent pass 1 on the geometry: w[i].w = q_i dtheta_i = 3 (q_i/m_i) sum_j V_j om zeta yh.(w_j - w_i)
+__global__ void __launch_bounds__(kQsBlock) k_qs_dtheta_g(int64_t n, const int64_t* __restrict__ row,
+                                                          const int32_t* __restrict__ col,
+                                                          const double4* __restrict__ g,
+                                                          const double4* __restrict__ ab,
+                                                          const double4* __restrict__ pt, double4* __restrict__ w) {
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
   const int lane = threadIdx.x & (kQsTpo - 1);
   const bool valid = i < n;
   double acc = 0.0;
   if (valid) {
-    const double4 xi = xv[i], yi = y[i], wi = w[i];
-    const double h = hp[i];
+    const double4 wi = w[i];
     for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
-      if (dmg[b]) continue;
-      const int32_t j = col[b];
-      const double4 xj = xv[j], yj = y[j], wj = w[j];
-      const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
-      const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
-      const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
-      const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
-      const double de = (Y0 * (wj.x - wi.x) + Y1 * (wj.y - wi.y) + Y2 * (wj.z - wi.z)) / dY;
-      acc += 3.0 * qs_omega(influence, zeta, h) * zeta * de * xj.w;
+      const double4 gb = g[b];
+      const double4 wj = w[col[b]];
+      acc += gb.w * (gb.x * (wj.x - wi.x) + gb.y * (wj.y - wi.y) + gb.z * (wj.z - wi.z));
     }
   }
   acc = qs_group_sum(acc);
-  if (valid && lane == 0) w[i].w = acc / pt[i].x;
+  if (valid && lane == 0) w[i].w = 3.0 * (ab[i].y / pt[i].x) * acc;
 }
 
-// Tangent pass 2: q = K p = -V d f (prescribed rows: q = p); block partials of p.q
-__global__ void __launch_bounds__(kQsBlock) k_qs_df(int64_t n, const int64_t* __restrict__ row,
-                                                    const int32_t* __restrict__ col,
-                                                    const uint8_t* __restrict__ dmg,
-                                                    const double4* __restrict__ xv,
-                                                    const double4* __restrict__ y,
-                                                    const double4* __restrict__ ab,
-                                                    const double* __restrict__ hp, int influence,
-                                                    const double4* __restrict__ w, const uint8_t* __restrict__ fixed,
-                                                    double* __restrict__ q, double* __restrict__ partial) {
+// Tangent pass 2 on the geometry: q = K p = -V d f (prescribed rows: q = p); block partials of p.q
+//   V_j [dT yh + (T/|Y|)(dw - yh de)] = c2 (q dth_i + q dth_j) yh + V_j om (a_i + a_j) de yh + V_j T/|Y| (dw - yh de)
+__global__ void __launch_bounds__(kQsBlock) k_qs_df_g(int64_t n, const int64_t* __restrict__ row,
+                                                      const int32_t* __restrict__ col,
+                                                      const double4* __restrict__ g,
+                                                      const double2* __restrict__ gc,
+                                                      const double4* __restrict__ xv,
+                                                      const double4* __restrict__ w,
+                                                      const uint8_t* __restrict__ fixed, double* __restrict__ q,
+                                                      double* __restrict__ partial) {
   __shared__ double spq[kQsBlock];
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
   const int lane = threadIdx.x & (kQsTpo - 1);
   const bool valid = i < n;
   double d0 = 0.0, d1 = 0.0, d2 = 0.0;
-  double4 wi = make_double4(0, 0, 0, 0), xi = make_double4(0, 0, 0, 1);
+  double4 wi = make_double4(0, 0, 0, 0);
   if (valid) {
-    xi = xv[i];
-    const double4 yi = y[i], ai = ab[i];
     wi = w[i];
-    const double h = hp[i];
     for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
-      if (dmg[b]) continue;
-      const int32_t j = col[b];
-      const double4 xj = xv[j], yj = y[j], wj = w[j], aj = ab[j];
-      const double X0 = xj.x - xi.x, X1 = xj.y - xi.y, X2 = xj.z - xi.z;
-      const double Y0 = yj.x - yi.x, Y1 = yj.y - yi.y, Y2 = yj.z - yi.z;
-      const double zeta = sqrt(X0 * X0 + X1 * X1 + X2 * X2);
-      const double dY = sqrt(Y0 * Y0 + Y1 * Y1 + Y2 * Y2);
-      const double e = dY - zeta;
+      const double4 gb = g[b];
+      const double2 cb = gc[b];
+      const double4 wj = w[col[b]];
       const double w0 = wj.x - wi.x, w1 = wj.y - wi.y, w2 = wj.z - wi.z;
-      const double de = (Y0 * w0 + Y1 * w1 + Y2 * w2) / dY;
-      const double om = qs_omega(influence, zeta, h);
-      const double T = om * (zeta * (ai.x * ai.y + aj.x * aj.y) + (ai.z + aj.z) * e);
-      const double dT = om * (zeta * (wi.w * ai.y + wj.w * aj.y) + (ai.z + aj.z) * de);
-      const double V = xj.w, inv = 1.0 / dY;
-      const double y0 = Y0 * inv, y1 = Y1 * inv, y2 = Y2 * inv;
-      d0 += V * (dT * y0 + T * (w0 - y0 * de) * inv);
-      d1 += V * (dT * y1 + T * (w1 - y1 * de) * inv);
-      d2 += V * (dT * y2 + T * (w2 - y2 * de) * inv);
+      const double de = gb.x * w0 + gb.y * w1 + gb.z * w2;
+      const double sy = gb.w * (wi.w + wj.w) + (cb.y - cb.x) * de;
+      d0 += sy * gb.x + cb.x * w0;
+      d1 += sy * gb.y + cb.x * w1;
+      d2 += sy * gb.z + cb.x * w2;
     }
   }
   d0 = qs_group_sum(d0);
@@ -218,7 +239,7 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_df(int64_t n, const int64_t* __
   if (valid && lane < 3) {
     const double d = lane == 0 ? d0 : (lane == 1 ? d1 : d2);
     const double p = lane == 0 ? wi.x : (lane == 1 ? wi.y : wi.z);
-    const double out = ((fixed[i] >> lane) & 1) ? p : -xi.w * d;
+    const double out = ((fixed[i] >> lane) & 1) ? p : -xv[i].w * d;
     q[3 * i + lane] = out;
     pq = p * out;
   }
@@ -458,6 +479,7 @@ static int qs_residual(pd_ctx* c, double* l2, double* linf) {
   const int64_t n = c->n;
   k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, c->u.p, s->du.p, s->yq.p);
   PD_CUDA_TRY(c, launch_fp64_eval_at(c, s->yq.p, s->abq.p, s->th.p, s->nd.p, s->f.p));
+  s->geo_dirty = true;
   k_qs_residual<<<kRedBlocks, kQsBlock, 0, c->stream>>>(n, s->f.p, c->xv.p, s->fixed.p, s->r.p, s->partial.p);
   k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 2, 1, s->scal.p + 8);
   PD_CUDA_TRY(c, cudaGetLastError());
@@ -485,14 +507,23 @@ static int qs_apply_precond(pd_ctx* c, int precond, const double* r, double* z) 
   return PD_OK;
 }
 
-// Tangent-vector product q = K w.xyz (w.w receives d theta).
+// Tangent-vector product q = K w.xyz (w.w receives q dtheta) on the per-bond
+// geometry, rebuilt first when the state changed.
 static int qs_tangent(pd_ctx* c) {
   QsState* s = c->qs;
   const int64_t n = c->n;
-  k_qs_dtheta<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, c->pt.p,
-                                                 c->hp.p, c->influence, s->w.p);
-  k_qs_df<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p, c->hp.p,
-                                             c->influence, s->w.p, s->fixed.p, s->q.p, s->partial.p);
+  if (s->geo_dirty || s->geo.count < (size_t)c->nb) {
+    if (s->geo.count < (size_t)c->nb) {
+      PD_CUDA_TRY(c, s->geo.alloc((size_t)c->nb));
+      PD_CUDA_TRY(c, s->gco.alloc((size_t)c->nb));
+    }
+    k_qs_bond_geom<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p, s->abq.p,
+                                                      c->hp.p, c->influence, s->geo.p, s->gco.p);
+    s->geo_dirty = false;
+  }
+  k_qs_dtheta_g<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->abq.p, c->pt.p, s->w.p);
+  k_qs_df_g<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->gco.p, c->xv.p, s->w.p,
+                                               s->fixed.p, s->q.p, s->partial.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
 }
@@ -698,6 +729,7 @@ static int qs_prepare_at(pd_ctx* c, const double* u_dev) {
   PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, 3 * n * sizeof(double), c->stream));
   k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, u_dev, s->du.p, s->yq.p);
   PD_CUDA_TRY(c, launch_fp64_eval_at(c, s->yq.p, s->abq.p, s->th.p, s->nd.p, s->f.p));
+  s->geo_dirty = true;
   k_qs_qm<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->pt.p, s->abq.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
