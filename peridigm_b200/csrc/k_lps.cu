@@ -132,9 +132,6 @@ constexpr int kUnroll = PD_BOND_UNROLL;
 // gathers and computes batch t, its batch t+1 of bond records and neighbor ids
 // is already in flight into its own slots (two stages; each thread reads only
 // what it copied, so no block barrier is needed).
-#ifndef PD_BOND_STAGE
-#define PD_BOND_STAGE 1
-#endif
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
@@ -149,23 +146,27 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Stages batch `base` (kUnroll bonds, stride TPO) of a lane into slot `st`.
+// Stages one batch of a lane's row (the bonds at row offsets TPO*k from the
+// lane's cursor, k < kUnroll; `rem` bonds remain from the cursor) into slot
+// `st`: bond records and neighbor ids by cp.async where the bond exists, and
+// past the row end a dummy bond (X = (1,0,0), the owner as its own neighbor)
+// whose arithmetic stays finite and is masked by a select.
 template <int TPO>
 __device__ __forceinline__ void stage_batch(float4 (*sq)[kUnroll][kBlock], int32_t (*sj)[kUnroll][kBlock], int st,
-                                            int64_t base, int64_t b1, const float4* __restrict__ bx,
-                                            const int32_t* __restrict__ col) {
+                                            int rem, const float4* __restrict__ pbx,
+                                            const int32_t* __restrict__ pcol, int32_t self) {
 #pragma unroll
   for (int k = 0; k < kUnroll; ++k) {
-    const int64_t b = base + (int64_t)k * TPO;
-    if (b < b1) {
-      cp_async16(&sq[st][k][threadIdx.x], bx + b);
-      cp_async4(&sj[st][k][threadIdx.x], col + b);
+    if (TPO * k < rem) {
+      cp_async16(&sq[st][k][threadIdx.x], pbx + TPO * k);
+      cp_async4(&sj[st][k][threadIdx.x], pcol + TPO * k);
+    } else {
+      sq[st][k][threadIdx.x] = make_float4(1.f, 0.f, 0.f, 0.f);
+      sj[st][k][threadIdx.x] = self;
     }
   }
   cp_commit();
 }
-__device__ __forceinline__ float4 ld_stream(const float4* p) { return __ldcs(p); }
-__device__ __forceinline__ int32_t ld_stream(const int32_t* p) { return __ldcs(p); }
 
 // ---------------------------------------------------------------------------
 // K1: weighted volume m_i = sum_j omega*|xi|^2*V_j (material_utilities.cxx:161-188)
@@ -252,78 +253,42 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     ow = own[i];
     const Rec8 ui = ld_rec(ur + i);
     const float s_c = damage_on ? ow.w : -1.0f;
-#if PD_BOND_STAGE
+    // Row-local cursors; branch-free masking (selects) of past-the-end and
+    // broken bonds.
     __shared__ float4 sq[2][kUnroll][kBlock];
     __shared__ int32_t sj[2][kUnroll][kBlock];
+    constexpr int kStep = kUnroll * TPO;
+    const float4* nbx = bx + b0 + lane;
+    const int32_t* ncol = col + b0 + lane;
+    uint8_t* pdm = dmg + b0 + lane;
+    int rem = (int)(b1 - b0) - lane;
     int st = 0;
-    stage_batch<TPO>(sq, sj, 0, b0 + lane, b1, bx, col);
+    stage_batch<TPO>(sq, sj, 0, rem, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (int64_t base = b0 + lane; base < b1; base += kUnroll * TPO) {
-      stage_batch<TPO>(sq, sj, st ^ 1, base + kUnroll * TPO, b1, bx, col);  // next batch (maybe empty)
-      cp_wait<1>();                                                          // this batch has landed
+    for (; rem > 0; rem -= kStep, pdm += kStep) {
+      nbx += kStep;
+      ncol += kStep;
+      stage_batch<TPO>(sq, sj, st ^ 1, rem - kStep, nbx, ncol, (int32_t)i);  // next batch (maybe all dummies)
+      cp_wait<1>();                                                         // this batch has landed
       int dd[kUnroll];
-      int32_t jj[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const int64_t b = base + (int64_t)k * TPO;
-        const bool in = b < b1;
-        dd[k] = in ? (int)dmg[b] : 2;  // 2: past the row end
-        jj[k] = in ? sj[st][k][threadIdx.x] : (int32_t)i;
-      }
+      for (int k = 0; k < kUnroll; ++k) dd[k] = (TPO * k < rem) ? (int)pdm[TPO * k] : 2;  // 2: past the row end
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + jj[k]);
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + sj[st][k][threadIdx.x]);
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
-        if (dd[k] == 1) {
-          broken++;
-        } else if (dd[k] == 0) {
-          const float4 q = sq[st][k][threadIdx.x];
-          const SplitBond s = split_bond(q, ui, uu[k]);
-          if (s_c >= 0.0f && s.e > s_c * s.zeta) {
-            dmg[base + (int64_t)k * TPO] = 1;
-            broken++;
-          } else {
-            th = fmaf(q.w * s.zeta, s.e, th);
-          }
-        }
+        const float4 q = sq[st][k][threadIdx.x];
+        const SplitBond sb = split_bond(q, ui, uu[k]);
+        const bool intact = dd[k] == 0;
+        const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
+        if (brk) pdm[TPO * k] = 1;
+        broken += (dd[k] == 1 || brk) ? 1 : 0;
+        th = fmaf((intact && !brk) ? q.w * sb.zeta : 0.0f, sb.e, th);
       }
       st ^= 1;
     }
     cp_wait<0>();
-#else
-#pragma unroll 1
-    for (int64_t base = b0 + lane; base < b1; base += kUnroll * TPO) {
-      int dd[kUnroll];
-      int32_t jj[kUnroll];
-      float4 qq[kUnroll];
-      Rec8 uu[kUnroll];
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const int64_t b = base + (int64_t)k * TPO;
-        const bool in = b < b1;
-        dd[k] = in ? (int)dmg[b] : 2;  // 2: past the row end
-        jj[k] = in ? ld_stream(col + b) : (int32_t)i;
-        qq[k] = in ? ld_stream(bx + b) : make_float4(1.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + jj[k]);
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        if (dd[k] == 1) {
-          broken++;
-        } else if (dd[k] == 0) {
-          const SplitBond s = split_bond(qq[k], ui, uu[k]);
-          if (s_c >= 0.0f && s.e > s_c * s.zeta) {
-            dmg[base + (int64_t)k * TPO] = 1;
-            broken++;
-          } else {
-            th = fmaf(qq[k].w * s.zeta, s.e, th);
-          }
-        }
-      }
-    }
-#endif
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
@@ -496,73 +461,41 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
   if (valid) {
     const Rec8 ui = ld_rec_nc(ur + i);
     const int64_t b1 = row[i + 1];
-#if PD_BOND_STAGE
     __shared__ float4 sq[2][kUnroll][kBlock];
     __shared__ int32_t sj[2][kUnroll][kBlock];
-    const int64_t bs = row[i] + lane;
+    constexpr int kStep = kUnroll * TPO;
+    const int64_t b0 = row[i];
+    const float4* nbx = bx + b0 + lane;
+    const int32_t* ncol = col + b0 + lane;
+    const uint8_t* pdm = dmg + b0 + lane;
+    int rem = (int)(b1 - b0) - lane;
     int st = 0;
-    stage_batch<TPO>(sq, sj, 0, bs, b1, bx, col);
+    stage_batch<TPO>(sq, sj, 0, rem, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (int64_t base = bs; base < b1; base += kUnroll * TPO) {
-      stage_batch<TPO>(sq, sj, st ^ 1, base + kUnroll * TPO, b1, bx, col);
+    for (; rem > 0; rem -= kStep, pdm += kStep) {
+      nbx += kStep;
+      ncol += kStep;
+      stage_batch<TPO>(sq, sj, st ^ 1, rem - kStep, nbx, ncol, (int32_t)i);
       cp_wait<1>();
       bool live[kUnroll];
-      int32_t jj[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const int64_t b = base + (int64_t)k * TPO;
-        const bool in = b < b1;
-        live[k] = in && !dmg[b];
-        jj[k] = in ? sj[st][k][threadIdx.x] : (int32_t)i;
-      }
+      for (int k = 0; k < kUnroll; ++k) live[k] = (TPO * k < rem) ? pdm[TPO * k] == 0 : false;
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + sj[st][k][threadIdx.x]);
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
-        if (live[k]) {
-          const float4 q = sq[st][k][threadIdx.x];
-          const SplitBond s = split_bond(q, ui, uu[k]);
-          const float T = fmaf(s.zeta, ui.v[6] + uu[k].v[6], s.e * (ui.v[7] + uu[k].v[7]));
-          const float w = T * q.w * s.ry;
-          fx = fmaf(w, s.Yx, fx);
-          fy = fmaf(w, s.Yy, fy);
-          fz = fmaf(w, s.Yz, fz);
-        }
+        const float4 q = sq[st][k][threadIdx.x];
+        const SplitBond sb = split_bond(q, ui, uu[k]);
+        const float T = fmaf(sb.zeta, ui.v[6] + uu[k].v[6], sb.e * (ui.v[7] + uu[k].v[7]));
+        const float w = live[k] ? T * q.w * sb.ry : 0.0f;
+        fx = fmaf(w, sb.Yx, fx);
+        fy = fmaf(w, sb.Yy, fy);
+        fz = fmaf(w, sb.Yz, fz);
       }
       st ^= 1;
     }
     cp_wait<0>();
-#else
-#pragma unroll 1
-    for (int64_t base = row[i] + lane; base < b1; base += kUnroll * TPO) {
-      bool live[kUnroll];
-      int32_t jj[kUnroll];
-      float4 qq[kUnroll];
-      Rec8 uu[kUnroll];
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const int64_t b = base + (int64_t)k * TPO;
-        const bool in = b < b1;
-        live[k] = in && !dmg[b];
-        jj[k] = in ? ld_stream(col + b) : (int32_t)i;
-        qq[k] = in ? ld_stream(bx + b) : make_float4(1.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        if (live[k]) {
-          const SplitBond s = split_bond(qq[k], ui, uu[k]);
-          const float T = fmaf(s.zeta, ui.v[6] + uu[k].v[6], s.e * (ui.v[7] + uu[k].v[7]));
-          const float w = T * qq[k].w * s.ry;
-          fx = fmaf(w, s.Yx, fx);
-          fy = fmaf(w, s.Yy, fy);
-          fz = fmaf(w, s.Yz, fz);
-        }
-      }
-    }
-#endif
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
