@@ -136,6 +136,18 @@ int pd_material_lps(pd_ctx* ctx, int32_t block, double bulk_modulus, double shea
 /* Per-point moduli (an extension for heterogeneous bodies; the owner's values
  * take the place of the block constants at src/materials/elastic.cxx:99,119). */
 int pd_material_lps_field(pd_ctx* ctx, const double* bulk_modulus, const double* shear_modulus);
+/* Elastic bond-based material of a block ("Elastic Bond Based",
+ * PeridigmNS::ElasticBondBasedMaterial, src/materials/Peridigm_ElasticBondBasedMaterial.cpp:52-95;
+ * force MATERIAL_EVALUATION::computeInternalForceElasticBondBased,
+ * src/materials/elastic_bond_based.cxx:55-124): pair force
+ * 0.5 (1 - d) s c per bond and end, c = 18K/(pi delta^4) in 3D, or
+ * 12K/(pi height delta^3) with plane != 0 ("Plane Strain" / "Plane Stress",
+ * height > 0). One bond pass per evaluation (no dilatation, no influence
+ * function). All blocks of a context use one material model; the
+ * quasi-static entry points support the LPS model only. */
+#define PD_MATERIAL_LPS 0
+#define PD_MATERIAL_BOND_BASED 1
+int pd_material_bond_based(pd_ctx* ctx, int32_t block, double K, double rho, int32_t plane, double height);
 /* "Critical Stretch" damage (CriticalStretchDamageModel ctor, src/damage/Peridigm_CriticalStretchDamageModel.cpp:52-77)
  * for one block; s_c < 0 disables damage on that block. */
 int pd_damage_critical_stretch(pd_ctx* ctx, int32_t block, double critical_stretch);

@@ -71,6 +71,9 @@ class Explicit(C.Structure):
         ("dt", C.c_double),
         ("t0", C.c_double),
         ("nsteps", C.c_int),
+        ("material", C.c_int),
+        ("plane", C.c_int),
+        ("height", C.c_double),
     ]
 
 
@@ -104,6 +107,8 @@ def lib():
         L.pdo_dilatation.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, C.c_int, C.c_double, _dp]
         L.pdo_force_lps.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp, _dp,
                                     C.c_int, C.c_double, _dp]
+        L.pdo_force_bond_based.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp, C.c_double, C.c_int,
+                                           C.c_double, _dp]
         L.pdo_critical_time_step.restype = C.c_double
         L.pdo_critical_time_step.argtypes = [C.c_int64, _dp, _dp, _i64p, _i32p, _dp, _dp, C.c_double]
         L.pdo_contact_count.restype = C.c_int64
@@ -130,6 +135,8 @@ def ref_lib():
         L.pdref_dilatation.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_int, C.c_double]
         L.pdref_force_linear_elastic.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_int,
                                                  C.c_double, C.c_double, C.c_double]
+        L.pdref_force_bond_based.argtypes = [_dp, _dp, _dp, _dp, _dp, _i32p, C.c_int, C.c_double, C.c_double,
+                                             C.c_int, C.c_double]
         _ref = L
     return _ref
 
@@ -416,7 +423,8 @@ def explicit_run(prob, u, v, bond_damage=None):
 
     ``prob`` keys: x, vol, rho, K, mu, row, col, horizon, dt, nsteps; optional
     influence, s_c (enables damage), contact dict {r_search, freq, r_contact,
-    k_spring, friction, horizon}, bc_mask/bc_a/bc_b, t0.
+    k_spring, friction, horizon}, bc_mask/bc_a/bc_b, t0, material ("lps" or
+    "bond_based") with plane/height for the bond-based constant.
     """
     x = _f64(prob["x"])
     n = x.size // 3
@@ -441,6 +449,9 @@ def explicit_run(prob, u, v, bond_damage=None):
     P.col = _i32(col)
     P.influence = int(prob.get("influence", 0))
     P.horizon = float(prob["horizon"])
+    P.material = 1 if prob.get("material", "lps") == "bond_based" else 0
+    P.plane = 1 if prob.get("plane", False) else 0
+    P.height = float(prob.get("height", 0.0))
     sc = prob.get("s_c")
     P.damage_on = 1 if sc is not None else 0
     P.s_c = _d(arr(_per_point(sc if sc is not None else 0.0, n)))
@@ -476,6 +487,34 @@ def explicit_run(prob, u, v, bond_damage=None):
 # ---------------------------------------------------------------------------
 # Reference kernels (compiled from the reference's sources)
 # ---------------------------------------------------------------------------
+def force_bond_based(x, y, vol, row, col, K, horizon, bond_damage=None, plane=False, height=0.0):
+    """Restated computeInternalForceElasticBondBased (elastic_bond_based.cxx:55-124)."""
+    x, y, vol = _f64(x), _f64(y), _f64(vol)
+    n = vol.size
+    row = np.asarray(row, np.int64)
+    dmg = np.zeros(int(row[-1])) if bond_damage is None else _f64(bond_damage)
+    f = np.zeros(3 * n)
+    lib().pdo_force_bond_based(n, _d(x), _d(y), _d(vol), _d(dmg), _i64(row), _i32(col),
+                               _d(_per_point(K, n)), float(horizon), 1 if plane else 0, float(height), _d(f))
+    return f
+
+
+def ref_force_bond_based(x, y, vol, nl, n, K, horizon, bond_damage=None, plane=False, height=0.0):
+    """The reference's own computeInternalForceElasticBondBased<double>, compiled
+    from src/materials/elastic_bond_based.cxx, on a zeroed force vector."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libpdref.so is not built")
+    x, y, vol = _f64(x), _f64(y), _f64(vol)
+    nl = np.ascontiguousarray(nl, dtype=np.int32)
+    nb = len(nl) - n
+    dmg = np.zeros(nb) if bond_damage is None else _f64(bond_damage)
+    f = np.zeros(3 * n)
+    L.pdref_force_bond_based(_d(x), _d(y), _d(vol), _d(dmg), _d(f), _i32(nl), n, float(K), float(horizon),
+                             1 if plane else 0, float(height))
+    return f
+
+
 def ref_eval(x, y, vol, nl, n, K, mu, horizon, bond_damage=None):
     """computeWeightedVolume + computeDilatation + computeInternalForceLinearElastic
     exactly as ElasticMaterial::initialize/computeForce call them

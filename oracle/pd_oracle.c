@@ -328,6 +328,42 @@ void pdo_force_lps(int64_t n, const double* x, const double* y, const double* m,
 }
 
 /* ---------------------------------------------------------------------------
+ * Elastic bond-based force: MATERIAL_EVALUATION::computeInternalForceElasticBondBased<double>
+ * (src/materials/elastic_bond_based.cxx:55-124), scatter form (:118-123),
+ * constant 18K/(pi h^4) in 3D (:77) or 12K/(pi H h^3) for plane strain/stress
+ * (:75); K is the owner's. f is zeroed first as in
+ * ElasticBondBasedMaterial::computeForce (Peridigm_ElasticBondBasedMaterial.cpp:116).
+ * ------------------------------------------------------------------------- */
+void pdo_force_bond_based(int64_t n, const double* x, const double* y, const double* vol,
+                          const double* dmg, const int64_t* row, const int32_t* col, const double* K,
+                          double horizon, int plane, double height, double* f) {
+  const double pi = 3.14159265358979323846;
+  memset(f, 0, sizeof(double) * 3 * (size_t)n);
+  for (int64_t p = 0; p < n; ++p) {
+    const double* X = &x[3 * p];
+    const double* Y = &y[3 * p];
+    double c = plane ? 12.0 * K[p] / (pi * height * horizon * horizon * horizon)
+                     : 18.0 * K[p] / (pi * horizon * horizon * horizon * horizon);
+    for (int64_t b = row[p]; b < row[p + 1]; ++b) {
+      int64_t j = col[b];
+      double zeta = sqrt((x[3 * j] - X[0]) * (x[3 * j] - X[0]) + (x[3 * j + 1] - X[1]) * (x[3 * j + 1] - X[1]) +
+                         (x[3 * j + 2] - X[2]) * (x[3 * j + 2] - X[2]));
+      double dY = sqrt((y[3 * j] - Y[0]) * (y[3 * j] - Y[0]) + (y[3 * j + 1] - Y[1]) * (y[3 * j + 1] - Y[1]) +
+                       (y[3 * j + 2] - Y[2]) * (y[3 * j + 2] - Y[2]));
+      double stretch = (dY - zeta) / zeta;
+      double t = 0.5 * (1.0 - dmg[b]) * stretch * c;
+      double fx = t * (y[3 * j] - Y[0]) / dY, fy = t * (y[3 * j + 1] - Y[1]) / dY, fz = t * (y[3 * j + 2] - Y[2]) / dY;
+      f[3 * p + 0] += fx * vol[j];
+      f[3 * p + 1] += fy * vol[j];
+      f[3 * p + 2] += fz * vol[j];
+      f[3 * j + 0] -= fx * vol[p];
+      f[3 * j + 1] -= fy * vol[p];
+      f[3 * j + 2] -= fz * vol[p];
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------
  * Stable time step: PeridigmNS::ComputeCriticalTimeStep
  * (src/core/Peridigm_CriticalTimeStep.cpp:52-130), constant horizon, owner K.
  * ------------------------------------------------------------------------- */
@@ -506,9 +542,14 @@ static void eval_model(const pdo_explicit* p, const double* y, const double* v, 
     pdo_damage_critical_stretch(n, p->x, y, p->row, p->col, p->s_c, dmg_n, dmg_np1, node_damage);
   else
     memcpy(dmg_np1, dmg_n, sizeof(double) * (size_t)p->row[n]);
-  pdo_dilatation(n, p->x, y, m, p->vol, dmg_np1, p->row, p->col, p->influence, p->horizon, theta);
-  pdo_force_lps(n, p->x, y, m, p->vol, theta, dmg_np1, p->row, p->col, p->K, p->mu, p->influence,
-                p->horizon, f);
+  if (p->material == 1) {
+    memset(theta, 0, sizeof(double) * (size_t)n);
+    pdo_force_bond_based(n, p->x, y, p->vol, dmg_np1, p->row, p->col, p->K, p->horizon, p->plane, p->height, f);
+  } else {
+    pdo_dilatation(n, p->x, y, m, p->vol, dmg_np1, p->row, p->col, p->influence, p->horizon, theta);
+    pdo_force_lps(n, p->x, y, m, p->vol, theta, dmg_np1, p->row, p->col, p->K, p->mu, p->influence,
+                  p->horizon, f);
+  }
   if (p->contact_on)
     pdo_contact_force(n, y, v, p->vol, cl->crow, cl->ccol, p->r_contact, p->k_spring, p->friction,
                       p->contact_horizon, fc);

@@ -54,6 +54,9 @@ void pdo_damage_critical_stretch(int64_t n, const double* x, const double* y, co
 void pdo_dilatation(int64_t n, const double* x, const double* y, const double* m,
                     const double* vol, const double* dmg, const int64_t* row, const int32_t* col,
                     int influence, double horizon, double* theta);
+void pdo_force_bond_based(int64_t n, const double* x, const double* y, const double* vol,
+                          const double* dmg, const int64_t* row, const int32_t* col, const double* K,
+                          double horizon, int plane, double height, double* f);
 void pdo_force_lps(int64_t n, const double* x, const double* y, const double* m,
                    const double* vol, const double* theta, const double* dmg, const int64_t* row,
                    const int32_t* col, const double* K, const double* mu, int influence,
@@ -108,6 +111,9 @@ typedef struct {
   double dt;
   double t0;
   int nsteps;
+  int material;           /* 0: LPS (elastic), 1: elastic bond based */
+  int plane;              /* bond based: plane strain/stress constant */
+  double height;
 } pdo_explicit;
 
 /* State in/out: u, v [3n]; outputs a, f (force density incl. contact), fc,

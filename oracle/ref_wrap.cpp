@@ -1,11 +1,13 @@
-// C entry points over the reference's own LPS kernels, compiled from the
-// reference sources (src/materials/elastic.cxx, src/materials/material_utilities.cxx,
+// C entry points over the reference's own LPS and bond-based kernels, compiled
+// from the reference sources (src/materials/elastic.cxx,
+// src/materials/elastic_bond_based.cxx, src/materials/material_utilities.cxx,
 // src/core/Peridigm_InfluenceFunction.cpp) by oracle/Makefile into oracle/_ref/.
 // Test infrastructure only: the product never links this library.
 #include <stdexcept>
 #include <string>
 #include "material_utilities.h"
 #include "elastic.h"
+#include "elastic_bond_based.h"
 
 extern "C" {
 
@@ -43,6 +45,16 @@ void pdref_force_linear_elastic(const double* x, const double* y, const double* 
                                 double K, double mu, double horizon) {
   MATERIAL_EVALUATION::computeInternalForceLinearElastic<double>(
       x, y, m, vol, theta, bond_damage, f, nullptr, nl, n_owned, K, mu, horizon, 0.0, nullptr);
+}
+
+// MATERIAL_EVALUATION::computeInternalForceElasticBondBased<double>
+// (src/materials/elastic_bond_based.cxx:55-124); the caller zeroes f first, as
+// ElasticBondBasedMaterial::computeForce does (Peridigm_ElasticBondBasedMaterial.cpp:116).
+void pdref_force_bond_based(const double* x, const double* y, const double* vol, const double* bond_damage,
+                            double* f, const int* nl, int n_owned, double K, double horizon, int plane,
+                            double height) {
+  MATERIAL_EVALUATION::computeInternalForceElasticBondBased<double>(x, y, vol, bond_damage, f, nl, n_owned, K,
+                                                                    horizon, plane != 0, height);
 }
 
 }  // extern "C"

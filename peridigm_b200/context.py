@@ -134,6 +134,11 @@ class Context:
     def material(self, K, mu, rho, block=0):
         self._ok(self.L.pd_material_lps(self.h, int(block), float(K), float(mu), float(rho)))
 
+    def material_bond_based(self, K, rho, block=0, plane=False, height=0.0):
+        """Elastic bond-based material ("Elastic Bond Based"): 3D, or plane strain/stress with the height."""
+        self._ok(self.L.pd_material_bond_based(self.h, int(block), float(K), float(rho), 1 if plane else 0,
+                                               float(height)))
+
     def material_field(self, K, mu):
         K, mu = _f64(K, self.n, "K"), _f64(mu, self.n, "mu")
         self._ok(self.L.pd_material_lps_field(self.h, _d(K), _d(mu)))

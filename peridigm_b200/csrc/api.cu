@@ -102,7 +102,21 @@ int alloc_state(pd_ctx* c) {
 int ensure_ready(pd_ctx* c) {
   TRY(ensure_device(c));
   if (c->n == 0 || !c->row.p) return fail(c, PD_ERR_STATE, "points and bonds must be set first");
-  if (!c->have_material) return fail(c, PD_ERR_STATE, "no material: call pd_material_lps first");
+  if (!c->have_material)
+    return fail(c, PD_ERR_STATE, "no material: call pd_material_lps or pd_material_bond_based first");
+  {
+    int model = -1;
+    for (int m : c->block_model) {
+      if (m < 0) continue;
+      if (model >= 0 && m != model)
+        return fail(c, PD_ERR_UNSUPPORTED, "all blocks of a context must use one material model");
+      model = m;
+    }
+    if (model >= 0 && model != c->material_model) {
+      c->material_model = model;
+      c->wv_done = false;
+    }
+  }
   if (!c->symmetric)
     return fail(c, PD_ERR_UNSUPPORTED,
                 "bond families are not symmetric (j in H(i) without i in H(j)); the gather force pass needs "
@@ -201,6 +215,7 @@ int pd_create(const pd_config* cfg, pd_ctx** out) {
   c->block_mu.assign(1, 0.0);
   c->block_rho.assign(1, 0.0);
   c->block_sc.assign(1, -1.0);
+  c->block_model.assign(1, -1);
   *out = c;
   return PD_OK;
 }
@@ -245,6 +260,7 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   c->block_mu.resize(nblk, 0.0);
   c->block_rho.resize(nblk, 0.0);
   c->block_sc.resize(nblk, -1.0);
+  c->block_model.resize(nblk, -1);
   std::vector<double4> xv(n);
   for (int64_t i = 0; i < n; ++i) xv[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], vol[i]);
   PD_CUDA_TRY(c, c->xv.alloc(n));
@@ -370,6 +386,25 @@ int pd_material_lps(pd_ctx* c, int32_t block, double K, double mu, double rho) {
   c->block_K[block] = K;
   c->block_mu[block] = mu;
   c->block_rho[block] = rho;
+  c->block_model[block] = PD_MATERIAL_LPS;
+  c->have_material = true;
+  c->wv_done = false;
+  coarse_release(c);
+  return PD_OK;
+}
+
+int pd_material_bond_based(pd_ctx* c, int32_t block, double K, double rho, int32_t plane, double height) {
+  CHECK_CTX(c);
+  if (block < 0 || block >= (int32_t)c->block_K.size()) return fail(c, PD_ERR_ARG, "pd_material_bond_based: bad block");
+  if (!(K > 0.0) || !(rho > 0.0)) return fail(c, PD_ERR_ARG, "pd_material_bond_based: modulus and density must be positive");
+  if (plane != 0 && !(height > 0.0))
+    return fail(c, PD_ERR_ARG, "pd_material_bond_based: in case of plane strain or plane stress the height must be given");
+  c->block_K[block] = K;
+  c->block_mu[block] = 0.0;
+  c->block_rho[block] = rho;
+  c->block_model[block] = PD_MATERIAL_BOND_BASED;
+  c->bb_plane = plane != 0;
+  c->bb_height = plane != 0 ? height : 0.0;
   c->have_material = true;
   c->wv_done = false;
   coarse_release(c);

@@ -569,6 +569,168 @@ __global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t*
 }
 
 // ---------------------------------------------------------------------------
+// Elastic bond-based material (MATERIAL_EVALUATION::computeInternalForceElasticBondBased,
+// src/materials/elastic_bond_based.cxx:55-124): one bond pass per evaluation,
+// the bond's critical-stretch damage first (CriticalStretchDamageModel order),
+// then the pair force of the intact bond
+//   t_ij = 0.5 (1 - d) s c_i,  s = (|Y| - |X|)/|X|,
+//   c = 18K/(pi delta^4) (3D, :77) or 12K/(pi H delta^3) (plane strain/stress, :75),
+//   f_i += (t_ij + t_ji) V_j Y/|Y|   (gather form of the scatter at :118-123),
+// then the Verlet epilogue. No dilatation, no influence function.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double bb_constant(double K, double h, int plane, double height) {
+  const double pi = 3.14159265358979323846;
+  return plane ? __ddiv_rn(__dmul_rn(12.0, K), __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(pi, height), h), h), h))
+               : __ddiv_rn(__dmul_rn(18.0, K), __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(pi, h), h), h), h));
+}
+
+// Split path: 0.5 c_i of every point in record slot 6 of both state buffers
+// (the Verlet epilogue writes only slots 0-5).
+__global__ void k_bb_terms(int64_t n, const double4* __restrict__ pt, const double* __restrict__ hp, int plane,
+                           double height, Rec8* __restrict__ ur0, Rec8* __restrict__ ur1) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float c = (float)(0.5 * bb_constant(pt[i].y, hp[i], plane, height));
+  ur0[i].v[6] = c;
+  ur0[i].v[7] = 0.0f;
+  ur1[i].v[6] = c;
+  ur1[i].v[7] = 0.0f;
+}
+
+// FP64 path, each term in the reference's operation order.
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __restrict__ row,
+                                                    const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+                                                    const double4* __restrict__ xv, const double4* __restrict__ st,
+                                                    const double4* __restrict__ pt, const double* __restrict__ sc,
+                                                    const double* __restrict__ hp, int damage_on, int plane,
+                                                    double height, double* __restrict__ node_damage, EpiArgs E) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  int broken = 0;
+  int64_t nbond = 0;
+  if (valid) {
+    const double4 xi = xv[i], yi = st[i];
+    const double ci = bb_constant(pt[i].y, hp[i], plane, height);
+    const double s_c = damage_on ? sc[i] : -1.0;
+    nbond = row[i + 1] - row[i];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
+      if (dmg[b]) {
+        broken++;
+        continue;
+      }
+      const int32_t j = col[b];
+      const double4 xj = xv[j], yj = st[j];
+      const double zeta = __dsqrt_rn(sq3_rn(__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z)));
+      const double Yx = __dsub_rn(yj.x, yi.x), Yy = __dsub_rn(yj.y, yi.y), Yz = __dsub_rn(yj.z, yi.z);
+      const double dY = __dsqrt_rn(sq3_rn(Yx, Yy, Yz));
+      const double stretch = __ddiv_rn(__dsub_rn(dY, zeta), zeta);
+      if (s_c >= 0.0 && stretch > s_c) {
+        dmg[b] = 1;
+        broken++;
+        continue;
+      }
+      const double cj = bb_constant(pt[j].y, hp[j], plane, height);
+      const double ti = __dmul_rn(__dmul_rn(0.5, stretch), ci);  // 0.5*(1-d)*stretch*constant, d = 0
+      const double tj = __dmul_rn(__dmul_rn(0.5, stretch), cj);
+      const double V = xj.w;
+      fx = __dadd_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yx), dY), V));
+      fy = __dadd_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yy), dY), V));
+      fz = __dadd_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yz), dY), V));
+      fx = __dsub_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yx), dY), V));
+      fy = __dsub_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yy), dY), V));
+      fz = __dsub_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yz), dY), V));
+    }
+  }
+  fx = group_sum<TPO>(fx);
+  fy = group_sum<TPO>(fy);
+  fz = group_sum<TPO>(fz);
+  broken = group_sum<TPO>(broken);
+  if (valid && lane == 0) node_damage[i] = nbond > 0 ? (double)broken / (double)nbond : 0.0;
+  if (valid && lane < 3) {
+    const double4 xi = xv[i];
+    const double f = lane == 0 ? fx : (lane == 1 ? fy : fz);
+    verlet_epilogue(E, i, lane, f, comp3(xi, lane), pt[i].w);
+  }
+}
+
+// Split-FP32 path: one staged pass (bond records, neighbor ids by cp.async as
+// in the LPS passes), damage and pair force per bond, FP64 epilogue.
+template <int TPO>
+__global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, const int64_t* __restrict__ row,
+                                                                   const int32_t* __restrict__ col,
+                                                                   uint8_t* __restrict__ dmg,
+                                                                   const float4* __restrict__ bx,
+                                                                   const Rec8* __restrict__ ur,
+                                                                   const float4* __restrict__ own, int damage_on,
+                                                                   const double4* __restrict__ pt,
+                                                                   double* __restrict__ node_damage, EpiArgs E) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  int broken = 0;
+  int64_t b0 = 0, b1 = 0;
+  if (valid) {
+    b0 = row[i];
+    b1 = row[i + 1];
+    const Rec8 ui = ld_rec_nc(ur + i);
+    const float s_c = damage_on ? own[i].w : -1.0f;
+    __shared__ float4 sq[2][kUnroll][kBlock];
+    __shared__ int32_t sj[2][kUnroll][kBlock];
+    constexpr int kStep = kUnroll * TPO;
+    const float4* nbx = bx + b0 + lane;
+    const int32_t* ncol = col + b0 + lane;
+    uint8_t* pdm = dmg + b0 + lane;
+    int rem = (int)(b1 - b0) - lane;
+    int st = 0;
+    stage_batch<TPO>(sq, sj, 0, rem, nbx, ncol, (int32_t)i);
+#pragma unroll 1
+    for (; rem > 0; rem -= kStep, pdm += kStep) {
+      nbx += kStep;
+      ncol += kStep;
+      stage_batch<TPO>(sq, sj, st ^ 1, rem - kStep, nbx, ncol, (int32_t)i);
+      cp_wait<1>();
+      int dd[kUnroll];
+      Rec8 uu[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) dd[k] = (TPO * k < rem) ? (int)pdm[TPO * k] : 2;  // 2: past the row end
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + sj[st][k][threadIdx.x]);
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        const float4 q = sq[st][k][threadIdx.x];
+        const SplitBond sb = split_bond(q, ui, uu[k]);
+        const bool intact = dd[k] == 0;
+        const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
+        if (brk) pdm[TPO * k] = 1;
+        broken += (dd[k] == 1 || brk) ? 1 : 0;
+        const float t = (ui.v[6] + uu[k].v[6]) * __fdividef(sb.e, sb.zeta);  // t_ij + t_ji
+        const float w = (intact && !brk) ? t * q.w * sb.ry : 0.0f;
+        fx = fmaf(w, sb.Yx, fx);
+        fy = fmaf(w, sb.Yy, fy);
+        fz = fmaf(w, sb.Yz, fz);
+      }
+      st ^= 1;
+    }
+    cp_wait<0>();
+  }
+  fx = group_sum<TPO>(fx);
+  fy = group_sum<TPO>(fy);
+  fz = group_sum<TPO>(fz);
+  broken = group_sum<TPO>(broken);
+  if (valid && lane == 0) node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
+  if (valid && lane < 3) {
+    const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
+    verlet_epilogue(E, i, lane, f, 0.0, pt[i].w);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // State conversions and the stable time step
 // ---------------------------------------------------------------------------
 // State from current coordinates y [3n]: u = y - x (FP64), then the gathered
@@ -685,9 +847,14 @@ cudaError_t launch_weighted_volume(const pd_ctx* c) {
 
 cudaError_t launch_pack_owner(pd_ctx* c) {
   if (c->n == 0 || c->precision != PD_SPLIT_FP32) return cudaSuccess;
+  const bool bb = c->material_model == PD_MATERIAL_BOND_BASED;
   k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->sc.p, c->own.p);
+  // the bond-based material has no influence function: bx.w = V_j
   PD_DISPATCH_TPO(c->tpo, k_pack_bonds, grid_for(c->n, c->tpo), c->n, c->row.p, c->col.p, c->xv.p, c->hp.p,
-                  c->influence, c->bx.p);
+                  bb ? PD_INFLUENCE_ONE : c->influence, c->bx.p);
+  if (bb)
+    k_bb_terms<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->hp.p, c->bb_plane, c->bb_height, c->ur[0].p,
+                                                     c->ur[1].p);
   return cudaGetLastError();
 }
 
@@ -728,16 +895,6 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
     c->kev_used += 3;
     cudaEventRecord(ev[0], c->stream);
   }
-  if (split) {
-    PD_DISPATCH_TPO(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
-                    c->own.p, sp.damage_on, c->theta.p, c->node_damage.p);
-  } else {
-    PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
-                    c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
-  }
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  if (ev) cudaEventRecord(ev[1], c->stream);
   EpiArgs E;
   E.dt = sp.dt;
   E.t0 = sp.t0;
@@ -757,6 +914,28 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   E.st_next = split ? nullptr : c->st[c->cur ^ 1].p;
   E.ur_next = split ? c->ur[c->cur ^ 1].p : nullptr;
   E.status = c->status.p;
+  if (c->material_model == PD_MATERIAL_BOND_BASED) {  // one pass: damage + pair force + epilogue
+    if (ev) cudaEventRecord(ev[1], c->stream);
+    if (split) {
+      PD_DISPATCH_TPO(tpo, k_bb_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->own.p,
+                      sp.damage_on, c->pt.p, c->node_damage.p, E);
+    } else {
+      PD_DISPATCH_TPO(tpo, k_bb_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p, c->sc.p,
+                      c->hp.p, sp.damage_on, c->bb_plane, c->bb_height, c->node_damage.p, E);
+    }
+    if (ev) cudaEventRecord(ev[2], c->stream);
+    return cudaGetLastError();
+  }
+  if (split) {
+    PD_DISPATCH_TPO(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
+                    c->own.p, sp.damage_on, c->theta.p, c->node_damage.p);
+  } else {
+    PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
+                    c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (ev) cudaEventRecord(ev[1], c->stream);
   if (split) {
     PD_DISPATCH_TPO(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E);
   } else {

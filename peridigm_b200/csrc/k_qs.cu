@@ -720,6 +720,10 @@ __global__ void k_qs_fixed_rows(int64_t n, const double* __restrict__ w, const u
 
 static int qs_prepare_at(pd_ctx* c, const double* u_dev) {
   TRY_RC(ensure_ready_internal(c));
+  if (c->material_model != PD_MATERIAL_LPS) {
+    c->err = "the quasi-static solve supports the LPS material model only";
+    return PD_ERR_UNSUPPORTED;
+  }
   TRY_RC(qs_alloc(c));
   QsState* s = c->qs;
   const int64_t n = c->n;
@@ -808,6 +812,10 @@ int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev) {
 
 int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {
   TRY_RC(ensure_ready_internal(c));
+  if (c->material_model != PD_MATERIAL_LPS) {
+    c->err = "the quasi-static solve supports the LPS material model only";
+    return PD_ERR_UNSUPPORTED;
+  }
   TRY_RC(qs_alloc(c));
   QsState* s = c->qs;
   const int64_t n = c->n, m = 3 * n;

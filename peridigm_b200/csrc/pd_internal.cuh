@@ -119,6 +119,10 @@ struct pd_ctx {
   int32_t n_blocks = 1;
   std::vector<double> block_h, block_K, block_mu, block_rho, block_sc;
   bool have_material = false;
+  std::vector<int> block_model;  // PD_MATERIAL_* per block (-1: not set)
+  int material_model = PD_MATERIAL_LPS;
+  int bb_plane = 0;              // bond-based: plane strain/stress constant
+  double bb_height = 0.0;
   std::vector<double> field_K, field_mu, field_sc;  // per-point overrides (empty = none)
   pdb::DBuf<double4> xv;
   pdb::DBuf<double> hp;  // horizon per point

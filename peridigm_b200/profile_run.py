@@ -4,6 +4,7 @@ of launches.
 
     python -m peridigm_b200.profile_run [--precision split|fp64] [--nx 400 --ny 200 --nz 4] [--steps 3]
     python -m peridigm_b200.profile_run --workload large_plate --steps 20 --compare
+    python -m peridigm_b200.profile_run --material bond_based --steps 200 --compare
 
 --workload picks the notched plate (default, sized by --nx/--ny/--nz), the
 32M-point heterogeneous plate (large_plate, 400x400x200) or the plate with a
@@ -21,13 +22,16 @@ import numpy as np
 from . import Context, workloads
 
 
-def _run(w, precision, steps, tpo, blocks):
+def _run(w, precision, steps, tpo, blocks, material="lps"):
     with Context(precision=precision, threads_per_point=tpo) as ctx:
         (workloads.setup_context_blocks if blocks else workloads.setup_context)(ctx, w)
+        if material == "bond_based":  # same bulk modulus and density, elastic bond-based model
+            for b in range(int(np.max(w["block"])) + 1 if blocks else 1):
+                ctx.material_bond_based(float(np.median(w["K"])), w["rho"], block=b)
         dt = w.get("safety", 0.7) * ctx.critical_time_step()
         st = ctx.verlet_run(dt, steps)
         nb = ctx.num_bonds()
-        line = {"workload": w["name"], "precision": precision, "points": int(len(w["vol"])), "bonds": int(nb),
+        line = {"workload": w["name"], "material": material, "precision": precision, "points": int(len(w["vol"])), "bonds": int(nb),
                 "steps": steps, "device_ms": st["device_ms"], "ms_per_step": st["device_ms"] / max(steps, 1),
                 "bond_evals_per_s": nb * steps / (st["device_ms"] / 1e3) if st["device_ms"] > 0 else 0.0,
                 "broken_bonds": st["broken_bonds"]}
@@ -44,6 +48,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--tpo", type=int, default=0)
     ap.add_argument("--compare", action="store_true")
+    ap.add_argument("--material", default="lps", choices=["lps", "bond_based"])
     a = ap.parse_args()
     blocks = False
     if a.workload == "large_plate":
@@ -55,7 +60,7 @@ def main():
     precisions = ["split", "fp64"] if a.compare else [a.precision]
     res = {}
     for p in precisions:
-        line, u, d = _run(w, p, a.steps, a.tpo, blocks)
+        line, u, d = _run(w, p, a.steps, a.tpo, blocks, a.material)
         res[p] = (u, d)
         print(json.dumps(line), flush=True)
     if a.compare:

@@ -291,7 +291,52 @@ def compression_qs():
     np.savez_compressed(os.path.join(OUT, "compression_qs.npz"), **out)
 
 
+# ---------------------------------------------------------------------------
+# 7. ElasticBondBased verification tests (3D, plane strain, plane stress):
+#    Exodus hex mesh (points = element centroids, Volume from the gold file),
+#    every point prescribed u_y = 0.001*y*t/1e-8 (and u_x = 0, u_z = 0 in 3D),
+#    Block_Data sums of Force over block_1 (bottom) and block_3 (top).
+# ---------------------------------------------------------------------------
+def _bond_based_case(sub, stem, gold, plane, height):
+    d = os.path.join(REF, "test/verification/ElasticBondBased", sub)
+    nc = netcdf_file(os.path.join(d, gold), "r", mmap=False)
+    x = np.stack([nc.variables["coordx"][:], nc.variables["coordy"][:], nc.variables["coordz"][:]], 1).astype(np.float64)
+    nblk = nc.dimensions["num_el_blk"]
+    ev = _names(nc, "name_elem_var")
+    n = x.shape[0]
+    vol, nn, block = np.zeros(n), np.zeros(n, np.int64), np.full(n, -1, np.int32)
+    for b in range(nblk):
+        pts = np.array(nc.variables["connect%d" % (b + 1)][:, 0], np.int64) - 1  # element -> output point
+        vol[pts] = nc.variables["vals_elem_var%deb%d" % (ev.index("Volume") + 1, b + 1)][0]
+        nn[pts] = nc.variables["vals_elem_var%deb%d" % (ev.index("Number_Of_Neighbors") + 1, b + 1)][0]
+        block[pts] = b
+    assert (block >= 0).all()
+    nv = _names(nc, "name_nod_var")
+    gv = _names(nc, "name_glo_var")
+    out = dict(x=x, vol=vol, block=block, nneigh=nn,
+               time=np.array(nc.variables["time_whole"][:], np.float64),
+               # density, bulk modulus, horizon, dt, final time, plane, height
+               params=np.array([7800.0, 200.0e9, 0.751, 2.0e-9, 1.0e-8, float(plane), height]))
+    for nm in ["DisplacementX", "DisplacementY", "DisplacementZ", "VelocityX", "VelocityY", "VelocityZ",
+               "ForceX", "ForceY", "ForceZ"]:
+        out[nm] = np.array(nc.variables["vals_nod_var%d" % (nv.index(nm) + 1)][:], np.float64)
+    glo = np.array(nc.variables["vals_glo_var"][:], np.float64)
+    for k, nm in enumerate(gv):
+        out[nm] = glo[:, k]
+    nc.close()
+    np.savez_compressed(os.path.join(OUT, stem + ".npz"), **out)
+
+
+def elastic_bond_based():
+    _bond_based_case("ElasticBondBased3D", "bond_based_3d", "ElasticBondBased3D_gold.e", False, 0.0)
+    _bond_based_case("ElasticBondBased2DPlaneStrain", "bond_based_plane_strain",
+                     "ElasticBondBased2DPlaneStrain_gold.e", True, 0.25)
+    _bond_based_case("ElasticBondBased2DPlaneStress", "bond_based_plane_stress",
+                     "ElasticBondBased2DPlaneStress_gold.e", True, 0.25)
+
+
 def main():
+    elastic_bond_based()
     unit_elastic()
     finite_plane()
     compression_qs()
