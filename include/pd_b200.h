@@ -67,6 +67,8 @@ extern "C" {
 #define PD_FIELD_BOND_DAMAGE 8      /* "Bond_Damage"        [nb] double, neighbor-list order */
 #define PD_FIELD_COORDINATES 9      /* "Coordinates" x+u    [3n] double */
 #define PD_FIELD_NUM_NEIGHBORS 10   /* "Number_Of_Neighbors" [n] double */
+#define PD_FIELD_FORCE 11           /* "Force" = Force_Density x Volume (Compute_Force) [3n] double */
+#define PD_FIELD_VOLUME 12          /* "Volume"             [n] double */
 
 typedef struct pd_ctx pd_ctx;
 
@@ -248,6 +250,23 @@ int pd_pack_state_device(pd_ctx* ctx, int64_t n_idx, const int32_t* idx, double*
 int pd_unpack_state_device(pd_ctx* ctx, int64_t n_idx, const int32_t* idx, const double* in);
 /* Reads a field (PD_FIELD_*) into host memory in the caller's order. */
 int pd_get_field(pd_ctx* ctx, int32_t field, double* out);
+
+/* ---- compute classes ------------------------------------------------------ */
+/* Block_Data (src/compute/Peridigm_Compute_Block_Data.cpp:121-210): the
+ * minimum, maximum or sum (PD_CALC_*) of a per-point field (PD_FIELD_*,
+ * scalar or vector) over the points of one block, into out[3] (scalars in
+ * out[0]). As in the reference the maximum starts from DBL_MIN. Sums run in
+ * a fixed order (bit-reproducible). */
+#define PD_CALC_MINIMUM 0
+#define PD_CALC_MAXIMUM 1
+#define PD_CALC_SUM 2
+int pd_block_data(pd_ctx* ctx, int32_t field, int32_t block, int32_t calculation, double* out);
+/* Kinetic_Energy (src/compute/Peridigm_Compute_Kinetic_Energy.cpp:79-150):
+ * global sum of 0.5 V rho |v|^2; per_point[n] (may be NULL) the local values. */
+int pd_kinetic_energy(pd_ctx* ctx, double* global, double* per_point);
+/* Linear_Momentum (src/compute/Peridigm_Compute_Linear_Momentum.cpp:110-150):
+ * global sum of rho V v into global[3]; per_point[3n] (may be NULL). */
+int pd_linear_momentum(pd_ctx* ctx, double* global, double* per_point);
 
 /* ---- quasi-static ---------------------------------------------------------- */
 #define PD_PRECOND_NONE 0         /* plain CG (the reference's default, usePreconditioner=false, Peridigm.cpp:2740) */

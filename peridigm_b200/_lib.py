@@ -37,6 +37,8 @@ FIELDS = {
     "Bond_Damage": 8,
     "Coordinates": 9,
     "Number_Of_Neighbors": 10,
+    "Force": 11,
+    "Volume": 12,
 }
 
 _dp = C.POINTER(C.c_double)
@@ -123,6 +125,9 @@ SIGNATURES = {
     "pd_mpnn_set_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "pd_mpnn_loss_grad": (C.c_int, [_vp, C.POINTER(C.c_float), _dp, C.POINTER(C.c_float)]),
     "pd_mpnn_coarse": (C.c_int, [_vp, C.c_double]),
+    "pd_block_data": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
+    "pd_kinetic_energy": (C.c_int, [_vp, _dp, _dp]),
+    "pd_linear_momentum": (C.c_int, [_vp, _dp, _dp]),
     "pd_qs_coarse_operator": (C.c_int, [_vp, _dp, C.c_double, _i64p, _i32p, _dp, _dp]),
     "pd_set_kernel_timing": (C.c_int, [_vp, C.c_int]),
     "pd_get_kernel_timing": (C.c_int, [_vp, _dp, _i64p]),

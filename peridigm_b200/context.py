@@ -330,6 +330,26 @@ class Context:
                                           g.ctypes.data_as(C.POINTER(C.c_float))))
         return loss.value, g
 
+    # -- compute classes --------------------------------------------------------
+    def block_data(self, field, block, calculation="Sum"):
+        """Block_Data compute class: "Minimum", "Maximum" or "Sum" of a field over a block (3 values)."""
+        calc = {"Minimum": 0, "Maximum": 1, "Sum": 2}[calculation]
+        out = np.zeros(3)
+        self._ok(self.L.pd_block_data(self.h, _lib.FIELDS[field], int(block), calc, _d(out)))
+        return out
+
+    def kinetic_energy(self, per_point=False):
+        g = np.zeros(1)
+        pp = np.zeros(self.n) if per_point else None
+        self._ok(self.L.pd_kinetic_energy(self.h, _d(g), _d(pp) if per_point else None))
+        return (g[0], pp) if per_point else g[0]
+
+    def linear_momentum(self, per_point=False):
+        g = np.zeros(3)
+        pp = np.zeros(3 * self.n) if per_point else None
+        self._ok(self.L.pd_linear_momentum(self.h, _d(g), _d(pp) if per_point else None))
+        return (g, pp) if per_point else g
+
     def kernel_timing(self, enable=True):
         self._ok(self.L.pd_set_kernel_timing(self.h, 1 if enable else 0))
 
@@ -341,7 +361,7 @@ class Context:
 
     def field(self, name):
         fid = _lib.FIELDS[name]
-        size = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 9: 3}.get(fid, 1) * self.n
+        size = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 9: 3, 11: 3}.get(fid, 1) * self.n
         if fid == _lib.FIELDS["Bond_Damage"]:
             size = self.num_bonds()
         out = np.zeros(size)

@@ -241,6 +241,7 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   if (n <= 0 || n >= (int64_t(1) << 31) || !x || !vol) return fail(c, PD_ERR_ARG, "pd_set_points: bad arguments");
   TRY(ensure_device(c));
   coarse_release(c);
+  c->blk_dev.release();
   c->n = n;
   c->hx.assign(x, x + 3 * n);
   c->hvol.assign(vol, vol + n);
@@ -928,6 +929,14 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
       for (int64_t b = 0; b < c->nb; ++b) out[b] = (double)h[b];
       return PD_OK;
     }
+    case PD_FIELD_FORCE: {
+      PD_CUDA_TRY(c, d2h(c, out, c->f.p, b3));
+      for (int64_t k = 0; k < 3 * n; ++k) out[k] *= c->hvol[k / 3];
+      return PD_OK;
+    }
+    case PD_FIELD_VOLUME:
+      for (int64_t i = 0; i < n; ++i) out[i] = c->hvol[i];
+      return PD_OK;
     case PD_FIELD_NUM_NEIGHBORS: {
       std::vector<int64_t> row(n + 1);
       PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (n + 1) * sizeof(int64_t)));
@@ -936,6 +945,30 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
     }
     default: return fail(c, PD_ERR_ARG, "pd_get_field: unknown field");
   }
+}
+
+int pd_block_data(pd_ctx* c, int32_t field, int32_t block, int32_t calculation, double* out) {
+  CHECK_CTX(c);
+  if (!out) return fail(c, PD_ERR_ARG, "pd_block_data: null output");
+  TRY(ensure_ready(c));
+  TRY(compute_block_data(c, field, block, calculation, out));
+  return check_status(c);
+}
+
+int pd_kinetic_energy(pd_ctx* c, double* global, double* per_point) {
+  CHECK_CTX(c);
+  if (!global) return fail(c, PD_ERR_ARG, "pd_kinetic_energy: null output");
+  TRY(ensure_ready(c));
+  TRY(compute_energy_momentum(c, 0, global, per_point));
+  return check_status(c);
+}
+
+int pd_linear_momentum(pd_ctx* c, double* global, double* per_point) {
+  CHECK_CTX(c);
+  if (!global) return fail(c, PD_ERR_ARG, "pd_linear_momentum: null output");
+  TRY(ensure_ready(c));
+  TRY(compute_energy_momentum(c, 1, global, per_point));
+  return check_status(c);
 }
 
 }  // extern "C"

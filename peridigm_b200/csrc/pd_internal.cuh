@@ -116,6 +116,7 @@ struct pd_ctx {
   int64_t n = 0;
   std::vector<double> hx, hvol;
   std::vector<int32_t> hblock;
+  pdb::DBuf<int32_t> blk_dev;  // block id per point on the device (compute classes), built on demand
   int32_t n_blocks = 1;
   std::vector<double> block_h, block_K, block_mu, block_rho, block_sc;
   bool have_material = false;
@@ -236,6 +237,8 @@ int coarse_apply_add_f(pd_ctx* c, const float* r, double* z, const uint8_t* fixe
 int coarse_aggregates(pd_ctx* c, int32_t* agg_dev);
 int coarse_copy_inverse(pd_ctx* c, double* dst_dev);
 int64_t coarse_size(const pd_ctx* c);
+int compute_block_data(pd_ctx* c, int field, int block, int calc, double* out3);
+int compute_energy_momentum(pd_ctx* c, int what, double* global, double* per_point_host);
 void coarse_release(pd_ctx* c);
 void coarse_invalidate(pd_ctx* c);  // the model changed: rebuild the operator before its next use
 bool coarse_valid(const pd_ctx* c);

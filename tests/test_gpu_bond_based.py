@@ -6,7 +6,7 @@
 * the ElasticBondBased3D / 2DPlaneStrain / 2DPlaneStress gold files
   (tests/golden/): Number_Of_Neighbors exactly; Displacement and Velocity
   to 1e-9 and Force (force density x volume) and the Block_Data reaction
-  sums to 1e-3 absolute (the .comp tolerances) on the FP64 path; the
+  sums (pd_block_data) to 1e-3 absolute (the .comp tolerances) on the FP64 path; the
   split path within 1e-6 of each field's largest magnitude;
 * a notched plate with critical-stretch damage vs the oracle's explicit run:
   FP64 break set identical, displacement <= 1e-9 relative; two runs
@@ -102,7 +102,7 @@ def test_bond_based_gold(case, precision):
                     assert np.abs(F[c::3] - gf).max() <= 1e-6 * np.abs(z["ForceY"][k]).max()
             for nm, b in (("Bottom_Reaction_Force", 0), ("Top_Reaction_Force", 2)):
                 ref = np.array([z[nm + ax][k] for ax in "XYZ"])
-                got = np.array([F[c::3][z["block"] == b].sum() for c in range(3)])
+                got = ctx.block_data("Force", b, "Sum")  # the Block_Data compute class on the device
                 tol = 1e-3 if precision == "fp64" else 1e-6 * np.abs(ref).max()
                 assert np.abs(got - ref).max() < tol
 
