@@ -135,6 +135,8 @@ def ref_lib():
         L.pdref_dilatation.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_int, C.c_double]
         L.pdref_force_linear_elastic.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_int,
                                                  C.c_double, C.c_double, C.c_double]
+        L.pdref_hex_centroid_volume.argtypes = [_dp, _dp, _dp]
+        L.pdref_tet_centroid_volume.argtypes = [_dp, _dp, _dp]
         L.pdref_force_bond_based.argtypes = [_dp, _dp, _dp, _dp, _dp, _i32p, C.c_int, C.c_double, C.c_double,
                                              C.c_int, C.c_double]
         _ref = L
@@ -513,6 +515,19 @@ def ref_force_bond_based(x, y, vol, nl, n, K, horizon, bond_damage=None, plane=F
     L.pdref_force_bond_based(_d(x), _d(y), _d(vol), _d(dmg), _d(f), _i32(nl), n, float(K), float(horizon),
                              1 if plane else 0, float(height))
     return f
+
+
+def ref_element_point(nodes):
+    """(centroid, volume) of one hex (8x3) or tet (4x3) element by the
+    reference's compiled hexCentroidAndVolume / tetCentroidAndVolume."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libpdref.so is not built")
+    P = np.ascontiguousarray(nodes, np.float64).ravel()
+    c = np.zeros(3)
+    v = np.zeros(1)
+    (L.pdref_hex_centroid_volume if P.size == 24 else L.pdref_tet_centroid_volume)(_d(P), _d(c), _d(v))
+    return c, v[0]
 
 
 def ref_eval(x, y, vol, nl, n, K, mu, horizon, bond_damage=None):

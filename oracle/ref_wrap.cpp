@@ -1,13 +1,15 @@
 // C entry points over the reference's own LPS and bond-based kernels, compiled
 // from the reference sources (src/materials/elastic.cxx,
 // src/materials/elastic_bond_based.cxx, src/materials/material_utilities.cxx,
-// src/core/Peridigm_InfluenceFunction.cpp) by oracle/Makefile into oracle/_ref/.
+// src/core/Peridigm_InfluenceFunction.cpp, src/io/discretization/Peridigm_GeometryUtils.cpp)
+// by oracle/Makefile into oracle/_ref/.
 // Test infrastructure only: the product never links this library.
 #include <stdexcept>
 #include <string>
 #include "material_utilities.h"
 #include "elastic.h"
 #include "elastic_bond_based.h"
+#include "Peridigm_GeometryUtils.hpp"
 
 extern "C" {
 
@@ -55,6 +57,16 @@ void pdref_force_bond_based(const double* x, const double* y, const double* vol,
                             double height) {
   MATERIAL_EVALUATION::computeInternalForceElasticBondBased<double>(x, y, vol, bond_damage, f, nl, n_owned, K,
                                                                     horizon, plane != 0, height);
+}
+
+// PeridigmNS::hexCentroidAndVolume / tetCentroidAndVolume
+// (src/io/discretization/Peridigm_GeometryUtils.cpp:52-339): the point an
+// Exodus element becomes (nodes: 8 or 4 xyz triples).
+void pdref_hex_centroid_volume(double* nodes, double* centroid, double* volume) {
+  PeridigmNS::hexCentroidAndVolume(nodes, centroid, volume);
+}
+void pdref_tet_centroid_volume(double* nodes, double* centroid, double* volume) {
+  PeridigmNS::tetCentroidAndVolume(nodes, centroid, volume);
 }
 
 }  // extern "C"

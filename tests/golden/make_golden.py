@@ -297,8 +297,17 @@ def compression_qs():
 #    every point prescribed u_y = 0.001*y*t/1e-8 (and u_x = 0, u_z = 0 in 3D),
 #    Block_Data sums of Force over block_1 (bottom) and block_3 (top).
 # ---------------------------------------------------------------------------
-def _bond_based_case(sub, stem, gold, plane, height):
+def _bond_based_case(sub, stem, gold, plane, height, mesh):
     d = os.path.join(REF, "test/verification/ElasticBondBased", sub)
+    # the genesis mesh itself, for the discretization reader's tests
+    g = netcdf_file(os.path.join(d, mesh), "r", mmap=False)
+    mesh_out = dict(mesh_X=np.stack([g.variables["coord" + a][:] for a in "xyz"], 1).astype(np.float64),
+                    mesh_blk_ids=np.array(g.variables["eb_prop1"][:], np.int64),
+                    mesh_elem_map=np.array(g.variables["elem_num_map"][:], np.int64),
+                    mesh_ns=np.array(g.variables["node_ns1"][:], np.int64))
+    for b in range(g.dimensions["num_el_blk"]):
+        mesh_out["mesh_conn%d" % (b + 1)] = np.array(g.variables["connect%d" % (b + 1)][:], np.int64)
+    g.close()
     nc = netcdf_file(os.path.join(d, gold), "r", mmap=False)
     x = np.stack([nc.variables["coordx"][:], nc.variables["coordy"][:], nc.variables["coordz"][:]], 1).astype(np.float64)
     nblk = nc.dimensions["num_el_blk"]
@@ -324,15 +333,17 @@ def _bond_based_case(sub, stem, gold, plane, height):
     for k, nm in enumerate(gv):
         out[nm] = glo[:, k]
     nc.close()
+    out.update(mesh_out)
     np.savez_compressed(os.path.join(OUT, stem + ".npz"), **out)
 
 
 def elastic_bond_based():
-    _bond_based_case("ElasticBondBased3D", "bond_based_3d", "ElasticBondBased3D_gold.e", False, 0.0)
+    _bond_based_case("ElasticBondBased3D", "bond_based_3d", "ElasticBondBased3D_gold.e", False, 0.0,
+                     "ElasticBondBased3D.g")
     _bond_based_case("ElasticBondBased2DPlaneStrain", "bond_based_plane_strain",
-                     "ElasticBondBased2DPlaneStrain_gold.e", True, 0.25)
+                     "ElasticBondBased2DPlaneStrain_gold.e", True, 0.25, "ElasticBondBased2D.g")
     _bond_based_case("ElasticBondBased2DPlaneStress", "bond_based_plane_stress",
-                     "ElasticBondBased2DPlaneStress_gold.e", True, 0.25)
+                     "ElasticBondBased2DPlaneStress_gold.e", True, 0.25, "ElasticBondBased2D.g")
 
 
 def main():
