@@ -329,6 +329,7 @@ def _bond_based_case(sub, stem, gold, plane, height, mesh):
     for nm in ["DisplacementX", "DisplacementY", "DisplacementZ", "VelocityX", "VelocityY", "VelocityZ",
                "ForceX", "ForceY", "ForceZ"]:
         out[nm] = np.array(nc.variables["vals_nod_var%d" % (nv.index(nm) + 1)][:], np.float64)
+    out.update(gold_nod_vars=np.array(nv), gold_elem_vars=np.array(ev), gold_glo_vars=np.array(gv))
     glo = np.array(nc.variables["vals_glo_var"][:], np.float64)
     for k, nm in enumerate(gv):
         out[nm] = glo[:, k]

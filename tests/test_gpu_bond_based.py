@@ -158,3 +158,45 @@ def test_quasi_static_rejects_bond_based():
     with ctx:
         with pytest.raises(Exception, match="LPS"):
             ctx.qs_load_step(0.0, 1.0, newton_tolerance=-1e-8)
+
+
+def test_bond_based_output_file(tmp_path):
+    """The 3D case written by peridigm_b200.output as the reference's deck asks
+    (Volume, Displacement, Velocity, Force, Number_Of_Neighbors, the two
+    Block_Data reaction forces, every step): the same variable names as the
+    gold file and its values within the .comp tolerances."""
+    from scipy.io import netcdf_file
+
+    from peridigm_b200 import output
+
+    z = np.load(os.path.join(G, "bond_based_3d.npz"))
+    path = str(tmp_path / "ElasticBondBased3D.e")
+    sums = {"Top_Reaction_Force": ("Force", 2, "Sum"), "Bottom_Reaction_Force": ("Force", 0, "Sum")}
+    with Context(precision="fp64") as ctx:
+        dt = _gold_ctx(ctx, z)
+        with output.ExodusWriter(path, z["x"].ravel(), z["block"], vector_fields=["Displacement", "Velocity", "Force"],
+                                 scalar_fields=["Volume", "Number_Of_Neighbors"], global_fields=list(sums)) as w:
+            output.write_context_step(w, ctx, 0.0, sums)
+            for k in range(1, len(z["time"])):
+                ctx.verlet_run(dt, 1, t0=z["time"][k - 1])
+                output.write_context_step(w, ctx, z["time"][k], sums)
+    nc = netcdf_file(path, "r", mmap=False)
+    try:
+        names = lambda key: [b"".join(r).decode().strip("\x00 ") for r in nc.variables[key][:]]
+        assert names("name_nod_var") == list(z["gold_nod_vars"])
+        assert names("name_elem_var") == list(z["gold_elem_vars"])
+        assert names("name_glo_var") == list(z["gold_glo_vars"])
+        assert np.abs(nc.variables["time_whole"][:] - z["time"]).max() < 1e-14
+        nod = names("name_nod_var")
+        for j, nm in enumerate(nod):
+            tol = 1e-3 if nm.startswith("Force") else 1e-9
+            assert np.abs(nc.variables["vals_nod_var%d" % (j + 1)][:] - z[nm]).max() < tol
+        glo = nc.variables["vals_glo_var"][:]
+        for j, nm in enumerate(names("name_glo_var")):
+            assert np.abs(glo[:, j] - z[nm]).max() < 1e-3
+        for b in range(3):
+            sel = z["block"] == b
+            assert np.array_equal(nc.variables["vals_elem_var1eb%d" % (b + 1)][0], z["vol"][sel])
+            assert np.array_equal(nc.variables["vals_elem_var2eb%d" % (b + 1)][0], z["nneigh"][sel].astype(float))
+    finally:
+        nc.close()
