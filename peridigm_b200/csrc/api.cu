@@ -161,6 +161,7 @@ int check_status(pd_ctx* c) {
 // evalModel on the configuration already in st[cur]; trial damage on dmg_trial.
 int eval_trial(pd_ctx* c, double* f_dev) {
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+  c->dmg_gen++;
   StepParams sp{};
   sp.mode = EVAL_ONLY;
   sp.damage_on = c->any_damage ? 1 : 0;
@@ -484,6 +485,7 @@ int pd_update_state(pd_ctx* c) {
   TRY(ensure_device(c));
   if (c->trial_valid) {
     PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg.p, c->dmg_trial.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+    c->dmg_gen++;
     PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->trial_valid = false;
   }
@@ -501,6 +503,7 @@ int pd_set_bond_damage(pd_ctx* c, const double* bd) {
   }
   TRY(ensure_device(c));
   PD_CUDA_TRY(c, h2d(c, c->dmg.p, h.data(), (size_t)c->nb));
+  c->dmg_gen++;
   c->trial_valid = false;
   coarse_invalidate(c);
   return PD_OK;
@@ -576,6 +579,7 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
   sp.has_contact = contact ? 1 : 0;
   // initial evaluation (Peridigm.cpp:1393-1423): its damage is not committed
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+  c->dmg_gen++;
   if (contact) {
     TRY(contact_prepare(c, 0));
     TRY(contact_eval(c));
@@ -638,6 +642,7 @@ int pd_verlet_begin(pd_ctx* c, double dt, double t0) {
   PD_CUDA_TRY(c, cudaEventRecord(c->vbeg, c->stream));
   // initial evaluation (Peridigm.cpp:1393-1423): its damage is not committed
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
+  c->dmg_gen++;
   if (sp.has_contact) {
     TRY(contact_prepare(c, 0));
     TRY(contact_eval(c));

@@ -22,6 +22,8 @@
 // displacement u[3n] stays the integration state.
 #include <math.h>
 
+#include <cub/cub.cuh>
+
 #include "pd_internal.cuh"
 
 namespace pdb {
@@ -146,26 +148,45 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Stages one batch of a lane's row (the bonds at row offsets TPO*k from the
-// lane's cursor, k < kUnroll; `rem` bonds remain from the cursor) into slot
-// `st`: bond records and neighbor ids by cp.async where the bond exists, and
-// past the row end a dummy bond (X = (1,0,0), the owner as its own neighbor)
-// whose arithmetic stays finite and is masked by a select.
-template <int TPO>
+// Stages one batch of a lane's bonds (slots k < kUnroll, STRIDE records
+// apart; `left` slots remain for this lane) into slot `st`: bond records and
+// neighbor ids by cp.async where the bond exists, and past the end a dummy
+// bond (X = (1,0,0), the owner as its own neighbor) whose arithmetic stays
+// finite and is masked by a select.
+template <int STRIDE>
 __device__ __forceinline__ void stage_batch(float4 (*sq)[kUnroll][kBlock], int32_t (*sj)[kUnroll][kBlock], int st,
-                                            int rem, const float4* __restrict__ pbx,
+                                            int left, const float4* __restrict__ pbx,
                                             const int32_t* __restrict__ pcol, int32_t self) {
 #pragma unroll
   for (int k = 0; k < kUnroll; ++k) {
-    if (TPO * k < rem) {
-      cp_async16(&sq[st][k][threadIdx.x], pbx + TPO * k);
-      cp_async4(&sj[st][k][threadIdx.x], pcol + TPO * k);
+    if (k < left) {
+      cp_async16(&sq[st][k][threadIdx.x], pbx + STRIDE * k);
+      cp_async4(&sj[st][k][threadIdx.x], pcol + STRIDE * k);
     } else {
       sq[st][k][threadIdx.x] = make_float4(1.f, 0.f, 0.f, 0.f);
       sj[st][k][threadIdx.x] = self;
     }
   }
   cp_commit();
+}
+
+// Bond-stream cursor of a lane. CSR: the owner's row, the lane's bonds TPO
+// apart. Sliced (4 lanes per point, SELL): the bonds of the 8 owners of a
+// warp interleaved so that one warp load is 32 consecutive records
+// (record of owner o, row offset r at soff[s]*32 + (r/4)*32 + 4o + r%4), each
+// row padded with dummy bonds (damage byte 2) to the slice's longest row.
+template <int TPO, bool SELL>
+__device__ __forceinline__ void bond_cursor(int64_t i, int lane, int64_t b0, int64_t b1,
+                                            const int64_t* __restrict__ soff, int64_t* base, int* left) {
+  if (SELL) {
+    const int64_t s = i >> 3, so = soff[s];
+    *base = so * 32 + (i & 7) * 4 + lane;
+    *left = (int)(soff[s + 1] - so);
+  } else {
+    const int rem = (int)(b1 - b0) - lane;
+    *base = b0 + lane;
+    *left = rem > 0 ? (rem + TPO - 1) / TPO : 0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -206,26 +227,79 @@ __global__ void k_pack_owner(int64_t n, const double4* __restrict__ pt, const do
                        (float)sc[i]);
 }
 
-// Split-path bond stream bx[b] = (X = x_j - x_i, omega(|X|, h_i) * V_j): the
-// difference and the influence weight in FP64, each rounded once to FP32.
-template <int TPO>
+// Split-path bond stream bx = (X = x_j - x_i, omega(|X|, h_i) * V_j): the
+// difference and the influence weight in FP64, each rounded once to FP32. In
+// CSR order (SELL false), or in the sliced order of bond_cursor (SELL true,
+// with the neighbor ids and damage bytes copied alongside).
+__device__ __forceinline__ int64_t sell_index(const int64_t* __restrict__ soff, int64_t i, int64_t r) {
+  return soff[i >> 3] * 32 + (r >> 2) * 32 + (i & 7) * 4 + (r & 3);
+}
+
+template <int TPO, bool SELL>
 __global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t* __restrict__ row,
                                                        const int32_t* __restrict__ col,
                                                        const double4* __restrict__ xv,
                                                        const double* __restrict__ hp, int influence,
-                                                       float4* __restrict__ bx) {
+                                                       float4* __restrict__ bx, const int64_t* __restrict__ soff,
+                                                       const uint8_t* __restrict__ dmg, int32_t* __restrict__ scol,
+                                                       uint8_t* __restrict__ sdmg) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
   if (i >= n) return;
   const double4 xi = xv[i];
   const double h = hp[i];
-  for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
-    const double4 xj = xv[col[b]];
+  const int64_t b0 = row[i];
+  for (int64_t b = b0 + lane; b < row[i + 1]; b += TPO) {
+    const int32_t j = col[b];
+    const double4 xj = xv[j];
     const double dx = __dsub_rn(xj.x, xi.x), dy = __dsub_rn(xj.y, xi.y), dz = __dsub_rn(xj.z, xi.z);
     const double om = omega_d(influence, __dsqrt_rn(sq3_rn(dx, dy, dz)), h);
-    bx[b] = make_float4((float)dx, (float)dy, (float)dz, (float)__dmul_rn(om, xj.w));
+    const float4 rec = make_float4((float)dx, (float)dy, (float)dz, (float)__dmul_rn(om, xj.w));
+    if (SELL) {
+      const int64_t k = sell_index(soff, i, b - b0);
+      bx[k] = rec;
+      scol[k] = j;
+      sdmg[k] = dmg[b];
+    } else {
+      bx[b] = rec;
+    }
   }
+  if (SELL) {  // padding to the slice's longest row: dummy bonds, damage byte 2
+    const int64_t len = row[i + 1] - b0, ms = soff[(i >> 3) + 1] - soff[i >> 3];
+    for (int64_t r = len + lane; r < 4 * ms; r += TPO) {
+      const int64_t k = sell_index(soff, i, r);
+      bx[k] = make_float4(1.f, 0.f, 0.f, 0.f);
+      scol[k] = (int32_t)i;
+      sdmg[k] = 2;
+    }
+  }
+}
+
+// Slots per slice (groups of 4 bonds of its longest row).
+__global__ void k_sell_count(int64_t n, const int64_t* __restrict__ row, int64_t* __restrict__ cnt) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ns = (n + 7) / 8;
+  if (s > ns) return;
+  int64_t m = 0;
+  if (s < ns)
+    for (int o = 0; o < 8; ++o) {
+      const int64_t i = 8 * s + o;
+      if (i < n) m = max(m, (row[i + 1] - row[i] + 3) / 4);
+    }
+  cnt[s] = m;
+}
+
+// The sliced damage mirror from the CSR damage (after writes outside the passes).
+__global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* __restrict__ row,
+                                                     const int64_t* __restrict__ soff,
+                                                     const uint8_t* __restrict__ dmg, uint8_t* __restrict__ sdmg) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / 4;
+  const int lane = threadIdx.x & 3;
+  if (i >= n) return;
+  const int64_t b0 = row[i];
+  for (int64_t b = b0 + lane; b < row[i + 1]; b += 4) sdmg[sell_index(soff, i, b - b0)] = dmg[b];
 }
 
 // ---------------------------------------------------------------------------
@@ -234,11 +308,12 @@ __global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t*
 //   theta_i = 3/m_i * sum omega*(1-d)*|X|*e*V_j  (material_utilities.cxx:284)
 // Writes the owner terms A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m into ur[i].
 // ---------------------------------------------------------------------------
-template <int TPO>
+template <int TPO, bool SELL>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const float4* __restrict__ bx, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
-    double* __restrict__ theta_out, double* __restrict__ node_damage) {
+    double* __restrict__ theta_out, double* __restrict__ node_damage, const int64_t* __restrict__ soff,
+    uint8_t* __restrict__ dmg_csr) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -253,27 +328,29 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     ow = own[i];
     const Rec8 ui = ld_rec(ur + i);
     const float s_c = damage_on ? ow.w : -1.0f;
-    // Row-local cursors; branch-free masking (selects) of past-the-end and
-    // broken bonds.
+    // Branch-free masking (selects) of past-the-end and broken bonds.
     __shared__ float4 sq[2][kUnroll][kBlock];
     __shared__ int32_t sj[2][kUnroll][kBlock];
-    constexpr int kStep = kUnroll * TPO;
-    const float4* nbx = bx + b0 + lane;
-    const int32_t* ncol = col + b0 + lane;
-    uint8_t* pdm = dmg + b0 + lane;
-    int rem = (int)(b1 - b0) - lane;
+    constexpr int kS = SELL ? 32 : TPO;
+    int64_t base;
+    int left;
+    bond_cursor<TPO, SELL>(i, lane, b0, b1, soff, &base, &left);
+    const float4* nbx = bx + base;
+    const int32_t* ncol = col + base;
+    uint8_t* pdm = dmg + base;
+    int mdone = 0;
     int st = 0;
-    stage_batch<TPO>(sq, sj, 0, rem, nbx, ncol, (int32_t)i);
+    stage_batch<kS>(sq, sj, 0, left, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (; rem > 0; rem -= kStep, pdm += kStep) {
-      nbx += kStep;
-      ncol += kStep;
-      stage_batch<TPO>(sq, sj, st ^ 1, rem - kStep, nbx, ncol, (int32_t)i);  // next batch (maybe all dummies)
-      cp_wait<1>();                                                         // this batch has landed
+    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, mdone += kUnroll) {
+      nbx += kUnroll * kS;
+      ncol += kUnroll * kS;
+      stage_batch<kS>(sq, sj, st ^ 1, left - kUnroll, nbx, ncol, (int32_t)i);  // next batch (maybe all dummies)
+      cp_wait<1>();                                                           // this batch has landed
       int dd[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) dd[k] = (TPO * k < rem) ? (int)pdm[TPO * k] : 2;  // 2: past the row end
+      for (int k = 0; k < kUnroll; ++k) dd[k] = (k < left) ? (int)pdm[kS * k] : 2;  // 2: past the row end
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + sj[st][k][threadIdx.x]);
 #pragma unroll
@@ -282,7 +359,10 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
         const SplitBond sb = split_bond(q, ui, uu[k]);
         const bool intact = dd[k] == 0;
         const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
-        if (brk) pdm[TPO * k] = 1;
+        if (brk) {
+          pdm[kS * k] = 1;
+          if (SELL) dmg_csr[b0 + lane + TPO * (mdone + k)] = 1;  // the CSR copy stays canonical
+        }
         broken += (dd[k] == 1 || brk) ? 1 : 0;
         th = fmaf((intact && !brk) ? q.w * sb.zeta : 0.0f, sb.e, th);
       }
@@ -446,13 +526,14 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
 //   f_i += (t_ij + t_ji) * V_j * Y/|Y|
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
-template <int TPO>
+template <int TPO, bool SELL>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
                                                                       const int32_t* __restrict__ col,
                                                                       const uint8_t* __restrict__ dmg,
                                                                       const float4* __restrict__ bx,
                                                                       const Rec8* __restrict__ ur,
-                                                                      const double4* __restrict__ pt, EpiArgs E) {
+                                                                      const double4* __restrict__ pt, EpiArgs E,
+                                                                      const int64_t* __restrict__ soff) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -463,24 +544,26 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
     const int64_t b1 = row[i + 1];
     __shared__ float4 sq[2][kUnroll][kBlock];
     __shared__ int32_t sj[2][kUnroll][kBlock];
-    constexpr int kStep = kUnroll * TPO;
+    constexpr int kS = SELL ? 32 : TPO;
     const int64_t b0 = row[i];
-    const float4* nbx = bx + b0 + lane;
-    const int32_t* ncol = col + b0 + lane;
-    const uint8_t* pdm = dmg + b0 + lane;
-    int rem = (int)(b1 - b0) - lane;
+    int64_t base;
+    int left;
+    bond_cursor<TPO, SELL>(i, lane, b0, b1, soff, &base, &left);
+    const float4* nbx = bx + base;
+    const int32_t* ncol = col + base;
+    const uint8_t* pdm = dmg + base;
     int st = 0;
-    stage_batch<TPO>(sq, sj, 0, rem, nbx, ncol, (int32_t)i);
+    stage_batch<kS>(sq, sj, 0, left, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (; rem > 0; rem -= kStep, pdm += kStep) {
-      nbx += kStep;
-      ncol += kStep;
-      stage_batch<TPO>(sq, sj, st ^ 1, rem - kStep, nbx, ncol, (int32_t)i);
+    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS) {
+      nbx += kUnroll * kS;
+      ncol += kUnroll * kS;
+      stage_batch<kS>(sq, sj, st ^ 1, left - kUnroll, nbx, ncol, (int32_t)i);
       cp_wait<1>();
       bool live[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) live[k] = (TPO * k < rem) ? pdm[TPO * k] == 0 : false;
+      for (int k = 0; k < kUnroll; ++k) live[k] = (k < left) ? pdm[kS * k] == 0 : false;
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + sj[st][k][threadIdx.x]);
 #pragma unroll
@@ -659,7 +742,7 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
 
 // Split-FP32 path: one staged pass (bond records, neighbor ids by cp.async as
 // in the LPS passes), damage and pair force per bond, FP64 epilogue.
-template <int TPO>
+template <int TPO, bool SELL>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, const int64_t* __restrict__ row,
                                                                    const int32_t* __restrict__ col,
                                                                    uint8_t* __restrict__ dmg,
@@ -667,7 +750,9 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
                                                                    const Rec8* __restrict__ ur,
                                                                    const float4* __restrict__ own, int damage_on,
                                                                    const double4* __restrict__ pt,
-                                                                   double* __restrict__ node_damage, EpiArgs E) {
+                                                                   double* __restrict__ node_damage, EpiArgs E,
+                                                                   const int64_t* __restrict__ soff,
+                                                                   uint8_t* __restrict__ dmg_csr) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -682,23 +767,26 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
     const float s_c = damage_on ? own[i].w : -1.0f;
     __shared__ float4 sq[2][kUnroll][kBlock];
     __shared__ int32_t sj[2][kUnroll][kBlock];
-    constexpr int kStep = kUnroll * TPO;
-    const float4* nbx = bx + b0 + lane;
-    const int32_t* ncol = col + b0 + lane;
-    uint8_t* pdm = dmg + b0 + lane;
-    int rem = (int)(b1 - b0) - lane;
+    constexpr int kS = SELL ? 32 : TPO;
+    int64_t base;
+    int left;
+    bond_cursor<TPO, SELL>(i, lane, b0, b1, soff, &base, &left);
+    const float4* nbx = bx + base;
+    const int32_t* ncol = col + base;
+    uint8_t* pdm = dmg + base;
+    int mdone = 0;
     int st = 0;
-    stage_batch<TPO>(sq, sj, 0, rem, nbx, ncol, (int32_t)i);
+    stage_batch<kS>(sq, sj, 0, left, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (; rem > 0; rem -= kStep, pdm += kStep) {
-      nbx += kStep;
-      ncol += kStep;
-      stage_batch<TPO>(sq, sj, st ^ 1, rem - kStep, nbx, ncol, (int32_t)i);
+    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, mdone += kUnroll) {
+      nbx += kUnroll * kS;
+      ncol += kUnroll * kS;
+      stage_batch<kS>(sq, sj, st ^ 1, left - kUnroll, nbx, ncol, (int32_t)i);
       cp_wait<1>();
       int dd[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) dd[k] = (TPO * k < rem) ? (int)pdm[TPO * k] : 2;  // 2: past the row end
+      for (int k = 0; k < kUnroll; ++k) dd[k] = (k < left) ? (int)pdm[kS * k] : 2;  // 2: past the row end
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + sj[st][k][threadIdx.x]);
 #pragma unroll
@@ -707,7 +795,10 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
         const SplitBond sb = split_bond(q, ui, uu[k]);
         const bool intact = dd[k] == 0;
         const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
-        if (brk) pdm[TPO * k] = 1;
+        if (brk) {
+          pdm[kS * k] = 1;
+          if (SELL) dmg_csr[b0 + lane + TPO * (mdone + k)] = 1;
+        }
         broken += (dd[k] == 1 || brk) ? 1 : 0;
         const float t = (ui.v[6] + uu[k].v[6]) * __fdividef(sb.e, sb.zeta);  // t_ij + t_ji
         const float w = (intact && !brk) ? t * q.w * sb.ry : 0.0f;
@@ -830,6 +921,14 @@ __global__ void k_min_reduce(int64_t m, const double* __restrict__ partial, doub
 static inline unsigned grid_for(int64_t n, int tpo) { return (unsigned)((n * tpo + kBlock - 1) / kBlock); }
 static inline unsigned grid1(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
+#define PD_DISPATCH_TPO_CSR(tpo, KERNEL, GRID, ...)                                  \
+  switch (tpo) {                                                                     \
+    case 4: KERNEL<4, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;    \
+    case 8: KERNEL<8, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;    \
+    case 16: KERNEL<16, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;  \
+    default: KERNEL<32, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;  \
+  }
+
 #define PD_DISPATCH_TPO(tpo, KERNEL, GRID, ...)                                      \
   switch (tpo) {                                                                     \
     case 4: KERNEL<4><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;           \
@@ -848,13 +947,46 @@ cudaError_t launch_weighted_volume(const pd_ctx* c) {
 cudaError_t launch_pack_owner(pd_ctx* c) {
   if (c->n == 0 || c->precision != PD_SPLIT_FP32) return cudaSuccess;
   const bool bb = c->material_model == PD_MATERIAL_BOND_BASED;
-  k_pack_owner<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->sc.p, c->own.p);
+  const int64_t n = c->n;
+  k_pack_owner<<<grid1(n), kBlock, 0, c->stream>>>(n, c->pt.p, c->sc.p, c->own.p);
   // the bond-based material has no influence function: bx.w = V_j
-  PD_DISPATCH_TPO(c->tpo, k_pack_bonds, grid_for(c->n, c->tpo), c->n, c->row.p, c->col.p, c->xv.p, c->hp.p,
-                  bb ? PD_INFLUENCE_ONE : c->influence, c->bx.p);
+  const int infl = bb ? PD_INFLUENCE_ONE : c->influence;
+  c->sell = c->tpo_split == 4;
+  if (c->sell) {  // sliced bond stream of the 4-lanes-per-point passes
+    const int64_t ns = (n + 7) / 8;
+    pdb::DBuf<int64_t> cnt;
+    cudaError_t e;
+    if ((e = cnt.alloc(ns + 1)) != cudaSuccess) return e;
+    if ((e = c->sell_off.alloc(ns + 1)) != cudaSuccess) return e;
+    k_sell_count<<<(unsigned)((ns + 1 + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(n, c->row.p, cnt.p);
+    size_t tmp_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt.p, c->sell_off.p, (int)(ns + 1), c->stream);
+    pdb::DBuf<unsigned char> tmp;
+    if ((e = tmp.alloc(tmp_bytes)) != cudaSuccess) return e;
+    if ((e = cub::DeviceScan::ExclusiveSum(tmp.p, tmp_bytes, cnt.p, c->sell_off.p, (int)(ns + 1), c->stream)) !=
+        cudaSuccess)
+      return e;
+    int64_t slots = 0;
+    if ((e = cudaMemcpyAsync(&slots, c->sell_off.p + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream)) !=
+        cudaSuccess)
+      return e;
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
+    const size_t recs = (size_t)std::max<int64_t>(32 * slots, 1);
+    if ((e = c->bx.alloc(recs)) != cudaSuccess) return e;
+    if ((e = c->sell_col.alloc(recs)) != cudaSuccess) return e;
+    if ((e = c->sell_dmg.alloc(recs)) != cudaSuccess) return e;
+    k_pack_bonds<4, true><<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, c->hp.p, infl,
+                                                                    c->bx.p, c->sell_off.p, c->dmg.p, c->sell_col.p,
+                                                                    c->sell_dmg.p);
+    c->sell_src = c->dmg.p;
+    c->sell_gen = c->dmg_gen;
+  } else {
+    PD_DISPATCH_TPO_CSR(c->tpo, k_pack_bonds, grid_for(n, c->tpo), n, c->row.p, c->col.p, c->xv.p, c->hp.p, infl,
+                        c->bx.p, nullptr, nullptr, nullptr, nullptr);
+  }
   if (bb)
-    k_bb_terms<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, c->pt.p, c->hp.p, c->bb_plane, c->bb_height, c->ur[0].p,
-                                                     c->ur[1].p);
+    k_bb_terms<<<grid1(n), kBlock, 0, c->stream>>>(n, c->pt.p, c->hp.p, c->bb_plane, c->bb_height, c->ur[0].p,
+                                                   c->ur[1].p);
   return cudaGetLastError();
 }
 
@@ -914,11 +1046,26 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   E.st_next = split ? nullptr : c->st[c->cur ^ 1].p;
   E.ur_next = split ? c->ur[c->cur ^ 1].p : nullptr;
   E.status = c->status.p;
+  // Split passes at 4 lanes per point read the sliced bond stream; its damage
+  // mirror follows the CSR damage array this evaluation uses.
+  const bool sell = split && c->sell && tpo == 4;
+  if (sell && (c->sell_src != dmg || c->sell_gen != c->dmg_gen)) {
+    k_sell_dmg<<<grid_for(c->n, 4), kBlock, 0, c->stream>>>(c->n, c->row.p, c->sell_off.p, dmg, c->sell_dmg.p);
+    c->sell_src = dmg;
+    c->sell_gen = c->dmg_gen;
+  }
+  const int32_t* scol = sell ? c->sell_col.p : c->col.p;
+  uint8_t* sdmg = sell ? c->sell_dmg.p : dmg;
+  const int64_t* soff = sell ? c->sell_off.p : nullptr;
   if (c->material_model == PD_MATERIAL_BOND_BASED) {  // one pass: damage + pair force + epilogue
     if (ev) cudaEventRecord(ev[1], c->stream);
-    if (split) {
-      PD_DISPATCH_TPO(tpo, k_bb_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->own.p,
-                      sp.damage_on, c->pt.p, c->node_damage.p, E);
+    if (sell) {
+      k_bb_split<4, true><<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p,
+                                                          c->own.p, sp.damage_on, c->pt.p, c->node_damage.p, E, soff,
+                                                          dmg);
+    } else if (split) {
+      PD_DISPATCH_TPO_CSR(tpo, k_bb_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->own.p,
+                          sp.damage_on, c->pt.p, c->node_damage.p, E, nullptr, nullptr);
     } else {
       PD_DISPATCH_TPO(tpo, k_bb_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p, c->sc.p,
                       c->hp.p, sp.damage_on, c->bb_plane, c->bb_height, c->node_damage.p, E);
@@ -926,9 +1073,13 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
     if (ev) cudaEventRecord(ev[2], c->stream);
     return cudaGetLastError();
   }
-  if (split) {
-    PD_DISPATCH_TPO(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
-                    c->own.p, sp.damage_on, c->theta.p, c->node_damage.p);
+  if (sell) {
+    k_dilatation_split<4, true><<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p,
+                                                                c->ur[c->cur].p, c->own.p, sp.damage_on, c->theta.p,
+                                                                c->node_damage.p, soff, dmg);
+  } else if (split) {
+    PD_DISPATCH_TPO_CSR(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
+                        c->own.p, sp.damage_on, c->theta.p, c->node_damage.p, nullptr, nullptr);
   } else {
     PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
                     c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
@@ -936,8 +1087,12 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], c->stream);
-  if (split) {
-    PD_DISPATCH_TPO(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E);
+  if (sell) {
+    k_force_split<4, true><<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p,
+                                                           c->pt.p, E, soff);
+  } else if (split) {
+    PD_DISPATCH_TPO_CSR(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
+                        nullptr);
   } else {
     PD_DISPATCH_TPO(tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
                     c->pt.p, c->hp.p, c->influence, E);

@@ -142,7 +142,17 @@ struct pd_ctx {
   bool wv_done = false;
   pdb::DBuf<double4> pt;     // (m, K, mu, rho)
   pdb::DBuf<double> sc;      // critical stretch (<0: off)
-  pdb::DBuf<float4> bx;      // split path: per bond (X, omega*V_j)
+  pdb::DBuf<float4> bx;      // split path: per bond (X, omega*V_j), CSR or sliced order
+  // Sliced (SELL) bond stream of the 4-lanes-per-point split passes: slot
+  // offsets per 8-owner slice, neighbor ids and a damage mirror in slice
+  // order (bx holds the records in that order). dmg_gen counts writes to the
+  // CSR damage outside the passes; the mirror is refreshed when it lags.
+  bool sell = false;
+  pdb::DBuf<int64_t> sell_off;
+  pdb::DBuf<int32_t> sell_col;
+  pdb::DBuf<uint8_t> sell_dmg;
+  const uint8_t* sell_src = nullptr;
+  int64_t dmg_gen = 0, sell_gen = -1;
   pdb::DBuf<float4> own;     // split path: (3/m, (3K-5mu)/m, 15mu/m, s_c)
   bool any_damage = false;
 
