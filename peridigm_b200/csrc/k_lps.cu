@@ -119,9 +119,12 @@ __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui,
 // wait on the damage byte, so each lane keeps 2*kUnroll loads in flight
 // instead of a damage -> id -> record chain per bond.
 // Batch depth and the launch bound were swept on the 320,000-point notched
-// plate (1, 2 or 4 bonds per batch; 2, 3 or 4 resident blocks per SM): with
-// the staged streams below, 4 bonds per batch and 4 blocks per SM (64
-// registers per thread, 40 KB of staging per block) are the fastest.
+// plate (1, 2 or 4 bonds per batch; 4 or 6 resident blocks per SM): with the
+// sliced stream loaded straight into registers, 4 bonds per batch and 4
+// blocks per SM (64 registers per thread, no shared memory) are the fastest.
+// (Staging the stream through shared memory by cp.async paid off only while
+// the stream was row-major; once each warp load is 32 consecutive records,
+// direct loads are faster: the force pass 139 -> 126 us on that plate.)
 #ifndef PD_BOND_UNROLL
 #define PD_BOND_UNROLL 4
 #endif
@@ -129,46 +132,6 @@ __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui,
 #define PD_BOND_MINB 4
 #endif
 constexpr int kUnroll = PD_BOND_UNROLL;
-
-// Bond streams staged through shared memory with cp.async: while a lane
-// gathers and computes batch t, its batch t+1 of bond records and neighbor ids
-// is already in flight into its own slots (two stages; each thread reads only
-// what it copied, so no block barrier is needed).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Stages one batch of a lane's bonds (slots k < kUnroll, STRIDE records
-// apart; `left` slots remain for this lane) into slot `st`: bond records and
-// neighbor ids by cp.async where the bond exists, and past the end a dummy
-// bond (X = (1,0,0), the owner as its own neighbor) whose arithmetic stays
-// finite and is masked by a select.
-template <int STRIDE>
-__device__ __forceinline__ void stage_batch(float4 (*sq)[kUnroll][kBlock], int32_t (*sj)[kUnroll][kBlock], int st,
-                                            int left, const float4* __restrict__ pbx,
-                                            const int32_t* __restrict__ pcol, int32_t self) {
-#pragma unroll
-  for (int k = 0; k < kUnroll; ++k) {
-    if (k < left) {
-      cp_async16(&sq[st][k][threadIdx.x], pbx + STRIDE * k);
-      cp_async4(&sj[st][k][threadIdx.x], pcol + STRIDE * k);
-    } else {
-      sq[st][k][threadIdx.x] = make_float4(1.f, 0.f, 0.f, 0.f);
-      sj[st][k][threadIdx.x] = self;
-    }
-  }
-  cp_commit();
-}
 
 // Bond-stream cursor of a lane. CSR: the owner's row, the lane's bonds TPO
 // apart. Sliced (4 lanes per point, SELL): the bonds of the 8 owners of a
@@ -328,9 +291,8 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     ow = own[i];
     const Rec8 ui = ld_rec(ur + i);
     const float s_c = damage_on ? ow.w : -1.0f;
-    // Branch-free masking (selects) of past-the-end and broken bonds.
-    __shared__ float4 sq[2][kUnroll][kBlock];
-    __shared__ int32_t sj[2][kUnroll][kBlock];
+    // Branch-free masking (selects) of past-the-end and broken bonds; the
+    // batch's bond-ordered loads first (independent), then its gathers.
     constexpr int kS = SELL ? 32 : TPO;
     int64_t base;
     int left;
@@ -339,23 +301,25 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     const int32_t* ncol = col + base;
     uint8_t* pdm = dmg + base;
     int mdone = 0;
-    int st = 0;
-    stage_batch<kS>(sq, sj, 0, left, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, mdone += kUnroll) {
-      nbx += kUnroll * kS;
-      ncol += kUnroll * kS;
-      stage_batch<kS>(sq, sj, st ^ 1, left - kUnroll, nbx, ncol, (int32_t)i);  // next batch (maybe all dummies)
-      cp_wait<1>();                                                           // this batch has landed
+    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS,
+                     mdone += kUnroll) {
       int dd[kUnroll];
+      float4 qq[kUnroll];
+      int32_t jj[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) dd[k] = (k < left) ? (int)pdm[kS * k] : 2;  // 2: past the row end
+      for (int k = 0; k < kUnroll; ++k) {
+        const bool in = k < left;
+        dd[k] = in ? (int)pdm[kS * k] : 2;  // 2: past the row end
+        jj[k] = in ? __ldcs(ncol + kS * k) : (int32_t)i;
+        qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
+      }
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + sj[st][k][threadIdx.x]);
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + jj[k]);
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
-        const float4 q = sq[st][k][threadIdx.x];
+        const float4 q = qq[k];
         const SplitBond sb = split_bond(q, ui, uu[k]);
         const bool intact = dd[k] == 0;
         const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
@@ -366,9 +330,7 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
         broken += (dd[k] == 1 || brk) ? 1 : 0;
         th = fmaf((intact && !brk) ? q.w * sb.zeta : 0.0f, sb.e, th);
       }
-      st ^= 1;
     }
-    cp_wait<0>();
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
@@ -542,8 +504,6 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
   if (valid) {
     const Rec8 ui = ld_rec_nc(ur + i);
     const int64_t b1 = row[i + 1];
-    __shared__ float4 sq[2][kUnroll][kBlock];
-    __shared__ int32_t sj[2][kUnroll][kBlock];
     constexpr int kS = SELL ? 32 : TPO;
     const int64_t b0 = row[i];
     int64_t base;
@@ -552,23 +512,24 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
     const float4* nbx = bx + base;
     const int32_t* ncol = col + base;
     const uint8_t* pdm = dmg + base;
-    int st = 0;
-    stage_batch<kS>(sq, sj, 0, left, nbx, ncol, (int32_t)i);
 #pragma unroll 1
-    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS) {
-      nbx += kUnroll * kS;
-      ncol += kUnroll * kS;
-      stage_batch<kS>(sq, sj, st ^ 1, left - kUnroll, nbx, ncol, (int32_t)i);
-      cp_wait<1>();
+    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS) {
       bool live[kUnroll];
+      float4 qq[kUnroll];
+      int32_t jj[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) live[k] = (k < left) ? pdm[kS * k] == 0 : false;
+      for (int k = 0; k < kUnroll; ++k) {
+        const bool in = k < left;
+        live[k] = in ? pdm[kS * k] == 0 : false;
+        jj[k] = in ? __ldcs(ncol + kS * k) : (int32_t)i;
+        qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
+      }
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + sj[st][k][threadIdx.x]);
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
-        const float4 q = sq[st][k][threadIdx.x];
+        const float4 q = qq[k];
         const SplitBond sb = split_bond(q, ui, uu[k]);
         const float T = fmaf(sb.zeta, ui.v[6] + uu[k].v[6], sb.e * (ui.v[7] + uu[k].v[7]));
         const float w = live[k] ? T * q.w * sb.ry : 0.0f;
@@ -576,9 +537,7 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
         fy = fmaf(w, sb.Yy, fy);
         fz = fmaf(w, sb.Yz, fz);
       }
-      st ^= 1;
     }
-    cp_wait<0>();
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
@@ -740,7 +699,7 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
   }
 }
 
-// Split-FP32 path: one staged pass (bond records, neighbor ids by cp.async as
+// Split-FP32 path: one pass (bond stream and neighbor ids loaded directly as
 // in the LPS passes), damage and pair force per bond, FP64 epilogue.
 template <int TPO, bool SELL>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, const int64_t* __restrict__ row,
@@ -759,45 +718,45 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
   const bool valid = i < n;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   int broken = 0;
-  int64_t b0 = 0, b1 = 0;
+  int len = 0;
   if (valid) {
-    b0 = row[i];
-    b1 = row[i + 1];
+    const int64_t b0 = row[i];
+    len = (int)(row[i + 1] - b0);
     const Rec8 ui = ld_rec_nc(ur + i);
     const float s_c = damage_on ? own[i].w : -1.0f;
-    __shared__ float4 sq[2][kUnroll][kBlock];
-    __shared__ int32_t sj[2][kUnroll][kBlock];
     constexpr int kS = SELL ? 32 : TPO;
     int64_t base;
     int left;
-    bond_cursor<TPO, SELL>(i, lane, b0, b1, soff, &base, &left);
+    bond_cursor<TPO, SELL>(i, lane, b0, b0 + len, soff, &base, &left);
     const float4* nbx = bx + base;
     const int32_t* ncol = col + base;
     uint8_t* pdm = dmg + base;
-    int mdone = 0;
-    int st = 0;
-    stage_batch<kS>(sq, sj, 0, left, nbx, ncol, (int32_t)i);
+    uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
 #pragma unroll 1
-    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, mdone += kUnroll) {
-      nbx += kUnroll * kS;
-      ncol += kUnroll * kS;
-      stage_batch<kS>(sq, sj, st ^ 1, left - kUnroll, nbx, ncol, (int32_t)i);
-      cp_wait<1>();
+    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS,
+                     cdm += SELL ? kUnroll * TPO : 0) {
       int dd[kUnroll];
+      float4 qq[kUnroll];
+      int32_t jj[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) dd[k] = (k < left) ? (int)pdm[kS * k] : 2;  // 2: past the row end
+      for (int k = 0; k < kUnroll; ++k) {
+        const bool in = k < left;
+        dd[k] = in ? (int)pdm[kS * k] : 2;  // 2: past the row end
+        jj[k] = in ? __ldcs(ncol + kS * k) : (int32_t)i;
+        qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
+      }
 #pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + sj[st][k][threadIdx.x]);
+      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
-        const float4 q = sq[st][k][threadIdx.x];
+        const float4 q = qq[k];
         const SplitBond sb = split_bond(q, ui, uu[k]);
         const bool intact = dd[k] == 0;
         const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
         if (brk) {
           pdm[kS * k] = 1;
-          if (SELL) dmg_csr[b0 + lane + TPO * (mdone + k)] = 1;
+          if (SELL) cdm[TPO * k] = 1;
         }
         broken += (dd[k] == 1 || brk) ? 1 : 0;
         const float t = (ui.v[6] + uu[k].v[6]) * __fdividef(sb.e, sb.zeta);  // t_ij + t_ji
@@ -806,15 +765,13 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
         fy = fmaf(w, sb.Yy, fy);
         fz = fmaf(w, sb.Yz, fz);
       }
-      st ^= 1;
     }
-    cp_wait<0>();
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
   fz = group_sum<TPO>(fz);
   broken = group_sum<TPO>(broken);
-  if (valid && lane == 0) node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
+  if (valid && lane == 0) node_damage[i] = len > 0 ? (double)broken / (double)len : 0.0;
   if (valid && lane < 3) {
     const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
     verlet_epilogue(E, i, lane, f, 0.0, pt[i].w);
