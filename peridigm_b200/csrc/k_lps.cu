@@ -125,6 +125,11 @@ __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui,
 // (Staging the stream through shared memory by cp.async paid off only while
 // the stream was row-major; once each warp load is 32 consecutive records,
 // direct loads are faster: the force pass 139 -> 126 us on that plate.)
+// The neighbor ids of the next batch are loaded one batch ahead, so a batch's
+// gathers never wait on its own id loads (dilatation 130 -> 114 us). Neither a
+// bulk L2 prefetch of the next 1 to 4 batches of the sliced streams (one lane
+// per warp, cp.async.bulk.prefetch) nor carrying the damage flag in the top
+// bit of the sliced ids instead of a damage byte made the passes faster.
 #ifndef PD_BOND_UNROLL
 #define PD_BOND_UNROLL 4
 #endif
@@ -283,36 +288,41 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
   const bool valid = i < n;
   float th = 0.0f;
   int broken = 0;
-  int64_t b0 = 0, b1 = 0;
-  float4 ow = make_float4(0.f, 0.f, 0.f, -1.f);
+  int len = 0;
   if (valid) {
-    b0 = row[i];
-    b1 = row[i + 1];
-    ow = own[i];
+    const int64_t b0 = row[i];
+    len = (int)(row[i + 1] - b0);
     const Rec8 ui = ld_rec(ur + i);
-    const float s_c = damage_on ? ow.w : -1.0f;
+    const float s_c = damage_on ? own[i].w : -1.0f;
     // Branch-free masking (selects) of past-the-end and broken bonds; the
     // batch's bond-ordered loads first (independent), then its gathers.
     constexpr int kS = SELL ? 32 : TPO;
     int64_t base;
     int left;
-    bond_cursor<TPO, SELL>(i, lane, b0, b1, soff, &base, &left);
+    bond_cursor<TPO, SELL>(i, lane, b0, b0 + len, soff, &base, &left);
     const float4* nbx = bx + base;
     const int32_t* ncol = col + base;
     uint8_t* pdm = dmg + base;
-    int mdone = 0;
+    uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
+    int32_t jn[kUnroll];  // neighbor ids of the next batch, loaded one batch ahead
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(ncol + kS * k) : (int32_t)i;
 #pragma unroll 1
     for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS,
-                     mdone += kUnroll) {
+                     cdm += SELL ? kUnroll * TPO : 0) {
       int dd[kUnroll];
       float4 qq[kUnroll];
       int32_t jj[kUnroll];
       Rec8 uu[kUnroll];
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
+        jj[k] = jn[k];
+        jn[k] = k + kUnroll < left ? __ldcs(ncol + kS * (k + kUnroll)) : (int32_t)i;
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
         const bool in = k < left;
         dd[k] = in ? (int)pdm[kS * k] : 2;  // 2: past the row end
-        jj[k] = in ? __ldcs(ncol + kS * k) : (int32_t)i;
         qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll
@@ -325,7 +335,7 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
         const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
         if (brk) {
           pdm[kS * k] = 1;
-          if (SELL) dmg_csr[b0 + lane + TPO * (mdone + k)] = 1;  // the CSR copy stays canonical
+          if (SELL) cdm[TPO * k] = 1;  // the CSR copy stays canonical
         }
         broken += (dd[k] == 1 || brk) ? 1 : 0;
         th = fmaf((intact && !brk) ? q.w * sb.zeta : 0.0f, sb.e, th);
@@ -335,10 +345,11 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
   if (valid && lane == 0) {
+    const float4 ow = own[i];
     const float theta = th * ow.x;
     *reinterpret_cast<float2*>(&ur[i].v[6]) = make_float2(theta * ow.y, ow.z);
     theta_out[i] = (double)theta;
-    node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
+    node_damage[i] = len > 0 ? (double)broken / (double)len : 0.0;
   }
 }
 
@@ -512,6 +523,9 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
     const float4* nbx = bx + base;
     const int32_t* ncol = col + base;
     const uint8_t* pdm = dmg + base;
+    int32_t jn[kUnroll];  // neighbor ids of the next batch, loaded one batch ahead
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(ncol + kS * k) : (int32_t)i;
 #pragma unroll 1
     for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS) {
       bool live[kUnroll];
@@ -520,9 +534,13 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
       Rec8 uu[kUnroll];
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
+        jj[k] = jn[k];
+        jn[k] = k + kUnroll < left ? __ldcs(ncol + kS * (k + kUnroll)) : (int32_t)i;
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
         const bool in = k < left;
         live[k] = in ? pdm[kS * k] == 0 : false;
-        jj[k] = in ? __ldcs(ncol + kS * k) : (int32_t)i;
         qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll
@@ -732,6 +750,9 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
     const int32_t* ncol = col + base;
     uint8_t* pdm = dmg + base;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
+    int32_t jn[kUnroll];  // neighbor ids of the next batch, loaded one batch ahead
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(ncol + kS * k) : (int32_t)i;
 #pragma unroll 1
     for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS,
                      cdm += SELL ? kUnroll * TPO : 0) {
@@ -741,9 +762,13 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, co
       Rec8 uu[kUnroll];
 #pragma unroll
       for (int k = 0; k < kUnroll; ++k) {
+        jj[k] = jn[k];
+        jn[k] = k + kUnroll < left ? __ldcs(ncol + kS * (k + kUnroll)) : (int32_t)i;
+      }
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
         const bool in = k < left;
         dd[k] = in ? (int)pdm[kS * k] : 2;  // 2: past the row end
-        jj[k] = in ? __ldcs(ncol + kS * k) : (int32_t)i;
         qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
       }
 #pragma unroll

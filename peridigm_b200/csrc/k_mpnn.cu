@@ -81,7 +81,19 @@ struct MpnnState {
   int every = 0;
   std::vector<DBuf<double>*> snap_r, snap_x;
   int nsnap = 0;
+  // Inference apply (13 small launches) as one CUDA graph, captured for one
+  // (r, z, fixed mask) triple; the buffers it reads are fixed once the
+  // patches are built, the weights and scales are read at replay.
+  cudaGraphExec_t apply_exec = nullptr;
+  const double* apply_r = nullptr;
+  double* apply_z = nullptr;
+  const uint8_t* apply_fixed = nullptr;
+  void drop_graph() {
+    if (apply_exec) cudaGraphExecDestroy(apply_exec);
+    apply_exec = nullptr;
+  }
   ~MpnnState() {
+    drop_graph();
     for (auto* p : snap_r) delete p;
     for (auto* p : snap_x) delete p;
   }
@@ -602,6 +614,7 @@ static int mp_patches(pd_ctx* c, MpnnState* s, double side) {
 int mpnn_init(pd_ctx* c, uint64_t seed, double patch) {
   if (!c->mpnn) c->mpnn = new MpnnState();
   MpnnState* s = mp_state(c);
+  s->drop_graph();  // the patch buffers are rebuilt
   TRY_RC(mp_patches(c, s, patch));
   // weights: W0 = 0.5 [I3; 0] and near-zero layers plus small uniform noise
   // from the seed, so G^T G starts near 0.25 I (a Jacobi-scaled middle level)
@@ -696,7 +709,17 @@ static int mp_backward(pd_ctx* c, MpnnState* s, int k, const float* U) {
   return PD_OK;
 }
 
-// z += Q S G^T G S Q^T r on the free dofs (inference).
+static int mp_apply_launches(pd_ctx* c, MpnnState* s, const double* r, double* z, const uint8_t* fixed) {
+  k_pt_restrict<double><<<gw(s->np), 256, 0, c->stream>>>(s->np, s->patch_cell.p, s->cstart.p, s->sorted.p, r, fixed,
+                                                          s->scale.p, 1.0, s->v[0].p);
+  TRY_RC(mp_forward(c, s, 0, false));
+  TRY_RC(mp_transpose(c, s, s->h[0][NL].p));
+  k_pt_prolong<<<g1(c->n), 256, 0, c->stream>>>(c->n, s->pid.p, s->out3.p, s->scale.p, 1.0, fixed, z);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+// z += Q S G^T G S Q^T r on the free dofs (inference), replayed as one graph.
 int mpnn_apply_add(pd_ctx* c, const double* r, double* z) {
   MpnnState* s = mp_state(c);
   if (!s || !s->ready || !s->patches || s->n != c->n) {
@@ -704,12 +727,26 @@ int mpnn_apply_add(pd_ctx* c, const double* r, double* z) {
     return PD_ERR_STATE;
   }
   const uint8_t* fixed = qs_fixed_mask(c);
-  k_pt_restrict<double><<<gw(s->np), 256, 0, c->stream>>>(s->np, s->patch_cell.p, s->cstart.p, s->sorted.p, r, fixed,
-                                                          s->scale.p, 1.0, s->v[0].p);
-  TRY_RC(mp_forward(c, s, 0, false));
-  TRY_RC(mp_transpose(c, s, s->h[0][NL].p));
-  k_pt_prolong<<<g1(c->n), 256, 0, c->stream>>>(c->n, s->pid.p, s->out3.p, s->scale.p, 1.0, fixed, z);
-  PD_CUDA_TRY(c, cudaGetLastError());
+  if (!s->apply_exec || s->apply_r != r || s->apply_z != z || s->apply_fixed != fixed) {
+    s->drop_graph();
+    PD_CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = mp_apply_launches(c, s, r, z, fixed);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);  // always ends the capture
+    if (rc != PD_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    PD_CUDA_TRY(c, e);
+    const cudaError_t ei = cudaGraphInstantiate(&s->apply_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) s->apply_exec = nullptr;
+    PD_CUDA_TRY(c, ei);
+    s->apply_r = r;
+    s->apply_z = z;
+    s->apply_fixed = fixed;
+  }
+  PD_CUDA_TRY(c, cudaGraphLaunch(s->apply_exec, c->stream));
   return PD_OK;
 }
 

@@ -404,15 +404,29 @@ __global__ void k_qs_update_p(int64_t n, const double* __restrict__ scal, const 
 }
 
 __global__ void k_qs_set_scalars(double* scal, const double* red, int what) {
-  // what 0: scal[1] = p.q ; what 1: rz_new -> beta
+  // scal: [0] r.z, [1] p.q, [3] beta, [4] r.r; red: [0] z.r, [2] r.r of the new
+  // residual, [4] z.q (flexible only).
+  // what 0: scal[1] = p.q ; what 1: beta = rz_new/rz_old (Fletcher-Reeves on the
+  // preconditioned residual); what 2: flexible beta = max(0, z_new.(r_new -
+  // r_old)/rz_old) with z_new.r_old = z_new.r_new + alpha z_new.q (Polak-Ribiere).
   if (threadIdx.x != 0) return;
   if (what == 0) {
     scal[1] = red[0];
-  } else {
+  } else if (what == 1) {
     const double rz_new = red[0];
-    scal[3] = rz_new / scal[0];  // beta (Fletcher-Reeves on the preconditioned residual)
+    scal[3] = rz_new / scal[0];
     scal[0] = rz_new;
-    scal[4] = red[2];  // r.r
+    scal[4] = red[2];
+  } else {
+    const double rz_old = scal[0];
+    const double alpha = __ddiv_rn(rz_old, scal[1]);
+    const double zr_new = red[0];
+    const double zr_old = __dadd_rn(zr_new, __dmul_rn(alpha, red[4]));
+    const double beta = __ddiv_rn(__dsub_rn(zr_new, zr_old), rz_old);
+    scal[3] = beta > 0.0 ? beta : 0.0;  // also 0 for a NaN beta
+    scal[0] = zr_new;
+    scal[2] = 0.0;
+    scal[4] = red[2];
   }
 }
 
@@ -631,7 +645,7 @@ static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* it
   PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   const double r0 = std::sqrt(h[2]);
-  double rz = h[0];
+  const double rz = h[0];
   *iters = 0;
   *rel_out = 0.0;
   if (r0 == 0.0) return PD_OK;
@@ -646,35 +660,17 @@ static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* it
     k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 0);
     k_qs_axpy2<<<g1(m), kQsBlock, 0, c->stream>>>(m, s->scal.p, s->w.p, s->q.p, s->x.p, s->r.p);
     TRY_RC(qs_apply_precond(c, precond, s->r.p, s->z.p));
-    if (flexible) {
-      // beta = z_new.(r_new - r_old)/rz_old = (z_new.r_new - z_new.r_old)/rz_old with r_old = r_new + alpha q
-      k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
-      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
-      double hz[3], sc[2];
-      PD_CUDA_TRY(c, cudaMemcpyAsync(hz, s->scal.p + 8, sizeof(hz), cudaMemcpyDeviceToHost, c->stream));
-      PD_CUDA_TRY(c, cudaMemcpyAsync(sc, s->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
+    k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
+    if (flexible) {  // z_new.q for beta = z_new.(r_new - r_old)/rz_old, r_old = r_new + alpha q
       k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->z.p, s->q.p, s->q.p, s->partial.p);
       k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 12);
-      double hq[3];
-      PD_CUDA_TRY(c, cudaMemcpyAsync(hq, s->scal.p + 12, sizeof(hq), cudaMemcpyDeviceToHost, c->stream));
-      PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-      const double alpha = sc[0] / sc[1];
-      const double zr_new = hz[0];
-      const double zr_old = zr_new + alpha * hq[0];  // z_new.r_old
-      const double beta = std::max(0.0, (zr_new - zr_old) / rz);
-      rz = zr_new;
-      const double hs[5] = {rz, sc[1], 0.0, beta, hz[2]};
-      PD_CUDA_TRY(c, cudaMemcpyAsync(s->scal.p, hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
-      rel = std::sqrt(hz[2]) / r0;
-    } else {
-      k_qs_dots<<<kRedBlocks, kQsBlock, 0, c->stream>>>(m, s->r.p, s->z.p, s->z.p, s->partial.p);
-      k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 3, 0, s->scal.p + 8);
-      k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, 1);
-      double rr;
-      PD_CUDA_TRY(c, cudaMemcpyAsync(&rr, s->scal.p + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-      PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-      rel = std::sqrt(rr) / r0;
     }
+    k_qs_set_scalars<<<1, 32, 0, c->stream>>>(s->scal.p, s->scal.p + 8, flexible ? 2 : 1);
+    double rr;  // the only host read of the iteration: |r|^2 for the stopping test
+    PD_CUDA_TRY(c, cudaMemcpyAsync(&rr, s->scal.p + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    rel = std::sqrt(rr) / r0;
     ++it;
     if (!std::isfinite(rel)) {
       if (every > 0) mpnn_drop_snapshots(c);
