@@ -48,10 +48,11 @@ def algorithmic_bytes(nb, n, precision="split"):
 
 
 # DRAM bytes (read + write) per launch of the split bond passes on this
-# workload, from one ncu capture (--set full, step 1 of the notched plate):
-# k_dilatation_split<4> 566.3 MB read + 5.7 MB written, k_force_split<4>
-# 633.1 MB read + 8.3 MB written.
-NCU_TRAFFIC = {"dilatation": 572.0e6, "force": 641.4e6}
+# workload, from one ncu capture (--set full, step 1 of the notched plate,
+# sliced bond stream): k_dilatation_split<4> 586.0 MB read + 5.2 MB written,
+# k_force_split<4> 606.1 MB read + 9.2 MB written. The excess over the
+# algorithmic bytes is the slices' padding records (6.3 % of the slots).
+NCU_TRAFFIC = {"dilatation": 591.2e6, "force": 615.3e6}
 
 
 class ClockSampler:
@@ -192,14 +193,18 @@ def qs_leg(local, load_steps):
                 ctx.mpnn_init(seed=0, patch=patch)
                 ctx.mpnn_set_weights(weights)
             st = None
+            clocks = ClockSampler(local)
+            clocks.start()
             t1 = time.perf_counter()
             for k in range(1, len(w2["times"])):
                 st = ctx.qs_load_step(w2["times"][k - 1], w2["times"][k], newton_tolerance=-1e-8,
                                       cg_relative_tolerance=1e-8, preconditioner=precond, stats=st)
             wall = time.perf_counter() - t1
+            clk = clocks.stop()
             out[precond] = {"seconds": st.device_ms / 1e3, "wall_seconds": wall, "cg_iterations": st.cg_iterations,
                             "newton_iterations": st.newton_iterations, "final_cg_residual": st.final_residual,
-                            "fallbacks": st.preconditioner_fallbacks}
+                            "fallbacks": st.preconditioner_fallbacks, "sm_mhz": clk["sm_mhz"],
+                            "clock_reasons": clk["reasons"]}
     bj = out["block_jacobi"]["seconds"]
     out["two_level_speedup_over_block_jacobi"] = bj / out["two_level"]["seconds"]
     out["mpnn_speedup_over_block_jacobi"] = bj / out["mpnn"]["seconds"]
@@ -308,7 +313,9 @@ def main():
 
     # ---- e2e: the drop-in computeForce call with host buffers ---------------
     # Each step: H2D of the current coordinates from pinned memory, damage +
-    # dilatation + force on the device, D2H of the force density.
+    # dilatation + force on the device, D2H of the force density, then the
+    # state update that commits the step's bond damage (the reference's
+    # evalModel + updateState cycle, Peridigm.cpp:1536, 1589).
     esteps = min(args.steps, 500)
     y = torch.from_numpy(ctx.field("Coordinates")).pin_memory()
     f = torch.zeros(3 * n, dtype=torch.float64).pin_memory()
@@ -318,14 +325,16 @@ def main():
     fp = C.cast(f.data_ptr(), C.POINTER(C.c_double))
     for _ in range(3):
         ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
+        ctx._ok(ctx.L.pd_update_state(ctx.h))
     barrier()
     t0 = time.perf_counter()
     for _ in range(esteps):
         ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
+        ctx._ok(ctx.L.pd_update_state(ctx.h))
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
-           "d2h_bytes_per_step": 24 * n, "steps": esteps, "api": "pd_compute_force (host y in, host force out)"}
+           "d2h_bytes_per_step": 24 * n, "steps": esteps, "api": "pd_compute_force (host y in, host force out) + pd_update_state"}
 
     # ---- quasi-static time to 1e-8 (rank 0 only) -----------------------------
     qs = None

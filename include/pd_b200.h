@@ -69,6 +69,7 @@ extern "C" {
 #define PD_FIELD_NUM_NEIGHBORS 10   /* "Number_Of_Neighbors" [n] double */
 #define PD_FIELD_FORCE 11           /* "Force" = Force_Density x Volume (Compute_Force) [3n] double */
 #define PD_FIELD_VOLUME 12          /* "Volume"             [n] double */
+#define PD_FIELD_MODEL_COORDINATES 13 /* "Model_Coordinates" x [3n] double */
 
 typedef struct pd_ctx pd_ctx;
 

@@ -39,6 +39,7 @@ FIELDS = {
     "Number_Of_Neighbors": 10,
     "Force": 11,
     "Volume": 12,
+    "Model_Coordinates": 13,
 }
 
 _dp = C.POINTER(C.c_double)

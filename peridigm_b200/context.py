@@ -361,7 +361,7 @@ class Context:
 
     def field(self, name):
         fid = _lib.FIELDS[name]
-        size = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 9: 3, 11: 3}.get(fid, 1) * self.n
+        size = {0: 3, 1: 3, 2: 3, 3: 3, 4: 3, 9: 3, 11: 3, 13: 3}.get(fid, 1) * self.n
         if fid == _lib.FIELDS["Bond_Damage"]:
             size = self.num_bonds()
         out = np.zeros(size)

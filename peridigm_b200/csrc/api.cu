@@ -161,7 +161,7 @@ int check_status(pd_ctx* c) {
 // evalModel on the configuration already in st[cur]; trial damage on dmg_trial.
 int eval_trial(pd_ctx* c, double* f_dev) {
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
-  c->dmg_gen++;
+  note_damage_copy(c, c->dmg_trial.p, c->dmg.p);
   StepParams sp{};
   sp.mode = EVAL_ONLY;
   sp.damage_on = c->any_damage ? 1 : 0;
@@ -485,7 +485,7 @@ int pd_update_state(pd_ctx* c) {
   TRY(ensure_device(c));
   if (c->trial_valid) {
     PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg.p, c->dmg_trial.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
-    c->dmg_gen++;
+    note_damage_copy(c, c->dmg.p, c->dmg_trial.p);
     PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->trial_valid = false;
   }
@@ -579,7 +579,7 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
   sp.has_contact = contact ? 1 : 0;
   // initial evaluation (Peridigm.cpp:1393-1423): its damage is not committed
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
-  c->dmg_gen++;
+  note_damage_copy(c, c->dmg_trial.p, c->dmg.p);
   if (contact) {
     TRY(contact_prepare(c, 0));
     TRY(contact_eval(c));
@@ -642,7 +642,7 @@ int pd_verlet_begin(pd_ctx* c, double dt, double t0) {
   PD_CUDA_TRY(c, cudaEventRecord(c->vbeg, c->stream));
   // initial evaluation (Peridigm.cpp:1393-1423): its damage is not committed
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
-  c->dmg_gen++;
+  note_damage_copy(c, c->dmg_trial.p, c->dmg.p);
   if (sp.has_contact) {
     TRY(contact_prepare(c, 0));
     TRY(contact_eval(c));
@@ -941,6 +941,9 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
     }
     case PD_FIELD_VOLUME:
       for (int64_t i = 0; i < n; ++i) out[i] = c->hvol[i];
+      return PD_OK;
+    case PD_FIELD_MODEL_COORDINATES:
+      for (int64_t k = 0; k < 3 * n; ++k) out[k] = c->hx[k];
       return PD_OK;
     case PD_FIELD_NUM_NEIGHBORS: {
       std::vector<int64_t> row(n + 1);

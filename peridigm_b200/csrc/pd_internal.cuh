@@ -192,6 +192,19 @@ struct pd_ctx {
   int64_t qs_fallbacks = 0;    // learned-preconditioner solves that fell back to block Jacobi
 };
 
+// A device copy src -> dst of the bond damage: the sliced damage mirror, if it
+// matched src, matches dst afterwards (the contents are equal); any other
+// write to a damage array only advances the generation, and the mirror is
+// refreshed before the next sliced pass.
+inline void note_damage_copy(pd_ctx* c, const uint8_t* dst, const uint8_t* src) {
+  const bool follows = c->sell_src == src && c->sell_gen == c->dmg_gen;
+  c->dmg_gen++;
+  if (follows) {
+    c->sell_src = dst;
+    c->sell_gen = c->dmg_gen;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Launch helpers (implemented in the .cu files)
 // ---------------------------------------------------------------------------

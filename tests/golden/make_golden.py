@@ -347,7 +347,27 @@ def elastic_bond_based():
                      "ElasticBondBased2DPlaneStress_gold.e", True, 0.25, "ElasticBondBased2D.g")
 
 
+def contact_perforation():
+    """The genesis mesh of the restart regression deck (projectile block_1 and
+    target block_2, HEX8, node set nodelist_1 = the projectile's nodes) for
+    the restart test, which checks Run1 + restart + Run2 against the full run
+    as the deck's driver does (its gold output is not in the tree)."""
+    d = os.path.join(REF, "test/regression/Contact_Perforation_With_Restart")
+    g = netcdf_file(os.path.join(d, "Contact_Perforation.g"), "r", mmap=False)
+    ne = g.dimensions["num_elem"]
+    emap = g.variables["elem_num_map"][:] if "elem_num_map" in g.variables else np.arange(1, ne + 1)
+    out = dict(mesh_X=np.stack([g.variables["coord" + a][:] for a in "xyz"], 1).astype(np.float64),
+               mesh_blk_ids=np.array(g.variables["eb_prop1"][:], np.int64),
+               mesh_elem_map=np.array(emap, np.int64),
+               mesh_ns=np.array(g.variables["node_ns1"][:], np.int64))
+    for b in range(g.dimensions["num_el_blk"]):
+        out["mesh_conn%d" % (b + 1)] = np.array(g.variables["connect%d" % (b + 1)][:], np.int64)
+    g.close()
+    np.savez_compressed(os.path.join(OUT, "contact_perforation.npz"), **out)
+
+
 def main():
+    contact_perforation()
     elastic_bond_based()
     unit_elastic()
     finite_plane()

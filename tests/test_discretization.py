@@ -19,6 +19,8 @@ import numpy as np
 import pytest
 from scipy.io import netcdf_file
 
+from _mesh import write_exodus
+
 from oracle import oracle as O
 from peridigm_b200 import discretization as D
 
@@ -46,39 +48,13 @@ def test_element_geometry_equals_compiled_reference():
         assert np.array_equal(c[k], rc) and v[k] == rv
 
 
-def _write_exodus(path, X, blocks, blk_ids, elem_map, node_sets):
-    """A minimal Exodus II genesis file: coordinates, element blocks
-    (connectivity 1-based, elem_type), element id map, node sets."""
-    nc = netcdf_file(path, "w", version=2)
-    nc.createDimension("num_nodes", X.shape[0])
-    nc.createDimension("num_dim", 3)
-    nc.createDimension("num_elem", sum(len(c) for c, _ in blocks))
-    nc.createDimension("num_el_blk", len(blocks))
-    nc.createDimension("num_node_sets", len(node_sets))
-    for a, k in zip("xyz", range(3)):
-        nc.createVariable("coord" + a, "d", ("num_nodes",))[:] = X[:, k]
-    nc.createVariable("eb_prop1", "i", ("num_el_blk",))[:] = blk_ids
-    for b, (conn, et) in enumerate(blocks):
-        nc.createDimension("num_el_in_blk%d" % (b + 1), conn.shape[0])
-        nc.createDimension("num_nod_per_el%d" % (b + 1), conn.shape[1])
-        v = nc.createVariable("connect%d" % (b + 1), "i", ("num_el_in_blk%d" % (b + 1), "num_nod_per_el%d" % (b + 1)))
-        v[:] = conn
-        v.elem_type = et
-    nc.createVariable("elem_num_map", "i", ("num_elem",))[:] = elem_map
-    nc.createVariable("ns_prop1", "i", ("num_node_sets",))[:] = np.arange(1, len(node_sets) + 1)
-    for s, nodes in enumerate(node_sets):
-        nc.createDimension("num_nod_ns%d" % (s + 1), len(nodes))
-        nc.createVariable("node_ns%d" % (s + 1), "i", ("num_nod_ns%d" % (s + 1),))[:] = nodes
-    nc.close()
-
-
 @pytest.mark.parametrize("case", ["bond_based_3d", "bond_based_plane_strain"])
 def test_genesis_mesh_matches_reference_output(case, tmp_path):
     z = np.load(os.path.join(G, case + ".npz"))
     nblk = len(z["mesh_blk_ids"])
     blocks = [(z["mesh_conn%d" % (b + 1)], "HEX8") for b in range(nblk)]
     path = str(tmp_path / "mesh.g")
-    _write_exodus(path, z["mesh_X"], blocks, z["mesh_blk_ids"], z["mesh_elem_map"], [z["mesh_ns"]])
+    write_exodus(path, z["mesh_X"], blocks, z["mesh_blk_ids"], z["mesh_elem_map"], [z["mesh_ns"]])
     d = D.exodus(path)
     x = d["x"].reshape(-1, 3)
     assert np.abs(x - z["x"]).max() <= 1e-12          # .comp COORDINATES absolute 1e-12
@@ -97,7 +73,7 @@ def test_mixed_mesh_and_node_sets(tmp_path):
     hexes = np.array([[1, 2, 3, 4, 5, 6, 7, 8], [2, 9, 10, 3, 6, 11, 12, 7]])
     tets = np.array([[6, 11, 7, 13], [11, 12, 7, 13]])
     elem_map = np.array([3, 1, 4, 2])  # global ids of the file's elements
-    _write_exodus(str(tmp_path / "m.g"), X, [(hexes, "HEX8"), (tets, "TETRA")], [5, 2], elem_map,
+    write_exodus(str(tmp_path / "m.g"), X, [(hexes, "HEX8"), (tets, "TETRA")], [5, 2], elem_map,
                   [np.array([13]), np.array([1, 4])])
     d = D.exodus(str(tmp_path / "m.g"))
     hc, hv = D.hex_centroid_volume(X[hexes - 1])

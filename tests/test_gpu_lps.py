@@ -169,6 +169,68 @@ def test_device_pointer_entry():
         assert np.array_equal(fd.cpu().numpy(), f_host)
 
 
+def test_sliced_damage_mirror_follows_the_state_cycle():
+    """The 4-lanes-per-point split passes read a sliced copy of the bond damage.
+    Through a cycle of trial evaluations, commits, damage set from the host and
+    Verlet steps, their bond damage equals the CSR split path's (8 lanes per
+    point, same per-bond arithmetic) exactly, and forces agree to 1e-6."""
+    x, vol, _, h = make_cloud(seed=5)
+    ys = [make_cloud(seed=5, strain=s)[2] for s in (1.0e-3, 2.0e-3, 2.5e-3, 3.5e-3, 4.5e-3)]
+    n = len(vol)
+    ctxs = [Context(precision="split", threads_per_point=t) for t in (4, 8)]
+    try:
+        for c in ctxs:
+            c.set_points(x, vol)
+            c.set_horizons([h])
+            c.build_bonds()
+            c.material(130e9, 78e9, 7800.0)
+            c.critical_stretch(1.5e-3)
+        nb = len(ctxs[0].bonds_csr()[1])
+        rng = np.random.default_rng(3)
+
+        def both(fn):
+            return [fn(c) for c in ctxs]
+
+        def same():
+            d4, d8 = both(lambda c: c.field("Bond_Damage"))
+            assert np.array_equal(d4, d8)
+            return d4
+
+        seen = []
+        f4, f8 = both(lambda c: c.compute_force(ys[0]))
+        assert rel_l2(f4, f8) < 1e-6
+        seen.append(same().sum())
+        both(lambda c: c.update_state())
+        f4, f8 = both(lambda c: c.compute_force(ys[2]))  # trial, not committed
+        assert rel_l2(f4, f8) < 1e-6
+        seen.append(same().sum())
+        f4, f8 = both(lambda c: c.compute_force(ys[1]))  # trial again from the committed damage
+        assert rel_l2(f4, f8) < 1e-6
+        same()
+        both(lambda c: c.update_state())
+        bd = (rng.random(nb) < 0.02).astype(float)
+        row, col = ctxs[0].bonds_csr()
+        owner = np.repeat(np.arange(n), np.diff(row))
+        key = {(int(i), int(j)) for i, j, b in zip(owner, col, bd) if b}
+        bd = np.array([1.0 if (int(i), int(j)) in key or (int(j), int(i)) in key else 0.0 for i, j in zip(owner, col)])
+        both(lambda c: c.set_bond_damage(bd))
+        f4, f8 = both(lambda c: c.compute_force(ys[3]))
+        assert rel_l2(f4, f8) < 1e-6
+        seen.append(same().sum())
+        both(lambda c: c.update_state())
+        dt = 0.5 * ctxs[0].critical_time_step()
+        both(lambda c: c.set_state((ys[3] - x) * 0.0, np.zeros_like(x)))
+        both(lambda c: c.verlet_run(dt, 3))
+        same()
+        f4, f8 = both(lambda c: c.compute_force(ys[4]))
+        assert rel_l2(f4, f8) < 1e-6
+        seen.append(same().sum())
+        assert seen[-1] > seen[0] and seen[-1] > 0  # bonds broke along the way
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_errors_are_reported():
     with Context() as ctx:
         y = np.zeros(3)
