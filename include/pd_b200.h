@@ -301,6 +301,34 @@ typedef struct {
  * iterations and device time. */
 int pd_qs_load_step(pd_ctx* ctx, double t_prev, double t_cur, const pd_qs_options* options, pd_stats* stats);
 
+/* ---- implicit dynamics ------------------------------------------------------ */
+typedef struct {
+  double beta;                  /* Newmark "Beta" (Peridigm.cpp:3647, default 0.25) */
+  double gamma;                 /* Newmark "Gamma" (:3648, default 0.50) */
+  double absolute_tolerance;    /* on ||R||_2, R = beta dt^2 (rho a - f) with the prescribed rows zeroed
+                                 * ("Absolute Tolerance", :3644, default 1e-6) */
+  double cg_relative_tolerance; /* of each linear solve (Belos "Convergence Tolerance" 1e-10, :3668) */
+  int32_t max_newton_iterations;/* "Maximum Solver Iterations" (:3645, default 10); as in the reference the
+                                 * Newton loop runs while the iteration count is <= this (:3815) */
+  int32_t max_cg_iterations;
+  int32_t preconditioner;       /* PD_PRECOND_NONE (the reference: plain CG) or PD_PRECOND_BLOCK_JACOBI on the
+                                 * 3x3 blocks of rho I + beta dt^2 K */
+} pd_implicit_options;
+
+/* nsteps implicit Newmark-beta steps of dt from t0, Peridigm::executeImplicit
+ * (src/core/Peridigm.cpp:3620-4016): per step the predictor u2 = u + dt v +
+ * dt^2 (1/2 - beta) a, v2 = v + dt (1 - gamma) a, then Newton on
+ * R = beta dt^2 (rho a - f) with the operator rho I + beta dt^2 K
+ * (computeImplicitJacobian :4319-4338, K = -d(V f)/du applied matrix-free)
+ * and CG; after each correction a = (u - u2)/(beta dt^2), v = v2 + dt gamma a.
+ * Prescribed dofs start at u = a t0 + b with velocity a and follow the
+ * predictor; their rows are left out of the solve. Bond damage is held fixed;
+ * LPS material only; the solve is FP64 whatever the context's precision.
+ * Updates displacement, velocity, acceleration and force density. stats (may
+ * be NULL) accumulates steps, Newton and CG iterations and device time. */
+int pd_implicit_run(pd_ctx* ctx, double dt, double t0, int64_t nsteps, const pd_implicit_options* options,
+                    pd_stats* stats);
+
 /* Material::computeJacobian (src/materials/Peridigm_Material.hpp:174-180,
  * FULL_MATRIX) in matrix-free form: kw = K w with K = -d(V f)/du at
  * displacement u (V-weighted, Scale(-1): Peridigm_ElasticMaterial.cpp:366-370,

@@ -349,6 +349,58 @@ def qs_solve(x, vol, row, col, K, mu, horizon, bc, times, tol, max_iter=50, u0=N
     return out
 
 
+def implicit_newmark(x, vol, row, col, K, mu, rho, horizon, u0, v0, dt, nsteps, beta=0.25, gamma=0.5,
+                     tol=1.0e-6, max_iter=10, bc_dofs=()):
+    """Implicit dynamics restated from Peridigm::executeImplicit
+    (Peridigm.cpp:3620-4016) with a dense linear solve in place of Belos CG.
+    Per step: u2 = un + dt vn + 0.5 dt^2 (1 - 2 beta) an, v2 = vn + dt (1 -
+    gamma) an (:3726-3730); u = u2, a = (u - u2)/(beta dt^2), v = v2 + dt
+    gamma a (:3752-3759); R = beta dt^2 (rho a - f) with the prescribed rows
+    zeroed (:3803-3810); while ||R||_2 > tol and at most max_iter + 1 times
+    (:3815): J = rho I + beta dt^2 K with K = -d(V f)/du
+    (computeImplicitJacobian :4319-4338), prescribed rows and columns zeroed
+    with a unit diagonal, J du = -R, u += du, a and v updated, R recomputed.
+    Prescribed dofs keep the predictor (the solve leaves them alone). rho per
+    point or scalar. Returns per step (u, v, a, f, Newton iterations)."""
+    n = len(vol)
+    rho3 = np.repeat(_per_point(rho, n), 3)
+    bc = list(bc_dofs)
+    u, v, a = _f64(u0).copy(), _f64(v0).copy(), np.zeros(3 * n)
+    bdt2 = beta * (dt * dt)
+    out = []
+    for _ in range(nsteps):
+        un, vn, an = u.copy(), v.copy(), a.copy()
+        u2 = (un + dt * vn) + (0.5 * (dt * dt) * (1.0 - 2.0 * beta)) * an
+        v2 = vn + (dt * (1.0 - gamma)) * an
+        u = u2.copy()
+        a = (u - u2) * (1.0 / bdt2)
+        v = v2 + (dt * gamma) * a
+
+        def resid(u, a):
+            f = eval_model(x, _f64(x) + u, vol, row, col, K, mu, horizon)["force"]
+            R = bdt2 * (rho3 * a - f)
+            R[bc] = 0.0
+            return f, R
+
+        f, R = resid(u, a)
+        it = 0
+        while np.linalg.norm(R) > tol and it <= max_iter:
+            J = bdt2 * tangent_dense(x, _f64(x) + u, vol, row, col, K, mu, horizon) + np.diag(rho3)
+            for d in bc:
+                J[d, :] = 0.0
+                J[:, d] = 0.0
+                J[d, d] = 1.0
+            du = np.linalg.solve(J, -R)
+            du[bc] = 0.0
+            u = u + du
+            a = (u - u2) * (1.0 / bdt2)
+            v = v2 + (dt * gamma) * a
+            f, R = resid(u, a)
+            it += 1
+        out.append((u.copy(), v.copy(), a.copy(), f.copy(), it))
+    return out
+
+
 def coarse_aggregates(x, horizon_max, cell=0.0, max_coarse=6144):
     """Aggregates of the two-level preconditioner (no reference counterpart):
     the non-empty cells, numbered in cell order (x fastest), of a grid of side

@@ -77,6 +77,12 @@ class QsOptions(C.Structure):
                 ("preconditioner", C.c_int32), ("use_predictor", C.c_int32), ("coarse_cell", C.c_double)]
 
 
+class ImplicitOptions(C.Structure):
+    _fields_ = [("beta", C.c_double), ("gamma", C.c_double), ("absolute_tolerance", C.c_double),
+                ("cg_relative_tolerance", C.c_double), ("max_newton_iterations", C.c_int32),
+                ("max_cg_iterations", C.c_int32), ("preconditioner", C.c_int32)]
+
+
 # name -> (restype, argtypes); every symbol include/pd_b200.h declares.
 SIGNATURES = {
     "pd_create": (C.c_int, [C.POINTER(Config), C.POINTER(_vp)]),
@@ -115,6 +121,7 @@ SIGNATURES = {
     "pd_contact_short_range": (C.c_int, [_vp, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "pd_contact_force": (C.c_int, [_vp, _dp, _dp, _dp]),
     "pd_qs_load_step": (C.c_int, [_vp, C.c_double, C.c_double, C.c_void_p, C.POINTER(Stats)]),
+    "pd_implicit_run": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int64, C.c_void_p, C.POINTER(Stats)]),
     "pd_jacobian_apply": (C.c_int, [_vp, _dp, _dp, _dp]),
     "pd_jacobian_block_diagonal": (C.c_int, [_vp, _dp, _dp]),
     "pd_mpnn_init": (C.c_int, [_vp, C.c_uint64, C.c_double]),

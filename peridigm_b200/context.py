@@ -259,6 +259,23 @@ class Context:
                                         C.byref(st)))
         return st
 
+    def implicit_run(self, dt, nsteps, t0=0.0, beta=0.25, gamma=0.5, absolute_tolerance=1.0e-6,
+                     cg_relative_tolerance=1.0e-10, max_newton=10, max_cg=None, preconditioner="block_jacobi",
+                     stats=None):
+        """nsteps implicit Newmark-beta steps (Peridigm::executeImplicit); preconditioner "none" (the
+        reference's plain CG) or "block_jacobi"."""
+        o = _lib.ImplicitOptions()
+        o.beta, o.gamma = float(beta), float(gamma)
+        o.absolute_tolerance = float(absolute_tolerance)
+        o.cg_relative_tolerance = float(cg_relative_tolerance)
+        o.max_newton_iterations = int(max_newton)
+        o.max_cg_iterations = int(max_cg if max_cg is not None else max(3 * self.n, 100))
+        o.preconditioner = {"none": _lib.PD_PRECOND_NONE, "block_jacobi": _lib.PD_PRECOND_BLOCK_JACOBI}[preconditioner]
+        st = stats if stats is not None else _lib.Stats()
+        self._ok(self.L.pd_implicit_run(self.h, float(dt), float(t0), int(nsteps), C.cast(C.byref(o), C.c_void_p),
+                                        C.byref(st)))
+        return st
+
     def jacobian_apply(self, u, w):
         u, w = _f64(u, 3 * self.n, "u"), _f64(w, 3 * self.n, "w")
         kw = np.zeros(3 * self.n)

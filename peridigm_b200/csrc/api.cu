@@ -734,6 +734,17 @@ int pd_qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options*
   return qs_load_step(c, t_prev, t_cur, o, st);
 }
 
+int pd_implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_implicit_options* o, pd_stats* st) {
+  CHECK_CTX(c);
+  if (!o) return fail(c, PD_ERR_ARG, "pd_implicit_run: null options");
+  if (!(dt > 0.0) || nsteps < 0 || !(o->beta > 0.0) || !(o->gamma >= 0.0) || !(o->absolute_tolerance >= 0.0) ||
+      !(o->cg_relative_tolerance > 0.0) || o->max_newton_iterations < 0 || o->max_cg_iterations <= 0 ||
+      (o->preconditioner != PD_PRECOND_NONE && o->preconditioner != PD_PRECOND_BLOCK_JACOBI))
+    return fail(c, PD_ERR_ARG, "pd_implicit_run: bad options");
+  if (!c->state_init) TRY(pd_set_state(c, nullptr, nullptr));
+  return implicit_run(c, dt, t0, nsteps, o, st);
+}
+
 int pd_mpnn_init(pd_ctx* c, uint64_t seed, double patch) {
   CHECK_CTX(c);
   if (!(patch > 0.0) || !std::isfinite(patch)) return fail(c, PD_ERR_ARG, "pd_mpnn_init: patch side must be positive");

@@ -55,6 +55,10 @@ struct QsState {
   double coarse_cell = -1.0;
   int64_t coarse_ref_iters = -1;
   bool coarse_rebuild = true;
+  // The operator the CG products and block-Jacobi blocks use: jm rho I + jk K
+  // (quasi-static: K; implicit dynamics: rho I + beta dt^2 K).
+  double jk = 1.0, jm = 0.0;
+  DBuf<double> v2;  // implicit dynamics: velocity predictor
 };
 
 __device__ __forceinline__ double qs_omega(int kind, double zeta, double h) {
@@ -202,7 +206,8 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_dtheta_g(int64_t n, const int64
   if (valid && lane == 0) w[i].w = 3.0 * (ab[i].y / pt[i].x) * acc;
 }
 
-// Tangent pass 2 on the geometry: q = K p = -V d f (prescribed rows: q = p); block partials of p.q
+// Tangent pass 2 on the geometry: q = K p = -V d f (prescribed rows: q = p), or
+// (jm rho I + jk K) p for implicit dynamics; block partials of p.q
 //   V_j [dT yh + (T/|Y|)(dw - yh de)] = c2 (q dth_i + q dth_j) yh + V_j om (a_i + a_j) de yh + V_j T/|Y| (dw - yh de)
 __global__ void __launch_bounds__(kQsBlock) k_qs_df_g(int64_t n, const int64_t* __restrict__ row,
                                                       const int32_t* __restrict__ col,
@@ -211,7 +216,8 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_df_g(int64_t n, const int64_t* 
                                                       const double4* __restrict__ xv,
                                                       const double4* __restrict__ w,
                                                       const uint8_t* __restrict__ fixed, double* __restrict__ q,
-                                                      double* __restrict__ partial) {
+                                                      double* __restrict__ partial, const double4* __restrict__ pt,
+                                                      double jk, double jm) {
   __shared__ double spq[kQsBlock];
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
   const int lane = threadIdx.x & (kQsTpo - 1);
@@ -239,7 +245,9 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_df_g(int64_t n, const int64_t* 
   if (valid && lane < 3) {
     const double d = lane == 0 ? d0 : (lane == 1 ? d1 : d2);
     const double p = lane == 0 ? wi.x : (lane == 1 ? wi.y : wi.z);
-    const double out = ((fixed[i] >> lane) & 1) ? p : -xv[i].w * d;
+    double kd = -xv[i].w * d;
+    if (jm != 0.0) kd = jm * pt[i].w * p + jk * kd;  // implicit dynamics: (rho I + beta dt^2 K) p
+    const double out = ((fixed[i] >> lane) & 1) ? p : kd;
     q[3 * i + lane] = out;
     pq = p * out;
   }
@@ -262,7 +270,8 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_block_diag(int64_t n, const int
                                                             const double4* __restrict__ pt,
                                                             const double* __restrict__ hp, int influence,
                                                             const uint8_t* __restrict__ fixed,
-                                                            double* __restrict__ dinv, int invert) {
+                                                            double* __restrict__ dinv, int invert, double jk = 1.0,
+                                                            double jm = 0.0) {
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
   const int lane = threadIdx.x & (kQsTpo - 1);
   const bool valid = i < n;
@@ -304,6 +313,8 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_block_diag(int64_t n, const int
     double A[9];
     for (int r = 0; r < 3; ++r)
       for (int c = 0; c < 3; ++c) A[3 * r + c] = -xi.w * (D[3 * r + c] - s * hv[r] * hv[c]);  // K_ii = -V_i D_i
+    if (jm != 0.0)  // implicit dynamics: blocks of rho I + beta dt^2 K
+      for (int k = 0; k < 9; ++k) A[k] = jk * A[k] + ((k % 4 == 0) ? jm * pt[i].w : 0.0);
     const uint8_t fx = fixed[i];
     for (int c = 0; c < 3; ++c)
       if ((fx >> c) & 1)
@@ -537,7 +548,7 @@ static int qs_tangent(pd_ctx* c) {
   }
   k_qs_dtheta_g<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->abq.p, c->pt.p, s->w.p);
   k_qs_df_g<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->gco.p, c->xv.p, s->w.p,
-                                               s->fixed.p, s->q.p, s->partial.p);
+                                               s->fixed.p, s->q.p, s->partial.p, c->pt.p, s->jk, s->jm);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
 }
@@ -923,6 +934,199 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   if (metric > newton_tol) {
     c->err = "quasi-static Newton iteration did not reach its tolerance";
     return PD_ERR_NOT_CONVERGED;
+  }
+  return PD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Implicit dynamics (Peridigm::executeImplicit, src/core/Peridigm.cpp:3620-4016):
+// Newmark-beta steps, each solved by Newton on R = beta dt^2 (rho a - f) with
+// the prescribed rows zeroed, the operator rho I + beta dt^2 K
+// (computeImplicitJacobian :4319-4338, K = -d(V f)/du as in the quasi-static
+// tangent) applied matrix-free, CG on it (Belos BlockCG in the reference).
+// Vector updates follow the reference's Epetra Update/Scale order, without
+// fused multiply-adds.
+// ---------------------------------------------------------------------------
+// u2 = un + dt vn + cu an, v2 = vn + cv an (:3726-3730); u = u2, a = (u - u2)
+// * (1/(beta dt^2)) = 0, v = v2 + dt gamma a = v2 (:3752-3759).
+__global__ void k_imp_predict(int64_t m, double dt, double cu, double cv, double* __restrict__ u,
+                              double* __restrict__ v, double* __restrict__ a, double* __restrict__ u2,
+                              double* __restrict__ v2) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const double un = u[k], vn = v[k], an = a[k];
+  const double p = __dadd_rn(__dadd_rn(un, __dmul_rn(dt, vn)), __dmul_rn(cu, an));
+  const double q = __dadd_rn(vn, __dmul_rn(cv, an));
+  u2[k] = p;
+  v2[k] = q;
+  u[k] = p;
+  a[k] = 0.0;
+  v[k] = q;
+}
+
+// u += du; a = (u - u2) * (1/(beta dt^2)); v = v2 + dt gamma a (:3893-3902).
+__global__ void k_imp_correct(int64_t m, double ibdt2, double dtg, const double* __restrict__ du,
+                              double* __restrict__ u, const double* __restrict__ u2, double* __restrict__ a,
+                              const double* __restrict__ v2, double* __restrict__ v) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const double uu = __dadd_rn(u[k], du[k]);
+  const double aa = __dmul_rn(__dsub_rn(uu, u2[k]), ibdt2);
+  u[k] = uu;
+  a[k] = aa;
+  v[k] = __dadd_rn(v2[k], __dmul_rn(dtg, aa));
+}
+
+// R = beta dt^2 (rho a - f) (:3803-3806) with the prescribed rows zeroed
+// (:3810); rhs = -R for J du = -R; block partials (sum R^2, max |R|).
+__global__ void k_imp_residual(int64_t n, double bdt2, const double* __restrict__ f, const double* __restrict__ a,
+                               const double4* __restrict__ pt, const uint8_t* __restrict__ fixed,
+                               double* __restrict__ rhs, double* __restrict__ partial) {
+  __shared__ double s2[kQsBlock], sm[kQsBlock];
+  double a2 = 0.0, am = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = k / 3;
+    const int c = (int)(k - 3 * i);
+    double r = __dmul_rn(bdt2, __dsub_rn(__dmul_rn(pt[i].w, a[k]), f[k]));
+    if ((fixed[i] >> c) & 1) r = 0.0;
+    rhs[k] = -r;
+    a2 += r * r;
+    am = fmax(am, fabs(r));
+  }
+  s2[threadIdx.x] = a2;
+  sm[threadIdx.x] = am;
+  __syncthreads();
+  for (int o = kQsBlock / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s2[threadIdx.x] += s2[threadIdx.x + o];
+      sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s2[0];
+    partial[2 * blockIdx.x + 1] = sm[0];
+  }
+}
+
+// Prescribed dofs at the run's start: u = a t0 + b, v = a (the rate).
+__global__ void k_imp_bc_start(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ ba,
+                               const double* __restrict__ bb, double t0, double* __restrict__ u,
+                               double* __restrict__ v, double* __restrict__ a) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int c = 0; c < 3; ++c)
+    if ((mask[i] >> c) & 1) {
+      const int64_t k = 3 * i + c;
+      u[k] = ba[k] * t0 + bb[k];
+      v[k] = ba[k];
+      a[k] = 0.0;
+    }
+}
+
+// Force density at x + u (frozen bond damage) and the residual norm ||R||_2.
+static int imp_residual(pd_ctx* c, double bdt2, double* norm) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, c->u.p, s->du.p, s->yq.p);
+  PD_CUDA_TRY(c, launch_fp64_eval_at(c, s->yq.p, s->abq.p, s->th.p, s->nd.p, s->f.p));
+  s->geo_dirty = true;
+  k_imp_residual<<<kRedBlocks, kQsBlock, 0, c->stream>>>(n, bdt2, s->f.p, c->a.p, c->pt.p, s->fixed.p, s->r.p,
+                                                         s->partial.p);
+  k_qs_reduce<<<1, kQsBlock, 0, c->stream>>>(s->partial.p, kRedBlocks, 2, 1, s->scal.p + 8);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  double h[2];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(h, s->scal.p + 8, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  *norm = std::sqrt(h[0]);
+  if (!std::isfinite(*norm)) {
+    c->err = "NaN returned by force evaluation";
+    return PD_ERR_NONFINITE;
+  }
+  return PD_OK;
+}
+
+int implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_implicit_options* o, pd_stats* st) {
+  TRY_RC(ensure_ready_internal(c));
+  if (c->material_model != PD_MATERIAL_LPS) {
+    c->err = "the implicit solve supports the LPS material model only";
+    return PD_ERR_UNSUPPORTED;
+  }
+  TRY_RC(qs_alloc(c));
+  QsState* s = c->qs;
+  const int64_t n = c->n, m = 3 * n;
+  PD_CUDA_TRY(c, s->v2.alloc(m));
+  std::vector<uint8_t> fx(n, 0);
+  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
+  PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
+  PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
+  if (c->has_bc)
+    k_imp_bc_start<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t0, c->u.p, c->v.p,
+                                                      c->a.p);
+  const double beta = o->beta, gamma = o->gamma;
+  const double dt2 = dt * dt, bdt2 = beta * dt2, ibdt2 = 1.0 / bdt2, dtg = dt * gamma;
+  const double cu = 0.5 * dt2 * (1.0 - 2.0 * beta), cv = dt * (1.0 - gamma);
+  s->jk = bdt2;
+  s->jm = 1.0;
+  s->coarse_on = false;
+  const int precond = o->preconditioner;
+  int64_t newton_total = 0, cg_total = 0;
+  double last_rel = 0.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c->stream);
+  int rc = PD_OK;
+  for (int64_t step = 0; step < nsteps && rc == PD_OK; ++step) {
+    k_imp_predict<<<g1(m), kQsBlock, 0, c->stream>>>(m, dt, cu, cv, c->u.p, c->v.p, c->a.p, s->pred.p, s->v2.p);
+    double norm = 0.0;
+    rc = imp_residual(c, bdt2, &norm);
+    int it = 0;
+    while (rc == PD_OK && norm > o->absolute_tolerance && it <= o->max_newton_iterations) {
+      if (precond == PD_PRECOND_BLOCK_JACOBI) {
+        k_qs_qm<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->pt.p, s->abq.p);
+        k_qs_block_diag<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, s->yq.p,
+                                                           s->abq.p, c->pt.p, c->hp.p, c->influence, s->fixed.p,
+                                                           s->dinv.p, 1, s->jk, s->jm);
+      }
+      int its = 0;
+      double rel = 0.0;
+      bool stalled = false;
+      const int r2 = qs_cg_run(c, precond, o->cg_relative_tolerance, o->max_cg_iterations, &its, &rel, &stalled);
+      if (r2 != PD_OK && r2 != PD_ERR_NOT_CONVERGED) {  // a CG that stops short is used as it is (:3870-3872)
+        rc = r2;
+        break;
+      }
+      cg_total += its;
+      last_rel = rel;
+      k_imp_correct<<<g1(m), kQsBlock, 0, c->stream>>>(m, ibdt2, dtg, s->x.p, c->u.p, s->pred.p, c->a.p, s->v2.p,
+                                                       c->v.p);
+      rc = imp_residual(c, bdt2, &norm);
+      ++it;
+    }
+    newton_total += it;
+  }
+  s->jk = 1.0;
+  s->jm = 0.0;
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != PD_OK) return rc;
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->f.p, s->f.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  PD_CUDA_TRY(c, cudaMemcpyAsync(c->theta.p, s->th.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  c->cur = 0;
+  PD_CUDA_TRY(c, launch_sync_state(c));
+  PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (st) {
+    st->steps += nsteps;
+    st->newton_iterations += newton_total;
+    st->cg_iterations += cg_total;
+    st->final_residual = last_rel;
+    st->device_ms += ms;
+    st->bonds = c->nb;
   }
   return PD_OK;
 }

@@ -226,6 +226,7 @@ int ensure_ready_internal(pd_ctx* c);
 
 // quasi-static (k_qs.cu) and the learned preconditioner (k_mpnn.cu)
 int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st);
+int implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_implicit_options* o, pd_stats* st);
 int qs_tangent_apply(pd_ctx* c, const double* u_dev, const double* w_dev, double* kw_dev);
 int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev);
 int qs_prepare_current(pd_ctx* c);

@@ -366,7 +366,30 @@ def contact_perforation():
     np.savez_compressed(os.path.join(OUT, "contact_perforation.npz"), **out)
 
 
+def compression_implicit():
+    """Gold output of the two implicit-dynamics verification decks (two points
+    at x = -1, 1, volume 2 each, horizon 2, K 130e9, mu 78e9, rho 7800,
+    Newmark beta 0.25, gamma 0.5, dt 1e-5, five steps, absolute tolerance 1e-10):
+    CompressionImplicit_2x1x1 (initial velocities +-1 in x) and
+    CompressionImplicitEssentialBC_2x1x1 (point 0 held at u_x = 0.1, point 1
+    at v_x = -1). Acceleration in the output is Compute_Acceleration
+    (Force_Density / density)."""
+    out = {}
+    for stem in ("CompressionImplicit_2x1x1", "CompressionImplicitEssentialBC_2x1x1"):
+        nc = netcdf_file(os.path.join(REF, "test/verification", stem, stem + "_gold.e"), "r", mmap=False)
+        nv = _names(nc, "name_nod_var")
+        key = "essential" if "Essential" in stem else "free"
+        out[key + "_time"] = np.array(nc.variables["time_whole"][:], np.float64)
+        out[key + "_x"] = np.stack([nc.variables["coord" + a][:] for a in "xyz"], 1).astype(np.float64)
+        for nm in ("Displacement", "Velocity", "Force", "Force_Density", "Acceleration"):
+            out[key + "_" + nm] = np.stack([np.array(nc.variables["vals_nod_var%d" % (nv.index(nm + c) + 1)][:],
+                                                     np.float64) for c in "XYZ"], 2)
+        nc.close()
+    np.savez_compressed(os.path.join(OUT, "compression_implicit.npz"), **out)
+
+
 def main():
+    compression_implicit()
     contact_perforation()
     elastic_bond_based()
     unit_elastic()
