@@ -109,6 +109,10 @@ def lib():
                                     C.c_int, C.c_double, _dp]
         L.pdo_force_bond_based.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp, C.c_double, C.c_int,
                                            C.c_double, _dp]
+        L.pdo_dilatation_linear_lps.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, C.c_int,
+                                                C.c_double, _dp]
+        L.pdo_force_linear_lps.argtypes = [C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _i64p, _i32p, _dp, _dp,
+                                           C.c_int, C.c_double, _dp]
         L.pdo_critical_time_step.restype = C.c_double
         L.pdo_critical_time_step.argtypes = [C.c_int64, _dp, _dp, _i64p, _i32p, _dp, _dp, C.c_double]
         L.pdo_contact_count.restype = C.c_int64
@@ -265,6 +269,28 @@ def force_lps(x, y, m, vol, theta, dmg, row, col, K, mu, horizon, influence=0):
     lib().pdo_force_lps(n, _d(x), _d(y), _d(m), _d(vol), _d(theta), _d(dmg), _i64(row), _i32(col),
                         _d(Kp), _d(mup), influence, horizon, _d(f))
     return f
+
+
+def eval_linear_lps(x, y, vol, row, col, K, mu, horizon, s_c=None, dmg_n=None, influence=0):
+    """The Linear LPS material's evaluation (LinearLPSPVMaterial::precompute +
+    computeForce, Peridigm_LinearLPSPVMaterial.cpp:231-394) after the damage
+    model, in evalModel order: weighted volume, dilatation, force density."""
+    x, y, vol = _f64(x), _f64(y), _f64(vol)
+    n = vol.size
+    m = weighted_volume(x, vol, row, col, horizon, influence)
+    if dmg_n is None:
+        dmg_n = np.zeros(len(col))
+    if s_c is not None:
+        dmg, nd = damage_critical_stretch(x, y, row, col, s_c, dmg_n)
+    else:
+        dmg, nd = np.asarray(dmg_n, dtype=np.float64).copy(), None
+    th = np.zeros(n)
+    lib().pdo_dilatation_linear_lps(n, _d(x), _d(y), _d(m), _d(vol), _d(dmg), _i64(row), _i32(col), influence,
+                                    horizon, _d(th))
+    f = np.zeros(3 * n)
+    lib().pdo_force_linear_lps(n, _d(x), _d(y), _d(m), _d(vol), _d(th), _d(dmg), _i64(row), _i32(col),
+                               _d(_per_point(K, n)), _d(_per_point(mu, n)), influence, horizon, _d(f))
+    return {"m": m, "theta": th, "force": f, "bond_damage": dmg, "damage": nd}
 
 
 def eval_model(x, y, vol, row, col, K, mu, horizon, s_c=None, dmg_n=None, influence=0, m=None):

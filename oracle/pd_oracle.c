@@ -364,6 +364,86 @@ void pdo_force_bond_based(int64_t n, const double* x, const double* y, const dou
 }
 
 /* ---------------------------------------------------------------------------
+ * Linear LPS ("Linear LPS Partial Volume" without partial volumes or improved
+ * quadrature): the loops of PeridigmNS::LinearLPSPVMaterial::precompute
+ * (src/materials/Peridigm_LinearLPSPVMaterial.cpp:231-292) and ::computeForce
+ * (:295-394), which the material runs (not the functions of
+ * linear_lps_pv.cxx, which square sqrt(|zeta|^2) instead of using |zeta|^2).
+ *   theta_i = 3/m_i * sum omega (1-d) zeta.(u_j - u_i) V_j
+ *   f = (1-d) (t1 zeta + t2 (zeta zeta^T)(u_j - u_i)),
+ *   t1 = (9K - 15mu) omega theta_i / (3 m_i), t2 = 15mu omega / (m_i |zeta|^2),
+ *   f_i += f V_j, f_j -= f V_i (scatter). omega is the bond's influence
+ *   value (computeAndStoreInfluenceFunctionValues, material_utilities.cxx:55-84).
+ * ------------------------------------------------------------------------- */
+static double lin_omega(int influence, const double* X, const double* XN, double horizon) {
+  double d = sqrt((X[0] - XN[0]) * (X[0] - XN[0]) + (X[1] - XN[1]) * (X[1] - XN[1]) + (X[2] - XN[2]) * (X[2] - XN[2]));
+  return pdo_influence(influence, d, horizon);
+}
+
+void pdo_dilatation_linear_lps(int64_t n, const double* x, const double* y, const double* m, const double* vol,
+                               const double* dmg, const int64_t* row, const int32_t* col, int influence,
+                               double horizon, double* theta) {
+  for (int64_t p = 0; p < n; ++p) {
+    const double* xs = &x[3 * p];
+    const double* ys = &y[3 * p];
+    double th = 0.0;
+    for (int64_t b = row[p]; b < row[p + 1]; ++b) {
+      int64_t j = col[b];
+      const double* xn = &x[3 * j];
+      const double* yn = &y[3 * j];
+      double zeta[3], u[3], un[3];
+      for (int i = 0; i < 3; ++i) {
+        zeta[i] = xn[i] - xs[i];
+        u[i] = ys[i] - xs[i];
+        un[i] = yn[i] - xn[i];
+      }
+      double omega = lin_omega(influence, xs, xn, horizon);
+      double dot = zeta[0] * (un[0] - u[0]) + zeta[1] * (un[1] - u[1]) + zeta[2] * (un[2] - u[2]);
+      th += omega * (1.0 - dmg[b]) * dot * vol[j];
+    }
+    if (row[p + 1] > row[p]) th *= 3.0 / m[p];
+    theta[p] = th;
+  }
+}
+
+void pdo_force_linear_lps(int64_t n, const double* x, const double* y, const double* m, const double* vol,
+                          const double* theta, const double* dmg, const int64_t* row, const int32_t* col,
+                          const double* K, const double* mu, int influence, double horizon, double* f) {
+  memset(f, 0, sizeof(double) * 3 * (size_t)n);
+  for (int64_t p = 0; p < n; ++p) {
+    const double* xs = &x[3 * p];
+    const double* ys = &y[3 * p];
+    for (int64_t b = row[p]; b < row[p + 1]; ++b) {
+      int64_t j = col[b];
+      const double* xn = &x[3 * j];
+      const double* yn = &y[3 * j];
+      double zeta[3], u[3], un[3], mv[3];
+      for (int i = 0; i < 3; ++i) {
+        zeta[i] = xn[i] - xs[i];
+        u[i] = ys[i] - xs[i];
+        un[i] = yn[i] - xn[i];
+      }
+      double z2 = zeta[0] * zeta[0] + zeta[1] * zeta[1] + zeta[2] * zeta[2];
+      double omega = lin_omega(influence, xs, xn, horizon);
+      double t1 = (9.0 * K[p] - 15.0 * mu[p]) * omega * (theta[p]) / (3.0 * (m[p]));
+      double t2 = 15.0 * mu[p] * omega / ((m[p]) * z2);
+      for (int i = 0; i < 3; ++i)
+        mv[i] = (zeta[i] * zeta[0]) * (un[0] - u[0]) + (zeta[i] * zeta[1]) * (un[1] - u[1]) +
+                (zeta[i] * zeta[2]) * (un[2] - u[2]);
+      double fx = (1.0 - dmg[b]) * (t1 * zeta[0] + t2 * mv[0]);
+      double fy = (1.0 - dmg[b]) * (t1 * zeta[1] + t2 * mv[1]);
+      double fz = (1.0 - dmg[b]) * (t1 * zeta[2] + t2 * mv[2]);
+      f[3 * p + 0] += fx * vol[j];
+      f[3 * p + 1] += fy * vol[j];
+      f[3 * p + 2] += fz * vol[j];
+      f[3 * j + 0] -= fx * vol[p];
+      f[3 * j + 1] -= fy * vol[p];
+      f[3 * j + 2] -= fz * vol[p];
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------
  * Stable time step: PeridigmNS::ComputeCriticalTimeStep
  * (src/core/Peridigm_CriticalTimeStep.cpp:52-130), constant horizon, owner K.
  * ------------------------------------------------------------------------- */

@@ -57,6 +57,12 @@ void pdo_dilatation(int64_t n, const double* x, const double* y, const double* m
 void pdo_force_bond_based(int64_t n, const double* x, const double* y, const double* vol,
                           const double* dmg, const int64_t* row, const int32_t* col, const double* K,
                           double horizon, int plane, double height, double* f);
+void pdo_dilatation_linear_lps(int64_t n, const double* x, const double* y, const double* m, const double* vol,
+                               const double* dmg, const int64_t* row, const int32_t* col, int influence,
+                               double horizon, double* theta);
+void pdo_force_linear_lps(int64_t n, const double* x, const double* y, const double* m, const double* vol,
+                          const double* theta, const double* dmg, const int64_t* row, const int32_t* col,
+                          const double* K, const double* mu, int influence, double horizon, double* f);
 void pdo_force_lps(int64_t n, const double* x, const double* y, const double* m,
                    const double* vol, const double* theta, const double* dmg, const int64_t* row,
                    const int32_t* col, const double* K, const double* mu, int influence,

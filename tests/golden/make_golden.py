@@ -388,7 +388,41 @@ def compression_implicit():
     np.savez_compressed(os.path.join(OUT, "compression_implicit.npz"), **out)
 
 
+def linear_lps_bar():
+    """LinearLPSBar (test/verification/LinearLPSBar): two separate bars of 500
+    points, blocks 1-3 Linear LPS Partial Volume and blocks 4-6 Elastic Partial
+    Volume (LPS), K 160e10, mu 79.3e10, horizon 0.1502, every dof prescribed
+    (u_x = 0.1 x t, u_y = u_z = 0), five quasi-static load steps to t = 1.
+    Stores the points, volumes, blocks, the gold displacement (x only; y and
+    z are zero), Force, Dilatation, Weighted_Volume and the reaction sums."""
+    d = os.path.join(REF, "test/verification/LinearLPSBar")
+    nc = netcdf_file(os.path.join(d, "LinearLPSBar_gold.e"), "r", mmap=False)
+    x = np.stack([nc.variables["coord" + a][:] for a in "xyz"], 1).astype(np.float64)
+    n = x.shape[0]
+    nv, ev, gv = _names(nc, "name_nod_var"), _names(nc, "name_elem_var"), _names(nc, "name_glo_var")
+    vol, wv = np.zeros(n), np.zeros(n)
+    block = np.full(n, -1, np.int32)
+    nt = nc.variables["time_whole"].shape[0]
+    th = np.zeros((nt, n))
+    for b in range(nc.dimensions["num_el_blk"]):
+        pts = np.array(nc.variables["connect%d" % (b + 1)][:, 0], np.int64) - 1
+        block[pts] = b
+        vol[pts] = nc.variables["vals_elem_var%deb%d" % (ev.index("Volume") + 1, b + 1)][0]
+        wv[pts] = nc.variables["vals_elem_var%deb%d" % (ev.index("Weighted_Volume") + 1, b + 1)][0]
+        th[:, pts] = nc.variables["vals_elem_var%deb%d" % (ev.index("Dilatation") + 1, b + 1)][:]
+    var = lambda nm: np.array(nc.variables["vals_nod_var%d" % (nv.index(nm) + 1)][:], np.float64)
+    for c in "YZ":
+        assert not var("Displacement" + c).any()
+    out = dict(x=x, vol=vol, block=block, weighted_volume=wv, dilatation=th,
+               time=np.array(nc.variables["time_whole"][:], np.float64), displacement_x=var("DisplacementX"),
+               force=np.stack([var("Force" + c) for c in "XYZ"], 2),
+               globals=np.array(nc.variables["vals_glo_var"][:], np.float64), global_names=np.array(gv))
+    nc.close()
+    np.savez_compressed(os.path.join(OUT, "linear_lps_bar.npz"), **out)
+
+
 def main():
+    linear_lps_bar()
     compression_implicit()
     contact_perforation()
     elastic_bond_based()
