@@ -151,6 +151,16 @@ int pd_material_lps_field(pd_ctx* ctx, const double* bulk_modulus, const double*
 #define PD_MATERIAL_LPS 0
 #define PD_MATERIAL_BOND_BASED 1
 int pd_material_bond_based(pd_ctx* ctx, int32_t block, double K, double rho, int32_t plane, double height);
+/* Linear LPS material of a block ("Linear LPS Partial Volume" with partial
+ * volumes and improved quadrature off, PeridigmNS::LinearLPSPVMaterial,
+ * src/materials/Peridigm_LinearLPSPVMaterial.cpp:62-394): the LPS model
+ * linearised about the reference configuration,
+ * theta = 3/m sum omega (1-d) zeta.(u_j - u_i) V_j and per bond
+ * (1-d) ((9K - 15mu) omega theta/(3m) zeta + 15mu omega/(m |zeta|^2) zeta zeta^T (u_j - u_i)).
+ * Evaluated on the FP64 path (contexts created with PD_FP64); the quasi-static
+ * and implicit solves support the LPS model only. */
+#define PD_MATERIAL_LINEAR_LPS 2
+int pd_material_linear_lps(pd_ctx* ctx, int32_t block, double K, double mu, double rho);
 /* "Critical Stretch" damage (CriticalStretchDamageModel ctor, src/damage/Peridigm_CriticalStretchDamageModel.cpp:52-77)
  * for one block; s_c < 0 disables damage on that block. */
 int pd_damage_critical_stretch(pd_ctx* ctx, int32_t block, double critical_stretch);

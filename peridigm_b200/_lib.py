@@ -98,6 +98,7 @@ SIGNATURES = {
     "pd_material_lps": (C.c_int, [_vp, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "pd_material_lps_field": (C.c_int, [_vp, _dp, _dp]),
     "pd_material_bond_based": (C.c_int, [_vp, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_double]),
+    "pd_material_linear_lps": (C.c_int, [_vp, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "pd_damage_critical_stretch": (C.c_int, [_vp, C.c_int32, C.c_double]),
     "pd_damage_critical_stretch_field": (C.c_int, [_vp, _dp]),
     "pd_weighted_volume": (C.c_int, [_vp, _dp]),

@@ -139,6 +139,10 @@ class Context:
         self._ok(self.L.pd_material_bond_based(self.h, int(block), float(K), float(rho), 1 if plane else 0,
                                                float(height)))
 
+    def material_linear_lps(self, K, mu, rho, block=0):
+        """Linear LPS material ("Linear LPS Partial Volume" without partial volumes); FP64 contexts only."""
+        self._ok(self.L.pd_material_linear_lps(self.h, int(block), float(K), float(mu), float(rho)))
+
     def material_field(self, K, mu):
         K, mu = _f64(K, self.n, "K"), _f64(mu, self.n, "mu")
         self._ok(self.L.pd_material_lps_field(self.h, _d(K), _d(mu)))

@@ -103,7 +103,7 @@ int ensure_ready(pd_ctx* c) {
   TRY(ensure_device(c));
   if (c->n == 0 || !c->row.p) return fail(c, PD_ERR_STATE, "points and bonds must be set first");
   if (!c->have_material)
-    return fail(c, PD_ERR_STATE, "no material: call pd_material_lps or pd_material_bond_based first");
+    return fail(c, PD_ERR_STATE, "no material: call pd_material_lps, pd_material_linear_lps or pd_material_bond_based first");
   {
     int model = -1;
     for (int m : c->block_model) {
@@ -117,6 +117,9 @@ int ensure_ready(pd_ctx* c) {
       c->wv_done = false;
     }
   }
+  if (c->material_model == PD_MATERIAL_LINEAR_LPS && c->precision != PD_FP64)
+    return fail(c, PD_ERR_UNSUPPORTED, "the Linear LPS material is evaluated in FP64 precision (create the context "
+                                       "with PD_FP64)");
   if (!c->symmetric)
     return fail(c, PD_ERR_UNSUPPORTED,
                 "bond families are not symmetric (j in H(i) without i in H(j)); the gather force pass needs "
@@ -407,6 +410,21 @@ int pd_material_bond_based(pd_ctx* c, int32_t block, double K, double rho, int32
   c->block_model[block] = PD_MATERIAL_BOND_BASED;
   c->bb_plane = plane != 0;
   c->bb_height = plane != 0 ? height : 0.0;
+  c->have_material = true;
+  c->wv_done = false;
+  coarse_release(c);
+  return PD_OK;
+}
+
+int pd_material_linear_lps(pd_ctx* c, int32_t block, double K, double mu, double rho) {
+  CHECK_CTX(c);
+  if (block < 0 || block >= (int32_t)c->block_K.size()) return fail(c, PD_ERR_ARG, "pd_material_linear_lps: bad block");
+  if (!(K > 0.0) || !(mu > 0.0) || !(rho > 0.0))
+    return fail(c, PD_ERR_ARG, "pd_material_linear_lps: moduli and density must be positive");
+  c->block_K[block] = K;
+  c->block_mu[block] = mu;
+  c->block_rho[block] = rho;
+  c->block_model[block] = PD_MATERIAL_LINEAR_LPS;
   c->have_material = true;
   c->wv_done = false;
   coarse_release(c);

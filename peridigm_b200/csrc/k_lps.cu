@@ -629,6 +629,134 @@ __global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t*
 }
 
 // ---------------------------------------------------------------------------
+// Linear LPS ("Linear LPS Partial Volume" without partial volumes or improved
+// quadrature): the loops PeridigmNS::LinearLPSPVMaterial::precompute and
+// ::computeForce run (src/materials/Peridigm_LinearLPSPVMaterial.cpp:231-394),
+// FP64, each term in the class's operation order:
+//   theta_i = (sum omega (1-d) zeta.(u_j - u_i) V_j) * (3/m_i)          (:283-290)
+//   t1 = (9K - 15mu) omega theta_i / (3 m_i), t2 = 15mu omega / (m_i |zeta|^2)
+//   f_ij = (1-d) (t1 zeta + t2 (zeta zeta^T)(u_j - u_i))                (:351-362)
+//   f_i += f_ij V_j, and from j's loop f_i -= f_ji V_j (:363-385), which in
+//   the gather form is + (t1_j zeta + t2_j (zeta zeta^T)(u_j - u_i)) V_j
+//   (zeta and u_j - u_i are exactly negated in j's frame).
+// The critical-stretch damage test runs first, on the actual stretch.
+// ab64[i] = (theta, 9K - 15mu, 15mu, m).
+// ---------------------------------------------------------------------------
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_dilatation_lin_fp64(
+    int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+    const double4* __restrict__ xv, const double4* __restrict__ st, const double4* __restrict__ pt,
+    const double* __restrict__ sc, const double* __restrict__ hp, int influence, int damage_on,
+    double4* __restrict__ ab64, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double th = 0.0;
+  int broken = 0;
+  int64_t b0 = 0, b1 = 0;
+  if (valid) {
+    b0 = row[i];
+    b1 = row[i + 1];
+    const double4 xi = xv[i];
+    const double4 yi = st[i];
+    const double s_c = damage_on ? sc[i] : -1.0;
+    const double h = hp[i];
+    const double ui0 = __dsub_rn(yi.x, xi.x), ui1 = __dsub_rn(yi.y, xi.y), ui2 = __dsub_rn(yi.z, xi.z);
+    for (int64_t b = b0 + lane; b < b1; b += TPO) {
+      if (dmg[b]) {
+        broken++;
+        continue;
+      }
+      const int32_t j = col[b];
+      const double4 xj = xv[j];
+      const double4 yj = st[j];
+      const double z0 = __dsub_rn(xj.x, xi.x), z1 = __dsub_rn(xj.y, xi.y), z2 = __dsub_rn(xj.z, xi.z);
+      const double zeta = __dsqrt_rn(sq3_rn(z0, z1, z2));
+      if (s_c >= 0.0) {
+        const double dY = __dsqrt_rn(sq3_rn(__dsub_rn(yj.x, yi.x), __dsub_rn(yj.y, yi.y), __dsub_rn(yj.z, yi.z)));
+        if (__ddiv_rn(__dsub_rn(dY, zeta), zeta) > s_c) {
+          dmg[b] = 1;
+          broken++;
+          continue;
+        }
+      }
+      const double d0 = __dsub_rn(__dsub_rn(yj.x, xj.x), ui0), d1 = __dsub_rn(__dsub_rn(yj.y, xj.y), ui1),
+                   d2 = __dsub_rn(__dsub_rn(yj.z, xj.z), ui2);
+      const double dot = __dadd_rn(__dadd_rn(__dmul_rn(z0, d0), __dmul_rn(z1, d1)), __dmul_rn(z2, d2));
+      const double om = omega_d(influence, zeta, h);
+      th = __dadd_rn(th, __dmul_rn(__dmul_rn(om, dot), xj.w));  // omega*(1-d)*dot*V with d = 0
+    }
+  }
+  th = group_sum<TPO>(th);
+  broken = group_sum<TPO>(broken);
+  if (valid && lane == 0) {
+    const double4 p = pt[i];
+    if (b1 > b0) th = __dmul_rn(th, __ddiv_rn(3.0, p.x));
+    ab64[i] = make_double4(th, __dsub_rn(__dmul_rn(9.0, p.y), __dmul_rn(15.0, p.z)), __dmul_rn(15.0, p.z), p.x);
+    theta_out[i] = th;
+    node_damage[i] = (b1 > b0) ? (double)broken / (double)(b1 - b0) : 0.0;
+  }
+}
+
+template <int TPO>
+__global__ void __launch_bounds__(kBlock) k_force_lin_fp64(int64_t n, const int64_t* __restrict__ row,
+                                                           const int32_t* __restrict__ col,
+                                                           const uint8_t* __restrict__ dmg,
+                                                           const double4* __restrict__ xv,
+                                                           const double4* __restrict__ st,
+                                                           const double4* __restrict__ ab64,
+                                                           const double4* __restrict__ pt,
+                                                           const double* __restrict__ hp, int influence,
+                                                           EpiArgs E) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / TPO;
+  const int lane = threadIdx.x & (TPO - 1);
+  const bool valid = i < n;
+  double f[3] = {0.0, 0.0, 0.0};
+  double4 xi = make_double4(0, 0, 0, 0);
+  if (valid) {
+    xi = xv[i];
+    const double4 yi = st[i];
+    const double4 ai = ab64[i];  // (theta, 9K - 15mu, 15mu, m)
+    const double hi = hp[i];
+    const double ui0 = __dsub_rn(yi.x, xi.x), ui1 = __dsub_rn(yi.y, xi.y), ui2 = __dsub_rn(yi.z, xi.z);
+    const int64_t b1 = row[i + 1];
+    for (int64_t b = row[i] + lane; b < b1; b += TPO) {
+      if (dmg[b]) continue;
+      const int32_t j = col[b];
+      const double4 xj = xv[j];
+      const double4 yj = st[j];
+      const double4 aj = ab64[j];
+      const double z[3] = {__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z)};
+      const double du[3] = {__dsub_rn(__dsub_rn(yj.x, xj.x), ui0), __dsub_rn(__dsub_rn(yj.y, xj.y), ui1),
+                            __dsub_rn(__dsub_rn(yj.z, xj.z), ui2)};
+      const double z2 = sq3_rn(z[0], z[1], z[2]);
+      const double zeta = __dsqrt_rn(z2);
+      const double om_i = omega_d(influence, zeta, hi);
+      const double om_j = influence == PD_INFLUENCE_ONE ? 1.0 : omega_d(influence, zeta, hp[j]);
+      const double t1i = __ddiv_rn(__dmul_rn(__dmul_rn(ai.y, om_i), ai.x), __dmul_rn(3.0, ai.w));
+      const double t2i = __ddiv_rn(__dmul_rn(ai.z, om_i), __dmul_rn(ai.w, z2));
+      const double t1j = __ddiv_rn(__dmul_rn(__dmul_rn(aj.y, om_j), aj.x), __dmul_rn(3.0, aj.w));
+      const double t2j = __ddiv_rn(__dmul_rn(aj.z, om_j), __dmul_rn(aj.w, z2));
+      const double V = xj.w;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const double mv = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(z[r], z[0]), du[0]), __dmul_rn(__dmul_rn(z[r], z[1]), du[1])),
+                                    __dmul_rn(__dmul_rn(z[r], z[2]), du[2]));
+        f[r] = __dadd_rn(f[r], __dmul_rn(__dadd_rn(__dmul_rn(t1i, z[r]), __dmul_rn(t2i, mv)), V));
+        f[r] = __dadd_rn(f[r], __dmul_rn(__dadd_rn(__dmul_rn(t1j, z[r]), __dmul_rn(t2j, mv)), V));
+      }
+    }
+  }
+  const double fx = group_sum<TPO>(f[0]), fy = group_sum<TPO>(f[1]), fz = group_sum<TPO>(f[2]);
+  if (valid && lane < 3) {
+    const double fc = lane == 0 ? fx : (lane == 1 ? fy : fz);
+    verlet_epilogue(E, i, lane, fc, comp3(xi, lane), pt[i].w);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Elastic bond-based material (MATERIAL_EVALUATION::computeInternalForceElasticBondBased,
 // src/materials/elastic_bond_based.cxx:55-124): one bond pass per evaluation,
 // the bond's critical-stretch damage first (CriticalStretchDamageModel order),
@@ -1062,6 +1190,9 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   } else if (split) {
     PD_DISPATCH_TPO_CSR(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
                         c->own.p, sp.damage_on, c->theta.p, c->node_damage.p, nullptr, nullptr);
+  } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
+    PD_DISPATCH_TPO(tpo, k_dilatation_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p,
+                    c->pt.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
   } else {
     PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
                     c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
@@ -1075,6 +1206,9 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   } else if (split) {
     PD_DISPATCH_TPO_CSR(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
                         nullptr);
+  } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
+    PD_DISPATCH_TPO(tpo, k_force_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
+                    c->pt.p, c->hp.p, c->influence, E);
   } else {
     PD_DISPATCH_TPO(tpo, k_force_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
                     c->pt.p, c->hp.p, c->influence, E);
