@@ -157,8 +157,11 @@ int pd_material_bond_based(pd_ctx* ctx, int32_t block, double K, double rho, int
  * linearised about the reference configuration,
  * theta = 3/m sum omega (1-d) zeta.(u_j - u_i) V_j and per bond
  * (1-d) ((9K - 15mu) omega theta/(3m) zeta + 15mu omega/(m |zeta|^2) zeta zeta^T (u_j - u_i)).
- * Evaluated on the FP64 path (contexts created with PD_FP64); the quasi-static
- * and implicit solves support the LPS model only. */
+ * FP64 contexts evaluate it in the class's operation order; split-FP32
+ * contexts at 4 lanes per point (the default) evaluate it from the sliced bond
+ * stream, with X in FP32 and the owner terms (9K - 15mu) theta/(3m) and 15mu/m
+ * of the LPS state record. The quasi-static and implicit solves support the
+ * LPS model only. */
 #define PD_MATERIAL_LINEAR_LPS 2
 int pd_material_linear_lps(pd_ctx* ctx, int32_t block, double K, double mu, double rho);
 /* "Critical Stretch" damage (CriticalStretchDamageModel ctor, src/damage/Peridigm_CriticalStretchDamageModel.cpp:52-77)

@@ -117,9 +117,9 @@ int ensure_ready(pd_ctx* c) {
       c->wv_done = false;
     }
   }
-  if (c->material_model == PD_MATERIAL_LINEAR_LPS && c->precision != PD_FP64)
-    return fail(c, PD_ERR_UNSUPPORTED, "the Linear LPS material is evaluated in FP64 precision (create the context "
-                                       "with PD_FP64)");
+  if (c->material_model == PD_MATERIAL_LINEAR_LPS && c->precision != PD_FP64 && c->tpo_split != 4)
+    return fail(c, PD_ERR_UNSUPPORTED, "the split-FP32 Linear LPS passes run at 4 lanes per point (the sliced bond "
+                                       "stream); use threads_per_point 0 or 4, or PD_FP64");
   if (!c->symmetric)
     return fail(c, PD_ERR_UNSUPPORTED,
                 "bond families are not symmetric (j in H(i) without i in H(j)); the gather force pass needs "

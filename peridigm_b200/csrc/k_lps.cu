@@ -89,7 +89,7 @@ __device__ __forceinline__ void split_hi_lo(double v, float* hi, float* lo) {
 // rounded from an exactly negated FP64 difference), so e and |X| are identical
 // and bond damage stays symmetric.
 struct SplitBond {
-  float Yx, Yy, Yz, zeta, ry, e;
+  float Yx, Yy, Yz, zeta, ry, e, xu, xx;  // xu = X.du, xx = |X|^2 (the linear LPS terms)
 };
 __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui, const Rec8& uj) {
   SplitBond s;
@@ -107,6 +107,8 @@ __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui,
   const float xu = fmaf(q.z, Uz, fmaf(q.y, Uy, q.x * Ux));
   const float uu = fmaf(Uz, Uz, fmaf(Uy, Uy, Ux * Ux));
   s.e = __fdividef(fmaf(2.0f, xu, uu), dY + s.zeta);  // |Y| - |X| without cancellation
+  s.xu = xu;
+  s.xx = xx;
   return s;
 }
 
@@ -276,7 +278,7 @@ __global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* _
 //   theta_i = 3/m_i * sum omega*(1-d)*|X|*e*V_j  (material_utilities.cxx:284)
 // Writes the owner terms A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m into ur[i].
 // ---------------------------------------------------------------------------
-template <int TPO, bool SELL>
+template <int TPO, bool SELL, bool LIN = false>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const float4* __restrict__ bx, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
@@ -338,7 +340,8 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
           if (SELL) cdm[TPO * k] = 1;  // the CSR copy stays canonical
         }
         broken += (dd[k] == 1 || brk) ? 1 : 0;
-        th = fmaf((intact && !brk) ? q.w * sb.zeta : 0.0f, sb.e, th);
+        // LPS: omega V_j |X| e; linear LPS: omega V_j X.du
+        th = fmaf((intact && !brk) ? (LIN ? q.w : q.w * sb.zeta) : 0.0f, LIN ? sb.xu : sb.e, th);
       }
     }
   }
@@ -499,7 +502,7 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
 //   f_i += (t_ij + t_ji) * V_j * Y/|Y|
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
-template <int TPO, bool SELL>
+template <int TPO, bool SELL, bool LIN = false>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
                                                                       const int32_t* __restrict__ col,
                                                                       const uint8_t* __restrict__ dmg,
@@ -549,11 +552,20 @@ __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n,
       for (int k = 0; k < kUnroll; ++k) {
         const float4 q = qq[k];
         const SplitBond sb = split_bond(q, ui, uu[k]);
-        const float T = fmaf(sb.zeta, ui.v[6] + uu[k].v[6], sb.e * (ui.v[7] + uu[k].v[7]));
-        const float w = live[k] ? T * q.w * sb.ry : 0.0f;
-        fx = fmaf(w, sb.Yx, fx);
-        fy = fmaf(w, sb.Yy, fy);
-        fz = fmaf(w, sb.Yz, fz);
+        if constexpr (LIN) {
+          // omega V_j ((A_i + A_j) X + (B_i + B_j) (X.du / |X|^2) X), along the reference bond X
+          const float c = fmaf(ui.v[7] + uu[k].v[7], __fdividef(sb.xu, sb.xx), ui.v[6] + uu[k].v[6]);
+          const float w = live[k] ? c * q.w : 0.0f;
+          fx = fmaf(w, q.x, fx);
+          fy = fmaf(w, q.y, fy);
+          fz = fmaf(w, q.z, fz);
+        } else {
+          const float T = fmaf(sb.zeta, ui.v[6] + uu[k].v[6], sb.e * (ui.v[7] + uu[k].v[7]));
+          const float w = live[k] ? T * q.w * sb.ry : 0.0f;
+          fx = fmaf(w, sb.Yx, fx);
+          fy = fmaf(w, sb.Yy, fy);
+          fz = fmaf(w, sb.Yz, fz);
+        }
       }
     }
   }
@@ -1184,7 +1196,8 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
     return cudaGetLastError();
   }
   if (sell) {
-    k_dilatation_split<4, true><<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p,
+    (c->material_model == PD_MATERIAL_LINEAR_LPS ? k_dilatation_split<4, true, true> : k_dilatation_split<4, true>)
+        <<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p,
                                                                 c->ur[c->cur].p, c->own.p, sp.damage_on, c->theta.p,
                                                                 c->node_damage.p, soff, dmg);
   } else if (split) {
@@ -1201,8 +1214,8 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], c->stream);
   if (sell) {
-    k_force_split<4, true><<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p,
-                                                           c->pt.p, E, soff);
+    (c->material_model == PD_MATERIAL_LINEAR_LPS ? k_force_split<4, true, true> : k_force_split<4, true>)
+        <<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E, soff);
   } else if (split) {
     PD_DISPATCH_TPO_CSR(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
                         nullptr);

@@ -28,6 +28,9 @@ def _run(w, precision, steps, tpo, blocks, material="lps"):
         if material == "bond_based":  # same bulk modulus and density, elastic bond-based model
             for b in range(int(np.max(w["block"])) + 1 if blocks else 1):
                 ctx.material_bond_based(float(np.median(w["K"])), w["rho"], block=b)
+        if material == "linear_lps":  # same moduli and density, the LPS model linearised
+            for b in range(int(np.max(w["block"])) + 1 if blocks else 1):
+                ctx.material_linear_lps(float(np.median(w["K"])), float(np.median(w["mu"])), w["rho"], block=b)
         dt = w.get("safety", 0.7) * ctx.critical_time_step()
         st = ctx.verlet_run(dt, steps)
         nb = ctx.num_bonds()
@@ -48,7 +51,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--tpo", type=int, default=0)
     ap.add_argument("--compare", action="store_true")
-    ap.add_argument("--material", default="lps", choices=["lps", "bond_based"])
+    ap.add_argument("--material", default="lps", choices=["lps", "bond_based", "linear_lps"])
     a = ap.parse_args()
     blocks = False
     if a.workload == "large_plate":

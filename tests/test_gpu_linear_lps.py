@@ -1,4 +1,4 @@
-"""Linear LPS material on the GPU (pd_material_linear_lps, FP64 path).
+"""Linear LPS material on the GPU (pd_material_linear_lps).
 
 * The reference's LinearLPSBar gold output: bar 1 (Linear LPS Partial Volume)
   and, in the same deck, bar 2 (Elastic Partial Volume = LPS) under
@@ -10,7 +10,9 @@
   dilatation 1e-12 and force 1e-11 relative L2.
 * Five velocity-Verlet steps against the same loop driven by the oracle's
   force: displacement and velocity 1e-10 relative.
-* The split-FP32 precision refuses the material (PD_ERR_UNSUPPORTED)."""
+* The split-FP32 path (sliced stream, 4 lanes per point) against the same
+  gold and the oracle at the split path's tolerances; other lane counts are
+  refused (PD_ERR_UNSUPPORTED)."""
 import os
 
 import numpy as np
@@ -113,9 +115,64 @@ def test_linear_lps_verlet_matches_oracle_loop():
     assert rel_l2(v_g, v) <= 1e-10
 
 
-def test_split_precision_refuses_linear_lps():
-    x, vol, y, h = _cloud()
+@pytest.mark.parametrize("bar", [0])
+def test_split_linear_lps_bar_gold(bar):
+    """Split-FP32 (sliced stream, 4 lanes per point): Force within 1e-6 of the
+    largest gold force, Dilatation 1e-6 of the largest, reaction sums 1e-6."""
+    z = np.load(os.path.join(G, "linear_lps_bar.npz"))
+    K, mu, h = 160.0e10, 79.3e10, 0.1502
+    pts = np.nonzero(np.isin(z["block"], (0, 1, 2)))[0]
+    x, vol, local = z["x"][pts], z["vol"][pts], z["block"][pts]
+    names = list(z["global_names"])
     with Context(precision="split") as ctx:
+        ctx.set_points(x.ravel(), vol, local)
+        ctx.set_horizons([h, h, h])
+        ctx.build_bonds()
+        for b in range(3):
+            ctx.material_linear_lps(K, mu, 8.05, block=b)
+        for s in range(1, len(z["time"])):
+            u = np.zeros_like(x)
+            u[:, 0] = z["displacement_x"][s][pts]
+            ctx.compute_force((x + u).ravel())
+            gF = z["force"][s][pts]
+            assert np.abs(ctx.field("Force").reshape(-1, 3) - gF).max() <= 1e-6 * np.abs(gF).max()
+            gth = z["dilatation"][s][pts]
+            assert np.abs(ctx.field("Dilatation") - gth).max() <= 1e-6 * np.abs(gth).max()
+            for side, b in (("Left", 0), ("Right", 2)):
+                g = z["globals"][s][names.index("%s_Reaction_Force_LLPSX" % side)]
+                assert abs(ctx.block_data("Force", b, "Sum")[0] - g) <= 1e-6 * abs(g)
+
+
+def test_split_linear_lps_matches_oracle():
+    """Split-FP32 against the oracle: bond-break sets identical except bonds
+    within 1e-6 s_c of s_c; dilatation and force 1e-6 relative L2."""
+    x, vol, y, h = _cloud()
+    K, mu, s_c = 130e9, 78e9, 2.5e-3
+    row, col = O.neighbor_search(x, h)
+    ref = O.eval_linear_lps(x, y, vol, row, col, K, mu, h, s_c=s_c)
+    n = len(vol)
+    owner = np.repeat(np.arange(n), np.diff(row))
+    P, Y = x.reshape(-1, 3), y.reshape(-1, 3)
+    zeta = np.linalg.norm(P[col] - P[owner], axis=1)
+    s = (np.linalg.norm(Y[col] - Y[owner], axis=1) - zeta) / zeta
+    near = np.abs(s - s_c) <= 1e-6 * s_c
+    with Context(precision="split") as ctx:
+        ctx.set_points(x, vol)
+        ctx.set_horizons([h])
+        ctx.build_bonds()
+        ctx.material_linear_lps(K, mu, 7800.0)
+        ctx.critical_stretch(s_c)
+        f = ctx.compute_force(y)
+        bd = ctx.field("Bond_Damage")
+        assert np.array_equal(bd[~near], ref["bond_damage"][~near])
+        if not near.any():
+            assert rel_l2(ctx.field("Dilatation"), ref["theta"]) <= 1e-6
+            assert rel_l2(f, ref["force"]) <= 1e-6
+
+
+def test_split_linear_lps_needs_four_lanes():
+    x, vol, y, h = _cloud()
+    with Context(precision="split", threads_per_point=8) as ctx:
         ctx.set_points(x, vol)
         ctx.set_horizons([h])
         ctx.build_bonds()
