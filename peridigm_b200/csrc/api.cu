@@ -162,14 +162,17 @@ int check_status(pd_ctx* c) {
 }
 
 // evalModel on the configuration already in st[cur]; trial damage on dmg_trial.
-int eval_trial(pd_ctx* c, double* f_dev) {
+// f_host (may be null): where the force density also goes on the host; *host_done
+// tells whether the evaluation copied it there.
+int eval_trial(pd_ctx* c, double* f_dev, double* f_host = nullptr, bool* host_done = nullptr) {
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
   note_damage_copy(c, c->dmg_trial.p, c->dmg.p);
   StepParams sp{};
   sp.mode = EVAL_ONLY;
   sp.damage_on = c->any_damage ? 1 : 0;
   sp.f_out = f_dev;
-  PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg_trial.p));
+  sp.f_host = f_host;
+  PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg_trial.p, host_done));
   c->trial_valid = true;
   return check_status(c);
 }
@@ -234,6 +237,9 @@ int pd_destroy(pd_ctx* c) {
   coarse_release(c);
   for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
   if (c->vbeg) cudaEventDestroy(c->vbeg);
+  for (cudaEvent_t e : c->chunk_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   cudaStream_t s = c->stream;
   delete c;
   if (s) cudaStreamDestroy(s);
@@ -488,8 +494,9 @@ int pd_compute_force(pd_ctx* c, const double* y, double* f_out) {
   // y is staged through the force buffer, then f is written there
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->f.p, y, bytes, cudaMemcpyHostToDevice, c->stream));
   PD_CUDA_TRY(c, launch_state_from_y(c, c->f.p));
-  TRY(eval_trial(c, c->f.p));
-  if (f_out) {
+  bool copied = false;
+  TRY(eval_trial(c, c->f.p, f_out, &copied));
+  if (f_out && !copied) {
     PD_CUDA_TRY(c, cudaMemcpyAsync(f_out, c->f.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }

@@ -502,16 +502,19 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
 //   f_i += (t_ij + t_ji) * V_j * Y/|Y|
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
-template <int TPO, bool SELL, bool LIN = false>
+template <int TPO, bool SELL, bool LIN = false, bool CHUNK = false>
 __global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
                                                                       const int32_t* __restrict__ col,
                                                                       const uint8_t* __restrict__ dmg,
                                                                       const float4* __restrict__ bx,
                                                                       const Rec8* __restrict__ ur,
                                                                       const double4* __restrict__ pt, EpiArgs E,
-                                                                      const int64_t* __restrict__ soff) {
+                                                                      const int64_t* __restrict__ soff,
+                                                                      int64_t i0 = 0) {
+  // CHUNK: owners i0 .. n-1 (a chunk of the points starts at a multiple of 64
+  // owners); otherwise i0 is not used and the pass covers 0 .. n-1
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t i = g / TPO;
+  const int64_t i = (CHUNK ? i0 : 0) + g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
   const bool valid = i < n;
   float fx = 0.f, fy = 0.f, fz = 0.f;
@@ -1128,9 +1131,29 @@ cudaError_t launch_sync_state(pd_ctx* c) {
   return cudaGetLastError();
 }
 
+#define TRY_CUDA(expr)                 \
+  do {                                 \
+    const cudaError_t e_ = (expr);     \
+    if (e_ != cudaSuccess) return e_;  \
+  } while (0)
+
+// The stream and events of the chunked force download (created on first use).
+static cudaError_t ensure_copy_stream(pd_ctx* c) {
+  if (c->copy_stream) return cudaSuccess;
+  TRY_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  for (int k = 0; k <= kHostChunks; ++k) TRY_CUDA(cudaEventCreateWithFlags(&c->chunk_ev[k], cudaEventDisableTiming));
+  return cudaSuccess;
+}
+
 // One model evaluation (damage -> dilatation -> force [-> Verlet epilogue]) on
 // the gathered state of parity c->cur, with bond damage dmg updated in place.
-cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
+// With sp.f_host set, the split sliced force pass also copies the force
+// density to that host buffer, overlapped with its own later chunks, and sets
+// *host_done; other paths leave the copy to the caller.
+cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* host_done) {
+  bool unused = false;
+  if (!host_done) host_done = &unused;
+  *host_done = false;
   if (c->n == 0) return cudaSuccess;
   const bool split = c->precision == PD_SPLIT_FP32;
   const int tpo = split ? c->tpo_split : c->tpo;
@@ -1214,8 +1237,34 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg) {
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], c->stream);
   if (sell) {
-    (c->material_model == PD_MATERIAL_LINEAR_LPS ? k_force_split<4, true, true> : k_force_split<4, true>)
-        <<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E, soff);
+    const bool lin = c->material_model == PD_MATERIAL_LINEAR_LPS;
+    if (sp.f_host && sp.f_out) {
+      auto* kf = lin ? k_force_split<4, true, true, true> : k_force_split<4, true, false, true>;
+      // Force in chunks of points; each chunk's force density goes to the host
+      // on the copy stream while the next chunk computes.
+      TRY_CUDA(ensure_copy_stream(c));
+      const int64_t n = c->n, per = ((n + kHostChunks - 1) / kHostChunks + 63) / 64 * 64;
+      // (all chunks are launched before the first copy: a copy to pageable
+      // memory holds the host until it is done)
+      for (int64_t i0 = 0, k = 0; i0 < n; i0 += per, ++k) {
+        const int64_t i1 = std::min(n, i0 + per);
+        kf<<<grid_for(i1 - i0, 4), kBlock, 0, c->stream>>>(i1, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p,
+                                                           E, soff, i0);
+        TRY_CUDA(cudaEventRecord(c->chunk_ev[k], c->stream));
+      }
+      for (int64_t i0 = 0, k = 0; i0 < n; i0 += per, ++k) {
+        const int64_t i1 = std::min(n, i0 + per);
+        TRY_CUDA(cudaStreamWaitEvent(c->copy_stream, c->chunk_ev[k], 0));
+        TRY_CUDA(cudaMemcpyAsync(sp.f_host + 3 * i0, sp.f_out + 3 * i0, 3 * (i1 - i0) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->copy_stream));
+      }
+      TRY_CUDA(cudaEventRecord(c->chunk_ev[kHostChunks], c->copy_stream));
+      TRY_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[kHostChunks], 0));
+      *host_done = true;
+    } else {
+      auto* kf = lin ? k_force_split<4, true, true> : k_force_split<4, true>;
+      kf<<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E, soff, 0);
+    }
   } else if (split) {
     PD_DISPATCH_TPO_CSR(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
                         nullptr);

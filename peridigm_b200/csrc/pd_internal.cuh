@@ -30,6 +30,10 @@
 
 namespace pdb {
 
+// Chunks of the force pass whose force density pd_compute_force copies to the
+// host while the later chunks compute.
+constexpr int kHostChunks = 4;
+
 // One 32-byte record per point, fetched with a single 256-bit load.
 struct __align__(32) Rec8 {
   float v[8];
@@ -57,6 +61,7 @@ struct StepParams {
   int has_bc;
   // outputs
   double* f_out;    // force density [3n] (may be null)
+  double* f_host = nullptr;  // host copy of f_out, overlapped with the force pass where it can be
 };
 
 // EVAL_ONLY: evaluation (force out) with no integration; EVAL_ADVANCE: finish
@@ -110,6 +115,9 @@ struct pd_ctx {
   int tpo = 16;       // lanes per point (FP64 path and setup kernels)
   int tpo_split = 4;  // lanes per point of the split-FP32 bond passes
   cudaStream_t stream = nullptr;
+  // chunked force download of pd_compute_force (created on first use)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t chunk_ev[pdb::kHostChunks + 1] = {};
   std::string err;
 
   // points
@@ -212,7 +220,7 @@ namespace pdb {
 
 cudaError_t launch_weighted_volume(const pd_ctx* c);
 cudaError_t launch_pack_owner(pd_ctx* c);
-cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg);
+cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* host_done = nullptr);
 cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev);
 cudaError_t launch_sync_state(pd_ctx* c);
 cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out);

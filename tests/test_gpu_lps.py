@@ -153,7 +153,8 @@ def test_critical_time_step_matches_oracle():
 
 
 def test_device_pointer_entry():
-    """pd_compute_force_device on torch-owned device buffers equals the host entry."""
+    """pd_compute_force_device on torch-owned device buffers equals the host entry,
+    with pageable and with pinned host buffers (630 points: the last chunk is not a multiple of 64)."""
     torch = pytest.importorskip("torch")
     x, vol, y, h = make_cloud(seed=4)
     with Context(precision="split") as ctx:
@@ -167,6 +168,13 @@ def test_device_pointer_entry():
         torch.cuda.synchronize()
         ctx.compute_force_device(yd.data_ptr(), fd.data_ptr())
         assert np.array_equal(fd.cpu().numpy(), f_host)
+        # pinned host buffers (the force download overlaps the chunked force pass)
+        yp = torch.tensor(y, dtype=torch.float64).pin_memory()
+        fp = torch.zeros(len(y), dtype=torch.float64).pin_memory()
+        for _ in range(2):
+            ctx._ok(ctx.L.pd_compute_force(ctx.h, C.cast(yp.data_ptr(), C.POINTER(C.c_double)),
+                                           C.cast(fp.data_ptr(), C.POINTER(C.c_double))))
+            assert np.array_equal(fp.numpy(), f_host)
 
 
 def test_sliced_damage_mirror_follows_the_state_cycle():
