@@ -144,7 +144,7 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def qs_leg(local, load_steps):
+def qs_leg(local, load_steps, cpu_threads=0):
     """Quasi-static time to 1e-8: the 60^3 tensile cube (216,000 points, h = 1 mm,
     delta = 3.015h, K log-uniform in [50, 200] GPa from seed 1000, mu = 0.6K, x = 0
     face clamped, x = max face pulled to 1e-4 m) over `load_steps` equal load
@@ -153,7 +153,10 @@ def qs_leg(local, load_steps):
     (block Jacobi + exact Galerkin coarse correction on aggregate cells of two
     horizons) and learned (two-level + the learned middle level on 3 mm patches,
     trained here on two-level solves of a 12^3 cube over six random moduli and
-    load paths). Times are device time of the Newton loops (CUDA events)."""
+    load paths). Times are device time of the Newton loops (CUDA events).
+    With cpu_threads > 0 the block-Jacobi arm also gets a CPU baseline: the
+    same CG step restated in C (oracle/cpu_qs.c) on that many host threads,
+    timed on a sample and scaled by the solve's Newton and CG counts."""
     from peridigm_b200 import Context, workloads
 
     patch = 3.0e-3
@@ -205,9 +208,32 @@ def qs_leg(local, load_steps):
                             "newton_iterations": st.newton_iterations, "final_cg_residual": st.final_residual,
                             "fallbacks": st.preconditioner_fallbacks, "sm_mhz": clk["sm_mhz"],
                             "clock_reasons": clk["reasons"]}
+            if precond == "block_jacobi" and cpu_threads:
+                # CPU baseline: the same block-Jacobi CG step restated in C on the
+                # host threads, timed on a sample at the solved state and scaled
+                # by this solve's Newton and CG counts
+                from oracle import cpu_qs
+
+                row, col = ctx.bonds_csr()
+                y = w2["x"] + ctx.field("Displacement")
+                fixed = np.zeros(len(w2["vol"]), np.uint8)
+                for bc in w2["bcs"]:
+                    fixed[bc["points"]] |= np.uint8(1 << bc["coordinate"])
+                smp = cpu_qs.sample(w2["x"], y, w2["vol"], row, col, w2["K"], w2["mu"], w2["horizon"], fixed,
+                                    threads=cpu_threads, cg_iters=20)
+                est = st.newton_iterations * smp["seconds_per_newton_setup"] + \
+                    st.cg_iterations * smp["seconds_per_cg_iteration"]
+                out["cpu_baseline"] = dict(smp, seconds=est, kind="port",
+                                           sample="block-Jacobi CG restated in C (matrix-free LPS tangent, "
+                                                  "3x3 block inverses) on %d host threads: 20 CG iterations and one "
+                                                  "Newton set-up at the solved state, scaled by the GPU solve's %d "
+                                                  "Newton and %d CG iterations" % (cpu_threads, st.newton_iterations,
+                                                                                  st.cg_iterations))
     bj = out["block_jacobi"]["seconds"]
     out["two_level_speedup_over_block_jacobi"] = bj / out["two_level"]["seconds"]
     out["mpnn_speedup_over_block_jacobi"] = bj / out["mpnn"]["seconds"]
+    if "cpu_baseline" in out:
+        out["block_jacobi_speedup_over_cpu"] = out["cpu_baseline"]["seconds"] / bj
     return out
 
 
@@ -339,7 +365,7 @@ def main():
     # ---- quasi-static time to 1e-8 (rank 0 only) -----------------------------
     qs = None
     if rank == 0 and not args.no_qs:
-        qs = qs_leg(local, args.qs_load_steps)
+        qs = qs_leg(local, args.qs_load_steps, cpu_threads=0 if args.no_cpu_baseline else (os.cpu_count() or 1))
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
