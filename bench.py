@@ -144,16 +144,19 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def qs_leg(local, load_steps, cpu_threads=0):
+def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
     """Quasi-static time to 1e-8: the 60^3 tensile cube (216,000 points, h = 1 mm,
     delta = 3.015h, K log-uniform in [50, 200] GPa from seed 1000, mu = 0.6K, x = 0
     face clamped, x = max face pulled to 1e-4 m) over `load_steps` equal load
     steps; Newton to 1e-8 of each load increment's residual, CG to 1e-8 relative.
-    Three preconditioners: block Jacobi (the reference's "Block 3x3"), two-level
+    Four preconditioners: block Jacobi (the reference's "Block 3x3"), two-level
     (block Jacobi + exact Galerkin coarse correction on aggregate cells of two
-    horizons) and learned (two-level + the learned middle level on 3 mm patches,
-    trained here on two-level solves of a 12^3 cube over six random moduli and
-    load paths). Times are device time of the Newton loops (CUDA events).
+    horizons, translations), two-level rigid (the coarse space with the three
+    rotations per aggregate as well) and learned (the learned middle level on
+    3 mm patches over the two-level base with `learned_modes` coarse modes,
+    trained here on such two-level solves of a 12^3 cube over six random
+    moduli and load paths). Times are device time of the Newton loops (CUDA
+    events).
     With cpu_threads > 0 the block-Jacobi arm also gets a CPU baseline: the
     same CG step restated in C (oracle/cpu_qs.c) on that many host threads,
     timed on a sample and scaled by the solve's Newton and CG counts."""
@@ -164,6 +167,7 @@ def qs_leg(local, load_steps, cpu_threads=0):
     w = workloads.qs_cube(n=12, h=1.0e-3, seed=11, jitter=0.05, load_steps=4)
     with Context(device=local, precision="fp64") as tr:
         workloads.setup_context(tr, w)
+        tr.coarse_modes(learned_modes)
         tr.mpnn_init(seed=7, patch=patch)
         tr.mpnn_collect(4)
         rng = np.random.default_rng(5)
@@ -188,11 +192,15 @@ def qs_leg(local, load_steps, cpu_threads=0):
     w2 = workloads.qs_cube(n=60, h=1.0e-3, seed=1000, load_steps=load_steps)
     out = {"workload": f"qs_cube_60x60x60 (seed 1000, {load_steps} load steps)", "points": int(len(w2["vol"])),
            "tolerance": 1e-8, "training": {"pairs": pairs, "epochs": 40, "final_loss": loss, "seconds": train_s,
-                                           "patch_m": patch}}
-    for precond in ("block_jacobi", "two_level", "mpnn"):
+                                           "patch_m": patch, "coarse_modes": learned_modes}}
+    for arm in ("block_jacobi", "two_level", "two_level_rigid", "mpnn"):
+        precond = "two_level" if arm == "two_level_rigid" else arm
         with Context(device=local, precision="fp64") as ctx:
             workloads.setup_context(ctx, w2)
+            if arm == "two_level_rigid":
+                ctx.coarse_modes(6)
             if precond == "mpnn":
+                ctx.coarse_modes(learned_modes)
                 ctx.mpnn_init(seed=0, patch=patch)
                 ctx.mpnn_set_weights(weights)
             st = None
@@ -204,11 +212,11 @@ def qs_leg(local, load_steps, cpu_threads=0):
                                       cg_relative_tolerance=1e-8, preconditioner=precond, stats=st)
             wall = time.perf_counter() - t1
             clk = clocks.stop()
-            out[precond] = {"seconds": st.device_ms / 1e3, "wall_seconds": wall, "cg_iterations": st.cg_iterations,
+            out[arm] = {"seconds": st.device_ms / 1e3, "wall_seconds": wall, "cg_iterations": st.cg_iterations,
                             "newton_iterations": st.newton_iterations, "final_cg_residual": st.final_residual,
                             "fallbacks": st.preconditioner_fallbacks, "sm_mhz": clk["sm_mhz"],
                             "clock_reasons": clk["reasons"]}
-            if precond == "block_jacobi" and cpu_threads:
+            if arm == "block_jacobi" and cpu_threads:
                 # CPU baseline: the same block-Jacobi CG step restated in C on the
                 # host threads, timed on a sample at the solved state and scaled
                 # by this solve's Newton and CG counts
@@ -231,6 +239,7 @@ def qs_leg(local, load_steps, cpu_threads=0):
                                                                                   st.cg_iterations))
     bj = out["block_jacobi"]["seconds"]
     out["two_level_speedup_over_block_jacobi"] = bj / out["two_level"]["seconds"]
+    out["two_level_rigid_speedup_over_block_jacobi"] = bj / out["two_level_rigid"]["seconds"]
     out["mpnn_speedup_over_block_jacobi"] = bj / out["mpnn"]["seconds"]
     if "cpu_baseline" in out:
         out["block_jacobi_speedup_over_cpu"] = out["cpu_baseline"]["seconds"] / bj

@@ -387,10 +387,21 @@ int pd_mpnn_loss_grad(pd_ctx* ctx, const float* pair, double* loss, float* grad)
  * aggregate cells of side max(cell, 2 * max horizon) (the default after
  * pd_mpnn_init, cell 0); cell < 0 puts it on block Jacobi alone. */
 int pd_mpnn_coarse(pd_ctx* ctx, double cell);
+/* Coarse dofs per aggregate of the two-level preconditioner (no counterpart
+ * in the reference): 3 (the default) = translations; 6 = translations and the
+ * three rotations about the aggregate's center, orthonormalised per aggregate
+ * (Gram-matrix Cholesky; near-dependent modes dropped), the Galerkin matrix
+ * assembled from 162 matrix-free tangent products per build (aggregates
+ * colored by cell coordinates mod 3). At most 6144 coarse dofs either way:
+ * with 6 modes the cells grow to hold at most 1024 aggregates. Applies to
+ * every coarse level of the context (two-level, and the learned
+ * preconditioner's base). */
+int pd_qs_coarse_modes(pd_ctx* ctx, int32_t modes);
 /* The coarse space of PD_PRECOND_TWO_LEVEL at displacement u (host [3n]):
- * n_coarse receives 3 x the number of aggregates; aggregate[n] the aggregate
- * of each point, A the assembled P0^T K P0 and A_inv its inverse (row-major
- * n_coarse^2, coarse dof 3I + c = component c of aggregate I). Call first with
+ * n_coarse receives 3 (6 with pd_qs_coarse_modes(ctx, 6)) x the number of
+ * aggregates; aggregate[n] the aggregate of each point, A the assembled
+ * P0^T K P0 and A_inv its inverse (row-major n_coarse^2, coarse dof 3I + c =
+ * component c of aggregate I; with 6 modes, 6I + k = orthonormal mode k). Call first with
  * aggregate, A and A_inv NULL to get n_coarse; on the second call *n_coarse
  * must hold at least that. */
 int pd_qs_coarse_operator(pd_ctx* ctx, const double* u, double cell, int64_t* n_coarse, int32_t* aggregate,

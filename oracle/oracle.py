@@ -427,12 +427,12 @@ def implicit_newmark(x, vol, row, col, K, mu, rho, horizon, u0, v0, dt, nsteps, 
     return out
 
 
-def coarse_aggregates(x, horizon_max, cell=0.0, max_coarse=6144):
+def coarse_aggregates(x, horizon_max, cell=0.0, max_coarse=6144, modes=3):
     """Aggregates of the two-level preconditioner (no reference counterpart):
     the non-empty cells, numbered in cell order (x fastest), of a grid of side
     max(cell, 2 * max horizon * (1 + 1e-6)) from the coordinate minimum, dims =
     floor(extent / side) + 1 per axis, the side grown 1.25x until there are at
-    most max_coarse / 3 aggregates. Returns (aggregate of each point, side)."""
+    most max_coarse / modes aggregates. Returns (aggregate of each point, side)."""
     x = _f64(x).reshape(-1, 3)
     lo, hi = x.min(axis=0), x.max(axis=0)
     side = max(float(cell), 2.0 * float(horizon_max) * (1.0 + 1.0e-6))
@@ -444,7 +444,7 @@ def coarse_aggregates(x, horizon_max, cell=0.0, max_coarse=6144):
         c = np.clip(np.floor((x - lo) / side).astype(np.int64), 0, dims - 1)
         cid = (c[:, 2] * dims[1] + c[:, 1]) * dims[0] + c[:, 0]
         cells = np.unique(cid)
-        if 3 * cells.size <= max_coarse:
+        if modes * cells.size <= max_coarse:
             return np.searchsorted(cells, cid).astype(np.int32), side
         side *= 1.25
 
@@ -464,6 +464,45 @@ def coarse_operator(T, agg, fixed_dofs=()):
     P[list(fixed_dofs), :] = 0.0
     A = P.T @ T @ P
     for k in range(nc):
+        if A[k, k] == 0.0:
+            A[k, k] = 1.0
+    return A, P
+
+
+def coarse_operator_rigid(T, x, agg, side, fixed_dofs=()):
+    """Galerkin coarse matrix of the rigid coarse space (6 modes per aggregate,
+    no reference counterpart): per aggregate the translations and the
+    rotations about its center (mean of its points), scaled by 1/side,
+    prescribed dofs masked, orthonormalised by QR with the columns whose
+    |R_kk| falls below 1e-4 of the largest dropped (1e-8 of the Gram
+    pivots, as the GPU's Cholesky does); dropped coarse dofs get a unit
+    diagonal. The basis differs from the GPU's by an orthogonal 6x6 map per
+    aggregate, so compare basis-free quantities. Returns (Ac, P)."""
+    x = _f64(x).reshape(-1, 3)
+    agg = np.asarray(agg, np.int64)
+    n = agg.size
+    na = int(agg.max()) + 1
+    P = np.zeros((3 * n, 6 * na))
+    fixed = np.zeros(3 * n, bool)
+    fixed[list(fixed_dofs)] = True
+    for a in range(na):
+        pts = np.nonzero(agg == a)[0]
+        c = x[pts].mean(axis=0)
+        d = (x[pts] - c) / side
+        B = np.zeros((3 * pts.size, 6))
+        for k in range(3):
+            B[k::3, k] = 1.0
+        B[0::3, 3], B[1::3, 3] = -d[:, 1], d[:, 0]
+        B[1::3, 4], B[2::3, 4] = -d[:, 2], d[:, 1]
+        B[2::3, 5], B[0::3, 5] = -d[:, 0], d[:, 2]
+        rows = (3 * pts[:, None] + np.arange(3)).ravel()
+        B[fixed[rows]] = 0.0
+        Q, Rm = np.linalg.qr(B)
+        dg = np.abs(np.diag(Rm))
+        keep = dg > 1e-4 * dg.max() if dg.max() > 0 else np.zeros(6, bool)
+        P[np.ix_(rows, 6 * a + np.nonzero(keep)[0])] = Q[:, keep]
+    A = P.T @ T @ P
+    for k in range(6 * na):
         if A[k, k] == 0.0:
             A[k, k] = 1.0
     return A, P

@@ -122,6 +122,7 @@ SIGNATURES = {
     "pd_contact_short_range": (C.c_int, [_vp, C.c_double, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "pd_contact_force": (C.c_int, [_vp, _dp, _dp, _dp]),
     "pd_qs_load_step": (C.c_int, [_vp, C.c_double, C.c_double, C.c_void_p, C.POINTER(Stats)]),
+    "pd_qs_coarse_modes": (C.c_int, [_vp, C.c_int32]),
     "pd_implicit_run": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int64, C.c_void_p, C.POINTER(Stats)]),
     "pd_jacobian_apply": (C.c_int, [_vp, _dp, _dp, _dp]),
     "pd_jacobian_block_diagonal": (C.c_int, [_vp, _dp, _dp]),

@@ -280,6 +280,10 @@ class Context:
                                         C.byref(st)))
         return st
 
+    def coarse_modes(self, modes):
+        """Coarse dofs per aggregate of the two-level preconditioner: 3 (translations) or 6 (with rotations)."""
+        self._ok(self.L.pd_qs_coarse_modes(self.h, int(modes)))
+
     def jacobian_apply(self, u, w):
         u, w = _f64(u, 3 * self.n, "u"), _f64(w, 3 * self.n, "w")
         kw = np.zeros(3 * self.n)

@@ -823,6 +823,16 @@ int pd_mpnn_coarse(pd_ctx* c, double cell) {
   return mpnn_set_coarse(c, cell);
 }
 
+int pd_qs_coarse_modes(pd_ctx* c, int32_t modes) {
+  CHECK_CTX(c);
+  if (modes != 3 && modes != 6) return fail(c, PD_ERR_ARG, "pd_qs_coarse_modes: modes must be 3 or 6");
+  if (modes != c->coarse_modes) {
+    c->coarse_modes = modes;
+    coarse_release(c);
+  }
+  return PD_OK;
+}
+
 int pd_qs_coarse_operator(pd_ctx* c, const double* u, double cell, int64_t* n_coarse, int32_t* aggregate, double* A,
                           double* A_inv) {
   CHECK_CTX(c);

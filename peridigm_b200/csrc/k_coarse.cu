@@ -26,6 +26,18 @@
 // atomics). Ac is inverted in place by blocked Gauss-Jordan (SPD, no pivoting)
 // and applied as a dense matrix-vector product. Bond damage is taken as
 // symmetric (d_ij = d_ji), as the critical-stretch law produces it.
+//
+// Rigid coarse space (6 modes per aggregate, pd_qs_coarse_modes): the three
+// translations and the three rotations about the aggregate's center (scaled
+// by 1/side), prescribed dofs masked, orthonormalised per aggregate through
+// the Cholesky factor of their 6x6 Gram matrix (modes whose pivot falls
+// below 1e-8 of the largest diagonal entry are dropped: identity rows). Ac is
+// assembled by colored probing: aggregates colored by their cell coordinates
+// mod 3 per axis (27 colors) have disjoint 3x3x3 cell neighborhoods, and K
+// couples points at most 2 delta <= one cell apart, so one tangent product
+// per (color, mode) gives the columns of every aggregate of that color; each
+// aggregate row reads its one neighbor of that color. 162 products per
+// build, deterministic, no atomics.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -41,6 +53,7 @@ constexpr int kGjB = 64;       // Gauss-Jordan block
 constexpr int kMaxCoarse = 6144;
 
 struct CoarseState {
+  int modes = 3;           // coarse dofs per aggregate: 3 translations, or 6 with the rotations
   bool built = false;      // aggregates
   bool have_op = false;    // Ac^-1 ready
   double cell = 0.0;
@@ -54,6 +67,8 @@ struct CoarseState {
   DBuf<double> P, R, C;    // Gauss-Jordan work
   DBuf<double> rc, zc;
   DBuf<int> status;
+  DBuf<double> center, T;   // rigid modes: aggregate centers [4 nagg], orthonormalising transforms [36 nagg]
+  DBuf<double> probe, kprobe;  // rigid modes: probe vector and its tangent image [3n]
 };
 
 __device__ __forceinline__ double co_omega(int kind, double zeta, double h) {
@@ -408,6 +423,210 @@ __global__ void k_coarse_prolong(int64_t n, const int32_t* __restrict__ agg_of, 
 }
 
 // ---------------------------------------------------------------------------
+// Rigid coarse space (6 modes per aggregate)
+// ---------------------------------------------------------------------------
+// Component c of raw mode k at offset d from the center (scaled by 1/side).
+__device__ __forceinline__ double rigid_raw(const double d[3], double inv_side, int c, int k) {
+  switch (k) {
+    case 0: case 1: case 2: return c == k ? 1.0 : 0.0;
+    case 3: return c == 0 ? -d[1] * inv_side : (c == 1 ? d[0] * inv_side : 0.0);  // about z
+    case 4: return c == 1 ? -d[2] * inv_side : (c == 2 ? d[1] * inv_side : 0.0);  // about x
+    default: return c == 2 ? -d[0] * inv_side : (c == 0 ? d[2] * inv_side : 0.0);  // about y
+  }
+}
+
+// The orthonormal mode values of point i (3 x 6, masked): out[c][k].
+__device__ __forceinline__ void rigid_modes(const double4& x, const double* center, const double* T, double inv_side,
+                                            uint8_t fixed, double out[3][6]) {
+  const double d[3] = {x.x - center[0], x.y - center[1], x.z - center[2]};
+  for (int c = 0; c < 3; ++c) {
+    const bool fr = !((fixed >> c) & 1);
+    for (int k = 0; k < 6; ++k) {
+      double v = 0.0;
+      if (fr)
+        for (int l = 0; l < 6; ++l) v += rigid_raw(d, inv_side, c, l) * T[6 * l + k];
+      out[c][k] = v;
+    }
+  }
+}
+
+__device__ __forceinline__ void agg_cell_xyz(const Grid& g, int q, int* cx, int* cy, int* cz) {
+  *cx = q % g.dims[0];
+  *cy = (q / g.dims[0]) % g.dims[1];
+  *cz = q / (g.dims[0] * g.dims[1]);
+}
+
+// Warp per aggregate: center (mean of its points), Gram matrix of the masked
+// raw modes, Cholesky with dropping, T = L^-T on the kept modes.
+__global__ void k_rigid_setup(int64_t nagg, const int32_t* __restrict__ agg_cell, const int64_t* __restrict__ cstart,
+                              const int32_t* __restrict__ sorted, const double4* __restrict__ xv,
+                              const uint8_t* __restrict__ fixed, double inv_side, double* __restrict__ center,
+                              double* __restrict__ Tm) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= nagg) return;
+  const int q = agg_cell[I];
+  const int64_t t0 = cstart[q], t1 = cstart[q + 1];
+  double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+  for (int64_t t = t0 + lane; t < t1; t += 32) {
+    const double4 x = xv[sorted[t]];
+    c0 += x.x, c1 += x.y, c2 += x.z;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+    c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+    c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+  }
+  const double cnt = (double)(t1 - t0);
+  const double cen[3] = {c0 / cnt, c1 / cnt, c2 / cnt};
+  double G[21];  // lower triangle, row-major
+  for (int k = 0; k < 21; ++k) G[k] = 0.0;
+  for (int64_t t = t0 + lane; t < t1; t += 32) {
+    const int64_t p = sorted[t];
+    const double4 x = xv[p];
+    const double d[3] = {x.x - cen[0], x.y - cen[1], x.z - cen[2]};
+    const uint8_t f = fixed[p];
+    for (int c = 0; c < 3; ++c) {
+      if ((f >> c) & 1) continue;
+      double v[6];
+      for (int k = 0; k < 6; ++k) v[k] = rigid_raw(d, inv_side, c, k);
+      for (int a = 0, e = 0; a < 6; ++a)
+        for (int b = 0; b <= a; ++b, ++e) G[e] += v[a] * v[b];
+    }
+  }
+  for (int k = 0; k < 21; ++k)
+    for (int o = 16; o > 0; o >>= 1) G[k] += __shfl_xor_sync(0xffffffffu, G[k], o);
+  if (lane != 0) return;
+  center[4 * I] = cen[0], center[4 * I + 1] = cen[1], center[4 * I + 2] = cen[2], center[4 * I + 3] = cnt;
+  double L[6][6] = {}, gmax = 0.0;
+  bool keep[6];
+  auto gv = [&](int a, int b) { return a >= b ? G[a * (a + 1) / 2 + b] : G[b * (b + 1) / 2 + a]; };
+  for (int k = 0; k < 6; ++k) gmax = fmax(gmax, gv(k, k));
+  for (int k = 0; k < 6; ++k) {
+    double sd = gv(k, k);
+    for (int j = 0; j < k; ++j) sd -= L[k][j] * L[k][j];
+    keep[k] = gmax > 0.0 && sd > 1.0e-8 * gmax;
+    if (!keep[k]) continue;
+    L[k][k] = sqrt(sd);
+    for (int i = k + 1; i < 6; ++i) {
+      double v = gv(i, k);
+      for (int j = 0; j < k; ++j) v -= L[i][j] * L[k][j];
+      L[i][k] = v / L[k][k];
+    }
+  }
+  // M = L^-1 on the kept modes (forward substitution), T = M^T
+  double M[6][6] = {};
+  for (int k = 0; k < 6; ++k) {
+    if (!keep[k]) continue;
+    for (int i = k; i < 6; ++i) {
+      if (!keep[i]) continue;
+      double v = i == k ? 1.0 : 0.0;
+      for (int j = k; j < i; ++j) v -= L[i][j] * M[j][k];
+      M[i][k] = v / L[i][i];
+    }
+  }
+  double* T = Tm + 36 * I;
+  for (int l = 0; l < 6; ++l)
+    for (int k = 0; k < 6; ++k) T[6 * l + k] = M[k][l];
+}
+
+// Probe: mode m of every aggregate of color cc (zero elsewhere).
+__global__ void k_rigid_probe(int64_t n, const int32_t* __restrict__ agg_of, const int32_t* __restrict__ agg_cell,
+                              Grid g, int cc, int m, const double* __restrict__ center, const double* __restrict__ Tm,
+                              const double4* __restrict__ xv, const uint8_t* __restrict__ fixed, double inv_side,
+                              double* __restrict__ w) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int I = agg_of[i];
+  int cx, cy, cz;
+  agg_cell_xyz(g, agg_cell[I], &cx, &cy, &cz);
+  double v[3][6];
+  if ((cx % 3) + 3 * (cy % 3) + 9 * (cz % 3) == cc) {
+    rigid_modes(xv[i], center + 4 * I, Tm + 36 * I, inv_side, fixed[i], v);
+    for (int c = 0; c < 3; ++c) w[3 * i + c] = v[c][m];
+  } else {
+    for (int c = 0; c < 3; ++c) w[3 * i + c] = 0.0;
+  }
+}
+
+// Warp per aggregate row I: Ac[6I + k][6J + m] = sum_{i in I} mode_k(i) . kw_i
+// for J the aggregate of color cc among I's 3x3x3 neighbor cells.
+__global__ void k_rigid_block(int64_t nagg, int nc, Grid g, int cc, int m, const int32_t* __restrict__ agg_cell,
+                              const int32_t* __restrict__ cell_agg, const int64_t* __restrict__ cstart,
+                              const int32_t* __restrict__ sorted, const double* __restrict__ center,
+                              const double* __restrict__ Tm, const double4* __restrict__ xv,
+                              const uint8_t* __restrict__ fixed, double inv_side, const double* __restrict__ kw,
+                              double* __restrict__ A) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= nagg) return;
+  const int q = agg_cell[I];
+  int c3[3];
+  agg_cell_xyz(g, q, &c3[0], &c3[1], &c3[2]);
+  const int want[3] = {cc % 3, (cc / 3) % 3, cc / 9};
+  int jc[3];
+  for (int a = 0; a < 3; ++a) {
+    int d = -1;
+    while (((c3[a] + d) % 3 + 3) % 3 != want[a]) ++d;
+    jc[a] = c3[a] + d;
+    if (jc[a] < 0 || jc[a] >= g.dims[a]) return;
+  }
+  const int J = cell_agg[(jc[2] * g.dims[1] + jc[1]) * g.dims[0] + jc[0]];
+  if (J < 0) return;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+    const int64_t p = sorted[t];
+    double v[3][6];
+    rigid_modes(xv[p], center + 4 * I, Tm + 36 * I, inv_side, fixed[p], v);
+    for (int k = 0; k < 6; ++k) acc[k] += v[0][k] * kw[3 * p] + v[1][k] * kw[3 * p + 1] + v[2][k] * kw[3 * p + 2];
+  }
+  for (int k = 0; k < 6; ++k)
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) A[(size_t)(6 * I + k) * nc + 6 * J + m] = acc[k];
+}
+
+template <typename T>
+__global__ void k_rigid_restrict(int64_t nagg, const int32_t* __restrict__ agg_cell, const int64_t* __restrict__ cstart,
+                                 const int32_t* __restrict__ sorted, const double* __restrict__ center,
+                                 const double* __restrict__ Tm, const double4* __restrict__ xv,
+                                 const uint8_t* __restrict__ fixed, double inv_side, const T* __restrict__ r,
+                                 double* __restrict__ rc) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (I >= nagg) return;
+  const int q = agg_cell[I];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+    const int64_t p = sorted[t];
+    double v[3][6];
+    rigid_modes(xv[p], center + 4 * I, Tm + 36 * I, inv_side, fixed[p], v);
+    const double r0 = (double)r[3 * p], r1 = (double)r[3 * p + 1], r2 = (double)r[3 * p + 2];
+    for (int k = 0; k < 6; ++k) acc[k] += v[0][k] * r0 + v[1][k] * r1 + v[2][k] * r2;
+  }
+  for (int k = 0; k < 6; ++k)
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if (lane == 0)
+    for (int k = 0; k < 6; ++k) rc[6 * I + k] = acc[k];
+}
+
+__global__ void k_rigid_prolong(int64_t n, const int32_t* __restrict__ agg_of, const double* __restrict__ center,
+                                const double* __restrict__ Tm, const double4* __restrict__ xv,
+                                const uint8_t* __restrict__ fixed, double inv_side, const double* __restrict__ zc,
+                                double scale, double* __restrict__ z) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t I = agg_of[i];
+  double v[3][6];
+  rigid_modes(xv[i], center + 4 * I, Tm + 36 * I, inv_side, fixed[i], v);
+  for (int c = 0; c < 3; ++c) {
+    double s = 0.0;
+    for (int k = 0; k < 6; ++k) s += v[c][k] * zc[6 * I + k];
+    if (!((fixed[i] >> c) & 1)) z[3 * i + c] += scale * s;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 static CoarseState* co_state(pd_ctx* c) {
@@ -436,7 +655,8 @@ static int co_aggregates(pd_ctx* c, CoarseState* s, double cell) {
   double hmax = 0.0;
   for (double h : c->block_h) hmax = std::max(hmax, h);
   double side = std::max(cell, 2.0 * hmax * (1.0 + 1.0e-6));
-  if (s->built && s->n == n && s->cell == side) return PD_OK;
+  const int modes = c->coarse_modes == 6 ? 6 : 3;
+  if (s->built && s->n == n && s->cell == side && s->modes == modes) return PD_OK;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int64_t i = 0; i < n; ++i)
     for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], c->hx[3 * i + k]), hi[k] = std::max(hi[k], c->hx[3 * i + k]);
@@ -462,13 +682,13 @@ static int co_aggregates(pd_ctx* c, CoarseState* s, double cell) {
     PD_CUDA_TRY(c, cudaGetLastError());
     int64_t nagg = 0;
     PD_CUDA_TRY(c, d2h(c, &nagg, nagg_d.p, sizeof(int64_t)));
-    if (3 * nagg > kMaxCoarse) {
+    if (modes * nagg > kMaxCoarse) {
       side *= 1.25;
       continue;
     }
     s->g = g;
     s->nagg = nagg;
-    s->nc = (int)(3 * nagg);
+    s->nc = (int)(modes * nagg);
     break;
   }
   PD_CUDA_TRY(c, s->agg_of.alloc(n));
@@ -484,6 +704,13 @@ static int co_aggregates(pd_ctx* c, CoarseState* s, double cell) {
   PD_CUDA_TRY(c, s->rc.alloc(nc));
   PD_CUDA_TRY(c, s->zc.alloc(nc));
   PD_CUDA_TRY(c, s->status.alloc(1));
+  if (modes == 6) {
+    PD_CUDA_TRY(c, s->center.alloc(4 * (size_t)s->nagg));
+    PD_CUDA_TRY(c, s->T.alloc(36 * (size_t)s->nagg));
+    PD_CUDA_TRY(c, s->probe.alloc(3 * (size_t)n));
+    PD_CUDA_TRY(c, s->kprobe.alloc(3 * (size_t)n));
+  }
+  s->modes = modes;
   s->n = n;
   s->cell = want;
   s->built = true;
@@ -500,6 +727,27 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
   TRY_RC(co_aggregates(c, s, cell));
   const int64_t n = c->n;
   const int nc = s->nc;
+  if (s->modes == 6) {  // rigid modes: orthonormal bases, then colored probing with the tangent
+    const double inv_side = 1.0 / s->g.cell;
+    const unsigned gw = (unsigned)((s->nagg * 32 + 255) / 256), gp = (unsigned)((n + 255) / 256);
+    k_rigid_setup<<<gw, 256, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, c->xv.p, fixed,
+                                             inv_side, s->center.p, s->T.p);
+    PD_CUDA_TRY(c, dzero(c, s->A.p, s->A.bytes()));
+    for (int cc = 0; cc < 27; ++cc)
+      for (int m = 0; m < 6; ++m) {
+        k_rigid_probe<<<gp, 256, 0, c->stream>>>(n, s->agg_of.p, s->agg_cell.p, s->g, cc, m, s->center.p, s->T.p,
+                                                 c->xv.p, fixed, inv_side, s->probe.p);
+        PD_CUDA_TRY(c, cudaGetLastError());
+        TRY_RC(qs_apply_K(c, s->probe.p, s->kprobe.p));
+        k_rigid_block<<<gw, 256, 0, c->stream>>>(s->nagg, nc, s->g, cc, m, s->agg_cell.p, s->cell_agg.p, s->cstart.p,
+                                                 s->sorted.p, s->center.p, s->T.p, c->xv.p, fixed, inv_side,
+                                                 s->kprobe.p, s->A.p);
+      }
+    k_coarse_unit_diag<<<(nc + 255) / 256, 256, 0, c->stream>>>(nc, s->A.p);
+    PD_CUDA_TRY(c, cudaGetLastError());
+    (void)y;
+    (void)ab;
+  } else {
   PD_CUDA_TRY(c, dzero(c, s->status.p, sizeof(int)));
   k_coarse_point<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(n, c->row.p, c->col.p, c->dmg.p, c->xv.p, y, ab,
                                                                      c->pt.p, c->hp.p, c->influence, fixed, s->g,
@@ -514,6 +762,7 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
   if (st) {
     c->err = "coarse space: a bond reaches past its point's 2x2x2 aggregate cells";
     return PD_ERR_STATE;
+  }
   }
   if (assembled)
     PD_CUDA_TRY(c, cudaMemcpyAsync(assembled, s->A.p, s->A.bytes(), cudaMemcpyDeviceToDevice, c->stream));
@@ -538,9 +787,19 @@ static int co_apply(pd_ctx* c, const T* r, double* z, const uint8_t* fixed, doub
     return PD_ERR_STATE;
   }
   const int64_t n = c->n;
-  k_coarse_restrict<T><<<(unsigned)((s->nagg * 32 + 255) / 256), 256, 0, c->stream>>>(s->nagg, s->agg_cell.p,
-                                                                                      s->cstart.p, s->sorted.p, r,
-                                                                                      s->rc.p);
+  const unsigned gw = (unsigned)((s->nagg * 32 + 255) / 256);
+  if (s->modes == 6) {
+    const double inv_side = 1.0 / s->g.cell;
+    k_rigid_restrict<T><<<gw, 256, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, s->center.p,
+                                                   s->T.p, c->xv.p, fixed, inv_side, r, s->rc.p);
+    k_coarse_gemv<<<(unsigned)(((int64_t)s->nc * 32 + 255) / 256), 256, 0, c->stream>>>(s->nc, s->A.p, s->rc.p,
+                                                                                        s->zc.p);
+    k_rigid_prolong<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, s->agg_of.p, s->center.p, s->T.p, c->xv.p,
+                                                                        fixed, inv_side, s->zc.p, scale, z);
+    PD_CUDA_TRY(c, cudaGetLastError());
+    return PD_OK;
+  }
+  k_coarse_restrict<T><<<gw, 256, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, r, s->rc.p);
   k_coarse_gemv<<<(unsigned)(((int64_t)s->nc * 32 + 255) / 256), 256, 0, c->stream>>>(s->nc, s->A.p, s->rc.p, s->zc.p);
   k_coarse_prolong<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, s->agg_of.p, s->zc.p, scale, fixed, z);
   PD_CUDA_TRY(c, cudaGetLastError());

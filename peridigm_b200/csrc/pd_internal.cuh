@@ -130,6 +130,7 @@ struct pd_ctx {
   bool have_material = false;
   std::vector<int> block_model;  // PD_MATERIAL_* per block (-1: not set)
   int material_model = PD_MATERIAL_LPS;
+  int coarse_modes = 3;  // coarse dofs per aggregate of the two-level preconditioner: 3 or 6 (rotations)
   int bb_plane = 0;              // bond-based: plane strain/stress constant
   double bb_height = 0.0;
   std::vector<double> field_K, field_mu, field_sc;  // per-point overrides (empty = none)
