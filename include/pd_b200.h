@@ -101,6 +101,7 @@ typedef struct {
   int64_t cg_iterations;
   double final_residual;  /* relative FP64 residual of the last linear solve */
   int64_t preconditioner_fallbacks; /* learned-preconditioner solves finished by block Jacobi */
+  int64_t coarse_builds;  /* coarse operators built by pd_qs_load_step (two-level and learned) */
 } pd_stats;
 
 /* ---- lifecycle ---------------------------------------------------------- */

@@ -62,7 +62,7 @@ class Stats(C.Structure):
     _fields_ = [("steps", C.c_int64), ("bonds", C.c_int64), ("broken_bonds", C.c_int64),
                 ("contact_pairs", C.c_int64), ("device_ms", C.c_double), ("newton_iterations", C.c_int64),
                 ("cg_iterations", C.c_int64), ("final_residual", C.c_double),
-                ("preconditioner_fallbacks", C.c_int64)]
+                ("preconditioner_fallbacks", C.c_int64), ("coarse_builds", C.c_int64)]
 
 
 PD_PRECOND_NONE = 0

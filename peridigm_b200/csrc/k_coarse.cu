@@ -36,8 +36,9 @@
 // mod 3 per axis (27 colors) have disjoint 3x3x3 cell neighborhoods, and K
 // couples points at most 2 delta <= one cell apart, so one tangent product
 // per (color, mode) gives the columns of every aggregate of that color; each
-// aggregate row reads its one neighbor of that color. 162 products per
-// build, deterministic, no atomics.
+// aggregate row reads its one neighbor of that color. The 6 modes of a color
+// go through one multi-vector tangent pass (27 per build), deterministic, no
+// atomics.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -68,7 +69,7 @@ struct CoarseState {
   DBuf<double> rc, zc;
   DBuf<int> status;
   DBuf<double> center, T;   // rigid modes: aggregate centers [4 nagg], orthonormalising transforms [36 nagg]
-  DBuf<double> probe, kprobe;  // rigid modes: probe vector and its tangent image [3n]
+  DBuf<double> probe, kprobe, pdth;  // rigid modes: 6 probes, their tangent images [18n], scratch [6n]
 };
 
 __device__ __forceinline__ double co_omega(int kind, double zeta, double h) {
@@ -530,33 +531,30 @@ __global__ void k_rigid_setup(int64_t nagg, const int32_t* __restrict__ agg_cell
     for (int k = 0; k < 6; ++k) T[6 * l + k] = M[k][l];
 }
 
-// Probe: mode m of every aggregate of color cc (zero elsewhere).
-__global__ void k_rigid_probe(int64_t n, const int32_t* __restrict__ agg_of, const int32_t* __restrict__ agg_cell,
-                              Grid g, int cc, int m, const double* __restrict__ center, const double* __restrict__ Tm,
-                              const double4* __restrict__ xv, const uint8_t* __restrict__ fixed, double inv_side,
-                              double* __restrict__ w) {
+// Probes of color cc, all 6 modes at once (point-major: w[(i*6 + m)*3 + c]).
+__global__ void k_rigid_probe6(int64_t n, const int32_t* __restrict__ agg_of, const int32_t* __restrict__ agg_cell,
+                               Grid g, int cc, const double* __restrict__ center, const double* __restrict__ Tm,
+                               const double4* __restrict__ xv, const uint8_t* __restrict__ fixed, double inv_side,
+                               double* __restrict__ w) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int I = agg_of[i];
   int cx, cy, cz;
   agg_cell_xyz(g, agg_cell[I], &cx, &cy, &cz);
   double v[3][6];
-  if ((cx % 3) + 3 * (cy % 3) + 9 * (cz % 3) == cc) {
-    rigid_modes(xv[i], center + 4 * I, Tm + 36 * I, inv_side, fixed[i], v);
-    for (int c = 0; c < 3; ++c) w[3 * i + c] = v[c][m];
-  } else {
-    for (int c = 0; c < 3; ++c) w[3 * i + c] = 0.0;
-  }
+  const bool on = (cx % 3) + 3 * (cy % 3) + 9 * (cz % 3) == cc;
+  if (on) rigid_modes(xv[i], center + 4 * I, Tm + 36 * I, inv_side, fixed[i], v);
+  for (int m = 0; m < 6; ++m)
+    for (int c = 0; c < 3; ++c) w[(i * 6 + m) * 3 + c] = on ? v[c][m] : 0.0;
 }
 
-// Warp per aggregate row I: Ac[6I + k][6J + m] = sum_{i in I} mode_k(i) . kw_i
-// for J the aggregate of color cc among I's 3x3x3 neighbor cells.
-__global__ void k_rigid_block(int64_t nagg, int nc, Grid g, int cc, int m, const int32_t* __restrict__ agg_cell,
-                              const int32_t* __restrict__ cell_agg, const int64_t* __restrict__ cstart,
-                              const int32_t* __restrict__ sorted, const double* __restrict__ center,
-                              const double* __restrict__ Tm, const double4* __restrict__ xv,
-                              const uint8_t* __restrict__ fixed, double inv_side, const double* __restrict__ kw,
-                              double* __restrict__ A) {
+// Warp per aggregate row I: Ac[6I + k][6J + m] for all 6 probe modes m of color cc.
+__global__ void k_rigid_block6(int64_t nagg, int nc, Grid g, int cc, const int32_t* __restrict__ agg_cell,
+                               const int32_t* __restrict__ cell_agg, const int64_t* __restrict__ cstart,
+                               const int32_t* __restrict__ sorted, const double* __restrict__ center,
+                               const double* __restrict__ Tm, const double4* __restrict__ xv,
+                               const uint8_t* __restrict__ fixed, double inv_side, const double* __restrict__ kw,
+                               double* __restrict__ A) {
   const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (I >= nagg) return;
@@ -573,17 +571,23 @@ __global__ void k_rigid_block(int64_t nagg, int nc, Grid g, int cc, int m, const
   }
   const int J = cell_agg[(jc[2] * g.dims[1] + jc[1]) * g.dims[0] + jc[0]];
   if (J < 0) return;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
+  double acc[6][6];
+  for (int k = 0; k < 6; ++k)
+    for (int m = 0; m < 6; ++m) acc[k][m] = 0.0;
   for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
     const int64_t p = sorted[t];
     double v[3][6];
     rigid_modes(xv[p], center + 4 * I, Tm + 36 * I, inv_side, fixed[p], v);
-    for (int k = 0; k < 6; ++k) acc[k] += v[0][k] * kw[3 * p] + v[1][k] * kw[3 * p + 1] + v[2][k] * kw[3 * p + 2];
+    const double* y = kw + p * 18;
+    for (int m = 0; m < 6; ++m)
+      for (int k = 0; k < 6; ++k) acc[k][m] += v[0][k] * y[3 * m] + v[1][k] * y[3 * m + 1] + v[2][k] * y[3 * m + 2];
   }
   for (int k = 0; k < 6; ++k)
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    for (int m = 0; m < 6; ++m)
+      for (int o = 16; o > 0; o >>= 1) acc[k][m] += __shfl_xor_sync(0xffffffffu, acc[k][m], o);
   if (lane == 0)
-    for (int k = 0; k < 6; ++k) A[(size_t)(6 * I + k) * nc + 6 * J + m] = acc[k];
+    for (int k = 0; k < 6; ++k)
+      for (int m = 0; m < 6; ++m) A[(size_t)(6 * I + k) * nc + 6 * J + m] = acc[k][m];
 }
 
 template <typename T>
@@ -707,8 +711,9 @@ static int co_aggregates(pd_ctx* c, CoarseState* s, double cell) {
   if (modes == 6) {
     PD_CUDA_TRY(c, s->center.alloc(4 * (size_t)s->nagg));
     PD_CUDA_TRY(c, s->T.alloc(36 * (size_t)s->nagg));
-    PD_CUDA_TRY(c, s->probe.alloc(3 * (size_t)n));
-    PD_CUDA_TRY(c, s->kprobe.alloc(3 * (size_t)n));
+    PD_CUDA_TRY(c, s->probe.alloc(18 * (size_t)n));
+    PD_CUDA_TRY(c, s->kprobe.alloc(18 * (size_t)n));
+    PD_CUDA_TRY(c, s->pdth.alloc(6 * (size_t)n));
   }
   s->modes = modes;
   s->n = n;
@@ -733,16 +738,15 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
     k_rigid_setup<<<gw, 256, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, c->xv.p, fixed,
                                              inv_side, s->center.p, s->T.p);
     PD_CUDA_TRY(c, dzero(c, s->A.p, s->A.bytes()));
-    for (int cc = 0; cc < 27; ++cc)
-      for (int m = 0; m < 6; ++m) {
-        k_rigid_probe<<<gp, 256, 0, c->stream>>>(n, s->agg_of.p, s->agg_cell.p, s->g, cc, m, s->center.p, s->T.p,
-                                                 c->xv.p, fixed, inv_side, s->probe.p);
-        PD_CUDA_TRY(c, cudaGetLastError());
-        TRY_RC(qs_apply_K(c, s->probe.p, s->kprobe.p));
-        k_rigid_block<<<gw, 256, 0, c->stream>>>(s->nagg, nc, s->g, cc, m, s->agg_cell.p, s->cell_agg.p, s->cstart.p,
-                                                 s->sorted.p, s->center.p, s->T.p, c->xv.p, fixed, inv_side,
-                                                 s->kprobe.p, s->A.p);
-      }
+    for (int cc = 0; cc < 27; ++cc) {  // one multi-vector tangent product per color (its 6 modes)
+      k_rigid_probe6<<<gp, 256, 0, c->stream>>>(n, s->agg_of.p, s->agg_cell.p, s->g, cc, s->center.p, s->T.p, c->xv.p,
+                                                fixed, inv_side, s->probe.p);
+      PD_CUDA_TRY(c, cudaGetLastError());
+      TRY_RC(qs_apply_K_multi(c, s->probe.p, s->kprobe.p, s->pdth.p));
+      k_rigid_block6<<<gw, 256, 0, c->stream>>>(s->nagg, nc, s->g, cc, s->agg_cell.p, s->cell_agg.p, s->cstart.p,
+                                                s->sorted.p, s->center.p, s->T.p, c->xv.p, fixed, inv_side,
+                                                s->kprobe.p, s->A.p);
+    }
     k_coarse_unit_diag<<<(nc + 255) / 256, 256, 0, c->stream>>>(nc, s->A.p);
     PD_CUDA_TRY(c, cudaGetLastError());
     (void)y;

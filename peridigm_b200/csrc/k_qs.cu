@@ -534,7 +534,7 @@ static int qs_apply_precond(pd_ctx* c, int precond, const double* r, double* z) 
 
 // Tangent-vector product q = K w.xyz (w.w receives q dtheta) on the per-bond
 // geometry, rebuilt first when the state changed.
-static int qs_tangent(pd_ctx* c) {
+static int qs_geometry(pd_ctx* c) {
   QsState* s = c->qs;
   const int64_t n = c->n;
   if (s->geo_dirty || s->geo.count < (size_t)c->nb) {
@@ -546,6 +546,14 @@ static int qs_tangent(pd_ctx* c) {
                                                       c->hp.p, c->influence, s->geo.p, s->gco.p);
     s->geo_dirty = false;
   }
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
+static int qs_tangent(pd_ctx* c) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  TRY_RC(qs_geometry(c));
   k_qs_dtheta_g<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->abq.p, c->pt.p, s->w.p);
   k_qs_df_g<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->gco.p, c->xv.p, s->w.p,
                                                s->fixed.p, s->q.p, s->partial.p, c->pt.p, s->jk, s->jm);
@@ -817,6 +825,116 @@ int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev) {
   return PD_OK;
 }
 
+// Tangent products of kQsMulti vectors at once (the probes of the rigid coarse
+// space): the bond geometry is streamed once for all of them. p and q hold the
+// vectors point-major, p[(i * kQsMulti + v) * 3 + c]; prescribed components of
+// p are dropped; prescribed rows of q = p. dth [kQsMulti n] scratch.
+__global__ void __launch_bounds__(kQsBlock) k_qs_dtheta_multi(int64_t n, const int64_t* __restrict__ row,
+                                                              const int32_t* __restrict__ col,
+                                                              const double4* __restrict__ g,
+                                                              const double4* __restrict__ ab,
+                                                              const double4* __restrict__ pt,
+                                                              const uint8_t* __restrict__ fixed,
+                                                              const double* __restrict__ p, double* __restrict__ dth) {
+  constexpr int NV = kQsMulti;
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
+  const int lane = threadIdx.x & (kQsTpo - 1);
+  const bool valid = i < n;
+  double acc[NV];
+  for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+  if (valid) {
+    double pi[NV][3];
+    const uint8_t fi = fixed[i];
+    for (int v = 0; v < NV; ++v)
+      for (int c = 0; c < 3; ++c) pi[v][c] = ((fi >> c) & 1) ? 0.0 : p[(i * NV + v) * 3 + c];
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+      const double4 gb = g[b];
+      const int32_t j = col[b];
+      const uint8_t fj = fixed[j];
+      const double* pj = p + (int64_t)j * NV * 3;
+      for (int v = 0; v < NV; ++v) {
+        const double w0 = ((fj & 1) ? 0.0 : pj[3 * v]) - pi[v][0];
+        const double w1 = ((fj & 2) ? 0.0 : pj[3 * v + 1]) - pi[v][1];
+        const double w2 = ((fj & 4) ? 0.0 : pj[3 * v + 2]) - pi[v][2];
+        acc[v] += gb.w * (gb.x * w0 + gb.y * w1 + gb.z * w2);
+      }
+    }
+  }
+  for (int v = 0; v < NV; ++v) acc[v] = qs_group_sum(acc[v]);
+  if (valid && lane == 0) {
+    const double s = 3.0 * (ab[i].y / pt[i].x);
+    for (int v = 0; v < NV; ++v) dth[i * NV + v] = s * acc[v];
+  }
+}
+
+__global__ void __launch_bounds__(kQsBlock) k_qs_df_multi(int64_t n, const int64_t* __restrict__ row,
+                                                          const int32_t* __restrict__ col,
+                                                          const double4* __restrict__ g,
+                                                          const double2* __restrict__ gc,
+                                                          const double4* __restrict__ xv,
+                                                          const uint8_t* __restrict__ fixed,
+                                                          const double* __restrict__ p,
+                                                          const double* __restrict__ dth, double* __restrict__ q) {
+  constexpr int NV = kQsMulti;
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kQsTpo;
+  const int lane = threadIdx.x & (kQsTpo - 1);
+  const bool valid = i < n;
+  double d[NV][3];
+  for (int v = 0; v < NV; ++v) d[v][0] = d[v][1] = d[v][2] = 0.0;
+  uint8_t fi = 0;
+  if (valid) {
+    double pi[NV][3], ti[NV];
+    fi = fixed[i];
+    for (int v = 0; v < NV; ++v) {
+      ti[v] = dth[i * NV + v];
+      for (int c = 0; c < 3; ++c) pi[v][c] = ((fi >> c) & 1) ? 0.0 : p[(i * NV + v) * 3 + c];
+    }
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+      const double4 gb = g[b];
+      const double2 cb = gc[b];
+      const int32_t j = col[b];
+      const uint8_t fj = fixed[j];
+      const double* pj = p + (int64_t)j * NV * 3;
+      const double* tj = dth + (int64_t)j * NV;
+      for (int v = 0; v < NV; ++v) {
+        const double w0 = ((fj & 1) ? 0.0 : pj[3 * v]) - pi[v][0];
+        const double w1 = ((fj & 2) ? 0.0 : pj[3 * v + 1]) - pi[v][1];
+        const double w2 = ((fj & 4) ? 0.0 : pj[3 * v + 2]) - pi[v][2];
+        const double de = gb.x * w0 + gb.y * w1 + gb.z * w2;
+        const double sy = gb.w * (ti[v] + tj[v]) + (cb.y - cb.x) * de;
+        d[v][0] += sy * gb.x + cb.x * w0;
+        d[v][1] += sy * gb.y + cb.x * w1;
+        d[v][2] += sy * gb.z + cb.x * w2;
+      }
+    }
+  }
+  for (int v = 0; v < NV; ++v)
+    for (int c = 0; c < 3; ++c) d[v][c] = qs_group_sum(d[v][c]);
+  if (valid && lane < 3) {
+    const int c = lane;
+    const double V = xv[i].w;
+    for (int v = 0; v < NV; ++v) {
+      const int64_t k = (i * NV + v) * 3 + c;
+      const double dv = c == 0 ? d[v][0] : (c == 1 ? d[v][1] : d[v][2]);
+      q[k] = ((fi >> c) & 1) ? p[k] : -V * dv;
+    }
+  }
+}
+
+// q = K p for kQsMulti vectors (point-major, see k_qs_dtheta_multi) with the
+// tangent prepared by qs_prepare_current; dth [kQsMulti n] scratch.
+int qs_apply_K_multi(pd_ctx* c, const double* p_dev, double* q_dev, double* dth_dev) {
+  QsState* s = c->qs;
+  const int64_t n = c->n;
+  TRY_RC(qs_geometry(c));
+  k_qs_dtheta_multi<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->abq.p, c->pt.p,
+                                                       s->fixed.p, p_dev, dth_dev);
+  k_qs_df_multi<<<gt(n), kQsBlock, 0, c->stream>>>(n, c->row.p, c->col.p, s->geo.p, s->gco.p, c->xv.p, s->fixed.p,
+                                                   p_dev, dth_dev, q_dev);
+  PD_CUDA_TRY(c, cudaGetLastError());
+  return PD_OK;
+}
+
 int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o, pd_stats* st) {
   TRY_RC(ensure_ready_internal(c));
   if (c->material_model != PD_MATERIAL_LPS) {
@@ -858,6 +976,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   double metric = l2 + 20.0 * linf;
   const double newton_tol = o->newton_tolerance < 0.0 ? -o->newton_tolerance * ref_metric : o->newton_tolerance;
   int newton = 0, cg_total = 0;
+  int64_t coarse_builds = 0;
   double last_rel = 0.0;
   const int64_t fallbacks0 = c->qs_fallbacks;
   cudaEvent_t e0, e1;
@@ -882,6 +1001,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
         s->coarse_cell = std::max(0.0, cell);
         s->coarse_ref_iters = -1;
         s->coarse_rebuild = false;
+        ++coarse_builds;
       }
       s->coarse_on = true;
     }
@@ -891,8 +1011,13 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
     cg_total += its;
     last_rel = rel;
     if (two_level) {
+      // rebuild when a solve needs clearly more iterations than the first one
+      // after the last build: 1.3x + 5 for the translations (a build costs a
+      // few CG iterations), 2x + 10 with the rotations (a build costs ~150)
+      const bool rigid = c->coarse_modes == 6;
       if (s->coarse_ref_iters < 0) s->coarse_ref_iters = its;
-      else if (its > (13 * s->coarse_ref_iters) / 10 + 5) s->coarse_rebuild = true;
+      else if (its > (rigid ? 2 * s->coarse_ref_iters + 10 : (13 * s->coarse_ref_iters) / 10 + 5))
+        s->coarse_rebuild = true;
     }
     if (rc != PD_OK && rc != PD_ERR_NOT_CONVERGED) return rc;
     // du += alpha * x, backtracking on the convergence metric
@@ -928,6 +1053,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
     st->cg_iterations += cg_total;
     st->final_residual = last_rel;
     st->preconditioner_fallbacks += c->qs_fallbacks - fallbacks0;
+    st->coarse_builds += coarse_builds;
     st->device_ms += ms;
     st->bonds = c->nb;
   }

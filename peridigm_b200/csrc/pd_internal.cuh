@@ -240,6 +240,8 @@ int qs_tangent_apply(pd_ctx* c, const double* u_dev, const double* w_dev, double
 int qs_tangent_blocks(pd_ctx* c, const double* u_dev, double* blocks_dev);
 int qs_prepare_current(pd_ctx* c);
 int qs_apply_K(pd_ctx* c, const double* w_dev, double* kw_dev);
+constexpr int kQsMulti = 6;  // vectors per multi-vector tangent product
+int qs_apply_K_multi(pd_ctx* c, const double* p_dev, double* q_dev, double* dth_dev);
 bool mpnn_ready(const pd_ctx* c);
 int mpnn_apply_add(pd_ctx* c, const double* r, double* z);
 int mpnn_prepare(pd_ctx* c, const double* dinv);
