@@ -155,8 +155,10 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
     rotations per aggregate as well) and learned (the learned middle level on
     3 mm patches over the two-level base with `learned_modes` coarse modes,
     trained here on such two-level solves of a 12^3 cube over six random
-    moduli and load paths). Times are device time of the Newton loops (CUDA
-    events).
+    moduli and load paths; the weights kept are the checkpoint, every 10
+    epochs from epoch 0, with the fewest CG iterations on a held-out 12^3
+    solve; the last epoch's weights are reported too). Times are device time
+    of the Newton loops (CUDA events).
     With cpu_threads > 0 the block-Jacobi arm also gets a CPU baseline: the
     same CG step restated in C (oracle/cpu_qs.c) on that many host threads,
     timed on a sample and scaled by the solve's Newton and CG counts."""
@@ -169,6 +171,7 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
         workloads.setup_context(tr, w)
         tr.coarse_modes(learned_modes)
         tr.mpnn_init(seed=7, patch=patch)
+        init_weights = tr.mpnn_weights()
         tr.mpnn_collect(4)
         rng = np.random.default_rng(5)
         for _ in range(6):
@@ -186,15 +189,40 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
                 st = tr.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=-1e-8,
                                      cg_relative_tolerance=1e-8, preconditioner="two_level", stats=st)
         pairs = tr.mpnn_num_pairs()
-        loss = tr.mpnn_train(40, learning_rate=1e-3, batch=8)
-        weights = tr.mpnn_weights()
+        # model selection: checkpoints every 10 epochs (epoch 0 = the starting
+        # weights), each scored by the CG iterations of a held-out 12^3 solve
+        wv = workloads.qs_cube(n=12, h=1.0e-3, seed=12, jitter=0.05, load_steps=2)
+
+        def validate(wts):
+            with Context(device=local, precision="fp64") as vc:
+                workloads.setup_context(vc, wv)
+                vc.coarse_modes(learned_modes)
+                vc.mpnn_init(seed=0, patch=patch)
+                vc.mpnn_set_weights(wts)
+                sv = None
+                for k in range(1, len(wv["times"])):
+                    sv = vc.qs_load_step(wv["times"][k - 1], wv["times"][k], newton_tolerance=-1e-8,
+                                         cg_relative_tolerance=1e-8, preconditioner="mpnn", stats=sv)
+                return int(sv.cg_iterations)
+
+        checkpoints = {0: (validate(init_weights), init_weights)}
+        loss = None
+        for epoch in (10, 20, 30, 40):
+            loss = tr.mpnn_train(10, learning_rate=1e-3, batch=8)
+            wts = tr.mpnn_weights()
+            checkpoints[epoch] = (validate(wts), wts)
+        last_weights = checkpoints[40][1]
+        best_epoch = min(checkpoints, key=lambda e: (checkpoints[e][0], e))
+        weights = checkpoints[best_epoch][1]
     train_s = time.perf_counter() - t0
     w2 = workloads.qs_cube(n=60, h=1.0e-3, seed=1000, load_steps=load_steps)
     out = {"workload": f"qs_cube_60x60x60 (seed 1000, {load_steps} load steps)", "points": int(len(w2["vol"])),
            "tolerance": 1e-8, "training": {"pairs": pairs, "epochs": 40, "final_loss": loss, "seconds": train_s,
-                                           "patch_m": patch, "coarse_modes": learned_modes}}
-    for arm in ("block_jacobi", "two_level", "two_level_rigid", "mpnn"):
-        precond = "two_level" if arm == "two_level_rigid" else arm
+                                           "patch_m": patch, "coarse_modes": learned_modes,
+                                           "validation_cg_iterations": {e: v[0] for e, v in checkpoints.items()},
+                                           "selected_epoch": best_epoch}}
+    for arm in ("block_jacobi", "two_level", "two_level_rigid", "mpnn", "mpnn_last_epoch"):
+        precond = {"two_level_rigid": "two_level", "mpnn_last_epoch": "mpnn"}.get(arm, arm)
         with Context(device=local, precision="fp64") as ctx:
             workloads.setup_context(ctx, w2)
             if arm == "two_level_rigid":
@@ -202,7 +230,7 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
             if precond == "mpnn":
                 ctx.coarse_modes(learned_modes)
                 ctx.mpnn_init(seed=0, patch=patch)
-                ctx.mpnn_set_weights(weights)
+                ctx.mpnn_set_weights(weights if arm == "mpnn" else last_weights)
             st = None
             clocks = ClockSampler(local)
             clocks.start()
@@ -214,7 +242,8 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
             clk = clocks.stop()
             out[arm] = {"seconds": st.device_ms / 1e3, "wall_seconds": wall, "cg_iterations": st.cg_iterations,
                             "newton_iterations": st.newton_iterations, "final_cg_residual": st.final_residual,
-                            "fallbacks": st.preconditioner_fallbacks, "sm_mhz": clk["sm_mhz"],
+                            "fallbacks": st.preconditioner_fallbacks, "coarse_builds": st.coarse_builds,
+                            "sm_mhz": clk["sm_mhz"],
                             "clock_reasons": clk["reasons"]}
             if arm == "block_jacobi" and cpu_threads:
                 # CPU baseline: the same block-Jacobi CG step restated in C on the
@@ -241,6 +270,7 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
     out["two_level_speedup_over_block_jacobi"] = bj / out["two_level"]["seconds"]
     out["two_level_rigid_speedup_over_block_jacobi"] = bj / out["two_level_rigid"]["seconds"]
     out["mpnn_speedup_over_block_jacobi"] = bj / out["mpnn"]["seconds"]
+    out["mpnn_last_epoch_speedup_over_block_jacobi"] = bj / out["mpnn_last_epoch"]["seconds"]
     if "cpu_baseline" in out:
         out["block_jacobi_speedup_over_cpu"] = out["cpu_baseline"]["seconds"] / bj
     return out

@@ -59,6 +59,7 @@ struct QsState {
   // (quasi-static: K; implicit dynamics: rho I + beta dt^2 K).
   double jk = 1.0, jm = 0.0;
   DBuf<double> v2;  // implicit dynamics: velocity predictor
+  DBuf<double> cg_b, cg_x0;  // learned-preconditioner CG: right-hand side and restart point (kept, not reallocated)
 };
 
 __device__ __forceinline__ double qs_omega(int kind, double zeta, double h) {
@@ -595,9 +596,10 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
     bool stalled = false;
     return qs_cg_run(c, precond, rel_tol, max_it, iters, rel_out, &stalled);
   }
-  DBuf<double> b, x0;
-  PD_CUDA_TRY(c, b.alloc(m));
-  PD_CUDA_TRY(c, x0.alloc(m));
+  if (s->cg_b.count < (size_t)m) PD_CUDA_TRY(c, s->cg_b.alloc(m));
+  if (s->cg_x0.count < (size_t)m) PD_CUDA_TRY(c, s->cg_x0.alloc(m));
+  DBuf<double>& b = s->cg_b;
+  DBuf<double>& x0 = s->cg_x0;
   PD_CUDA_TRY(c, cudaMemcpyAsync(b.p, s->r.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   bool stalled = false;
   int its = 0;
