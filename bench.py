@@ -158,7 +158,8 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
     moduli and load paths; the weights kept are the checkpoint, every 10
     epochs from epoch 0, with the fewest CG iterations on a held-out 12^3
     solve; the last epoch's weights are reported too). Times are device time
-    of the Newton loops (CUDA events).
+    of the Newton loops (CUDA events); each arm first runs one untimed load
+    step in a throwaway context of the same cube.
     With cpu_threads > 0 the block-Jacobi arm also gets a CPU baseline: the
     same CG step restated in C (oracle/cpu_qs.c) on that many host threads,
     timed on a sample and scaled by the solve's Newton and CG counts."""
@@ -221,16 +222,25 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
                                            "patch_m": patch, "coarse_modes": learned_modes,
                                            "validation_cg_iterations": {e: v[0] for e, v in checkpoints.items()},
                                            "selected_epoch": best_epoch}}
+    def arm_context(arm, precond):
+        ctx = Context(device=local, precision="fp64")
+        workloads.setup_context(ctx, w2)
+        if arm == "two_level_rigid":
+            ctx.coarse_modes(6)
+        if precond == "mpnn":
+            ctx.coarse_modes(learned_modes)
+            ctx.mpnn_init(seed=0, patch=patch)
+            ctx.mpnn_set_weights(weights if arm == "mpnn" else last_weights)
+        return ctx
+
     for arm in ("block_jacobi", "two_level", "two_level_rigid", "mpnn", "mpnn_last_epoch"):
         precond = {"two_level_rigid": "two_level", "mpnn_last_epoch": "mpnn"}.get(arm, arm)
-        with Context(device=local, precision="fp64") as ctx:
-            workloads.setup_context(ctx, w2)
-            if arm == "two_level_rigid":
-                ctx.coarse_modes(6)
-            if precond == "mpnn":
-                ctx.coarse_modes(learned_modes)
-                ctx.mpnn_init(seed=0, patch=patch)
-                ctx.mpnn_set_weights(weights if arm == "mpnn" else last_weights)
+        # warm-up: one untimed load step in a throwaway context of the same
+        # cube (first-use costs of kernels and of the full-size buffers)
+        with arm_context(arm, precond) as warm:
+            warm.qs_load_step(w2["times"][0], w2["times"][1], newton_tolerance=-1e-8, cg_relative_tolerance=1e-8,
+                              preconditioner=precond)
+        with arm_context(arm, precond) as ctx:
             st = None
             clocks = ClockSampler(local)
             clocks.start()
