@@ -4,6 +4,7 @@ profiler sees the tangent, preconditioner and reduction launches of a short
 CG solve.
 
     python -m peridigm_b200.qs_profile_run [--precond block_jacobi|two_level|mpnn] [--n 60] [--tol 1e-4]
+        [--coarse-modes 3|6]
 
 With --precond mpnn the learned middle level runs untrained (its starting
 weights): the launch sequence and its cost are those of a trained one.
@@ -22,10 +23,12 @@ def main():
     ap.add_argument("--n", type=int, default=60)
     ap.add_argument("--tol", type=float, default=1e-4)
     ap.add_argument("--patch", type=float, default=3.0e-3)
+    ap.add_argument("--coarse-modes", type=int, default=3, choices=[3, 6])
     a = ap.parse_args()
     w = workloads.qs_cube(n=a.n, h=1.0e-3, seed=1000, load_steps=20)
     with Context(precision="fp64") as ctx:
         workloads.setup_context(ctx, w)
+        ctx.coarse_modes(a.coarse_modes)
         if a.precond == "mpnn":
             ctx.mpnn_init(seed=0, patch=a.patch)
         st = ctx.qs_load_step(w["times"][0], w["times"][1], newton_tolerance=-1e-3, cg_relative_tolerance=a.tol,
