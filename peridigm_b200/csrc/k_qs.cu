@@ -33,6 +33,10 @@ namespace pdb {
 
 constexpr int kQsBlock = 256;
 constexpr int kQsTpo = 8;
+#ifndef PD_QS_BATCH
+#define PD_QS_BATCH 4
+#endif
+constexpr int kQsBatch = PD_QS_BATCH;  // bonds per lane in flight in the tangent passes
 constexpr int kRedBlocks = 296;  // 2 x 148 SMs: fixed, so reductions are deterministic
 
 struct QsState {
@@ -197,7 +201,22 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_dtheta_g(int64_t n, const int64
   double acc = 0.0;
   if (valid) {
     const double4 wi = w[i];
-    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
+    const int64_t b1 = row[i + 1];
+    int64_t b = row[i] + lane;
+    // batches of kQsBatch bonds per lane: stream loads, then gathers, then the
+    // sums in bond order (the same order as one bond at a time)
+    for (; b + (kQsBatch - 1) * kQsTpo < b1; b += kQsBatch * kQsTpo) {
+      double4 gb[kQsBatch], wj[kQsBatch];
+      int32_t j[kQsBatch];
+#pragma unroll
+      for (int k = 0; k < kQsBatch; ++k) gb[k] = g[b + k * kQsTpo], j[k] = col[b + k * kQsTpo];
+#pragma unroll
+      for (int k = 0; k < kQsBatch; ++k) wj[k] = w[j[k]];
+#pragma unroll
+      for (int k = 0; k < kQsBatch; ++k)
+        acc += gb[k].w * (gb[k].x * (wj[k].x - wi.x) + gb[k].y * (wj[k].y - wi.y) + gb[k].z * (wj[k].z - wi.z));
+    }
+    for (; b < b1; b += kQsTpo) {
       const double4 gb = g[b];
       const double4 wj = w[col[b]];
       acc += gb.w * (gb.x * (wj.x - wi.x) + gb.y * (wj.y - wi.y) + gb.z * (wj.z - wi.z));
@@ -227,17 +246,28 @@ __global__ void __launch_bounds__(kQsBlock) k_qs_df_g(int64_t n, const int64_t* 
   double4 wi = make_double4(0, 0, 0, 0);
   if (valid) {
     wi = w[i];
-    for (int64_t b = row[i] + lane; b < row[i + 1]; b += kQsTpo) {
-      const double4 gb = g[b];
-      const double2 cb = gc[b];
-      const double4 wj = w[col[b]];
+    const int64_t b1 = row[i + 1];
+    int64_t b = row[i] + lane;
+    auto bond = [&](const double4& gb, const double2& cb, const double4& wj) {
       const double w0 = wj.x - wi.x, w1 = wj.y - wi.y, w2 = wj.z - wi.z;
       const double de = gb.x * w0 + gb.y * w1 + gb.z * w2;
       const double sy = gb.w * (wi.w + wj.w) + (cb.y - cb.x) * de;
       d0 += sy * gb.x + cb.x * w0;
       d1 += sy * gb.y + cb.x * w1;
       d2 += sy * gb.z + cb.x * w2;
+    };
+    for (; b + (kQsBatch - 1) * kQsTpo < b1; b += kQsBatch * kQsTpo) {  // batched as in k_qs_dtheta_g
+      double4 gb[kQsBatch], wj[kQsBatch];
+      double2 cb[kQsBatch];
+      int32_t j[kQsBatch];
+#pragma unroll
+      for (int k = 0; k < kQsBatch; ++k) gb[k] = g[b + k * kQsTpo], cb[k] = gc[b + k * kQsTpo], j[k] = col[b + k * kQsTpo];
+#pragma unroll
+      for (int k = 0; k < kQsBatch; ++k) wj[k] = w[j[k]];
+#pragma unroll
+      for (int k = 0; k < kQsBatch; ++k) bond(gb[k], cb[k], wj[k]);
     }
+    for (; b < b1; b += kQsTpo) bond(g[b], gc[b], w[col[b]]);
   }
   d0 = qs_group_sum(d0);
   d1 = qs_group_sum(d1);
