@@ -136,9 +136,13 @@ __device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui,
 #define PD_BOND_UNROLL 4
 #endif
 #ifndef PD_BOND_MINB
-#define PD_BOND_MINB 4
+#define PD_BOND_MINB 8
 #endif
 constexpr int kUnroll = PD_BOND_UNROLL;
+// Threads per block of the split bond passes: 8 blocks of 128 fill an SM's
+// 1024 threads at 64 registers, and the last partial wave of a ~5000-block
+// grid costs half of what it does with 256-thread blocks.
+constexpr int kSplitBlock = 128;
 
 // Bond-stream cursor of a lane. CSR: the owner's row, the lane's bonds TPO
 // apart. Sliced (4 lanes per point, SELL): the bonds of the 8 owners of a
@@ -279,7 +283,7 @@ __global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* _
 // Writes the owner terms A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m into ur[i].
 // ---------------------------------------------------------------------------
 template <int TPO, bool SELL, bool LIN = false>
-__global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_dilatation_split(
+__global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const float4* __restrict__ bx, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
     double* __restrict__ theta_out, double* __restrict__ node_damage, const int64_t* __restrict__ soff,
@@ -503,7 +507,7 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
 template <int TPO, bool SELL, bool LIN = false, bool CHUNK = false>
-__global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
+__global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
                                                                       const int32_t* __restrict__ col,
                                                                       const uint8_t* __restrict__ dmg,
                                                                       const float4* __restrict__ bx,
@@ -863,7 +867,7 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
 // Split-FP32 path: one pass (bond stream and neighbor ids loaded directly as
 // in the LPS passes), damage and pair force per bond, FP64 epilogue.
 template <int TPO, bool SELL>
-__global__ void __launch_bounds__(kBlock, PD_BOND_MINB) k_bb_split(int64_t n, const int64_t* __restrict__ row,
+__global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t n, const int64_t* __restrict__ row,
                                                                    const int32_t* __restrict__ col,
                                                                    uint8_t* __restrict__ dmg,
                                                                    const float4* __restrict__ bx,
@@ -1045,13 +1049,16 @@ __global__ void k_min_reduce(int64_t m, const double* __restrict__ partial, doub
 // ---------------------------------------------------------------------------
 static inline unsigned grid_for(int64_t n, int tpo) { return (unsigned)((n * tpo + kBlock - 1) / kBlock); }
 static inline unsigned grid1(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+static inline unsigned grid_split(int64_t n, int tpo) {
+  return (unsigned)((n * tpo + kSplitBlock - 1) / kSplitBlock);
+}
 
-#define PD_DISPATCH_TPO_CSR(tpo, KERNEL, GRID, ...)                                  \
+#define PD_DISPATCH_TPO_CSR(tpo, KERNEL, GRID, BLOCK, ...)                          \
   switch (tpo) {                                                                     \
-    case 4: KERNEL<4, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;    \
-    case 8: KERNEL<8, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;    \
-    case 16: KERNEL<16, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;  \
-    default: KERNEL<32, false><<<GRID, kBlock, 0, c->stream>>>(__VA_ARGS__); break;  \
+    case 4: KERNEL<4, false><<<GRID, BLOCK, 0, c->stream>>>(__VA_ARGS__); break;     \
+    case 8: KERNEL<8, false><<<GRID, BLOCK, 0, c->stream>>>(__VA_ARGS__); break;     \
+    case 16: KERNEL<16, false><<<GRID, BLOCK, 0, c->stream>>>(__VA_ARGS__); break;   \
+    default: KERNEL<32, false><<<GRID, BLOCK, 0, c->stream>>>(__VA_ARGS__); break;   \
   }
 
 #define PD_DISPATCH_TPO(tpo, KERNEL, GRID, ...)                                      \
@@ -1106,7 +1113,7 @@ cudaError_t launch_pack_owner(pd_ctx* c) {
     c->sell_src = c->dmg.p;
     c->sell_gen = c->dmg_gen;
   } else {
-    PD_DISPATCH_TPO_CSR(c->tpo, k_pack_bonds, grid_for(n, c->tpo), n, c->row.p, c->col.p, c->xv.p, c->hp.p, infl,
+    PD_DISPATCH_TPO_CSR(c->tpo, k_pack_bonds, grid_for(n, c->tpo), kBlock, n, c->row.p, c->col.p, c->xv.p, c->hp.p, infl,
                         c->bx.p, nullptr, nullptr, nullptr, nullptr);
   }
   if (bb)
@@ -1157,7 +1164,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   if (c->n == 0) return cudaSuccess;
   const bool split = c->precision == PD_SPLIT_FP32;
   const int tpo = split ? c->tpo_split : c->tpo;
-  const unsigned grid = grid_for(c->n, tpo);
+  const unsigned grid = grid_for(c->n, tpo), sgrid = grid_split(c->n, tpo);
   cudaEvent_t* ev = nullptr;
   if (c->ktime) {
     if (c->kev_used + 3 > c->kev.size()) {
@@ -1205,11 +1212,11 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   if (c->material_model == PD_MATERIAL_BOND_BASED) {  // one pass: damage + pair force + epilogue
     if (ev) cudaEventRecord(ev[1], c->stream);
     if (sell) {
-      k_bb_split<4, true><<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p,
+      k_bb_split<4, true><<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p,
                                                           c->own.p, sp.damage_on, c->pt.p, c->node_damage.p, E, soff,
                                                           dmg);
     } else if (split) {
-      PD_DISPATCH_TPO_CSR(tpo, k_bb_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->own.p,
+      PD_DISPATCH_TPO_CSR(tpo, k_bb_split, sgrid, kSplitBlock, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->own.p,
                           sp.damage_on, c->pt.p, c->node_damage.p, E, nullptr, nullptr);
     } else {
       PD_DISPATCH_TPO(tpo, k_bb_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p, c->sc.p,
@@ -1220,11 +1227,11 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   }
   if (sell) {
     (c->material_model == PD_MATERIAL_LINEAR_LPS ? k_dilatation_split<4, true, true> : k_dilatation_split<4, true>)
-        <<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p,
+        <<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p,
                                                                 c->ur[c->cur].p, c->own.p, sp.damage_on, c->theta.p,
                                                                 c->node_damage.p, soff, dmg);
   } else if (split) {
-    PD_DISPATCH_TPO_CSR(tpo, k_dilatation_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
+    PD_DISPATCH_TPO_CSR(tpo, k_dilatation_split, sgrid, kSplitBlock, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
                         c->own.p, sp.damage_on, c->theta.p, c->node_damage.p, nullptr, nullptr);
   } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
     PD_DISPATCH_TPO(tpo, k_dilatation_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p,
@@ -1248,7 +1255,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       // memory holds the host until it is done)
       for (int64_t i0 = 0, k = 0; i0 < n; i0 += per, ++k) {
         const int64_t i1 = std::min(n, i0 + per);
-        kf<<<grid_for(i1 - i0, 4), kBlock, 0, c->stream>>>(i1, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p,
+        kf<<<grid_split(i1 - i0, 4), kSplitBlock, 0, c->stream>>>(i1, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p,
                                                            E, soff, i0);
         TRY_CUDA(cudaEventRecord(c->chunk_ev[k], c->stream));
       }
@@ -1263,10 +1270,10 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       *host_done = true;
     } else {
       auto* kf = lin ? k_force_split<4, true, true> : k_force_split<4, true>;
-      kf<<<grid, kBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E, soff, 0);
+      kf<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E, soff, 0);
     }
   } else if (split) {
-    PD_DISPATCH_TPO_CSR(tpo, k_force_split, grid, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
+    PD_DISPATCH_TPO_CSR(tpo, k_force_split, sgrid, kSplitBlock, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
                         nullptr);
   } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
     PD_DISPATCH_TPO(tpo, k_force_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
