@@ -383,6 +383,11 @@ int pd_mpnn_set_weights(pd_ctx* ctx, const float* weights);
  * With the coarse level on, z includes P0 Ac^-1 P0^T r of the current
  * displacement. */
 int pd_mpnn_loss_grad(pd_ctx* ctx, const float* pair, double* loss, float* grad);
+/* The middle level alone, z = Q S G^T G S Q^T r (host arrays [3n], prescribed
+ * dofs of z left zero), with S from the block-Jacobi blocks at the current
+ * displacement: the product each PD_PRECOND_MPNN CG iteration adds, for
+ * parity checks of the inference kernels. */
+int pd_mpnn_apply(pd_ctx* ctx, const double* r, double* z);
 /* Coarse level under the network (training, loss and PD_PRECOND_MPNN solves):
  * cell >= 0 puts the network on top of the two-level preconditioner with
  * aggregate cells of side max(cell, 2 * max horizon) (the default after

@@ -134,6 +134,7 @@ SIGNATURES = {
     "pd_mpnn_get_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "pd_mpnn_set_weights": (C.c_int, [_vp, C.POINTER(C.c_float)]),
     "pd_mpnn_loss_grad": (C.c_int, [_vp, C.POINTER(C.c_float), _dp, C.POINTER(C.c_float)]),
+    "pd_mpnn_apply": (C.c_int, [_vp, _dp, _dp]),
     "pd_mpnn_coarse": (C.c_int, [_vp, C.c_double]),
     "pd_block_data": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "pd_kinetic_energy": (C.c_int, [_vp, _dp, _dp]),

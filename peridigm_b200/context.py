@@ -355,6 +355,13 @@ class Context:
                                           g.ctypes.data_as(C.POINTER(C.c_float))))
         return loss.value, g
 
+    def mpnn_apply(self, r):
+        """Middle level of the learned preconditioner alone: Q S G^T G S Q^T r."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros(3 * self.n)
+        self._ok(self.L.pd_mpnn_apply(self.h, _d(r), _d(z)))
+        return z
+
     # -- compute classes --------------------------------------------------------
     def block_data(self, field, block, calculation="Sum"):
         """Block_Data compute class: "Minimum", "Maximum" or "Sum" of a field over a block (3 values)."""

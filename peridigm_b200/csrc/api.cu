@@ -869,6 +869,13 @@ int pd_mpnn_loss_grad(pd_ctx* c, const float* pair, double* loss, float* grad) {
   return mpnn_loss_grad(c, pair, loss, grad);
 }
 
+int pd_mpnn_apply(pd_ctx* c, const double* r, double* z) {
+  CHECK_CTX(c);
+  if (!r || !z) return fail(c, PD_ERR_ARG, "pd_mpnn_apply: null argument");
+  TRY(ensure_device(c));
+  return mpnn_middle_apply(c, r, z);
+}
+
 int pd_jacobian_apply(pd_ctx* c, const double* u, const double* w, double* kw) {
   CHECK_CTX(c);
   if (!u || !w || !kw) return fail(c, PD_ERR_ARG, "pd_jacobian_apply: null argument");

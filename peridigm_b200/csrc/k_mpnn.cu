@@ -54,8 +54,15 @@ constexpr int OFF_W0 = 0;       // W0 [H][3]
 constexpr int OFF_L = 3 * H;    // per layer: Ws [H][H], Wn [H][H]
 constexpr int LSZ = 2 * H * H;
 constexpr int NPARAM = OFF_L + NL * LSZ;
+// The BF16 copy holds the parameters in their own layout [0, NPARAM) and, from
+// OFF_KM, every layer's [Ws | Wn] again k-major ([l][part*H + k][o]), the
+// layout the forward layer multiplies in, so that its staging is a copy.
+constexpr int OFF_KM = NPARAM;
+constexpr int WB_SIZE = NPARAM + NL * LSZ;
+static_assert((OFF_L * 2) % 16 == 0 && (OFF_KM * 2) % 16 == 0 && (LSZ * 2) % 16 == 0,
+              "16-byte weight loads need 16-byte aligned layer offsets");
 constexpr int kRed = 148;
-constexpr int kTile = 32;       // patches per block tile of the layer kernels
+constexpr int kTile = 16;       // patches per block tile of the layer kernels (half a warp each)
 
 struct MpnnState {
   bool ready = false;    // weights initialised (trained or loaded)
@@ -81,7 +88,7 @@ struct MpnnState {
   int every = 0;
   std::vector<DBuf<double>*> snap_r, snap_x;
   int nsnap = 0;
-  // Inference apply (13 small launches) as one CUDA graph, captured for one
+  // Inference apply (10 small launches) as one CUDA graph, captured for one
   // (r, z, fixed mask) triple; the buffers it reads are fixed once the
   // patches are built, the weights and scales are read at replay.
   cudaGraphExec_t apply_exec = nullptr;
@@ -243,77 +250,108 @@ __global__ void k_pt_encode_t(int64_t np, const float* __restrict__ x, const __n
   if (lane == 0) out[3 * I] = s[0], out[3 * I + 1] = s[1], out[3 * I + 2] = s[2];
 }
 
+// Sum over the patch's neighbor rows J (CSR b0..b1) of x_J's features
+// 4hl..4hl+3 (half a warp per patch, 16 lanes x float4 = 64 features): eight
+// rows in flight, added in groups of four in row order.
+__device__ __forceinline__ float4 nbr_sum4(const float4* __restrict__ x4, const int32_t* __restrict__ pcol,
+                                           int64_t b0, int64_t b1, int hl, float4 a) {
+  auto add4 = [&](const float4& u0, const float4& u1, const float4& u2, const float4& u3) {
+    a.x += (u0.x + u1.x) + (u2.x + u3.x);
+    a.y += (u0.y + u1.y) + (u2.y + u3.y);
+    a.z += (u0.z + u1.z) + (u2.z + u3.z);
+    a.w += (u0.w + u1.w) + (u2.w + u3.w);
+  };
+  int64_t b = b0;
+  for (; b + 8 <= b1; b += 8) {
+    int32_t j[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) j[k] = pcol[b + k];
+    float4 u[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) u[k] = x4[(int64_t)(H / 4) * j[k] + hl];
+    add4(u[0], u[1], u[2], u[3]);
+    add4(u[4], u[5], u[6], u[7]);
+  }
+  if (b + 4 <= b1) {
+    const int32_t j0 = pcol[b], j1 = pcol[b + 1], j2 = pcol[b + 2], j3 = pcol[b + 3];
+    add4(x4[(int64_t)(H / 4) * j0 + hl], x4[(int64_t)(H / 4) * j1 + hl], x4[(int64_t)(H / 4) * j2 + hl],
+         x4[(int64_t)(H / 4) * j3 + hl]);
+    b += 4;
+  }
+  for (; b < b1; ++b) {
+    const float4 u = x4[(int64_t)(H / 4) * pcol[b] + hl];
+    a.x += u.x;
+    a.y += u.y;
+    a.z += u.z;
+    a.w += u.w;
+  }
+  return a;
+}
+
 // One layer: hout = hin + Ws hin + Wn mean_J hin_J (mout receives the mean).
-// Block tiles of 32 patches: phase 1 gathers [h | mean] rows into shared
-// memory (one warp per 4 patches, 2 features per lane), phase 2 multiplies by
-// [Ws | Wn] staged k-major in shared memory (8 outputs per thread, 16-byte
-// weight loads, FP32 accumulation).
+// Block tiles of 16 patches (256 threads): phase 1 copies the k-major
+// weights [Ws | Wn] into shared memory (16-byte loads, 4 per thread, all in
+// flight before the first store) and gathers [h | mean] rows (half a warp per
+// patch, 4 features per lane, eight neighbor rows in flight); phase 2
+// multiplies (4 outputs per thread, 8-byte weight reads, FP32 accumulation).
 __global__ void __launch_bounds__(256) k_pt_layer(int64_t np, const int64_t* __restrict__ prow,
                                                   const int32_t* __restrict__ pcol,
-                                                  const __nv_bfloat16* __restrict__ wl, const float* __restrict__ hin,
+                                                  const __nv_bfloat16* __restrict__ wk, const float* __restrict__ hin,
                                                   float* __restrict__ hout, float* __restrict__ mout) {
   __shared__ __align__(16) __nv_bfloat16 sW[2 * H][H + 8];  // sW[k][o] (rows padded: 144 B, 16-B aligned)
-  __shared__ float sX[kTile][2 * H + 1];
-  for (int t = threadIdx.x; t < 2 * H * H; t += blockDim.x) {  // coalesced read, transposed store
-    const int part = t / (H * H), o = (t % (H * H)) / H, k = t % H;
-    sW[part * H + k][o] = wl[t];
+  __shared__ __align__(16) float sX[kTile][2 * H + 4];
+  {
+    constexpr int kW16 = 2 * H * H / 8;  // 16-byte words of [Ws | Wn]
+    static_assert(kW16 == 4 * 256, "launched with 256 threads");
+    const uint4* w4 = reinterpret_cast<const uint4*>(wk);
+    uint4 wr[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) wr[q] = __ldg(w4 + threadIdx.x + 256 * q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t8 = threadIdx.x + 256 * q;
+      *reinterpret_cast<uint4*>(&sW[t8 / (H / 8)][(t8 % (H / 8)) * 8]) = wr[q];
+    }
   }
-  __syncthreads();
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nl = threadIdx.x >> 3, ob = (threadIdx.x & 7) * 8;
+  const int hl = threadIdx.x & 15, r = threadIdx.x >> 4;  // phase 1: patch r of the tile
+  const int nl = threadIdx.x >> 4, ob = (threadIdx.x & 15) * 4;  // phase 2: patch nl, outputs ob..ob+3
+  const float4* h4 = reinterpret_cast<const float4*>(hin);
   for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile) {
-    for (int q = 0; q < kTile / 8; ++q) {
-      const int r = wid * (kTile / 8) + q;
+    {
       const int64_t I = i0 + r;
-      float2 hv = make_float2(0.f, 0.f), mv = make_float2(0.f, 0.f);
+      float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), mv = make_float4(0.f, 0.f, 0.f, 0.f);
       if (I < np) {
-        hv = reinterpret_cast<const float2*>(hin)[(int64_t)(H / 2) * I + lane];
+        hv = h4[(int64_t)(H / 4) * I + hl];
         const int64_t b0 = prow[I], b1 = prow[I + 1];
-        const float2* h2 = reinterpret_cast<const float2*>(hin);
-        int64_t b = b0;
-        for (; b + 4 <= b1; b += 4) {  // four independent neighbor loads in flight
-          const int32_t j0 = pcol[b], j1 = pcol[b + 1], j2 = pcol[b + 2], j3 = pcol[b + 3];
-          const float2 u0 = h2[(int64_t)(H / 2) * j0 + lane], u1 = h2[(int64_t)(H / 2) * j1 + lane];
-          const float2 u2 = h2[(int64_t)(H / 2) * j2 + lane], u3 = h2[(int64_t)(H / 2) * j3 + lane];
-          mv.x += (u0.x + u1.x) + (u2.x + u3.x);
-          mv.y += (u0.y + u1.y) + (u2.y + u3.y);
-        }
-        for (; b < b1; ++b) {
-          const float2 u = h2[(int64_t)(H / 2) * pcol[b] + lane];
-          mv.x += u.x;
-          mv.y += u.y;
-        }
+        mv = nbr_sum4(h4, pcol, b0, b1, hl, mv);
         const float inv = b1 > b0 ? 1.0f / (float)(b1 - b0) : 0.0f;
         mv.x *= inv;
         mv.y *= inv;
-        if (mout) reinterpret_cast<float2*>(mout)[(int64_t)(H / 2) * I + lane] = mv;
+        mv.z *= inv;
+        mv.w *= inv;
+        if (mout) reinterpret_cast<float4*>(mout)[(int64_t)(H / 4) * I + hl] = mv;
       }
-      sX[r][2 * lane] = hv.x;
-      sX[r][2 * lane + 1] = hv.y;
-      sX[r][H + 2 * lane] = mv.x;
-      sX[r][H + 2 * lane + 1] = mv.y;
+      *reinterpret_cast<float4*>(&sX[r][4 * hl]) = hv;
+      *reinterpret_cast<float4*>(&sX[r][H + 4 * hl]) = mv;
     }
     __syncthreads();
-    float acc[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
-#pragma unroll 4
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
     for (int k = 0; k < 2 * H; ++k) {
       const float x = sX[nl][k];
-      const uint4 wv = *reinterpret_cast<const uint4*>(&sW[k][ob]);
+      const uint2 wv = *reinterpret_cast<const uint2*>(&sW[k][ob]);
       const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < 2; ++j) {
         const float2 f = __bfloat1622float2(w2[j]);
         acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
         acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
       }
     }
     const int64_t I = i0 + nl;
-    if (I < np) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) hout[(int64_t)H * I + ob + j] = sX[nl][ob + j] + acc[j];
-    }
+    if (I < np)
+      *reinterpret_cast<float4*>(hout + (int64_t)H * I + ob) =
+          make_float4(sX[nl][ob] + acc[0], sX[nl][ob + 1] + acc[1], sX[nl][ob + 2] + acc[2], sX[nl][ob + 3] + acc[3]);
     __syncthreads();
   }
 }
@@ -324,77 +362,159 @@ __global__ void __launch_bounds__(256) k_pt_layer_t(int64_t np, const int64_t* _
                                                     const __nv_bfloat16* __restrict__ wl, const float* __restrict__ d,
                                                     float* __restrict__ s_out, float* __restrict__ t_out) {
   __shared__ __align__(16) __nv_bfloat16 sW[H][2 * H];  // sW[o][k']: k' < H: Ws[o][k'], else Wn[o][k'-H]
-  __shared__ float sX[kTile][H + 1];
-  for (int t = threadIdx.x; t < 2 * H * H; t += blockDim.x) {
-    const int o = t / (2 * H), k = t % (2 * H);
-    sW[o][k] = k < H ? wl[o * H + k] : wl[H * H + o * H + (k - H)];
+  __shared__ __align__(16) float sX[kTile][H + 4];
+  {
+    constexpr int kW16 = 2 * H * H / 8;  // 16-byte words of [Ws | Wn] in their own layout
+    static_assert(kW16 == 4 * 256, "launched with 256 threads");
+    const uint4* w4 = reinterpret_cast<const uint4*>(wl);
+    uint4 wr[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) wr[q] = __ldg(w4 + threadIdx.x + 256 * q);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t8 = threadIdx.x + 256 * q;  // part, row o, 8-column segment
+      const int part = t8 / (H * H / 8), o = (t8 % (H * H / 8)) / (H / 8), seg = t8 % (H / 8);
+      *reinterpret_cast<uint4*>(&sW[o][part * H + seg * 8]) = wr[q];
+    }
   }
-  __syncthreads();
-  const int nl = threadIdx.x >> 3, ob = (threadIdx.x & 7) * 16;
+  const int nl = threadIdx.x >> 4, ob = (threadIdx.x & 15) * 8;  // patch nl, outputs ob..ob+7 of [s | t]
+  const float4* d4 = reinterpret_cast<const float4*>(d);
   for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile) {
-    for (int t = threadIdx.x; t < kTile * H; t += blockDim.x) {
-      const int r = t / H, o = t % H;
+#pragma unroll
+    for (int q = 0; q < kTile * H / 4 / 256; ++q) {
+      const int t = threadIdx.x + 256 * q, r = t / (H / 4), o4 = t % (H / 4);
       const int64_t I = i0 + r;
-      sX[r][o] = I < np ? d[(int64_t)H * I + o] : 0.f;
+      *reinterpret_cast<float4*>(&sX[r][4 * o4]) = I < np ? d4[(int64_t)(H / 4) * I + o4] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
-    float acc[16];
+    float acc[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) acc[j] = 0.f;
+    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
 #pragma unroll 4
     for (int o = 0; o < H; ++o) {
       const float x = sX[nl][o];
+      const uint4 wv = *reinterpret_cast<const uint4*>(&sW[o][ob]);
+      const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
 #pragma unroll
-      for (int half = 0; half < 2; ++half) {
-        const uint4 wv = *reinterpret_cast<const uint4*>(&sW[o][ob + 8 * half]);
-        const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const float2 f = __bfloat1622float2(w2[j]);
-          acc[8 * half + 2 * j] = fmaf(x, f.x, acc[8 * half + 2 * j]);
-          acc[8 * half + 2 * j + 1] = fmaf(x, f.y, acc[8 * half + 2 * j + 1]);
-        }
+      for (int j = 0; j < 4; ++j) {
+        const float2 f = __bfloat1622float2(w2[j]);
+        acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
+        acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
       }
     }
     const int64_t I = i0 + nl;
-    if (I < np) {
-      const int64_t deg = prow[I + 1] - prow[I];
-      const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
+    if (I < np) {  // the 8 outputs lie in one part: s (ob < H) or t
+      float4* o4;
+      float v[8];
+      if (ob < H) {
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int k = ob + j;
-        if (k < H) s_out[(int64_t)H * I + k] = sX[nl][k] + acc[j];
-        else t_out[(int64_t)H * I + (k - H)] = acc[j] * inv;
+        for (int j = 0; j < 8; ++j) v[j] = sX[nl][ob + j] + acc[j];
+        o4 = reinterpret_cast<float4*>(s_out + (int64_t)H * I + ob);
+      } else {
+        const int64_t deg = prow[I + 1] - prow[I];
+        const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = acc[j] * inv;
+        o4 = reinterpret_cast<float4*>(t_out + (int64_t)H * I + (ob - H));
       }
+      o4[0] = make_float4(v[0], v[1], v[2], v[3]);
+      o4[1] = make_float4(v[4], v[5], v[6], v[7]);
     }
     __syncthreads();
   }
 }
 
-// x_J = s_J + sum_{I in N(J)} t_I  (warp per patch, 2 features per lane)
-__global__ void __launch_bounds__(256) k_pt_gather_t(int64_t np, const int64_t* __restrict__ prow,
-                                                     const int32_t* __restrict__ pcol, const float* __restrict__ s,
-                                                     const float* __restrict__ t, float* __restrict__ x) {
-  const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// x_J = s_J + sum_{I in N(J)} t_I  (half a warp per patch, 4 features per lane)
+__global__ void k_pt_gather_t(int64_t np, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+                              const float* __restrict__ s, const float* __restrict__ t, float* __restrict__ x) {
+  const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+  const int hl = threadIdx.x & 15;
+  if (J >= np) return;  // no shuffles below: each half warp may leave on its own
+  float4 a = reinterpret_cast<const float4*>(s)[(int64_t)(H / 4) * J + hl];
+  a = nbr_sum4(reinterpret_cast<const float4*>(t), pcol, prow[J], prow[J + 1], hl, a);
+  reinterpret_cast<float4*>(x)[(int64_t)(H / 4) * J + hl] = a;
+}
+
+// Inference head, restrict then encode: v_I = s_I sum_{i in I, free} r_i,
+// h0_I = W0 v_I (warp per patch; the same sums in the same order as
+// k_pt_restrict and k_pt_encode).
+__global__ void __launch_bounds__(256) k_pt_head(int64_t np, const int32_t* __restrict__ patch_cell,
+                                                 const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
+                                                 const double* __restrict__ r, const uint8_t* __restrict__ fixed,
+                                                 const float* __restrict__ scale, const __nv_bfloat16* __restrict__ wb,
+                                                 float* __restrict__ h0) {
+  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (J >= np) return;
-  const float2* t2 = reinterpret_cast<const float2*>(t);
-  float2 a = reinterpret_cast<const float2*>(s)[(int64_t)(H / 2) * J + lane];
-  const int64_t b1 = prow[J + 1];
-  int64_t b = prow[J];
-  for (; b + 4 <= b1; b += 4) {
-    const int32_t j0 = pcol[b], j1 = pcol[b + 1], j2 = pcol[b + 2], j3 = pcol[b + 3];
-    const float2 u0 = t2[(int64_t)(H / 2) * j0 + lane], u1 = t2[(int64_t)(H / 2) * j1 + lane];
-    const float2 u2 = t2[(int64_t)(H / 2) * j2 + lane], u3 = t2[(int64_t)(H / 2) * j3 + lane];
-    a.x += (u0.x + u1.x) + (u2.x + u3.x);
-    a.y += (u0.y + u1.y) + (u2.y + u3.y);
+  if (I >= np) return;
+  const int q = patch_cell[I];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+    const int64_t p = sorted[t];
+    const uint8_t f = fixed ? fixed[p] : 0;
+    if (!(f & 1)) s0 += r[3 * p];
+    if (!(f & 2)) s1 += r[3 * p + 1];
+    if (!(f & 4)) s2 += r[3 * p + 2];
   }
-  for (; b < b1; ++b) {
-    const float2 u = t2[(int64_t)(H / 2) * pcol[b] + lane];
-    a.x += u.x;
-    a.y += u.y;
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
   }
-  reinterpret_cast<float2*>(x)[(int64_t)(H / 2) * J + lane] = a;
+  // lane 0's sums (the butterfly leaves each lane its own rounding)
+  s0 = __shfl_sync(0xffffffffu, s0, 0);
+  s1 = __shfl_sync(0xffffffffu, s1, 0);
+  s2 = __shfl_sync(0xffffffffu, s2, 0);
+  const double sc = 1.0 * (double)scale[I];
+  const float v[3] = {(float)(sc * s0), (float)(sc * s1), (float)(sc * s2)};
+  float2 h;
+  {
+    const int o = 2 * lane;
+    float a = 0.f, b = 0.f;
+    for (int c = 0; c < 3; ++c) a = fmaf(__bfloat162float(wb[OFF_W0 + 3 * o + c]), v[c], a);
+    for (int c = 0; c < 3; ++c) b = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 1) + c]), v[c], b);
+    h = make_float2(a, b);
+  }
+  reinterpret_cast<float2*>(h0)[(int64_t)(H / 2) * I + lane] = h;
+}
+
+// Inference tail, the last transposed gather, W0^T and the prolongation:
+// x_J = s_J + sum_{I in N(J)} t_I, out_J = W0^T x_J, z_i += s_J out_J on the
+// free dofs of J's points (half a warp per patch; a half warp past np keeps
+// to the shuffles and touches no memory).
+__global__ void k_pt_tail(int64_t np, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
+                          const float* __restrict__ s, const float* __restrict__ t,
+                          const __nv_bfloat16* __restrict__ wb, const int32_t* __restrict__ patch_cell,
+                          const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
+                          const float* __restrict__ scale, const uint8_t* __restrict__ fixed, double* __restrict__ z) {
+  const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+  const int hl = threadIdx.x & 15;
+  if (((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) >> 4 >= np) return;  // whole warp past np
+  const bool live = J < np;
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (live) {
+    a = reinterpret_cast<const float4*>(s)[(int64_t)(H / 4) * J + hl];
+    a = nbr_sum4(reinterpret_cast<const float4*>(t), pcol, prow[J], prow[J + 1], hl, a);
+  }
+  auto w0t = [&](int c) {  // sum over the 64 features of W0[o][c] x_o
+    const int o = 4 * hl;
+    float v = __bfloat162float(wb[OFF_W0 + 3 * o + c]) * a.x;
+    v = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 1) + c]), a.y, v);
+    v = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 2) + c]), a.z, v);
+    v = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 3) + c]), a.w, v);
+    for (int k = 8; k > 0; k >>= 1) v += __shfl_xor_sync(0xffffffffu, v, k, 16);
+    return (double)__shfl_sync(0xffffffffu, v, 0, 16);  // the half warp's first lane
+  };
+  const double out0 = w0t(0), out1 = w0t(1), out2 = w0t(2);
+  if (!live) return;
+  const double sc = 1.0 * (double)scale[J];
+  const int q = patch_cell[J];
+  for (int64_t k = cstart[q] + hl; k < cstart[q + 1]; k += 16) {
+    const int64_t p = sorted[k];
+    const uint8_t f = fixed ? fixed[p] : 0;
+    if (!(f & 1)) z[3 * p] += sc * out0;
+    if (!(f & 2)) z[3 * p + 1] += sc * out1;
+    if (!(f & 4)) z[3 * p + 2] += sc * out2;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -431,6 +551,18 @@ __global__ void k_pt_wgrad_reduce(int nblk, int entries, const float* __restrict
   }
 }
 
+// BF16 weight k into both places it lives (its own layout; for a layer weight
+// also the k-major copy at OFF_KM).
+__device__ __forceinline__ void put_wb(int k, float x, __nv_bfloat16* __restrict__ wb) {
+  const __nv_bfloat16 b = __float2bfloat16(x);
+  wb[k] = b;
+  if (k >= OFF_L) {
+    const int r = k - OFF_L, l = r / LSZ, q = r % LSZ;
+    const int part = q / (H * H), o = (q % (H * H)) / H, kk = q % H;
+    wb[OFF_KM + l * LSZ + (part * H + kk) * H + o] = b;
+  }
+}
+
 __global__ void k_mp_adam(int np, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
                           float* __restrict__ v, float lr, float b1, float b2, float c1, float c2, float scale,
                           __nv_bfloat16* __restrict__ wb) {
@@ -440,12 +572,12 @@ __global__ void k_mp_adam(int np, float* __restrict__ w, const float* __restrict
   m[k] = b1 * m[k] + (1.f - b1) * gk;
   v[k] = b2 * v[k] + (1.f - b2) * gk * gk;
   w[k] -= lr * (m[k] / c1) / (sqrtf(v[k] / c2) + 1e-8f);
-  wb[k] = __float2bfloat16(w[k]);
+  put_wb(k, w[k], wb);
 }
 
 __global__ void k_mp_cast(int np, const float* __restrict__ w, __nv_bfloat16* __restrict__ wb) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < np) wb[k] = __float2bfloat16(w[k]);
+  if (k < np) put_wb(k, w[k], wb);
 }
 
 // z = a (FP64 from float), prescribed dofs zero
@@ -533,6 +665,7 @@ __global__ void k_mp_make_pair(int64_t n, const double* __restrict__ dinv, const
 // ---------------------------------------------------------------------------
 static unsigned gw(int64_t n) { return (unsigned)((n * 32 + 255) / 256); }
 static unsigned g1(int64_t n) { return (unsigned)((n + 255) / 256); }
+static unsigned gh(int64_t n) { return (unsigned)((n * 16 + 255) / 256); }  // half a warp per patch
 static unsigned gtile(int64_t np) { return (unsigned)std::min<int64_t>((np + kTile - 1) / kTile, 148 * 8); }
 
 static MpnnState* mp_state(pd_ctx* c) { return reinterpret_cast<MpnnState*>(c->mpnn); }
@@ -625,7 +758,7 @@ int mpnn_init(pd_ctx* c, uint64_t seed, double patch) {
   for (int l = 0; l < NL; ++l)
     for (int k = 0; k < LSZ; ++k) w[OFF_L + l * LSZ + k] = uni(0.01f);
   PD_CUDA_TRY(c, s->w.alloc(NPARAM));
-  PD_CUDA_TRY(c, s->wb.alloc(NPARAM));
+  PD_CUDA_TRY(c, s->wb.alloc(WB_SIZE));
   PD_CUDA_TRY(c, s->g_.alloc(NPARAM));
   PD_CUDA_TRY(c, s->am.alloc(NPARAM));
   PD_CUDA_TRY(c, s->av.alloc(NPARAM));
@@ -666,7 +799,7 @@ static int mp_forward(pd_ctx* c, MpnnState* s, int k, bool save) {
   const int64_t np = s->np;
   k_pt_encode<<<g1(np * H), 256, 0, c->stream>>>(np, s->v[k].p, s->wb.p, s->h[k][0].p);
   for (int l = 0; l < NL; ++l)
-    k_pt_layer<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->wb.p + OFF_L + l * LSZ, s->h[k][l].p,
+    k_pt_layer<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->wb.p + OFF_KM + l * LSZ, s->h[k][l].p,
                                                  s->h[k][l + 1].p, save ? s->m[k][l].p : nullptr);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
@@ -679,7 +812,7 @@ static int mp_transpose(pd_ctx* c, MpnnState* s, const float* y) {
   for (int l = NL - 1; l >= 0; --l) {
     k_pt_layer_t<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->wb.p + OFF_L + l * LSZ, cur, s->s_buf.p,
                                                    s->t_buf.p);
-    k_pt_gather_t<<<gw(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
+    k_pt_gather_t<<<gh(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
     cur = s->d.p;
   }
   k_pt_encode_t<<<gw(np), 256, 0, c->stream>>>(np, cur, s->wb.p, s->out3.p);
@@ -701,7 +834,7 @@ static int mp_backward(pd_ctx* c, MpnnState* s, int k, const float* U) {
     mp_wgrad(c, s, H, cur, s->m[k][l].p, OFF_L + l * LSZ + H * H);
     k_pt_layer_t<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->wb.p + OFF_L + l * LSZ, cur, s->s_buf.p,
                                                    s->t_buf.p);
-    k_pt_gather_t<<<gw(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
+    k_pt_gather_t<<<gh(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
     cur = s->d.p;
   }
   mp_wgrad(c, s, 3, cur, s->v[k].p, OFF_W0);
@@ -709,12 +842,26 @@ static int mp_backward(pd_ctx* c, MpnnState* s, int k, const float* U) {
   return PD_OK;
 }
 
+// z += Q S G^T G S Q^T r: head (restrict + W0), 3 layers, 3 transposed
+// layers with 2 gathers between them, tail (gather + W0^T + prolongation).
 static int mp_apply_launches(pd_ctx* c, MpnnState* s, const double* r, double* z, const uint8_t* fixed) {
-  k_pt_restrict<double><<<gw(s->np), 256, 0, c->stream>>>(s->np, s->patch_cell.p, s->cstart.p, s->sorted.p, r, fixed,
-                                                          s->scale.p, 1.0, s->v[0].p);
-  TRY_RC(mp_forward(c, s, 0, false));
-  TRY_RC(mp_transpose(c, s, s->h[0][NL].p));
-  k_pt_prolong<<<g1(c->n), 256, 0, c->stream>>>(c->n, s->pid.p, s->out3.p, s->scale.p, 1.0, fixed, z);
+  const int64_t np = s->np;
+  k_pt_head<<<gw(np), 256, 0, c->stream>>>(np, s->patch_cell.p, s->cstart.p, s->sorted.p, r, fixed, s->scale.p,
+                                           s->wb.p, s->h[0][0].p);
+  for (int l = 0; l < NL; ++l)
+    k_pt_layer<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->wb.p + OFF_KM + l * LSZ, s->h[0][l].p,
+                                                 s->h[0][l + 1].p, nullptr);
+  const float* cur = s->h[0][NL].p;
+  for (int l = NL - 1; l >= 0; --l) {
+    k_pt_layer_t<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->wb.p + OFF_L + l * LSZ, cur, s->s_buf.p,
+                                                   s->t_buf.p);
+    if (l > 0) {
+      k_pt_gather_t<<<gh(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
+      cur = s->d.p;
+    }
+  }
+  k_pt_tail<<<gh(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->wb.p,
+                                           s->patch_cell.p, s->cstart.p, s->sorted.p, s->scale.p, fixed, z);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
 }
@@ -821,6 +968,31 @@ int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_
   PD_CUDA_TRY(c, cudaMemsetAsync(s->g_.p, 0, NPARAM * sizeof(float), c->stream));
   TRY_RC(mp_pair_grad(c, s, pair.p, 1.0, loss));
   if (grad_host) PD_CUDA_TRY(c, d2h(c, grad_host, s->g_.p, NPARAM * sizeof(float)));
+  return PD_OK;
+}
+
+// z = Q S G^T G S Q^T r (the middle level alone, host arrays [3n]) with the
+// scales of the current displacement's block-Jacobi blocks, through the same
+// graph-replayed apply the CG iterations use.
+int mpnn_middle_apply(pd_ctx* c, const double* r_host, double* z_host) {
+  MpnnState* s = mp_state(c);
+  if (!s || !s->ready || !s->patches || s->n != c->n) {
+    c->err = "learned preconditioner not initialised";
+    return PD_ERR_STATE;
+  }
+  TRY_RC(qs_prepare_current(c));
+  const double* dinv = nullptr;
+  TRY_RC(qs_block_jacobi_current(c, &dinv));
+  TRY_RC(mpnn_prepare(c, dinv));
+  const size_t b3 = 3 * (size_t)c->n * sizeof(double);
+  DBuf<double> r, z;
+  PD_CUDA_TRY(c, r.alloc(3 * c->n));
+  PD_CUDA_TRY(c, z.alloc(3 * c->n));
+  PD_CUDA_TRY(c, h2d(c, r.p, r_host, b3));
+  PD_CUDA_TRY(c, dzero(c, z.p, b3));
+  TRY_RC(mpnn_apply_add(c, r.p, z.p));
+  PD_CUDA_TRY(c, d2h(c, z_host, z.p, b3));
+  s->drop_graph();  // captured for the buffers freed on return
   return PD_OK;
 }
 

@@ -250,6 +250,7 @@ void mpnn_release(pd_ctx* c);
 int mpnn_init(pd_ctx* c, uint64_t seed, double patch);
 int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out);
 int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_host);
+int mpnn_middle_apply(pd_ctx* c, const double* r_host, double* z_host);
 int mpnn_set_capture(pd_ctx* c, int every);
 int mpnn_capture_every(const pd_ctx* c);
 int mpnn_snapshot(pd_ctx* c, const double* r, const double* x);

@@ -6,6 +6,8 @@ gains inside the quasi-static CG.
   vs oracle/mpnn.py with the oracle's dense tangent, the device's block-Jacobi
   blocks and coarse operator, on the same BF16 weights: loss to 1e-4
   relative, gradient to 2e-2 relative L2 (FP32 vs FP64 sums);
+* pd_mpnn_apply (the inference graph) vs the oracle's Q S G^T G S Q^T r, and
+  bit-identical on a second call;
 * two-level QS solves with capture produce pairs, and training lowers the loss;
 * the trained preconditioner solves a held-out QS problem to the two-level
   displacement (1e-8 relative) in fewer CG iterations than the same
@@ -64,6 +66,41 @@ def test_mpnn_gradient_matches_oracle(coarse):
     Lr, gr = M.loss_grad(wts, a, r, e, K, dofs, pid, nbrs, scale, z0=z0)
     assert abs(L - Lr) <= 1e-4 * abs(Lr)
     assert np.linalg.norm(g - gr) <= 2e-2 * np.linalg.norm(gr)
+
+
+@pytest.mark.parametrize("seed", [6, 9])
+def test_mpnn_apply_matches_oracle(seed):
+    """The inference product each learned CG iteration adds (head, 3 layers,
+    3 transposed layers, tail: one replayed graph) against the oracle's
+    Q S G^T G S Q^T r on the same BF16 weights (FP32 activations: 1e-5)."""
+    w = _bar(seed=seed)
+    n = len(w["vol"])
+    h = w["h"]
+    dofs = sorted({3 * int(p) + b["coordinate"] for b in w["bcs"] for p in b["points"]})
+    rng = np.random.default_rng(seed)
+    wts = (rng.standard_normal(M.NPARAM) * 0.08).astype(np.float32)
+    r = rng.standard_normal(3 * n)
+    with Context(precision="fp64") as ctx:
+        workloads.setup_context(ctx, w)
+        ctx.mpnn_init(seed=3, patch=2.0 * h)
+        ctx.mpnn_set_weights(wts)
+        blocks = ctx.jacobian_blocks(np.zeros(3 * n))
+        z = ctx.mpnn_apply(r)
+        z2 = ctx.mpnn_apply(r)
+    pid, nbrs = M.patches(w["x"], 2.0 * h)
+    npatch = int(pid.max()) + 1
+    scale = M.scales(np.linalg.inv(blocks), pid, dofs)
+    fixed = np.zeros(3 * n, bool)
+    fixed[dofs] = True
+    Am = M._mean_matrix(nbrs)
+    Q = M._q(pid, fixed, npatch)
+    S = np.repeat(np.asarray(scale, np.float64), 3)
+    wb = M.bf16(wts).astype(np.float64)
+    y, _ = M.forward(wb, (S * (Q.T @ r)).reshape(npatch, 3), Am)
+    zr = Q @ (S * M.transpose(wb, y, Am).ravel())
+    assert np.all(z[fixed] == 0.0)
+    assert np.array_equal(z, z2)
+    assert np.linalg.norm(z - zr) <= 1e-5 * np.linalg.norm(zr)
 
 
 def test_mpnn_trains_and_helps_cg():
