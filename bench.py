@@ -49,10 +49,10 @@ def algorithmic_bytes(nb, n, precision="split"):
 
 # DRAM bytes (read + write) per launch of the split bond passes on this
 # workload, from one ncu capture (--set full, step 1 of the notched plate,
-# sliced bond stream): k_dilatation_split<4> 586.0 MB read + 5.2 MB written,
-# k_force_split<4> 606.1 MB read + 9.2 MB written. The excess over the
+# sliced bond stream, 128-thread blocks): k_dilatation_split<4> 586.0 MB read
+# + 7.7 MB written, k_force_split<4> 605.8 MB read + 8.0 MB written. The excess over the
 # algorithmic bytes is the slices' padding records (6.3 % of the slots).
-NCU_TRAFFIC = {"dilatation": 591.2e6, "force": 615.3e6}
+NCU_TRAFFIC = {"dilatation": 593.7e6, "force": 613.9e6}
 
 
 class ClockSampler:
