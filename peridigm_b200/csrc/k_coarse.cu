@@ -65,7 +65,7 @@ struct CoarseState {
   DBuf<int64_t> cstart;
   DBuf<double> slots;      // [n][8][15]
   DBuf<double> A;          // nc x nc, the inverse after coarse_build
-  DBuf<double> P, R, C;    // Gauss-Jordan work
+  DBuf<double> P, R, C;    // Gauss-Jordan work: pivot inverse, row panel, column panel (transposed)
   DBuf<double> rc, zc;
   DBuf<int> status;
   DBuf<double> center, T;   // rigid modes: aggregate centers [4 nagg], orthonormalising transforms [36 nagg]
@@ -260,11 +260,17 @@ __global__ void k_coarse_agg_of(int64_t n, const double4* __restrict__ xv, Grid 
 // Dense SPD inverse: blocked in-place Gauss-Jordan (no pivoting), 64-wide steps
 //   P = A_kk^-1; R = P A_k* (new block row); C = A_*k (old block column);
 //   A_ij -= C_i R_j (i, j outside block k); A_kj = R_j; A_ik = -C_i P; A_kk = P
+// With P written into R's block-k columns, every row outside block k takes
+// A_ij = [j outside block k] A_ij - C_i R_j, and the rows of block k take R.
 // ---------------------------------------------------------------------------
-// P = inverse of the bk x bk diagonal block at k0 (one block of 256 threads).
+// P = inverse of the bk x bk diagonal block at k0 (one block of 256 threads;
+// each elimination step reads the old row and column k, then writes: two
+// barriers a step).
 __global__ void __launch_bounds__(256) k_gj_pivot(int nc, int k0, int bk, const double* __restrict__ A,
                                                   double* __restrict__ P) {
   __shared__ double S[kGjB][kGjB + 1];
+  constexpr int kPer = kGjB * kGjB / 256;
+  static_assert(kPer * 256 == kGjB * kGjB, "launched with 256 threads");
   for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
     const int r = t / kGjB, c = t % kGjB;
     S[r][c] = (r < bk && c < bk) ? A[(size_t)(k0 + r) * nc + k0 + c] : 0.0;
@@ -272,36 +278,56 @@ __global__ void __launch_bounds__(256) k_gj_pivot(int nc, int k0, int bk, const 
   __syncthreads();
   for (int k = 0; k < bk; ++k) {
     const double p = 1.0 / S[k][k];
-    __syncthreads();
-    for (int c = threadIdx.x; c < bk; c += blockDim.x) S[k][c] = (c == k) ? p : S[k][c] * p;
-    __syncthreads();
-    for (int t = threadIdx.x; t < bk * bk; t += blockDim.x) {
-      const int r = t / bk, c = t % bk;
-      if (r != k && c != k) S[r][c] -= S[r][k] * S[k][c];
+    double nv[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int t = threadIdx.x + 256 * q, r = t / kGjB, c = t % kGjB;
+      double v = S[r][c];
+      if (r < bk && c < bk) {
+        if (r == k) {
+          v = (c == k) ? p : S[k][c] * p;
+        } else if (c == k) {
+          v = -S[r][k] * p;
+        } else {
+          const double nkc = S[k][c] * p;  // the new row k
+          v = S[r][c] - S[r][k] * nkc;
+        }
+      }
+      nv[q] = v;
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < bk; r += blockDim.x)
-      if (r != k) S[r][k] = -S[r][k] * p;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      const int t = threadIdx.x + 256 * q;
+      S[t / kGjB][t % kGjB] = nv[q];
+    }
     __syncthreads();
   }
   for (int t = threadIdx.x; t < bk * bk; t += blockDim.x) P[t] = S[t / bk][t % bk];
 }
 
-// R[r][j] = sum_t P[r][t] A[k0+t][j] (bk x nc); C[i][t] = A[i][k0+t] (nc x bk).
-// Block x: 64 columns j (R) or 64 rows i (C, blocks past the R range).
+// R[r][j] = sum_t P[r][t] A[k0+t][j] (bk x nc; P itself in the block-k
+// columns); Ct[t][i] = A[i][k0+t] (bk x nc: the old block column, transposed
+// through shared memory). Block x: 64 columns j (R) or 64 rows i (Ct, blocks
+// past the R range).
 __global__ void __launch_bounds__(256) k_gj_panel(int nc, int k0, int bk, const double* __restrict__ A,
                                                   const double* __restrict__ P, double* __restrict__ R,
-                                                  double* __restrict__ C) {
+                                                  double* __restrict__ Ct) {
   const int ntile = (nc + kGjB - 1) / kGjB;
-  if ((int)blockIdx.x >= ntile) {  // copy the old block column
+  __shared__ double sP[kGjB][kGjB + 1];
+  if ((int)blockIdx.x >= ntile) {  // the old block column
     const int i0 = ((int)blockIdx.x - ntile) * kGjB;
-    for (int t = threadIdx.x; t < kGjB * bk; t += blockDim.x) {
-      const int i = i0 + t / bk, c = t % bk;
-      if (i < nc) C[(size_t)i * bk + c] = A[(size_t)i * nc + k0 + c];
+    for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+      const int r = t / kGjB, c = t % kGjB;
+      sP[r][c] = (i0 + r < nc && c < bk) ? A[(size_t)(i0 + r) * nc + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+      const int c = t / kGjB, r = t % kGjB;
+      if (c < bk && i0 + r < nc) Ct[(size_t)c * nc + i0 + r] = sP[r][c];
     }
     return;
   }
-  __shared__ double sP[kGjB][kGjB + 1];
   const int j0 = blockIdx.x * kGjB;
   for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
     const int r = t / kGjB, c = t % kGjB;
@@ -310,68 +336,111 @@ __global__ void __launch_bounds__(256) k_gj_panel(int nc, int k0, int bk, const 
   __syncthreads();
   for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
     const int r = t / kGjB, c = t % kGjB;
-    if (r >= bk || j0 + c >= nc) continue;
-    const double* a = A + (size_t)k0 * nc + j0 + c;
+    const int j = j0 + c;
+    if (r >= bk || j >= nc) continue;
+    if (j >= k0 && j < k0 + bk) {
+      R[(size_t)r * nc + j] = sP[r][j - k0];
+      continue;
+    }
+    const double* a = A + (size_t)k0 * nc + j;
     double s = 0.0;
     for (int k = 0; k < bk; ++k) s = fma(sP[r][k], a[(size_t)k * nc], s);
-    R[(size_t)r * nc + j0 + c] = s;
+    R[(size_t)r * nc + j] = s;
   }
 }
 
-// 64x64 output tiles, 4x4 per thread, k in chunks of 16.
-__global__ void __launch_bounds__(256) k_gj_update(int nc, int k0, int bk, double* __restrict__ A,
-                                                   const double* __restrict__ P, const double* __restrict__ R,
-                                                   const double* __restrict__ C) {
-  const int i0 = blockIdx.y * kGjB, j0 = blockIdx.x * kGjB;
-  const bool rowk = (i0 == k0), colk = (j0 == k0);
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  if (rowk) {  // new block row (and the pivot block)
-    for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
-      const int r = t / kGjB, c = t % kGjB;
-      if (r < bk && j0 + c < nc) A[(size_t)(i0 + r) * nc + j0 + c] = colk ? P[r * bk + c] : R[(size_t)r * nc + j0 + c];
-    }
-    return;
+// Trailing update on 128x128 tiles, 8x8 per thread (rows ty + 16a, columns
+// tx + 16b), one block per SM. The block's A tile goes to shared memory by
+// cp.async at the start (read back for the final A - C R), and the two bk x nc
+// panels come in k chunks of 16, double-buffered by cp.async, so that no load
+// latency sits between the FP64 fma chains. Sums over t in order, one fma chain.
+constexpr int kUT = 128, kUK = 16;
+constexpr size_t kUpdSmem = (size_t)(kUT * kUT + 4 * kUK * kUT) * sizeof(double);  // 192 KiB
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, double* __restrict__ A,
+                                                      const double* __restrict__ R, const double* __restrict__ Ct) {
+  extern __shared__ __align__(16) double smem[];
+  double* sA = smem;                   // [kUT][kUT]
+  double* sC = smem + kUT * kUT;       // [2][kUK][kUT]
+  double* sR = sC + 2 * kUK * kUT;     // [2][kUK][kUT]
+  const int i0 = blockIdx.y * kUT, j0 = blockIdx.x * kUT;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int t = threadIdx.x; t < kUT * kUT; t += blockDim.x) {  // group 0: the A tile
+    const int r = t / kUT, x = t % kUT;
+    if (i0 + r < nc && j0 + x < nc) cp_async8(sA + t, A + (size_t)(i0 + r) * nc + j0 + x);
   }
-  __shared__ double sC[kGjB][17], sR[16][kGjB + 1];
-  double acc[4][4];
+  cp_async_commit();
+  auto stage = [&](int buf, int kc) {  // one group per chunk; zeros past the edges
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+    for (int q = 0; q < kUK * kUT / 256; ++q) {
+      const int t = threadIdx.x + 256 * q, k = t / kUT, x = t % kUT;
+      double* dc = sC + (buf * kUK + k) * kUT + x;
+      double* dr = sR + (buf * kUK + k) * kUT + x;
+      const bool kin = kc + k < bk;
+      if (kin && i0 + x < nc) cp_async8(dc, Ct + (size_t)(kc + k) * nc + i0 + x);
+      else *dc = 0.0;
+      if (kin && j0 + x < nc) cp_async8(dr, R + (size_t)(kc + k) * nc + j0 + x);
+      else *dr = 0.0;
+    }
+    cp_async_commit();
+  };
+  double acc[8][8];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int kc = 0; kc < bk; kc += 16) {
-    for (int t = threadIdx.x; t < kGjB * 16; t += blockDim.x) {
-      const int r = t / 16, k = t % 16;
-      sC[r][k] = (i0 + r < nc && kc + k < bk) ? C[(size_t)(i0 + r) * bk + kc + k] : 0.0;
-      const int kk = t / kGjB, c = t % kGjB;
-      double v = 0.0;
-      if (kc + kk < bk && j0 + c < nc && (!colk || c < bk))
-        v = colk ? P[(kc + kk) * bk + c] : R[(size_t)(kc + kk) * nc + j0 + c];
-      sR[kk][c] = v;
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+  stage(0, 0);
+  int buf = 0;
+  for (int kc = 0; kc < bk; kc += kUK, buf ^= 1) {
+    if (kc + kUK < bk) {
+      stage(buf ^ 1, kc + kUK);
+      cp_async_wait<1>();  // everything but the chunk just issued
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const double* cb = sC + buf * kUK * kUT;
+    const double* rb = sR + buf * kUK * kUT;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      double cv[4], rv[4];
+    for (int k = 0; k < kUK; ++k) {
+      double cv[8], rv[8];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) cv[a] = sC[ty + 16 * a][k];
+      for (int a = 0; a < 8; ++a) cv[a] = cb[k * kUT + ty + 16 * a];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) rv[b] = sR[k][tx + 16 * b];
+      for (int b = 0; b < 8; ++b) rv[b] = rb[k * kUT + tx + 16 * b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(cv[a], rv[b], acc[a][b]);
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(cv[a], rv[b], acc[a][b]);
     }
-    __syncthreads();
+    __syncthreads();  // the next iteration's stage overwrites this buffer
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a) {
+    const int r = ty + 16 * a, i = i0 + r;
+    if (i >= nc) continue;
+    const bool rowk = i >= k0 && i < k0 + bk;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
-      if (i >= nc || j >= nc || (colk && j - k0 >= bk)) continue;
-      double* o = A + (size_t)i * nc + j;
-      *o = colk ? -acc[a][b] : *o - acc[a][b];
+    for (int b = 0; b < 8; ++b) {
+      const int x = tx + 16 * b, j = j0 + x;
+      if (j >= nc) continue;
+      double v;
+      if (rowk) v = R[(size_t)(i - k0) * nc + j];
+      else if (j >= k0 && j < k0 + bk) v = -acc[a][b];
+      else v = sA[r * kUT + x] - acc[a][b];
+      A[(size_t)i * nc + j] = v;
     }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -770,12 +839,13 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
   }
   if (assembled)
     PD_CUDA_TRY(c, cudaMemcpyAsync(assembled, s->A.p, s->A.bytes(), cudaMemcpyDeviceToDevice, c->stream));
-  const int ntile = (nc + kGjB - 1) / kGjB;
+  const int ntile = (nc + kGjB - 1) / kGjB, nut = (nc + kUT - 1) / kUT;
+  PD_CUDA_TRY(c, cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
   for (int k0 = 0; k0 < nc; k0 += kGjB) {
     const int bk = std::min(kGjB, nc - k0);
     k_gj_pivot<<<1, 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p);
     k_gj_panel<<<2 * ntile, 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p, s->R.p, s->C.p);
-    k_gj_update<<<dim3(ntile, ntile), 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p, s->R.p, s->C.p);
+    k_gj_update<<<dim3(nut, nut), 256, kUpdSmem, c->stream>>>(nc, k0, bk, s->A.p, s->R.p, s->C.p);
   }
   PD_CUDA_TRY(c, cudaGetLastError());
   s->have_op = true;

@@ -5,7 +5,9 @@ oracle (no reference counterpart; it preconditions the reference's CG).
   oracle's restatement;
 * the assembled Galerkin matrix P0^T K P0 equals the oracle's product with its
   dense tangent to 1e-11 of its largest entry (jittered bar, prescribed dofs);
-* the Gauss-Jordan inverse: |Ac^-1 Ac - I| <= 1e-9;
+* the Gauss-Jordan inverse: |Ac^-1 Ac - I| <= 1e-9, also over several 64-wide
+  elimination steps and 128-wide update tiles with ragged edges (375 and 750
+  coarse dofs);
 * two-level CG solves a jittered cube to the block-Jacobi displacement (1e-8
   relative) in fewer CG iterations;
 * the rigid coarse space (6 modes per aggregate): aggregates equal the
@@ -121,3 +123,19 @@ def test_two_level_rigid_fewer_iterations():
     print(f"CG iterations: translations {i3}, with rotations {i6}")
     assert np.linalg.norm(u6 - u3) <= 1e-8 * np.linalg.norm(u3)
     assert i6 < i3
+
+
+@pytest.mark.parametrize("modes", [3, 6])
+def test_coarse_inverse_multi_block(modes):
+    """15^3 jittered lattice, cells of 3.02h: 125 aggregates, 375 or 750 coarse
+    dofs (not multiples of the 64-wide steps or the 128-wide update tiles)."""
+    w = _bar(nx=15, ny=15, nz=15, seed=8)
+    n = len(w["vol"])
+    u = np.random.default_rng(5).normal(0.0, 2e-6, 3 * n)
+    with Context(precision="fp64") as ctx:
+        workloads.setup_context(ctx, w)
+        ctx.coarse_modes(modes)
+        agg, A, Ai = ctx.coarse_operator(u)
+    nc = A.shape[0]
+    assert nc == modes * (int(agg.max()) + 1) == modes * 125
+    assert np.abs(Ai @ A - np.eye(nc)).max() <= 1e-9
