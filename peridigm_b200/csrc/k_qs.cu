@@ -618,7 +618,7 @@ static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* it
 // two-level preconditioner) as the fallback: when the flexible iteration
 // stalls, or when the true FP64 residual |b - K x| (recomputed, not the
 // recursive one) misses the tolerance, the solve restarts from the current x
-// with the base. The true residual is the judge.
+// with the base. The true residual decides.
 static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out) {
   QsState* s = c->qs;
   const int64_t m = 3 * c->n;
