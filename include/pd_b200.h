@@ -362,8 +362,11 @@ int pd_jacobian_block_diagonal(pd_ctx* ctx, const double* u, double* blocks);
  * the block-Jacobi blocks; G: a linear message-passing network on the patch
  * graph (3 layers, hidden 64, BF16 weights, FP32 activations and
  * accumulation). M is symmetric positive definite, so PD_PRECOND_MPNN solves
- * run plain CG; a stall, or a true FP64 residual above the tolerance, falls
- * back to the same preconditioner without the network. */
+ * run preconditioned CG, with the flexible (Polak-Ribiere) beta
+ * z_new.(r_new - r_old) / (z_old.r_old): the standard beta for a fixed SPD M,
+ * and tolerant of the FP32 rounding of the network's product. A stall, or a
+ * true FP64 residual above the tolerance, falls back to the same
+ * preconditioner without the network. */
 int pd_mpnn_init(pd_ctx* ctx, uint64_t seed, double patch);
 /* While every > 0, block-Jacobi and two-level CG solves of pd_qs_load_step
  * store training pairs (r_k, x* - x_k) from every every-th iterate

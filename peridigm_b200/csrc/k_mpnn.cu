@@ -18,7 +18,9 @@
 //
 // with hidden 64, BF16 weights and FP32 activations and accumulation. G^T G is
 // symmetric positive semi-definite and S diagonal positive, so M stays
-// symmetric positive definite and plain CG keeps its optimality. The middle
+// symmetric positive definite and CG keeps its optimality (the solver takes
+// the flexible Polak-Ribiere beta, equal to the standard one for a fixed SPD
+// M, against the FP32 rounding of the network's product). The middle
 // level covers the band between block Jacobi (the nearest neighbors) and the
 // coarse cells (two horizons): an exact patch-level solve halves the two-level
 // CG iterations on a 24^3 cube; G^T G is trained to approximate it locally.
