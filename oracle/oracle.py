@@ -469,6 +469,37 @@ def coarse_operator(T, agg, fixed_dofs=()):
     return A, P
 
 
+def gauss_jordan_blocked(A, bk=64):
+    """In-place blocked Gauss-Jordan inverse without pivoting of an SPD matrix,
+    the step structure of peridigm_b200/csrc/k_coarse.cu (k_gj_pivot,
+    k_gj_panel, k_gj_update) in numpy. For each block k of width bk (the last
+    one ragged):
+
+      P  = A_kk^-1                      (pivot block)
+      R  = P A_k*, with P itself in R's block-k columns   (row panel)
+      Ct = A_*k^T                       (old block column, transposed)
+      rows i of block k:   A_i* = R_(i-k0)*
+      other rows i:        A_ij = [j outside block k] A_ij - (Ct_*i . R_*j)
+
+    which is A_ij -= C_i R_j, A_kj = R_j, A_ik = -C_i P and A_kk = P. Returns the
+    inverse (a new array)."""
+    A = np.array(A, dtype=np.float64, copy=True)
+    nc = A.shape[0]
+    for k0 in range(0, nc, bk):
+        k1 = min(nc, k0 + bk)
+        P = np.linalg.inv(A[k0:k1, k0:k1])
+        R = P @ A[k0:k1, :]
+        R[:, k0:k1] = P
+        Ct = A[:, k0:k1].T.copy()
+        upd = Ct.T @ R
+        keep = np.ones(nc, bool)
+        keep[k0:k1] = False
+        A[:, ~keep] = 0.0
+        A -= upd
+        A[k0:k1, :] = R
+    return A
+
+
 def coarse_operator_rigid(T, x, agg, side, fixed_dofs=()):
     """Galerkin coarse matrix of the rigid coarse space (6 modes per aggregate,
     no reference counterpart): per aggregate the translations and the
