@@ -426,7 +426,9 @@ __global__ void __launch_bounds__(256) k_pt_layer_t(int64_t np, const int64_t* _
   }
 }
 
-// x_J = s_J + sum_{I in N(J)} t_I  (half a warp per patch, 4 features per lane)
+// x_J = s_J + sum_{I in N(J)} t_I  (half a warp per patch, 4 features per lane).
+// No __launch_bounds__ here or on k_pt_tail: with (256) ptxas held both to 32
+// registers and spilled; without it they take 34 and 38, no spills.
 __global__ void k_pt_gather_t(int64_t np, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
                               const float* __restrict__ s, const float* __restrict__ t, float* __restrict__ x) {
   const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
