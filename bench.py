@@ -1,15 +1,34 @@
 """Benchmark: bond evaluations per second of the explicit LPS + critical-stretch
-step on the notched-plate workload (400x200x4 = 320,000 points, h = 0.5 mm,
-jitter +-0.05h seed 1, delta = 3.015h, s_c = 5e-4, +-2 m/s prescribed pulls).
+step, split-FP32 against FP64, on one B200; quasi-static time to 1e-8.
+
+Headline workload (default): the memory-scale heterogeneous plate,
+400x400x200 = 32,000,000 points, h = 0.5 mm, jitter +-0.05h (seed 4),
+delta = 3.015h, per-point bulk modulus lognormal (median 130 GPa, sigma 0.3,
+seed 5), mu = 0.6K, critical stretch uniform in [3e-4, 6e-4] (seed 6),
++-1 m/s prescribed pulls on the x faces (3 layers). --workload picks another:
+notched_plate (400x200x4, 320,000 points, s_c = 5e-4, +-2 m/s pulls),
+plate_sphere (400x400x40 plate + dropped sphere, contact) or bar_wave
+(100x10x10 bar, Gaussian velocity pulse, no damage).
 
 One bench step = one velocity-Verlet step: damage + dilatation pass, force
 pass with the Verlet epilogue, over every bond. value = bonds x steps /
 device time (CUDA events on the library's stream, max over ranks, summed over
-ranks for N > 1: each rank runs its own plate, weak scaling).
+ranks for N > 1: each rank runs its own body, weak scaling).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload W]
 
-Prints one JSON line on rank 0.
+Prints one JSON line on rank 0. Two further modes print one JSON line per
+run for profilers (no timing claims beyond the device time they print):
+
+    python bench.py --profile [--workload W] [--nx --ny --nz] [--precision split|fp64|both]
+                    [--material lps|bond_based|linear_lps] [--profile-steps 3]
+        a few explicit steps; with --precision both, the split and FP64 runs
+        and the relative L2 difference of their displacements
+    python bench.py --qs-profile block_jacobi|two_level|mpnn [--qs-n 60] [--qs-tol 1e-4]
+                    [--coarse-modes 3|6] [--coarse-build-only]
+        one load step of the quasi-static cube (the learned level at its
+        starting weights), or, with --coarse-build-only, the two-level coarse
+        operator built once at zero displacement
 """
 from __future__ import annotations
 
@@ -31,28 +50,61 @@ UNIT = "bond evals/s"
 
 
 def algorithmic_bytes(nb, n, precision="split"):
-    """Bytes each bond pass must move at minimum with this layout (one launch),
-    every per-point record counted once (ideal reuse of gathered neighbors).
+    """Bytes an explicit step must move at minimum (every per-point record
+    counted once: ideal reuse of gathered neighbors), per pass and per step.
 
-    Split-FP32, per bond, both passes: col 4 + bond damage 1 + bond vector
-    record (X in FP32, omega*V_j) 16 = 21 B.
+    Split-FP32, per bond and pass: neighbor id 4 + bond damage 1 + reference
+    bond vector X in FP32 12 = 17 B; per step 34 B.
     Per point, dilatation pass: row 8, owner terms 16, displacement record 32,
     writes A/B 8, theta 8, node damage 8 -> 80 B.
-    Per point, force pass: row 8, displacement record 32, rho 8, v read+write 48,
-    acceleration 24, u read+write 48, next displacement record 24, BC mask 1 -> 193 B.
-    FP64 path (no bond records): per bond col 4 + damage 1; per point the
-    gathered FP64 coordinates, material and owner terms (144 B / 217 B)."""
+    Per point, force pass: row 8, displacement record 32, rho 8, v read+write
+    48, acceleration 24, u read+write 48, next displacement record 24, BC mask
+    1 -> 193 B.
+    Per step (both passes, per-point terms counted once): 34 nb + 176 n.
+    FP64 path per step: X in FP64 (24 B) instead of FP32, 58 nb + 200 n."""
     if precision == "split":
-        return {"dilatation": 21 * nb + 80 * n, "force": 21 * nb + 193 * n}
-    return {"dilatation": 5 * nb + 144 * n, "force": 5 * nb + 217 * n}
+        return {"dilatation": 17 * nb + 80 * n, "force": 17 * nb + 193 * n, "step": 34 * nb + 176 * n}
+    return {"step": 58 * nb + 200 * n}
 
 
-# DRAM bytes (read + write) per launch of the split bond passes on this
-# workload, from one ncu capture (--set full, step 1 of the notched plate,
-# sliced bond stream, 128-thread blocks): k_dilatation_split<4> 586.0 MB read
-# + 7.7 MB written, k_force_split<4> 605.8 MB read + 8.0 MB written. The excess over the
-# algorithmic bytes is the slices' padding records (6.3 % of the slots).
-NCU_TRAFFIC = {"dilatation": 593.7e6, "force": 613.9e6}
+# DRAM bytes (read + write) per launch of the split bond passes from one ncu
+# capture (--set full) of step 1 of the heterogeneous plate at 200x200x50
+# (2,000,000 points, sliced bond stream, 128-thread blocks), with the streamed
+# slots of that run. Launches of other sizes are scaled by their slot counts.
+NCU_TRAFFIC = {"workload": "large_plate_200x200x50", "slots": None, "dilatation": None, "force": None}
+
+WORKLOADS = ("large_plate", "notched_plate", "plate_sphere", "bar_wave")
+
+
+def make_workload(name, dims=None):
+    from peridigm_b200 import workloads
+
+    kw = {k: v for k, v in zip(("nx", "ny", "nz"), dims or ()) if v}
+    if name == "large_plate":
+        return workloads.large_plate(**kw), False
+    if name == "notched_plate":
+        return workloads.notched_plate(**kw), False
+    if name == "plate_sphere":
+        return workloads.plate_sphere(**kw), True
+    if name == "bar_wave":
+        return workloads.bar_wave(**kw), False
+    raise ValueError(name)
+
+
+def setup(ctx, w, blocks):
+    from peridigm_b200 import workloads
+
+    (workloads.setup_context_blocks if blocks else workloads.setup_context)(ctx, w)
+    return ctx
+
+
+def sliced_slots(ctx):
+    """Streamed slots of the 4-lanes-per-point split passes: each 8-owner
+    slice holds 32 slots per group of 4 bonds of its longest row."""
+    lens = ctx.field("Number_Of_Neighbors").astype(np.int64)
+    pad = (-lens.size) % 8
+    lens = np.concatenate([lens, np.zeros(pad, np.int64)]).reshape(-1, 8)
+    return int(32 * ((lens.max(axis=1) + 3) // 4).sum())
 
 
 class ClockSampler:
@@ -108,40 +160,70 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
 
 
+def peak_hbm():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# CPU sample of the heterogeneous plate: a 128x128x64 block of the same
+# lattice spacing, jitter, material statistics and pulls (1,048,576 points).
+CPU_SAMPLE_DIMS = {"large_plate": (128, 128, 64), "notched_plate": (100, 200, 4), "plate_sphere": None,
+                   "bar_wave": (100, 10, 10)}
+
+
+def cpu_sample(name):
+    """The bounded CPU sample of a workload: the reference's compiled kernels
+    run with block constants (the reference has per-block K, mu and s_c; the
+    heterogeneous plate's medians are used, which costs the same)."""
+    dims = CPU_SAMPLE_DIMS.get(name)
+    if dims is None:
+        dims = (100, 200, 4)
+        name = "notched_plate"
+    w, _ = make_workload(name, dims)
+    return w, name, dims
+
+
 def reference_arm(args, world, rank):
     """The reference's own CPU implementation of the step (oracle/_ref: its
     computeDilatation + computeInternalForceLinearElastic compiled from source,
     with the restated critical-stretch damage and Verlet loops) on all host
-    cores, over a bounded sample of the workload: the left 100 columns of the
-    notched plate (80,000 points, the notch included)."""
+    cores, over a bounded sample of the workload (cpu_sample)."""
     if rank != 0:
         return
     from oracle import cpu_baseline
     from oracle import oracle as O
-    from peridigm_b200 import workloads
 
     O.build()
-    w = workloads.notched_plate(nx=100)
+    w, sname, dims = cpu_sample(args.workload)
     row, col = O.neighbor_search(w["x"], w["horizon"], w["planes"])
     r = cpu_baseline.run(w, row, col, steps=args.steps, warmup=args.warmup)
     value = r["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "notched_plate_100x200x4 (sample of notched_plate_400x200x4)",
+            "config": {"workload": f"{workload_name(args.workload)} (sample: {sname}_{dims[0]}x{dims[1]}x{dims[2]})",
                        "points": int(len(w["vol"])), "bonds": int(len(col)), "precision": "fp64"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
-                             "sample": f"{args.steps} explicit steps of a 100x200x4 slab of the plate "
+                             "sample": f"{args.steps} explicit steps of {sname}_{dims[0]}x{dims[1]}x{dims[2]} "
                                        f"({len(col)} bonds), {r['cores']} processes"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def workload_name(name):
+    w = {"large_plate": "large_plate_400x400x200", "notched_plate": "notched_plate_400x200x4",
+         "plate_sphere": "plate_sphere_400x400x40_r25", "bar_wave": "bar_wave_100x10x10"}
+    return w[name]
 
 
 def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
@@ -222,6 +304,7 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
                                            "patch_m": patch, "coarse_modes": learned_modes,
                                            "validation_cg_iterations": {e: v[0] for e, v in checkpoints.items()},
                                            "selected_epoch": best_epoch}}
+
     def arm_context(arm, precond):
         ctx = Context(device=local, precision="fp64")
         workloads.setup_context(ctx, w2)
@@ -244,17 +327,13 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
             st = None
             clocks = ClockSampler(local)
             clocks.start()
-            t1 = time.perf_counter()
             for k in range(1, len(w2["times"])):
                 st = ctx.qs_load_step(w2["times"][k - 1], w2["times"][k], newton_tolerance=-1e-8,
                                       cg_relative_tolerance=1e-8, preconditioner=precond, stats=st)
-            wall = time.perf_counter() - t1
             clk = clocks.stop()
-            out[arm] = {"seconds": st.device_ms / 1e3, "wall_seconds": wall, "cg_iterations": st.cg_iterations,
-                            "newton_iterations": st.newton_iterations, "final_cg_residual": st.final_residual,
-                            "fallbacks": st.preconditioner_fallbacks, "coarse_builds": st.coarse_builds,
-                            "sm_mhz": clk["sm_mhz"],
-                            "clock_reasons": clk["reasons"]}
+            out[arm] = {"seconds": st.device_ms / 1e3, "cg_iterations": st.cg_iterations,
+                        "newton_iterations": st.newton_iterations, "fallbacks": st.preconditioner_fallbacks,
+                        "coarse_builds": st.coarse_builds, "sm_mhz": clk["sm_mhz"], "clock_reasons": clk["reasons"]}
             if arm == "block_jacobi" and cpu_threads:
                 # CPU baseline: the same block-Jacobi CG step restated in C on the
                 # host threads, timed on a sample at the solved state and scaled
@@ -271,44 +350,192 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
                 est = st.newton_iterations * smp["seconds_per_newton_setup"] + \
                     st.cg_iterations * smp["seconds_per_cg_iteration"]
                 out["cpu_baseline"] = dict(smp, seconds=est, kind="port",
-                                           sample="block-Jacobi CG restated in C (matrix-free LPS tangent, "
-                                                  "3x3 block inverses) on %d host threads: 20 CG iterations and one "
-                                                  "Newton set-up at the solved state, scaled by the GPU solve's %d "
-                                                  "Newton and %d CG iterations" % (cpu_threads, st.newton_iterations,
-                                                                                  st.cg_iterations))
+                                           sample="block-Jacobi CG restated in C on %d host threads: 20 CG "
+                                                  "iterations and one Newton set-up at the solved state, scaled by "
+                                                  "the GPU solve's Newton and CG counts" % cpu_threads)
     bj = out["block_jacobi"]["seconds"]
-    out["two_level_speedup_over_block_jacobi"] = bj / out["two_level"]["seconds"]
-    out["two_level_rigid_speedup_over_block_jacobi"] = bj / out["two_level_rigid"]["seconds"]
-    out["mpnn_speedup_over_block_jacobi"] = bj / out["mpnn"]["seconds"]
-    out["mpnn_last_epoch_speedup_over_block_jacobi"] = bj / out["mpnn_last_epoch"]["seconds"]
+    for arm in ("two_level", "two_level_rigid", "mpnn", "mpnn_last_epoch"):
+        out[f"{arm}_speedup_over_block_jacobi"] = bj / out[arm]["seconds"]
     if "cpu_baseline" in out:
         out["block_jacobi_speedup_over_cpu"] = out["cpu_baseline"]["seconds"] / bj
     return out
 
 
+def explicit_leg(w, blocks, local, steps, warmup, precision, world, max_over_ranks, barrier, timed_clocks=False):
+    """W untimed + K timed Verlet steps from rest of workload w; returns the
+    context (still open) and the timing."""
+    from peridigm_b200 import Context
+
+    ctx = Context(device=local, precision=precision)
+    setup(ctx, w, blocks)
+    nb = ctx.num_bonds()
+    dt = w.get("safety", 0.7) * ctx.critical_time_step()
+    ctx.verlet_run(dt, warmup)
+    barrier()
+    clocks = ClockSampler(local) if timed_clocks else None
+    if clocks:
+        clocks.start()
+    st = ctx.verlet_run(dt, steps, t0=warmup * dt)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    ms = max_over_ranks(st["device_ms"])
+    return ctx, {"nb": nb, "dt": dt, "ms": ms, "value": world * nb * steps / (ms / 1e3), "t_done": (warmup + steps) * dt,
+                 "clocks": clk, "broken_bonds": st["broken_bonds"]}
+
+
+def kernel_roofline(ctx, dt, t0, ksteps, nb, n, hbm, peak_src, slots):
+    """Per-launch CUDA-event durations of the two split passes over ksteps
+    steps and the dominant pass's roofline on the algorithmic bytes."""
+    ctx.kernel_timing(True)
+    ctx.verlet_run(dt, ksteps, t0=t0)
+    kt = ctx.kernel_times()
+    ctx.kernel_timing(False)
+    per = {"dilatation": kt["dilatation_ms"] / kt["evaluations"], "force": kt["force_ms"] / kt["evaluations"]}
+    algo = algorithmic_bytes(nb, n, "split")
+    dom = max(per, key=per.get)
+    achieved = algo[dom] / (per[dom] / 1e3) / 1e9
+    traffic = None
+    if NCU_TRAFFIC.get("slots") and NCU_TRAFFIC.get(dom):
+        traffic = NCU_TRAFFIC[dom] * slots / NCU_TRAFFIC["slots"]
+    return {"bound": "hbm", "kernel": f"k_{dom}_split", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic, "algorithmic_bytes": algo[dom],
+            "launch_ms": per[dom], "per_kernel_ms": per, "steps_timed": ksteps,
+            "per_kernel_frac": {k: algo[k] / (per[k] / 1e3) / 1e9 / hbm for k in per},
+            "streamed_slots": slots, "bonds": nb}
+
+
+def e2e_leg(ctx, n, nb, esteps, world, max_over_ranks, barrier):
+    """The drop-in computeForce call with host buffers: each step the H2D of the
+    current coordinates from pinned memory, damage + dilatation + force on the
+    device, D2H of the force density, then the state update that commits the
+    step's bond damage (the reference's evalModel + updateState cycle,
+    Peridigm.cpp:1536, 1589)."""
+    import ctypes as C
+
+    import torch
+
+    y = torch.from_numpy(ctx.field("Coordinates")).pin_memory()
+    f = torch.zeros(3 * n, dtype=torch.float64).pin_memory()
+    yp = C.cast(y.data_ptr(), C.POINTER(C.c_double))
+    fp = C.cast(f.data_ptr(), C.POINTER(C.c_double))
+    for _ in range(3):
+        ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
+        ctx._ok(ctx.L.pd_update_state(ctx.h))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(esteps):
+        ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
+        ctx._ok(ctx.L.pd_update_state(ctx.h))
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    return {"value": world * nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
+            "d2h_bytes_per_step": 24 * n, "steps": esteps,
+            "api": "pd_compute_force (host y in, host force out) + pd_update_state"}
+
+
+def profile_mode(args):
+    """A few explicit steps for a profiler (replaces a separate driver)."""
+    from peridigm_b200 import Context
+
+    w, blocks = make_workload(args.workload, (args.nx, args.ny, args.nz))
+    precisions = ["split", "fp64"] if args.precision == "both" else [args.precision]
+    res = {}
+    for p in precisions:
+        with Context(precision=p, threads_per_point=args.tpo) as ctx:
+            setup(ctx, w, blocks)
+            nblk = int(np.max(w["block"])) + 1 if blocks else 1
+            for b in range(nblk):
+                if args.material == "bond_based":
+                    ctx.material_bond_based(float(np.median(w["K"])), w["rho"], block=b)
+                elif args.material == "linear_lps":
+                    ctx.material_linear_lps(float(np.median(w["K"])), float(np.median(w["mu"])), w["rho"], block=b)
+            dt = w.get("safety", 0.7) * ctx.critical_time_step()
+            st = ctx.verlet_run(dt, args.profile_steps)
+            nb = ctx.num_bonds()
+            line = {"workload": w["name"], "material": args.material, "precision": p, "points": int(len(w["vol"])),
+                    "bonds": int(nb), "steps": args.profile_steps, "device_ms": st["device_ms"],
+                    "ms_per_step": st["device_ms"] / max(args.profile_steps, 1),
+                    "bond_evals_per_s": nb * args.profile_steps / (st["device_ms"] / 1e3) if st["device_ms"] else 0.0,
+                    "broken_bonds": st["broken_bonds"]}
+            if p == "split" and args.tpo in (0, 4):
+                line["streamed_slots"] = sliced_slots(ctx)
+            print(json.dumps(line), flush=True)
+            res[p] = (ctx.field("Displacement"), ctx.field("Damage"))
+    if len(res) == 2:
+        (us, ds), (u6, d6) = res["split"], res["fp64"]
+        print(json.dumps({"split_vs_fp64_u_rel_l2": float(np.linalg.norm(us - u6) / max(np.linalg.norm(u6), 1e-300)),
+                          "max_node_damage_diff": float(np.max(np.abs(ds - d6)))}), flush=True)
+
+
+def qs_profile_mode(args):
+    """One quasi-static load step of the cube with a chosen preconditioner, or
+    the two-level coarse operator alone (replaces a separate driver)."""
+    from peridigm_b200 import Context, workloads
+
+    w = workloads.qs_cube(n=args.qs_n, h=1.0e-3, seed=1000, load_steps=20)
+    with Context(precision="fp64") as ctx:
+        workloads.setup_context(ctx, w)
+        ctx.coarse_modes(args.coarse_modes)
+        if args.coarse_build_only:
+            _, A, Ai = ctx.coarse_operator(np.zeros(3 * len(w["vol"])))
+            m = min(256, A.shape[0])
+            err = float(np.abs(Ai[:m] @ A - np.eye(A.shape[0])[:m]).max())
+            print(json.dumps({"coarse_dofs": int(A.shape[0]), "max_abs_inverse_error": err}))
+            return
+        if args.qs_profile == "mpnn":
+            ctx.mpnn_init(seed=0, patch=args.patch)
+        st = ctx.qs_load_step(w["times"][0], w["times"][1], newton_tolerance=-1e-3, cg_relative_tolerance=args.qs_tol,
+                              preconditioner=args.qs_profile)
+        print(json.dumps({"precond": args.qs_profile, "points": int(len(w["vol"])), "cg_iterations": st.cg_iterations,
+                          "newton_iterations": st.newton_iterations, "device_ms": st.device_ms}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="large_plate", choices=WORKLOADS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-qs", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the notched-plate extra line")
     ap.add_argument("--qs-load-steps", type=int, default=20)
+    ap.add_argument("--kernel-steps", type=int, default=50, help="steps of the per-kernel event timing")
+    ap.add_argument("--e2e-steps", type=int, default=200, help="steps of the host-buffer e2e leg")
+    ap.add_argument("--fp64-steps", type=int, default=20, help="timed steps of the FP64 leg")
+    # profiling modes
+    ap.add_argument("--profile", action="store_true")
+    ap.add_argument("--precision", default="split", choices=["split", "fp64", "both"])
+    ap.add_argument("--material", default="lps", choices=["lps", "bond_based", "linear_lps"])
+    ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--nx", type=int, default=0)
+    ap.add_argument("--ny", type=int, default=0)
+    ap.add_argument("--nz", type=int, default=0)
+    ap.add_argument("--tpo", type=int, default=0)
+    ap.add_argument("--qs-profile", default=None, choices=["block_jacobi", "two_level", "mpnn"])
+    ap.add_argument("--qs-n", type=int, default=60)
+    ap.add_argument("--qs-tol", type=float, default=1e-4)
+    ap.add_argument("--patch", type=float, default=3.0e-3)
+    ap.add_argument("--coarse-modes", type=int, default=3, choices=[3, 6])
+    ap.add_argument("--coarse-build-only", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    world, rank, local = dist_setup(args.gpus)
+    world, rank, local = dist_setup()
 
     if args.impl == "reference":
         reference_arm(args, world, rank)
         return
+    if args.profile:
+        profile_mode(args)
+        return
+    if args.qs_profile or args.coarse_build_only:
+        args.qs_profile = args.qs_profile or "two_level"
+        qs_profile_mode(args)
+        return
 
     # CPU baseline processes are spawned before any CUDA call in this process.
-    from peridigm_b200 import Context, workloads
-
-    w = workloads.notched_plate()
-    n = int(len(w["vol"]))
-
     import torch
 
     torch.cuda.set_device(local)
@@ -333,83 +560,58 @@ def main():
         if pg is not None:
             pg.barrier()
 
-    ctx = Context(device=local, precision="split")
-    workloads.setup_context(ctx, w)
-    nb = ctx.num_bonds()
-    dt = 0.7 * ctx.critical_time_step()
+    hbm, peak_src = peak_hbm()
+    w, blocks = make_workload(args.workload)
+    n = int(len(w["vol"]))
 
     # ---- value: split-FP32 explicit steps, state resident in HBM -----------
-    ctx.verlet_run(dt, args.warmup)
-    t_done = args.warmup * dt
-    barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    st = ctx.verlet_run(dt, args.steps, t0=t_done)
-    barrier()
-    clk = clocks.stop()
-    t_done += args.steps * dt
-    ms = max_over_ranks(st["device_ms"])
-    value = world * nb * args.steps / (ms / 1e3)
+    ctx, sp = explicit_leg(w, blocks, local, args.steps, args.warmup, "split", world, max_over_ranks, barrier,
+                           timed_clocks=True)
+    nb, dt = sp["nb"], sp["dt"]
+    u_split = ctx.field("Displacement")
+    d_split = ctx.field("Damage")
+    slots = sliced_slots(ctx)
+    step_bytes = algorithmic_bytes(nb, n, "split")["step"]
 
     # ---- per-kernel launch durations (CUDA events around each launch) -------
-    ksteps = min(args.steps, 500)
-    ctx.kernel_timing(True)
-    ctx.verlet_run(dt, ksteps, t0=t_done)
-    kt = ctx.kernel_times()
-    ctx.kernel_timing(False)
-    t_done += ksteps * dt
-    per = {"dilatation": kt["dilatation_ms"] / kt["evaluations"], "force": kt["force_ms"] / kt["evaluations"]}
-    dom = max(per, key=per.get)
-    algo = algorithmic_bytes(nb, n, "split")
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        hbm, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        hbm, peak_src = 6650.0, "fallback"
-    achieved = algo[dom] / (per[dom] / 1e3) / 1e9
-    traffic = NCU_TRAFFIC[dom]
-    roofline = {"bound": "hbm", "kernel": f"k_{dom}_split", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic,
-                "algorithmic_bytes": algo[dom], "launch_ms": per[dom],
-                "per_kernel_ms": per}
-
-    # ---- plain FP64 path, same workload --------------------------------------
-    fsteps = min(args.steps, 1000)
-    c64 = Context(device=local, precision="fp64")
-    workloads.setup_context(c64, w)
-    c64.verlet_run(dt, args.warmup)
-    barrier()
-    st64 = c64.verlet_run(dt, fsteps, t0=args.warmup * dt)
-    barrier()
-    ms64 = max_over_ranks(st64["device_ms"])
-    value64 = world * nb * fsteps / (ms64 / 1e3)
-    c64.close()
+    roofline = kernel_roofline(ctx, dt, sp["t_done"], args.kernel_steps, nb, n, hbm, peak_src, slots)
+    roofline["step_frac"] = step_bytes / (sp["ms"] / args.steps / 1e3) / 1e9 / hbm
 
     # ---- e2e: the drop-in computeForce call with host buffers ---------------
-    # Each step: H2D of the current coordinates from pinned memory, damage +
-    # dilatation + force on the device, D2H of the force density, then the
-    # state update that commits the step's bond damage (the reference's
-    # evalModel + updateState cycle, Peridigm.cpp:1536, 1589).
-    esteps = min(args.steps, 500)
-    y = torch.from_numpy(ctx.field("Coordinates")).pin_memory()
-    f = torch.zeros(3 * n, dtype=torch.float64).pin_memory()
-    import ctypes as C
+    e2e = e2e_leg(ctx, n, nb, args.e2e_steps, world, max_over_ranks, barrier)
+    ctx.close()
 
-    yp = C.cast(y.data_ptr(), C.POINTER(C.c_double))
-    fp = C.cast(f.data_ptr(), C.POINTER(C.c_double))
-    for _ in range(3):
-        ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
-        ctx._ok(ctx.L.pd_update_state(ctx.h))
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(esteps):
-        ctx._ok(ctx.L.pd_compute_force(ctx.h, yp, fp))
-        ctx._ok(ctx.L.pd_update_state(ctx.h))
-    barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = {"value": world * nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
-           "d2h_bytes_per_step": 24 * n, "steps": esteps, "api": "pd_compute_force (host y in, host force out) + pd_update_state"}
+    # ---- plain FP64 path, same workload, same steps from rest ----------------
+    fp64 = None
+    if not args.no_fp64:
+        c64, s64 = explicit_leg(w, blocks, local, args.fp64_steps if args.fp64_steps else args.steps, args.warmup,
+                                "fp64", world, max_over_ranks, barrier)
+        k64 = args.fp64_steps if args.fp64_steps else args.steps
+        fp64 = {"value": s64["value"], "split_over_fp64": sp["value"] / s64["value"], "ms_per_step": s64["ms"] / k64,
+                "steps": k64,
+                "step_frac": algorithmic_bytes(nb, n, "fp64")["step"] / (s64["ms"] / k64 / 1e3) / 1e9 / hbm,
+                "split_step_frac": roofline["step_frac"]}
+        if k64 == args.steps:  # same step count from rest: the two paths' states compare
+            u64, d64 = c64.field("Displacement"), c64.field("Damage")
+            fp64["split_vs_fp64_after_steps"] = args.warmup + args.steps
+            fp64["u_rel_l2"] = float(np.linalg.norm(u_split - u64) / max(np.linalg.norm(u64), 1e-300))
+            fp64["node_damage_max_diff"] = float(np.max(np.abs(d_split - d64)))
+        c64.close()
+
+    # ---- the notched plate (the split/FP64 comparison case) as an extra ------
+    extra = None
+    if not args.no_extra and args.workload != "notched_plate":
+        wp, _ = make_workload("notched_plate")
+        cp, spn = explicit_leg(wp, False, local, max(args.steps, 200), args.warmup, "split", world, max_over_ranks,
+                               barrier)
+        nbp, npt = spn["nb"], int(len(wp["vol"]))
+        rp = kernel_roofline(cp, spn["dt"], spn["t_done"], max(args.kernel_steps, 200), nbp, npt, hbm, peak_src,
+                             sliced_slots(cp))
+        extra = {"workload": "notched_plate_400x200x4", "value": spn["value"],
+                 "ms_per_step": spn["ms"] / max(args.steps, 200), "bonds": nbp,
+                 "force_frac": rp["per_kernel_frac"]["force"], "dilatation_frac": rp["per_kernel_frac"]["dilatation"],
+                 "per_kernel_ms": rp["per_kernel_ms"]}
+        cp.close()
 
     # ---- quasi-static time to 1e-8 (rank 0 only) -----------------------------
     qs = None
@@ -422,25 +624,25 @@ def main():
         from oracle import cpu_baseline
         from oracle import oracle as O
 
-        row, col = ctx.bonds_csr()
         O.build()
-        r = cpu_baseline.run(w, row, col, steps=40, dt=dt)
+        ws, sname, dims = cpu_sample(args.workload)
+        row, col = O.neighbor_search(ws["x"], ws["horizon"], ws["planes"])
+        r = cpu_baseline.run(ws, row, col, steps=40)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
-               "sample": f"{r['steps']} explicit steps of the full 400x200x4 plate on {r['cores']} processes "
-                         f"(slabs with ghost layers, reference LPS kernels compiled from source)"}
-    ctx.close()
+               "sample": f"{r['steps']} explicit steps of {sname}_{dims[0]}x{dims[1]}x{dims[2]} ({len(col)} bonds) "
+                         f"on {r['cores']} processes (slabs with ghost layers, reference LPS kernels compiled from "
+                         f"source, block constants)"}
 
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": sp["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sp["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
-            "config": {"workload": "notched_plate_400x200x4", "points": n, "bonds": nb, "horizon_over_h": 3.015,
-                       "critical_stretch": 5e-4, "dt": dt, "precision": "split_fp32",
-                       "l2": "inputs larger than L2 (about 1.2 GB read per step vs 126 MB L2)",
+            "config": {"workload": workload_name(args.workload), "points": n, "bonds": nb, "horizon_over_h": 3.015,
+                       "dt": dt, "precision": "split_fp32",
+                       "l2": "inputs larger than L2 (%.1f GB of algorithmic bytes per step vs 126 MB L2)"
+                             % (step_bytes / 1e9),
                        "parallelism": f"replicas x{world}"},
-            "fp64": {"value": value64, "unit": UNIT, "steps": fsteps, "ms_per_step": ms64 / fsteps,
-                     "split_over_fp64": value / value64},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "qs": qs, "clocks": clk,
-            "gpu_launches": 2 * args.steps}
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": sp["clocks"],
+            "gpu_launches": 2 * args.steps, "notched_plate": extra, "qs": qs, "fp64": fp64}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg is not None:

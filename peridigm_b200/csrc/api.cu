@@ -53,14 +53,17 @@ int upload_material(pd_ctx* c) {
   }
   PD_CUDA_TRY(c, c->pt.alloc(n));
   PD_CUDA_TRY(c, c->sc.alloc(n));
-  if (c->precision == PD_SPLIT_FP32) {
-    PD_CUDA_TRY(c, c->bx.alloc((size_t)c->nb));
-    PD_CUDA_TRY(c, c->own.alloc(n));
-  }
   PD_CUDA_TRY(c, h2d(c, c->pt.p, pt.data(), n * sizeof(double4)));
   PD_CUDA_TRY(c, h2d(c, c->sc.p, sc.data(), n * sizeof(double)));
   PD_CUDA_TRY(c, h2d(c, c->hp.p, hp.data(), n * sizeof(double)));
-  return PD_OK;
+  if (c->precision == PD_SPLIT_FP32) {
+    PD_CUDA_TRY(c, c->own.alloc(n));
+    std::vector<float> scf(n);
+    for (int64_t i = 0; i < n; ++i) scf[i] = (float)sc[i];
+    PD_CUDA_TRY(c, c->scf.alloc(n));
+    PD_CUDA_TRY(c, h2d(c, c->scf.p, scf.data(), n * sizeof(float)));
+  }
+  return check_sc_pairs(c);
 }
 
 int upload_horizons(pd_ctx* c) {
@@ -120,6 +123,18 @@ int ensure_ready(pd_ctx* c) {
   if (c->material_model == PD_MATERIAL_LINEAR_LPS && c->precision != PD_FP64 && c->tpo_split != 4)
     return fail(c, PD_ERR_UNSUPPORTED, "the split-FP32 Linear LPS passes run at 4 lanes per point (the sliced bond "
                                        "stream); use threads_per_point 0 or 4, or PD_FP64");
+  if (c->precision == PD_SPLIT_FP32 && c->influence != PD_INFLUENCE_ONE &&
+      c->material_model != PD_MATERIAL_BOND_BASED) {
+    // The split passes weight both halves of a bond, t_ij and t_ji, with the
+    // owner's omega(|X|, h_i); that equals the neighbor's omega(|X|, h_j) only
+    // when every point has the same horizon.
+    const double* h = c->block_h.data();
+    for (size_t b = 1; b < c->block_h.size(); ++b)
+      if (h[b] != h[0])
+        return fail(c, PD_ERR_UNSUPPORTED,
+                    "the split-FP32 passes support the Parabolic Decay and Gaussian influence functions only when all "
+                    "blocks have one horizon; use PD_FP64 or the \"One\" influence function");
+  }
   if (!c->symmetric)
     return fail(c, PD_ERR_UNSUPPORTED,
                 "bond families are not symmetric (j in H(i) without i in H(j)); the gather force pass needs "
@@ -527,7 +542,9 @@ int pd_set_bond_damage(pd_ctx* c, const double* bd) {
     else return fail(c, PD_ERR_UNSUPPORTED, "bond damage must be 0 or 1 (critical-stretch values)");
   }
   TRY(ensure_device(c));
-  PD_CUDA_TRY(c, h2d(c, c->dmg.p, h.data(), (size_t)c->nb));
+  // the rows' own halves, then each bond's partner half (bit 1) from the partner's row
+  PD_CUDA_TRY(c, h2d(c, c->dmg_trial.p, h.data(), (size_t)c->nb));
+  TRY(mirror_damage(c, c->dmg_trial.p, c->dmg.p));
   c->dmg_gen++;
   c->trial_valid = false;
   coarse_invalidate(c);
@@ -984,7 +1001,7 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
       std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
       const uint8_t* src = c->trial_valid ? c->dmg_trial.p : c->dmg.p;
       PD_CUDA_TRY(c, d2h(c, h.data(), src, (size_t)c->nb));
-      for (int64_t b = 0; b < c->nb; ++b) out[b] = (double)h[b];
+      for (int64_t b = 0; b < c->nb; ++b) out[b] = (double)(h[b] & 1);  // the row's own half
       return PD_OK;
     }
     case PD_FIELD_FORCE: {

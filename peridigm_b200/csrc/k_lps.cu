@@ -13,13 +13,18 @@
 // a fixed xor-shuffle tree, so results are deterministic.
 //
 // Split-FP32 path data:
-//   bx[b] = (X, omega*V_j)             per bond, streamed: X = fp32(x_j - x_i)
-//                                      formed in FP64, rounded once
-//   ur[j] = (u_hi[3], u_lo[3], A, B)   per point, one 256-bit gather per bond;
-//                                      u_hi = fp32(u), u_lo = fp32(u - u_hi)
-// du = (u_hi_j - u_hi_i) + (u_lo_j - u_lo_i) is the displacement difference to
-// within one FP32 ulp, with no FP64 instruction in the bond loop. The FP64
-// displacement u[3n] stays the integration state.
+//   bx3 = X per bond, streamed (12 B): X = fp32(x_j - x_i) formed in FP64,
+//         rounded once; 32-slot groups of three planes (x[32], y[32], z[32])
+//         so that one warp load of a component is 128 consecutive bytes
+//   ur[j] = (u_hi[3], lo_xy, lo_z|q, V, A, B) per point, one 256-bit gather
+//         per bond: u_hi = fp32(u); the residual u - u_hi of each component as
+//         a 16-bit multiple of a power of two q shared by the three (q in the
+//         top half of slot 4, 2^-14 of the largest component's FP32 ulp, so
+//         u_hi + lo carries u to ~2^-39 of |u|); V = the point's volume
+// du = (u_hi_j - u_hi_i) + (lo_j - lo_i) is the displacement difference to
+// within one FP32 ulp plus 2^-38 |u|, with no FP64 instruction in the bond
+// loop. The influence weight omega(|X|) is evaluated in the loop (1 for the
+// "One" function). The FP64 displacement u[3n] stays the integration state.
 #include <math.h>
 
 #include <cub/cub.cuh>
@@ -77,40 +82,140 @@ __device__ __forceinline__ Rec8 ld_rec(const Rec8* p) {
   return r;
 }
 
-__device__ __forceinline__ void split_hi_lo(double v, float* hi, float* lo) {
-  const float h = __double2float_rn(v);
-  *hi = h;
-  *lo = __double2float_rn(v - (double)h);
+// ---------------------------------------------------------------------------
+// Split-path displacement record (slots 0-4 of Rec8). The residual of each
+// component, u_c - fp32(u_c), is stored as k_c * q with k_c a 16-bit integer
+// (biased by 2^15) and q = 2^(eb - 165), eb the largest biased FP32 exponent
+// of the three u_hi: |u_c - u_hi_c| <= ulp(u_hi_c)/2 <= 2^14 q, so k_c fits,
+// and the rounding of k_c leaves an error of at most q/2 ~ 2^-39 |u|.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kQShift = 38;  // q = 2^-14 * 2^-24 of the largest component's binade
+
+// The record's 16-bit residual k (biased) as a float: 2^23 + k exactly.
+__device__ __forceinline__ float lo_magic(uint32_t k16) { return __uint_as_float(0x4B000000u | k16); }
+
+struct ULo {
+  float x, y, z;
+};
+// Residuals of a record: (2^23 + k) q - (2^23 + 2^15) q = (k - 2^15) q, exact.
+__device__ __forceinline__ ULo decode_lo(const Rec8& r) {
+  const uint32_t w3 = __float_as_uint(r.v[3]), w4 = __float_as_uint(r.v[4]);
+  const float q = __uint_as_float(w4 & 0xffff0000u);
+  const float c = -8421376.0f * q;  // -(2^23 + 2^15) q
+  ULo l;
+  l.x = fmaf(lo_magic(w3 & 0xffffu), q, c);
+  l.y = fmaf(__uint_as_float(__byte_perm(w3, 0x4B00u, 0x5432u)), q, c);  // high half of w3 under 0x4B00
+  l.z = fmaf(lo_magic(w4 & 0xffffu), q, c);
+  return l;
 }
 
-// Bond geometry of the split path from the bond's stored X (FP32, q.xyz) and
-// the two endpoints' displacement records. Identical operations in both passes;
-// with both endpoints swapped X, du and Y are exactly negated (X_ji = -X_ij is
-// rounded from an exactly negated FP64 difference), so e and |X| are identical
-// and bond damage stays symmetric.
+// 16-bit residual (biased) of component value uc with FP32 part h, quantum
+// 2^(eb - 165); 0x8000 (zero residual) when the point's displacement is below
+// 2^-88 and q would not be a normal float.
+__device__ __forceinline__ uint32_t lo_code(double uc, float h, uint32_t eb) {
+  if (eb <= kQShift) return 0x8000u;
+  const double inv = __longlong_as_double((long long)(1023 + 127 + kQShift - eb) << 52);  // 1/q, exact
+  int k = __double2int_rn((uc - (double)h) * inv);  // uc - h is exact in FP64
+  k = min(max(k, -32768), 32767);
+  return (uint32_t)(k + 32768);
+}
+__device__ __forceinline__ uint32_t q_bits(uint32_t eb) { return eb > kQShift ? (eb - kQShift) << 23 : 0u; }
+__device__ __forceinline__ uint32_t f32_exp(float h) { return (__float_as_uint(h) >> 23) & 0xffu; }
+
+// Record slots 0-4 from one thread's FP64 displacement (slots 5-7 untouched).
+__device__ __forceinline__ void store_u_record(Rec8* rec, double u0, double u1, double u2) {
+  const float h0 = __double2float_rn(u0), h1 = __double2float_rn(u1), h2 = __double2float_rn(u2);
+  const uint32_t eb = max(f32_exp(h0), max(f32_exp(h1), f32_exp(h2)));
+  const uint32_t k0 = lo_code(u0, h0, eb), k1 = lo_code(u1, h1, eb), k2 = lo_code(u2, h2, eb);
+  *reinterpret_cast<float4*>(rec->v) = make_float4(h0, h1, h2, __uint_as_float(k0 | (k1 << 16)));
+  rec->v[4] = __uint_as_float(k2 | q_bits(eb));
+}
+
+template <int TPO>
+__device__ __forceinline__ uint32_t group_max_u32(uint32_t v) {
+#pragma unroll
+  for (int o = TPO / 2; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// The same from a lane group: lane c < 3 holds component c (other lanes pass
+// 0). Every lane of the warp calls it; only groups with `store` write.
+template <int TPO>
+__device__ __forceinline__ void store_u_record_group(Rec8* rec, int lane, double uc, bool store) {
+  const float h = __double2float_rn(uc);
+  const uint32_t eb = group_max_u32<TPO>(lane < 3 ? f32_exp(h) : 0u);
+  const uint32_t k = lo_code(uc, h, eb);
+  const float h1 = __shfl_down_sync(0xffffffffu, h, 1, TPO);
+  const float h2 = __shfl_down_sync(0xffffffffu, h, 2, TPO);
+  const uint32_t k1 = __shfl_down_sync(0xffffffffu, k, 1, TPO);  // lane 0: k_y; lane 1: k_z
+  if (store && lane == 0) *reinterpret_cast<float4*>(rec->v) = make_float4(h, h1, h2, __uint_as_float(k | (k1 << 16)));
+  if (store && lane == 1) rec->v[4] = __uint_as_float(k1 | q_bits(eb));
+}
+
+// FP64 displacement held by a record.
+__device__ __forceinline__ void load_u_record(const Rec8& r, double* u) {
+  const ULo l = decode_lo(r);
+  u[0] = (double)r.v[0] + (double)l.x;
+  u[1] = (double)r.v[1] + (double)l.y;
+  u[2] = (double)r.v[2] + (double)l.z;
+}
+
+// Influence function in FP32 for the split passes (same branches as omega_d).
+__device__ __forceinline__ float omega_f(int kind, float zeta, float h) {
+  if (kind == PD_INFLUENCE_ONE) return 1.0f;
+  if (kind == PD_INFLUENCE_PARABOLIC_DECAY) {
+    if (zeta > h) return 0.0f;
+    const float s = zeta / h;
+    return s < 0.5f ? 1.0f : fmaf(-4.0f * s, s, 4.0f * s);
+  }
+  return expf(-(zeta * zeta) / (h * h * 0.16f));
+}
+
+// The owner's own displacement (hi and decoded residual) and its volume-free
+// record terms, read once per row.
+struct OwnU {
+  float hx, hy, hz, lx, ly, lz;
+};
+__device__ __forceinline__ OwnU own_u(const Rec8& r) {
+  const ULo l = decode_lo(r);
+  OwnU o;
+  o.hx = r.v[0], o.hy = r.v[1], o.hz = r.v[2];
+  o.lx = l.x, o.ly = l.y, o.lz = l.z;
+  return o;
+}
+
+// Bond geometry of the split path from the bond's stored X (FP32) and the two
+// endpoints' displacements. Identical operations in both passes; with both
+// endpoints swapped X, du and Y are exactly negated (X_ji = -X_ij is rounded
+// from an exactly negated FP64 difference), so e and |X| are identical and
+// bond damage stays symmetric.
 struct SplitBond {
   float Yx, Yy, Yz, zeta, ry, e, xu, xx;  // xu = X.du, xx = |X|^2 (the linear LPS terms)
 };
-__device__ __forceinline__ SplitBond split_bond(const float4& q, const Rec8& ui, const Rec8& uj) {
+__device__ __forceinline__ SplitBond split_bond(float X0, float X1, float X2, const OwnU& ui, const Rec8& uj) {
   SplitBond s;
-  const float Ux = (uj.v[0] - ui.v[0]) + (uj.v[3] - ui.v[3]);
-  const float Uy = (uj.v[1] - ui.v[1]) + (uj.v[4] - ui.v[4]);
-  const float Uz = (uj.v[2] - ui.v[2]) + (uj.v[5] - ui.v[5]);
-  const float xx = fmaf(q.z, q.z, fmaf(q.y, q.y, q.x * q.x));
-  s.Yx = q.x + Ux;
-  s.Yy = q.y + Uy;
-  s.Yz = q.z + Uz;
+  const ULo lj = decode_lo(uj);
+  const float Ux = (uj.v[0] - ui.hx) + (lj.x - ui.lx);
+  const float Uy = (uj.v[1] - ui.hy) + (lj.y - ui.ly);
+  const float Uz = (uj.v[2] - ui.hz) + (lj.z - ui.lz);
+  const float xx = fmaf(X2, X2, fmaf(X1, X1, X0 * X0));
+  s.Yx = X0 + Ux;
+  s.Yy = X1 + Uy;
+  s.Yz = X2 + Uz;
   const float yy = fmaf(s.Yz, s.Yz, fmaf(s.Yy, s.Yy, s.Yx * s.Yx));
   s.ry = rsqrtf(yy);
   s.zeta = xx * rsqrtf(xx);
   const float dY = yy * s.ry;
-  const float xu = fmaf(q.z, Uz, fmaf(q.y, Uy, q.x * Ux));
+  const float xu = fmaf(X2, Uz, fmaf(X1, Uy, X0 * Ux));
   const float uu = fmaf(Uz, Uz, fmaf(Uy, Uy, Ux * Ux));
   s.e = __fdividef(fmaf(2.0f, xu, uu), dY + s.zeta);  // |Y| - |X| without cancellation
   s.xu = xu;
   s.xx = xx;
   return s;
 }
+
+// Position of the X of stream slot k in bx3 (component c at +32c).
+__device__ __forceinline__ int64_t xs_index(int64_t k) { return 96 * (k >> 5) + (k & 31); }
 
 // Streaming loads of bond-ordered data (read once per pass; kept out of L1 so
 // the neighbor records stay resident there).
@@ -144,22 +249,171 @@ constexpr int kUnroll = PD_BOND_UNROLL;
 // grid costs half of what it does with 256-thread blocks.
 constexpr int kSplitBlock = 128;
 
-// Bond-stream cursor of a lane. CSR: the owner's row, the lane's bonds TPO
-// apart. Sliced (4 lanes per point, SELL): the bonds of the 8 owners of a
-// warp interleaved so that one warp load is 32 consecutive records
-// (record of owner o, row offset r at soff[s]*32 + (r/4)*32 + 4o + r%4), each
-// row padded with dummy bonds (damage byte 2) to the slice's longest row.
-template <int TPO, bool SELL>
-__device__ __forceinline__ void bond_cursor(int64_t i, int lane, int64_t b0, int64_t b1,
-                                            const int64_t* __restrict__ soff, int64_t* base, int* left) {
-  if (SELL) {
-    const int64_t s = i >> 3, so = soff[s];
-    *base = so * 32 + (i & 7) * 4 + lane;
-    *left = (int)(soff[s + 1] - so);
-  } else {
-    const int rem = (int)(b1 - b0) - lane;
-    *base = b0 + lane;
-    *left = rem > 0 ? (rem + TPO - 1) / TPO : 0;
+// Bond damage byte of bond (i, j) in row i: bit 0 = d_ij, the damage of the
+// row's own half (the reference's bondDamage of i's family), bit 1 = d_ji,
+// the partner half's (j's family), kept in step by evaluating j's own
+// critical-stretch test in i's row as well: the stretch of a bond is computed
+// identically in both rows, so the two bytes stay mirrored without a reverse
+// index. With one critical stretch on both sides of every bond the two bits
+// are equal. kDummyBond marks padding slots and masked lanes (neither half
+// present). The force gathers t_ij with (1 - d_ij) and t_ji with (1 - d_ji),
+// as the reference's scatter does from the two families
+// (elastic.cxx:119-130).
+constexpr int kDummyBond = 4;
+
+// Bond-stream cursor of a lane in CSR order: the owner's row, the lane's
+// bonds TPO apart.
+template <int TPO>
+__device__ __forceinline__ void csr_cursor(int lane, int64_t b0, int64_t b1, int64_t* base, int* left) {
+  const int rem = (int)(b1 - b0) - lane;
+  *base = b0 + lane;
+  *left = rem > 0 ? (rem + TPO - 1) / TPO : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Sliced (SELL) bond stream of the 4-lanes-per-point passes. Slice s = the 8
+// owners of a warp; lane l32 = 4*o + (r mod 4) of the warp takes owner o's
+// bonds r = l32 mod 4, +4, +8, ...; each row is padded with dummy bonds
+// (damage byte 2) to the slice's longest, G = soff[s+1] - soff[s] groups of
+// 32 slots (one bond per lane) from slot 32*soff[s].
+// Blocked layout: the slice's first 4*floor(G/4) groups form blocks of 4
+// groups (128 slots) in which a lane's 4 bonds are adjacent (slot 4*l32 + k,
+// k = group mod 4), so that a lane reads a block's 4 ids as one int4, its 4
+// damage bytes as one word and each X component of its 4 bonds as one
+// float4, and a warp load is 512 consecutive bytes. The tail (< 4 groups)
+// keeps one slot per lane per group (slot l32 of the group). X sits in units
+// of 3 planes: a block's X at 3*(its first slot), planes 128 floats apart; a
+// tail group's at 3*(its first slot), planes 32 floats apart.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t sell_index(const int64_t* __restrict__ soff, int64_t i, int64_t r) {
+  const int64_t s = i >> 3, so = soff[s], full = (soff[s + 1] - so) & ~int64_t(3), g = r >> 2;
+  const int l32 = (int)((i & 7) * 4 + (r & 3));
+  return g < full ? 32 * (so + (g & ~int64_t(3))) + 4 * l32 + (g & 3) : 32 * (so + g) + l32;
+}
+// Index of plane 0 of the X of that slot in bx3, and the plane stride.
+__device__ __forceinline__ int64_t sell_x_index(const int64_t* __restrict__ soff, int64_t i, int64_t r, int* stride) {
+  const int64_t s = i >> 3, so = soff[s], full = (soff[s + 1] - so) & ~int64_t(3), g = r >> 2;
+  const int l32 = (int)((i & 7) * 4 + (r & 3));
+  if (g < full) {
+    *stride = 128;
+    return 96 * (so + (g & ~int64_t(3))) + 4 * l32 + (g & 3);
+  }
+  *stride = 32;
+  return 96 * (so + g) + l32;
+}
+
+template <bool NC>
+__device__ __forceinline__ Rec8 ld_rec_t(const Rec8* p) {
+  return NC ? ld_rec_nc(p) : ld_rec(p);
+}
+
+// Walks lane `lane` of owner i through its bonds of the sliced stream: the
+// full blocks with one int4 of ids (loaded one block ahead), one damage word
+// and three float4 of X per block, then the tail groups. For each bond, in
+// the lane's row order, body(X0, X1, X2, damage byte, neighbor record,
+// neighbor's critical stretch, the bond's damage byte in the stream, row
+// offset r - lane). NC: neighbor records through the read-only path (no
+// record written by the kernel). PAIR: the neighbors' critical stretch
+// scf[j] is gathered with their records (else -1 is passed).
+template <bool NC, bool PAIR, typename Body>
+__device__ __forceinline__ void sell_walk(int64_t i, int lane, const int64_t* __restrict__ soff,
+                                          const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+                                          const float* __restrict__ bx3, const Rec8* __restrict__ ur,
+                                          const float* __restrict__ scf, Body&& body) {
+  const int64_t s = i >> 3, so = soff[s];
+  const int G = (int)(soff[s + 1] - so), F = G >> 2;
+  const int l32 = (int)(i & 7) * 4 + lane;
+  const int4* pc = reinterpret_cast<const int4*>(col + 32 * so + 4 * l32);
+  uint32_t* pd = reinterpret_cast<uint32_t*>(dmg + 32 * so + 4 * l32);
+  const float4* px = reinterpret_cast<const float4*>(bx3 + 96 * so + 4 * l32);
+  int4 jn = F > 0 ? __ldcs(pc) : make_int4(0, 0, 0, 0);
+#pragma unroll 1
+  for (int b = 0; b < F; ++b, pc += 32, pd += 32, px += 96) {
+    const int4 jj = jn;
+    if (b + 1 < F) jn = __ldcs(pc + 32);
+    const uint32_t dw = __ldcs(pd);
+    const float4 xa = __ldcs(px), xb = __ldcs(px + 32), xc = __ldcs(px + 64);
+    const Rec8 u0 = ld_rec_t<NC>(ur + jj.x), u1 = ld_rec_t<NC>(ur + jj.y), u2 = ld_rec_t<NC>(ur + jj.z),
+               u3 = ld_rec_t<NC>(ur + jj.w);
+    float4 sj = make_float4(-1.f, -1.f, -1.f, -1.f);
+    if (PAIR) sj = make_float4(__ldg(scf + jj.x), __ldg(scf + jj.y), __ldg(scf + jj.z), __ldg(scf + jj.w));
+    uint8_t* pb = reinterpret_cast<uint8_t*>(pd);
+    const int r0 = 16 * b;
+    body(xa.x, xb.x, xc.x, (int)(dw & 0xffu), u0, sj.x, pb, r0);
+    body(xa.y, xb.y, xc.y, (int)((dw >> 8) & 0xffu), u1, sj.y, pb + 1, r0 + 4);
+    body(xa.z, xb.z, xc.z, (int)((dw >> 16) & 0xffu), u2, sj.z, pb + 2, r0 + 8);
+    body(xa.w, xb.w, xc.w, (int)(dw >> 24), u3, sj.w, pb + 3, r0 + 12);
+  }
+  const int T = G - 4 * F;
+  if (T > 0) {  // tail groups: masked, one slot per lane per group
+    const int64_t t0 = 32 * (so + 4 * F) + l32;
+    const float* pt = bx3 + 96 * (so + 4 * F) + l32;
+    int32_t jj[3];
+    int dd[3];
+    float X0[3], X1[3], X2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const bool in = k < T;
+      jj[k] = in ? __ldcs(col + t0 + 32 * k) : (int32_t)i;
+      dd[k] = in ? (int)dmg[t0 + 32 * k] : kDummyBond;
+      X0[k] = in ? __ldcs(pt + 96 * k) : 1.0f;
+      X1[k] = in ? __ldcs(pt + 96 * k + 32) : 0.0f;
+      X2[k] = in ? __ldcs(pt + 96 * k + 64) : 0.0f;
+    }
+    Rec8 uu[3];
+    float sj[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      uu[k] = ld_rec_t<NC>(ur + jj[k]);
+      sj[k] = PAIR ? __ldg(scf + jj[k]) : -1.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      body(X0[k], X1[k], X2[k], dd[k], uu[k], sj[k], dmg + t0 + 32 * k, 16 * F + 4 * k);
+  }
+}
+
+// The same walk over a CSR row (TPO lanes per point, the lane's bonds TPO
+// apart), kUnroll bonds per batch with the next batch's ids loaded ahead.
+template <int TPO, bool NC, bool PAIR, typename Body>
+__device__ __forceinline__ void csr_walk(int64_t i, int lane, int64_t b0, int64_t b1, const int32_t* __restrict__ col,
+                                         uint8_t* __restrict__ dmg, const float* __restrict__ bx3,
+                                         const Rec8* __restrict__ ur, const float* __restrict__ scf, Body&& body) {
+  int64_t slot;
+  int left;
+  csr_cursor<TPO>(lane, b0, b1, &slot, &left);
+  int32_t jn[kUnroll];
+#pragma unroll
+  for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(col + slot + TPO * k) : (int32_t)i;
+#pragma unroll 1
+  for (; left > 0; left -= kUnroll, slot += kUnroll * TPO) {
+    int dd[kUnroll];
+    float X0[kUnroll], X1[kUnroll], X2[kUnroll];
+    int32_t jj[kUnroll];
+    Rec8 uu[kUnroll];
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      jj[k] = jn[k];
+      jn[k] = k + kUnroll < left ? __ldcs(col + slot + TPO * (k + kUnroll)) : (int32_t)i;
+    }
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const bool in = k < left;
+      const float* p = bx3 + xs_index(slot + TPO * k);
+      dd[k] = in ? (int)dmg[slot + TPO * k] : kDummyBond;  // past the row end
+      X0[k] = in ? __ldcs(p) : 1.0f;
+      X1[k] = in ? __ldcs(p + 32) : 0.0f;
+      X2[k] = in ? __ldcs(p + 64) : 0.0f;
+    }
+    float sj[kUnroll];
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      uu[k] = ld_rec_t<NC>(ur + jj[k]);
+      sj[k] = PAIR ? __ldg(scf + jj[k]) : -1.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k)
+      body(X0[k], X1[k], X2[k], dd[k], uu[k], sj[k], dmg + slot + TPO * k, (int)(slot + TPO * k - b0 - lane));
   }
 }
 
@@ -201,20 +455,21 @@ __global__ void k_pack_owner(int64_t n, const double4* __restrict__ pt, const do
                        (float)sc[i]);
 }
 
-// Split-path bond stream bx = (X = x_j - x_i, omega(|X|, h_i) * V_j): the
-// difference and the influence weight in FP64, each rounded once to FP32. In
-// CSR order (SELL false), or in the sliced order of bond_cursor (SELL true,
-// with the neighbor ids and damage bytes copied alongside).
-__device__ __forceinline__ int64_t sell_index(const int64_t* __restrict__ soff, int64_t i, int64_t r) {
-  return soff[i >> 3] * 32 + (r >> 2) * 32 + (i & 7) * 4 + (r & 3);
+// Split-path bond stream bx3: X = x_j - x_i in FP64, rounded once to FP32, at
+// the slot's position in the grouped planes (xs_index). In CSR order (SELL
+// false), or in the sliced order of bond_cursor (SELL true, with the neighbor
+// ids and damage bytes copied alongside).
+__device__ __forceinline__ void put_x(float* __restrict__ p, int stride, float X0, float X1, float X2) {
+  p[0] = X0;
+  p[stride] = X1;
+  p[2 * stride] = X2;
 }
 
 template <int TPO, bool SELL>
 __global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t* __restrict__ row,
                                                        const int32_t* __restrict__ col,
-                                                       const double4* __restrict__ xv,
-                                                       const double* __restrict__ hp, int influence,
-                                                       float4* __restrict__ bx, const int64_t* __restrict__ soff,
+                                                       const double4* __restrict__ xv, float* __restrict__ bx3,
+                                                       const int64_t* __restrict__ soff,
                                                        const uint8_t* __restrict__ dmg, int32_t* __restrict__ scol,
                                                        uint8_t* __restrict__ sdmg) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -222,32 +477,43 @@ __global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t*
   const int lane = threadIdx.x & (TPO - 1);
   if (i >= n) return;
   const double4 xi = xv[i];
-  const double h = hp[i];
   const int64_t b0 = row[i];
   for (int64_t b = b0 + lane; b < row[i + 1]; b += TPO) {
     const int32_t j = col[b];
     const double4 xj = xv[j];
-    const double dx = __dsub_rn(xj.x, xi.x), dy = __dsub_rn(xj.y, xi.y), dz = __dsub_rn(xj.z, xi.z);
-    const double om = omega_d(influence, __dsqrt_rn(sq3_rn(dx, dy, dz)), h);
-    const float4 rec = make_float4((float)dx, (float)dy, (float)dz, (float)__dmul_rn(om, xj.w));
+    const float X0 = (float)__dsub_rn(xj.x, xi.x), X1 = (float)__dsub_rn(xj.y, xi.y),
+                X2 = (float)__dsub_rn(xj.z, xi.z);
     if (SELL) {
       const int64_t k = sell_index(soff, i, b - b0);
-      bx[k] = rec;
+      int stride;
+      put_x(bx3 + sell_x_index(soff, i, b - b0, &stride), stride, X0, X1, X2);
       scol[k] = j;
       sdmg[k] = dmg[b];
     } else {
-      bx[b] = rec;
+      put_x(bx3 + xs_index(b), 32, X0, X1, X2);
     }
   }
-  if (SELL) {  // padding to the slice's longest row: dummy bonds, damage byte 2
+  if (SELL) {  // padding to the slice's longest row: dummy bonds (kDummyBond)
     const int64_t len = row[i + 1] - b0, ms = soff[(i >> 3) + 1] - soff[i >> 3];
     for (int64_t r = len + lane; r < 4 * ms; r += TPO) {
       const int64_t k = sell_index(soff, i, r);
-      bx[k] = make_float4(1.f, 0.f, 0.f, 0.f);
+      int stride;
+      put_x(bx3 + sell_x_index(soff, i, r, &stride), stride, 1.f, 0.f, 0.f);
       scol[k] = (int32_t)i;
-      sdmg[k] = 2;
+      sdmg[k] = kDummyBond;
     }
   }
+}
+
+// Split-path point volumes in record slot 5 of both state buffers (the state
+// writers touch slots 0-4, the dilatation pass slots 6-7).
+__global__ void k_pack_volume(int64_t n, const double4* __restrict__ xv, Rec8* __restrict__ ur0,
+                              Rec8* __restrict__ ur1) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float V = (float)xv[i].w;
+  ur0[i].v[5] = V;
+  ur1[i].v[5] = V;
 }
 
 // Slots per slice (groups of 4 bonds of its longest row).
@@ -282,12 +548,17 @@ __global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* _
 //   theta_i = 3/m_i * sum omega*(1-d)*|X|*e*V_j  (material_utilities.cxx:284)
 // Writes the owner terms A_i = theta_i*(3K-5mu)/m, B_i = 15mu/m into ur[i].
 // ---------------------------------------------------------------------------
-template <int TPO, bool SELL, bool LIN = false>
-__global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_dilatation_split(
+// WEIGHT: an influence function other than "One", omega(|X|, h_i) evaluated per bond.
+// (the weighted variants get 96 registers: the omega evaluation would spill at 64)
+// PAIR: the two halves of a bond can differ (critical stretch varying along
+// bonds, or half-broken bonds set by the caller): the partner's test runs
+// with its own s_c,j, gathered per bond.
+template <int TPO, bool SELL, bool LIN = false, bool WEIGHT = false, bool PAIR = false>
+__global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
-    const float4* __restrict__ bx, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
+    const float* __restrict__ bx3, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
     double* __restrict__ theta_out, double* __restrict__ node_damage, const int64_t* __restrict__ soff,
-    uint8_t* __restrict__ dmg_csr) {
+    uint8_t* __restrict__ dmg_csr, const double* __restrict__ hp, int influence, const float* __restrict__ scf) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -298,56 +569,32 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_dilatation_split(
   if (valid) {
     const int64_t b0 = row[i];
     len = (int)(row[i + 1] - b0);
-    const Rec8 ui = ld_rec(ur + i);
+    const OwnU ui = own_u(ld_rec(ur + i));
     const float s_c = damage_on ? own[i].w : -1.0f;
-    // Branch-free masking (selects) of past-the-end and broken bonds; the
-    // batch's bond-ordered loads first (independent), then its gathers.
-    constexpr int kS = SELL ? 32 : TPO;
-    int64_t base;
-    int left;
-    bond_cursor<TPO, SELL>(i, lane, b0, b0 + len, soff, &base, &left);
-    const float4* nbx = bx + base;
-    const int32_t* ncol = col + base;
-    uint8_t* pdm = dmg + base;
+    const float hi = WEIGHT ? (float)hp[i] : 1.0f;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
-    int32_t jn[kUnroll];  // neighbor ids of the next batch, loaded one batch ahead
-#pragma unroll
-    for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(ncol + kS * k) : (int32_t)i;
-#pragma unroll 1
-    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS,
-                     cdm += SELL ? kUnroll * TPO : 0) {
-      int dd[kUnroll];
-      float4 qq[kUnroll];
-      int32_t jj[kUnroll];
-      Rec8 uu[kUnroll];
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        jj[k] = jn[k];
-        jn[k] = k + kUnroll < left ? __ldcs(ncol + kS * (k + kUnroll)) : (int32_t)i;
+    // Branch-free masking (selects) of dummy and broken bonds.
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, float scj, uint8_t* pdm, int r) {
+      const SplitBond sb = split_bond(X0, X1, X2, ui, uj);
+      const bool own_ok = (d & 5) == 0;  // own half intact (and a real bond)
+      const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
+      // the partner's half: its own test, or the same test on both halves
+      const bool brkp = PAIR ? ((d & 6) == 0 && damage_on && scj >= 0.0f && sb.e > scj * sb.zeta) : brk;
+      if (brk || brkp) {
+        const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
+        *pdm = nd;
+        if (SELL) cdm[r] = nd;  // the CSR copy stays canonical
       }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const bool in = k < left;
-        dd[k] = in ? (int)pdm[kS * k] : 2;  // 2: past the row end
-        qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec(ur + jj[k]);
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const float4 q = qq[k];
-        const SplitBond sb = split_bond(q, ui, uu[k]);
-        const bool intact = dd[k] == 0;
-        const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
-        if (brk) {
-          pdm[kS * k] = 1;
-          if (SELL) cdm[TPO * k] = 1;  // the CSR copy stays canonical
-        }
-        broken += (dd[k] == 1 || brk) ? 1 : 0;
-        // LPS: omega V_j |X| e; linear LPS: omega V_j X.du
-        th = fmaf((intact && !brk) ? (LIN ? q.w : q.w * sb.zeta) : 0.0f, LIN ? sb.xu : sb.e, th);
-      }
-    }
+      broken += ((d & 1) || brk) ? 1 : 0;
+      float wv = uj.v[5];  // V_j
+      if constexpr (WEIGHT) wv *= omega_f(influence, sb.zeta, hi);
+      // LPS: omega V_j |X| e; linear LPS: omega V_j X.du
+      th = fmaf((own_ok && !brk) ? (LIN ? wv : wv * sb.zeta) : 0.0f, LIN ? sb.xu : sb.e, th);
+    };
+    if constexpr (SELL)
+      sell_walk<false, PAIR>(i, lane, soff, col, dmg, bx3, ur, scf, body);
+    else
+      csr_walk<TPO, false, PAIR>(i, lane, b0, b0 + len, col, dmg, bx3, ur, scf, body);
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
@@ -371,7 +618,7 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_fp64(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const double4* __restrict__ xv, const double4* __restrict__ st, const double4* __restrict__ pt,
     const double* __restrict__ sc, const double* __restrict__ hp, int influence, int damage_on,
-    double4* __restrict__ ab64, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+    double4* __restrict__ ab64, double* __restrict__ theta_out, double* __restrict__ node_damage, int pair) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -389,7 +636,8 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_fp64(
     const double s_c = damage_on ? sc[i] : -1.0;
     const double h = hp[i];
     for (int64_t b = b0 + lane; b < b1; b += TPO) {
-      if (dmg[b]) {
+      const int d = dmg[b];  // bit 0: this half broken, bit 1: the partner's half
+      if ((d & 3) == 3) {
         broken++;
         continue;
       }
@@ -398,8 +646,17 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_fp64(
       const double4 yj = st[j];
       const double zeta = __dsqrt_rn(sq3_rn(__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z)));
       const double dY = __dsqrt_rn(sq3_rn(__dsub_rn(yj.x, yi.x), __dsub_rn(yj.y, yi.y), __dsub_rn(yj.z, yi.z)));
-      if (s_c >= 0.0 && __ddiv_rn(__dsub_rn(dY, zeta), zeta) > s_c) {
-        dmg[b] = 1;
+      // this half's test with s_c,i; the partner's with s_c,j (the same test
+      // on both halves when the critical stretch is one along every bond)
+      const double scj = pair && damage_on ? sc[j] : s_c;
+      bool brk = false, brkp = false;
+      if ((s_c >= 0.0 && !(d & 1)) || (scj >= 0.0 && !(d & 2))) {
+        const double rel = __ddiv_rn(__dsub_rn(dY, zeta), zeta);
+        brk = !(d & 1) && s_c >= 0.0 && rel > s_c;
+        brkp = !(d & 2) && scj >= 0.0 && rel > scj;
+      }
+      if (brk || brkp) dmg[b] = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
+      if ((d & 1) || brk) {
         broken++;
         continue;
       }
@@ -455,14 +712,17 @@ __device__ __forceinline__ double* comp_ptr(double4* q, int c) {
   return c == 0 ? &q->x : (c == 1 ? &q->y : &q->z);
 }
 
-__device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int c, double f, double xc,
-                                                double rho) {
+// Returns the new displacement component (the FP64 u written back); the split
+// passes pack it into the next record afterwards (store_u_record_group, which
+// needs the group's three components at once).
+__device__ __forceinline__ double verlet_epilogue(const EpiArgs& E, int64_t i, int c, double f, double xc,
+                                                  double rho) {
   const int64_t k = 3 * i + c;
   double ftot = f;
   if (E.has_contact) ftot = __dadd_rn(ftot, E.fc[k]);
   if (!isfinite(ftot)) atomicOr(E.status, ST_NONFINITE_FORCE);
   if (E.f_out) E.f_out[k] = ftot;
-  if (E.mode == EVAL_ONLY) return;
+  if (E.mode == EVAL_ONLY) return 0.0;
   const double dt = E.dt, dt2 = E.dt / 2.0;
   const double acc = __ddiv_rn(__dadd_rn(ftot, 0.0), rho);
   double v = E.v[k];
@@ -470,7 +730,7 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
   if (E.mode == EVAL_LAST) {
     E.v[k] = v;
     E.a[k] = acc;
-    return;
+    return 0.0;
   }
   // first half of step s+1
   double vh = __dadd_rn(v, __dmul_rn(dt2, acc));
@@ -490,14 +750,21 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
   const double u = E.u[k];
   const double un = __dadd_rn(u, step_dx);  // u += dt*v
   E.u[k] = un;
-  if (E.split) {
-    float hi, lo;
-    split_hi_lo(un, &hi, &lo);
-    E.ur_next[i].v[c] = hi;
-    E.ur_next[i].v[c + 3] = lo;
-  } else {
-    *comp_ptr(&E.st_next[i], c) = __dadd_rn(__dadd_rn(xc, u), step_dx);  // y = x+u+dt*v
+  if (!E.split) *comp_ptr(&E.st_next[i], c) = __dadd_rn(__dadd_rn(xc, u), step_dx);  // y = x+u+dt*v
+  return un;
+}
+
+// Split passes: the group's epilogue (lanes 0-2, one component each) and the
+// next displacement record. Every lane of the warp calls it.
+template <int TPO>
+__device__ __forceinline__ void split_epilogue(const EpiArgs& E, int64_t i, int lane, bool valid, float fx, float fy,
+                                               float fz, const double4* __restrict__ pt) {
+  double un = 0.0;
+  if (valid && lane < 3) {
+    const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
+    un = verlet_epilogue(E, i, lane, f, 0.0, pt[i].w);
   }
+  if (E.mode == EVAL_ADVANCE) store_u_record_group<TPO>(E.ur_next + i, lane, un, valid);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,14 +773,18 @@ __device__ __forceinline__ void verlet_epilogue(const EpiArgs& E, int64_t i, int
 //   f_i += (t_ij + t_ji) * V_j * Y/|Y|
 // Broken bonds carry t = 0 (elastic.cxx:120 with d = 1) and are skipped.
 // ---------------------------------------------------------------------------
-template <int TPO, bool SELL, bool LIN = false, bool CHUNK = false>
-__global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
+#ifndef PD_FORCE_NC
+#define PD_FORCE_NC 1
+#endif
+template <int TPO, bool SELL, bool LIN = false, bool CHUNK = false, bool WEIGHT = false, bool PAIR = false>
+__global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_force_split(int64_t n, const int64_t* __restrict__ row,
                                                                       const int32_t* __restrict__ col,
                                                                       const uint8_t* __restrict__ dmg,
-                                                                      const float4* __restrict__ bx,
+                                                                      const float* __restrict__ bx3,
                                                                       const Rec8* __restrict__ ur,
                                                                       const double4* __restrict__ pt, EpiArgs E,
                                                                       const int64_t* __restrict__ soff,
+                                                                      const double* __restrict__ hp, int influence,
                                                                       int64_t i0 = 0) {
   // CHUNK: owners i0 .. n-1 (a chunk of the points starts at a multiple of 64
   // owners); otherwise i0 is not used and the pass covers 0 .. n-1
@@ -523,66 +794,48 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_force_split(int64
   const bool valid = i < n;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (valid) {
-    const Rec8 ui = ld_rec_nc(ur + i);
-    const int64_t b1 = row[i + 1];
-    constexpr int kS = SELL ? 32 : TPO;
-    const int64_t b0 = row[i];
-    int64_t base;
-    int left;
-    bond_cursor<TPO, SELL>(i, lane, b0, b1, soff, &base, &left);
-    const float4* nbx = bx + base;
-    const int32_t* ncol = col + base;
-    const uint8_t* pdm = dmg + base;
-    int32_t jn[kUnroll];  // neighbor ids of the next batch, loaded one batch ahead
-#pragma unroll
-    for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(ncol + kS * k) : (int32_t)i;
-#pragma unroll 1
-    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS) {
-      bool live[kUnroll];
-      float4 qq[kUnroll];
-      int32_t jj[kUnroll];
-      Rec8 uu[kUnroll];
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        jj[k] = jn[k];
-        jn[k] = k + kUnroll < left ? __ldcs(ncol + kS * (k + kUnroll)) : (int32_t)i;
+    const Rec8 ri = ld_rec_t<PD_FORCE_NC>(ur + i);
+    const OwnU ui = own_u(ri);
+    const float Ai = ri.v[6], Bi = ri.v[7];
+    const float hi = WEIGHT ? (float)hp[i] : 1.0f;
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, float, uint8_t*, int) {
+      const SplitBond sb = split_bond(X0, X1, X2, ui, uj);
+      float wv = uj.v[5];  // V_j
+      if constexpr (WEIGHT) wv *= omega_f(influence, sb.zeta, hi);
+      // owner terms of the intact halves: t_ij with (1 - d_ij), t_ji with (1 - d_ji)
+      float a, b;
+      if constexpr (PAIR) {
+        const bool own_live = (d & 5) == 0, part_live = (d & 6) == 0;
+        a = (own_live ? Ai : 0.0f) + (part_live ? uj.v[6] : 0.0f);
+        b = (own_live ? Bi : 0.0f) + (part_live ? uj.v[7] : 0.0f);
+      } else {
+        a = Ai + uj.v[6];
+        b = Bi + uj.v[7];
+        wv = d == 0 ? wv : 0.0f;
       }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const bool in = k < left;
-        live[k] = in ? pdm[kS * k] == 0 : false;
-        qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
+      if constexpr (LIN) {
+        // omega V_j ((A_i + A_j) X + (B_i + B_j) (X.du / |X|^2) X), along the reference bond X
+        const float w = fmaf(b, __fdividef(sb.xu, sb.xx), a) * wv;
+        fx = fmaf(w, X0, fx);
+        fy = fmaf(w, X1, fy);
+        fz = fmaf(w, X2, fz);
+      } else {
+        const float w = fmaf(sb.zeta, a, sb.e * b) * wv * sb.ry;
+        fx = fmaf(w, sb.Yx, fx);
+        fy = fmaf(w, sb.Yy, fy);
+        fz = fmaf(w, sb.Yz, fz);
       }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const float4 q = qq[k];
-        const SplitBond sb = split_bond(q, ui, uu[k]);
-        if constexpr (LIN) {
-          // omega V_j ((A_i + A_j) X + (B_i + B_j) (X.du / |X|^2) X), along the reference bond X
-          const float c = fmaf(ui.v[7] + uu[k].v[7], __fdividef(sb.xu, sb.xx), ui.v[6] + uu[k].v[6]);
-          const float w = live[k] ? c * q.w : 0.0f;
-          fx = fmaf(w, q.x, fx);
-          fy = fmaf(w, q.y, fy);
-          fz = fmaf(w, q.z, fz);
-        } else {
-          const float T = fmaf(sb.zeta, ui.v[6] + uu[k].v[6], sb.e * (ui.v[7] + uu[k].v[7]));
-          const float w = live[k] ? T * q.w * sb.ry : 0.0f;
-          fx = fmaf(w, sb.Yx, fx);
-          fy = fmaf(w, sb.Yy, fy);
-          fz = fmaf(w, sb.Yz, fz);
-        }
-      }
-    }
+    };
+    uint8_t* dm = const_cast<uint8_t*>(dmg);  // not written by this pass
+    if constexpr (SELL)
+      sell_walk<PD_FORCE_NC, false>(i, lane, soff, col, dm, bx3, ur, nullptr, body);
+    else
+      csr_walk<TPO, PD_FORCE_NC, false>(i, lane, row[i], row[i + 1], col, dm, bx3, ur, nullptr, body);
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
   fz = group_sum<TPO>(fz);
-  if (valid && lane < 3) {
-    const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
-    verlet_epilogue(E, i, lane, f, 0.0, pt[i].w);
-  }
+  split_epilogue<TPO>(E, i, lane, valid, fx, fy, fz, pt);
 }
 
 // ---------------------------------------------------------------------------
@@ -614,7 +867,8 @@ __global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t*
     const double hi = hp[i];
     const int64_t b1 = row[i + 1];
     for (int64_t b = row[i] + lane; b < b1; b += TPO) {
-      if (dmg[b]) continue;
+      const int d = dmg[b];  // bit 0: t_ij's half broken, bit 1: t_ji's
+      if ((d & 3) == 3) continue;
       const int32_t j = col[b];
       const double4 xj = xv[j];
       const double4 yj = st[j];
@@ -630,12 +884,16 @@ __global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t*
       const double tj = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(om_j, aj.x), aj.y), zeta),
                                   __dmul_rn(__dmul_rn(om_j, aj.z), e));
       const double V = xj.w;
-      fx = __dadd_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yx), dY), V));
-      fy = __dadd_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yy), dY), V));
-      fz = __dadd_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yz), dY), V));
-      fx = __dsub_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yx), dY), V));
-      fy = __dsub_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yy), dY), V));
-      fz = __dsub_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yz), dY), V));
+      if (!(d & 1)) {
+        fx = __dadd_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yx), dY), V));
+        fy = __dadd_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yy), dY), V));
+        fz = __dadd_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yz), dY), V));
+      }
+      if (!(d & 2)) {
+        fx = __dsub_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yx), dY), V));
+        fy = __dsub_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yy), dY), V));
+        fz = __dsub_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yz), dY), V));
+      }
     }
   }
   fx = group_sum<TPO>(fx);
@@ -666,7 +924,7 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_lin_fp64(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const double4* __restrict__ xv, const double4* __restrict__ st, const double4* __restrict__ pt,
     const double* __restrict__ sc, const double* __restrict__ hp, int influence, int damage_on,
-    double4* __restrict__ ab64, double* __restrict__ theta_out, double* __restrict__ node_damage) {
+    double4* __restrict__ ab64, double* __restrict__ theta_out, double* __restrict__ node_damage, int pair) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -683,7 +941,8 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_lin_fp64(
     const double h = hp[i];
     const double ui0 = __dsub_rn(yi.x, xi.x), ui1 = __dsub_rn(yi.y, xi.y), ui2 = __dsub_rn(yi.z, xi.z);
     for (int64_t b = b0 + lane; b < b1; b += TPO) {
-      if (dmg[b]) {
+      const int d = dmg[b];  // bit 0: this half broken, bit 1: the partner's half
+      if ((d & 3) == 3) {
         broken++;
         continue;
       }
@@ -692,13 +951,18 @@ __global__ void __launch_bounds__(kBlock) k_dilatation_lin_fp64(
       const double4 yj = st[j];
       const double z0 = __dsub_rn(xj.x, xi.x), z1 = __dsub_rn(xj.y, xi.y), z2 = __dsub_rn(xj.z, xi.z);
       const double zeta = __dsqrt_rn(sq3_rn(z0, z1, z2));
-      if (s_c >= 0.0) {
+      const double scj = pair && damage_on ? sc[j] : s_c;
+      bool brk = false, brkp = false;
+      if ((s_c >= 0.0 && !(d & 1)) || (scj >= 0.0 && !(d & 2))) {
         const double dY = __dsqrt_rn(sq3_rn(__dsub_rn(yj.x, yi.x), __dsub_rn(yj.y, yi.y), __dsub_rn(yj.z, yi.z)));
-        if (__ddiv_rn(__dsub_rn(dY, zeta), zeta) > s_c) {
-          dmg[b] = 1;
-          broken++;
-          continue;
-        }
+        const double rel = __ddiv_rn(__dsub_rn(dY, zeta), zeta);
+        brk = !(d & 1) && s_c >= 0.0 && rel > s_c;
+        brkp = !(d & 2) && scj >= 0.0 && rel > scj;
+      }
+      if (brk || brkp) dmg[b] = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
+      if ((d & 1) || brk) {
+        broken++;
+        continue;
       }
       const double d0 = __dsub_rn(__dsub_rn(yj.x, xj.x), ui0), d1 = __dsub_rn(__dsub_rn(yj.y, xj.y), ui1),
                    d2 = __dsub_rn(__dsub_rn(yj.z, xj.z), ui2);
@@ -742,7 +1006,8 @@ __global__ void __launch_bounds__(kBlock) k_force_lin_fp64(int64_t n, const int6
     const double ui0 = __dsub_rn(yi.x, xi.x), ui1 = __dsub_rn(yi.y, xi.y), ui2 = __dsub_rn(yi.z, xi.z);
     const int64_t b1 = row[i + 1];
     for (int64_t b = row[i] + lane; b < b1; b += TPO) {
-      if (dmg[b]) continue;
+      const int d = dmg[b];  // bit 0: t_ij's half broken, bit 1: t_ji's
+      if ((d & 3) == 3) continue;
       const int32_t j = col[b];
       const double4 xj = xv[j];
       const double4 yj = st[j];
@@ -763,8 +1028,8 @@ __global__ void __launch_bounds__(kBlock) k_force_lin_fp64(int64_t n, const int6
       for (int r = 0; r < 3; ++r) {
         const double mv = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(z[r], z[0]), du[0]), __dmul_rn(__dmul_rn(z[r], z[1]), du[1])),
                                     __dmul_rn(__dmul_rn(z[r], z[2]), du[2]));
-        f[r] = __dadd_rn(f[r], __dmul_rn(__dadd_rn(__dmul_rn(t1i, z[r]), __dmul_rn(t2i, mv)), V));
-        f[r] = __dadd_rn(f[r], __dmul_rn(__dadd_rn(__dmul_rn(t1j, z[r]), __dmul_rn(t2j, mv)), V));
+        if (!(d & 1)) f[r] = __dadd_rn(f[r], __dmul_rn(__dadd_rn(__dmul_rn(t1i, z[r]), __dmul_rn(t2i, mv)), V));
+        if (!(d & 2)) f[r] = __dadd_rn(f[r], __dmul_rn(__dadd_rn(__dmul_rn(t1j, z[r]), __dmul_rn(t2j, mv)), V));
       }
     }
   }
@@ -811,7 +1076,7 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
                                                     const double4* __restrict__ xv, const double4* __restrict__ st,
                                                     const double4* __restrict__ pt, const double* __restrict__ sc,
                                                     const double* __restrict__ hp, int damage_on, int plane,
-                                                    double height, double* __restrict__ node_damage, EpiArgs E) {
+                                                    double height, double* __restrict__ node_damage, EpiArgs E, int pair) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -825,7 +1090,8 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
     const double s_c = damage_on ? sc[i] : -1.0;
     nbond = row[i + 1] - row[i];
     for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
-      if (dmg[b]) {
+      const int d = dmg[b];  // bit 0: this half broken, bit 1: the partner's half
+      if ((d & 3) == 3) {
         broken++;
         continue;
       }
@@ -835,21 +1101,27 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
       const double Yx = __dsub_rn(yj.x, yi.x), Yy = __dsub_rn(yj.y, yi.y), Yz = __dsub_rn(yj.z, yi.z);
       const double dY = __dsqrt_rn(sq3_rn(Yx, Yy, Yz));
       const double stretch = __ddiv_rn(__dsub_rn(dY, zeta), zeta);
-      if (s_c >= 0.0 && stretch > s_c) {
-        dmg[b] = 1;
-        broken++;
-        continue;
-      }
+      const double scj = pair && damage_on ? sc[j] : s_c;
+      const bool brk = !(d & 1) && s_c >= 0.0 && stretch > s_c;
+      const bool brkp = !(d & 2) && scj >= 0.0 && stretch > scj;
+      if (brk || brkp) dmg[b] = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
+      const bool own_live = !(d & 1) && !brk, part_live = !(d & 2) && !brkp;
+      if (!own_live) broken++;
+      if (!own_live && !part_live) continue;
       const double cj = bb_constant(pt[j].y, hp[j], plane, height);
       const double ti = __dmul_rn(__dmul_rn(0.5, stretch), ci);  // 0.5*(1-d)*stretch*constant, d = 0
       const double tj = __dmul_rn(__dmul_rn(0.5, stretch), cj);
       const double V = xj.w;
-      fx = __dadd_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yx), dY), V));
-      fy = __dadd_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yy), dY), V));
-      fz = __dadd_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yz), dY), V));
-      fx = __dsub_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yx), dY), V));
-      fy = __dsub_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yy), dY), V));
-      fz = __dsub_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yz), dY), V));
+      if (own_live) {
+        fx = __dadd_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yx), dY), V));
+        fy = __dadd_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yy), dY), V));
+        fz = __dadd_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(ti, Yz), dY), V));
+      }
+      if (part_live) {
+        fx = __dsub_rn(fx, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yx), dY), V));
+        fy = __dsub_rn(fy, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yy), dY), V));
+        fz = __dsub_rn(fz, __dmul_rn(__ddiv_rn(__dmul_rn(tj, -Yz), dY), V));
+      }
     }
   }
   fx = group_sum<TPO>(fx);
@@ -866,17 +1138,18 @@ __global__ void __launch_bounds__(kBlock) k_bb_fp64(int64_t n, const int64_t* __
 
 // Split-FP32 path: one pass (bond stream and neighbor ids loaded directly as
 // in the LPS passes), damage and pair force per bond, FP64 epilogue.
-template <int TPO, bool SELL>
+template <int TPO, bool SELL, bool PAIR = false>
 __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t n, const int64_t* __restrict__ row,
                                                                    const int32_t* __restrict__ col,
                                                                    uint8_t* __restrict__ dmg,
-                                                                   const float4* __restrict__ bx,
+                                                                   const float* __restrict__ bx3,
                                                                    const Rec8* __restrict__ ur,
                                                                    const float4* __restrict__ own, int damage_on,
                                                                    const double4* __restrict__ pt,
                                                                    double* __restrict__ node_damage, EpiArgs E,
                                                                    const int64_t* __restrict__ soff,
-                                                                   uint8_t* __restrict__ dmg_csr) {
+                                                                   uint8_t* __restrict__ dmg_csr,
+                                                                   const float* __restrict__ scf) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -887,74 +1160,48 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
   if (valid) {
     const int64_t b0 = row[i];
     len = (int)(row[i + 1] - b0);
-    const Rec8 ui = ld_rec_nc(ur + i);
+    const Rec8 ri = ld_rec_nc(ur + i);
+    const OwnU ui = own_u(ri);
+    const float ci = ri.v[6];
     const float s_c = damage_on ? own[i].w : -1.0f;
-    constexpr int kS = SELL ? 32 : TPO;
-    int64_t base;
-    int left;
-    bond_cursor<TPO, SELL>(i, lane, b0, b0 + len, soff, &base, &left);
-    const float4* nbx = bx + base;
-    const int32_t* ncol = col + base;
-    uint8_t* pdm = dmg + base;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
-    int32_t jn[kUnroll];  // neighbor ids of the next batch, loaded one batch ahead
-#pragma unroll
-    for (int k = 0; k < kUnroll; ++k) jn[k] = k < left ? __ldcs(ncol + kS * k) : (int32_t)i;
-#pragma unroll 1
-    for (; left > 0; left -= kUnroll, pdm += kUnroll * kS, nbx += kUnroll * kS, ncol += kUnroll * kS,
-                     cdm += SELL ? kUnroll * TPO : 0) {
-      int dd[kUnroll];
-      float4 qq[kUnroll];
-      int32_t jj[kUnroll];
-      Rec8 uu[kUnroll];
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        jj[k] = jn[k];
-        jn[k] = k + kUnroll < left ? __ldcs(ncol + kS * (k + kUnroll)) : (int32_t)i;
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, float scj, uint8_t* pdm, int r) {
+      const SplitBond sb = split_bond(X0, X1, X2, ui, uj);
+      const bool own_ok = (d & 5) == 0;
+      const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
+      const bool part_ok = PAIR ? (d & 6) == 0 : own_ok;
+      const bool brkp = PAIR ? (part_ok && damage_on && scj >= 0.0f && sb.e > scj * sb.zeta) : brk;
+      if (brk || brkp) {
+        const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
+        *pdm = nd;
+        if (SELL) cdm[r] = nd;
       }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const bool in = k < left;
-        dd[k] = in ? (int)pdm[kS * k] : 2;  // 2: past the row end
-        qq[k] = in ? __ldcs(nbx + kS * k) : make_float4(1.f, 0.f, 0.f, 0.f);
-      }
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_nc(ur + jj[k]);
-#pragma unroll
-      for (int k = 0; k < kUnroll; ++k) {
-        const float4 q = qq[k];
-        const SplitBond sb = split_bond(q, ui, uu[k]);
-        const bool intact = dd[k] == 0;
-        const bool brk = intact && s_c >= 0.0f && sb.e > s_c * sb.zeta;
-        if (brk) {
-          pdm[kS * k] = 1;
-          if (SELL) cdm[TPO * k] = 1;
-        }
-        broken += (dd[k] == 1 || brk) ? 1 : 0;
-        const float t = (ui.v[6] + uu[k].v[6]) * __fdividef(sb.e, sb.zeta);  // t_ij + t_ji
-        const float w = (intact && !brk) ? t * q.w * sb.ry : 0.0f;
-        fx = fmaf(w, sb.Yx, fx);
-        fy = fmaf(w, sb.Yy, fy);
-        fz = fmaf(w, sb.Yz, fz);
-      }
-    }
+      broken += ((d & 1) || brk) ? 1 : 0;
+      // t_ij + t_ji over the intact halves
+      const float c = ((own_ok && !brk) ? ci : 0.0f) + ((part_ok && !brkp) ? uj.v[6] : 0.0f);
+      const float w = c * __fdividef(sb.e, sb.zeta) * uj.v[5] * sb.ry;
+      fx = fmaf(w, sb.Yx, fx);
+      fy = fmaf(w, sb.Yy, fy);
+      fz = fmaf(w, sb.Yz, fz);
+    };
+    if constexpr (SELL)
+      sell_walk<true, PAIR>(i, lane, soff, col, dmg, bx3, ur, scf, body);
+    else
+      csr_walk<TPO, true, PAIR>(i, lane, b0, b0 + len, col, dmg, bx3, ur, scf, body);
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
   fz = group_sum<TPO>(fz);
   broken = group_sum<TPO>(broken);
   if (valid && lane == 0) node_damage[i] = len > 0 ? (double)broken / (double)len : 0.0;
-  if (valid && lane < 3) {
-    const double f = lane == 0 ? (double)fx : (lane == 1 ? (double)fy : (double)fz);
-    verlet_epilogue(E, i, lane, f, 0.0, pt[i].w);
-  }
+  split_epilogue<TPO>(E, i, lane, valid, fx, fy, fz, pt);
 }
 
 // ---------------------------------------------------------------------------
 // State conversions and the stable time step
 // ---------------------------------------------------------------------------
 // State from current coordinates y [3n]: u = y - x (FP64), then the gathered
-// copy (split: hi/lo record, FP64: y itself).
+// copy (split: displacement record, FP64: y itself).
 __global__ void k_state_from_y(int64_t n, const double* __restrict__ y, const double4* __restrict__ xv,
                                double* __restrict__ u, double4* __restrict__ st, Rec8* __restrict__ ur) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -966,25 +1213,21 @@ __global__ void k_state_from_y(int64_t n, const double* __restrict__ y, const do
   u[3 * i + 1] = u1;
   u[3 * i + 2] = u2;
   if (ur) {
-    split_hi_lo(u0, &ur[i].v[0], &ur[i].v[3]);
-    split_hi_lo(u1, &ur[i].v[1], &ur[i].v[4]);
-    split_hi_lo(u2, &ur[i].v[2], &ur[i].v[5]);
+    store_u_record(ur + i, u0, u1, u2);
   } else {
     st[i] = make_double4(y0, y1, y2, 0.0);
   }
 }
 
 // Gathered state from the displacement u [3n] (after pd_set_state): split ->
-// hi/lo record, FP64 -> y = x + u.
+// displacement record, FP64 -> y = x + u.
 __global__ void k_state_from_u(int64_t n, const double* __restrict__ u, const double4* __restrict__ xv,
                                double4* __restrict__ st, Rec8* __restrict__ ur) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 x = xv[i];
   if (ur) {
-    split_hi_lo(u[3 * i], &ur[i].v[0], &ur[i].v[3]);
-    split_hi_lo(u[3 * i + 1], &ur[i].v[1], &ur[i].v[4]);
-    split_hi_lo(u[3 * i + 2], &ur[i].v[2], &ur[i].v[5]);
+    store_u_record(ur + i, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
   } else {
     st[i] = make_double4(__dadd_rn(x.x, u[3 * i]), __dadd_rn(x.y, u[3 * i + 1]), __dadd_rn(x.z, u[3 * i + 2]), 0.0);
   }
@@ -1081,13 +1324,12 @@ cudaError_t launch_pack_owner(pd_ctx* c) {
   const bool bb = c->material_model == PD_MATERIAL_BOND_BASED;
   const int64_t n = c->n;
   k_pack_owner<<<grid1(n), kBlock, 0, c->stream>>>(n, c->pt.p, c->sc.p, c->own.p);
-  // the bond-based material has no influence function: bx.w = V_j
-  const int infl = bb ? PD_INFLUENCE_ONE : c->influence;
+  k_pack_volume<<<grid1(n), kBlock, 0, c->stream>>>(n, c->xv.p, c->ur[0].p, c->ur[1].p);
   c->sell = c->tpo_split == 4;
+  cudaError_t e;
   if (c->sell) {  // sliced bond stream of the 4-lanes-per-point passes
     const int64_t ns = (n + 7) / 8;
     pdb::DBuf<int64_t> cnt;
-    cudaError_t e;
     if ((e = cnt.alloc(ns + 1)) != cudaSuccess) return e;
     if ((e = c->sell_off.alloc(ns + 1)) != cudaSuccess) return e;
     k_sell_count<<<(unsigned)((ns + 1 + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(n, c->row.p, cnt.p);
@@ -1103,18 +1345,22 @@ cudaError_t launch_pack_owner(pd_ctx* c) {
         cudaSuccess)
       return e;
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
-    const size_t recs = (size_t)std::max<int64_t>(32 * slots, 1);
-    if ((e = c->bx.alloc(recs)) != cudaSuccess) return e;
-    if ((e = c->sell_col.alloc(recs)) != cudaSuccess) return e;
-    if ((e = c->sell_dmg.alloc(recs)) != cudaSuccess) return e;
-    k_pack_bonds<4, true><<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, c->hp.p, infl,
-                                                                    c->bx.p, c->sell_off.p, c->dmg.p, c->sell_col.p,
+    // slots counts 32-record groups: 32 ids and damage bytes, 96 floats of X each
+    const size_t groups = (size_t)std::max<int64_t>(slots, 1);
+    c->bx3.release();  // the old stream first: at memory scale both would not fit
+    if ((e = c->bx3.alloc(96 * groups)) != cudaSuccess) return e;
+    if ((e = c->sell_col.alloc(32 * groups)) != cudaSuccess) return e;
+    if ((e = c->sell_dmg.alloc(32 * groups)) != cudaSuccess) return e;
+    k_pack_bonds<4, true><<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, c->bx3.p,
+                                                                    c->sell_off.p, c->dmg.p, c->sell_col.p,
                                                                     c->sell_dmg.p);
     c->sell_src = c->dmg.p;
     c->sell_gen = c->dmg_gen;
   } else {
-    PD_DISPATCH_TPO_CSR(c->tpo, k_pack_bonds, grid_for(n, c->tpo), kBlock, n, c->row.p, c->col.p, c->xv.p, c->hp.p, infl,
-                        c->bx.p, nullptr, nullptr, nullptr, nullptr);
+    c->bx3.release();
+    if ((e = c->bx3.alloc(96 * (size_t)((c->nb + 31) / 32))) != cudaSuccess) return e;
+    PD_DISPATCH_TPO_CSR(c->tpo, k_pack_bonds, grid_for(n, c->tpo), kBlock, n, c->row.p, c->col.p, c->xv.p, c->bx3.p,
+                        nullptr, nullptr, nullptr, nullptr);
   }
   if (bb)
     k_bb_terms<<<grid1(n), kBlock, 0, c->stream>>>(n, c->pt.p, c->hp.p, c->bb_plane, c->bb_height, c->ur[0].p,
@@ -1143,6 +1389,55 @@ cudaError_t launch_sync_state(pd_ctx* c) {
     const cudaError_t e_ = (expr);     \
     if (e_ != cudaSuccess) return e_;  \
   } while (0)
+
+// Split-pass kernels by lanes per point (sliced stream at 4), material,
+// influence weighting and half-bond damage (all instances of a pass share one
+// signature).
+template <bool LIN, bool W, bool P>
+static decltype(&k_dilatation_split<4, true>) dil_split_kernel(int tpo, bool sell) {
+  if (sell || LIN) return &k_dilatation_split<4, true, LIN, W, P>;  // linear LPS runs on the sliced stream only
+  switch (tpo) {
+    case 4: return &k_dilatation_split<4, false, false, W, P>;
+    case 8: return &k_dilatation_split<8, false, false, W, P>;
+    case 16: return &k_dilatation_split<16, false, false, W, P>;
+    default: return &k_dilatation_split<32, false, false, W, P>;
+  }
+}
+template <bool LIN, bool CHUNK, bool W, bool P>
+static decltype(&k_force_split<4, true>) force_split_kernel(int tpo, bool sell) {
+  if (sell || LIN || CHUNK) return &k_force_split<4, true, LIN, CHUNK, W, P>;
+  switch (tpo) {
+    case 4: return &k_force_split<4, false, false, false, W, P>;
+    case 8: return &k_force_split<8, false, false, false, W, P>;
+    case 16: return &k_force_split<16, false, false, false, W, P>;
+    default: return &k_force_split<32, false, false, false, W, P>;
+  }
+}
+template <bool LIN, bool W>
+static decltype(&k_dilatation_split<4, true>) dil_split_for(bool pair, int tpo, bool sell) {
+  return pair ? dil_split_kernel<LIN, W, true>(tpo, sell) : dil_split_kernel<LIN, W, false>(tpo, sell);
+}
+template <bool CHUNK, bool W>
+static decltype(&k_force_split<4, true>) force_split_w(const pd_ctx* c, bool pair, int tpo, bool sell) {
+  const bool lin = c->material_model == PD_MATERIAL_LINEAR_LPS;
+  return lin ? (pair ? force_split_kernel<true, CHUNK, W, true>(tpo, sell) : force_split_kernel<true, CHUNK, W, false>(tpo, sell))
+             : (pair ? force_split_kernel<false, CHUNK, W, true>(tpo, sell) : force_split_kernel<false, CHUNK, W, false>(tpo, sell));
+}
+template <bool CHUNK>
+static decltype(&k_force_split<4, true>) force_split_for(const pd_ctx* c, bool pair, int tpo, bool sell) {
+  return c->influence != PD_INFLUENCE_ONE ? force_split_w<CHUNK, true>(c, pair, tpo, sell)
+                                          : force_split_w<CHUNK, false>(c, pair, tpo, sell);
+}
+template <bool P>
+static decltype(&k_bb_split<4, true>) bb_split_kernel(int tpo, bool sell) {
+  if (sell) return &k_bb_split<4, true, P>;
+  switch (tpo) {
+    case 4: return &k_bb_split<4, false, P>;
+    case 8: return &k_bb_split<8, false, P>;
+    case 16: return &k_bb_split<16, false, P>;
+    default: return &k_bb_split<32, false, P>;
+  }
+}
 
 // The stream and events of the chunked force download (created on first use).
 static cudaError_t ensure_copy_stream(pd_ctx* c) {
@@ -1209,44 +1504,45 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   const int32_t* scol = sell ? c->sell_col.p : c->col.p;
   uint8_t* sdmg = sell ? c->sell_dmg.p : dmg;
   const int64_t* soff = sell ? c->sell_off.p : nullptr;
+  // half-bond damage: the two halves of a bond can differ (critical stretch
+  // varying along bonds, or caller-set damage with differing halves)
+  const bool pair = c->sc_pair || c->dmg_asym;
+  const int ipair = pair ? 1 : 0;
   if (c->material_model == PD_MATERIAL_BOND_BASED) {  // one pass: damage + pair force + epilogue
     if (ev) cudaEventRecord(ev[1], c->stream);
-    if (sell) {
-      k_bb_split<4, true><<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p,
-                                                          c->own.p, sp.damage_on, c->pt.p, c->node_damage.p, E, soff,
-                                                          dmg);
-    } else if (split) {
-      PD_DISPATCH_TPO_CSR(tpo, k_bb_split, sgrid, kSplitBlock, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->own.p,
-                          sp.damage_on, c->pt.p, c->node_damage.p, E, nullptr, nullptr);
+    if (split) {
+      auto* kb = pair ? bb_split_kernel<true>(tpo, sell) : bb_split_kernel<false>(tpo, sell);
+      kb<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p,
+                                               sp.damage_on, c->pt.p, c->node_damage.p, E, soff, sell ? dmg : nullptr,
+                                               c->scf.p);
     } else {
       PD_DISPATCH_TPO(tpo, k_bb_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p, c->sc.p,
-                      c->hp.p, sp.damage_on, c->bb_plane, c->bb_height, c->node_damage.p, E);
+                      c->hp.p, sp.damage_on, c->bb_plane, c->bb_height, c->node_damage.p, E, ipair);
     }
     if (ev) cudaEventRecord(ev[2], c->stream);
     return cudaGetLastError();
   }
-  if (sell) {
-    (c->material_model == PD_MATERIAL_LINEAR_LPS ? k_dilatation_split<4, true, true> : k_dilatation_split<4, true>)
-        <<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p,
-                                                                c->ur[c->cur].p, c->own.p, sp.damage_on, c->theta.p,
-                                                                c->node_damage.p, soff, dmg);
-  } else if (split) {
-    PD_DISPATCH_TPO_CSR(tpo, k_dilatation_split, sgrid, kSplitBlock, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p,
-                        c->own.p, sp.damage_on, c->theta.p, c->node_damage.p, nullptr, nullptr);
+  if (split) {
+    const bool lin = c->material_model == PD_MATERIAL_LINEAR_LPS, w = c->influence != PD_INFLUENCE_ONE;
+    auto* kd = lin ? (w ? dil_split_for<true, true>(pair, tpo, sell) : dil_split_for<true, false>(pair, tpo, sell))
+                   : (w ? dil_split_for<false, true>(pair, tpo, sell) : dil_split_for<false, false>(pair, tpo, sell));
+    kd<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p,
+                                             sp.damage_on, c->theta.p, c->node_damage.p, soff, sell ? dmg : nullptr,
+                                             c->hp.p, c->influence, c->scf.p);
   } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
     PD_DISPATCH_TPO(tpo, k_dilatation_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p,
-                    c->pt.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
+                    c->pt.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p,
+                    ipair);
   } else {
     PD_DISPATCH_TPO(tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p,
-                    c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p);
+                    c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p, ipair);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (ev) cudaEventRecord(ev[1], c->stream);
   if (sell) {
-    const bool lin = c->material_model == PD_MATERIAL_LINEAR_LPS;
     if (sp.f_host && sp.f_out) {
-      auto* kf = lin ? k_force_split<4, true, true, true> : k_force_split<4, true, false, true>;
+      auto* kf = force_split_for<true>(c, pair, tpo, sell);
       // Force in chunks of points; each chunk's force density goes to the host
       // on the copy stream while the next chunk computes.
       TRY_CUDA(ensure_copy_stream(c));
@@ -1255,8 +1551,8 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       // memory holds the host until it is done)
       for (int64_t i0 = 0, k = 0; i0 < n; i0 += per, ++k) {
         const int64_t i1 = std::min(n, i0 + per);
-        kf<<<grid_split(i1 - i0, 4), kSplitBlock, 0, c->stream>>>(i1, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p,
-                                                           E, soff, i0);
+        kf<<<grid_split(i1 - i0, 4), kSplitBlock, 0, c->stream>>>(i1, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p,
+                                                                  c->pt.p, E, soff, c->hp.p, c->influence, i0);
         TRY_CUDA(cudaEventRecord(c->chunk_ev[k], c->stream));
       }
       for (int64_t i0 = 0, k = 0; i0 < n; i0 += per, ++k) {
@@ -1269,12 +1565,14 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       TRY_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[kHostChunks], 0));
       *host_done = true;
     } else {
-      auto* kf = lin ? k_force_split<4, true, true> : k_force_split<4, true>;
-      kf<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E, soff, 0);
+      auto* kf = force_split_for<false>(c, pair, tpo, sell);
+      kf<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->pt.p, E, soff,
+                                               c->hp.p, c->influence, 0);
     }
   } else if (split) {
-    PD_DISPATCH_TPO_CSR(tpo, k_force_split, sgrid, kSplitBlock, c->n, c->row.p, c->col.p, dmg, c->bx.p, c->ur[c->cur].p, c->pt.p, E,
-                        nullptr);
+    auto* kf = force_split_for<false>(c, pair, tpo, false);
+    kf<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, c->col.p, dmg, c->bx3.p, c->ur[c->cur].p, c->pt.p, E,
+                                             nullptr, c->hp.p, c->influence, 0);
   } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
     PD_DISPATCH_TPO(tpo, k_force_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->ab64.p,
                     c->pt.p, c->hp.p, c->influence, E);
@@ -1311,7 +1609,7 @@ cudaError_t launch_fp64_eval_at(pd_ctx* c, const double4* y4, double4* ab, doubl
   if (c->n == 0) return cudaSuccess;
   const unsigned grid = grid_for(c->n, c->tpo);
   PD_DISPATCH_TPO(c->tpo, k_dilatation_fp64, grid, c->n, c->row.p, c->col.p, c->dmg.p, c->xv.p, y4, c->pt.p,
-                  c->sc.p, c->hp.p, c->influence, 0, ab, theta, nd);
+                  c->sc.p, c->hp.p, c->influence, 0, ab, theta, nd, 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   EpiArgs E{};
@@ -1350,8 +1648,9 @@ namespace pdb {
 __global__ void k_u_from_record(int64_t n, const Rec8* __restrict__ ur, double* __restrict__ u) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const Rec8 r = ur[i];
-  for (int c = 0; c < 3; ++c) u[3 * i + c] = (double)r.v[c] + (double)r.v[c + 3];
+  double uu[3];
+  load_u_record(ur[i], uu);
+  for (int c = 0; c < 3; ++c) u[3 * i + c] = uu[c];
 }
 
 // Displacement held by the split-path record of the given parity.
@@ -1385,8 +1684,9 @@ __global__ void k_pack_state(int64_t n, int64_t n_idx, const int32_t* __restrict
   o[0] = u0, o[1] = u1, o[2] = u2, o[3] = y.x, o[4] = y.y, o[5] = y.z;
 }
 
-// The receiving side: u and the record the next evaluation gathers (hi/lo
-// split of u on the split path, y on the FP64 path), both as the owner holds them.
+// The receiving side: u and the record the next evaluation gathers (the
+// displacement record on the split path, y on the FP64 path), both as the
+// owner holds them.
 __global__ void k_unpack_state(int64_t n, int64_t n_idx, const int32_t* __restrict__ idx,
                                const double* __restrict__ in, double* __restrict__ u, double4* __restrict__ st,
                                Rec8* __restrict__ ur, int* __restrict__ status) {
@@ -1400,7 +1700,7 @@ __global__ void k_unpack_state(int64_t n, int64_t n_idx, const int32_t* __restri
   const double* v = in + 6 * k;
   for (int c = 0; c < 3; ++c) u[3 * i + c] = v[c];
   if (ur) {
-    for (int c = 0; c < 3; ++c) split_hi_lo(v[c], &ur[i].v[c], &ur[i].v[c + 3]);
+    store_u_record(ur + i, v[0], v[1], v[2]);
   } else {
     st[i] = make_double4(v[3], v[4], v[5], 0.0);
   }
@@ -1423,13 +1723,79 @@ cudaError_t launch_unpack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, co
   return cudaGetLastError();
 }
 
+// Broken bonds of the families: bond damage bytes with the row's own half (bit 0) set.
 __global__ void k_count_nonzero(int64_t m, const uint8_t* __restrict__ d, unsigned long long* __restrict__ out) {
   unsigned long long cnt = 0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
-    cnt += d[k] != 0;
+    cnt += d[k] & 1;
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
 }
+
+// Position of bond (j, i) in row j (rows strictly ascending; families symmetric).
+__device__ __forceinline__ int64_t partner_bond(const int64_t* __restrict__ row, const int32_t* __restrict__ col,
+                                                int64_t i, int32_t j) {
+  int64_t lo = row[j], hi = row[j + 1];
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (col[mid] < (int32_t)i) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Half-bond damage bytes from per-bond damage of the rows' own halves (src,
+// bit 0): bit 1 of bond (i, j) = bit 0 of bond (j, i). flag[0] is set when a
+// bond's two halves differ.
+__global__ void k_mirror_damage(int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col,
+                                const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, int* __restrict__ flag) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int lane = threadIdx.x & 7;
+  if (i >= n) return;
+  bool asym = false;
+  for (int64_t b = row[i] + lane; b < row[i + 1]; b += 8) {
+    const int32_t j = col[b];
+    const int64_t bp = partner_bond(row, col, i, j);
+    const int own = src[b] & 1, part = (bp < row[j + 1] && col[bp] == (int32_t)i) ? (src[bp] & 1) : own;
+    dst[b] = (uint8_t)(own | (part << 1));
+    asym |= own != part;
+  }
+  if (asym) atomicOr(flag, 1);
+}
+
+// flag[0] set when some bond joins points of different critical stretch.
+__global__ void k_pair_check(int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col,
+                             const double* __restrict__ sc, int* __restrict__ flag) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int lane = threadIdx.x & 7;
+  if (i >= n) return;
+  const double si = sc[i];
+  bool diff = false;
+  for (int64_t b = row[i] + lane; b < row[i + 1]; b += 8) diff |= sc[col[b]] != si;
+  if (diff) atomicOr(flag, 1);
+}
+
+static int run_flag_kernel(pd_ctx* c, int which, const uint8_t* src, uint8_t* dst, bool* out) {
+  DBuf<int> flag;
+  PD_CUDA_TRY(c, flag.alloc(1));
+  PD_CUDA_TRY(c, cudaMemsetAsync(flag.p, 0, sizeof(int), c->stream));
+  const unsigned g = (unsigned)((c->n * 8 + kBlock - 1) / kBlock);
+  if (c->n > 0) {
+    if (which == 0) k_mirror_damage<<<g, kBlock, 0, c->stream>>>(c->n, c->row.p, c->col.p, src, dst, flag.p);
+    else k_pair_check<<<g, kBlock, 0, c->stream>>>(c->n, c->row.p, c->col.p, c->sc.p, flag.p);
+    PD_CUDA_TRY(c, cudaGetLastError());
+  }
+  int h = 0;
+  PD_CUDA_TRY(c, d2h(c, &h, flag.p, sizeof(int)));
+  *out = h != 0;
+  return PD_OK;
+}
+
+// Damage bytes of both halves from own-half damage in src (device), into dst.
+int mirror_damage(pd_ctx* c, const uint8_t* src, uint8_t* dst) { return run_flag_kernel(c, 0, src, dst, &c->dmg_asym); }
+
+// Whether the critical stretch differs across some bond (the sc array is uploaded).
+int check_sc_pairs(pd_ctx* c) { return run_flag_kernel(c, 1, nullptr, nullptr, &c->sc_pair); }
 
 int count_broken(pd_ctx* c, int64_t* out) {
   *out = 0;

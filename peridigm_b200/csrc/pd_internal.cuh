@@ -8,10 +8,11 @@
 //   pt[n]        double4 (m, K, mu, rho) per-point material, sc[n] critical stretch, hp[n] horizon
 //   u[3n], v[3n], a[3n], f[3n], fc[3n] FP64 integration state (interleaved xyz)
 // Split-FP32 path:
-//   bx[nb]       float4 (X in FP32, omega(|X|)*V_j) per bond, streamed in bond order;
-//                X = x_j - x_i formed in FP64 and rounded once, constant
-//   ur[2][n]     Rec8 (u_hi[3], u_lo[3], A, B) gathered per neighbor with one
-//                256-bit load; double buffered across steps
+//   bx3          X = x_j - x_i per bond in FP32 (formed in FP64, rounded once,
+//                constant), streamed; 32-bond groups of x[32], y[32], z[32]
+//   ur[2][n]     Rec8 (u_hi[3], lo_xy, lo_z|q, V, A, B) gathered per neighbor
+//                with one 256-bit load; u = u_hi + 16-bit residuals times a
+//                shared power of two q; double buffered across steps
 //   own[n]       float4 (3/m, (3K-5mu)/m, 15mu/m, s_c)  owner terms
 // FP64 path:
 //   st[2][n]     double4 (y_x, y_y, y_z, 0) current coordinates, double buffered
@@ -151,10 +152,10 @@ struct pd_ctx {
   bool wv_done = false;
   pdb::DBuf<double4> pt;     // (m, K, mu, rho)
   pdb::DBuf<double> sc;      // critical stretch (<0: off)
-  pdb::DBuf<float4> bx;      // split path: per bond (X, omega*V_j), CSR or sliced order
+  pdb::DBuf<float> bx3;      // split path: per bond X in FP32, 32-slot groups of x/y/z planes, CSR or sliced order
   // Sliced (SELL) bond stream of the 4-lanes-per-point split passes: slot
   // offsets per 8-owner slice, neighbor ids and a damage mirror in slice
-  // order (bx holds the records in that order). dmg_gen counts writes to the
+  // order (bx3 holds the bond vectors in that order). dmg_gen counts writes to the
   // CSR damage outside the passes; the mirror is refreshed when it lags.
   bool sell = false;
   pdb::DBuf<int64_t> sell_off;
@@ -163,7 +164,13 @@ struct pd_ctx {
   const uint8_t* sell_src = nullptr;
   int64_t dmg_gen = 0, sell_gen = -1;
   pdb::DBuf<float4> own;     // split path: (3/m, (3K-5mu)/m, 15mu/m, s_c)
+  pdb::DBuf<float> scf;      // split path: s_c per point, gathered for the partner half's test
   bool any_damage = false;
+  // Half-bond damage (bit 1 of the damage bytes differs from bit 0 somewhere,
+  // or can come to): the critical stretch differs across some bond, or the
+  // caller set damage whose two halves differ.
+  bool sc_pair = false;
+  bool dmg_asym = false;
 
   // state
   pdb::DBuf<double4> st[2];   // FP64 path gathered coordinates
@@ -297,8 +304,12 @@ cudaError_t launch_u_from_record(pd_ctx* c, int parity, double* u_out);  // spli
 // evaluation reads, 6 doubles per point; unpack overwrites it.
 cudaError_t launch_pack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, double* out);
 cudaError_t launch_unpack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, const double* in);
-// Number of broken bonds (damage byte set) of the committed damage.
+// Number of broken bonds (own half, bit 0 of the damage byte) of the committed damage.
 int count_broken(pd_ctx* c, int64_t* out);
+// Damage bytes of both halves (bit 1 = the partner's bit 0) from src into dst; sets dmg_asym.
+int mirror_damage(pd_ctx* c, const uint8_t* src, uint8_t* dst);
+// Sets sc_pair: whether some bond joins points of different critical stretch.
+int check_sc_pairs(pd_ctx* c);
 void qs_release(pd_ctx* c);
 
 // status bits

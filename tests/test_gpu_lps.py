@@ -108,10 +108,46 @@ def test_eval_model_matches_oracle(precision):
             np.linalg.norm(P[col] - P[owner], axis=1)
         near = np.abs(s - 1.5e-3) <= 1e-6 * 1.5e-3
         assert np.array_equal(bdn[~near], ref["bond_damage"][~near])
-        if not near.any():
-            assert rel_l2(th, ref["theta"]) < 1e-6
-            assert rel_l2(f, ref["force"]) < 1e-6
-            assert np.abs(f - ref["force"]).max() < 1e-5 * np.abs(ref["force"]).max()
+        # a bond within 1e-6 s_c of s_c may break on one path and not the
+        # other: its endpoints' dilatation and the force of every point within
+        # a family of them are left out of the comparison (none on most seeds)
+        touched = np.zeros(n, bool)
+        touched[owner[near]] = True
+        touched[col[near]] = True
+        th_ok = ~touched
+        f_ok = ~np.isin(np.arange(n), np.unique(np.concatenate([owner[touched[col]], np.nonzero(touched)[0]])))
+        assert f_ok.sum() > 0.8 * n
+        assert rel_l2(th[th_ok], ref["theta"][th_ok]) < 1e-6
+        fm, rm = f.reshape(-1, 3)[f_ok], ref["force"].reshape(-1, 3)[f_ok]
+        assert rel_l2(fm, rm) < 1e-6
+        assert np.abs(fm - rm).max() < 1e-5 * np.abs(ref["force"]).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_half_broken_bonds_match_oracle(precision):
+    """Bond damage whose two halves differ (d_ij = 1, d_ji = 0; what a
+    critical stretch differing between the blocks or points of a bond leaves
+    behind): each row's own half enters its dilatation and t_ij, the partner's
+    half t_ji, as in the reference's scatter from both families."""
+    x, vol, y, h = make_cloud(seed=11)
+    row, col = O.neighbor_search(x, h)
+    n = len(vol)
+    owner = np.repeat(np.arange(n), np.diff(row))
+    bd = (np.random.default_rng(4).random(len(col)) < 0.08).astype(float)  # rows set independently
+    K = 130e9 * np.exp(0.3 * np.random.default_rng(5).standard_normal(n))
+    ref = O.eval_model(x, y, vol, row, col, K, 0.6 * K, h, s_c=None, dmg_n=bd)
+    with Context(precision=precision) as ctx:
+        ctx.set_points(x, vol)
+        ctx.set_horizons([h])
+        ctx.build_bonds()
+        ctx.material(130e9, 78e9, 7800.0)
+        ctx.material_field(K, 0.6 * K)
+        ctx.set_bond_damage(bd)
+        f = ctx.compute_force(y)
+        assert np.array_equal(ctx.field("Bond_Damage"), bd)
+    assert (bd != bd[np.array([row[j] + np.searchsorted(col[row[j]:row[j + 1]], i)
+                                for i, j in zip(owner, col)])]).any(), "the halves should differ"
+    assert rel_l2(f, ref["force"]) < (1e-11 if precision == "fp64" else 1e-6)
 
 
 @pytest.mark.parametrize("case", ["1a", "1b", "2a", "2b", "3a"])
