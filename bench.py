@@ -160,6 +160,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+T_START = time.perf_counter()
+
+
+def log(msg):
+    """Progress of the run on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - T_START:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -563,11 +571,13 @@ def main():
     hbm, peak_src = peak_hbm()
     w, blocks = make_workload(args.workload)
     n = int(len(w["vol"]))
+    log(f"workload {w['name']}: {n} points")
 
     # ---- value: split-FP32 explicit steps, state resident in HBM -----------
     ctx, sp = explicit_leg(w, blocks, local, args.steps, args.warmup, "split", world, max_over_ranks, barrier,
                            timed_clocks=True)
     nb, dt = sp["nb"], sp["dt"]
+    log(f"split: {nb} bonds, {sp['ms'] / args.steps:.3f} ms/step")
     u_split = ctx.field("Displacement")
     d_split = ctx.field("Damage")
     slots = sliced_slots(ctx)
@@ -577,9 +587,11 @@ def main():
     roofline = kernel_roofline(ctx, dt, sp["t_done"], args.kernel_steps, nb, n, hbm, peak_src, slots)
     roofline["step_frac"] = step_bytes / (sp["ms"] / args.steps / 1e3) / 1e9 / hbm
 
+    log(f"per-kernel ms {roofline['per_kernel_ms']}")
     # ---- e2e: the drop-in computeForce call with host buffers ---------------
     e2e = e2e_leg(ctx, n, nb, args.e2e_steps, world, max_over_ranks, barrier)
     ctx.close()
+    log(f"e2e {e2e['value']:.3e}")
 
     # ---- plain FP64 path, same workload, same steps from rest ----------------
     fp64 = None
@@ -597,6 +609,7 @@ def main():
             fp64["u_rel_l2"] = float(np.linalg.norm(u_split - u64) / max(np.linalg.norm(u64), 1e-300))
             fp64["node_damage_max_diff"] = float(np.max(np.abs(d_split - d64)))
         c64.close()
+        log(f"fp64 {fp64['value']:.3e}, split/fp64 {fp64['split_over_fp64']:.2f}")
 
     # ---- the notched plate (the split/FP64 comparison case) as an extra ------
     extra = None
@@ -615,11 +628,13 @@ def main():
 
     # ---- quasi-static time to 1e-8 (rank 0 only) -----------------------------
     qs = None
+    log("qs leg")
     if rank == 0 and not args.no_qs:
         qs = qs_leg(local, args.qs_load_steps, cpu_threads=0 if args.no_cpu_baseline else (os.cpu_count() or 1))
 
     # ---- CPU baseline (rank 0, N = 1 only) ----------------------------------
     cpu = None
+    log("cpu baseline")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import cpu_baseline
         from oracle import oracle as O

@@ -20,6 +20,10 @@
  *    (multiply by volume for forces, src/core/Peridigm.cpp:1881-1884).
  *  - The context owns its device memory. One context per host thread at a
  *    time; contexts are independent.
+ *  - Every entry point that takes a context makes the context's device the
+ *    calling thread's current CUDA device (cudaSetDevice) and leaves it so; a
+ *    caller that drives other devices from the same thread sets its own
+ *    device again after the call.
  */
 #ifndef PD_B200_H
 #define PD_B200_H
@@ -228,7 +232,10 @@ int pd_critical_time_step(pd_ctx* ctx, double* dt_out);
  *  - the array is shared by all contexts on a device, so calls that overlap on
  *    one device (from two threads) race and must be serialised by the caller;
  *  - the first call on each device resolves the array's address and may load
- *    the library's module there: make it before any stream capture begins.
+ *    the library's module there: make it before any stream capture begins;
+ *  - the resolved address is kept for the life of the process: no
+ *    cudaDeviceReset of that device may come between calls (a reset unloads
+ *    the module the address belongs to).
  * The result is copied to the host double *dt_out after a stream synchronise. */
 int pd_critical_time_step_static(pd_ctx* ctx, double* dt_out);
 /* Initial displacement / velocity (DirichletBC "Initial Displacement"/"Initial Velocity",

@@ -56,10 +56,14 @@ int upload_material(pd_ctx* c) {
   PD_CUDA_TRY(c, h2d(c, c->pt.p, pt.data(), n * sizeof(double4)));
   PD_CUDA_TRY(c, h2d(c, c->sc.p, sc.data(), n * sizeof(double)));
   PD_CUDA_TRY(c, h2d(c, c->hp.p, hp.data(), n * sizeof(double)));
+  c->sc_min = INFINITY;
   if (c->precision == PD_SPLIT_FP32) {
     PD_CUDA_TRY(c, c->own.alloc(n));
     std::vector<float> scf(n);
-    for (int64_t i = 0; i < n; ++i) scf[i] = (float)sc[i];
+    for (int64_t i = 0; i < n; ++i) {
+      scf[i] = (float)sc[i];
+      if (scf[i] >= 0.0f) c->sc_min = std::min(c->sc_min, scf[i]);
+    }
     PD_CUDA_TRY(c, c->scf.alloc(n));
     PD_CUDA_TRY(c, h2d(c, c->scf.p, scf.data(), n * sizeof(float)));
   }

@@ -192,6 +192,9 @@ __device__ __forceinline__ OwnU own_u(const Rec8& r) {
 struct SplitBond {
   float Yx, Yy, Yz, zeta, ry, e, xu, xx;  // xu = X.du, xx = |X|^2 (the linear LPS terms)
 };
+// |Y|^2 = |X|^2 + (2X.du + du.du) and e = (2X.du + du.du)/(|Y| + |X|); Y = X +
+// du and 1/|Y| only with Y (the dilatation pass needs neither).
+template <bool Y = true>
 __device__ __forceinline__ SplitBond split_bond(float X0, float X1, float X2, const OwnU& ui, const Rec8& uj) {
   SplitBond s;
   const ULo lj = decode_lo(uj);
@@ -199,18 +202,21 @@ __device__ __forceinline__ SplitBond split_bond(float X0, float X1, float X2, co
   const float Uy = (uj.v[1] - ui.hy) + (lj.y - ui.ly);
   const float Uz = (uj.v[2] - ui.hz) + (lj.z - ui.lz);
   const float xx = fmaf(X2, X2, fmaf(X1, X1, X0 * X0));
-  s.Yx = X0 + Ux;
-  s.Yy = X1 + Uy;
-  s.Yz = X2 + Uz;
-  const float yy = fmaf(s.Yz, s.Yz, fmaf(s.Yy, s.Yy, s.Yx * s.Yx));
-  s.ry = rsqrtf(yy);
-  s.zeta = xx * rsqrtf(xx);
-  const float dY = yy * s.ry;
   const float xu = fmaf(X2, Uz, fmaf(X1, Uy, X0 * Ux));
   const float uu = fmaf(Uz, Uz, fmaf(Uy, Uy, Ux * Ux));
-  s.e = __fdividef(fmaf(2.0f, xu, uu), dY + s.zeta);  // |Y| - |X| without cancellation
+  const float num = fmaf(2.0f, xu, uu);
+  const float yy = xx + num;
+  const float ry = rsqrtf(yy);
+  s.zeta = xx * rsqrtf(xx);
+  s.e = __fdividef(num, yy * ry + s.zeta);  // |Y| - |X| without cancellation
   s.xu = xu;
   s.xx = xx;
+  if (Y) {
+    s.ry = ry;
+    s.Yx = X0 + Ux;
+    s.Yy = X1 + Uy;
+    s.Yz = X2 + Uz;
+  }
   return s;
 }
 
@@ -242,6 +248,9 @@ __device__ __forceinline__ int64_t xs_index(int64_t k) { return 96 * (k >> 5) + 
 #endif
 #ifndef PD_BOND_MINB
 #define PD_BOND_MINB 8
+#endif
+#ifndef PD_STREAM_AHEAD
+#define PD_STREAM_AHEAD 0
 #endif
 constexpr int kUnroll = PD_BOND_UNROLL;
 // Threads per block of the split bond passes: 8 blocks of 128 fill an SM's
@@ -302,24 +311,32 @@ __device__ __forceinline__ int64_t sell_x_index(const int64_t* __restrict__ soff
   return 96 * (so + g) + l32;
 }
 
-template <bool NC>
+// Slots 0-5 of a record (displacement and volume: what the dilatation pass
+// reads of a neighbor), coherent; slots 6-7 are left 0.
+__device__ __forceinline__ Rec8 ld_rec_u(const Rec8* p) {
+  Rec8 r;
+  asm("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]) : "l"(p));
+  asm("ld.global.v2.f32 {%0,%1}, [%2];" : "=f"(r.v[4]), "=f"(r.v[5]) : "l"(p->v + 4));
+  r.v[6] = r.v[7] = 0.0f;
+  return r;
+}
+// Neighbor record loads of the walks: NC (0) coherent 256-bit load, (1) the
+// read-only path (no record written by the kernel), (2) slots 0-5 only.
+template <int NC>
 __device__ __forceinline__ Rec8 ld_rec_t(const Rec8* p) {
-  return NC ? ld_rec_nc(p) : ld_rec(p);
+  return NC == 2 ? ld_rec_u(p) : (NC == 1 ? ld_rec_nc(p) : ld_rec(p));
 }
 
 // Walks lane `lane` of owner i through its bonds of the sliced stream: the
 // full blocks with one int4 of ids (loaded one block ahead), one damage word
 // and three float4 of X per block, then the tail groups. For each bond, in
 // the lane's row order, body(X0, X1, X2, damage byte, neighbor record,
-// neighbor's critical stretch, the bond's damage byte in the stream, row
-// offset r - lane). NC: neighbor records through the read-only path (no
-// record written by the kernel). PAIR: the neighbors' critical stretch
-// scf[j] is gathered with their records (else -1 is passed).
-template <bool NC, bool PAIR, typename Body>
+// neighbor id, the bond's damage byte in the stream, row offset r - lane).
+// NC: how neighbor records are loaded (ld_rec_t).
+template <int NC, typename Body>
 __device__ __forceinline__ void sell_walk(int64_t i, int lane, const int64_t* __restrict__ soff,
                                           const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
-                                          const float* __restrict__ bx3, const Rec8* __restrict__ ur,
-                                          const float* __restrict__ scf, Body&& body) {
+                                          const float* __restrict__ bx3, const Rec8* __restrict__ ur, Body&& body) {
   const int64_t s = i >> 3, so = soff[s];
   const int G = (int)(soff[s + 1] - so), F = G >> 2;
   const int l32 = (int)(i & 7) * 4 + lane;
@@ -327,22 +344,38 @@ __device__ __forceinline__ void sell_walk(int64_t i, int lane, const int64_t* __
   uint32_t* pd = reinterpret_cast<uint32_t*>(dmg + 32 * so + 4 * l32);
   const float4* px = reinterpret_cast<const float4*>(bx3 + 96 * so + 4 * l32);
   int4 jn = F > 0 ? __ldcs(pc) : make_int4(0, 0, 0, 0);
+#if PD_STREAM_AHEAD
+  // the next block's damage word and X held in registers one block ahead
+  uint32_t dwn = 0;
+  float4 xan = make_float4(0.f, 0.f, 0.f, 0.f), xbn = xan, xcn = xan;
+  if (F > 0) {
+    dwn = __ldcs(pd);
+    xan = __ldcs(px), xbn = __ldcs(px + 32), xcn = __ldcs(px + 64);
+  }
+#endif
 #pragma unroll 1
   for (int b = 0; b < F; ++b, pc += 32, pd += 32, px += 96) {
     const int4 jj = jn;
     if (b + 1 < F) jn = __ldcs(pc + 32);
+#if PD_STREAM_AHEAD
+    const uint32_t dw = dwn;
+    const float4 xa = xan, xb = xbn, xc = xcn;
+    if (b + 1 < F) {
+      dwn = __ldcs(pd + 32);
+      xan = __ldcs(px + 96), xbn = __ldcs(px + 128), xcn = __ldcs(px + 160);
+    }
+#else
     const uint32_t dw = __ldcs(pd);
     const float4 xa = __ldcs(px), xb = __ldcs(px + 32), xc = __ldcs(px + 64);
+#endif
     const Rec8 u0 = ld_rec_t<NC>(ur + jj.x), u1 = ld_rec_t<NC>(ur + jj.y), u2 = ld_rec_t<NC>(ur + jj.z),
                u3 = ld_rec_t<NC>(ur + jj.w);
-    float4 sj = make_float4(-1.f, -1.f, -1.f, -1.f);
-    if (PAIR) sj = make_float4(__ldg(scf + jj.x), __ldg(scf + jj.y), __ldg(scf + jj.z), __ldg(scf + jj.w));
     uint8_t* pb = reinterpret_cast<uint8_t*>(pd);
     const int r0 = 16 * b;
-    body(xa.x, xb.x, xc.x, (int)(dw & 0xffu), u0, sj.x, pb, r0);
-    body(xa.y, xb.y, xc.y, (int)((dw >> 8) & 0xffu), u1, sj.y, pb + 1, r0 + 4);
-    body(xa.z, xb.z, xc.z, (int)((dw >> 16) & 0xffu), u2, sj.z, pb + 2, r0 + 8);
-    body(xa.w, xb.w, xc.w, (int)(dw >> 24), u3, sj.w, pb + 3, r0 + 12);
+    body(xa.x, xb.x, xc.x, (int)(dw & 0xffu), u0, jj.x, pb, r0);
+    body(xa.y, xb.y, xc.y, (int)((dw >> 8) & 0xffu), u1, jj.y, pb + 1, r0 + 4);
+    body(xa.z, xb.z, xc.z, (int)((dw >> 16) & 0xffu), u2, jj.z, pb + 2, r0 + 8);
+    body(xa.w, xb.w, xc.w, (int)(dw >> 24), u3, jj.w, pb + 3, r0 + 12);
   }
   const int T = G - 4 * F;
   if (T > 0) {  // tail groups: masked, one slot per lane per group
@@ -361,24 +394,19 @@ __device__ __forceinline__ void sell_walk(int64_t i, int lane, const int64_t* __
       X2[k] = in ? __ldcs(pt + 96 * k + 64) : 0.0f;
     }
     Rec8 uu[3];
-    float sj[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      uu[k] = ld_rec_t<NC>(ur + jj[k]);
-      sj[k] = PAIR ? __ldg(scf + jj[k]) : -1.0f;
-    }
+    for (int k = 0; k < 3; ++k) uu[k] = ld_rec_t<NC>(ur + jj[k]);
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
-      body(X0[k], X1[k], X2[k], dd[k], uu[k], sj[k], dmg + t0 + 32 * k, 16 * F + 4 * k);
+    for (int k = 0; k < 3; ++k) body(X0[k], X1[k], X2[k], dd[k], uu[k], jj[k], dmg + t0 + 32 * k, 16 * F + 4 * k);
   }
 }
 
 // The same walk over a CSR row (TPO lanes per point, the lane's bonds TPO
 // apart), kUnroll bonds per batch with the next batch's ids loaded ahead.
-template <int TPO, bool NC, bool PAIR, typename Body>
+template <int TPO, int NC, typename Body>
 __device__ __forceinline__ void csr_walk(int64_t i, int lane, int64_t b0, int64_t b1, const int32_t* __restrict__ col,
                                          uint8_t* __restrict__ dmg, const float* __restrict__ bx3,
-                                         const Rec8* __restrict__ ur, const float* __restrict__ scf, Body&& body) {
+                                         const Rec8* __restrict__ ur, Body&& body) {
   int64_t slot;
   int left;
   csr_cursor<TPO>(lane, b0, b1, &slot, &left);
@@ -405,15 +433,11 @@ __device__ __forceinline__ void csr_walk(int64_t i, int lane, int64_t b0, int64_
       X1[k] = in ? __ldcs(p + 32) : 0.0f;
       X2[k] = in ? __ldcs(p + 64) : 0.0f;
     }
-    float sj[kUnroll];
 #pragma unroll
-    for (int k = 0; k < kUnroll; ++k) {
-      uu[k] = ld_rec_t<NC>(ur + jj[k]);
-      sj[k] = PAIR ? __ldg(scf + jj[k]) : -1.0f;
-    }
+    for (int k = 0; k < kUnroll; ++k) uu[k] = ld_rec_t<NC>(ur + jj[k]);
 #pragma unroll
     for (int k = 0; k < kUnroll; ++k)
-      body(X0[k], X1[k], X2[k], dd[k], uu[k], sj[k], dmg + slot + TPO * k, (int)(slot + TPO * k - b0 - lane));
+      body(X0[k], X1[k], X2[k], dd[k], uu[k], jj[k], dmg + slot + TPO * k, (int)(slot + TPO * k - b0 - lane));
   }
 }
 
@@ -552,13 +576,20 @@ __global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* _
 // (the weighted variants get 96 registers: the omega evaluation would spill at 64)
 // PAIR: the two halves of a bond can differ (critical stretch varying along
 // bonds, or half-broken bonds set by the caller): the partner's test runs
-// with its own s_c,j, gathered per bond.
+// with its own s_c,j, read only for bonds stretched past s_min, the smallest
+// critical stretch of the body (no bond below it can break on either side).
+// The pass reads 24 of the 32 record bytes of a neighbor (not A, B), which
+// frees their registers.
+#ifndef PD_DIL_MINB
+#define PD_DIL_MINB 8
+#endif
 template <int TPO, bool SELL, bool LIN = false, bool WEIGHT = false, bool PAIR = false>
-__global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_dilatation_split(
+__global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilatation_split(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const float* __restrict__ bx3, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
     double* __restrict__ theta_out, double* __restrict__ node_damage, const int64_t* __restrict__ soff,
-    uint8_t* __restrict__ dmg_csr, const double* __restrict__ hp, int influence, const float* __restrict__ scf) {
+    uint8_t* __restrict__ dmg_csr, const double* __restrict__ hp, int influence, const float* __restrict__ scf,
+    float s_min) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -574,12 +605,19 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_dila
     const float hi = WEIGHT ? (float)hp[i] : 1.0f;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
     // Branch-free masking (selects) of dummy and broken bonds.
-    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, float scj, uint8_t* pdm, int r) {
-      const SplitBond sb = split_bond(X0, X1, X2, ui, uj);
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t j, uint8_t* pdm, int r) {
+      const SplitBond sb = split_bond<false>(X0, X1, X2, ui, uj);
       const bool own_ok = (d & 5) == 0;  // own half intact (and a real bond)
       const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
       // the partner's half: its own test, or the same test on both halves
-      const bool brkp = PAIR ? ((d & 6) == 0 && damage_on && scj >= 0.0f && sb.e > scj * sb.zeta) : brk;
+      bool brkp = brk;
+      if (PAIR) {
+        brkp = false;
+        if ((d & 6) == 0 && damage_on && sb.e > s_min * sb.zeta) {  // rare: past the body's smallest s_c
+          const float scj = __ldg(scf + j);
+          brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
+        }
+      }
       if (brk || brkp) {
         const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
         *pdm = nd;
@@ -592,9 +630,9 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_dila
       th = fmaf((own_ok && !brk) ? (LIN ? wv : wv * sb.zeta) : 0.0f, LIN ? sb.xu : sb.e, th);
     };
     if constexpr (SELL)
-      sell_walk<false, PAIR>(i, lane, soff, col, dmg, bx3, ur, scf, body);
+      sell_walk<2>(i, lane, soff, col, dmg, bx3, ur, body);
     else
-      csr_walk<TPO, false, PAIR>(i, lane, b0, b0 + len, col, dmg, bx3, ur, scf, body);
+      csr_walk<TPO, 2>(i, lane, b0, b0 + len, col, dmg, bx3, ur, body);
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
@@ -798,8 +836,8 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_forc
     const OwnU ui = own_u(ri);
     const float Ai = ri.v[6], Bi = ri.v[7];
     const float hi = WEIGHT ? (float)hp[i] : 1.0f;
-    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, float, uint8_t*, int) {
-      const SplitBond sb = split_bond(X0, X1, X2, ui, uj);
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t, uint8_t*, int) {
+      const SplitBond sb = split_bond<true>(X0, X1, X2, ui, uj);
       float wv = uj.v[5];  // V_j
       if constexpr (WEIGHT) wv *= omega_f(influence, sb.zeta, hi);
       // owner terms of the intact halves: t_ij with (1 - d_ij), t_ji with (1 - d_ji)
@@ -828,9 +866,9 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_forc
     };
     uint8_t* dm = const_cast<uint8_t*>(dmg);  // not written by this pass
     if constexpr (SELL)
-      sell_walk<PD_FORCE_NC, false>(i, lane, soff, col, dm, bx3, ur, nullptr, body);
+      sell_walk<PD_FORCE_NC>(i, lane, soff, col, dm, bx3, ur, body);
     else
-      csr_walk<TPO, PD_FORCE_NC, false>(i, lane, row[i], row[i + 1], col, dm, bx3, ur, nullptr, body);
+      csr_walk<TPO, PD_FORCE_NC>(i, lane, row[i], row[i + 1], col, dm, bx3, ur, body);
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
@@ -1149,7 +1187,7 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
                                                                    double* __restrict__ node_damage, EpiArgs E,
                                                                    const int64_t* __restrict__ soff,
                                                                    uint8_t* __restrict__ dmg_csr,
-                                                                   const float* __restrict__ scf) {
+                                                                   const float* __restrict__ scf, float s_min) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -1165,12 +1203,19 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
     const float ci = ri.v[6];
     const float s_c = damage_on ? own[i].w : -1.0f;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
-    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, float scj, uint8_t* pdm, int r) {
-      const SplitBond sb = split_bond(X0, X1, X2, ui, uj);
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t j, uint8_t* pdm, int r) {
+      const SplitBond sb = split_bond<true>(X0, X1, X2, ui, uj);
       const bool own_ok = (d & 5) == 0;
       const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
       const bool part_ok = PAIR ? (d & 6) == 0 : own_ok;
-      const bool brkp = PAIR ? (part_ok && damage_on && scj >= 0.0f && sb.e > scj * sb.zeta) : brk;
+      bool brkp = brk;
+      if (PAIR) {
+        brkp = false;
+        if (part_ok && damage_on && sb.e > s_min * sb.zeta) {
+          const float scj = __ldg(scf + j);
+          brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
+        }
+      }
       if (brk || brkp) {
         const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
         *pdm = nd;
@@ -1185,9 +1230,9 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
       fz = fmaf(w, sb.Yz, fz);
     };
     if constexpr (SELL)
-      sell_walk<true, PAIR>(i, lane, soff, col, dmg, bx3, ur, scf, body);
+      sell_walk<1>(i, lane, soff, col, dmg, bx3, ur, body);
     else
-      csr_walk<TPO, true, PAIR>(i, lane, b0, b0 + len, col, dmg, bx3, ur, scf, body);
+      csr_walk<TPO, 1>(i, lane, b0, b0 + len, col, dmg, bx3, ur, body);
   }
   fx = group_sum<TPO>(fx);
   fy = group_sum<TPO>(fy);
@@ -1514,7 +1559,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       auto* kb = pair ? bb_split_kernel<true>(tpo, sell) : bb_split_kernel<false>(tpo, sell);
       kb<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p,
                                                sp.damage_on, c->pt.p, c->node_damage.p, E, soff, sell ? dmg : nullptr,
-                                               c->scf.p);
+                                               c->scf.p, c->sc_min);
     } else {
       PD_DISPATCH_TPO(tpo, k_bb_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p, c->sc.p,
                       c->hp.p, sp.damage_on, c->bb_plane, c->bb_height, c->node_damage.p, E, ipair);
@@ -1528,7 +1573,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
                    : (w ? dil_split_for<false, true>(pair, tpo, sell) : dil_split_for<false, false>(pair, tpo, sell));
     kd<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p,
                                              sp.damage_on, c->theta.p, c->node_damage.p, soff, sell ? dmg : nullptr,
-                                             c->hp.p, c->influence, c->scf.p);
+                                             c->hp.p, c->influence, c->scf.p, c->sc_min);
   } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
     PD_DISPATCH_TPO(tpo, k_dilatation_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p,
                     c->pt.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p,

@@ -171,6 +171,7 @@ struct pd_ctx {
   // caller set damage whose two halves differ.
   bool sc_pair = false;
   bool dmg_asym = false;
+  float sc_min = 0.0f;  // smallest critical stretch >= 0 of the points (FP32; +inf when none)
 
   // state
   pdb::DBuf<double4> st[2];   // FP64 path gathered coordinates
