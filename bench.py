@@ -68,10 +68,11 @@ def algorithmic_bytes(nb, n, precision="split"):
 
 
 # DRAM bytes (read + write) per launch of the split bond passes from one ncu
-# capture (--set full) of step 1 of the heterogeneous plate at 200x200x50
-# (2,000,000 points, sliced bond stream, 128-thread blocks), with the streamed
-# slots of that run. Launches of other sizes are scaled by their slot counts.
-NCU_TRAFFIC = {"workload": "large_plate_200x200x50", "slots": None, "dilatation": None, "force": None}
+# capture (--set full) of step 1 of the heterogeneous plate at 160x160x40
+# (1,024,000 points, 108,999,624 bonds, half-bond variants), with the
+# streamed slots of that run. Launches of other sizes are scaled by their slot
+# counts (the per-slot traffic, not the per-point share, dominates).
+NCU_TRAFFIC = {"workload": "large_plate_160x160x40", "slots": 114618496, "dilatation": 2.0419e9, "force": 2.1915e9}
 
 WORKLOADS = ("large_plate", "notched_plate", "plate_sphere", "bar_wave")
 

@@ -176,3 +176,75 @@ def loss_grad(w, a, r, e, K, fixed_dofs, pid, nbrs, scale, z0=None, round_bf16=T
     y1, sv1 = forward(wb, v1, Am)
     g = backward(wb, v0, sv0, y1, Am) + backward(wb, v1, sv1, y0, Am)
     return L, g
+
+
+def loss_grad_steps(w, r, e, K, Mfix, fixed_dofs, pid, nbrs, scale, ksteps, round_bf16=True):
+    """Loss after `ksteps` steps of preconditioned steepest descent and dL/dw.
+
+    From x0 = 0 on K x = r (r = K e): z_t = M r_t with M = Mfix + Q S G^T G S Q^T
+    (Mfix: block Jacobi and coarse correction, a dense symmetric matrix here),
+    q_t = K z_t, alpha_t = (r_t.z_t)/(z_t.q_t), e_{t+1} = e_t - alpha_t z_t,
+    r_{t+1} = r_t - alpha_t q_t; L = (e_k.r_k)/(e_0.r_0), the energy-norm error
+    left after k steps (1 step: the single-step loss above). The exact step
+    makes L invariant to the scale of M; the error after several steps is
+    made of the slow modes of M K, which set CG's iteration count. The
+    gradient runs the recurrence backwards (M and K symmetric):
+        abar = -(z_t.ebar) - (q_t.rbar)
+        zbar = -alpha ebar + abar (r_t/b - a q_t/b^2),  qbar = -alpha rbar - abar a z_t/b^2
+        zbar += K qbar;  rbar += abar z_t/b + M zbar;  dL/dw += d<zbar, N r_t>/dw
+    with a = r_t.z_t, b = z_t.q_t, ebar and rbar starting at r_k/E0 and e_k/E0."""
+    wb = (bf16(np.asarray(w, np.float32)) if round_bf16 else np.asarray(w, np.float32)).astype(np.float64)
+    n = pid.size
+    npatch = int(pid.max()) + 1
+    fixed = np.zeros(3 * n, bool)
+    fixed[list(fixed_dofs)] = True
+    Am = _mean_matrix(nbrs)
+    Q = _q(pid, fixed, npatch)
+    S = np.repeat(np.asarray(scale, np.float64), 3)
+    free = ~fixed
+
+    def net(x):
+        v = (S * (Q.T @ x)).reshape(npatch, 3)
+        y, sv = forward(wb, v, Am)
+        out = Q @ (S * transpose(wb, y, Am).ravel())
+        out[fixed] = 0.0
+        return out, v, y, sv
+
+    def M(x):
+        out = Mfix @ x + net(x)[0]
+        out[fixed] = 0.0
+        return out
+
+    rt = np.asarray(r, np.float64).copy()
+    et = np.asarray(e, np.float64).copy()
+    rt[fixed] = 0.0
+    et[fixed] = 0.0
+    E0 = float(et @ rt)
+    hist = []
+    for _ in range(ksteps):
+        z = M(rt)
+        q = K @ z
+        q[fixed] = 0.0
+        a, b = float(rt @ z), float(z @ q)
+        if not b > 0.0:  # converged exactly: the remaining steps change nothing
+            break
+        al = a / b
+        hist.append((rt.copy(), z, q, a, b, al))
+        et = et - al * z
+        rt = rt - al * q
+    L = float(et @ rt) / E0
+    ebar = rt / E0
+    rbar = et / E0
+    g = np.zeros(NPARAM)
+    for rt_, z, q, a, b, al in reversed(hist):
+        abar = -float(z @ ebar) - float(q @ rbar)
+        zbar = -al * ebar + abar * (rt_ / b - a * q / (b * b))
+        qbar = -al * rbar - abar * a * z / (b * b)
+        zbar = zbar + K @ qbar
+        zbar[~free] = 0.0
+        _, v0, y0, sv0 = net(rt_)
+        Mz, v1, y1, sv1 = net(zbar)
+        g += backward(wb, v0, sv0, y1, Am) + backward(wb, v1, sv1, y0, Am)
+        rbar = rbar + abar * z / b + Mfix @ zbar + Mz
+        rbar[fixed] = 0.0
+    return L, g

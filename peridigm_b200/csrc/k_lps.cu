@@ -578,8 +578,6 @@ __global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* _
 // bonds, or half-broken bonds set by the caller): the partner's test runs
 // with its own s_c,j, read only for bonds stretched past s_min, the smallest
 // critical stretch of the body (no bond below it can break on either side).
-// The pass reads 24 of the 32 record bytes of a neighbor (not A, B), which
-// frees their registers.
 #ifndef PD_DIL_MINB
 #define PD_DIL_MINB 8
 #endif
@@ -605,7 +603,7 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilat
     const float hi = WEIGHT ? (float)hp[i] : 1.0f;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
     // Branch-free masking (selects) of dummy and broken bonds.
-    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t j, uint8_t* pdm, int r) {
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t, uint8_t* pdm, int r) {
       const SplitBond sb = split_bond<false>(X0, X1, X2, ui, uj);
       const bool own_ok = (d & 5) == 0;  // own half intact (and a real bond)
       const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
@@ -614,7 +612,9 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilat
       if (PAIR) {
         brkp = false;
         if ((d & 6) == 0 && damage_on && sb.e > s_min * sb.zeta) {  // rare: past the body's smallest s_c
-          const float scj = __ldg(scf + j);
+          // the neighbor id again from the bond's stream slot (keeping the
+          // batch's ids live for this branch would cost registers)
+          const float scj = __ldg(scf + __ldg(col + (pdm - dmg)));
           brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
         }
       }
@@ -629,10 +629,15 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilat
       // LPS: omega V_j |X| e; linear LPS: omega V_j X.du
       th = fmaf((own_ok && !brk) ? (LIN ? wv : wv * sb.zeta) : 0.0f, LIN ? sb.xu : sb.e, th);
     };
+    // neighbor records: slots 0-5 only (displacement, volume; the pass never
+    // reads a neighbor's A, B), two loads per record and fewer registers;
+    // the half-bond variant, whose extra tests keep the L1 busier, takes the
+    // whole record in one load (two loads per record double its L1 lookups)
+    constexpr int kRec = PAIR ? 0 : 2;
     if constexpr (SELL)
-      sell_walk<2>(i, lane, soff, col, dmg, bx3, ur, body);
+      sell_walk<kRec>(i, lane, soff, col, dmg, bx3, ur, body);
     else
-      csr_walk<TPO, 2>(i, lane, b0, b0 + len, col, dmg, bx3, ur, body);
+      csr_walk<TPO, kRec>(i, lane, b0, b0 + len, col, dmg, bx3, ur, body);
   }
   th = group_sum<TPO>(th);
   broken = group_sum<TPO>(broken);
@@ -1203,7 +1208,7 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
     const float ci = ri.v[6];
     const float s_c = damage_on ? own[i].w : -1.0f;
     uint8_t* cdm = SELL ? dmg_csr + b0 + lane : nullptr;  // the lane's bonds in the canonical CSR damage
-    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t j, uint8_t* pdm, int r) {
+    auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t, uint8_t* pdm, int r) {
       const SplitBond sb = split_bond<true>(X0, X1, X2, ui, uj);
       const bool own_ok = (d & 5) == 0;
       const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
@@ -1212,7 +1217,7 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
       if (PAIR) {
         brkp = false;
         if (part_ok && damage_on && sb.e > s_min * sb.zeta) {
-          const float scj = __ldg(scf + j);
+          const float scj = __ldg(scf + __ldg(col + (pdm - dmg)));
           brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
         }
       }
