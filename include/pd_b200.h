@@ -372,8 +372,8 @@ int pd_jacobian_block_diagonal(pd_ctx* ctx, const double* u, double* blocks);
  * run preconditioned CG, with the flexible (Polak-Ribiere) beta
  * z_new.(r_new - r_old) / (z_old.r_old): the standard beta for a fixed SPD M,
  * and tolerant of the FP32 rounding of the network's product. A stall, or a
- * true FP64 residual above the tolerance, falls back to the same
- * preconditioner without the network. */
+ * true FP64 residual above the tolerance, falls back to 3x3 block Jacobi
+ * from the current iterate (the FP64 residual decides). */
 int pd_mpnn_init(pd_ctx* ctx, uint64_t seed, double patch);
 /* While every > 0, block-Jacobi and two-level CG solves of pd_qs_load_step
  * store training pairs (r_k, x* - x_k) from every every-th iterate

@@ -613,12 +613,11 @@ static void k_qs_pack_x(int64_t n, QsState* s, pd_ctx* c) {
 static int qs_cg_run(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out,
                      bool* stalled);
 
-// CG with the learned preconditioner first and its base without the network
-// (block Jacobi, with the coarse correction when the network sits on the
-// two-level preconditioner) as the fallback: when the flexible iteration
+// CG with the learned preconditioner first and 3x3 block Jacobi (the
+// reference's "Block 3x3") as the fallback: when the flexible iteration
 // stalls, or when the true FP64 residual |b - K x| (recomputed, not the
 // recursive one) misses the tolerance, the solve restarts from the current x
-// with the base. The true residual decides.
+// with block Jacobi. The true residual decides.
 static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters, double* rel_out) {
   QsState* s = c->qs;
   const int64_t m = 3 * c->n;
@@ -668,8 +667,7 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
   const double tol2 = (std::isfinite(true_rel) && true_rel > 0) ? std::min(1.0, rel_tol / true_rel) : rel_tol;
   int its2 = 0;
   double rel2 = 0.0;
-  rc = qs_cg_run(c, s->coarse_on ? PD_PRECOND_TWO_LEVEL : PD_PRECOND_BLOCK_JACOBI, tol2, max_it, &its2, &rel2,
-                 &stalled);
+  rc = qs_cg_run(c, PD_PRECOND_BLOCK_JACOBI, tol2, max_it, &its2, &rel2, &stalled);
   k_qs_axpy<<<g1(m), kQsBlock, 0, c->stream>>>(m, 1.0, x0.p, s->x.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   *iters = its + its2;

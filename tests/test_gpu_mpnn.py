@@ -4,14 +4,21 @@ gains inside the quasi-static CG.
 
 * pd_mpnn_loss_grad (1 - (r.z)^2/((z.K z)(e.r)), z = P_bj r [+ coarse] + Q S G^T G S Q^T r)
   vs oracle/mpnn.py with the oracle's dense tangent, the device's block-Jacobi
-  blocks and coarse operator, on the same BF16 weights: loss to 1e-4
-  relative, gradient to 2e-2 relative L2 (FP32 vs FP64 sums);
+  blocks and coarse operator, on the same BF16 weights: loss to 1e-6
+  relative, gradient to 1e-5 relative L2 (measured 1e-7: FP32 activations
+  and sums against FP64);
 * pd_mpnn_apply (the inference graph) vs the oracle's Q S G^T G S Q^T r, and
   bit-identical on a second call;
 * two-level QS solves with capture produce pairs, and training lowers the loss;
-* the trained preconditioner solves a held-out QS problem to the two-level
-  displacement (1e-8 relative) in fewer CG iterations than the same
-  preconditioner without the network (two-level), with no fallback.
+* on the translation two-level base, the trained preconditioner solves a
+  held-out QS problem to the two-level displacement (1e-8 relative) in fewer
+  CG iterations than the same preconditioner without the network, with no
+  fallback;
+* on the rigid two-level base (translations and rotations, the base the
+  bench uses), what training gains over the same network at its starting
+  weights and over no network: measured within +-10 % of the base's CG
+  iterations either way (an exact patch-level solve in place of the network
+  saves at most about 12 % there, so a trained approximation has little room).
 """
 import numpy as np
 import pytest
@@ -64,8 +71,8 @@ def test_mpnn_gradient_matches_oracle(coarse):
         _, P0 = O.coarse_operator(K, agg, dofs)
         z0 = P0 @ (Ai @ (P0.T @ r.astype(np.float64)))
     Lr, gr = M.loss_grad(wts, a, r, e, K, dofs, pid, nbrs, scale, z0=z0)
-    assert abs(L - Lr) <= 1e-4 * abs(Lr)
-    assert np.linalg.norm(g - gr) <= 2e-2 * np.linalg.norm(gr)
+    assert abs(L - Lr) <= 1e-6 * abs(Lr)
+    assert np.linalg.norm(g - gr) <= 1e-5 * np.linalg.norm(gr)
 
 
 @pytest.mark.parametrize("seed", [6, 9])
@@ -138,3 +145,49 @@ def test_mpnn_trains_and_helps_cg():
     assert np.linalg.norm(um - ub) <= 1e-8 * np.linalg.norm(ub)
     assert fb == 0
     assert im < ib
+
+
+def test_mpnn_training_gain_on_rigid_base():
+    """Trained network against the same network at its starting weights and
+    against the rigid two-level base alone, on a held-out cube: all three
+    reach the same displacement with no fallback, training lowers its loss,
+    and the trained network's CG iterations stay within 10 % of the base's
+    (the measured gain on this base is nil)."""
+    h, patch = 1.0e-3, 3.0e-3
+    w = workloads.qs_cube(n=12, h=h, seed=11, jitter=0.05, load_steps=4)
+    with Context(precision="fp64") as tr:
+        workloads.setup_context(tr, w)
+        tr.coarse_modes(6)
+        tr.mpnn_init(seed=7, patch=patch)
+        w0 = tr.mpnn_weights()
+        tr.mpnn_collect(2)
+        st = None
+        for k in range(1, len(w["times"])):
+            st = tr.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=-1e-8, cg_relative_tolerance=1e-8,
+                                 preconditioner="two_level", stats=st)
+        l1 = tr.mpnn_train(1, learning_rate=1e-3, batch=8)
+        l2 = tr.mpnn_train(10, learning_rate=1e-3, batch=8)
+        assert l2 < l1
+        wt = tr.mpnn_weights()
+    w2 = workloads.qs_cube(n=12, h=h, seed=23, jitter=0.05, load_steps=2)
+    out = {}
+    for arm, wts in (("base", None), ("init", w0), ("trained", wt)):
+        with Context(precision="fp64") as ctx:
+            workloads.setup_context(ctx, w2)
+            ctx.coarse_modes(6)
+            pre = "two_level"
+            if wts is not None:
+                ctx.mpnn_init(seed=0, patch=patch)
+                ctx.mpnn_set_weights(wts)
+                pre = "mpnn"
+            st = None
+            for k in range(1, len(w2["times"])):
+                st = ctx.qs_load_step(w2["times"][k - 1], w2["times"][k], newton_tolerance=-1e-8,
+                                      cg_relative_tolerance=1e-8, preconditioner=pre, stats=st)
+            out[arm] = (ctx.field("Displacement"), st.cg_iterations, st.preconditioner_fallbacks)
+    print("CG iterations on the rigid base: " + ", ".join(f"{a} {out[a][1]}" for a in out))
+    ub = out["base"][0]
+    for arm in ("init", "trained"):
+        assert np.linalg.norm(out[arm][0] - ub) <= 1e-8 * np.linalg.norm(ub)
+        assert out[arm][2] == 0
+    assert abs(out["trained"][1] - out["base"][1]) <= 0.1 * out["base"][1]
