@@ -80,3 +80,35 @@ def test_bf16_rounding():
     assert out[2] == 1.015625     # halfway, ties to even (odd -> even upward)
     assert out[3] == 1.0          # below halfway
     assert out[4] == -3.140625
+
+
+def test_multistep_loss_gradient_matches_finite_differences():
+    """The loss after k steps of preconditioned steepest descent (block Jacobi
+    plus the learned term) and its adjoint gradient: central differences along
+    a random weight direction, and k = 1 equal to the one-step loss."""
+    x, n, dofs, K, pid, nbrs, scale = _problem(seed=3)
+    rng = np.random.default_rng(2)
+    w = (rng.standard_normal(M.NPARAM) * 0.1).astype(np.float32)
+    e = rng.standard_normal(3 * n)
+    e[dofs] = 0.0
+    r = K @ e
+    blocks = np.stack([K[3 * i:3 * i + 3, 3 * i:3 * i + 3] for i in range(n)])
+    Mfix = np.zeros((3 * n, 3 * n))
+    for i in range(n):
+        Mfix[3 * i:3 * i + 3, 3 * i:3 * i + 3] = np.linalg.inv(blocks[i])
+    Mfix[dofs, :] = 0.0
+    Mfix[:, dofs] = 0.0
+    L1, g1 = M.loss_grad_steps(w, r, e, K, Mfix, dofs, pid, nbrs, scale, 1, round_bf16=False)
+    Lr, gr = M.loss_grad(w, (Mfix @ r).astype(np.float32), r.astype(np.float32), e.astype(np.float32), K, dofs, pid,
+                         nbrs, scale, round_bf16=False)
+    assert abs(L1 - Lr) <= 1e-6 * Lr and np.linalg.norm(g1 - gr) <= 1e-5 * np.linalg.norm(gr)
+    for k in (1, 4):
+        L, g = M.loss_grad_steps(w, r, e, K, Mfix, dofs, pid, nbrs, scale, k, round_bf16=False)
+        d = rng.standard_normal(M.NPARAM)
+        wp = (w + 1e-3 * d).astype(np.float32)
+        wm = (w - 1e-3 * d).astype(np.float32)
+        Lp = M.loss_grad_steps(wp, r, e, K, Mfix, dofs, pid, nbrs, scale, k, round_bf16=False)[0]
+        Lm = M.loss_grad_steps(wm, r, e, K, Mfix, dofs, pid, nbrs, scale, k, round_bf16=False)[0]
+        fd, an = Lp - Lm, g @ (wp.astype(np.float64) - wm.astype(np.float64))
+        assert abs(fd - an) <= 1e-3 * abs(fd), (k, fd, an)
+        assert 0.0 <= L <= 1.0
