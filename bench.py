@@ -12,8 +12,9 @@ plate_sphere (400x400x40 plate + dropped sphere, contact) or bar_wave
 
 One bench step = one velocity-Verlet step: damage + dilatation pass, force
 pass with the Verlet epilogue, over every bond. value = bonds x steps /
-device time (CUDA events on the library's stream, max over ranks, summed over
-ranks for N > 1: each rank runs its own body, weak scaling).
+device time (CUDA events on the library's stream). With N > 1 GPUs the body
+is split into N slabs with ghost layers and one NCCL exchange per step
+(strong scaling; bonds of owned points, max over ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload W]
 
@@ -414,7 +415,7 @@ def kernel_roofline(ctx, dt, t0, ksteps, nb, n, hbm, peak_src, slots):
             "streamed_slots": slots, "bonds": nb}
 
 
-def e2e_leg(ctx, n, nb, esteps, world, max_over_ranks, barrier):
+def e2e_leg(ctx, n, nb, esteps, ranks, max_over_ranks, barrier):
     """The drop-in computeForce call with host buffers: each step the H2D of the
     current coordinates from pinned memory, damage + dilatation + force on the
     device, D2H of the force density, then the state update that commits the
@@ -438,9 +439,69 @@ def e2e_leg(ctx, n, nb, esteps, world, max_over_ranks, barrier):
         ctx._ok(ctx.L.pd_update_state(ctx.h))
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    return {"value": world * nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n,
-            "d2h_bytes_per_step": 24 * n, "steps": esteps,
+    # nb: the bonds evaluated per step over all ranks; n: this rank's points
+    # (ranks of about equal size copy about ranks x 24 n bytes each way)
+    return {"value": nb * esteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 24 * n * ranks,
+            "d2h_bytes_per_step": 24 * n * ranks, "steps": esteps,
             "api": "pd_compute_force (host y in, host force out) + pd_update_state"}
+
+
+def slab_leg(args, world, rank, local, max_over_ranks, barrier, hbm, peak_src):
+    """N > 1: one body split over the ranks (peridigm_b200.slabs: equal-count
+    slabs along the longest axis, a ghost layer two horizons deep, one NCCL
+    point-to-point exchange of ghost state per step), strong scaling. value =
+    bond evaluations of all ranks' owned points per second over the device
+    time of the step loop (library stream events, exchanges included), max
+    over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from peridigm_b200 import Context, slabs
+
+    w, blocks = make_workload(args.workload)
+    n = int(len(w["vol"]))
+    plan = slabs.slab_plan(w["x"], w["horizon"], world, rank)
+    lw = slabs.local_workload(w, plan)
+    log(f"rank {rank}: {len(plan.owned)} owned of {n} points, {len(plan.local) - len(plan.owned)} ghosts, "
+        f"peers {sorted(set(plan.send) | set(plan.recv))}")
+    ctx = Context(device=local, precision="split")
+    setup(ctx, lw, blocks)
+    dt_t = torch.tensor([w.get("safety", 0.7) * ctx.critical_time_step()], dtype=torch.float64, device="cuda")
+    dist.all_reduce(dt_t, op=dist.ReduceOp.MIN)  # ghosts' truncated families only over-estimate theirs
+    dt = float(dt_t.item())
+    owned_bonds = int(ctx.field("Number_Of_Neighbors")[plan.owned_local].sum())
+    tot = torch.tensor([owned_bonds], dtype=torch.float64, device="cuda")
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    nb = int(tot.item())
+    engine = slabs.ContextEngine(ctx)
+    halo = slabs.HaloExchange(plan, torch.device("cuda", local), dist)
+    slabs.run_slab(engine, halo, dt, args.warmup)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    st = slabs.run_slab(engine, halo, dt, args.steps, t0=args.warmup * dt)
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(st["device_ms"])
+    value = nb * args.steps / (ms / 1e3)
+    ghost_bytes = 48 * sum(len(v) for v in plan.recv.values())
+    # e2e: the drop-in computeForce on every rank's slab with host buffers (the
+    # ghost layer makes the owned points' forces exact without an exchange)
+    e2e = e2e_leg(ctx, len(plan.local), nb, args.e2e_steps, world, max_over_ranks, barrier)
+    ctx.close()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
+            "config": {"workload": workload_name(args.workload), "points": n, "bonds": nb, "horizon_over_h": 3.015,
+                       "dt": dt, "precision": "split_fp32", "l2": "inputs larger than L2",
+                       "parallelism": f"slabs x{world} (ghost layer 2 horizons, NCCL point-to-point exchange "
+                                      f"per step, {ghost_bytes} bytes received by rank 0)"},
+            "roofline": {"bound": "hbm", "kernel": "split passes (slab of rank 0)", "achieved": None, "peak": hbm,
+                         "unit": "GB/s", "frac": None, "peak_source": peak_src, "traffic": None},
+            "cpu_baseline": None, "e2e": e2e, "clocks": clk,
+            "gpu_launches": (2 + 2 * len(halo.peers)) * args.steps}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def profile_mode(args):
@@ -515,6 +576,7 @@ def main():
     ap.add_argument("--kernel-steps", type=int, default=50, help="steps of the per-kernel event timing")
     ap.add_argument("--e2e-steps", type=int, default=200, help="steps of the host-buffer e2e leg")
     ap.add_argument("--fp64-steps", type=int, default=20, help="timed steps of the FP64 leg")
+    ap.add_argument("--slabs", action="store_true", help="the slab path (the default for N > 1) also at N = 1")
     # profiling modes
     ap.add_argument("--profile", action="store_true")
     ap.add_argument("--precision", default="split", choices=["split", "fp64", "both"])
@@ -550,11 +612,18 @@ def main():
 
     torch.cuda.set_device(local)
     pg = None
-    if world > 1:
+    if world > 1 or args.slabs:
         import datetime
 
         import torch.distributed as dist
 
+        if "MASTER_ADDR" not in os.environ:  # one process outside torchrun
+            import socket
+
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0",
+                                  WORLD_SIZE="1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
 
@@ -571,6 +640,10 @@ def main():
             pg.barrier()
 
     hbm, peak_src = peak_hbm()
+    if world > 1 or args.slabs:
+        slab_leg(args, world, rank, local, max_over_ranks, barrier, hbm, peak_src)
+        pg.destroy_process_group()
+        return
     w, blocks = make_workload(args.workload)
     n = int(len(w["vol"]))
     log(f"workload {w['name']}: {n} points")
@@ -591,7 +664,7 @@ def main():
 
     log(f"per-kernel ms {roofline['per_kernel_ms']}")
     # ---- e2e: the drop-in computeForce call with host buffers ---------------
-    e2e = e2e_leg(ctx, n, nb, args.e2e_steps, world, max_over_ranks, barrier)
+    e2e = e2e_leg(ctx, n, nb, args.e2e_steps, 1, max_over_ranks, barrier)
     ctx.close()
     log(f"e2e {e2e['value']:.3e}")
 
@@ -651,13 +724,13 @@ def main():
                          f"source, block constants)"}
 
     line = {"metric": METRIC, "value": sp["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": sp["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": sp["ms"] / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
             "config": {"workload": workload_name(args.workload), "points": n, "bonds": nb, "horizon_over_h": 3.015,
                        "dt": dt, "precision": "split_fp32",
                        "l2": "inputs larger than L2 (%.1f GB of algorithmic bytes per step vs 126 MB L2)"
                              % (step_bytes / 1e9),
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": "one GPU"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": sp["clocks"],
             "gpu_launches": 2 * args.steps, "notched_plate": extra, "qs": qs, "fp64": fp64}
     if rank == 0:

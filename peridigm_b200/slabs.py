@@ -85,6 +85,40 @@ def slab_plans(x, horizon, nranks, depth=2.0, axis=None):
     return plans
 
 
+def slab_plan(x, horizon, nranks, rank, depth=2.0, axis=None):
+    """This rank's plan alone, equal to slab_plans(...)[rank], from vectorised
+    passes over the points (what a rank of a large body computes)."""
+    P = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+    owner, axis = slab_owner(P, nranks, axis)
+    h = float(np.max(horizon))
+    c = P[:, axis]
+    lo = np.full(nranks, np.inf)
+    hi = np.full(nranks, -np.inf)
+    np.minimum.at(lo, owner, c)
+    np.maximum.at(hi, owner, c)
+
+    def within(r):  # coordinates inside rank r's owned range widened by depth horizons
+        return (c >= lo[r] - depth * h) & (c <= hi[r] + depth * h)
+
+    mine = owner == rank
+    local = np.nonzero(mine | within(rank))[0] if mine.any() else np.zeros(0, np.int64)
+    owned = np.nonzero(mine)[0]
+    plan = SlabPlan(rank=rank, nranks=nranks, axis=axis, owned=owned, local=local,
+                    owned_local=np.searchsorted(local, owned))
+    here = np.zeros(len(c), bool)
+    here[local] = True
+    for p in range(nranks):
+        if p == rank or not np.isfinite(lo[p]):
+            continue
+        out = np.nonzero(mine & within(p))[0]
+        inc = np.nonzero((owner == p) & here)[0]
+        if len(out):
+            plan.send[p] = np.searchsorted(local, out).astype(np.int32)
+        if len(inc):
+            plan.recv[p] = np.searchsorted(local, inc).astype(np.int32)
+    return plan
+
+
 def local_workload(w, plan):
     """The workload restricted to a rank's local points (same keys as the
     workload dicts of peridigm_b200.workloads)."""

@@ -91,3 +91,20 @@ def test_two_gloo_ranks_match_one_domain(tmp_path):
     assert (seen == 1).all()
     assert np.array_equal(u.ravel(), ref.u)
     assert np.array_equal(v.ravel(), ref.v)
+
+
+def test_single_rank_plan_equals_the_full_plans():
+    """slab_plan (one rank, vectorised) gives each rank exactly its entry of slab_plans."""
+    w = _plate()
+    for nr in (2, 3, 4):
+        full = slabs.slab_plans(w["x"], w["horizon"], nr)
+        for r in range(nr):
+            one = slabs.slab_plan(w["x"], w["horizon"], nr, r)
+            assert one.axis == full[r].axis
+            assert np.array_equal(one.owned, full[r].owned) and np.array_equal(one.local, full[r].local)
+            assert np.array_equal(one.owned_local, full[r].owned_local)
+            assert set(one.send) == set(full[r].send) and set(one.recv) == set(full[r].recv)
+            for q in one.send:
+                assert np.array_equal(one.send[q], full[r].send[q])
+            for q in one.recv:
+                assert np.array_equal(one.recv[q], full[r].recv[q])
