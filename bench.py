@@ -335,6 +335,7 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
             warm.qs_load_step(w2["times"][0], w2["times"][1], newton_tolerance=-1e-8, cg_relative_tolerance=1e-8,
                               preconditioner=precond)
         with arm_context(arm, precond) as ctx:
+            out["_bonds"] = ctx.num_bonds()
             st = None
             clocks = ClockSampler(local)
             clocks.start()
@@ -364,6 +365,29 @@ def qs_leg(local, load_steps, cpu_threads=0, learned_modes=6):
                                            sample="block-Jacobi CG restated in C on %d host threads: 20 CG "
                                                   "iterations and one Newton set-up at the solved state, scaled by "
                                                   "the GPU solve's Newton and CG counts" % cpu_threads)
+    # Roofline of the CG iterations: bytes one iteration must move at least,
+    # over the solve's device time per iteration (Newton set-up included, so
+    # the fractions are lower bounds). Tangent apply: pass 1 streams the bond
+    # geometry (32 B) and neighbor id (4 B), pass 2 the geometry, the
+    # coefficient pair (16 B) and the id: 88 B per bond; per point the
+    # gathered vector, dilatation increments and output (about 64 B) and about
+    # ten FP64 3-vectors of CG and block Jacobi (240 B). The coarse arms also
+    # read the dense FP64 coarse inverse (modes x aggregates squared x 8 B;
+    # aggregates: the non-empty cells of side two horizons).
+    nb2 = out.pop("_bonds")
+    n2 = len(w2["vol"])
+    side = 2.0 * w2["horizon"] * (1.0 + 1.0e-6)
+    P2 = w2["x"].reshape(-1, 3)
+    cells = np.floor((P2 - P2.min(0)) / side).astype(np.int64)
+    naggr = len(np.unique(cells @ np.array([1, 1 << 20, 1 << 40], np.int64)))
+    hbm, peak_src = peak_hbm()
+    it_bytes = 88 * nb2 + 304 * n2
+    roof = {"bytes_per_cg_iteration": it_bytes, "aggregates": naggr, "peak_gbs": hbm, "peak_source": peak_src}
+    for arm, modes in (("block_jacobi", 0), ("two_level", 3), ("two_level_rigid", 6)):
+        b = it_bytes + 8 * (modes * naggr) ** 2
+        ach = b * out[arm]["cg_iterations"] / out[arm]["seconds"] / 1e9
+        roof[arm] = {"bytes_per_cg_iteration": b, "achieved_gbs": ach, "frac": ach / hbm}
+    out["roofline"] = roof
     bj = out["block_jacobi"]["seconds"]
     for arm in ("two_level", "two_level_rigid", "mpnn", "mpnn_last_epoch"):
         out[f"{arm}_speedup_over_block_jacobi"] = bj / out[arm]["seconds"]

@@ -249,9 +249,6 @@ __device__ __forceinline__ int64_t xs_index(int64_t k) { return 96 * (k >> 5) + 
 #ifndef PD_BOND_MINB
 #define PD_BOND_MINB 8
 #endif
-#ifndef PD_STREAM_AHEAD
-#define PD_STREAM_AHEAD 0
-#endif
 constexpr int kUnroll = PD_BOND_UNROLL;
 // Threads per block of the split bond passes: 8 blocks of 128 fill an SM's
 // 1024 threads at 64 registers, and the last partial wave of a ~5000-block
@@ -344,30 +341,12 @@ __device__ __forceinline__ void sell_walk(int64_t i, int lane, const int64_t* __
   uint32_t* pd = reinterpret_cast<uint32_t*>(dmg + 32 * so + 4 * l32);
   const float4* px = reinterpret_cast<const float4*>(bx3 + 96 * so + 4 * l32);
   int4 jn = F > 0 ? __ldcs(pc) : make_int4(0, 0, 0, 0);
-#if PD_STREAM_AHEAD
-  // the next block's damage word and X held in registers one block ahead
-  uint32_t dwn = 0;
-  float4 xan = make_float4(0.f, 0.f, 0.f, 0.f), xbn = xan, xcn = xan;
-  if (F > 0) {
-    dwn = __ldcs(pd);
-    xan = __ldcs(px), xbn = __ldcs(px + 32), xcn = __ldcs(px + 64);
-  }
-#endif
 #pragma unroll 1
   for (int b = 0; b < F; ++b, pc += 32, pd += 32, px += 96) {
     const int4 jj = jn;
     if (b + 1 < F) jn = __ldcs(pc + 32);
-#if PD_STREAM_AHEAD
-    const uint32_t dw = dwn;
-    const float4 xa = xan, xb = xbn, xc = xcn;
-    if (b + 1 < F) {
-      dwn = __ldcs(pd + 32);
-      xan = __ldcs(px + 96), xbn = __ldcs(px + 128), xcn = __ldcs(px + 160);
-    }
-#else
     const uint32_t dw = __ldcs(pd);
     const float4 xa = __ldcs(px), xb = __ldcs(px + 32), xc = __ldcs(px + 64);
-#endif
     const Rec8 u0 = ld_rec_t<NC>(ur + jj.x), u1 = ld_rec_t<NC>(ur + jj.y), u2 = ld_rec_t<NC>(ur + jj.z),
                u3 = ld_rec_t<NC>(ur + jj.w);
     uint8_t* pb = reinterpret_cast<uint8_t*>(pd);
