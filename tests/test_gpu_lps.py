@@ -290,3 +290,35 @@ def test_errors_are_reported():
         with pytest.raises(PDError) as e:
             ctx.compute_force(np.zeros(6))
         assert e.value.code == 6
+
+
+def test_split_refuses_weighted_influence_across_horizons():
+    """The split passes weight both halves of a bond with the owner's
+    omega(|X|, h_i); with an influence function other than "One" and blocks of
+    different horizons that would differ from the neighbor's omega(|X|, h_j),
+    so the split context refuses (PD_ERR_UNSUPPORTED) where FP64 runs; with
+    one horizon the Gaussian split force matches the FP64 path to 1e-6."""
+    x, vol, y, h = make_cloud(seed=2)
+    n = len(vol)
+    block = (np.arange(n) % 2).astype(np.int32)
+    row, col = O.neighbor_search(x, h)
+    nl = O.csr_to_nl(row, col)  # symmetric families (one search radius), given through pd_set_bonds
+    f = {}
+    for precision in ("fp64", "split"):
+        for horizons in ([h, 1.2 * h], [h, h]):
+            with Context(precision=precision, influence="Gaussian") as ctx:
+                ctx.set_points(x, vol, block)
+                ctx.set_horizons(horizons)
+                ctx.set_bonds(nl)
+                for b in (0, 1):
+                    ctx.material(130e9, 78e9, 7800.0, block=b)
+                if precision == "split" and horizons[1] != horizons[0]:
+                    with pytest.raises(PDError) as e:
+                        ctx.compute_force(y)
+                    assert e.value.code == 6 and b"horizon" in ctx.L.pd_last_error(ctx.h)
+                    continue
+                if horizons[1] == horizons[0]:
+                    f[precision] = ctx.compute_force(y)
+                else:
+                    ctx.compute_force(y)  # FP64 handles both horizons (omega_j with h_j)
+    assert rel_l2(f["split"], f["fp64"]) < 1e-6
