@@ -396,7 +396,9 @@ int pd_mpnn_loss_grad(pd_ctx* ctx, const float* pair, double* loss, float* grad)
 /* The middle level alone, z = Q S G^T G S Q^T r (host arrays [3n], prescribed
  * dofs of z left zero), with S from the block-Jacobi blocks at the current
  * displacement: the product each PD_PRECOND_MPNN CG iteration adds, for
- * parity checks of the inference kernels. */
+ * parity checks of the inference kernels. It runs as one cooperative launch
+ * whose phases meet at grid barriers with bounded waits; PD_ERR_TIMEOUT if
+ * one ran out (here, or at the end of a PD_PRECOND_MPNN CG solve). */
 int pd_mpnn_apply(pd_ctx* ctx, const double* r, double* z);
 /* Coarse level under the network (training, loss and PD_PRECOND_MPNN solves):
  * cell >= 0 puts the network on top of the two-level preconditioner with

@@ -80,8 +80,9 @@ struct MpnnState {
   DBuf<float> w, g_, am, av, gpart;
   DBuf<__nv_bfloat16> wb;
   int64_t adam_t = 0;
-  // activations: two sets (v and the gradient input), FP32
-  DBuf<float> v[2], h[2][NL + 1], m[2][NL], d, s_buf, t_buf, out3;
+  // activations: two sets (v and the gradient input), FP32; the fused apply's
+  // transposed layers write (s_buf, t_buf), (d, t_alt), (s_alt, t_alt2)
+  DBuf<float> v[2], h[2][NL + 1], m[2][NL], d, s_buf, t_buf, s_alt, t_alt, t_alt2, out3;
   // training set: per pair a, r, e (float, 3n each)
   DBuf<float> pairs;
   int64_t npairs = 0, cap = 0;
@@ -90,19 +91,11 @@ struct MpnnState {
   int every = 0;
   std::vector<DBuf<double>*> snap_r, snap_x;
   int nsnap = 0;
-  // Inference apply (10 small launches) as one CUDA graph, captured for one
-  // (r, z, fixed mask) triple; the buffers it reads are fixed once the
-  // patches are built, the weights and scales are read at replay.
-  cudaGraphExec_t apply_exec = nullptr;
-  const double* apply_r = nullptr;
-  double* apply_z = nullptr;
-  const uint8_t* apply_fixed = nullptr;
-  void drop_graph() {
-    if (apply_exec) cudaGraphExecDestroy(apply_exec);
-    apply_exec = nullptr;
-  }
+  // Inference apply: one cooperative launch of apply_grid blocks; bar holds
+  // its grid barrier (arrivals, generation).
+  DBuf<unsigned int> bar;
+  int apply_grid = 0;
   ~MpnnState() {
-    drop_graph();
     for (auto* p : snap_r) delete p;
     for (auto* p : snap_x) delete p;
   }
@@ -255,8 +248,8 @@ __global__ void k_pt_encode_t(int64_t np, const float* __restrict__ x, const __n
 // Sum over the patch's neighbor rows J (CSR b0..b1) of x_J's features
 // 4hl..4hl+3 (half a warp per patch, 16 lanes x float4 = 64 features): eight
 // rows in flight, added in groups of four in row order.
-__device__ __forceinline__ float4 nbr_sum4(const float4* __restrict__ x4, const int32_t* __restrict__ pcol,
-                                           int64_t b0, int64_t b1, int hl, float4 a) {
+__device__ __forceinline__ float4 nbr_sum4(const float4* __restrict__ x4, const int32_t* __restrict__ pcol, int64_t b0,
+                                           int64_t b1, int hl, float4 a) {
   auto add4 = [&](const float4& u0, const float4& u1, const float4& u2, const float4& u3) {
     a.x += (u0.x + u1.x) + (u2.x + u3.x);
     a.y += (u0.y + u1.y) + (u2.y + u3.y);
@@ -290,145 +283,181 @@ __device__ __forceinline__ float4 nbr_sum4(const float4* __restrict__ x4, const 
   return a;
 }
 
-// One layer: hout = hin + Ws hin + Wn mean_J hin_J (mout receives the mean).
-// Block tiles of 16 patches (256 threads): phase 1 copies the k-major
-// weights [Ws | Wn] into shared memory (16-byte loads, 4 per thread, all in
-// flight before the first store) and gathers [h | mean] rows (half a warp per
-// patch, 4 features per lane, eight neighbor rows in flight); phase 2
-// multiplies (4 outputs per thread, 8-byte weight reads, FP32 accumulation).
+// Shared memory of one layer tile: the k-major weights [Ws | Wn] (rows padded
+// to 144 B, 16-byte aligned) and the tile's [h | mean] rows.
+struct LayerSmem {
+  __nv_bfloat16 sW[2 * H][H + 8];
+  float sX[kTile][2 * H + 4];
+};
+// ... of one transposed-layer tile: sW[o][k'] (k' < H: Ws[o][k'], else
+// Wn[o][k'-H]) and the tile's input rows.
+struct LayerTSmem {
+  __nv_bfloat16 sW[H][2 * H];
+  float sX[kTile][H + 4];
+};
+
+// Copy a layer's k-major [Ws | Wn] into shared memory (16-byte loads, 4 per
+// thread, all in flight before the first store; 256 threads).
+__device__ __forceinline__ void layer_stage_w(LayerSmem& S, const __nv_bfloat16* __restrict__ wk) {
+  constexpr int kW16 = 2 * H * H / 8;  // 16-byte words of [Ws | Wn]
+  static_assert(kW16 == 4 * 256, "launched with 256 threads");
+  const uint4* w4 = reinterpret_cast<const uint4*>(wk);
+  uint4 wr[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) wr[q] = __ldg(w4 + threadIdx.x + 256 * q);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int t8 = threadIdx.x + 256 * q;
+    *reinterpret_cast<uint4*>(&S.sW[t8 / (H / 8)][(t8 % (H / 8)) * 8]) = wr[q];
+  }
+}
+
+// One tile of 16 patches from i0 of a layer: hout = hin + Ws hin + Wn mean_J
+// hin_J (mout, when given, receives the mean). Phase 1 gathers [h | mean]
+// rows (half a warp per patch, 4 features per lane, eight neighbor rows in
+// flight); phase 2 multiplies (4 outputs per thread, 8-byte weight reads,
+// FP32 accumulation). Block-uniform; leaves shared memory free for reuse.
+__device__ __forceinline__ void layer_tile(LayerSmem& S, int64_t i0, int64_t np, const int64_t* __restrict__ prow,
+                                           const int32_t* __restrict__ pcol, const float* hin, float* hout,
+                                           float* mout) {
+  const int hl = threadIdx.x & 15, r = threadIdx.x >> 4;  // phase 1: patch r of the tile
+  const int nl = threadIdx.x >> 4, ob = (threadIdx.x & 15) * 4;  // phase 2: patch nl, outputs ob..ob+3
+  const float4* h4 = reinterpret_cast<const float4*>(hin);
+  {
+    const int64_t I = i0 + r;
+    float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), mv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (I < np) {
+      hv = h4[(int64_t)(H / 4) * I + hl];
+      const int64_t b0 = prow[I], b1 = prow[I + 1];
+      mv = nbr_sum4(h4, pcol, b0, b1, hl, mv);
+      const float inv = b1 > b0 ? 1.0f / (float)(b1 - b0) : 0.0f;
+      mv.x *= inv;
+      mv.y *= inv;
+      mv.z *= inv;
+      mv.w *= inv;
+      if (mout) reinterpret_cast<float4*>(mout)[(int64_t)(H / 4) * I + hl] = mv;
+    }
+    *reinterpret_cast<float4*>(&S.sX[r][4 * hl]) = hv;
+    *reinterpret_cast<float4*>(&S.sX[r][H + 4 * hl]) = mv;
+  }
+  __syncthreads();
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
+  for (int k = 0; k < 2 * H; ++k) {
+    const float x = S.sX[nl][k];
+    const uint2 wv = *reinterpret_cast<const uint2*>(&S.sW[k][ob]);
+    const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const float2 f = __bfloat1622float2(w2[j]);
+      acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
+      acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
+    }
+  }
+  const int64_t I = i0 + nl;
+  if (I < np)
+    *reinterpret_cast<float4*>(hout + (int64_t)H * I + ob) = make_float4(
+        S.sX[nl][ob] + acc[0], S.sX[nl][ob + 1] + acc[1], S.sX[nl][ob + 2] + acc[2], S.sX[nl][ob + 3] + acc[3]);
+  __syncthreads();
+}
+
+// One layer over all patches in block tiles of 16 (256 threads).
 __global__ void __launch_bounds__(256) k_pt_layer(int64_t np, const int64_t* __restrict__ prow,
                                                   const int32_t* __restrict__ pcol,
                                                   const __nv_bfloat16* __restrict__ wk, const float* __restrict__ hin,
                                                   float* __restrict__ hout, float* __restrict__ mout) {
-  __shared__ __align__(16) __nv_bfloat16 sW[2 * H][H + 8];  // sW[k][o] (rows padded: 144 B, 16-B aligned)
-  __shared__ __align__(16) float sX[kTile][2 * H + 4];
-  {
-    constexpr int kW16 = 2 * H * H / 8;  // 16-byte words of [Ws | Wn]
-    static_assert(kW16 == 4 * 256, "launched with 256 threads");
-    const uint4* w4 = reinterpret_cast<const uint4*>(wk);
-    uint4 wr[4];
+  __shared__ __align__(16) LayerSmem S;
+  layer_stage_w(S, wk);
+  for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile)
+    layer_tile(S, i0, np, prow, pcol, hin, hout, mout);
+}
+
+// Copy a layer's [Ws | Wn] (their own layout) into shared memory as sW[o][k'].
+__device__ __forceinline__ void layer_t_stage_w(LayerTSmem& S, const __nv_bfloat16* __restrict__ wl) {
+  constexpr int kW16 = 2 * H * H / 8;  // 16-byte words of [Ws | Wn] in their own layout
+  static_assert(kW16 == 4 * 256, "launched with 256 threads");
+  const uint4* w4 = reinterpret_cast<const uint4*>(wl);
+  uint4 wr[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) wr[q] = __ldg(w4 + threadIdx.x + 256 * q);
+  for (int q = 0; q < 4; ++q) wr[q] = __ldg(w4 + threadIdx.x + 256 * q);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int t8 = threadIdx.x + 256 * q;
-      *reinterpret_cast<uint4*>(&sW[t8 / (H / 8)][(t8 % (H / 8)) * 8]) = wr[q];
-    }
-  }
-  const int hl = threadIdx.x & 15, r = threadIdx.x >> 4;  // phase 1: patch r of the tile
-  const int nl = threadIdx.x >> 4, ob = (threadIdx.x & 15) * 4;  // phase 2: patch nl, outputs ob..ob+3
-  const float4* h4 = reinterpret_cast<const float4*>(hin);
-  for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile) {
-    {
-      const int64_t I = i0 + r;
-      float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), mv = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (I < np) {
-        hv = h4[(int64_t)(H / 4) * I + hl];
-        const int64_t b0 = prow[I], b1 = prow[I + 1];
-        mv = nbr_sum4(h4, pcol, b0, b1, hl, mv);
-        const float inv = b1 > b0 ? 1.0f / (float)(b1 - b0) : 0.0f;
-        mv.x *= inv;
-        mv.y *= inv;
-        mv.z *= inv;
-        mv.w *= inv;
-        if (mout) reinterpret_cast<float4*>(mout)[(int64_t)(H / 4) * I + hl] = mv;
-      }
-      *reinterpret_cast<float4*>(&sX[r][4 * hl]) = hv;
-      *reinterpret_cast<float4*>(&sX[r][H + 4 * hl]) = mv;
-    }
-    __syncthreads();
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 8
-    for (int k = 0; k < 2 * H; ++k) {
-      const float x = sX[nl][k];
-      const uint2 wv = *reinterpret_cast<const uint2*>(&sW[k][ob]);
-      const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const float2 f = __bfloat1622float2(w2[j]);
-        acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
-        acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
-      }
-    }
-    const int64_t I = i0 + nl;
-    if (I < np)
-      *reinterpret_cast<float4*>(hout + (int64_t)H * I + ob) =
-          make_float4(sX[nl][ob] + acc[0], sX[nl][ob + 1] + acc[1], sX[nl][ob + 2] + acc[2], sX[nl][ob + 3] + acc[3]);
-    __syncthreads();
+  for (int q = 0; q < 4; ++q) {
+    const int t8 = threadIdx.x + 256 * q;  // part, row o, 8-column segment
+    const int part = t8 / (H * H / 8), o = (t8 % (H * H / 8)) / (H / 8), seg = t8 % (H / 8);
+    *reinterpret_cast<uint4*>(&S.sW[o][part * H + seg * 8]) = wr[q];
   }
 }
 
-// Transposed layer, per patch: s = d + Ws^T d, t = Wn^T d / deg (the gather
-// of t over the symmetric patch graph completes it, k_pt_gather_t).
+// Transposed-layer input rows of the tile at i0: d_I (zero past np).
+__device__ __forceinline__ void layer_t_load(LayerTSmem& S, int64_t i0, int64_t np, const float* d) {
+  const float4* d4 = reinterpret_cast<const float4*>(d);
+#pragma unroll
+  for (int q = 0; q < kTile * H / 4 / 256; ++q) {
+    const int t = threadIdx.x + 256 * q, r = t / (H / 4), o4 = t % (H / 4);
+    const int64_t I = i0 + r;
+    *reinterpret_cast<float4*>(&S.sX[r][4 * o4]) =
+        I < np ? d4[(int64_t)(H / 4) * I + o4] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// Transposed layer on the tile's rows in shared memory: s = d + Ws^T d,
+// t = Wn^T d / deg (the gather of t over the symmetric patch graph completes
+// it). Block-uniform; leaves shared memory free for reuse.
+__device__ __forceinline__ void layer_t_mul(LayerTSmem& S, int64_t i0, int64_t np, const int64_t* __restrict__ prow,
+                                            float* s_out, float* t_out) {
+  __syncthreads();
+  const int nl = threadIdx.x >> 4, ob = (threadIdx.x & 15) * 8;  // patch nl, outputs ob..ob+7 of [s | t]
+  float acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+#pragma unroll 4
+  for (int o = 0; o < H; ++o) {
+    const float x = S.sX[nl][o];
+    const uint4 wv = *reinterpret_cast<const uint4*>(&S.sW[o][ob]);
+    const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float2 f = __bfloat1622float2(w2[j]);
+      acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
+      acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
+    }
+  }
+  const int64_t I = i0 + nl;
+  if (I < np) {  // the 8 outputs lie in one part: s (ob < H) or t
+    float4* o4;
+    float v[8];
+    if (ob < H) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = S.sX[nl][ob + j] + acc[j];
+      o4 = reinterpret_cast<float4*>(s_out + (int64_t)H * I + ob);
+    } else {
+      const int64_t deg = prow[I + 1] - prow[I];
+      const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = acc[j] * inv;
+      o4 = reinterpret_cast<float4*>(t_out + (int64_t)H * I + (ob - H));
+    }
+    o4[0] = make_float4(v[0], v[1], v[2], v[3]);
+    o4[1] = make_float4(v[4], v[5], v[6], v[7]);
+  }
+  __syncthreads();
+}
+
+// Transposed layer, per patch, over all patches in block tiles of 16.
 __global__ void __launch_bounds__(256) k_pt_layer_t(int64_t np, const int64_t* __restrict__ prow,
                                                     const __nv_bfloat16* __restrict__ wl, const float* __restrict__ d,
                                                     float* __restrict__ s_out, float* __restrict__ t_out) {
-  __shared__ __align__(16) __nv_bfloat16 sW[H][2 * H];  // sW[o][k']: k' < H: Ws[o][k'], else Wn[o][k'-H]
-  __shared__ __align__(16) float sX[kTile][H + 4];
-  {
-    constexpr int kW16 = 2 * H * H / 8;  // 16-byte words of [Ws | Wn] in their own layout
-    static_assert(kW16 == 4 * 256, "launched with 256 threads");
-    const uint4* w4 = reinterpret_cast<const uint4*>(wl);
-    uint4 wr[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) wr[q] = __ldg(w4 + threadIdx.x + 256 * q);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int t8 = threadIdx.x + 256 * q;  // part, row o, 8-column segment
-      const int part = t8 / (H * H / 8), o = (t8 % (H * H / 8)) / (H / 8), seg = t8 % (H / 8);
-      *reinterpret_cast<uint4*>(&sW[o][part * H + seg * 8]) = wr[q];
-    }
-  }
-  const int nl = threadIdx.x >> 4, ob = (threadIdx.x & 15) * 8;  // patch nl, outputs ob..ob+7 of [s | t]
-  const float4* d4 = reinterpret_cast<const float4*>(d);
+  __shared__ __align__(16) LayerTSmem S;
+  layer_t_stage_w(S, wl);
   for (int64_t i0 = (int64_t)blockIdx.x * kTile; i0 < np; i0 += (int64_t)gridDim.x * kTile) {
-#pragma unroll
-    for (int q = 0; q < kTile * H / 4 / 256; ++q) {
-      const int t = threadIdx.x + 256 * q, r = t / (H / 4), o4 = t % (H / 4);
-      const int64_t I = i0 + r;
-      *reinterpret_cast<float4*>(&sX[r][4 * o4]) = I < np ? d4[(int64_t)(H / 4) * I + o4] : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    __syncthreads();
-    float acc[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
-#pragma unroll 4
-    for (int o = 0; o < H; ++o) {
-      const float x = sX[nl][o];
-      const uint4 wv = *reinterpret_cast<const uint4*>(&sW[o][ob]);
-      const __nv_bfloat162* w2 = reinterpret_cast<const __nv_bfloat162*>(&wv);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float2 f = __bfloat1622float2(w2[j]);
-        acc[2 * j] = fmaf(x, f.x, acc[2 * j]);
-        acc[2 * j + 1] = fmaf(x, f.y, acc[2 * j + 1]);
-      }
-    }
-    const int64_t I = i0 + nl;
-    if (I < np) {  // the 8 outputs lie in one part: s (ob < H) or t
-      float4* o4;
-      float v[8];
-      if (ob < H) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = sX[nl][ob + j] + acc[j];
-        o4 = reinterpret_cast<float4*>(s_out + (int64_t)H * I + ob);
-      } else {
-        const int64_t deg = prow[I + 1] - prow[I];
-        const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = acc[j] * inv;
-        o4 = reinterpret_cast<float4*>(t_out + (int64_t)H * I + (ob - H));
-      }
-      o4[0] = make_float4(v[0], v[1], v[2], v[3]);
-      o4[1] = make_float4(v[4], v[5], v[6], v[7]);
-    }
-    __syncthreads();
+    layer_t_load(S, i0, np, d);
+    layer_t_mul(S, i0, np, prow, s_out, t_out);
   }
 }
 
 // x_J = s_J + sum_{I in N(J)} t_I  (half a warp per patch, 4 features per lane).
-// No __launch_bounds__ here or on k_pt_tail: with (256) ptxas held both to 32
-// registers and spilled; without it they take 34 and 38, no spills.
+// No __launch_bounds__ here: with (256) ptxas held it to 32 registers and
+// spilled; without it it takes 34, no spills.
 __global__ void k_pt_gather_t(int64_t np, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
                               const float* __restrict__ s, const float* __restrict__ t, float* __restrict__ x) {
   const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
@@ -439,85 +468,457 @@ __global__ void k_pt_gather_t(int64_t np, const int64_t* __restrict__ prow, cons
   reinterpret_cast<float4*>(x)[(int64_t)(H / 4) * J + hl] = a;
 }
 
-// Inference head, restrict then encode: v_I = s_I sum_{i in I, free} r_i,
-// h0_I = W0 v_I (warp per patch; the same sums in the same order as
-// k_pt_restrict and k_pt_encode).
-__global__ void __launch_bounds__(256) k_pt_head(int64_t np, const int32_t* __restrict__ patch_cell,
-                                                 const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
-                                                 const double* __restrict__ r, const uint8_t* __restrict__ fixed,
-                                                 const float* __restrict__ scale, const __nv_bfloat16* __restrict__ wb,
-                                                 float* __restrict__ h0) {
-  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (I >= np) return;
-  const int q = patch_cell[I];
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
-    const int64_t p = sorted[t];
-    const uint8_t f = fixed ? fixed[p] : 0;
-    if (!(f & 1)) s0 += r[3 * p];
-    if (!(f & 2)) s1 += r[3 * p + 1];
-    if (!(f & 4)) s2 += r[3 * p + 2];
+// ---------------------------------------------------------------------------
+// Inference apply, one cooperative launch
+// ---------------------------------------------------------------------------
+// The apply's phases are chains of dependent loads (neighbor ids, then their
+// rows; point ids, then their masks and residuals), so a block keeps its
+// tile's ids in shared memory for the whole launch and every phase starts
+// from them: no more tiles than blocks leaves each block one tile.
+constexpr int kMaxDeg = 26;     // a patch's neighbors: the other non-empty cells of its 3x3x3 block
+constexpr int kTilePts = 1024;  // point ids of a tile kept in shared memory (past that, read per use)
+
+struct ApplyArgs {
+  int64_t np;
+  const int64_t* prow;
+  const int32_t* pcol;
+  const int32_t* patch_cell;
+  const int64_t* cstart;
+  const int32_t* sorted;
+  const double* r;
+  const uint8_t* fixed;
+  const float* scale;
+  const __nv_bfloat16* wb;
+  float* h[NL + 1];  // encoder output and the layers' outputs
+  float* s[NL];      // transposed layers' s and t, one pair per layer (each
+  float* t[NL];      // written once per launch)
+  double* z;
+  unsigned int* bar;  // grid barrier: arrivals, generation
+  int* status;
+};
+
+// A tile's patches: neighbor ids and counts, point ids and fixed masks.
+struct __align__(16) TileMeta {
+  int32_t nbr[kTile][kMaxDeg];
+  int32_t deg[kTile];
+  int32_t cnt[kTile];
+  int32_t pbeg[kTile + 1];  // tile-local offsets into pts
+  int32_t pts[kTilePts];
+  uint8_t pfix[kTilePts];
+};
+// The tile's rows ([h | mean] of a layer, 2H, or the input of a transposed
+// layer, H) and the phase's weights as B fragments: word [ks][n][t] holds
+// B[16ks + 2t .. +1][n] and word [ks][n][4 + t] B[16ks + 2t + 8 .. +9][n]
+// (K = 128, N = 64 for a layer; K = 64, N = 128 for a transposed one).
+struct ApplySmem {
+  float sX[kTile][2 * H + 4];
+  uint32_t sB[2 * H * H / 2];
+};
+// Tiles whose ids a block keeps (a block of a grid smaller than the tile
+// count takes two or more tiles; past kMetaSlots they are reloaded per use).
+constexpr int kMetaSlots = 2;
+constexpr size_t kApplySmem = kMetaSlots * sizeof(TileMeta) + sizeof(ApplySmem);
+
+// Polls of the barrier's generation before a block gives up (0.2 to 1.5 s
+// depending on how long the sleeps between polls last).
+constexpr unsigned kBarSpin = 1u << 22;
+
+// Grid-wide barrier of a cooperative launch (every block resident). Arrival
+// is a release-acquire add on the count; the last block to arrive resets it
+// and advances the generation with a release; the others poll the generation
+// with acquire loads, at most kBarSpin times, after which the block sets
+// ST_TIMEOUT and returns false (the kernel then ends; blocks still waiting
+// for it run out the same way).
+__device__ bool grid_barrier(unsigned int* bar, int* status) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int g, old;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(bar + 1) : "memory");
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
+    int good = 1;
+    if (old == gridDim.x - 1) {
+      asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(bar), "r"(0u) : "memory");
+      asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar + 1) : "memory");
+    } else {
+      for (unsigned it = 0;; ++it) {
+        unsigned int cur;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar + 1) : "memory");
+        if (cur != g) break;
+        if (it >= kBarSpin) {
+          atomicOr(status, ST_TIMEOUT);
+          good = 0;
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    ok = good;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-  }
-  // lane 0's sums (the butterfly leaves each lane its own rounding)
-  s0 = __shfl_sync(0xffffffffu, s0, 0);
-  s1 = __shfl_sync(0xffffffffu, s1, 0);
-  s2 = __shfl_sync(0xffffffffu, s2, 0);
-  const double sc = 1.0 * (double)scale[I];
-  const float v[3] = {(float)(sc * s0), (float)(sc * s1), (float)(sc * s2)};
-  float2 h;
-  {
-    const int o = 2 * lane;
-    float a = 0.f, b = 0.f;
-    for (int c = 0; c < 3; ++c) a = fmaf(__bfloat162float(wb[OFF_W0 + 3 * o + c]), v[c], a);
-    for (int c = 0; c < 3; ++c) b = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 1) + c]), v[c], b);
-    h = make_float2(a, b);
-  }
-  reinterpret_cast<float2*>(h0)[(int64_t)(H / 2) * I + lane] = h;
+  __syncthreads();
+  return ok != 0;
 }
 
-// Inference tail, the last transposed gather, W0^T and the prolongation:
-// x_J = s_J + sum_{I in N(J)} t_I, out_J = W0^T x_J, z_i += s_J out_J on the
-// free dofs of J's points (half a warp per patch; a half warp past np keeps
-// to the shuffles and touches no memory).
-__global__ void k_pt_tail(int64_t np, const int64_t* __restrict__ prow, const int32_t* __restrict__ pcol,
-                          const float* __restrict__ s, const float* __restrict__ t,
-                          const __nv_bfloat16* __restrict__ wb, const int32_t* __restrict__ patch_cell,
-                          const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
-                          const float* __restrict__ scale, const uint8_t* __restrict__ fixed, double* __restrict__ z) {
-  const int64_t J = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
-  const int hl = threadIdx.x & 15;
-  if (((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) >> 4 >= np) return;  // whole warp past np
-  const bool live = J < np;
-  float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (live) {
-    a = reinterpret_cast<const float4*>(s)[(int64_t)(H / 4) * J + hl];
-    a = nbr_sum4(reinterpret_cast<const float4*>(t), pcol, prow[J], prow[J + 1], hl, a);
+// The tile's ids at i0 into shared memory (half a warp per patch).
+__device__ void load_tile_meta(TileMeta& M, const ApplyArgs& a, int64_t i0) {
+  const int r = threadIdx.x >> 4, hl = threadIdx.x & 15;
+  const int64_t I = i0 + r;
+  int deg = 0, cnt = 0;
+  int64_t b0 = 0, c0 = 0;
+  if (I < a.np) {
+    b0 = a.prow[I];
+    deg = (int)(a.prow[I + 1] - b0);
+    const int q = a.patch_cell[I];
+    c0 = a.cstart[q];
+    cnt = (int)(a.cstart[q + 1] - c0);
   }
-  auto w0t = [&](int c) {  // sum over the 64 features of W0[o][c] x_o
-    const int o = 4 * hl;
-    float v = __bfloat162float(wb[OFF_W0 + 3 * o + c]) * a.x;
-    v = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 1) + c]), a.y, v);
-    v = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 2) + c]), a.z, v);
-    v = fmaf(__bfloat162float(wb[OFF_W0 + 3 * (o + 3) + c]), a.w, v);
-    for (int k = 8; k > 0; k >>= 1) v += __shfl_xor_sync(0xffffffffu, v, k, 16);
-    return (double)__shfl_sync(0xffffffffu, v, 0, 16);  // the half warp's first lane
+  if (deg > kMaxDeg) {  // not from the patch graph's construction: keep shared memory in bounds
+    if (hl == 0) atomicOr(a.status, ST_BAD_INDEX);
+    deg = kMaxDeg;
+  }
+  for (int k = hl; k < deg; k += 16) M.nbr[r][k] = a.pcol[b0 + k];
+  if (hl == 0) M.deg[r] = deg, M.cnt[r] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int k = 0; k < kTile; ++k) M.pbeg[k] = o, o += M.cnt[k];
+    M.pbeg[kTile] = o;
+  }
+  __syncthreads();
+  if (M.pbeg[kTile] <= kTilePts)
+    for (int k = hl; k < cnt; k += 16) {
+      const int32_t p = a.sorted[c0 + k];
+      M.pts[M.pbeg[r] + k] = p;
+      M.pfix[M.pbeg[r] + k] = a.fixed ? a.fixed[p] : 0;
+    }
+  __syncthreads();
+}
+
+// Sum of the rows x_J, J in idx[0..deg) (shared memory), features
+// 4hl..4hl+3, eight rows in flight: groups of four in order, then the last
+// deg mod 4 rows one by one (the order of nbr_sum4). Plain loads: every
+// buffer the apply gathers from is written once per launch, before the
+// barrier that precedes its reads.
+__device__ __forceinline__ float4 nbr_sum_idx(const float4* x4, const int32_t* idx, int deg, int hl, float4 a) {
+  auto add4 = [&](const float4& u0, const float4& u1, const float4& u2, const float4& u3) {
+    a.x += (u0.x + u1.x) + (u2.x + u3.x);
+    a.y += (u0.y + u1.y) + (u2.y + u3.y);
+    a.z += (u0.z + u1.z) + (u2.z + u3.z);
+    a.w += (u0.w + u1.w) + (u2.w + u3.w);
   };
-  const double out0 = w0t(0), out1 = w0t(1), out2 = w0t(2);
-  if (!live) return;
-  const double sc = 1.0 * (double)scale[J];
-  const int q = patch_cell[J];
-  for (int64_t k = cstart[q] + hl; k < cstart[q + 1]; k += 16) {
-    const int64_t p = sorted[k];
-    const uint8_t f = fixed ? fixed[p] : 0;
-    if (!(f & 1)) z[3 * p] += sc * out0;
-    if (!(f & 2)) z[3 * p + 1] += sc * out1;
-    if (!(f & 4)) z[3 * p + 2] += sc * out2;
+  for (int b = 0; b < deg; b += 8) {
+    const int m = min(8, deg - b);
+    float4 u[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k < m) u[k] = x4[(int64_t)(H / 4) * idx[b + k] + hl];
+    if (m >= 4) add4(u[0], u[1], u[2], u[3]);
+    if (m == 8) {
+      add4(u[4], u[5], u[6], u[7]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k >= (m & 4) && k < m) {  // the last batch's rows past its group
+          a.x += u[k].x;
+          a.y += u[k].y;
+          a.z += u[k].z;
+          a.w += u[k].w;
+        }
+    }
+  }
+  return a;
+}
+
+// D += A B on the tensor cores: m16n8k16, BF16 operands, FP32 accumulation.
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) { return *reinterpret_cast<uint32_t*>(&v); }
+
+// An FP32 pair as three BF16 pairs, x = hi + mid + lo: each residual is
+// exact in FP32, so the three parts carry x's 24 bits and the BF16 products
+// with the (BF16) weights are exact.
+__device__ __forceinline__ void split3(float2 x, uint32_t& hi, uint32_t& mid, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x.x, x.y);
+  const float2 hf = __bfloat1622float2(h);
+  const float r0 = x.x - hf.x, r1 = x.y - hf.y;
+  const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+  const float2 mf = __bfloat1622float2(m);
+  hi = bf2_bits(h);
+  mid = bf2_bits(m);
+  lo = bf2_bits(__floats2bfloat162_rn(r0 - mf.x, r1 - mf.y));
+}
+
+// acc += X[16 x 16 at column k0] B for the warp's B fragment (b0, b1): the
+// row-major A fragment of the tile's rows g, g+8 (sX, FP32) in three BF16
+// parts, smallest first.
+__device__ __forceinline__ void mma_rows(float (&acc)[4], const float (*sX)[2 * H + 4], int k0, uint32_t b0,
+                                         uint32_t b1) {
+  const int g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+  uint32_t hi[4], mid[4], lo[4];
+  split3(*reinterpret_cast<const float2*>(&sX[g][k0 + 2 * t]), hi[0], mid[0], lo[0]);
+  split3(*reinterpret_cast<const float2*>(&sX[g + 8][k0 + 2 * t]), hi[1], mid[1], lo[1]);
+  split3(*reinterpret_cast<const float2*>(&sX[g][k0 + 2 * t + 8]), hi[2], mid[2], lo[2]);
+  split3(*reinterpret_cast<const float2*>(&sX[g + 8][k0 + 2 * t + 8]), hi[3], mid[3], lo[3]);
+  mma_bf16(acc, lo, b0, b1);
+  mma_bf16(acc, mid, b0, b1);
+  mma_bf16(acc, hi, b0, b1);
+}
+
+// A layer's B fragments into shared memory: B[k][n] = Ws[n][k] (k < H),
+// Wn[n][k - H], from the weights' own layout (pairs of consecutive k are one
+// 32-bit word: word (n, k/2) of part k / H).
+__device__ __forceinline__ void stage_layer_b(uint32_t* sB, const __nv_bfloat16* __restrict__ wl) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(wl);
+  for (int e = threadIdx.x; e < H * H; e += blockDim.x) {  // e = (ks, n, j): j < 8
+    const int j = e & 7, n = (e >> 3) % H, ks = (e >> 3) / H;
+    const int k = 16 * ks + 2 * (j & 3) + 8 * (j >> 2);
+    sB[e] = __ldg(w + ((k / H) * H * H + n * H + k % H) / 2);
+  }
+}
+
+// ... a transposed layer's: B[o][n'] = Ws[o][n'] (n' < H), Wn[o][n' - H],
+// from the k-major copy ([part*H + k][o]: pairs of consecutive o are one word).
+__device__ __forceinline__ void stage_layer_t_b(uint32_t* sB, const __nv_bfloat16* __restrict__ wk) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(wk);
+  for (int e = threadIdx.x; e < H * H; e += blockDim.x) {  // e = (ks, n', j)
+    const int j = e & 7, n = (e >> 3) % (2 * H), ks = (e >> 3) / (2 * H);
+    const int o = 16 * ks + 2 * (j & 3) + 8 * (j >> 2);
+    sB[e] = __ldg(w + (n * H + o) / 2);
+  }
+}
+
+// Layer tile: h_out = h + Ws h + Wn mean_J h_J on the tile at i0 (the gather
+// of layer_tile; the product on the tensor cores, FP32-exact operands in
+// three BF16 parts and FP32 accumulation: warp w, outputs 8w..8w+7).
+__device__ __forceinline__ void apply_layer_tile(ApplySmem& S, const TileMeta& M, int64_t i0, int64_t np,
+                                                 const float* hin, float* hout) {
+  const int hl = threadIdx.x & 15, r = threadIdx.x >> 4;
+  const float4* h4 = reinterpret_cast<const float4*>(hin);
+  {
+    const int64_t I = i0 + r;
+    float4 hv = make_float4(0.f, 0.f, 0.f, 0.f), mv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (I < np) {
+      hv = h4[(int64_t)(H / 4) * I + hl];
+      const int deg = M.deg[r];
+      mv = nbr_sum_idx(h4, M.nbr[r], deg, hl, mv);
+      const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
+      mv.x *= inv;
+      mv.y *= inv;
+      mv.z *= inv;
+      mv.w *= inv;
+    }
+    *reinterpret_cast<float4*>(&S.sX[r][4 * hl]) = hv;
+    *reinterpret_cast<float4*>(&S.sX[r][H + 4 * hl]) = mv;
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+  for (int ks = 0; ks < 2 * H / 16; ++ks) {
+    const uint32_t* bw = S.sB + ((ks * H) + 8 * w + g) * 8;
+    mma_rows(acc, S.sX, 16 * ks, bw[t], bw[4 + t]);
+  }
+  const int n = 8 * w + 2 * t;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int row = g + 8 * h;
+    const int64_t I = i0 + row;
+    if (I < np)
+      *reinterpret_cast<float2*>(hout + (int64_t)H * I + n) =
+          make_float2(S.sX[row][n] + acc[2 * h], S.sX[row][n + 1] + acc[2 * h + 1]);
+  }
+  __syncthreads();
+}
+
+// Transposed-layer tile: rows of d (own rows) or the gathered s_J + sum t_I,
+// then s = x + Ws^T x, t = Wn^T x / deg (warp w: outputs 16w..16w+15 of [s | t]).
+__device__ __forceinline__ void apply_layer_t_tile(ApplySmem& S, const TileMeta& M, int64_t i0, int64_t np,
+                                                   const float* d, const float* sin, const float* tin, float* s_out,
+                                                   float* t_out) {
+  const int hl = threadIdx.x & 15, r = threadIdx.x >> 4;
+  {
+    const int64_t J = i0 + r;
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (J < np) {
+      if (d) {
+        x = reinterpret_cast<const float4*>(d)[(int64_t)(H / 4) * J + hl];
+      } else {
+        x = reinterpret_cast<const float4*>(sin)[(int64_t)(H / 4) * J + hl];
+        x = nbr_sum_idx(reinterpret_cast<const float4*>(tin), M.nbr[r], M.deg[r], hl, x);
+      }
+    }
+    *reinterpret_cast<float4*>(&S.sX[r][4 * hl]) = x;
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, g = (threadIdx.x & 31) >> 2, t = threadIdx.x & 3;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+    for (int ks = 0; ks < H / 16; ++ks) {
+      const uint32_t* bw = S.sB + ((ks * 2 * H) + 16 * w + 8 * j + g) * 8;
+      mma_rows(acc, S.sX, 16 * ks, bw[t], bw[4 + t]);
+    }
+    const int n = 16 * w + 8 * j + 2 * t;  // the pair lies in one part: s (n < H) or t
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = g + 8 * h;
+      const int64_t I = i0 + row;
+      if (I >= np) continue;
+      if (n < H) {
+        *reinterpret_cast<float2*>(s_out + (int64_t)H * I + n) =
+            make_float2(S.sX[row][n] + acc[2 * h], S.sX[row][n + 1] + acc[2 * h + 1]);
+      } else {
+        const int deg = M.deg[row];
+        const float inv = deg > 0 ? 1.0f / (float)deg : 0.0f;
+        *reinterpret_cast<float2*>(t_out + (int64_t)H * I + (n - H)) =
+            make_float2(acc[2 * h] * inv, acc[2 * h + 1] * inv);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// z += Q S G^T G S Q^T r on the free dofs in phases separated by grid
+// barriers: the head (restrict, W0), three layers, three transposed layers
+// with the gathers between them, the tail (last gather, W0^T,
+// prolongation). Per patch it computes what the one-pass kernels of the
+// training path do (k_pt_restrict + k_pt_encode, k_pt_layer, k_pt_layer_t,
+// k_pt_gather_t, k_pt_encode_t + k_pt_prolong): the same gathers in the same
+// order, the point sums in FP64 over half a warp, the layer products on the
+// tensor cores (mma.sync, FP32 accumulation, which rounds in its own order).
+// Every phase walks the same tiles, so the last layer and the first
+// transposed layer need no barrier between them.
+__global__ void __launch_bounds__(256, 4) k_pt_apply(ApplyArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  TileMeta* slots = reinterpret_cast<TileMeta*>(smem);
+  ApplySmem& S = *reinterpret_cast<ApplySmem*>(smem + kMetaSlots * sizeof(TileMeta));
+  static_assert(sizeof(TileMeta) % 16 == 0, "16-byte aligned layer tiles");
+  const int64_t np = a.np;
+  const int hl = threadIdx.x & 15, r = threadIdx.x >> 4;
+  const int64_t tile0 = (int64_t)blockIdx.x * kTile, tstride = (int64_t)gridDim.x * kTile;
+  int64_t held[kMetaSlots];  // the tiles whose ids the slots hold
+  for (int k = 0; k < kMetaSlots; ++k) held[k] = -1;
+  const TileMeta* cur_meta = slots;
+  auto meta = [&](int64_t i0) {  // the block's k-th tile goes to slot min(k, kMetaSlots - 1)
+    const int64_t kt = (i0 - tile0) / tstride;
+    const int k = kt < kMetaSlots - 1 ? (int)kt : kMetaSlots - 1;
+    if (held[k] != i0) load_tile_meta(slots[k], a, i0), held[k] = i0;
+    cur_meta = slots + k;
+  };
+  auto point = [&](int64_t I, int k) -> int32_t {  // point k of patch r of the tile at I - r
+    return cur_meta->pbeg[kTile] <= kTilePts ? cur_meta->pts[cur_meta->pbeg[r] + k] : a.sorted[a.cstart[a.patch_cell[I]] + k];
+  };
+  auto pfixed = [&](int k, int32_t p) -> uint8_t {
+    return cur_meta->pbeg[kTile] <= kTilePts ? cur_meta->pfix[cur_meta->pbeg[r] + k] : (a.fixed ? a.fixed[p] : (uint8_t)0);
+  };
+
+  // head: v_I = s_I sum_{i in I, free} r_i, h0_I = W0 v_I
+  for (int64_t i0 = tile0; i0 < np; i0 += tstride) {
+    meta(i0);
+    const int64_t I = i0 + r;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (I < np) {
+      const int cnt = cur_meta->cnt[r];
+      for (int k = hl; k < cnt; k += 16) {
+        const int32_t p = point(I, k);
+        const uint8_t f = pfixed(k, p);
+        if (!(f & 1)) s0 += a.r[3 * (int64_t)p];
+        if (!(f & 2)) s1 += a.r[3 * (int64_t)p + 1];
+        if (!(f & 4)) s2 += a.r[3 * (int64_t)p + 2];
+      }
+    }
+    for (int o = 8; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o, 16);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o, 16);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o, 16);
+    }
+    // the half warp's first lane's sums (the butterfly leaves each lane its own rounding)
+    s0 = __shfl_sync(0xffffffffu, s0, 0, 16);
+    s1 = __shfl_sync(0xffffffffu, s1, 0, 16);
+    s2 = __shfl_sync(0xffffffffu, s2, 0, 16);
+    if (I < np) {
+      const double sc = 1.0 * (double)a.scale[I];
+      const float v[3] = {(float)(sc * s0), (float)(sc * s1), (float)(sc * s2)};
+      float h[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int o = 4 * hl + j;
+        float acc = 0.f;
+        for (int c = 0; c < 3; ++c) acc = fmaf(__bfloat162float(a.wb[OFF_W0 + 3 * o + c]), v[c], acc);
+        h[j] = acc;
+      }
+      reinterpret_cast<float4*>(a.h[0])[(int64_t)(H / 4) * I + hl] = make_float4(h[0], h[1], h[2], h[3]);
+    }
+  }
+  if (!grid_barrier(a.bar, a.status)) return;
+
+  // layers: h_{l+1} = h_l + Ws h_l + Wn mean_J h_l,J
+  for (int l = 0; l < NL; ++l) {
+    stage_layer_b(S.sB, a.wb + OFF_L + l * LSZ);  // read after the tile's first barrier
+    for (int64_t i0 = tile0; i0 < np; i0 += tstride) {
+      meta(i0);
+      apply_layer_tile(S, *cur_meta, i0, np, a.h[l], a.h[l + 1]);
+    }
+    if (l + 1 < NL && !grid_barrier(a.bar, a.status)) return;
+  }
+
+  // transposed layers, last first: the first on the block's own rows of h_NL,
+  // the others on the gathered output of the one before; layer l writes pair
+  // NL-1-l
+  for (int l = NL - 1; l >= 0; --l) {
+    __syncthreads();  // the last tile's products have read the layer's fragments
+    stage_layer_t_b(S.sB, a.wb + OFF_KM + l * LSZ);
+    const int out = NL - 1 - l, in = out - 1;
+    for (int64_t i0 = tile0; i0 < np; i0 += tstride) {
+      meta(i0);
+      apply_layer_t_tile(S, *cur_meta, i0, np, l == NL - 1 ? a.h[NL] : nullptr, in >= 0 ? a.s[in] : nullptr,
+                         in >= 0 ? a.t[in] : nullptr, a.s[out], a.t[out]);
+    }
+    if (!grid_barrier(a.bar, a.status)) return;
+  }
+
+  // tail: x_J = s_J + sum_{I in N(J)} t_I, out_J = W0^T x_J, z_i += s_J out_J
+  // on the free dofs of J's points (half a warp per patch; the shuffles see
+  // both halves: the tile loop is block-uniform)
+  const float* sl = a.s[NL - 1];
+  const float* tl = a.t[NL - 1];
+  for (int64_t i0 = tile0; i0 < np; i0 += tstride) {
+    meta(i0);
+    const int64_t J = i0 + r;
+    const bool live = J < np;
+    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (live) {
+      x = reinterpret_cast<const float4*>(sl)[(int64_t)(H / 4) * J + hl];
+      x = nbr_sum_idx(reinterpret_cast<const float4*>(tl), cur_meta->nbr[r], cur_meta->deg[r], hl, x);
+    }
+    auto w0t = [&](int c) {  // sum over the 64 features of W0[o][c] x_o
+      const int o = 4 * hl;
+      float v = __bfloat162float(a.wb[OFF_W0 + 3 * o + c]) * x.x;
+      v = fmaf(__bfloat162float(a.wb[OFF_W0 + 3 * (o + 1) + c]), x.y, v);
+      v = fmaf(__bfloat162float(a.wb[OFF_W0 + 3 * (o + 2) + c]), x.z, v);
+      v = fmaf(__bfloat162float(a.wb[OFF_W0 + 3 * (o + 3) + c]), x.w, v);
+      for (int k = 8; k > 0; k >>= 1) v += __shfl_xor_sync(0xffffffffu, v, k, 16);
+      return (double)__shfl_sync(0xffffffffu, v, 0, 16);  // the half warp's first lane
+    };
+    const double out0 = w0t(0), out1 = w0t(1), out2 = w0t(2);
+    if (live) {
+      const double sc = 1.0 * (double)a.scale[J];
+      const int cnt = cur_meta->cnt[r];
+#pragma unroll 4
+      for (int k = hl; k < cnt; k += 16) {
+        const int32_t p = point(J, k);
+        const uint8_t f = pfixed(k, p);
+        if (!(f & 1)) a.z[3 * (int64_t)p] += sc * out0;
+        if (!(f & 2)) a.z[3 * (int64_t)p + 1] += sc * out1;
+        if (!(f & 4)) a.z[3 * (int64_t)p + 2] += sc * out2;
+      }
+    }
   }
 }
 
@@ -739,19 +1140,22 @@ static int mp_patches(pd_ctx* c, MpnnState* s, double side) {
   PD_CUDA_TRY(c, s->d.alloc((size_t)H * np));
   PD_CUDA_TRY(c, s->s_buf.alloc((size_t)H * np));
   PD_CUDA_TRY(c, s->t_buf.alloc((size_t)H * np));
+  PD_CUDA_TRY(c, s->s_alt.alloc((size_t)H * np));
+  PD_CUDA_TRY(c, s->t_alt.alloc((size_t)H * np));
+  PD_CUDA_TRY(c, s->t_alt2.alloc((size_t)H * np));
   PD_CUDA_TRY(c, s->out3.alloc(3 * np));
   s->g = g;
   s->np = np;
   s->n = n;
   s->patch = side;
   s->patches = true;
+  s->apply_grid = 0;  // the fused apply's grid follows the patch count
   return PD_OK;
 }
 
 int mpnn_init(pd_ctx* c, uint64_t seed, double patch) {
   if (!c->mpnn) c->mpnn = new MpnnState();
   MpnnState* s = mp_state(c);
-  s->drop_graph();  // the patch buffers are rebuilt
   TRY_RC(mp_patches(c, s, patch));
   // weights: W0 = 0.5 [I3; 0] and near-zero layers plus small uniform noise
   // from the seed, so G^T G starts near 0.25 I (a Jacobi-scaled middle level)
@@ -846,59 +1250,70 @@ static int mp_backward(pd_ctx* c, MpnnState* s, int k, const float* U) {
   return PD_OK;
 }
 
-// z += Q S G^T G S Q^T r: head (restrict + W0), 3 layers, 3 transposed
-// layers with 2 gathers between them, tail (gather + W0^T + prolongation).
-static int mp_apply_launches(pd_ctx* c, MpnnState* s, const double* r, double* z, const uint8_t* fixed) {
-  const int64_t np = s->np;
-  k_pt_head<<<gw(np), 256, 0, c->stream>>>(np, s->patch_cell.p, s->cstart.p, s->sorted.p, r, fixed, s->scale.p,
-                                           s->wb.p, s->h[0][0].p);
-  for (int l = 0; l < NL; ++l)
-    k_pt_layer<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->wb.p + OFF_KM + l * LSZ, s->h[0][l].p,
-                                                 s->h[0][l + 1].p, nullptr);
-  const float* cur = s->h[0][NL].p;
-  for (int l = NL - 1; l >= 0; --l) {
-    k_pt_layer_t<<<gtile(np), 256, 0, c->stream>>>(np, s->prow.p, s->wb.p + OFF_L + l * LSZ, cur, s->s_buf.p,
-                                                   s->t_buf.p);
-    if (l > 0) {
-      k_pt_gather_t<<<gh(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->d.p);
-      cur = s->d.p;
-    }
-  }
-  k_pt_tail<<<gh(np), 256, 0, c->stream>>>(np, s->prow.p, s->pcol.p, s->s_buf.p, s->t_buf.p, s->wb.p,
-                                           s->patch_cell.p, s->cstart.p, s->sorted.p, s->scale.p, fixed, z);
-  PD_CUDA_TRY(c, cudaGetLastError());
-  return PD_OK;
-}
-
-// z += Q S G^T G S Q^T r on the free dofs (inference), replayed as one graph.
+// z += Q S G^T G S Q^T r on the free dofs (inference): one cooperative
+// launch of k_pt_apply (every block resident, so its grid barriers are met).
 int mpnn_apply_add(pd_ctx* c, const double* r, double* z) {
   MpnnState* s = mp_state(c);
   if (!s || !s->ready || !s->patches || s->n != c->n) {
     c->err = "learned preconditioner not initialised";
     return PD_ERR_STATE;
   }
-  const uint8_t* fixed = qs_fixed_mask(c);
-  if (!s->apply_exec || s->apply_r != r || s->apply_z != z || s->apply_fixed != fixed) {
-    s->drop_graph();
-    PD_CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = mp_apply_launches(c, s, r, z, fixed);
-    cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);  // always ends the capture
-    if (rc != PD_OK) {
-      if (g) cudaGraphDestroy(g);
-      return rc;
-    }
-    PD_CUDA_TRY(c, e);
-    const cudaError_t ei = cudaGraphInstantiate(&s->apply_exec, g, 0);
-    cudaGraphDestroy(g);
-    if (ei != cudaSuccess) s->apply_exec = nullptr;
-    PD_CUDA_TRY(c, ei);
-    s->apply_r = r;
-    s->apply_z = z;
-    s->apply_fixed = fixed;
+  if (!s->bar.p) {
+    PD_CUDA_TRY(c, s->bar.alloc(2));
+    PD_CUDA_TRY(c, dzero(c, s->bar.p, 2 * sizeof(unsigned int)));
   }
-  PD_CUDA_TRY(c, cudaGraphLaunch(s->apply_exec, c->stream));
+  if (s->apply_grid == 0) {
+    int per_sm = 0, sms = 0;
+    PD_CUDA_TRY(c, cudaFuncSetAttribute(k_pt_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem));
+    PD_CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt_apply, 256, kApplySmem));
+    PD_CUDA_TRY(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    if (per_sm < 1) {
+      c->err = "learned preconditioner: the fused apply kernel cannot be resident";
+      return PD_ERR_CUDA;
+    }
+    const int64_t tiles = std::max<int64_t>(1, (s->np + kTile - 1) / kTile);
+    s->apply_grid = (int)std::min<int64_t>(tiles, (int64_t)per_sm * sms);
+  }
+  ApplyArgs a{};
+  a.np = s->np;
+  a.prow = s->prow.p;
+  a.pcol = s->pcol.p;
+  a.patch_cell = s->patch_cell.p;
+  a.cstart = s->cstart.p;
+  a.sorted = s->sorted.p;
+  a.r = r;
+  a.fixed = qs_fixed_mask(c);
+  a.scale = s->scale.p;
+  a.wb = s->wb.p;
+  for (int l = 0; l <= NL; ++l) a.h[l] = s->h[0][l].p;
+  a.s[0] = s->s_buf.p;
+  a.t[0] = s->t_buf.p;
+  a.s[1] = s->d.p;
+  a.t[1] = s->t_alt.p;
+  a.s[2] = s->s_alt.p;
+  a.t[2] = s->t_alt2.p;
+  static_assert(NL == 3, "one (s, t) pair per transposed layer");
+  a.z = z;
+  a.bar = s->bar.p;
+  a.status = c->status.p;
+  void* args[] = {&a};
+  PD_CUDA_TRY(c, cudaLaunchCooperativeKernel((const void*)k_pt_apply, dim3((unsigned)s->apply_grid), dim3(256), args,
+                                             kApplySmem, c->stream));
   return PD_OK;
+}
+
+// After a stream synchronisation: PD_ERR_TIMEOUT when a barrier wait of the
+// fused apply ran out (the status bit is cleared and the barrier reset).
+int mpnn_check_status(pd_ctx* c) {
+  int st = 0;
+  PD_CUDA_TRY(c, d2h(c, &st, c->status.p, sizeof(int)));
+  if (!(st & ST_TIMEOUT)) return PD_OK;
+  const int rest = st & ~(int)ST_TIMEOUT;
+  PD_CUDA_TRY(c, h2d(c, c->status.p, &rest, sizeof(int)));
+  MpnnState* s = mp_state(c);
+  if (s && s->bar.p) PD_CUDA_TRY(c, dzero(c, s->bar.p, 2 * sizeof(unsigned int)));
+  c->err = "learned preconditioner: a grid barrier wait of the fused apply ran out";
+  return PD_ERR_TIMEOUT;
 }
 
 // One pair (a = P_bj r, r, e as float [3n] each, captured at modulus kscale x
@@ -977,7 +1392,7 @@ int mpnn_loss_grad(pd_ctx* c, const float* pair_host, double* loss, float* grad_
 
 // z = Q S G^T G S Q^T r (the middle level alone, host arrays [3n]) with the
 // scales of the current displacement's block-Jacobi blocks, through the same
-// graph-replayed apply the CG iterations use.
+// fused apply the CG iterations use.
 int mpnn_middle_apply(pd_ctx* c, const double* r_host, double* z_host) {
   MpnnState* s = mp_state(c);
   if (!s || !s->ready || !s->patches || s->n != c->n) {
@@ -996,8 +1411,7 @@ int mpnn_middle_apply(pd_ctx* c, const double* r_host, double* z_host) {
   PD_CUDA_TRY(c, dzero(c, z.p, b3));
   TRY_RC(mpnn_apply_add(c, r.p, z.p));
   PD_CUDA_TRY(c, d2h(c, z_host, z.p, b3));
-  s->drop_graph();  // captured for the buffers freed on return
-  return PD_OK;
+  return mpnn_check_status(c);
 }
 
 int mpnn_train(pd_ctx* c, int epochs, double lr, int batch, double* loss_out) {

@@ -635,6 +635,7 @@ static int qs_cg(pd_ctx* c, int precond, double rel_tol, int max_it, int* iters,
   double rel = 0.0;
   int rc = qs_cg_run(c, PD_PRECOND_MPNN, rel_tol, max_it, &its, &rel, &stalled);
   if (rc != PD_OK && rc != PD_ERR_NOT_CONVERGED && rc != PD_ERR_NONFINITE) return rc;
+  TRY_RC(mpnn_check_status(c));
   // true residual r = b - K x
   const int64_t n = c->n;
   k_qs_pack_x(n, s, c);

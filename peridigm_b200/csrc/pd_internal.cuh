@@ -252,6 +252,8 @@ constexpr int kQsMulti = 6;  // vectors per multi-vector tangent product
 int qs_apply_K_multi(pd_ctx* c, const double* p_dev, double* q_dev, double* dth_dev);
 bool mpnn_ready(const pd_ctx* c);
 int mpnn_apply_add(pd_ctx* c, const double* r, double* z);
+// PD_ERR_TIMEOUT (status bit cleared) when a grid barrier wait of the apply ran out.
+int mpnn_check_status(pd_ctx* c);
 int mpnn_prepare(pd_ctx* c, const double* dinv);
 int qs_block_jacobi_current(pd_ctx* c, const double** dinv_out);
 void mpnn_release(pd_ctx* c);

@@ -7,8 +7,8 @@ gains inside the quasi-static CG.
   blocks and coarse operator, on the same BF16 weights: loss to 1e-6
   relative, gradient to 1e-5 relative L2 (measured 1e-7: FP32 activations
   and sums against FP64);
-* pd_mpnn_apply (the inference graph) vs the oracle's Q S G^T G S Q^T r, and
-  bit-identical on a second call;
+* pd_mpnn_apply (one cooperative launch, grid barriers between the phases)
+  vs the oracle's Q S G^T G S Q^T r, and bit-identical on a second call;
 * two-level QS solves with capture produce pairs, and training lowers the loss;
 * on the translation two-level base, the trained preconditioner solves a
   held-out QS problem to the two-level displacement (1e-8 relative) in fewer
@@ -78,7 +78,7 @@ def test_mpnn_gradient_matches_oracle(coarse):
 @pytest.mark.parametrize("seed", [6, 9])
 def test_mpnn_apply_matches_oracle(seed):
     """The inference product each learned CG iteration adds (head, 3 layers,
-    3 transposed layers, tail: one replayed graph) against the oracle's
+    3 transposed layers, tail: one cooperative launch) against the oracle's
     Q S G^T G S Q^T r on the same BF16 weights (FP32 activations: 1e-5)."""
     w = _bar(seed=seed)
     n = len(w["vol"])
