@@ -220,7 +220,7 @@ def reference_arm(args, world, rank):
     value = r["value"]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{workload_name(args.workload)} (sample: {sname}_{dims[0]}x{dims[1]}x{dims[2]})",
                        "points": int(len(w["vol"])), "bonds": int(len(col)), "precision": "fp64"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
@@ -401,9 +401,12 @@ def explicit_leg(w, blocks, local, steps, warmup, precision, world, max_over_ran
     context (still open) and the timing."""
     from peridigm_b200 import Context
 
+    import torch
+
     ctx = Context(device=local, precision=precision)
     setup(ctx, w, blocks)
     nb = ctx.num_bonds()
+    free_b, total_b = torch.cuda.mem_get_info(local)
     dt = w.get("safety", 0.7) * ctx.critical_time_step()
     ctx.verlet_run(dt, warmup)
     barrier()
@@ -415,7 +418,7 @@ def explicit_leg(w, blocks, local, steps, warmup, precision, world, max_over_ran
     clk = clocks.stop() if clocks else None
     ms = max_over_ranks(st["device_ms"])
     return ctx, {"nb": nb, "dt": dt, "ms": ms, "value": world * nb * steps / (ms / 1e3), "t_done": (warmup + steps) * dt,
-                 "clocks": clk, "broken_bonds": st["broken_bonds"]}
+                 "clocks": clk, "broken_bonds": st["broken_bonds"], "device_gb": (total_b - free_b) / 1e9}
 
 
 def kernel_roofline(ctx, dt, t0, ksteps, nb, n, hbm, peak_src, slots):
@@ -751,7 +754,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": sp["ms"] / args.steps, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
             "config": {"workload": workload_name(args.workload), "points": n, "bonds": nb, "horizon_over_h": 3.015,
-                       "dt": dt, "precision": "split_fp32",
+                       "dt": dt, "precision": "split_fp32", "device_gb_in_use": round(sp["device_gb"], 1),
                        "l2": "inputs larger than L2 (%.1f GB of algorithmic bytes per step vs 126 MB L2)"
                              % (step_bytes / 1e9),
                        "parallelism": "one GPU"},
