@@ -470,10 +470,11 @@ def coarse_operator(T, agg, fixed_dofs=()):
 
 
 def gauss_jordan_blocked(A, bk=64):
-    """In-place blocked Gauss-Jordan inverse without pivoting of an SPD matrix,
-    the step structure of peridigm_b200/csrc/k_coarse.cu (k_gj_pivot,
-    k_gj_panel, k_gj_update) in numpy. For each block k of width bk (the last
-    one ragged):
+    """In-place blocked Gauss-Jordan inverse without pivoting of an SPD matrix
+    with every entry updated, in numpy: the step structure that
+    gauss_jordan_sym_blocked (the form peridigm_b200/csrc/k_coarse.cu runs)
+    restricts to the tiles on and above the diagonal. For each block k of
+    width bk (the last one ragged):
 
       P  = A_kk^-1                      (pivot block)
       R  = P A_k*, with P itself in R's block-k columns   (row panel)
@@ -497,6 +498,49 @@ def gauss_jordan_blocked(A, bk=64):
         A[:, ~keep] = 0.0
         A -= upd
         A[k0:k1, :] = R
+    return A
+
+
+def gauss_jordan_sym_blocked(A, bk=64, tile=128):
+    """The symmetric form of gauss_jordan_blocked that k_coarse.cu runs
+    (k_gj_pivot, k_gj_panel_sym, k_gj_update on the tiles on and above the
+    diagonal, k_gj_mirror), in numpy. Sweeping pivot blocks of a symmetric
+    matrix keeps it sign-symmetric: M_ba = -M_ab when exactly one of a, b lies
+    in a block already swept, M_ba = M_ab otherwise (the inverse, all blocks
+    swept, is symmetric). So only the entries of tiles (I, J), I <= J (tile
+    side `tile`, a multiple of bk), are kept; for block k (rows k0..k1):
+
+      P  = A_kk^-1                   (the diagonal tile holds every entry)
+      W  = the true block row M_k*:  A[k, j] where tile(j) >= tile(k0),
+                                     -A[j, k] where tile(j) < tile(k0)
+      R  = P W, with P in R's block-k columns
+      Ct = s W, s_j = -1 for j < k0  (the true block column, transposed)
+      kept entries (i, j): rows of block k take R, the others
+                           [j outside block k] A_ij - (Ct_*i . R_*j)
+
+    and at the end every entry below the diagonal is the transpose of the one
+    above (inside the diagonal tiles too, where both halves were kept and
+    round apart): the inverse is exactly symmetric. Returns it (a new array)."""
+    A = np.array(A, dtype=np.float64, copy=True)
+    nc = A.shape[0]
+    tid = np.arange(nc) // tile
+    kept = tid[:, None] <= tid[None, :]
+    A[~kept] = np.nan  # never read
+    for k0 in range(0, nc, bk):
+        k1 = min(nc, k0 + bk)
+        tk = k0 // tile
+        P = np.linalg.inv(A[k0:k1, k0:k1])
+        W = np.where((tid >= tk)[None, :], A[k0:k1, :], -A[:, k0:k1].T)
+        Ct = W * np.where(np.arange(nc) < k0, -1.0, 1.0)[None, :]
+        R = P @ W
+        R[:, k0:k1] = P
+        outside = np.ones(nc, bool)
+        outside[k0:k1] = False
+        new = np.where(outside[None, :], A, 0.0) - Ct.T @ R
+        new[k0:k1, :] = R
+        A = np.where(kept, new, A)
+    low = np.tril(np.ones((nc, nc), bool), -1)
+    A[low] = A.T[low]
     return A
 
 

@@ -66,10 +66,18 @@ struct CoarseState {
   DBuf<double> slots;      // [n][8][15]
   DBuf<double> A;          // nc x nc, the inverse after coarse_build
   DBuf<double> P, R, C;    // Gauss-Jordan work: pivot inverse, row panel, column panel (transposed)
+  DBuf<double> D;          // the next pivot block, updated ahead of the trailing update
+  cudaStream_t aux = nullptr;  // the next pivot's inverse, beside the trailing update
+  cudaEvent_t e_diag = nullptr, e_piv = nullptr;
   DBuf<double> rc, zc;
   DBuf<int> status;
   DBuf<double> center, T;   // rigid modes: aggregate centers [4 nagg], orthonormalising transforms [36 nagg]
   DBuf<double> probe, kprobe, pdth;  // rigid modes: 6 probes, their tangent images [18n], scratch [6n]
+  ~CoarseState() {
+    if (e_diag) cudaEventDestroy(e_diag);
+    if (e_piv) cudaEventDestroy(e_piv);
+    if (aux) cudaStreamDestroy(aux);
+  }
 };
 
 __device__ __forceinline__ double co_omega(int kind, double zeta, double h) {
@@ -262,18 +270,25 @@ __global__ void k_coarse_agg_of(int64_t n, const double4* __restrict__ xv, Grid 
 //   A_ij -= C_i R_j (i, j outside block k); A_kj = R_j; A_ik = -C_i P; A_kk = P
 // With P written into R's block-k columns, every row outside block k takes
 // A_ij = [j outside block k] A_ij - C_i R_j, and the rows of block k take R.
+// The matrix stays sign-symmetric under these sweeps: A_ba = -A_ab when
+// exactly one of a, b lies in a block already swept, A_ba = A_ab otherwise.
+// So only the 128 x 128 tiles on and above the diagonal are updated (the
+// diagonal tiles whole); the panel reads the true block row and column from
+// where they are kept, and the entries below the diagonal are mirrored from
+// those above once every block is swept (the inverse is symmetric).
 // ---------------------------------------------------------------------------
-// P = inverse of the bk x bk diagonal block at k0 (one block of 256 threads;
-// each elimination step reads the old row and column k, then writes: two
-// barriers a step).
-__global__ void __launch_bounds__(256) k_gj_pivot(int nc, int k0, int bk, const double* __restrict__ A,
+constexpr int kUT = 128, kUK = 16;  // update tile side, k chunk of the staged panels
+// P = inverse of a bk x bk diagonal block (src, leading dimension ld; one
+// block of 256 threads; each elimination step reads the old row and column
+// k, then writes: two barriers a step).
+__global__ void __launch_bounds__(256) k_gj_pivot(const double* __restrict__ src, int ld, int bk,
                                                   double* __restrict__ P) {
   __shared__ double S[kGjB][kGjB + 1];
   constexpr int kPer = kGjB * kGjB / 256;
   static_assert(kPer * 256 == kGjB * kGjB, "launched with 256 threads");
   for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
     const int r = t / kGjB, c = t % kGjB;
-    S[r][c] = (r < bk && c < bk) ? A[(size_t)(k0 + r) * nc + k0 + c] : 0.0;
+    S[r][c] = (r < bk && c < bk) ? src[(size_t)r * ld + c] : 0.0;
   }
   __syncthreads();
   for (int k = 0; k < bk; ++k) {
@@ -306,55 +321,116 @@ __global__ void __launch_bounds__(256) k_gj_pivot(int nc, int k0, int bk, const 
   for (int t = threadIdx.x; t < bk * bk; t += blockDim.x) P[t] = S[t / bk][t % bk];
 }
 
-// R[r][j] = sum_t P[r][t] A[k0+t][j] (bk x nc; P itself in the block-k
-// columns); Ct[t][i] = A[i][k0+t] (bk x nc: the old block column, transposed
-// through shared memory). Block x: 64 columns j (R) or 64 rows i (Ct, blocks
-// past the R range).
+// Row panel of block k: W = the true block row A_k* (A[k0+t][j] where column
+// j's tile is at or right of block k's, else -A[j][k0+t], transposed through
+// shared memory), R = P W with P itself in the block-k columns, and
+// Ct = s W (s_j = -1 for j < k0, the swept columns): the true old block
+// column A_*k, transposed. One block per 64 columns (which share a tile).
+constexpr size_t kPanelSmem = 2 * sizeof(double[kGjB][kGjB + 1]);  // 65 KiB: dynamic
 __global__ void __launch_bounds__(256) k_gj_panel(int nc, int k0, int bk, const double* __restrict__ A,
                                                   const double* __restrict__ P, double* __restrict__ R,
                                                   double* __restrict__ Ct) {
-  const int ntile = (nc + kGjB - 1) / kGjB;
-  __shared__ double sP[kGjB][kGjB + 1];
-  if ((int)blockIdx.x >= ntile) {  // the old block column
-    const int i0 = ((int)blockIdx.x - ntile) * kGjB;
-    for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
-      const int r = t / kGjB, c = t % kGjB;
-      sP[r][c] = (i0 + r < nc && c < bk) ? A[(size_t)(i0 + r) * nc + k0 + c] : 0.0;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
-      const int c = t / kGjB, r = t % kGjB;
-      if (c < bk && i0 + r < nc) Ct[(size_t)c * nc + i0 + r] = sP[r][c];
-    }
-    return;
-  }
+  extern __shared__ __align__(16) double psm[];
+  double(*sW)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(psm);
+  double(*sP)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(psm + kGjB * (kGjB + 1));
+  static_assert(kUT % kGjB == 0, "a block's 64 columns lie in one update tile");
   const int j0 = blockIdx.x * kGjB;
+  const bool row_kept = j0 / kUT >= k0 / kUT;
   for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
     const int r = t / kGjB, c = t % kGjB;
+    if (row_kept)
+      sW[r][c] = (r < bk && j0 + c < nc) ? A[(size_t)(k0 + r) * nc + j0 + c] : 0.0;
+    else
+      sW[c][r] = (j0 + r < nc && c < bk) ? -A[(size_t)(j0 + r) * nc + k0 + c] : 0.0;
     sP[r][c] = (r < bk && c < bk) ? P[r * bk + c] : 0.0;
   }
   __syncthreads();
   for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
-    const int r = t / kGjB, c = t % kGjB;
-    const int j = j0 + c;
+    const int r = t / kGjB, c = t % kGjB, j = j0 + c;
     if (r >= bk || j >= nc) continue;
+    const double w = sW[r][c];
+    Ct[(size_t)r * nc + j] = j < k0 ? -w : w;
+    double v;
     if (j >= k0 && j < k0 + bk) {
-      R[(size_t)r * nc + j] = sP[r][j - k0];
-      continue;
+      v = sP[r][j - k0];
+    } else {
+      v = 0.0;
+      for (int k = 0; k < bk; ++k) v = fma(sP[r][k], sW[k][c], v);
     }
-    const double* a = A + (size_t)k0 * nc + j;
-    double s = 0.0;
-    for (int k = 0; k < bk; ++k) s = fma(sP[r][k], a[(size_t)k * nc], s);
-    R[(size_t)r * nc + j] = s;
+    R[(size_t)r * nc + j] = v;
   }
 }
 
-// Trailing update on 128x128 tiles, 8x8 per thread (rows ty + 16a, columns
-// tx + 16b), one block per SM. The block's A tile goes to shared memory by
-// cp.async at the start (read back for the final A - C R), and the two bk x nc
-// panels come in k chunks of 16, double-buffered by cp.async, so that no load
-// latency sits between the FP64 fma chains. Sums over t in order, one fma chain.
-constexpr int kUT = 128, kUK = 16;
+// The diagonal block of the next step (rows and columns k1..k1+bk1) as the
+// trailing update of block k will leave it, A_ij - sum_t Ct[t][i] R[t][j]
+// (sum over t in order), into D (bk1 x bk1): read before that update runs,
+// so the next pivot can run beside it. The update still writes the block in
+// place, but the next step replaces it with P before anything reads it.
+__global__ void __launch_bounds__(256) k_gj_next_diag(int nc, int k1, int bk1, int bk, const double* __restrict__ A,
+                                                      const double* __restrict__ R, const double* __restrict__ Ct,
+                                                      double* __restrict__ D) {
+  extern __shared__ __align__(16) double psm[];
+  double(*sC)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(psm);                      // sC[t][r]
+  double(*sR)[kGjB + 1] = reinterpret_cast<double(*)[kGjB + 1]>(psm + kGjB * (kGjB + 1));  // sR[t][c]
+  for (int e = threadIdx.x; e < kGjB * kGjB; e += blockDim.x) {
+    const int t = e / kGjB, x = e % kGjB;
+    const bool in = t < bk && x < bk1;
+    sC[t][x] = in ? Ct[(size_t)t * nc + k1 + x] : 0.0;
+    sR[t][x] = in ? R[(size_t)t * nc + k1 + x] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // rows ty + 16a, columns tx + 16b
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int t = 0; t < bk; ++t) {
+    double cv[4], rv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) cv[a] = sC[t][ty + 16 * a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) rv[b] = sR[t][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(cv[a], rv[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = ty + 16 * a, cc = tx + 16 * b;
+      if (r < bk1 && cc < bk1) D[r * bk1 + cc] = A[(size_t)(k1 + r) * nc + k1 + cc] - acc[a][b];
+    }
+}
+
+// Entries below the diagonal from those above, once every block is swept:
+// 64 x 64 blocks (rows bi, columns bj <= bi) transposed through shared memory.
+__global__ void __launch_bounds__(256) k_gj_mirror(int nc, double* __restrict__ A) {
+  __shared__ double sT[kGjB][kGjB + 1];
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bj > bi) return;
+  const int r0 = bi * kGjB, c0 = bj * kGjB;
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {  // sT[r][c] = A[c0 + r][r0 + c]
+    const int r = t / kGjB, c = t % kGjB;
+    sT[r][c] = (c0 + r < nc && r0 + c < nc) ? A[(size_t)(c0 + r) * nc + r0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kGjB * kGjB; t += blockDim.x) {
+    const int r = t / kGjB, c = t % kGjB, a = r0 + r, b = c0 + c;
+    if (a < nc && b < nc && a > b) A[(size_t)a * nc + b] = sT[c][r];
+  }
+}
+
+// Trailing update on the 128x128 tiles on and above the diagonal (block x =
+// the upper-triangle tile pair, row-major), 8x8 per thread (rows ty + 16a,
+// columns tx + 16b), one block per SM. The two bk x nc panels come in k
+// chunks of 16, double-buffered by cp.async, so that no load latency sits
+// between the FP64 fma chains; the block's A tile (read back for the final
+// A - C R) follows the first chunk by cp.async and is first waited for with
+// the second, so the first chunk's products overlap its load. Sums over t in
+// order, one fma chain.
 constexpr size_t kUpdSmem = (size_t)(kUT * kUT + 4 * kUK * kUT) * sizeof(double);  // 192 KiB
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
@@ -373,13 +449,12 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
   double* sA = smem;                   // [kUT][kUT]
   double* sC = smem + kUT * kUT;       // [2][kUK][kUT]
   double* sR = sC + 2 * kUK * kUT;     // [2][kUK][kUT]
-  const int i0 = blockIdx.y * kUT, j0 = blockIdx.x * kUT;
+  int bj = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);  // tile pair L = bj (bj + 1) / 2 + bi, bi <= bj
+  while ((bj + 1) * (bj + 2) / 2 <= (int)blockIdx.x) ++bj;
+  while (bj * (bj + 1) / 2 > (int)blockIdx.x) --bj;
+  const int bi = (int)blockIdx.x - bj * (bj + 1) / 2;
+  const int i0 = bi * kUT, j0 = bj * kUT;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  for (int t = threadIdx.x; t < kUT * kUT; t += blockDim.x) {  // group 0: the A tile
-    const int r = t / kUT, x = t % kUT;
-    if (i0 + r < nc && j0 + x < nc) cp_async8(sA + t, A + (size_t)(i0 + r) * nc + j0 + x);
-  }
-  cp_async_commit();
   auto stage = [&](int buf, int kc) {  // one group per chunk; zeros past the edges
 #pragma unroll
     for (int q = 0; q < kUK * kUT / 256; ++q) {
@@ -399,12 +474,20 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
   for (int a = 0; a < 8; ++a)
 #pragma unroll
     for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
-  stage(0, 0);
+  stage(0, 0);  // group 0
+  for (int t = threadIdx.x; t < kUT * kUT; t += blockDim.x) {  // group 1: the A tile
+    const int r = t / kUT, x = t % kUT;
+    if (i0 + r < nc && j0 + x < nc) cp_async8(sA + t, A + (size_t)(i0 + r) * nc + j0 + x);
+  }
+  cp_async_commit();
   int buf = 0;
   for (int kc = 0; kc < bk; kc += kUK, buf ^= 1) {
     if (kc + kUK < bk) {
       stage(buf ^ 1, kc + kUK);
-      cp_async_wait<1>();  // everything but the chunk just issued
+      if (kc == 0) cp_async_wait<2>();  // chunk 0; the A tile and chunk 1 may still land
+      else cp_async_wait<1>();          // everything but the chunk just issued
+    } else if (kc == 0) {
+      cp_async_wait<1>();  // a single chunk: the A tile may still land
     } else {
       cp_async_wait<0>();
     }
@@ -425,6 +508,8 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
     }
     __syncthreads();  // the next iteration's stage overwrites this buffer
   }
+  cp_async_wait<0>();  // the A tile
+  __syncthreads();
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     const int r = ty + 16 * a, i = i0 + r;
@@ -841,12 +926,35 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
     PD_CUDA_TRY(c, cudaMemcpyAsync(assembled, s->A.p, s->A.bytes(), cudaMemcpyDeviceToDevice, c->stream));
   const int ntile = (nc + kGjB - 1) / kGjB, nut = (nc + kUT - 1) / kUT;
   PD_CUDA_TRY(c, cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
-  for (int k0 = 0; k0 < nc; k0 += kGjB) {
-    const int bk = std::min(kGjB, nc - k0);
-    k_gj_pivot<<<1, 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p);
-    k_gj_panel<<<2 * ntile, 256, 0, c->stream>>>(nc, k0, bk, s->A.p, s->P.p, s->R.p, s->C.p);
-    k_gj_update<<<dim3(nut, nut), 256, kUpdSmem, c->stream>>>(nc, k0, bk, s->A.p, s->R.p, s->C.p);
+  PD_CUDA_TRY(c, cudaFuncSetAttribute(k_gj_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem));
+  PD_CUDA_TRY(c, cudaFuncSetAttribute(k_gj_next_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem));
+  if (!s->aux) {
+    int lo = 0, hi = 0;  // the highest priority: the pivot takes the first SM the update frees
+    PD_CUDA_TRY(c, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    PD_CUDA_TRY(c, cudaStreamCreateWithPriority(&s->aux, cudaStreamNonBlocking, hi));
+    PD_CUDA_TRY(c, cudaEventCreateWithFlags(&s->e_diag, cudaEventDisableTiming));
+    PD_CUDA_TRY(c, cudaEventCreateWithFlags(&s->e_piv, cudaEventDisableTiming));
   }
+  if (s->D.count < (size_t)kGjB * kGjB) PD_CUDA_TRY(c, s->D.alloc((size_t)kGjB * kGjB));
+  // Lookahead: after the panel of block k, the next diagonal block as the
+  // trailing update will leave it goes to D, and its inverse runs on the
+  // second stream beside that update; the next panel waits for it.
+  k_gj_pivot<<<1, 256, 0, c->stream>>>(s->A.p, nc, std::min(kGjB, nc), s->P.p);
+  for (int k0 = 0; k0 < nc; k0 += kGjB) {
+    const int bk = std::min(kGjB, nc - k0), k1 = k0 + bk;
+    if (k0 > 0) PD_CUDA_TRY(c, cudaStreamWaitEvent(c->stream, s->e_piv, 0));
+    k_gj_panel<<<ntile, 256, kPanelSmem, c->stream>>>(nc, k0, bk, s->A.p, s->P.p, s->R.p, s->C.p);
+    if (k1 < nc) {
+      const int bk1 = std::min(kGjB, nc - k1);
+      k_gj_next_diag<<<1, 256, kPanelSmem, c->stream>>>(nc, k1, bk1, bk, s->A.p, s->R.p, s->C.p, s->D.p);
+      PD_CUDA_TRY(c, cudaEventRecord(s->e_diag, c->stream));
+      PD_CUDA_TRY(c, cudaStreamWaitEvent(s->aux, s->e_diag, 0));
+      k_gj_pivot<<<1, 256, 0, s->aux>>>(s->D.p, bk1, bk1, s->P.p);
+      PD_CUDA_TRY(c, cudaEventRecord(s->e_piv, s->aux));
+    }
+    k_gj_update<<<(unsigned)(nut * (nut + 1) / 2), 256, kUpdSmem, c->stream>>>(nc, k0, bk, s->A.p, s->R.p, s->C.p);
+  }
+  k_gj_mirror<<<dim3(ntile, ntile), 256, 0, c->stream>>>(nc, s->A.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   s->have_op = true;
   return PD_OK;
