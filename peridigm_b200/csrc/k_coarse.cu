@@ -424,14 +424,15 @@ __global__ void __launch_bounds__(256) k_gj_mirror(int nc, double* __restrict__ 
 }
 
 // Trailing update on the 128x128 tiles on and above the diagonal (block x =
-// the upper-triangle tile pair, row-major), 8x8 per thread (rows ty + 16a,
-// columns tx + 16b), one block per SM. The two bk x nc panels come in k
-// chunks of 16, double-buffered by cp.async, so that no load latency sits
-// between the FP64 fma chains; the block's A tile (read back for the final
-// A - C R) follows the first chunk by cp.async and is first waited for with
-// the second, so the first chunk's products overlap its load. Sums over t in
-// order, one fma chain.
-constexpr size_t kUpdSmem = (size_t)(kUT * kUT + 4 * kUK * kUT) * sizeof(double);  // 192 KiB
+// the upper-triangle tile pair, row-major) on the FP64 tensor cores:
+// mma.sync m8n8k4 (D = A B + C in FP64), each warp a 32 x 64 region (4 x 8
+// outputs of 8 x 8), one block of 8 warps per SM. The two bk x nc panels come
+// in k chunks of 16, double-buffered by cp.async (rows padded to kUP doubles
+// so that a fragment load is two wavefronts); the block's A tile (read back
+// for the final A - C R) follows the first chunk by cp.async and is first
+// waited for with the second, so the first chunk's products overlap its load.
+constexpr int kUP = kUT + 8;  // padded panel row (doubles)
+constexpr size_t kUpdSmem = (size_t)(kUT * kUT + 4 * kUK * kUP) * sizeof(double);  // 196 KiB
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -443,24 +444,34 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// d += a b for one 8 x 8 x 4 FP64 product: a = A[lane / 4][lane % 4],
+// b = B[lane % 4][lane / 4], d = D[lane / 4][2 (lane % 4) + {0, 1}].
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, double* __restrict__ A,
                                                       const double* __restrict__ R, const double* __restrict__ Ct) {
   extern __shared__ __align__(16) double smem[];
   double* sA = smem;                   // [kUT][kUT]
-  double* sC = smem + kUT * kUT;       // [2][kUK][kUT]
-  double* sR = sC + 2 * kUK * kUT;     // [2][kUK][kUT]
+  double* sC = smem + kUT * kUT;       // [2][kUK][kUP]: Ct rows (k), tile rows i
+  double* sR = sC + 2 * kUK * kUP;     // [2][kUK][kUP]: R rows (k), tile columns j
   int bj = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);  // tile pair L = bj (bj + 1) / 2 + bi, bi <= bj
   while ((bj + 1) * (bj + 2) / 2 <= (int)blockIdx.x) ++bj;
   while (bj * (bj + 1) / 2 > (int)blockIdx.x) --bj;
   const int bi = (int)blockIdx.x - bj * (bj + 1) / 2;
   const int i0 = bi * kUT, j0 = bj * kUT;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wr = 32 * (w >> 1), wc = 64 * (w & 1);  // the warp's region: rows wr.., columns wc..
   auto stage = [&](int buf, int kc) {  // one group per chunk; zeros past the edges
 #pragma unroll
     for (int q = 0; q < kUK * kUT / 256; ++q) {
       const int t = threadIdx.x + 256 * q, k = t / kUT, x = t % kUT;
-      double* dc = sC + (buf * kUK + k) * kUT + x;
-      double* dr = sR + (buf * kUK + k) * kUT + x;
+      double* dc = sC + (buf * kUK + k) * kUP + x;
+      double* dr = sR + (buf * kUK + k) * kUP + x;
       const bool kin = kc + k < bk;
       if (kin && i0 + x < nc) cp_async8(dc, Ct + (size_t)(kc + k) * nc + i0 + x);
       else *dc = 0.0;
@@ -469,11 +480,11 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
     }
     cp_async_commit();
   };
-  double acc[8][8];
+  double acc[4][8][2];
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 8; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   stage(0, 0);  // group 0
   for (int t = threadIdx.x; t < kUT * kUT; t += blockDim.x) {  // group 1: the A tile
     const int r = t / kUT, x = t % kUT;
@@ -492,38 +503,41 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
       cp_async_wait<0>();
     }
     __syncthreads();
-    const double* cb = sC + buf * kUK * kUT;
-    const double* rb = sR + buf * kUK * kUT;
+    const double* cb = sC + buf * kUK * kUP;
+    const double* rb = sR + buf * kUK * kUP;
 #pragma unroll
-    for (int k = 0; k < kUK; ++k) {
-      double cv[8], rv[8];
+    for (int ks = 0; ks < kUK; ks += 4) {
+      double av[4], bv[8];
 #pragma unroll
-      for (int a = 0; a < 8; ++a) cv[a] = cb[k * kUT + ty + 16 * a];
+      for (int a = 0; a < 4; ++a) av[a] = cb[(ks + t4) * kUP + wr + 8 * a + g];  // A[i][k] = Ct[k][i]
 #pragma unroll
-      for (int b = 0; b < 8; ++b) rv[b] = rb[k * kUT + tx + 16 * b];
+      for (int b = 0; b < 8; ++b) bv[b] = rb[(ks + t4) * kUP + wc + 8 * b + g];  // B[k][j] = R[k][j]
 #pragma unroll
-      for (int a = 0; a < 8; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc[a][b] = fma(cv[a], rv[b], acc[a][b]);
+        for (int b = 0; b < 8; ++b) dmma(acc[a][b], av[a], bv[b]);
     }
     __syncthreads();  // the next iteration's stage overwrites this buffer
   }
   cp_async_wait<0>();  // the A tile
   __syncthreads();
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    const int r = ty + 16 * a, i = i0 + r;
+  for (int a = 0; a < 4; ++a) {
+    const int r = wr + 8 * a + g, i = i0 + r;
     if (i >= nc) continue;
     const bool rowk = i >= k0 && i < k0 + bk;
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const int x = tx + 16 * b, j = j0 + x;
-      if (j >= nc) continue;
-      double v;
-      if (rowk) v = R[(size_t)(i - k0) * nc + j];
-      else if (j >= k0 && j < k0 + bk) v = -acc[a][b];
-      else v = sA[r * kUT + x] - acc[a][b];
-      A[(size_t)i * nc + j] = v;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int x = wc + 8 * b + 2 * t4 + e, j = j0 + x;
+        if (j >= nc) continue;
+        double v;
+        if (rowk) v = R[(size_t)(i - k0) * nc + j];
+        else if (j >= k0 && j < k0 + bk) v = -acc[a][b][e];
+        else v = sA[r * kUT + x] - acc[a][b][e];
+        A[(size_t)i * nc + j] = v;
+      }
     }
   }
 }
