@@ -183,7 +183,8 @@ int check_status(pd_ctx* c) {
 // evalModel on the configuration already in st[cur]; trial damage on dmg_trial.
 // f_host (may be null): where the force density also goes on the host; *host_done
 // tells whether the evaluation copied it there.
-int eval_trial(pd_ctx* c, double* f_dev, double* f_host = nullptr, bool* host_done = nullptr) {
+int eval_trial(pd_ctx* c, double* f_dev, double* f_host = nullptr, bool* host_done = nullptr,
+               const double* y_host = nullptr) {
   PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg_trial.p, c->dmg.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
   note_damage_copy(c, c->dmg_trial.p, c->dmg.p);
   StepParams sp{};
@@ -191,6 +192,7 @@ int eval_trial(pd_ctx* c, double* f_dev, double* f_host = nullptr, bool* host_do
   sp.damage_on = c->any_damage ? 1 : 0;
   sp.f_out = f_dev;
   sp.f_host = f_host;
+  sp.y_host = y_host;
   PD_CUDA_TRY(c, launch_eval(c, sp, c->dmg_trial.p, host_done));
   c->trial_valid = true;
   return check_status(c);
@@ -256,6 +258,8 @@ int pd_destroy(pd_ctx* c) {
   coarse_release(c);
   for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
   if (c->vbeg) cudaEventDestroy(c->vbeg);
+  for (cudaEvent_t e : c->up_ev)
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : c->chunk_ev)
     if (e) cudaEventDestroy(e);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -510,11 +514,10 @@ int pd_compute_force(pd_ctx* c, const double* y, double* f_out) {
   if (!y) return fail(c, PD_ERR_ARG, "pd_compute_force: null coordinates");
   TRY(ensure_ready(c));
   const size_t bytes = 3 * (size_t)c->n * sizeof(double);
-  // y is staged through the force buffer, then f is written there
-  PD_CUDA_TRY(c, cudaMemcpyAsync(c->f.p, y, bytes, cudaMemcpyHostToDevice, c->stream));
-  PD_CUDA_TRY(c, launch_state_from_y(c, c->f.p));
+  // y is uploaded (in chunks, beside the dilatation, where the path allows)
+  // through the force buffer, then f is written there
   bool copied = false;
-  TRY(eval_trial(c, c->f.p, f_out, &copied));
+  TRY(eval_trial(c, c->f.p, f_out, &copied, y));
   if (f_out && !copied) {
     PD_CUDA_TRY(c, cudaMemcpyAsync(f_out, c->f.p, bytes, cudaMemcpyDeviceToHost, c->stream));
     PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));

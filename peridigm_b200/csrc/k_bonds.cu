@@ -291,6 +291,7 @@ int finalize_bonds(pd_ctx* c, bool sort_rows) {
   PD_CUDA_TRY(c, cudaMemsetAsync(c->dmg.p, 0, c->dmg.bytes(), c->stream));
   c->dmg_gen++;
   c->dmg_asym = false;
+  c->chunk_hi_nb = -1;  // the upload chunks' neighbor bounds follow the bond set
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->trial_valid = false;
   c->wv_done = false;

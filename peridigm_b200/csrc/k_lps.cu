@@ -566,9 +566,10 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilat
     const float* __restrict__ bx3, Rec8* __restrict__ ur, const float4* __restrict__ own, int damage_on,
     double* __restrict__ theta_out, double* __restrict__ node_damage, const int64_t* __restrict__ soff,
     uint8_t* __restrict__ dmg_csr, const double* __restrict__ hp, int influence, const float* __restrict__ scf,
-    float s_min) {
+    float s_min, int64_t i0 = 0) {
+  // owners i0 .. n-1 (a chunk starts at a multiple of 64 owners)
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t i = g / TPO;
+  const int64_t i = i0 + g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
   const bool valid = i < n;
   float th = 0.0f;
@@ -1231,9 +1232,11 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
 // ---------------------------------------------------------------------------
 // State from current coordinates y [3n]: u = y - x (FP64), then the gathered
 // copy (split: displacement record, FP64: y itself).
+// (points i0 .. n-1)
 __global__ void k_state_from_y(int64_t n, const double* __restrict__ y, const double4* __restrict__ xv,
-                               double* __restrict__ u, double4* __restrict__ st, Rec8* __restrict__ ur) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+                               double* __restrict__ u, double4* __restrict__ st, Rec8* __restrict__ ur,
+                               int64_t i0 = 0) {
+  const int64_t i = i0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 x = xv[i];
   const double y0 = y[3 * i], y1 = y[3 * i + 1], y2 = y[3 * i + 2];
@@ -1397,11 +1400,13 @@ cudaError_t launch_pack_owner(pd_ctx* c) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev) {
-  if (c->n == 0) return cudaSuccess;
+cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev, int64_t i0, int64_t i1) {
+  if (i1 < 0) i1 = c->n;
+  if (i1 <= i0) return cudaSuccess;
   const bool split = c->precision == PD_SPLIT_FP32;
-  k_state_from_y<<<grid1(c->n), kBlock, 0, c->stream>>>(c->n, y_dev, c->xv.p, c->u.p, split ? nullptr : c->st[c->cur].p,
-                                                        split ? c->ur[c->cur].p : nullptr);
+  k_state_from_y<<<grid1(i1 - i0), kBlock, 0, c->stream>>>(i1, y_dev, c->xv.p, c->u.p,
+                                                           split ? nullptr : c->st[c->cur].p,
+                                                           split ? c->ur[c->cur].p : nullptr, i0);
   return cudaGetLastError();
 }
 
@@ -1473,6 +1478,44 @@ static cudaError_t ensure_copy_stream(pd_ctx* c) {
   if (c->copy_stream) return cudaSuccess;
   TRY_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
   for (int k = 0; k <= kHostChunks; ++k) TRY_CUDA(cudaEventCreateWithFlags(&c->chunk_ev[k], cudaEventDisableTiming));
+  for (int k = 0; k < kHostChunks; ++k) TRY_CUDA(cudaEventCreateWithFlags(&c->up_ev[k], cudaEventDisableTiming));
+  return cudaSuccess;
+}
+
+// Points per host-transfer chunk (a multiple of 64: whole slices of the
+// sliced stream).
+static int64_t host_chunk(int64_t n) { return ((n + kHostChunks - 1) / kHostChunks + 63) / 64 * 64; }
+
+// hi[k] = the largest neighbor index of the rows of chunk k (one block per chunk).
+__global__ void __launch_bounds__(256) k_chunk_hi(int64_t n, int64_t per, const int64_t* __restrict__ row,
+                                                  const int32_t* __restrict__ col, int64_t* __restrict__ hi) {
+  __shared__ int64_t sm[256];
+  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(n, i0 + per);
+  int64_t m = i1 > i0 ? i1 - 1 : 0;  // the chunk's own points
+  if (i1 > i0)
+    for (int64_t b = row[i0] + threadIdx.x; b < row[i1]; b += blockDim.x) m = max(m, (int64_t)col[b]);
+  sm[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sm[threadIdx.x] = max(sm[threadIdx.x], sm[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) hi[blockIdx.x] = sm[0];
+}
+
+// c->chunk_hi for the current bond set (computed once per bond set).
+static cudaError_t ensure_chunk_hi(pd_ctx* c) {
+  if (c->chunk_hi_row == c->row.p && c->chunk_hi_nb == c->nb && (int)c->chunk_hi.size() == kHostChunks)
+    return cudaSuccess;
+  const int64_t n = c->n, per = host_chunk(n);
+  DBuf<int64_t> hi;
+  TRY_CUDA(hi.alloc(kHostChunks));
+  k_chunk_hi<<<kHostChunks, 256, 0, c->stream>>>(n, per, c->row.p, c->col.p, hi.p);
+  TRY_CUDA(cudaGetLastError());
+  c->chunk_hi.assign(kHostChunks, 0);
+  TRY_CUDA(d2h(c, c->chunk_hi.data(), hi.p, kHostChunks * sizeof(int64_t)));
+  c->chunk_hi_row = c->row.p;
+  c->chunk_hi_nb = c->nb;
   return cudaSuccess;
 }
 
@@ -1533,6 +1576,14 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   const int32_t* scol = sell ? c->sell_col.p : c->col.p;
   uint8_t* sdmg = sell ? c->sell_dmg.p : dmg;
   const int64_t* soff = sell ? c->sell_off.p : nullptr;
+  // host coordinates: chunked beside the dilatation on the sliced split path
+  // (LPS and linear LPS), else one upload before the passes
+  const bool chunk_in = sp.y_host && sp.f_out && sell && c->material_model != PD_MATERIAL_BOND_BASED;
+  if (sp.y_host && !chunk_in) {
+    TRY_CUDA(cudaMemcpyAsync(sp.f_out, sp.y_host, 3 * (size_t)c->n * sizeof(double), cudaMemcpyHostToDevice,
+                             c->stream));
+    TRY_CUDA(launch_state_from_y(c, sp.f_out));
+  }
   // half-bond damage: the two halves of a bond can differ (critical stretch
   // varying along bonds, or caller-set damage with differing halves)
   const bool pair = c->sc_pair || c->dmg_asym;
@@ -1555,9 +1606,45 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
     const bool lin = c->material_model == PD_MATERIAL_LINEAR_LPS, w = c->influence != PD_INFLUENCE_ONE;
     auto* kd = lin ? (w ? dil_split_for<true, true>(pair, tpo, sell) : dil_split_for<true, false>(pair, tpo, sell))
                    : (w ? dil_split_for<false, true>(pair, tpo, sell) : dil_split_for<false, false>(pair, tpo, sell));
-    kd<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p,
-                                             sp.damage_on, c->theta.p, c->node_damage.p, soff, sell ? dmg : nullptr,
-                                             c->hp.p, c->influence, c->scf.p, c->sc_min);
+    if (chunk_in) {
+      // The coordinates go up in chunks on the copy stream; the displacement
+      // records of a chunk are formed once it has landed, and the dilatation
+      // of chunk k runs once every chunk up to the one holding its rows'
+      // largest neighbor index has its records.
+      TRY_CUDA(ensure_copy_stream(c));
+      TRY_CUDA(ensure_chunk_hi(c));
+      // (every earlier use of the staging buffer ended with its call: the
+      // entry points synchronise both streams before they return)
+      const int64_t n = c->n, per = host_chunk(n);
+      int nk = 0;
+      for (int64_t i0 = 0; i0 < n; i0 += per, ++nk) {
+        const int64_t i1 = std::min(n, i0 + per);
+        TRY_CUDA(cudaMemcpyAsync(sp.f_out + 3 * i0, sp.y_host + 3 * i0, 3 * (i1 - i0) * sizeof(double),
+                                 cudaMemcpyHostToDevice, c->copy_stream));
+        TRY_CUDA(cudaEventRecord(c->up_ev[nk], c->copy_stream));
+      }
+      int formed = 0;  // chunks whose records are formed
+      auto form_through = [&](int k) -> cudaError_t {
+        for (; formed <= k && formed < nk; ++formed) {
+          const int64_t j0 = formed * per, j1 = std::min(n, j0 + per);
+          TRY_CUDA(cudaStreamWaitEvent(c->stream, c->up_ev[formed], 0));
+          TRY_CUDA(launch_state_from_y(c, sp.f_out, j0, j1));
+        }
+        return cudaSuccess;
+      };
+      for (int k = 0; k < nk; ++k) {
+        const int64_t i0 = k * per, i1 = std::min(n, i0 + per);
+        TRY_CUDA(form_through(std::max<int>(k, (int)(c->chunk_hi[k] / per))));
+        kd<<<grid_split(i1 - i0, tpo), kSplitBlock, 0, c->stream>>>(
+            i1, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p, sp.damage_on, c->theta.p,
+            c->node_damage.p, soff, dmg, c->hp.p, c->influence, c->scf.p, c->sc_min, i0);
+      }
+      TRY_CUDA(form_through(nk - 1));
+    } else {
+      kd<<<sgrid, kSplitBlock, 0, c->stream>>>(c->n, c->row.p, scol, sdmg, c->bx3.p, c->ur[c->cur].p, c->own.p,
+                                               sp.damage_on, c->theta.p, c->node_damage.p, soff, sell ? dmg : nullptr,
+                                               c->hp.p, c->influence, c->scf.p, c->sc_min, 0);
+    }
   } else if (c->material_model == PD_MATERIAL_LINEAR_LPS) {
     PD_DISPATCH_TPO(tpo, k_dilatation_lin_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p,
                     c->pt.p, c->sc.p, c->hp.p, c->influence, sp.damage_on, c->ab64.p, c->theta.p, c->node_damage.p,
@@ -1575,7 +1662,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       // Force in chunks of points; each chunk's force density goes to the host
       // on the copy stream while the next chunk computes.
       TRY_CUDA(ensure_copy_stream(c));
-      const int64_t n = c->n, per = ((n + kHostChunks - 1) / kHostChunks + 63) / 64 * 64;
+      const int64_t n = c->n, per = host_chunk(n);
       // (all chunks are launched before the first copy: a copy to pageable
       // memory holds the host until it is done)
       for (int64_t i0 = 0, k = 0; i0 < n; i0 += per, ++k) {

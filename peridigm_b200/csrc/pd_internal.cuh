@@ -31,9 +31,10 @@
 
 namespace pdb {
 
-// Chunks of the force pass whose force density pd_compute_force copies to the
-// host while the later chunks compute.
-constexpr int kHostChunks = 4;
+// Point chunks of pd_compute_force's host transfers: the coordinates go up in
+// chunks while the dilatation of the chunks already there computes, and the
+// force density comes down chunk by chunk while the later chunks compute.
+constexpr int kHostChunks = 8;
 
 // One 32-byte record per point, fetched with a single 256-bit load.
 struct __align__(32) Rec8 {
@@ -63,6 +64,9 @@ struct StepParams {
   // outputs
   double* f_out;    // force density [3n] (may be null)
   double* f_host = nullptr;  // host copy of f_out, overlapped with the force pass where it can be
+  // host coordinates [3n] to evaluate at, uploaded through f_out (which then
+  // receives the force density), overlapped with the dilatation where it can be
+  const double* y_host = nullptr;
 };
 
 // EVAL_ONLY: evaluation (force out) with no integration; EVAL_ADVANCE: finish
@@ -119,6 +123,12 @@ struct pd_ctx {
   // chunked force download of pd_compute_force (created on first use)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t chunk_ev[pdb::kHostChunks + 1] = {};
+  cudaEvent_t up_ev[pdb::kHostChunks] = {};  // the chunked coordinate upload
+  // per upload chunk: the largest neighbor index of its rows (the last upload
+  // chunk its dilatation reads), for the bond set of (chunk_hi_row, chunk_hi_nb)
+  std::vector<int64_t> chunk_hi;
+  const int64_t* chunk_hi_row = nullptr;
+  int64_t chunk_hi_nb = -1;
   std::string err;
 
   // points
@@ -230,7 +240,8 @@ namespace pdb {
 cudaError_t launch_weighted_volume(const pd_ctx* c);
 cudaError_t launch_pack_owner(pd_ctx* c);
 cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* host_done = nullptr);
-cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev);
+// Gathered state of points i0 .. i1-1 (i1 < 0: all) from current coordinates y_dev [3n].
+cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev, int64_t i0 = 0, int64_t i1 = -1);
 cudaError_t launch_sync_state(pd_ctx* c);
 cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out);
 // The critical-dt kernels with the block partials in caller memory: partial
