@@ -531,9 +531,12 @@ int pd_update_state(pd_ctx* c) {
   CHECK_CTX(c);
   TRY(ensure_device(c));
   if (c->trial_valid) {
-    PD_CUDA_TRY(c, cudaMemcpyAsync(c->dmg.p, c->dmg_trial.p, (size_t)c->nb, cudaMemcpyDeviceToDevice, c->stream));
-    note_damage_copy(c, c->dmg.p, c->dmg_trial.p);
-    PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    // commit by exchanging the buffers: the trial's damage becomes the
+    // committed one (the evaluation has completed: its call synchronised);
+    // the next trial starts from a copy of it. The sliced mirror's source is
+    // tracked by address, which moves with the buffer.
+    std::swap(c->dmg.p, c->dmg_trial.p);
+    std::swap(c->dmg.count, c->dmg_trial.count);
     c->trial_valid = false;
   }
   return PD_OK;

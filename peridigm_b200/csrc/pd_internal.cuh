@@ -34,7 +34,7 @@ namespace pdb {
 // Point chunks of pd_compute_force's host transfers: the coordinates go up in
 // chunks while the dilatation of the chunks already there computes, and the
 // force density comes down chunk by chunk while the later chunks compute.
-constexpr int kHostChunks = 8;
+constexpr int kHostChunks = 16;
 
 // One 32-byte record per point, fetched with a single 256-bit load.
 struct __align__(32) Rec8 {
