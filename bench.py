@@ -750,16 +750,18 @@ def main():
                          f"on {r['cores']} processes (slabs with ghost layers, reference LPS kernels compiled from "
                          f"source, block constants)"}
 
+    # the compact comparison keys first (fp64, e2e, roofline), the long QS object last
     line = {"metric": METRIC, "value": sp["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sp["ms"] / args.steps, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic",
+            "vs_baseline": None, "dtype": "split-f32 (f64 state)", "data": "synthetic", "fp64": fp64, "e2e": e2e,
+            "roofline": roofline,
             "config": {"workload": workload_name(args.workload), "points": n, "bonds": nb, "horizon_over_h": 3.015,
                        "dt": dt, "precision": "split_fp32", "device_gb_in_use": round(sp["device_gb"], 1),
                        "l2": "inputs larger than L2 (%.1f GB of algorithmic bytes per step vs 126 MB L2)"
                              % (step_bytes / 1e9),
                        "parallelism": "one GPU"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": sp["clocks"],
-            "gpu_launches": 2 * args.steps, "notched_plate": extra, "qs": qs, "fp64": fp64}
+            "cpu_baseline": cpu, "clocks": sp["clocks"], "gpu_launches": 2 * args.steps, "notched_plate": extra,
+            "qs": qs}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg is not None:
