@@ -186,7 +186,10 @@ int pd_weighted_volume(pd_ctx* ctx, double* m_out);
  * computeDilatation + computeInternalForceLinearElastic). y = current
  * coordinates [3n] (host). Damage is trial damage (NP1) on top of the
  * committed state (N); pd_update_state commits it. force_density_out [3n]
- * may be NULL. */
+ * may be NULL. On the split path the coordinates go up in point chunks
+ * beside the dilatation pass and the force density comes down in chunks
+ * beside the force pass (page-locked host buffers let the copies run
+ * asynchronously; pageable ones work but serialise them). */
 int pd_compute_force(pd_ctx* ctx, const double* y, double* force_density_out);
 /* Same with device pointers. */
 int pd_compute_force_device(pd_ctx* ctx, const double* y_dev, double* force_density_dev);
