@@ -27,7 +27,7 @@ def test_blocked_gauss_jordan_inverts(n, bk):
 
 
 @pytest.mark.parametrize("n,bk,tile", [(40, 64, 128), (128, 64, 128), (300, 64, 128), (375, 64, 128),
-                                       (97, 16, 32), (200, 16, 64)])
+                                       (97, 16, 32), (200, 16, 64), (300, 128, 128), (401, 128, 128)])
 def test_symmetric_gauss_jordan_inverts(n, bk, tile):
     A = _spd(n, n + bk + tile)
     Ai = O.gauss_jordan_sym_blocked(A, bk=bk, tile=tile)
