@@ -1486,21 +1486,31 @@ static cudaError_t ensure_copy_stream(pd_ctx* c) {
 // sliced stream).
 static int64_t host_chunk(int64_t n) { return ((n + kHostChunks - 1) / kHostChunks + 63) / 64 * 64; }
 
-// hi[k] = the largest neighbor index of the rows of chunk k (one block per chunk).
+// hi[k] = the largest neighbor index of the rows of chunk k (at least the
+// chunk's last point): a thread per point, then per chunk that the block's
+// 256 points reach (chunks are multiples of 64 points: at most four) a block
+// maximum and one atomicMax. hi must start at 0.
 __global__ void __launch_bounds__(256) k_chunk_hi(int64_t n, int64_t per, const int64_t* __restrict__ row,
-                                                  const int32_t* __restrict__ col, int64_t* __restrict__ hi) {
-  __shared__ int64_t sm[256];
-  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(n, i0 + per);
-  int64_t m = i1 > i0 ? i1 - 1 : 0;  // the chunk's own points
-  if (i1 > i0)
-    for (int64_t b = row[i0] + threadIdx.x; b < row[i1]; b += blockDim.x) m = max(m, (int64_t)col[b]);
-  sm[threadIdx.x] = m;
-  __syncthreads();
-  for (int o = 128; o > 0; o >>= 1) {
-    if ((int)threadIdx.x < o) sm[threadIdx.x] = max(sm[threadIdx.x], sm[threadIdx.x + o]);
+                                                  const int32_t* __restrict__ col, unsigned long long* __restrict__ hi) {
+  __shared__ unsigned long long sm[256];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t first = (int64_t)blockIdx.x * blockDim.x;
+  unsigned long long m = 0;
+  if (i < n) {
+    m = (unsigned long long)i;
+    for (int64_t b = row[i]; b < row[i + 1]; ++b) m = max(m, (unsigned long long)col[b]);
+  }
+  const int64_t last = min(n, first + (int64_t)blockDim.x) - 1;
+  for (int64_t k = first / per; k <= last / per; ++k) {  // block-uniform
+    sm[threadIdx.x] = (i < n && i / per == k) ? m : 0ull;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o) sm[threadIdx.x] = max(sm[threadIdx.x], sm[threadIdx.x + o]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicMax(hi + k, sm[0]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) hi[blockIdx.x] = sm[0];
 }
 
 // c->chunk_hi for the current bond set (computed once per bond set).
@@ -1508,12 +1518,15 @@ static cudaError_t ensure_chunk_hi(pd_ctx* c) {
   if (c->chunk_hi_row == c->row.p && c->chunk_hi_nb == c->nb && (int)c->chunk_hi.size() == kHostChunks)
     return cudaSuccess;
   const int64_t n = c->n, per = host_chunk(n);
-  DBuf<int64_t> hi;
+  DBuf<unsigned long long> hi;
   TRY_CUDA(hi.alloc(kHostChunks));
-  k_chunk_hi<<<kHostChunks, 256, 0, c->stream>>>(n, per, c->row.p, c->col.p, hi.p);
+  TRY_CUDA(dzero(c, hi.p, kHostChunks * sizeof(unsigned long long)));
+  if (n > 0)
+    k_chunk_hi<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, per, c->row.p, c->col.p, hi.p);
   TRY_CUDA(cudaGetLastError());
-  c->chunk_hi.assign(kHostChunks, 0);
-  TRY_CUDA(d2h(c, c->chunk_hi.data(), hi.p, kHostChunks * sizeof(int64_t)));
+  std::vector<unsigned long long> h(kHostChunks, 0);
+  TRY_CUDA(d2h(c, h.data(), hi.p, kHostChunks * sizeof(unsigned long long)));
+  c->chunk_hi.assign(h.begin(), h.end());
   c->chunk_hi_row = c->row.p;
   c->chunk_hi_nb = c->nb;
   return cudaSuccess;
