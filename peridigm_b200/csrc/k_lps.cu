@@ -586,17 +586,24 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilat
     auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t, uint8_t* pdm, int r) {
       const SplitBond sb = split_bond<false>(X0, X1, X2, ui, uj);
       const bool own_ok = (d & 5) == 0;  // own half intact (and a real bond)
-      const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
       // the partner's half: its own test, or the same test on both halves
-      bool brkp = brk;
+      bool brk, brkp;
       if (PAIR) {
-        brkp = false;
-        if ((d & 6) == 0 && damage_on && sb.e > s_min * sb.zeta) {  // rare: past the body's smallest s_c
-          // the neighbor id again from the bond's stream slot (keeping the
-          // batch's ids live for this branch would cost registers)
-          const float scj = __ldg(scf + __ldg(col + (pdm - dmg)));
-          brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
+        // Every critical stretch of the body is at least s_min (products
+        // round monotonically): a bond not past s_min breaks on neither side,
+        // so both tests run only past it (rare).
+        brk = brkp = false;
+        if (damage_on && sb.e > s_min * sb.zeta) {
+          brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
+          if ((d & 6) == 0) {
+            // the neighbor id again from the bond's stream slot (keeping the
+            // batch's ids live for this branch would cost registers)
+            const float scj = __ldg(scf + __ldg(col + (pdm - dmg)));
+            brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
+          }
         }
+      } else {
+        brk = brkp = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
       }
       if (brk || brkp) {
         const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
@@ -1191,15 +1198,19 @@ __global__ void __launch_bounds__(kSplitBlock, PD_BOND_MINB) k_bb_split(int64_t 
     auto body = [&](float X0, float X1, float X2, int d, const Rec8& uj, int32_t, uint8_t* pdm, int r) {
       const SplitBond sb = split_bond<true>(X0, X1, X2, ui, uj);
       const bool own_ok = (d & 5) == 0;
-      const bool brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
       const bool part_ok = PAIR ? (d & 6) == 0 : own_ok;
-      bool brkp = brk;
-      if (PAIR) {
-        brkp = false;
-        if (part_ok && damage_on && sb.e > s_min * sb.zeta) {
-          const float scj = __ldg(scf + __ldg(col + (pdm - dmg)));
-          brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
+      bool brk, brkp;
+      if (PAIR) {  // both tests only past the body's smallest s_c (as the dilatation pass)
+        brk = brkp = false;
+        if (damage_on && sb.e > s_min * sb.zeta) {
+          brk = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
+          if (part_ok) {
+            const float scj = __ldg(scf + __ldg(col + (pdm - dmg)));
+            brkp = scj >= 0.0f && sb.e > scj * sb.zeta;
+          }
         }
+      } else {
+        brk = brkp = own_ok && s_c >= 0.0f && sb.e > s_c * sb.zeta;
       }
       if (brk || brkp) {
         const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
