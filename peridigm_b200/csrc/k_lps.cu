@@ -835,9 +835,13 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_BOND_MINB) k_forc
       // owner terms of the intact halves: t_ij with (1 - d_ij), t_ji with (1 - d_ji)
       float a, b;
       if constexpr (PAIR) {
-        const bool own_live = (d & 5) == 0, part_live = (d & 6) == 0;
-        a = (own_live ? Ai : 0.0f) + (part_live ? uj.v[6] : 0.0f);
-        b = (own_live ? Bi : 0.0f) + (part_live ? uj.v[7] : 0.0f);
+        a = Ai + uj.v[6];
+        b = Bi + uj.v[7];
+        if (d != 0) {  // a broken half or a padding slot (both intact is the common case)
+          const bool own_live = (d & 5) == 0, part_live = (d & 6) == 0;
+          a = (own_live ? Ai : 0.0f) + (part_live ? uj.v[6] : 0.0f);
+          b = (own_live ? Bi : 0.0f) + (part_live ? uj.v[7] : 0.0f);
+        }
       } else {
         a = Ai + uj.v[6];
         b = Bi + uj.v[7];
