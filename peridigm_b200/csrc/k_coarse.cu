@@ -65,6 +65,7 @@ struct CoarseState {
   DBuf<int64_t> cstart;
   DBuf<double> slots;      // [n][8][15]
   DBuf<double> A;          // nc x nc, the inverse after coarse_build
+  DBuf<float> Af;          // its FP32 copy, the one each CG iteration reads
   DBuf<double> P, R, C;    // Gauss-Jordan work: pivot inverse, row panel, column panel (transposed)
   DBuf<double> D;          // the next pivot block, updated ahead of the trailing update
   cudaStream_t aux = nullptr;  // the next pivot's inverse, beside the trailing update
@@ -543,42 +544,72 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
 }
 
 // ---------------------------------------------------------------------------
-// Application: rc = P0^T r (warp per aggregate), zc = Ac^-1 rc (warp per row),
-// z += P0 zc on free dofs
+// Application: rc = P0^T r (block per aggregate), zc = Ac^-1 rc (warp per row,
+// the FP32 copy of the inverse), z += P0 zc on free dofs
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void k_coarse_restrict(int64_t nagg, const int32_t* __restrict__ agg_cell,
-                                  const int64_t* __restrict__ cstart, const int32_t* __restrict__ sorted,
-                                  const T* __restrict__ r, double* __restrict__ rc) {
-  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (I >= nagg) return;
-  const int q = agg_cell[I];
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
-    const int64_t p = sorted[t];
-    s0 += (double)r[3 * p];
-    s1 += (double)r[3 * p + 1];
-    s2 += (double)r[3 * p + 2];
+// Block sum of kRestrictT threads' partial sums, in a fixed order (thread 0
+// gets the total): a tree over shared memory.
+constexpr int kRestrictT = 128;
+template <int K>
+__device__ __forceinline__ void block_sum(double (&acc)[K], double (*sh)[kRestrictT]) {
+  for (int k = 0; k < K; ++k) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int o = kRestrictT / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int k = 0; k < K; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+    __syncthreads();
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-  }
-  if (lane == 0) rc[3 * I] = s0, rc[3 * I + 1] = s1, rc[3 * I + 2] = s2;
+  for (int k = 0; k < K; ++k) acc[k] = sh[k][0];
 }
 
-__global__ void k_coarse_gemv(int nc, const double* __restrict__ A, const double* __restrict__ x,
-                              double* __restrict__ y) {
+// rc_I = sum of r over the free dofs of aggregate I's points (a block of
+// kRestrictT threads per aggregate: the points in flight at once, then one
+// fixed-order block sum).
+template <typename T>
+__global__ void __launch_bounds__(kRestrictT) k_coarse_restrict(int64_t nagg, const int32_t* __restrict__ agg_cell,
+                                                                const int64_t* __restrict__ cstart,
+                                                                const int32_t* __restrict__ sorted,
+                                                                const T* __restrict__ r, double* __restrict__ rc) {
+  __shared__ double sh[3][kRestrictT];
+  const int64_t I = blockIdx.x;
+  const int q = agg_cell[I];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t t = cstart[q] + threadIdx.x; t < cstart[q + 1]; t += kRestrictT) {
+    const int64_t p = sorted[t];
+    acc[0] += (double)r[3 * p];
+    acc[1] += (double)r[3 * p + 1];
+    acc[2] += (double)r[3 * p + 2];
+  }
+  block_sum<3>(acc, sh);
+  if (threadIdx.x == 0) rc[3 * I] = acc[0], rc[3 * I + 1] = acc[1], rc[3 * I + 2] = acc[2];
+}
+
+// y = A x with the FP32 copy of the inverse, FP64 products and sums (warp per
+// row, four entries per lane per load: the row's order of terms is fixed).
+__global__ void k_coarse_gemv_f(int nc, const float* __restrict__ A, const double* __restrict__ x,
+                                double* __restrict__ y) {
   const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (i >= nc) return;
-  const double* a = A + (size_t)i * nc;
+  const float* a = A + (size_t)i * nc;
   double s = 0.0;
-  for (int k = lane; k < nc; k += 32) s = fma(a[k], x[k], s);
+  const int n4 = (nc & 3) == 0 ? nc / 4 : 0;  // rows start 16-byte aligned when nc % 4 == 0
+  const float4* a4 = reinterpret_cast<const float4*>(a);
+  for (int k = lane; k < n4; k += 32) {
+    const float4 v = a4[k];
+    s = fma((double)v.x, x[4 * k], s);
+    s = fma((double)v.y, x[4 * k + 1], s);
+    s = fma((double)v.z, x[4 * k + 2], s);
+    s = fma((double)v.w, x[4 * k + 3], s);
+  }
+  for (int k = 4 * n4 + lane; k < nc; k += 32) s = fma((double)a[k], x[k], s);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if (lane == 0) y[i] = s;
+}
+
+__global__ void k_to_f32(int64_t m, const double* __restrict__ a, float* __restrict__ b) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m) b[k] = (float)a[k];
 }
 
 __global__ void k_coarse_prolong(int64_t n, const int32_t* __restrict__ agg_of, const double* __restrict__ zc,
@@ -758,27 +789,31 @@ __global__ void k_rigid_block6(int64_t nagg, int nc, Grid g, int cc, const int32
       for (int m = 0; m < 6; ++m) A[(size_t)(6 * I + k) * nc + 6 * J + m] = acc[k][m];
 }
 
+// rc_I = P0_I^T r: the orthonormalised rigid modes of aggregate I at its
+// points against r (a block of kRestrictT threads per aggregate, fixed-order
+// block sum).
 template <typename T>
-__global__ void k_rigid_restrict(int64_t nagg, const int32_t* __restrict__ agg_cell, const int64_t* __restrict__ cstart,
-                                 const int32_t* __restrict__ sorted, const double* __restrict__ center,
-                                 const double* __restrict__ Tm, const double4* __restrict__ xv,
-                                 const uint8_t* __restrict__ fixed, double inv_side, const T* __restrict__ r,
-                                 double* __restrict__ rc) {
-  const int64_t I = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (I >= nagg) return;
+__global__ void __launch_bounds__(kRestrictT) k_rigid_restrict(int64_t nagg, const int32_t* __restrict__ agg_cell,
+                                                               const int64_t* __restrict__ cstart,
+                                                               const int32_t* __restrict__ sorted,
+                                                               const double* __restrict__ center,
+                                                               const double* __restrict__ Tm,
+                                                               const double4* __restrict__ xv,
+                                                               const uint8_t* __restrict__ fixed, double inv_side,
+                                                               const T* __restrict__ r, double* __restrict__ rc) {
+  __shared__ double sh[6][kRestrictT];
+  const int64_t I = blockIdx.x;
   const int q = agg_cell[I];
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t t = cstart[q] + lane; t < cstart[q + 1]; t += 32) {
+  for (int64_t t = cstart[q] + threadIdx.x; t < cstart[q + 1]; t += kRestrictT) {
     const int64_t p = sorted[t];
     double v[3][6];
     rigid_modes(xv[p], center + 4 * I, Tm + 36 * I, inv_side, fixed[p], v);
     const double r0 = (double)r[3 * p], r1 = (double)r[3 * p + 1], r2 = (double)r[3 * p + 2];
     for (int k = 0; k < 6; ++k) acc[k] += v[0][k] * r0 + v[1][k] * r1 + v[2][k] * r2;
   }
-  for (int k = 0; k < 6; ++k)
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-  if (lane == 0)
+  block_sum<6>(acc, sh);
+  if (threadIdx.x == 0)
     for (int k = 0; k < 6; ++k) rc[6 * I + k] = acc[k];
 }
 
@@ -969,6 +1004,10 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
     k_gj_update<<<(unsigned)(nut * (nut + 1) / 2), 256, kUpdSmem, c->stream>>>(nc, k0, bk, s->A.p, s->R.p, s->C.p);
   }
   k_gj_mirror<<<dim3(ntile, ntile), 256, 0, c->stream>>>(nc, s->A.p);
+  // the FP32 copy each CG iteration's coarse product reads (half the bytes;
+  // the products and sums stay FP64)
+  if (s->Af.count < (size_t)nc * nc) PD_CUDA_TRY(c, s->Af.alloc((size_t)nc * nc));
+  k_to_f32<<<(unsigned)(((int64_t)nc * nc + 255) / 256), 256, 0, c->stream>>>((int64_t)nc * nc, s->A.p, s->Af.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   s->have_op = true;
   return PD_OK;
@@ -983,20 +1022,20 @@ static int co_apply(pd_ctx* c, const T* r, double* z, const uint8_t* fixed, doub
     return PD_ERR_STATE;
   }
   const int64_t n = c->n;
-  const unsigned gw = (unsigned)((s->nagg * 32 + 255) / 256);
+  const unsigned ga = (unsigned)s->nagg, gv = (unsigned)(((int64_t)s->nc * 32 + 255) / 256);
   if (s->modes == 6) {
     const double inv_side = 1.0 / s->g.cell;
-    k_rigid_restrict<T><<<gw, 256, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, s->center.p,
-                                                   s->T.p, c->xv.p, fixed, inv_side, r, s->rc.p);
-    k_coarse_gemv<<<(unsigned)(((int64_t)s->nc * 32 + 255) / 256), 256, 0, c->stream>>>(s->nc, s->A.p, s->rc.p,
-                                                                                        s->zc.p);
+    k_rigid_restrict<T><<<ga, kRestrictT, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p,
+                                                          s->center.p, s->T.p, c->xv.p, fixed, inv_side, r, s->rc.p);
+    k_coarse_gemv_f<<<gv, 256, 0, c->stream>>>(s->nc, s->Af.p, s->rc.p, s->zc.p);
     k_rigid_prolong<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, s->agg_of.p, s->center.p, s->T.p, c->xv.p,
                                                                         fixed, inv_side, s->zc.p, scale, z);
     PD_CUDA_TRY(c, cudaGetLastError());
     return PD_OK;
   }
-  k_coarse_restrict<T><<<gw, 256, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, r, s->rc.p);
-  k_coarse_gemv<<<(unsigned)(((int64_t)s->nc * 32 + 255) / 256), 256, 0, c->stream>>>(s->nc, s->A.p, s->rc.p, s->zc.p);
+  k_coarse_restrict<T><<<ga, kRestrictT, 0, c->stream>>>(s->nagg, s->agg_cell.p, s->cstart.p, s->sorted.p, r,
+                                                         s->rc.p);
+  k_coarse_gemv_f<<<gv, 256, 0, c->stream>>>(s->nc, s->Af.p, s->rc.p, s->zc.p);
   k_coarse_prolong<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, s->agg_of.p, s->zc.p, scale, fixed, z);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
