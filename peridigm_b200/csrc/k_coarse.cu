@@ -426,8 +426,9 @@ __global__ void __launch_bounds__(256) k_gj_mirror(int nc, double* __restrict__ 
 
 // Trailing update on the 128x128 tiles on and above the diagonal (block x =
 // the upper-triangle tile pair, row-major) on the FP64 tensor cores:
-// mma.sync m8n8k4 (D = A B + C in FP64), each warp a 32 x 64 region (4 x 8
-// outputs of 8 x 8), one block of 8 warps per SM. The two bk x nc panels come
+// mma.sync m8n8k4 (D = A B + C in FP64), each warp a 32 x 32 region (4 x 4
+// outputs of 8 x 8), one block of 16 warps per SM (16 warps cover the MMA
+// latency that 8 warps with twice the outputs each left exposed). The two bk x nc panels come
 // in k chunks of 16, double-buffered by cp.async (rows padded to kUP doubles
 // so that a fragment load is two wavefronts); the block's A tile (read back
 // for the final A - C R) follows the first chunk by cp.async and is first
@@ -453,8 +454,9 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, double* __restrict__ A,
-                                                      const double* __restrict__ R, const double* __restrict__ Ct) {
+constexpr int kUpdT = 512;
+__global__ void __launch_bounds__(kUpdT, 1) k_gj_update(int nc, int k0, int bk, double* __restrict__ A,
+                                                        const double* __restrict__ R, const double* __restrict__ Ct) {
   extern __shared__ __align__(16) double smem[];
   double* sA = smem;                   // [kUT][kUT]
   double* sC = smem + kUT * kUT;       // [2][kUK][kUP]: Ct rows (k), tile rows i
@@ -466,11 +468,11 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
   const int i0 = bi * kUT, j0 = bj * kUT;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane >> 2, t4 = lane & 3;
-  const int wr = 32 * (w >> 1), wc = 64 * (w & 1);  // the warp's region: rows wr.., columns wc..
+  const int wr = 32 * (w >> 2), wc = 32 * (w & 3);  // the warp's region: rows wr.., columns wc..
   auto stage = [&](int buf, int kc) {  // one group per chunk; zeros past the edges
 #pragma unroll
-    for (int q = 0; q < kUK * kUT / 256; ++q) {
-      const int t = threadIdx.x + 256 * q, k = t / kUT, x = t % kUT;
+    for (int q = 0; q < kUK * kUT / kUpdT; ++q) {
+      const int t = threadIdx.x + kUpdT * q, k = t / kUT, x = t % kUT;
       double* dc = sC + (buf * kUK + k) * kUP + x;
       double* dr = sR + (buf * kUK + k) * kUP + x;
       const bool kin = kc + k < bk;
@@ -481,11 +483,11 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
     }
     cp_async_commit();
   };
-  double acc[4][8][2];
+  double acc[4][4][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
   stage(0, 0);  // group 0
   for (int t = threadIdx.x; t < kUT * kUT; t += blockDim.x) {  // group 1: the A tile
     const int r = t / kUT, x = t % kUT;
@@ -508,15 +510,15 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
     const double* rb = sR + buf * kUK * kUP;
 #pragma unroll
     for (int ks = 0; ks < kUK; ks += 4) {
-      double av[4], bv[8];
+      double av[4], bv[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) av[a] = cb[(ks + t4) * kUP + wr + 8 * a + g];  // A[i][k] = Ct[k][i]
 #pragma unroll
-      for (int b = 0; b < 8; ++b) bv[b] = rb[(ks + t4) * kUP + wc + 8 * b + g];  // B[k][j] = R[k][j]
+      for (int b = 0; b < 4; ++b) bv[b] = rb[(ks + t4) * kUP + wc + 8 * b + g];  // B[k][j] = R[k][j]
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 8; ++b) dmma(acc[a][b], av[a], bv[b]);
+        for (int b = 0; b < 4; ++b) dmma(acc[a][b], av[a], bv[b]);
     }
     __syncthreads();  // the next iteration's stage overwrites this buffer
   }
@@ -528,7 +530,7 @@ __global__ void __launch_bounds__(256, 1) k_gj_update(int nc, int k0, int bk, do
     if (i >= nc) continue;
     const bool rowk = i >= k0 && i < k0 + bk;
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
+    for (int b = 0; b < 4; ++b) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         const int x = wc + 8 * b + 2 * t4 + e, j = j0 + x;
@@ -1001,7 +1003,8 @@ int coarse_build(pd_ctx* c, const double4* y, const double4* ab, const uint8_t* 
       k_gj_pivot<<<1, 256, 0, s->aux>>>(s->D.p, bk1, bk1, s->P.p);
       PD_CUDA_TRY(c, cudaEventRecord(s->e_piv, s->aux));
     }
-    k_gj_update<<<(unsigned)(nut * (nut + 1) / 2), 256, kUpdSmem, c->stream>>>(nc, k0, bk, s->A.p, s->R.p, s->C.p);
+    k_gj_update<<<(unsigned)(nut * (nut + 1) / 2), kUpdT, kUpdSmem, c->stream>>>(nc, k0, bk, s->A.p, s->R.p,
+                                                                                 s->C.p);
   }
   k_gj_mirror<<<dim3(ntile, ntile), 256, 0, c->stream>>>(nc, s->A.p);
   // the FP32 copy each CG iteration's coarse product reads (half the bytes;
