@@ -62,9 +62,16 @@ def algorithmic_bytes(nb, n, precision="split"):
     48, acceleration 24, u read+write 48, next displacement record 24, BC mask
     1 -> 193 B.
     Per step (both passes, per-point terms counted once): 34 nb + 176 n.
-    FP64 path per step: X in FP64 (24 B) instead of FP32, 58 nb + 200 n."""
+    FP64 paths per step: X in FP64 (24 B) instead of FP32, 58 nb + 200 n.
+    FP64 sliced passes: 29 B per bond and pass; per point, dilatation: row 8,
+    m/K/mu 24, s_c 8, own (y, V) 32, writes (A, B, theta) 32, theta 8, node
+    damage 8 -> 120 B; force: own (y, V) 32 and (A, B) 16, x 24, rho 8, v
+    read+write 48, acceleration 24, u read+write 48, next y 24, BC mask 1 ->
+    225 B."""
     if precision == "split":
         return {"dilatation": 17 * nb + 80 * n, "force": 17 * nb + 193 * n, "step": 34 * nb + 176 * n}
+    if precision == "fp64_sliced":
+        return {"dilatation": 29 * nb + 120 * n, "force": 29 * nb + 225 * n, "step": 58 * nb + 200 * n}
     return {"step": 58 * nb + 200 * n}
 
 
@@ -421,21 +428,23 @@ def explicit_leg(w, blocks, local, steps, warmup, precision, world, max_over_ran
                  "clocks": clk, "broken_bonds": st["broken_bonds"], "device_gb": (total_b - free_b) / 1e9}
 
 
-def kernel_roofline(ctx, dt, t0, ksteps, nb, n, hbm, peak_src, slots):
-    """Per-launch CUDA-event durations of the two split passes over ksteps
-    steps and the dominant pass's roofline on the algorithmic bytes."""
+def kernel_roofline(ctx, dt, t0, ksteps, nb, n, hbm, peak_src, slots, precision="split"):
+    """Per-launch CUDA-event durations of the two bond passes (split, or the
+    FP64 sliced passes) over ksteps steps and the dominant pass's roofline on
+    the algorithmic bytes."""
     ctx.kernel_timing(True)
     ctx.verlet_run(dt, ksteps, t0=t0)
     kt = ctx.kernel_times()
     ctx.kernel_timing(False)
     per = {"dilatation": kt["dilatation_ms"] / kt["evaluations"], "force": kt["force_ms"] / kt["evaluations"]}
-    algo = algorithmic_bytes(nb, n, "split")
+    algo = algorithmic_bytes(nb, n, precision)
     dom = max(per, key=per.get)
     achieved = algo[dom] / (per[dom] / 1e3) / 1e9
     traffic = None
-    if NCU_TRAFFIC.get("slots") and NCU_TRAFFIC.get(dom):
+    if precision == "split" and NCU_TRAFFIC.get("slots") and NCU_TRAFFIC.get(dom):
         traffic = NCU_TRAFFIC[dom] * slots / NCU_TRAFFIC["slots"]
-    return {"bound": "hbm", "kernel": f"k_{dom}_split", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    kname = f"k_{dom}_split" if precision == "split" else f"k_{dom}_f64s"
+    return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": achieved / hbm, "peak_source": peak_src, "traffic": traffic, "algorithmic_bytes": algo[dom],
             "launch_ms": per[dom], "per_kernel_ms": per, "steps_timed": ksteps,
             "per_kernel_frac": {k: algo[k] / (per[k] / 1e3) / 1e9 / hbm for k in per},
@@ -606,7 +615,7 @@ def main():
     ap.add_argument("--slabs", action="store_true", help="the slab path (the default for N > 1) also at N = 1")
     # profiling modes
     ap.add_argument("--profile", action="store_true")
-    ap.add_argument("--precision", default="split", choices=["split", "fp64", "both"])
+    ap.add_argument("--precision", default="split", choices=["split", "fp64", "fp64_sliced", "both"])
     ap.add_argument("--material", default="lps", choices=["lps", "bond_based", "linear_lps"])
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--nx", type=int, default=0)
@@ -705,13 +714,28 @@ def main():
                 "steps": k64,
                 "step_frac": algorithmic_bytes(nb, n, "fp64")["step"] / (s64["ms"] / k64 / 1e3) / 1e9 / hbm,
                 "split_step_frac": roofline["step_frac"]}
+        u64, d64 = c64.field("Displacement"), c64.field("Damage")
         if k64 == args.steps:  # same step count from rest: the two paths' states compare
-            u64, d64 = c64.field("Displacement"), c64.field("Damage")
             fp64["split_vs_fp64_after_steps"] = args.warmup + args.steps
             fp64["u_rel_l2"] = float(np.linalg.norm(u_split - u64) / max(np.linalg.norm(u64), 1e-300))
             fp64["node_damage_max_diff"] = float(np.max(np.abs(d_split - d64)))
         c64.close()
         log(f"fp64 {fp64['value']:.3e}, split/fp64 {fp64['split_over_fp64']:.2f}")
+
+        # the same FP64 formulas on the split passes' layout (sliced stream at
+        # 4 lanes per point, X streamed in FP64): the ratio on equal engineering
+        c6, s6 = explicit_leg(w, blocks, local, k64, args.warmup, "fp64_sliced", world, max_over_ranks, barrier)
+        r6 = kernel_roofline(c6, s6["dt"], s6["t_done"], min(k64, args.kernel_steps), nb, n, hbm, peak_src, slots,
+                             precision="fp64_sliced")
+        u6s, d6s = c6.field("Displacement"), c6.field("Damage")
+        c6.close()
+        fp64["sliced"] = {
+            "value": s6["value"], "split_over_fp64_sliced": sp["value"] / s6["value"], "ms_per_step": s6["ms"] / k64,
+            "step_frac": algorithmic_bytes(nb, n, "fp64")["step"] / (s6["ms"] / k64 / 1e3) / 1e9 / hbm,
+            "per_kernel_ms": r6["per_kernel_ms"], "per_kernel_frac": r6["per_kernel_frac"],
+            "u_rel_l2_vs_fp64": float(np.linalg.norm(u6s - u64) / max(np.linalg.norm(u64), 1e-300)),
+            "node_damage_max_diff_vs_fp64": float(np.max(np.abs(d6s - d64)))}
+        log(f"fp64 sliced {s6['value']:.3e}, split/fp64_sliced {fp64['sliced']['split_over_fp64_sliced']:.2f}")
 
     # ---- the notched plate (the split/FP64 comparison case) as an extra ------
     extra = None

@@ -53,6 +53,14 @@ extern "C" {
  * displacement/velocity state, weighted volume and reductions. */
 #define PD_FP64 0
 #define PD_SPLIT_FP32 1
+/* PD_FP64_SLICED: every per-bond quantity in FP64 as PD_FP64, on the split
+ * path's data layout: the sliced bond stream at 4 lanes per point with X
+ * streamed in FP64 (24 B per bond), one gathered record per neighbor, one
+ * division per bond and the owner constants folded (3/m, the c1 and alpha
+ * terms), so rounding differs from PD_FP64 in the last bits. LPS elastic with
+ * the "One" influence function; other materials and influence functions
+ * return PD_ERR_UNSUPPORTED. */
+#define PD_FP64_SLICED 2
 
 /* Influence functions (src/core/Peridigm_InfluenceFunction.hpp:69-87). */
 #define PD_INFLUENCE_ONE 0
@@ -79,7 +87,7 @@ typedef struct pd_ctx pd_ctx;
 
 typedef struct {
   int device;     /* CUDA device ordinal */
-  int precision;  /* PD_FP64 or PD_SPLIT_FP32 */
+  int precision;  /* PD_FP64, PD_SPLIT_FP32 or PD_FP64_SLICED */
   int influence;  /* PD_INFLUENCE_* */
   int threads_per_point; /* lanes cooperating on one point's bond family: 0 = auto, else 4/8/16/32 */
 } pd_config;

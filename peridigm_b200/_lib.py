@@ -24,6 +24,7 @@ PD_ERR_NOT_CONVERGED = 8
 
 PD_FP64 = 0
 PD_SPLIT_FP32 = 1
+PD_FP64_SLICED = 2
 
 FIELDS = {
     "Displacement": 0,

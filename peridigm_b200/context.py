@@ -36,7 +36,14 @@ class Context:
         self.L = _lib.load()
         cfg = _lib.Config()
         cfg.device = int(device)
-        cfg.precision = _lib.PD_SPLIT_FP32 if precision in ("split", "split_fp32", _lib.PD_SPLIT_FP32) else _lib.PD_FP64
+        names = {"fp64": _lib.PD_FP64, "split": _lib.PD_SPLIT_FP32, "split_fp32": _lib.PD_SPLIT_FP32,
+                 "fp64_sliced": _lib.PD_FP64_SLICED}
+        if precision in names:
+            cfg.precision = names[precision]
+        elif precision in names.values():
+            cfg.precision = int(precision)
+        else:
+            raise ValueError(f"precision {precision!r}: one of {sorted(names)}")
         cfg.influence = {"One": 0, "Parabolic Decay": 1, "Gaussian": 2}[influence]
         cfg.threads_per_point = int(threads_per_point)
         h = C.c_void_p()

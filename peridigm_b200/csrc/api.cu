@@ -57,6 +57,12 @@ int upload_material(pd_ctx* c) {
   PD_CUDA_TRY(c, h2d(c, c->sc.p, sc.data(), n * sizeof(double)));
   PD_CUDA_TRY(c, h2d(c, c->hp.p, hp.data(), n * sizeof(double)));
   c->sc_min = INFINITY;
+  {
+    double m = INFINITY;
+    for (int64_t i = 0; i < n; ++i)
+      if (sc[i] >= 0.0) m = std::min(m, sc[i]);
+    c->sc_gate64 = m * (1.0 - 1e-12);
+  }
   if (c->precision == PD_SPLIT_FP32) {
     PD_CUDA_TRY(c, c->own.alloc(n));
     std::vector<float> scf(n);
@@ -90,7 +96,7 @@ int alloc_state(pd_ctx* c) {
       PD_CUDA_TRY(c, dzero(c, c->st[k].p, c->st[k].bytes()));
     }
   }
-  PD_CUDA_TRY(c, c->ab64.alloc(c->precision == PD_FP64 ? n : 1));
+  PD_CUDA_TRY(c, c->ab64.alloc(c->precision != PD_SPLIT_FP32 ? n : 1));
   PD_CUDA_TRY(c, c->u.alloc(3 * n));
   PD_CUDA_TRY(c, c->v.alloc(3 * n));
   PD_CUDA_TRY(c, c->a.alloc(3 * n));
@@ -127,6 +133,10 @@ int ensure_ready(pd_ctx* c) {
   if (c->material_model == PD_MATERIAL_LINEAR_LPS && c->precision != PD_FP64 && c->tpo_split != 4)
     return fail(c, PD_ERR_UNSUPPORTED, "the split-FP32 Linear LPS passes run at 4 lanes per point (the sliced bond "
                                        "stream); use threads_per_point 0 or 4, or PD_FP64");
+  if (c->precision == PD_FP64_SLICED &&
+      (c->material_model != PD_MATERIAL_LPS || c->influence != PD_INFLUENCE_ONE))
+    return fail(c, PD_ERR_UNSUPPORTED, "PD_FP64_SLICED runs the LPS elastic material with the \"One\" influence "
+                                       "function; use PD_FP64 for other materials and influence functions");
   if (c->precision == PD_SPLIT_FP32 && c->influence != PD_INFLUENCE_ONE &&
       c->material_model != PD_MATERIAL_BOND_BASED) {
     // The split passes weight both halves of a bond, t_ij and t_ji, with the
@@ -220,7 +230,7 @@ int pd_create(const pd_config* cfg, pd_ctx** out) {
     c->influence = cfg->influence;
     if (cfg->threads_per_point) c->tpo = c->tpo_split = cfg->threads_per_point;
   }
-  if (c->precision != PD_FP64 && c->precision != PD_SPLIT_FP32) {
+  if (c->precision != PD_FP64 && c->precision != PD_SPLIT_FP32 && c->precision != PD_FP64_SLICED) {
     delete c;
     return PD_ERR_ARG;
   }

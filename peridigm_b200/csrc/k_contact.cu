@@ -298,7 +298,7 @@ int contact_prepare(pd_ctx* c, int64_t step) {
   if (!search) return PD_OK;
   const int64_t n = c->n;
   const unsigned g1 = (unsigned)((n + 255) / 256);
-  if (c->precision == PD_FP64) {
+  if (c->precision != PD_SPLIT_FP32) {
     const double4* src = step == 0 ? c->st[c->cur].p : c->st[c->cur ^ 1].p;
     k_contact_positions<<<g1, 256, 0, c->stream>>>(n, c->xv.p, nullptr, src, cs->pos.p, nullptr);
   } else if (step == 0) {
@@ -318,7 +318,7 @@ int contact_eval(pd_ctx* c) {
   if (!cs) return PD_OK;
   const int64_t n = c->n;
   const unsigned g1 = (unsigned)((n + 255) / 256);
-  const double4* st = c->precision == PD_FP64 ? c->st[c->cur].p : nullptr;
+  const double4* st = c->precision != PD_SPLIT_FP32 ? c->st[c->cur].p : nullptr;
   k_contact_positions<<<g1, 256, 0, c->stream>>>(n, c->xv.p, c->u.p, st, cs->pos.p, cs->y.p);
   k_contact_force<<<g1, 256, 0, c->stream>>>(n, cs->crow.p, cs->ccol.p, cs->y.p, c->v.p, c->xv.p, cs->kappa.p,
                                              cs->r_contact, cs->friction, c->fc.p, c->status.p);

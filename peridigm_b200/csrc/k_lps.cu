@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t*
     if (SELL) {
       const int64_t k = sell_index(soff, i, b - b0);
       int stride;
-      put_x(bx3 + sell_x_index(soff, i, b - b0, &stride), stride, X0, X1, X2);
+      if (bx3) put_x(bx3 + sell_x_index(soff, i, b - b0, &stride), stride, X0, X1, X2);
       scol[k] = j;
       sdmg[k] = dmg[b];
     } else {
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(kBlock) k_pack_bonds(int64_t n, const int64_t*
     for (int64_t r = len + lane; r < 4 * ms; r += TPO) {
       const int64_t k = sell_index(soff, i, r);
       int stride;
-      put_x(bx3 + sell_x_index(soff, i, r, &stride), stride, 1.f, 0.f, 0.f);
+      if (bx3) put_x(bx3 + sell_x_index(soff, i, r, &stride), stride, 1.f, 0.f, 0.f);
       scol[k] = (int32_t)i;
       sdmg[k] = kDummyBond;
     }
@@ -940,6 +940,241 @@ __global__ void __launch_bounds__(kBlock) k_force_fp64(int64_t n, const int64_t*
 }
 
 // ---------------------------------------------------------------------------
+// FP64 passes on the sliced bond stream (PD_FP64_SLICED): the FP64 LPS and
+// critical-stretch formulas of k_dilatation_fp64 / k_force_fp64 on the split
+// passes' layout, so that the two precisions compare on equal engineering.
+// Per lane and block of 4 bonds: one int4 of neighbor ids (loaded a block
+// ahead), one damage word and one 256-bit load per component of X (FP64
+// planes of 128 values), then one gathered st record (y, V) per bond and, in
+// the force pass, the neighbor's (A, B) from ab64. Owner constants are folded
+// (theta = 3/m * sum V|X|e; t_ij + t_ji = (A_i + A_j)|X| + (B_i + B_j) e with
+// A = theta (3K/m - alpha/3), B = alpha, elastic.cxx:99,119-120) and the force
+// divides once per bond by |Y|, so the last bits differ from PD_FP64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ldcs_f64x4(const double* p, double* o) {
+  asm("ld.global.cs.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3]) : "l"(p));
+}
+// 32-byte record of a point (read-only during the pass).
+__device__ __forceinline__ double4 ld_f64x4_nc(const double4* p) {
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ double2 ld_f64x2_nc(const double4* p) {
+  return __ldg(reinterpret_cast<const double2*>(p));
+}
+
+// Walks lane `lane` of owner i through its bonds of the sliced stream (the
+// order of sell_walk): body(X0, X1, X2, damage byte, neighbor (y, V),
+// neighbor (A, B) (zeros unless AB), the bond's damage byte in the stream,
+// row offset r - lane).
+template <bool AB, typename Body>
+__device__ __forceinline__ void sell_walk64(int64_t i, int lane, const int64_t* __restrict__ soff,
+                                            const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+                                            const double* __restrict__ bx, const double4* __restrict__ st,
+                                            const double4* __restrict__ ab, Body&& body) {
+  const int64_t s = i >> 3, so = soff[s];
+  const int G = (int)(soff[s + 1] - so), F = G >> 2;
+  const int l32 = (int)(i & 7) * 4 + lane;
+  const int4* pc = reinterpret_cast<const int4*>(col + 32 * so + 4 * l32);
+  uint32_t* pd = reinterpret_cast<uint32_t*>(dmg + 32 * so + 4 * l32);
+  const double* px = bx + 96 * so + 4 * l32;
+  int4 jn = F > 0 ? __ldcs(pc) : make_int4(0, 0, 0, 0);
+#pragma unroll 1
+  for (int b = 0; b < F; ++b, pc += 32, pd += 32, px += 384) {
+    const int jv[4] = {jn.x, jn.y, jn.z, jn.w};
+    if (b + 1 < F) jn = __ldcs(pc + 32);
+    const uint32_t dw = __ldcs(pd);
+    double X0[4], X1[4], X2[4];
+    ldcs_f64x4(px, X0);
+    ldcs_f64x4(px + 128, X1);
+    ldcs_f64x4(px + 256, X2);
+    double4 yj[4];
+    double2 aj[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      yj[k] = ld_f64x4_nc(st + jv[k]);
+      aj[k] = AB ? ld_f64x2_nc(ab + jv[k]) : make_double2(0.0, 0.0);
+    }
+    uint8_t* pb = reinterpret_cast<uint8_t*>(pd);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) body(X0[k], X1[k], X2[k], (int)((dw >> (8 * k)) & 0xffu), yj[k], aj[k], pb + k, 16 * b + 4 * k);
+  }
+  const int T = G - 4 * F;
+  if (T > 0) {  // tail groups: masked, one slot per lane per group
+    const int64_t t0 = 32 * (so + 4 * F) + l32;
+    const double* pt = bx + 96 * (so + 4 * F) + l32;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const bool in = k < T;
+      const int32_t j = in ? __ldcs(col + t0 + 32 * k) : (int32_t)i;
+      const int d = in ? (int)dmg[t0 + 32 * k] : kDummyBond;
+      const double X0 = in ? __ldcs(pt + 96 * k) : 1.0;
+      const double X1 = in ? __ldcs(pt + 96 * k + 32) : 0.0;
+      const double X2 = in ? __ldcs(pt + 96 * k + 64) : 0.0;
+      const double4 yj = ld_f64x4_nc(st + j);
+      const double2 aj = AB ? ld_f64x2_nc(ab + j) : make_double2(0.0, 0.0);
+      body(X0, X1, X2, d, yj, aj, dmg + t0 + 32 * k, 16 * F + 4 * k);
+    }
+  }
+}
+
+// Damage + dilatation. The break test is the reference's
+// rel = (|Y| - |X|)/|X| > s_c (CriticalStretchDamageModel.cpp:155-158), run
+// only for bonds with e > s_gate |X|, s_gate = s_min (1 - 1e-12) below every
+// critical stretch of the body by more than the roundings of e/|X| and
+// s_gate |X|, so that no bond the reference breaks skips it.
+template <bool PAIR>
+__global__ void __launch_bounds__(kSplitBlock, 4) k_dilatation_f64s(
+    int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
+    const double* __restrict__ bx, const double4* __restrict__ st, const double4* __restrict__ pt,
+    const double* __restrict__ sc, int damage_on, double s_gate, double4* __restrict__ ab64,
+    double* __restrict__ theta_out, double* __restrict__ node_damage, const int64_t* __restrict__ soff,
+    uint8_t* __restrict__ dmg_csr) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / 4;
+  const int lane = threadIdx.x & 3;
+  const bool valid = i < n;
+  double th = 0.0;
+  int broken = 0;
+  int len = 0;
+  if (valid) {
+    const int64_t b0 = row[i];
+    len = (int)(row[i + 1] - b0);
+    const double4 yi = ld_f64x4_nc(st + i);
+    const double s_c = damage_on ? sc[i] : -1.0;
+    uint8_t* cdm = dmg_csr + b0 + lane;  // the lane's bonds in the canonical CSR damage
+    auto body = [&](double X0, double X1, double X2, int d, const double4& yj, const double2&, uint8_t* pdm,
+                    int r) {
+      // |X|, |Y| and e in the reference's operation order: the break test
+      // sees the reference's stretch bit for bit
+      const double Yx = __dsub_rn(yj.x, yi.x), Yy = __dsub_rn(yj.y, yi.y), Yz = __dsub_rn(yj.z, yi.z);
+      const double zeta = __dsqrt_rn(sq3_rn(X0, X1, X2));
+      const double e = __dsub_rn(__dsqrt_rn(sq3_rn(Yx, Yy, Yz)), zeta);
+      const bool own_ok = (d & 5) == 0;  // own half intact (and a real bond)
+      bool brk = false, brkp = false;
+      if (damage_on && e > s_gate * zeta) {
+        const double rel = __ddiv_rn(e, zeta);
+        brk = own_ok && s_c >= 0.0 && rel > s_c;
+        if (PAIR) {
+          if ((d & 6) == 0) {
+            const double scj = __ldg(sc + __ldg(col + (pdm - dmg)));
+            brkp = scj >= 0.0 && rel > scj;
+          }
+        } else {
+          brkp = brk;
+        }
+      }
+      if (brk || brkp) {
+        const uint8_t nd = (uint8_t)(d | (brk ? 1 : 0) | (brkp ? 2 : 0));
+        *pdm = nd;
+        cdm[r] = nd;  // the CSR copy stays canonical
+      }
+      broken += ((d & 1) || brk) ? 1 : 0;
+      th = fma((own_ok && !brk) ? yj.w * zeta : 0.0, e, th);  // V_j |X| e
+    };
+    sell_walk64<false>(i, lane, soff, col, dmg, bx, st, nullptr, body);
+  }
+  th = group_sum<4>(th);
+  broken = group_sum<4>(broken);
+  if (valid && lane == 0) {
+    const double4 p = pt[i];  // (m, K, mu, rho)
+    const double theta = 3.0 * th / p.x;
+    const double alpha = 15.0 * p.z / p.x;
+    const double q = 3.0 * p.y / p.x - alpha / 3.0;
+    ab64[i] = make_double4(theta * q, alpha, theta, 0.0);
+    theta_out[i] = theta;
+    node_damage[i] = len > 0 ? (double)broken / (double)len : 0.0;
+  }
+}
+
+// Force gather + Verlet epilogue:
+//   f_i += V_j (t_ij + t_ji) Y/|Y|,  t_ij = (1 - d_ij)(A_i |X| + B_i e),  t_ji likewise with j's terms
+template <bool PAIR>
+__global__ void __launch_bounds__(kSplitBlock, 4) k_force_f64s(int64_t n, const int32_t* __restrict__ col,
+                                                               const uint8_t* __restrict__ dmg,
+                                                               const double* __restrict__ bx,
+                                                               const double4* __restrict__ st,
+                                                               const double4* __restrict__ ab64,
+                                                               const double4* __restrict__ xv,
+                                                               const double4* __restrict__ pt, EpiArgs E,
+                                                               const int64_t* __restrict__ soff) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / 4;
+  const int lane = threadIdx.x & 3;
+  const bool valid = i < n;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  if (valid) {
+    const double4 yi = ld_f64x4_nc(st + i);
+    const double2 ai = ld_f64x2_nc(ab64 + i);
+    auto body = [&](double X0, double X1, double X2, int d, const double4& yj, const double2& aj, uint8_t*, int) {
+      const double Yx = __dsub_rn(yj.x, yi.x), Yy = __dsub_rn(yj.y, yi.y), Yz = __dsub_rn(yj.z, yi.z);
+      const double zeta = __dsqrt_rn(sq3_rn(X0, X1, X2));
+      const double dY = __dsqrt_rn(sq3_rn(Yx, Yy, Yz));
+      const double e = __dsub_rn(dY, zeta);
+      double a = ai.x + aj.x, b = ai.y + aj.y;
+      if (d != 0) {  // a broken half or a padding slot (both intact is the common case)
+        const bool own_live = (d & 5) == 0, part_live = PAIR ? (d & 6) == 0 : own_live;
+        a = (own_live ? ai.x : 0.0) + (part_live ? aj.x : 0.0);
+        b = (own_live ? ai.y : 0.0) + (part_live ? aj.y : 0.0);
+      }
+      // a padding slot gathers its own owner (Y = 0): no term, and no 0/0
+      const double w = (d & kDummyBond) ? 0.0 : fma(zeta, a, e * b) * yj.w / dY;
+      fx = fma(w, Yx, fx);
+      fy = fma(w, Yy, fy);
+      fz = fma(w, Yz, fz);
+    };
+    uint8_t* dm = const_cast<uint8_t*>(dmg);  // not written by this pass
+    sell_walk64<true>(i, lane, soff, col, dm, bx, st, ab64, body);
+  }
+  fx = group_sum<4>(fx);
+  fy = group_sum<4>(fy);
+  fz = group_sum<4>(fz);
+  if (valid && lane < 3) {
+    const double f = lane == 0 ? fx : (lane == 1 ? fy : fz);
+    verlet_epilogue(E, i, lane, f, comp3(xv[i], lane), pt[i].w);
+  }
+}
+
+// FP64 X of the sliced stream (the slots and planes of k_pack_bonds<4, true>;
+// padding slots X = (1, 0, 0)).
+__global__ void __launch_bounds__(kBlock) k_pack_x64(int64_t n, const int64_t* __restrict__ row,
+                                                     const int32_t* __restrict__ col,
+                                                     const double4* __restrict__ xv, double* __restrict__ bx,
+                                                     const int64_t* __restrict__ soff) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t i = g / 4;
+  const int lane = threadIdx.x & 3;
+  if (i >= n) return;
+  const double4 xi = xv[i];
+  const int64_t b0 = row[i], len = row[i + 1] - b0, ms = soff[(i >> 3) + 1] - soff[i >> 3];
+  for (int64_t r = lane; r < 4 * ms; r += 4) {
+    double X0 = 1.0, X1 = 0.0, X2 = 0.0;
+    if (r < len) {
+      const double4 xj = xv[col[b0 + r]];
+      X0 = __dsub_rn(xj.x, xi.x);
+      X1 = __dsub_rn(xj.y, xi.y);
+      X2 = __dsub_rn(xj.z, xi.z);
+    }
+    int stride;
+    double* p = bx + sell_x_index(soff, i, r, &stride);
+    p[0] = X0;
+    p[stride] = X1;
+    p[2 * stride] = X2;
+  }
+}
+
+// Volume in slot w of both FP64 coordinate records (the state writers keep it).
+__global__ void k_st_volume(int64_t n, const double4* __restrict__ xv, double4* __restrict__ st0,
+                            double4* __restrict__ st1) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double V = xv[i].w;
+  st0[i].w = V;
+  st1[i].w = V;
+}
+
+// ---------------------------------------------------------------------------
 // Linear LPS ("Linear LPS Partial Volume" without partial volumes or improved
 // quadrature): the loops PeridigmNS::LinearLPSPVMaterial::precompute and
 // ::computeForce run (src/materials/Peridigm_LinearLPSPVMaterial.cpp:231-394),
@@ -1262,7 +1497,7 @@ __global__ void k_state_from_y(int64_t n, const double* __restrict__ y, const do
   if (ur) {
     store_u_record(ur + i, u0, u1, u2);
   } else {
-    st[i] = make_double4(y0, y1, y2, 0.0);
+    st[i] = make_double4(y0, y1, y2, x.w);
   }
 }
 
@@ -1276,7 +1511,7 @@ __global__ void k_state_from_u(int64_t n, const double* __restrict__ u, const do
   if (ur) {
     store_u_record(ur + i, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
   } else {
-    st[i] = make_double4(__dadd_rn(x.x, u[3 * i]), __dadd_rn(x.y, u[3 * i + 1]), __dadd_rn(x.z, u[3 * i + 2]), 0.0);
+    st[i] = make_double4(__dadd_rn(x.x, u[3 * i]), __dadd_rn(x.y, u[3 * i + 1]), __dadd_rn(x.z, u[3 * i + 2]), x.w);
   }
 }
 
@@ -1367,12 +1602,17 @@ cudaError_t launch_weighted_volume(const pd_ctx* c) {
 }
 
 cudaError_t launch_pack_owner(pd_ctx* c) {
-  if (c->n == 0 || c->precision != PD_SPLIT_FP32) return cudaSuccess;
+  if (c->n == 0 || c->precision == PD_FP64) return cudaSuccess;
+  const bool f64s = c->precision == PD_FP64_SLICED;
   const bool bb = c->material_model == PD_MATERIAL_BOND_BASED;
   const int64_t n = c->n;
-  k_pack_owner<<<grid1(n), kBlock, 0, c->stream>>>(n, c->pt.p, c->sc.p, c->own.p);
-  k_pack_volume<<<grid1(n), kBlock, 0, c->stream>>>(n, c->xv.p, c->ur[0].p, c->ur[1].p);
-  c->sell = c->tpo_split == 4;
+  if (f64s) {
+    k_st_volume<<<grid1(n), kBlock, 0, c->stream>>>(n, c->xv.p, c->st[0].p, c->st[1].p);
+  } else {
+    k_pack_owner<<<grid1(n), kBlock, 0, c->stream>>>(n, c->pt.p, c->sc.p, c->own.p);
+    k_pack_volume<<<grid1(n), kBlock, 0, c->stream>>>(n, c->xv.p, c->ur[0].p, c->ur[1].p);
+  }
+  c->sell = f64s || c->tpo_split == 4;
   cudaError_t e;
   if (c->sell) {  // sliced bond stream of the 4-lanes-per-point passes
     const int64_t ns = (n + 7) / 8;
@@ -1392,15 +1632,30 @@ cudaError_t launch_pack_owner(pd_ctx* c) {
         cudaSuccess)
       return e;
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
-    // slots counts 32-record groups: 32 ids and damage bytes, 96 floats of X each
+    // slots counts 32-record groups: 32 ids and damage bytes, 96 values of X each
     const size_t groups = (size_t)std::max<int64_t>(slots, 1);
     c->bx3.release();  // the old stream first: at memory scale both would not fit
-    if ((e = c->bx3.alloc(96 * groups)) != cudaSuccess) return e;
+    c->bx64.release();
+    if (f64s) {
+      if ((e = c->bx64.alloc(96 * groups)) != cudaSuccess) return e;
+    } else {
+      if ((e = c->bx3.alloc(96 * groups)) != cudaSuccess) return e;
+    }
     if ((e = c->sell_col.alloc(32 * groups)) != cudaSuccess) return e;
     if ((e = c->sell_dmg.alloc(32 * groups)) != cudaSuccess) return e;
-    k_pack_bonds<4, true><<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, c->bx3.p,
-                                                                    c->sell_off.p, c->dmg.p, c->sell_col.p,
-                                                                    c->sell_dmg.p);
+    // ids, damage and (split) FP32 X; on the FP64 sliced path no FP32 X, and
+    // k_pack_x64 writes the FP64 planes
+    if (f64s) {
+      k_pack_bonds<4, true><<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, nullptr,
+                                                                      c->sell_off.p, c->dmg.p, c->sell_col.p,
+                                                                      c->sell_dmg.p);
+      k_pack_x64<<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, c->bx64.p,
+                                                           c->sell_off.p);
+    } else {
+      k_pack_bonds<4, true><<<grid_for(n, 4), kBlock, 0, c->stream>>>(n, c->row.p, c->col.p, c->xv.p, c->bx3.p,
+                                                                      c->sell_off.p, c->dmg.p, c->sell_col.p,
+                                                                      c->sell_dmg.p);
+    }
     c->sell_src = c->dmg.p;
     c->sell_gen = c->dmg_gen;
   } else {
@@ -1595,8 +1850,9 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   E.status = c->status.p;
   // Split passes at 4 lanes per point read the sliced bond stream; its damage
   // mirror follows the CSR damage array this evaluation uses.
+  const bool f64s = c->precision == PD_FP64_SLICED;
   const bool sell = split && c->sell && tpo == 4;
-  if (sell && (c->sell_src != dmg || c->sell_gen != c->dmg_gen)) {
+  if ((sell || f64s) && (c->sell_src != dmg || c->sell_gen != c->dmg_gen)) {
     k_sell_dmg<<<grid_for(c->n, 4), kBlock, 0, c->stream>>>(c->n, c->row.p, c->sell_off.p, dmg, c->sell_dmg.p);
     c->sell_src = dmg;
     c->sell_gen = c->dmg_gen;
@@ -1616,6 +1872,21 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   // varying along bonds, or caller-set damage with differing halves)
   const bool pair = c->sc_pair || c->dmg_asym;
   const int ipair = pair ? 1 : 0;
+  if (f64s) {  // LPS only (other materials are refused when the context is made ready)
+    auto* kd = pair ? &k_dilatation_f64s<true> : &k_dilatation_f64s<false>;
+    kd<<<grid_split(c->n, 4), kSplitBlock, 0, c->stream>>>(c->n, c->row.p, c->sell_col.p, c->sell_dmg.p, c->bx64.p,
+                                                           c->st[c->cur].p, c->pt.p, c->sc.p, sp.damage_on,
+                                                           c->sc_gate64, c->ab64.p, c->theta.p, c->node_damage.p,
+                                                           c->sell_off.p, dmg);
+    TRY_CUDA(cudaGetLastError());
+    if (ev) cudaEventRecord(ev[1], c->stream);
+    auto* kf = pair ? &k_force_f64s<true> : &k_force_f64s<false>;
+    kf<<<grid_split(c->n, 4), kSplitBlock, 0, c->stream>>>(c->n, c->sell_col.p, c->sell_dmg.p, c->bx64.p,
+                                                           c->st[c->cur].p, c->ab64.p, c->xv.p, c->pt.p, E,
+                                                           c->sell_off.p);
+    if (ev) cudaEventRecord(ev[2], c->stream);
+    return cudaGetLastError();
+  }
   if (c->material_model == PD_MATERIAL_BOND_BASED) {  // one pass: damage + pair force + epilogue
     if (ev) cudaEventRecord(ev[1], c->stream);
     if (split) {
@@ -1846,7 +2117,7 @@ __global__ void k_unpack_state(int64_t n, int64_t n_idx, const int32_t* __restri
   if (ur) {
     store_u_record(ur + i, v[0], v[1], v[2]);
   } else {
-    st[i] = make_double4(v[3], v[4], v[5], 0.0);
+    st[i] = make_double4(v[3], v[4], v[5], st[i].w);
   }
 }
 

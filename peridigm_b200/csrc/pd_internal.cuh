@@ -14,9 +14,11 @@
 //                with one 256-bit load; u = u_hi + 16-bit residuals times a
 //                shared power of two q; double buffered across steps
 //   own[n]       float4 (3/m, (3K-5mu)/m, 15mu/m, s_c)  owner terms
-// FP64 path:
-//   st[2][n]     double4 (y_x, y_y, y_z, 0) current coordinates, double buffered
-//   ab64[n]      double4 (theta, 3K/m - alpha/3, alpha, 0)
+// FP64 paths:
+//   st[2][n]     double4 (y_x, y_y, y_z, V) current coordinates and volume, double buffered
+//   ab64[n]      double4 (theta, 3K/m - alpha/3, alpha, 0); on the FP64 sliced
+//                path (A, B, theta, 0) with A = theta*(3K/m - alpha/3), B = alpha
+//   bx64         X per bond in FP64 on the sliced stream (FP64 sliced path)
 // A = theta*(3K-5mu)/m and B = 15mu/m are the owner terms of the LPS force
 // state t = (1-d)[A*omega*|xi| + (1-d)*B*omega*e] (elastic.cxx:99,119-120).
 #pragma once
@@ -163,6 +165,7 @@ struct pd_ctx {
   pdb::DBuf<double4> pt;     // (m, K, mu, rho)
   pdb::DBuf<double> sc;      // critical stretch (<0: off)
   pdb::DBuf<float> bx3;      // split path: per bond X in FP32, 32-slot groups of x/y/z planes, CSR or sliced order
+  pdb::DBuf<double> bx64;    // FP64 sliced path: per bond X in FP64, the sliced order and planes of bx3
   // Sliced (SELL) bond stream of the 4-lanes-per-point split passes: slot
   // offsets per 8-owner slice, neighbor ids and a damage mirror in slice
   // order (bx3 holds the bond vectors in that order). dmg_gen counts writes to the
@@ -182,6 +185,7 @@ struct pd_ctx {
   bool sc_pair = false;
   bool dmg_asym = false;
   float sc_min = 0.0f;  // smallest critical stretch >= 0 of the points (FP32; +inf when none)
+  double sc_gate64 = 0.0;  // FP64 sliced path: the smallest s_c >= 0 times (1 - 1e-12) (+inf when none)
 
   // state
   pdb::DBuf<double4> st[2];   // FP64 path gathered coordinates
