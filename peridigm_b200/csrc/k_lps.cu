@@ -1024,8 +1024,14 @@ __device__ __forceinline__ void sell_walk64(int64_t i, int lane, const int64_t* 
 // only for bonds with e > s_gate |X|, s_gate = s_min (1 - 1e-12) below every
 // critical stretch of the body by more than the roundings of e/|X| and
 // s_gate |X|, so that no bond the reference breaks skips it.
+#ifndef PD_F64S_DIL_MINB
+#define PD_F64S_DIL_MINB 4
+#endif
+#ifndef PD_F64S_FORCE_MINB
+#define PD_F64S_FORCE_MINB 4
+#endif
 template <bool PAIR>
-__global__ void __launch_bounds__(kSplitBlock, 4) k_dilatation_f64s(
+__global__ void __launch_bounds__(kSplitBlock, PD_F64S_DIL_MINB) k_dilatation_f64s(
     int64_t n, const int64_t* __restrict__ row, const int32_t* __restrict__ col, uint8_t* __restrict__ dmg,
     const double* __restrict__ bx, const double4* __restrict__ st, const double4* __restrict__ pt,
     const double* __restrict__ sc, int damage_on, double s_gate, double4* __restrict__ ab64,
@@ -1091,7 +1097,7 @@ __global__ void __launch_bounds__(kSplitBlock, 4) k_dilatation_f64s(
 // Force gather + Verlet epilogue:
 //   f_i += V_j (t_ij + t_ji) Y/|Y|,  t_ij = (1 - d_ij)(A_i |X| + B_i e),  t_ji likewise with j's terms
 template <bool PAIR>
-__global__ void __launch_bounds__(kSplitBlock, 4) k_force_f64s(int64_t n, const int32_t* __restrict__ col,
+__global__ void __launch_bounds__(kSplitBlock, PD_F64S_FORCE_MINB) k_force_f64s(int64_t n, const int32_t* __restrict__ col,
                                                                const uint8_t* __restrict__ dmg,
                                                                const double* __restrict__ bx,
                                                                const double4* __restrict__ st,
