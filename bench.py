@@ -725,9 +725,9 @@ def main():
         # the same FP64 formulas on the split passes' layout (sliced stream at
         # 4 lanes per point, X streamed in FP64): the ratio on equal engineering
         c6, s6 = explicit_leg(w, blocks, local, k64, args.warmup, "fp64_sliced", world, max_over_ranks, barrier)
+        u6s, d6s = c6.field("Displacement"), c6.field("Damage")  # after the same steps as the FP64 leg
         r6 = kernel_roofline(c6, s6["dt"], s6["t_done"], min(k64, args.kernel_steps), nb, n, hbm, peak_src, slots,
                              precision="fp64_sliced")
-        u6s, d6s = c6.field("Displacement"), c6.field("Damage")
         c6.close()
         fp64["sliced"] = {
             "value": s6["value"], "split_over_fp64_sliced": sp["value"] / s6["value"], "ms_per_step": s6["ms"] / k64,

@@ -68,6 +68,7 @@ class Explicit(C.Structure):
         ("bc_mask", _u8p),
         ("bc_a", _dp),
         ("bc_b", _dp),
+        ("bc_vals", _dp),
         ("dt", C.c_double),
         ("t0", C.c_double),
         ("nsteps", C.c_int),
@@ -617,8 +618,10 @@ def explicit_run(prob, u, v, bond_damage=None):
 
     ``prob`` keys: x, vol, rho, K, mu, row, col, horizon, dt, nsteps; optional
     influence, s_c (enables damage), contact dict {r_search, freq, r_contact,
-    k_spring, friction, horizon}, bc_mask/bc_a/bc_b, t0, material ("lps" or
-    "bond_based") with plane/height for the bond-based constant.
+    k_spring, friction, horizon}, bc_mask/bc_a/bc_b (or bc_vals, the prescribed
+    values at t0 + k dt, k = 0..nsteps, for non-linear prescribed functions),
+    t0, material ("lps" or "bond_based") with plane/height for the bond-based
+    constant.
     """
     x = _f64(prob["x"])
     n = x.size // 3
@@ -662,6 +665,10 @@ def explicit_run(prob, u, v, bond_damage=None):
         P.bc_mask = arr(np.asarray(prob["bc_mask"], np.uint8)).ctypes.data_as(_u8p)
         P.bc_a = _d(arr(_f64(prob["bc_a"])))
         P.bc_b = _d(arr(_f64(prob["bc_b"])))
+        if prob.get("bc_vals") is not None:  # [(nsteps+1) x 3n] prescribed values at t0 + k dt
+            bv = arr(_f64(prob["bc_vals"]))
+            assert bv.size == (int(prob["nsteps"]) + 1) * 3 * n
+            P.bc_vals = _d(bv)
     P.dt = float(prob["dt"])
     P.t0 = float(prob.get("t0", 0.0))
     P.nsteps = int(prob["nsteps"])

@@ -672,9 +672,19 @@ int pdo_explicit_run(const pdo_explicit* p, double* u, double* v, double* a, dou
         if (!p->bc_mask[i]) continue;
         for (int c = 0; c < 3; ++c) {
           if (!(p->bc_mask[i] >> c & 1)) continue;
-          double cur = p->bc_a[3 * i + c] * tc + p->bc_b[3 * i + c];
-          double prev = p->bc_a[3 * i + c] * tp + p->bc_b[3 * i + c];
-          v[3 * i + c] = 0.0 * (cur - prev) + 1.0 * (cur - prev) * (1.0 / (tc - tp));
+          const size_t k = 3 * (size_t)i + c;
+          double cur, prev;
+          if (p->bc_vals) {
+            cur = p->bc_vals[(size_t)step * n3 + k];
+            prev = p->bc_vals[(size_t)(step - 1) * n3 + k];
+          } else {
+            cur = p->bc_a[k] * tc + p->bc_b[k];
+            prev = p->bc_a[k] * tp + p->bc_b[k];
+          }
+          /* a zero increment takes the previous value from the displacement
+             field (Peridigm_BoundaryCondition.cpp:137-142) */
+          if (cur - prev == 0.0) prev = u[k];
+          v[k] = 0.0 * (cur - prev) + 1.0 * (cur - prev) * (1.0 / (tc - tp));
         }
       }
     }

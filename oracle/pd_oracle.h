@@ -114,6 +114,10 @@ typedef struct {
   const uint8_t* bc_mask; /* [n] bit k: coordinate k has a prescribed displacement */
   const double* bc_a;     /* [3n] prescribed displacement u(t) = a*t + b */
   const double* bc_b;     /* [3n] */
+  /* [(nsteps+1) x 3n] or NULL: the prescribed displacement of each dof at
+   * t0 + k dt (row k), for prescribed values that are not a*t + b (an
+   * expression of x, y, z, t evaluated by the caller); replaces bc_a/bc_b */
+  const double* bc_vals;
   double dt;
   double t0;
   int nsteps;
