@@ -257,6 +257,27 @@ int pd_set_state(pd_ctx* ctx, const double* u, const double* v);
  * v_c = (u_c(t) - u_c(t_prev)) / (t - t_prev)). */
 int pd_add_prescribed_displacement(pd_ctx* ctx, int64_t n_points, const int64_t* points, int32_t coordinate,
                                    double a, double b);
+/* Prescribed displacement u_c = f(x, y, z, t) on coordinate c of the listed
+ * points, f given as the reference's "Value" string: the body its run-time
+ * compiler runs with variables x, y, z (the point's model coordinates), t and
+ * value, "value = " prepended when the string does not mention value
+ * (Peridigm_BoundaryCondition.cpp:68-84, 217-220), e.g. "0.001*y*t/1.0e-8" or
+ * "if (t <= 1) { value = -y*1.0e-6*t; } else { value = -y*1.0e-6; }".
+ * Language: numbers, + - * / % ^ (power), comparisons, && || !, if/else,
+ * assignments to new variables, and sin cos tan asin acos atan sinh cosh
+ * tanh exp log log10 sqrt abs fabs floor ceil pow atan2 fmod min max. Each
+ * explicit step evaluates f at the step's two times on the device (FP64) and
+ * sets v_c = (f(t) - f(t_prev)) / (t - t_prev) as DirichletIncrementBC does
+ * (:222-241); a zero increment takes f(t_prev) from the displacement field
+ * (:137-142). PD_ERR_ARG with the message in pd_last_error on a syntax error
+ * or an unknown name; PD_ERR_NONFINITE when a value is not finite. The
+ * quasi-static and implicit solves refuse contexts with such functions
+ * (PD_ERR_UNSUPPORTED). */
+int pd_add_prescribed_displacement_function(pd_ctx* ctx, int64_t n_points, const int64_t* points,
+                                            int32_t coordinate, const char* function);
+/* Evaluates such a function once on the host (no context, no device): for
+ * checking a "Value" string. PD_ERR_ARG when it does not compile. */
+int pd_expr_eval(const char* function, double x, double y, double z, double t, double* value);
 int pd_clear_boundary_conditions(pd_ctx* ctx);
 /* Velocity-Verlet loop of Peridigm::executeExplicit (src/core/Peridigm.cpp:1290-1593):
  * initial evaluation at t0, then nsteps steps of size dt. State stays on the

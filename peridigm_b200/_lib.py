@@ -117,6 +117,8 @@ SIGNATURES = {
     "pd_unpack_state_device": (C.c_int, [_vp, C.c_int64, _vp, _vp]),
     "pd_set_state": (C.c_int, [_vp, _dp, _dp]),
     "pd_add_prescribed_displacement": (C.c_int, [_vp, C.c_int64, _i64p, C.c_int32, C.c_double, C.c_double]),
+    "pd_add_prescribed_displacement_function": (C.c_int, [_vp, C.c_int64, _i64p, C.c_int32, C.c_char_p]),
+    "pd_expr_eval": (C.c_int, [C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_double, _dp]),
     "pd_clear_boundary_conditions": (C.c_int, [_vp]),
     "pd_verlet_run": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int64, C.POINTER(Stats)]),
     "pd_get_field": (C.c_int, [_vp, C.c_int32, _dp]),

@@ -29,6 +29,18 @@ def _f64(a, size=None, name="array"):
     return a
 
 
+def expr_eval(function, x=0.0, y=0.0, z=0.0, t=0.0):
+    """A prescribed-displacement "Value" string evaluated once on the host
+    (pd_expr_eval; no device needed): the value the explicit path prescribes
+    at model coordinates (x, y, z) and time t."""
+    L = _lib.load()
+    out = C.c_double()
+    rc = L.pd_expr_eval(function.encode(), float(x), float(y), float(z), float(t), C.byref(out))
+    if rc != 0:
+        raise PDError(rc, f"boundary-condition function {function!r} does not compile")
+    return out.value
+
+
 class Context:
     """One device-resident discretization (points, bond family, material, state)."""
 
@@ -213,6 +225,12 @@ class Context:
         p = np.ascontiguousarray(points, dtype=np.int64)
         self._ok(self.L.pd_add_prescribed_displacement(self.h, p.size, p.ctypes.data_as(_i64p), int(coordinate),
                                                        float(a), float(b)))
+
+    def prescribed_displacement_function(self, points, coordinate, function):
+        """u_c = f(x, y, z, t) from a reference "Value" string (pd_add_prescribed_displacement_function)."""
+        p = np.ascontiguousarray(points, dtype=np.int64)
+        self._ok(self.L.pd_add_prescribed_displacement_function(self.h, p.size, p.ctypes.data_as(_i64p),
+                                                                int(coordinate), function.encode()))
 
     def clear_boundary_conditions(self):
         self._ok(self.L.pd_clear_boundary_conditions(self.h))

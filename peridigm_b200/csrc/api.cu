@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "bc_expr.cuh"
 #include "pd_internal.cuh"
 
 using namespace pdb;
@@ -173,6 +174,27 @@ int ensure_ready(pd_ctx* c) {
       PD_CUDA_TRY(c, h2d(c, c->bc_a.p, c->h_bc_a.data(), 3 * n * sizeof(double)));
       PD_CUDA_TRY(c, h2d(c, c->bc_b.p, c->h_bc_b.data(), 3 * n * sizeof(double)));
     }
+    // prescribed functions: the dofs that use one and the programs
+    std::vector<int32_t> dofs, starts;
+    for (int64_t k = 0; k < 3 * n; ++k)
+      if (c->h_bc_prog[k] >= 0 && ((c->h_bc_mask[k / 3] >> (k % 3 + 3)) & 1)) {
+        dofs.push_back((int32_t)k);
+        starts.push_back((int32_t)c->h_bc_prog[k]);
+      }
+    c->n_bc_expr = (int64_t)dofs.size();
+    if (c->n_bc_expr) {
+      PD_CUDA_TRY(c, c->bc_dofs.alloc(dofs.size()));
+      PD_CUDA_TRY(c, c->bc_start.alloc(starts.size()));
+      PD_CUDA_TRY(c, c->bc_code.alloc(c->h_bc_code.size()));
+      PD_CUDA_TRY(c, c->bc_konst.alloc(std::max<size_t>(c->h_bc_konst.size(), 1)));
+      PD_CUDA_TRY(c, c->bc_cp.alloc(3 * n));
+      PD_CUDA_TRY(c, dzero(c, c->bc_cp.p, c->bc_cp.bytes()));
+      PD_CUDA_TRY(c, h2d(c, c->bc_dofs.p, dofs.data(), dofs.size() * sizeof(int32_t)));
+      PD_CUDA_TRY(c, h2d(c, c->bc_start.p, starts.data(), starts.size() * sizeof(int32_t)));
+      PD_CUDA_TRY(c, h2d(c, c->bc_code.p, c->h_bc_code.data(), c->h_bc_code.size() * sizeof(int32_t)));
+      if (!c->h_bc_konst.empty())
+        PD_CUDA_TRY(c, h2d(c, c->bc_konst.p, c->h_bc_konst.data(), c->h_bc_konst.size() * sizeof(double)));
+    }
     c->bc_dirty = false;
   }
   return PD_OK;
@@ -183,6 +205,8 @@ int check_status(pd_ctx* c) {
   PD_CUDA_TRY(c, cudaMemcpyAsync(&st, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   if (st) PD_CUDA_TRY(c, cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  // a non-finite prescribed value first: it makes the next forces non-finite too
+  if (st & ST_NONFINITE_BC) return fail(c, PD_ERR_NONFINITE, "NaN returned by dirichlet increment BC evaluation");
   if (st & ST_NONFINITE_FORCE) return fail(c, PD_ERR_NONFINITE, "NaN returned by force evaluation");
   if (st & ST_NONFINITE_CONTACT) return fail(c, PD_ERR_NONFINITE, "NaN returned by contact force evaluation");
   if (st & ST_TIMEOUT) return fail(c, PD_ERR_TIMEOUT, "a bounded device wait ran out");
@@ -317,6 +341,9 @@ int pd_set_points(pd_ctx* c, int64_t n, const double* x, const double* vol, cons
   c->h_bc_mask.assign(n, 0);
   c->h_bc_a.assign(3 * n, 0.0);
   c->h_bc_b.assign(3 * n, 0.0);
+  c->h_bc_prog.assign(3 * n, -1);
+  c->h_bc_code.clear();
+  c->h_bc_konst.clear();
   c->bc_dirty = true;
   coarse_invalidate(c);
   c->field_K.clear();
@@ -608,8 +635,31 @@ int pd_add_prescribed_displacement(pd_ctx* c, int64_t np, const int64_t* pts, in
     const int64_t i = pts[k];
     if (i < 0 || i >= c->n) return fail(c, PD_ERR_ARG, "boundary-condition point out of range");
     c->h_bc_mask[i] |= (uint8_t)(1u << coord);
+    c->h_bc_mask[i] &= (uint8_t)~(1u << (coord + 3));
     c->h_bc_a[3 * i + coord] = a;
     c->h_bc_b[3 * i + coord] = b;
+    c->h_bc_prog[3 * i + coord] = -1;
+  }
+  c->bc_dirty = true;
+  coarse_invalidate(c);
+  return PD_OK;
+}
+
+int pd_add_prescribed_displacement_function(pd_ctx* c, int64_t np, const int64_t* pts, int32_t coord,
+                                            const char* function) {
+  CHECK_CTX(c);
+  if (c->n == 0) return fail(c, PD_ERR_STATE, "points not set");
+  if (coord < 0 || coord > 2 || np < 0 || (np > 0 && !pts) || !function)
+    return fail(c, PD_ERR_ARG, "bad boundary condition");
+  for (int64_t k = 0; k < np; ++k)
+    if (pts[k] < 0 || pts[k] >= c->n) return fail(c, PD_ERR_ARG, "boundary-condition point out of range");
+  int64_t start = 0;
+  std::string err;
+  if (!expr_compile(function, c->h_bc_code, c->h_bc_konst, &start, &err)) return fail(c, PD_ERR_ARG, err);
+  for (int64_t k = 0; k < np; ++k) {
+    const int64_t i = pts[k];
+    c->h_bc_mask[i] |= (uint8_t)((1u << coord) | (1u << (coord + 3)));
+    c->h_bc_prog[3 * i + coord] = start;
   }
   c->bc_dirty = true;
   coarse_invalidate(c);
@@ -619,6 +669,9 @@ int pd_add_prescribed_displacement(pd_ctx* c, int64_t np, const int64_t* pts, in
 int pd_clear_boundary_conditions(pd_ctx* c) {
   CHECK_CTX(c);
   std::fill(c->h_bc_mask.begin(), c->h_bc_mask.end(), 0);
+  std::fill(c->h_bc_prog.begin(), c->h_bc_prog.end(), -1);
+  c->h_bc_code.clear();
+  c->h_bc_konst.clear();
   c->bc_dirty = true;
   coarse_invalidate(c);
   return PD_OK;

@@ -732,6 +732,7 @@ struct EpiArgs {
   const uint8_t* bc_mask;
   const double* bc_a;
   const double* bc_b;
+  const double2* bc_cp;  // (u(t_c), u(t_p)) of function dofs (mask bit 3 + c), or null
   double4* st_next;  // FP64 path: next coordinates
   Rec8* ur_next;     // split path: next displacement record
   int* status;
@@ -768,10 +769,20 @@ __device__ __forceinline__ double verlet_epilogue(const EpiArgs& E, int64_t i, i
     const double tc = __dadd_rn(E.t0, __dmul_rn((double)(E.step + 1), dt));
     const double tp = E.step == 0 ? E.t0 : __dadd_rn(E.t0, __dmul_rn((double)E.step, dt));
     if (tc != tp) {
-      const double cur = __dadd_rn(__dmul_rn(E.bc_a[k], tc), E.bc_b[k]);
-      const double prev = __dadd_rn(__dmul_rn(E.bc_a[k], tp), E.bc_b[k]);
-      const double d = __dsub_rn(cur, prev);
+      double cur, prev;
+      if (E.bc_cp && ((E.bc_mask[i] >> (c + 3)) & 1)) {
+        const double2 q = E.bc_cp[k];
+        cur = q.x, prev = q.y;
+      } else {
+        cur = __dadd_rn(__dmul_rn(E.bc_a[k], tc), E.bc_b[k]);
+        prev = __dadd_rn(__dmul_rn(E.bc_a[k], tp), E.bc_b[k]);
+      }
+      // a zero increment takes the previous value from the displacement
+      // field (Peridigm_BoundaryCondition.cpp:137-142)
+      double d = __dsub_rn(cur, prev);
+      if (d == 0.0) d = __dsub_rn(cur, E.u[k]);
       vh = __dadd_rn(__dmul_rn(0.0, d), __dmul_rn(__dmul_rn(1.0, d), __ddiv_rn(1.0, __dsub_rn(tc, tp))));
+      if (!isfinite(vh)) atomicOr(E.status, ST_NONFINITE_BC);
     }
   }
   E.v[k] = vh;
@@ -1851,6 +1862,9 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   E.bc_mask = c->bc_mask.p;
   E.bc_a = c->bc_a.p;
   E.bc_b = c->bc_b.p;
+  E.bc_cp = c->n_bc_expr ? c->bc_cp.p : nullptr;
+  // values of the prescribed functions at this evaluation's two times
+  if (c->n_bc_expr && sp.has_bc && sp.mode == EVAL_ADVANCE) TRY_CUDA(launch_bc_expr(c, sp.step, sp.t0, sp.dt));
   E.st_next = split ? nullptr : c->st[c->cur ^ 1].p;
   E.ur_next = split ? c->ur[c->cur ^ 1].p : nullptr;
   E.status = c->status.p;

@@ -207,6 +207,15 @@ struct pd_ctx {
   bool has_bc = false;
   pdb::DBuf<uint8_t> bc_mask;
   pdb::DBuf<double> bc_a, bc_b;
+  // prescribed functions of x, y, z, t (bc_expr.cuh): per dof the start of its
+  // program in h_bc_code (-1: a*t + b); bit 3 + c of the mask marks such dofs
+  std::vector<int64_t> h_bc_prog;
+  std::vector<int32_t> h_bc_code;
+  std::vector<double> h_bc_konst;
+  int64_t n_bc_expr = 0;              // function dofs on the device
+  pdb::DBuf<int32_t> bc_dofs, bc_start, bc_code;
+  pdb::DBuf<double> bc_konst;
+  pdb::DBuf<double2> bc_cp;           // per dof (u(t_c), u(t_p)) of the evaluation in flight
 
   // misc
   pdb::DBuf<int> status;      // device status word (non-finite etc.)
@@ -244,6 +253,8 @@ namespace pdb {
 cudaError_t launch_weighted_volume(const pd_ctx* c);
 cudaError_t launch_pack_owner(pd_ctx* c);
 cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* host_done = nullptr);
+// Values of the prescribed functions for evaluation `step` (bc_cp).
+cudaError_t launch_bc_expr(pd_ctx* c, int64_t step, double t0, double dt);
 // Gathered state of points i0 .. i1-1 (i1 < 0: all) from current coordinates y_dev [3n].
 cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev, int64_t i0 = 0, int64_t i1 = -1);
 cudaError_t launch_sync_state(pd_ctx* c);
@@ -331,7 +342,7 @@ int check_sc_pairs(pd_ctx* c);
 void qs_release(pd_ctx* c);
 
 // status bits
-enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4, ST_BAD_INDEX = 8 };
+enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4, ST_BAD_INDEX = 8, ST_NONFINITE_BC = 16 };
 
 }  // namespace pdb
 
