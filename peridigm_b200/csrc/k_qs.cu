@@ -770,11 +770,6 @@ static int qs_prepare_at(pd_ctx* c, const double* u_dev) {
     c->err = "the quasi-static solve supports the LPS material model only";
     return PD_ERR_UNSUPPORTED;
   }
-  if (c->n_bc_expr) {
-    c->err = "prescribed displacement functions of x, y, z, t run on the explicit path; give the implicit and "
-             "quasi-static solves a*t + b";
-    return PD_ERR_UNSUPPORTED;
-  }
   TRY_RC(qs_alloc(c));
   QsState* s = c->qs;
   const int64_t n = c->n;
@@ -975,6 +970,11 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   TRY_RC(ensure_ready_internal(c));
   if (c->material_model != PD_MATERIAL_LPS) {
     c->err = "the quasi-static solve supports the LPS material model only";
+    return PD_ERR_UNSUPPORTED;
+  }
+  if (c->n_bc_expr) {
+    c->err = "prescribed displacement functions of x, y, z, t run on the explicit path; give the implicit and "
+             "quasi-static solves a*t + b";
     return PD_ERR_UNSUPPORTED;
   }
   TRY_RC(qs_alloc(c));
