@@ -354,7 +354,9 @@ def qs_solve(x, vol, row, col, K, mu, horizon, bc, times, tol, max_iter=50, u0=N
     (Peridigm.cpp:2651-3043) with a dense linear solve in place of Belos CG and
     full Newton steps: per step, prescribed increments on the BC dofs, then
     Newton on the free dofs until ||r||_2 + 20||r||_inf <= tol.
-    bc: list of (dof, a, b) with u_dof(t) = a t + b. Returns u per time."""
+    bc: list of (dof, a, b) with u_dof(t) = a t + b; a zero increment takes
+    the previous value from u (Peridigm_BoundaryCondition.cpp:137-142).
+    Returns u per time."""
     n = len(vol)
     u = np.zeros(3 * n) if u0 is None else _f64(u0).copy()
     dofs = [d for d, a, b in bc]
@@ -362,7 +364,10 @@ def qs_solve(x, vol, row, col, K, mu, horizon, bc, times, tol, max_iter=50, u0=N
     for s in range(1, len(times)):
         tp, tc = times[s - 1], times[s]
         for d, a, b in bc:
-            u[d] += (a * tc + b) - (a * tp + b)
+            inc = (a * tc + b) - (a * tp + b)
+            # a zero increment takes the previous value from the displacement
+            # (Peridigm_BoundaryCondition.cpp:137-142)
+            u[d] += inc if inc != 0.0 else (a * tc + b) - u[d]
         r, nrm = qs_residual(x, u, vol, row, col, K, mu, horizon, dofs)
         it = 0
         while nrm > tol and it < max_iter:

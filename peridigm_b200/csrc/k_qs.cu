@@ -478,13 +478,17 @@ __global__ void k_qs_axpy(int64_t m, double a, const double* __restrict__ x, dou
 }
 
 __global__ void k_qs_apply_bc(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ a,
-                              const double* __restrict__ b, double tc, double tp, double* __restrict__ du) {
+                              const double* __restrict__ b, double tc, double tp, const double* __restrict__ u,
+                              double* __restrict__ du) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int c = 0; c < 3; ++c)
     if ((mask[i] >> c) & 1) {
       const int64_t k = 3 * i + c;
-      du[k] = (a[k] * tc + b[k]) - (a[k] * tp + b[k]);  // DirichletIncrementBC coeff 1 (Peridigm_BoundaryCondition.cpp:235)
+      // DirichletIncrementBC coeff 1 (Peridigm_BoundaryCondition.cpp:235); a
+      // zero increment takes the previous value from the displacement (:137-142)
+      const double cur = a[k] * tc + b[k], d = cur - (a[k] * tp + b[k]);
+      du[k] = d == 0.0 ? cur - u[k] : d;
     }
 }
 
@@ -999,14 +1003,16 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   if (o->newton_tolerance < 0.0 || !predict) {
     PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
     if (c->has_bc)
-      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, s->du.p);
+      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, c->u.p,
+                                                        s->du.p);
     TRY_RC(qs_residual(c, &l2, &linf));
     ref_metric = l2 + 20.0 * linf;
   }
   if (predict) {
     PD_CUDA_TRY(c, cudaMemcpyAsync(s->du.p, s->pred.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if (c->has_bc)
-      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, s->du.p);
+      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, c->u.p,
+                                                        s->du.p);
     TRY_RC(qs_residual(c, &l2, &linf));
   }
   double metric = l2 + 20.0 * linf;

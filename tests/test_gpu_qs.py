@@ -94,3 +94,28 @@ def test_cube_matches_oracle_and_block_jacobi_helps():
     for precond, (u, its) in res.items():
         assert np.linalg.norm(u - us[-1]) <= 1e-8 * np.linalg.norm(us[-1]), precond
     assert res["block_jacobi"][1] < res["none"][1]
+
+
+def test_constant_prescribed_displacement_is_applied():
+    """A prescribed displacement that does not change between load steps
+    (a = 0, b != 0): its zero increment takes the previous value from the
+    displacement (Peridigm_BoundaryCondition.cpp:137-142), so the first load
+    step moves the face to b, as in the oracle."""
+    w = workloads.qs_cube(n=7, h=1.0e-3, seed=3, jitter=0.05, load_steps=2)
+    for b in w["bcs"]:
+        if b["a"] != 0.0:  # the displaced face: held at a constant instead of ramped
+            b["b"], b["a"] = b["a"] * w["times"][-1], 0.0
+    assert any(b["b"] != 0.0 for b in w["bcs"])
+    with Context(precision="fp64") as ctx:
+        workloads.setup_context(ctx, w)
+        for k in range(1, len(w["times"])):
+            ctx.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=1e-6, cg_relative_tolerance=1e-10)
+        u = ctx.field("Displacement")
+        row, col = ctx.bonds_csr()
+    bc = []
+    for b in w["bcs"]:
+        bc += [(3 * int(p) + b["coordinate"], b["a"], b["b"]) for p in b["points"]]
+    us = O.qs_solve(w["x"], w["vol"], row, col, w["K"], w["mu"], w["horizon"], bc, w["times"], 1e-6)
+    moved = [d for d, a, bb in bc if bb != 0.0]
+    assert np.abs(us[1][moved] - [bb for d, a, bb in bc if bb != 0.0]).max() <= 1e-18
+    assert np.linalg.norm(u - us[-1]) <= 1e-8 * np.linalg.norm(us[-1])
