@@ -150,10 +150,8 @@ int ensure_ready(pd_ctx* c) {
                     "the split-FP32 passes support the Parabolic Decay and Gaussian influence functions only when all "
                     "blocks have one horizon; use PD_FP64 or the \"One\" influence function");
   }
-  if (!c->symmetric)
-    return fail(c, PD_ERR_UNSUPPORTED,
-                "bond families are not symmetric (j in H(i) without i in H(j)); the gather force pass needs "
-                "symmetric families");
+  if (!c->symmetric)  // (the bond set-up adds the missing reverse halves)
+    return fail(c, PD_ERR_STATE, "bond families are not symmetric after the bond set-up");
   TRY(alloc_state(c));
   if (!c->wv_done) {
     TRY(upload_material(c));
@@ -427,14 +425,14 @@ int pd_set_bonds(pd_ctx* c, const int32_t* nl, int64_t len) {
 
 int pd_num_bonds(const pd_ctx* c, int64_t* nb) {
   if (!c || !nb) return PD_ERR_ARG;
-  *nb = c->nb;
+  *nb = c->nb_user;  // the families' bonds (the device rows may also hold phantom halves)
   return PD_OK;
 }
 
 int pd_get_bonds(pd_ctx* c, int32_t* nl, int64_t cap, int64_t* len) {
   CHECK_CTX(c);
   if (!len) return fail(c, PD_ERR_ARG, "pd_get_bonds: null len");
-  *len = c->n + c->nb;
+  *len = c->n + c->nb_user;
   if (cap == 0) return PD_OK;
   if (!nl || cap < *len) return fail(c, PD_ERR_ARG, "pd_get_bonds: buffer too small");
   TRY(ensure_device(c));
@@ -443,9 +441,11 @@ int pd_get_bonds(pd_ctx* c, int32_t* nl, int64_t cap, int64_t* len) {
   PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (c->n + 1) * sizeof(int64_t)));
   if (c->nb) PD_CUDA_TRY(c, d2h(c, col.data(), c->col.p, c->nb * sizeof(int32_t)));
   int64_t k = 0;
-  for (int64_t i = 0; i < c->n; ++i) {
-    nl[k++] = (int32_t)(row[i + 1] - row[i]);
-    for (int64_t b = row[i]; b < row[i + 1]; ++b) nl[k++] = col[b];
+  for (int64_t i = 0; i < c->n; ++i) {  // the families as given or built (no phantom halves)
+    const int64_t head = k++;
+    for (int64_t b = row[i]; b < row[i + 1]; ++b)
+      if (!c->phantoms || c->h_orig[b]) nl[k++] = col[b];
+    nl[head] = (int32_t)(k - head - 1);
   }
   return PD_OK;
 }
@@ -583,9 +583,14 @@ int pd_set_bond_damage(pd_ctx* c, const double* bd) {
   CHECK_CTX(c);
   if (!bd || !c->dmg.p) return fail(c, PD_ERR_STATE, "pd_set_bond_damage: bonds not set");
   std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
-  for (int64_t b = 0; b < c->nb; ++b) {
-    if (bd[b] == 0.0) h[b] = 0;
-    else if (bd[b] == 1.0) h[b] = 1;
+  for (int64_t b = 0, u = 0; b < c->nb; ++b) {
+    if (c->phantoms && !c->h_orig[b]) {  // a phantom half: its own half does not exist
+      h[b] = (uint8_t)(1 | kPhantomOwn);
+      continue;
+    }
+    const double v = bd[u++];
+    if (v == 0.0) h[b] = 0;
+    else if (v == 1.0) h[b] = 1;
     else return fail(c, PD_ERR_UNSUPPORTED, "bond damage must be 0 or 1 (critical-stretch values)");
   }
   TRY(ensure_device(c));
@@ -728,7 +733,7 @@ int pd_verlet_run(pd_ctx* c, double dt, double t0, int64_t nsteps, pd_stats* sta
   int rc = check_status(c);
   if (stats) {
     stats->steps = nsteps;
-    stats->bonds = c->nb;
+    stats->bonds = c->nb_user;
     stats->device_ms = ms;
     TRY(count_broken(c, &stats->broken_bonds));
     stats->contact_pairs = contact_pairs(c);
@@ -815,7 +820,7 @@ int pd_verlet_finish(pd_ctx* c, pd_stats* stats) {
   const int rc = check_status(c);
   if (stats) {
     stats->steps = c->vstep;
-    stats->bonds = c->nb;
+    stats->bonds = c->nb_user;
     stats->device_ms = ms;
     TRY(count_broken(c, &stats->broken_bonds));
     stats->contact_pairs = contact_pairs(c);
@@ -1074,7 +1079,8 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
       std::vector<uint8_t> h((size_t)std::max<int64_t>(c->nb, 1));
       const uint8_t* src = c->trial_valid ? c->dmg_trial.p : c->dmg.p;
       PD_CUDA_TRY(c, d2h(c, h.data(), src, (size_t)c->nb));
-      for (int64_t b = 0; b < c->nb; ++b) out[b] = (double)(h[b] & 1);  // the row's own half
+      for (int64_t b = 0, u = 0; b < c->nb; ++b)  // the row's own half, the families' bonds only
+        if (!c->phantoms || c->h_orig[b]) out[u++] = (double)(h[b] & 1);
       return PD_OK;
     }
     case PD_FIELD_FORCE: {
@@ -1091,7 +1097,7 @@ int pd_get_field(pd_ctx* c, int32_t field, double* out) {
     case PD_FIELD_NUM_NEIGHBORS: {
       std::vector<int64_t> row(n + 1);
       PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (n + 1) * sizeof(int64_t)));
-      for (int64_t i = 0; i < n; ++i) out[i] = (double)(row[i + 1] - row[i]);
+      for (int64_t i = 0; i < n; ++i) out[i] = (double)(row[i + 1] - row[i] - (c->phantoms ? c->h_nph[i] : 0));
       return PD_OK;
     }
     default: return fail(c, PD_ERR_ARG, "pd_get_field: unknown field");

@@ -283,14 +283,104 @@ static int sort_and_check_rows(pd_ctx* c, bool sort_rows) {
   return PD_OK;
 }
 
+// Families with j in H(i) but i not in H(j): the reference builds each
+// point's family with its own block's horizon (NeighborhoodList.cxx:382-389,
+// Peridigm_HorizonManager.cpp:71-77) and scatters both halves of each of its
+// own bonds, so the force on i holds t_ij for j in H(i) and t_ji for j with i
+// in H(j). The gather passes read both halves from row i, so the missing
+// reverse (j, i) joins row j as a phantom: its own half marked absent (bit 0
+// and kPhantomOwn), and (i, j) marked without a partner half (bit 1 and
+// kPhantomPartner). Rows stay strictly ascending (merge of two ascending
+// lists); the caller's families are recorded in h_orig for the outputs.
+static int symmetrize_bonds(pd_ctx* c) {
+  const int64_t n = c->n, nb = c->nb;
+  std::vector<int64_t> row(n + 1);
+  std::vector<int32_t> col((size_t)std::max<int64_t>(nb, 1));
+  PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (n + 1) * sizeof(int64_t)));
+  if (nb) PD_CUDA_TRY(c, d2h(c, col.data(), c->col.p, nb * sizeof(int32_t)));
+  auto has = [&](int64_t i, int32_t j) {  // j in row i (ascending)
+    const int32_t* b = col.data() + row[i];
+    const int32_t* e = col.data() + row[i + 1];
+    const int32_t* p = std::lower_bound(b, e, j);
+    return p != e && *p == j;
+  };
+  std::vector<uint8_t> norev((size_t)std::max<int64_t>(nb, 1), 0);
+  std::vector<int64_t> extra(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t b = row[i]; b < row[i + 1]; ++b)
+      if (!has(col[b], (int32_t)i)) {
+        norev[b] = 1;
+        extra[col[b] + 1]++;
+      }
+  for (int64_t i = 0; i < n; ++i) extra[i + 1] += extra[i];  // phantom offsets per row
+  std::vector<int32_t> ph((size_t)std::max<int64_t>(extra[n], 1));
+  {
+    std::vector<int64_t> cur(extra.begin(), extra.end() - 1);
+    for (int64_t i = 0; i < n; ++i)  // ascending i: each row's phantoms come out ascending
+      for (int64_t b = row[i]; b < row[i + 1]; ++b)
+        if (norev[b]) ph[cur[col[b]]++] = (int32_t)i;
+  }
+  const int64_t nbs = nb + extra[n];
+  std::vector<int64_t> nrow(n + 1, 0);
+  std::vector<int32_t> ncol((size_t)std::max<int64_t>(nbs, 1));
+  c->h_orig.assign((size_t)nbs, 0);
+  c->h_dmg0.assign((size_t)nbs, 0);
+  c->h_nph.assign(n, 0);
+  int64_t k = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    nrow[i] = k;
+    int64_t a = row[i], p = extra[i];
+    const int64_t ae = row[i + 1], pe = extra[i + 1];
+    c->h_nph[i] = (int32_t)(pe - p);
+    while (a < ae || p < pe) {
+      if (p >= pe || (a < ae && col[a] < ph[p])) {
+        ncol[k] = col[a];
+        c->h_orig[k] = 1;
+        c->h_dmg0[k] = norev[a] ? (uint8_t)(2 | kPhantomPartner) : 0;
+        ++a;
+      } else {
+        ncol[k] = ph[p];
+        c->h_dmg0[k] = (uint8_t)(1 | kPhantomOwn);
+        ++p;
+      }
+      ++k;
+    }
+  }
+  nrow[n] = k;
+  c->row.release();
+  c->col.release();
+  PD_CUDA_TRY(c, c->row.alloc(n + 1));
+  PD_CUDA_TRY(c, c->col.alloc((size_t)std::max<int64_t>(nbs, 1)));
+  PD_CUDA_TRY(c, h2d(c, c->row.p, nrow.data(), (n + 1) * sizeof(int64_t)));
+  if (nbs) PD_CUDA_TRY(c, h2d(c, c->col.p, ncol.data(), nbs * sizeof(int32_t)));
+  int mx = 0;
+  for (int64_t i = 0; i < n; ++i) mx = std::max<int>(mx, (int)(nrow[i + 1] - nrow[i]));
+  c->max_row = mx;
+  c->nb_user = nb;
+  c->nb = nbs;
+  c->phantoms = true;
+  c->symmetric = true;
+  return PD_OK;
+}
+
 int finalize_bonds(pd_ctx* c, bool sort_rows) {
   int rc = sort_and_check_rows(c, sort_rows);
   if (rc != PD_OK) return rc;
+  c->phantoms = false;
+  c->nb_user = c->nb;
+  c->h_orig.clear();
+  c->h_nph.clear();
+  c->h_dmg0.clear();
+  if (!c->symmetric) {
+    rc = symmetrize_bonds(c);
+    if (rc != PD_OK) return rc;
+  }
   PD_CUDA_TRY(c, c->dmg.alloc((size_t)c->nb));
   PD_CUDA_TRY(c, c->dmg_trial.alloc((size_t)c->nb));
   PD_CUDA_TRY(c, cudaMemsetAsync(c->dmg.p, 0, c->dmg.bytes(), c->stream));
+  if (c->phantoms && c->nb) PD_CUDA_TRY(c, h2d(c, c->dmg.p, c->h_dmg0.data(), (size_t)c->nb));
   c->dmg_gen++;
-  c->dmg_asym = false;
+  c->dmg_asym = c->phantoms;  // the two halves differ along every phantom bond
   c->chunk_hi_nb = -1;  // the upload chunks' neighbor bounds follow the bond set
   PD_CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->trial_valid = false;

@@ -156,6 +156,16 @@ int compute_block_data(pd_ctx* c, int field, int block, int calc, double* out3) 
     return PD_ERR_ARG;
   }
   TRY_RC(ensure_block_ids(c));
+  DBuf<double> nn;
+  if (f.kind == 4 && c->phantoms) {  // own-family sizes (rows also hold phantom halves)
+    std::vector<int64_t> row(c->n + 1);
+    PD_CUDA_TRY(c, d2h(c, row.data(), c->row.p, (c->n + 1) * sizeof(int64_t)));
+    std::vector<double> h(std::max<int64_t>(c->n, 1));
+    for (int64_t i = 0; i < c->n; ++i) h[i] = (double)(row[i + 1] - row[i] - c->h_nph[i]);
+    PD_CUDA_TRY(c, nn.alloc(h.size()));
+    PD_CUDA_TRY(c, h2d(c, nn.p, h.data(), h.size() * sizeof(double)));
+    f.p = nn.p, f.kind = 0;
+  }
   DBuf<double> part, out;
   PD_CUDA_TRY(c, part.alloc(3 * kCGrid));
   PD_CUDA_TRY(c, out.alloc(3));

@@ -428,7 +428,10 @@ __global__ void __launch_bounds__(kBlock) k_weighted_volume(int64_t n, const int
                                                             const int32_t* __restrict__ col,
                                                             const double4* __restrict__ xv,
                                                             const double* __restrict__ hp, int influence,
-                                                            double4* __restrict__ pt) {
+                                                            double4* __restrict__ pt,
+                                                            const uint8_t* __restrict__ phantom) {
+  // phantom: the damage bytes when the device rows hold phantom halves (not
+  // in the point's own family), else null
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
   const int lane = threadIdx.x & (TPO - 1);
@@ -438,6 +441,7 @@ __global__ void __launch_bounds__(kBlock) k_weighted_volume(int64_t n, const int
     const double4 xi = xv[i];
     const double h = hp[i];
     for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
+      if (phantom && (phantom[b] & kPhantomOwn)) continue;
       const double4 xj = xv[col[b]];
       const double z2 = sq3_rn(__dsub_rn(xj.x, xi.x), __dsub_rn(xj.y, xi.y), __dsub_rn(xj.z, xi.z));
       const double om = omega_d(influence, __dsqrt_rn(z2), h);
@@ -1540,7 +1544,9 @@ __global__ void __launch_bounds__(kBlock) k_critical_dt(int64_t n, const int64_t
                                                         const int32_t* __restrict__ col,
                                                         const double4* __restrict__ xv,
                                                         const double4* __restrict__ pt,
-                                                        const double* __restrict__ hp, double* __restrict__ partial) {
+                                                        const double* __restrict__ hp, double* __restrict__ partial,
+                                                        const uint8_t* __restrict__ phantom) {
+  // phantom: as k_weighted_volume (the sum runs over the point's own family)
   __shared__ double smin[kBlock / TPO];
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t i = g / TPO;
@@ -1554,14 +1560,16 @@ __global__ void __launch_bounds__(kBlock) k_critical_dt(int64_t n, const int64_t
     const double h = hp[i];
     const double spring =
         __ddiv_rn(__dmul_rn(18.0, p.y), __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(3.14159265358979323846, h), h), h), h));
-    nn = row[i + 1] - row[i];
     for (int64_t b = row[i] + lane; b < row[i + 1]; b += TPO) {
+      if (phantom && (phantom[b] & kPhantomOwn)) continue;
+      ++nn;
       const double4 xj = xv[col[b]];
       const double d = __dsqrt_rn(sq3_rn(__dsub_rn(xi.x, xj.x), __dsub_rn(xi.y, xj.y), __dsub_rn(xi.z, xj.z)));
       den = __dadd_rn(den, __ddiv_rn(__dmul_rn(xj.w, spring), d));
     }
   }
   den = group_sum<TPO>(den);
+  nn = group_sum<TPO>(nn);
   double cts = 1.0e50;
   if (valid && nn > 0) cts = __dsqrt_rn(__ddiv_rn(__dmul_rn(2.0, pt[i].w), den));
   if (lane == 0) smin[threadIdx.x / TPO] = cts;
@@ -1614,7 +1622,7 @@ static inline unsigned grid_split(int64_t n, int tpo) {
 cudaError_t launch_weighted_volume(const pd_ctx* c) {
   if (c->n == 0) return cudaSuccess;
   PD_DISPATCH_TPO(c->tpo, k_weighted_volume, grid_for(c->n, c->tpo), c->n, c->row.p, c->col.p, c->xv.p, c->hp.p,
-                  c->influence, c->pt.p);
+                  c->influence, c->pt.p, c->phantoms ? c->dmg.p : nullptr);
   return cudaGetLastError();
 }
 
@@ -1819,6 +1827,17 @@ static cudaError_t ensure_chunk_hi(pd_ctx* c) {
   return cudaSuccess;
 }
 
+__global__ void k_node_damage_own(int64_t n, const int64_t* __restrict__ row, const uint8_t* __restrict__ dmg,
+                                  double* __restrict__ node_damage);
+// With phantom halves in the rows the passes count them as broken; the node
+// damage is then recounted over the own families.
+static cudaError_t own_node_damage(pd_ctx* c, const uint8_t* dmg) {
+  if (!c->phantoms || c->n == 0) return cudaSuccess;
+  k_node_damage_own<<<(unsigned)((c->n * 8 + kBlock - 1) / kBlock), kBlock, 0, c->stream>>>(c->n, c->row.p, dmg,
+                                                                                             c->node_damage.p);
+  return cudaGetLastError();
+}
+
 // One model evaluation (damage -> dilatation -> force [-> Verlet epilogue]) on
 // the gathered state of parity c->cur, with bond damage dmg updated in place.
 // With sp.f_host set, the split sliced force pass also copies the force
@@ -1899,6 +1918,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
                                                            c->sc_gate64, c->ab64.p, c->theta.p, c->node_damage.p,
                                                            c->sell_off.p, dmg);
     TRY_CUDA(cudaGetLastError());
+    TRY_CUDA(own_node_damage(c, dmg));
     if (ev) cudaEventRecord(ev[1], c->stream);
     auto* kf = pair ? &k_force_f64s<true> : &k_force_f64s<false>;
     kf<<<grid_split(c->n, 4), kSplitBlock, 0, c->stream>>>(c->n, c->sell_col.p, c->sell_dmg.p, c->bx64.p,
@@ -1918,6 +1938,8 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
       PD_DISPATCH_TPO(tpo, k_bb_fp64, grid, c->n, c->row.p, c->col.p, dmg, c->xv.p, c->st[c->cur].p, c->pt.p, c->sc.p,
                       c->hp.p, sp.damage_on, c->bb_plane, c->bb_height, c->node_damage.p, E, ipair);
     }
+    TRY_CUDA(cudaGetLastError());
+    TRY_CUDA(own_node_damage(c, dmg));
     if (ev) cudaEventRecord(ev[2], c->stream);
     return cudaGetLastError();
   }
@@ -1974,6 +1996,7 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  TRY_CUDA(own_node_damage(c, dmg));
   if (ev) cudaEventRecord(ev[1], c->stream);
   if (sell) {
     if (sp.f_host && sp.f_out) {
@@ -2019,6 +2042,26 @@ cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* hos
   return cudaGetLastError();
 }
 
+// Node damage over the points' own families (phantom halves are neither
+// bonds nor breaks of the row): CriticalStretchDamageModel.cpp:170-183.
+__global__ void k_node_damage_own(int64_t n, const int64_t* __restrict__ row, const uint8_t* __restrict__ dmg,
+                                  double* __restrict__ node_damage) {
+  const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int lane = threadIdx.x & 7;
+  int own = 0, broken = 0;
+  if (i < n)  // (every lane reaches the shuffles)
+    for (int64_t b = row[i] + lane; b < row[i + 1]; b += 8) {
+      const int d = dmg[b];
+      own += (d & kPhantomOwn) ? 0 : 1;
+      broken += (d & (1 | kPhantomOwn)) == 1 ? 1 : 0;
+    }
+  for (int o = 4; o > 0; o >>= 1) {
+    own += __shfl_xor_sync(0xffffffffu, own, o, 8);
+    broken += __shfl_xor_sync(0xffffffffu, broken, o, 8);
+  }
+  if (i < n && lane == 0) node_damage[i] = own > 0 ? (double)broken / (double)own : 0.0;
+}
+
 // Folds the recorded bond-pass events into c->kms (synchronizes on the last one).
 cudaError_t collect_kernel_times(pd_ctx* c) {
   if (c->kev_used == 0) return cudaSuccess;
@@ -2062,7 +2105,8 @@ cudaError_t launch_critical_dt(pd_ctx* c, double* dt_out_dev) {
     cudaError_t e = c->scratch.alloc((size_t)grid + 1);
     if (e != cudaSuccess) return e;
   }
-  PD_DISPATCH_TPO(c->tpo, k_critical_dt, grid, c->n, c->row.p, c->col.p, c->xv.p, c->pt.p, c->hp.p, c->scratch.p);
+  PD_DISPATCH_TPO(c->tpo, k_critical_dt, grid, c->n, c->row.p, c->col.p, c->xv.p, c->pt.p, c->hp.p, c->scratch.p,
+                  c->phantoms ? c->dmg.p : nullptr);
   k_min_reduce<<<1, kBlock, 0, c->stream>>>((int64_t)grid, c->scratch.p, dt_out_dev);
   return cudaGetLastError();
 }
@@ -2071,7 +2115,8 @@ int64_t critical_dt_partials(const pd_ctx* c) { return (int64_t)grid_for(c->n, c
 
 cudaError_t launch_critical_dt_into(pd_ctx* c, double* partial, double* dt_out_dev) {
   const unsigned grid = grid_for(c->n, c->tpo);
-  PD_DISPATCH_TPO(c->tpo, k_critical_dt, grid, c->n, c->row.p, c->col.p, c->xv.p, c->pt.p, c->hp.p, partial);
+  PD_DISPATCH_TPO(c->tpo, k_critical_dt, grid, c->n, c->row.p, c->col.p, c->xv.p, c->pt.p, c->hp.p, partial,
+                  c->phantoms ? c->dmg.p : nullptr);
   k_min_reduce<<<1, kBlock, 0, c->stream>>>((int64_t)grid, partial, dt_out_dev);
   return cudaGetLastError();
 }
@@ -2158,11 +2203,11 @@ cudaError_t launch_unpack_state(pd_ctx* c, int64_t n_idx, const int32_t* idx, co
   return cudaGetLastError();
 }
 
-// Broken bonds of the families: bond damage bytes with the row's own half (bit 0) set.
+// Broken bonds of the families: bond damage bytes with the row's own half (bit 0) set, phantom halves not counted.
 __global__ void k_count_nonzero(int64_t m, const uint8_t* __restrict__ d, unsigned long long* __restrict__ out) {
   unsigned long long cnt = 0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
-    cnt += d[k] & 1;
+    cnt += (d[k] & (1 | kPhantomOwn)) == 1 ? 1 : 0;
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
 }
@@ -2191,8 +2236,12 @@ __global__ void k_mirror_damage(int64_t n, const int64_t* __restrict__ row, cons
   for (int64_t b = row[i] + lane; b < row[i + 1]; b += 8) {
     const int32_t j = col[b];
     const int64_t bp = partner_bond(row, col, i, j);
-    const int own = src[b] & 1, part = (bp < row[j + 1] && col[bp] == (int32_t)i) ? (src[bp] & 1) : own;
-    dst[b] = (uint8_t)(own | (part << 1));
+    const bool found = bp < row[j + 1] && col[bp] == (int32_t)i;
+    const int own = src[b] & 1, part = found ? (src[bp] & 1) : own;
+    // phantom halves keep their markers: the own one from this byte, the
+    // partner one from the partner's own marker
+    const int mk = (src[b] & kPhantomOwn) | (found && (src[bp] & kPhantomOwn) ? kPhantomPartner : 0);
+    dst[b] = (uint8_t)(own | (part << 1) | mk);
     asym |= own != part;
   }
   if (asym) atomicOr(flag, 1);

@@ -774,6 +774,10 @@ static int qs_prepare_at(pd_ctx* c, const double* u_dev) {
     c->err = "the quasi-static solve supports the LPS material model only";
     return PD_ERR_UNSUPPORTED;
   }
+  if (c->phantoms) {
+    c->err = "the implicit and quasi-static solves need symmetric bond families (one horizon across the blocks)";
+    return PD_ERR_UNSUPPORTED;
+  }
   TRY_RC(qs_alloc(c));
   QsState* s = c->qs;
   const int64_t n = c->n;
@@ -981,6 +985,10 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
              "quasi-static solves a*t + b";
     return PD_ERR_UNSUPPORTED;
   }
+  if (c->phantoms) {
+    c->err = "the implicit and quasi-static solves need symmetric bond families (one horizon across the blocks)";
+    return PD_ERR_UNSUPPORTED;
+  }
   TRY_RC(qs_alloc(c));
   QsState* s = c->qs;
   const int64_t n = c->n, m = 3 * n;
@@ -1097,7 +1105,7 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
     st->preconditioner_fallbacks += c->qs_fallbacks - fallbacks0;
     st->coarse_builds += coarse_builds;
     st->device_ms += ms;
-    st->bonds = c->nb;
+    st->bonds = c->nb_user;
   }
   if (metric > newton_tol) {
     c->err = "quasi-static Newton iteration did not reach its tolerance";
@@ -1225,6 +1233,10 @@ int implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_impli
              "quasi-static solves a*t + b";
     return PD_ERR_UNSUPPORTED;
   }
+  if (c->phantoms) {
+    c->err = "the implicit and quasi-static solves need symmetric bond families (one horizon across the blocks)";
+    return PD_ERR_UNSUPPORTED;
+  }
   TRY_RC(qs_alloc(c));
   QsState* s = c->qs;
   const int64_t n = c->n, m = 3 * n;
@@ -1299,7 +1311,7 @@ int implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_impli
     st->cg_iterations += cg_total;
     st->final_residual = last_rel;
     st->device_ms += ms;
-    st->bonds = c->nb;
+    st->bonds = c->nb_user;
   }
   return PD_OK;
 }

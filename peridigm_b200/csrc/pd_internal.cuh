@@ -154,6 +154,18 @@ struct pd_ctx {
   int64_t nb = 0;
   int max_row = 0;
   bool symmetric = true;
+  // Families with j in H(i) but i not in H(j) (blocks of different horizons,
+  // or a caller's list): the device CSR holds every bond in both rows, the
+  // added reverse (j, i) as a phantom whose own half does not exist (damage
+  // bits 0 and kPhantomOwn), the original (i, j) then without a partner half
+  // (bits 1 and kPhantomPartner). nb counts the device CSR, nb_user the
+  // caller's families; h_orig marks the device bonds that are the caller's,
+  // h_nph counts each row's phantoms.
+  bool phantoms = false;
+  int64_t nb_user = 0;
+  std::vector<uint8_t> h_orig;
+  std::vector<int32_t> h_nph;
+  std::vector<uint8_t> h_dmg0;  // the device CSR's damage bytes with no bond broken
   pdb::DBuf<int64_t> row;
   pdb::DBuf<int32_t> col;
   pdb::DBuf<uint8_t> dmg;        // committed (N) bond damage
@@ -342,6 +354,9 @@ int check_sc_pairs(pd_ctx* c);
 void qs_release(pd_ctx* c);
 
 // status bits
+// Damage-byte markers of phantom halves (bits 0 and 1 are also set for them).
+constexpr int kPhantomOwn = 8, kPhantomPartner = 16;
+
 enum StatusBits { ST_NONFINITE_FORCE = 1, ST_NONFINITE_CONTACT = 2, ST_TIMEOUT = 4, ST_BAD_INDEX = 8, ST_NONFINITE_BC = 16 };
 
 }  // namespace pdb

@@ -284,12 +284,20 @@ def test_errors_are_reported():
         ctx.set_points(np.zeros(6) + np.array([0, 0, 0, 1, 0, 0.0]), np.ones(2))
         with pytest.raises(PDError):
             ctx.set_bonds(np.array([1, 5, 0], np.int32))  # neighbor id out of range
-        ctx.set_bonds(np.array([1, 1, 0], np.int32))  # 0->1 without 1->0
+        ctx.set_bonds(np.array([1, 1, 0], np.int32))  # 0->1 without 1->0: a one-sided family
         ctx.set_horizons([2.0])
         ctx.material(1.0, 1.0, 1.0)
+        # both points at one place: |Y| = 0, a NaN force (the reference terminates)
         with pytest.raises(PDError) as e:
             ctx.compute_force(np.zeros(6))
-        assert e.value.code == 6
+        assert e.value.code == 3
+        # stretched: the one-sided bond scatters t_01 to both points, as the oracle does
+        x = np.array([0, 0, 0, 1, 0, 0.0])
+        y = np.array([0, 0, 0, 1.001, 0.0005, 0.0])
+        f = ctx.compute_force(y)
+        ref = O.eval_model(x, y, np.ones(2), np.array([0, 1, 1], np.int64), np.array([1], np.int32), 1.0, 1.0, 2.0)
+        assert np.abs(f - ref["force"]).max() <= 1e-6 * np.abs(ref["force"]).max()
+        assert np.abs(f[:3] + f[3:]).max() <= 1e-6 * np.abs(f).max()  # equal volumes: equal and opposite
 
 
 def test_split_refuses_weighted_influence_across_horizons():
