@@ -139,7 +139,11 @@ int pd_set_block_horizons(pd_ctx* ctx, int32_t n_blocks, const double* horizon);
  * with ZoltanSearchTree::FindPointsWithinRadius (src/io/Peridigm_ZoltanSearchTree.cpp:214-247)
  * and FinitePlaneFilter (src/io/pdneigh/BondFilter.cxx:123-150). */
 int pd_build_bonds(pd_ctx* ctx, const pd_plane_filter* filters, int32_t n_filters);
-/* Bond family from a Peridigm neighbor list of length len (accepted verbatim). */
+/* Bond family from a Peridigm neighbor list of length len (accepted verbatim).
+ * Families may be one-sided (j in H(i) without i in H(j), as blocks of different
+ * horizons give): each bond's force then acts as the reference's scatter of
+ * i's family adds it (elastic.cxx:121-130); pd_get_bonds, pd_num_bonds and the
+ * per-bond fields keep the list as given. */
 int pd_set_bonds(pd_ctx* ctx, const int32_t* neighborhood_list, int64_t len);
 int pd_num_bonds(const pd_ctx* ctx, int64_t* nb);
 /* Neighbor list in Peridigm format; *len receives the length (cap may be 0 to query). */
