@@ -275,7 +275,8 @@ int pd_add_prescribed_displacement(pd_ctx* ctx, int64_t n_points, const int64_t*
  * (:222-241); a zero increment takes f(t_prev) from the displacement field
  * (:137-142). PD_ERR_ARG with the message in pd_last_error on a syntax error
  * or an unknown name; PD_ERR_NONFINITE when a value is not finite. The
- * quasi-static and implicit solves refuse contexts with such functions
+ * quasi-static solve evaluates them at each load step's two times (the same
+ * increment rule); the implicit solve refuses contexts with such functions
  * (PD_ERR_UNSUPPORTED). */
 int pd_add_prescribed_displacement_function(pd_ctx* ctx, int64_t n_points, const int64_t* points,
                                             int32_t coordinate, const char* function);

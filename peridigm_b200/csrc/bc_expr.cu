@@ -278,6 +278,8 @@ bool expr_compile(const std::string& body_in, std::vector<int32_t>& code, std::v
 
 // One evaluation's prescribed values of the function dofs: cp[k] = (u_k(t_c),
 // u_k(t_p)) at the times the Verlet epilogue of evaluation `step` uses.
+// step >= 0: the times of the Verlet epilogue of evaluation `step`; step < 0:
+// the given times t0 (current) and dt (previous), a quasi-static load step's.
 __global__ void k_bc_expr(int64_t nd, const int32_t* __restrict__ dofs, const int32_t* __restrict__ start,
                           const int32_t* __restrict__ code, const double* __restrict__ konst,
                           const double4* __restrict__ xv, int64_t step, double t0, double dt, double2* __restrict__ cp,
@@ -286,14 +288,18 @@ __global__ void k_bc_expr(int64_t nd, const int32_t* __restrict__ dofs, const in
   if (q >= nd) return;
   const int64_t k = dofs[q];
   const double4 x = xv[k / 3];
-  const double tc = __dadd_rn(t0, __dmul_rn((double)(step + 1), dt));
-  const double tp = step == 0 ? t0 : __dadd_rn(t0, __dmul_rn((double)step, dt));
+  const double tc = step < 0 ? t0 : __dadd_rn(t0, __dmul_rn((double)(step + 1), dt));
+  const double tp = step < 0 ? dt : (step == 0 ? t0 : __dadd_rn(t0, __dmul_rn((double)step, dt)));
   bool ok1 = false, ok2 = false;
   const int32_t* prog = code + start[q];
   const double cur = expr_run(prog, konst, x.x, x.y, x.z, tc, max_ops, &ok1);
   const double prev = expr_run(prog, konst, x.x, x.y, x.z, tp, max_ops, &ok2);
   if (!ok1 || !ok2) atomicOr(status, ST_NONFINITE_BC);
   cp[k] = make_double2(cur, prev);
+}
+
+cudaError_t launch_bc_expr_at(pd_ctx* c, double t_cur, double t_prev) {
+  return launch_bc_expr(c, -1, t_cur, t_prev);
 }
 
 cudaError_t launch_bc_expr(pd_ctx* c, int64_t step, double t0, double dt) {

@@ -478,16 +478,24 @@ __global__ void k_qs_axpy(int64_t m, double a, const double* __restrict__ x, dou
 }
 
 __global__ void k_qs_apply_bc(int64_t n, const uint8_t* __restrict__ mask, const double* __restrict__ a,
-                              const double* __restrict__ b, double tc, double tp, const double* __restrict__ u,
-                              double* __restrict__ du) {
+                              const double* __restrict__ b, const double2* __restrict__ fcp, double tc, double tp,
+                              const double* __restrict__ u, double* __restrict__ du) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int c = 0; c < 3; ++c)
     if ((mask[i] >> c) & 1) {
       const int64_t k = 3 * i + c;
       // DirichletIncrementBC coeff 1 (Peridigm_BoundaryCondition.cpp:235); a
-      // zero increment takes the previous value from the displacement (:137-142)
-      const double cur = a[k] * tc + b[k], d = cur - (a[k] * tp + b[k]);
+      // zero increment takes the previous value from the displacement
+      // (:137-142); function dofs (mask bit 3 + c) from their values at the
+      // two times (fcp)
+      double cur, prev;
+      if (fcp && ((mask[i] >> (c + 3)) & 1)) {
+        cur = fcp[k].x, prev = fcp[k].y;
+      } else {
+        cur = a[k] * tc + b[k], prev = a[k] * tp + b[k];
+      }
+      const double d = cur - prev;
       du[k] = d == 0.0 ? cur - u[k] : d;
     }
 }
@@ -782,7 +790,7 @@ static int qs_prepare_at(pd_ctx* c, const double* u_dev) {
   QsState* s = c->qs;
   const int64_t n = c->n;
   std::vector<uint8_t> fx(n, 0);
-  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
+  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : (uint8_t)(c->h_bc_mask[i] & 7);  // the coordinates held
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
   PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, 3 * n * sizeof(double), c->stream));
   k_qs_positions<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->xv.p, u_dev, s->du.p, s->yq.p);
@@ -980,11 +988,6 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
     c->err = "the quasi-static solve supports the LPS material model only";
     return PD_ERR_UNSUPPORTED;
   }
-  if (c->n_bc_expr) {
-    c->err = "prescribed displacement functions of x, y, z, t run on the explicit path; give the implicit and "
-             "quasi-static solves a*t + b";
-    return PD_ERR_UNSUPPORTED;
-  }
   if (c->phantoms) {
     c->err = "the implicit and quasi-static solves need symmetric bond families (one horizon across the blocks)";
     return PD_ERR_UNSUPPORTED;
@@ -999,10 +1002,16 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   }
   // prescribed dofs and their increments (DirichletIncrementBC on deltaU)
   std::vector<uint8_t> fx(n, 0);
-  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
+  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : (uint8_t)(c->h_bc_mask[i] & 7);  // the coordinates held
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
   const double dt = t_cur - t_prev;
   const bool predict = o->use_predictor && st && st->steps > 0;
+  // prescribed functions of x, y, z, t: their values at the two times
+  const double2* fcp = nullptr;
+  if (c->n_bc_expr && c->has_bc) {
+    PD_CUDA_TRY(c, launch_bc_expr_at(c, t_cur, t_prev));
+    fcp = c->bc_cp.p;
+  }
   double l2, linf;
   // Negative tolerance: relative to the metric of this load step's start
   // without the predictor (prescribed increments only), the scale of the load
@@ -1011,16 +1020,16 @@ int qs_load_step(pd_ctx* c, double t_prev, double t_cur, const pd_qs_options* o,
   if (o->newton_tolerance < 0.0 || !predict) {
     PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
     if (c->has_bc)
-      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, c->u.p,
-                                                        s->du.p);
+      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, fcp, t_cur, t_prev,
+                                                        c->u.p, s->du.p);
     TRY_RC(qs_residual(c, &l2, &linf));
     ref_metric = l2 + 20.0 * linf;
   }
   if (predict) {
     PD_CUDA_TRY(c, cudaMemcpyAsync(s->du.p, s->pred.p, m * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if (c->has_bc)
-      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, t_cur, t_prev, c->u.p,
-                                                        s->du.p);
+      k_qs_apply_bc<<<g1(n), kQsBlock, 0, c->stream>>>(n, c->bc_mask.p, c->bc_a.p, c->bc_b.p, fcp, t_cur, t_prev,
+                                                        c->u.p, s->du.p);
     TRY_RC(qs_residual(c, &l2, &linf));
   }
   double metric = l2 + 20.0 * linf;
@@ -1229,8 +1238,8 @@ int implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_impli
     return PD_ERR_UNSUPPORTED;
   }
   if (c->n_bc_expr) {
-    c->err = "prescribed displacement functions of x, y, z, t run on the explicit path; give the implicit and "
-             "quasi-static solves a*t + b";
+    c->err = "prescribed displacement functions of x, y, z, t run on the explicit and quasi-static paths; give "
+             "the implicit solve a*t + b";
     return PD_ERR_UNSUPPORTED;
   }
   if (c->phantoms) {
@@ -1242,7 +1251,7 @@ int implicit_run(pd_ctx* c, double dt, double t0, int64_t nsteps, const pd_impli
   const int64_t n = c->n, m = 3 * n;
   PD_CUDA_TRY(c, s->v2.alloc(m));
   std::vector<uint8_t> fx(n, 0);
-  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : c->h_bc_mask[i];
+  for (int64_t i = 0; i < n; ++i) fx[i] = c->h_bc_mask.empty() ? 0 : (uint8_t)(c->h_bc_mask[i] & 7);  // the coordinates held
   PD_CUDA_TRY(c, cudaMemcpyAsync(s->fixed.p, fx.data(), n, cudaMemcpyHostToDevice, c->stream));
   PD_CUDA_TRY(c, cudaMemsetAsync(s->du.p, 0, m * sizeof(double), c->stream));
   if (c->has_bc)

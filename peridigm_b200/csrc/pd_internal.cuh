@@ -267,6 +267,8 @@ cudaError_t launch_pack_owner(pd_ctx* c);
 cudaError_t launch_eval(pd_ctx* c, const StepParams& sp, uint8_t* dmg, bool* host_done = nullptr);
 // Values of the prescribed functions for evaluation `step` (bc_cp).
 cudaError_t launch_bc_expr(pd_ctx* c, int64_t step, double t0, double dt);
+// The same at the given current and previous times (a quasi-static load step).
+cudaError_t launch_bc_expr_at(pd_ctx* c, double t_cur, double t_prev);
 // Gathered state of points i0 .. i1-1 (i1 < 0: all) from current coordinates y_dev [3n].
 cudaError_t launch_state_from_y(pd_ctx* c, const double* y_dev, int64_t i0 = 0, int64_t i1 = -1);
 cudaError_t launch_sync_state(pd_ctx* c);

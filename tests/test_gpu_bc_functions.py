@@ -15,7 +15,8 @@ previous value from the displacement field, :137-142).
   closed form a = 0, b = const) go to that value in the first step, as in
   the oracle.
 * A function that is not finite stops the run with PD_ERR_NONFINITE; the
-  quasi-static solve refuses contexts with functions.
+  implicit solve refuses contexts with functions; the quasi-static solve with
+  the cube's prescribed faces as functions equals its closed-form run.
 """
 import math
 
@@ -163,5 +164,26 @@ def test_nonfinite_function_and_qs_refusal():
         ctx.material(130e9, 78e9, 7800.0)
         ctx.prescribed_displacement_function(left, 0, "1.0e-6*t")
         with pytest.raises(PDError) as e:
-            ctx.qs_load_step(0.0, 1.0, newton_tolerance=1e-8)
+            ctx.implicit_run(1.0e-6, 1)
         assert e.value.code == 6
+
+
+def test_quasi_static_functions_match_closed_forms():
+    """The quasi-static cube with its prescribed faces given as functions
+    (the same ramps, and a constant written as a function) equals the run with
+    the closed forms, increments included."""
+    w = workloads.qs_cube(n=7, h=1.0e-3, seed=3, jitter=0.05, load_steps=3)
+    res = []
+    for as_function in (False, True):
+        with Context(precision="fp64") as ctx:
+            workloads.setup_context(ctx, w)
+            if as_function:
+                ctx.clear_boundary_conditions()
+                for b in w["bcs"]:
+                    ctx.prescribed_displacement_function(b["points"], b["coordinate"], f"{b['a']!r}*t + {b['b']!r}")
+            for k in range(1, len(w["times"])):
+                ctx.qs_load_step(w["times"][k - 1], w["times"][k], newton_tolerance=1e-6,
+                                 cg_relative_tolerance=1e-10)
+            res.append(ctx.field("Displacement"))
+    assert np.abs(res[1]).max() > 1e-6
+    assert np.abs(res[1] - res[0]).max() <= 1e-12 * np.abs(res[0]).max()
