@@ -246,13 +246,18 @@ __device__ __forceinline__ int64_t xs_index(int64_t k) { return 96 * (k >> 5) + 
 #ifndef PD_BOND_UNROLL
 #define PD_BOND_UNROLL 4
 #endif
+// Resident blocks of 128 threads per SM (the launch bound): 7 (72 registers,
+// 28 warps) against 8 (64 registers, 32 warps, where the half-bond
+// dilatation spills): dilatation 14.94 -> 13.84 ms and force 16.25 -> 15.46 ms
+// at the 32,000,000-point heterogeneous plate, 0.1173 -> 0.1162 ms and
+// 0.1196 -> 0.1090 ms at the notched plate; 6 blocks (80 registers) were
+// slower than 8 on both.
 #ifndef PD_BOND_MINB
-#define PD_BOND_MINB 8
+#define PD_BOND_MINB 7
 #endif
 constexpr int kUnroll = PD_BOND_UNROLL;
-// Threads per block of the split bond passes: 8 blocks of 128 fill an SM's
-// 1024 threads at 64 registers, and the last partial wave of a ~5000-block
-// grid costs half of what it does with 256-thread blocks.
+// Threads per block of the split bond passes: 128-thread blocks keep the last
+// partial wave of a ~5000-block grid at half the cost of 256-thread blocks.
 constexpr int kSplitBlock = 128;
 
 // Bond damage byte of bond (i, j) in row i: bit 0 = d_ij, the damage of the
@@ -562,7 +567,7 @@ __global__ void __launch_bounds__(kBlock) k_sell_dmg(int64_t n, const int64_t* _
 // with its own s_c,j, read only for bonds stretched past s_min, the smallest
 // critical stretch of the body (no bond below it can break on either side).
 #ifndef PD_DIL_MINB
-#define PD_DIL_MINB 8
+#define PD_DIL_MINB 7
 #endif
 template <int TPO, bool SELL, bool LIN = false, bool WEIGHT = false, bool PAIR = false>
 __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilatation_split(
