@@ -26,7 +26,15 @@ Grid make_grid(int64_t n, const double lo[3], const double hi[3], double reach);
 // Bins n positions (xyz of double4) into grid g: sorted_idx lists the points
 // cell by cell (ascending id within a cell), cell_start[q] the first entry of
 // cell q (cell_start[ncell] = n).
+// scratch (optional): the binning's temporaries kept between calls, so that
+// a repeated search (contact, every search_frequency steps) allocates and
+// frees no device memory once its buffers are large enough; sorted_idx and
+// cell_start are then also only grown.
+struct BinScratch {
+  DBuf<int32_t> cid, idx, cid_s;
+  DBuf<unsigned char> tmp;
+};
 int bin_points(pd_ctx* c, const double4* pos, int64_t n, const Grid& g, DBuf<int32_t>& sorted_idx,
-               DBuf<int64_t>& cell_start);
+               DBuf<int64_t>& cell_start, BinScratch* scratch = nullptr);
 
 }  // namespace pdb

@@ -407,26 +407,37 @@ Grid make_grid(int64_t n, const double lo[3], const double hi[3], double reach) 
 }
 
 int bin_points(pd_ctx* c, const double4* pos, int64_t n, const Grid& g, DBuf<int32_t>& idx_s,
-               DBuf<int64_t>& cell_start) {
+               DBuf<int64_t>& cell_start, BinScratch* scratch) {
   const int64_t ncell = (int64_t)g.dims[0] * g.dims[1] * g.dims[2];
-  DBuf<int32_t> cid, idx, cid_s;
-  PD_CUDA_TRY(c, cid.alloc(n));
-  PD_CUDA_TRY(c, idx.alloc(n));
-  PD_CUDA_TRY(c, cid_s.alloc(n));
-  PD_CUDA_TRY(c, idx_s.alloc(n));
-  PD_CUDA_TRY(c, cell_start.alloc(ncell + 1));
+  BinScratch local;
+  BinScratch& S = scratch ? *scratch : local;
+  if (scratch) {
+    PD_CUDA_TRY(c, S.cid.reserve(n));
+    PD_CUDA_TRY(c, S.idx.reserve(n));
+    PD_CUDA_TRY(c, S.cid_s.reserve(n));
+    PD_CUDA_TRY(c, idx_s.reserve(n));
+    PD_CUDA_TRY(c, cell_start.reserve(ncell + 1));
+  } else {
+    PD_CUDA_TRY(c, S.cid.alloc(n));
+    PD_CUDA_TRY(c, S.idx.alloc(n));
+    PD_CUDA_TRY(c, S.cid_s.alloc(n));
+    PD_CUDA_TRY(c, idx_s.alloc(n));
+    PD_CUDA_TRY(c, cell_start.alloc(ncell + 1));
+  }
   const unsigned g1 = (unsigned)((n + 255) / 256);
-  k_cell_ids<<<g1, 256, 0, c->stream>>>(n, pos, g, cid.p, idx.p);
+  k_cell_ids<<<g1, 256, 0, c->stream>>>(n, pos, g, S.cid.p, S.idx.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   int end_bit = 1;
   while (end_bit < 31 && (int64_t(1) << end_bit) <= ncell) ++end_bit;
   size_t tmp_bytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, cid.p, cid_s.p, idx.p, idx_s.p, (int)n, 0, end_bit, c->stream);
-  DBuf<unsigned char> tmp;
-  PD_CUDA_TRY(c, tmp.alloc(tmp_bytes));
-  PD_CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, cid.p, cid_s.p, idx.p, idx_s.p, (int)n, 0, end_bit,
-                                                 c->stream));
-  k_cell_bounds<<<(unsigned)((n + 1 + 255) / 256), 256, 0, c->stream>>>(n, ncell, cid_s.p, cell_start.p);
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, S.cid.p, S.cid_s.p, S.idx.p, idx_s.p, (int)n, 0, end_bit,
+                                  c->stream);
+  if (scratch) PD_CUDA_TRY(c, S.tmp.reserve(tmp_bytes));
+  else PD_CUDA_TRY(c, S.tmp.alloc(tmp_bytes));
+  tmp_bytes = S.tmp.count;
+  PD_CUDA_TRY(c, cub::DeviceRadixSort::SortPairs(S.tmp.p, tmp_bytes, S.cid.p, S.cid_s.p, S.idx.p, idx_s.p, (int)n, 0,
+                                                 end_bit, c->stream));
+  k_cell_bounds<<<(unsigned)((n + 1 + 255) / 256), 256, 0, c->stream>>>(n, ncell, S.cid_s.p, cell_start.p);
   PD_CUDA_TRY(c, cudaGetLastError());
   return PD_OK;
 }

@@ -41,6 +41,14 @@ struct ContactState {
   DBuf<int32_t> ccol;
   int64_t npairs = 0;
   bool have_list = false;
+  // search temporaries kept between searches (grown only): a search between
+  // steps then allocates and frees no device memory, whose driver calls can
+  // wait behind other processes' queries of the device
+  DBuf<double> part;
+  DBuf<int32_t> idx_s;
+  DBuf<int64_t> cell_start, counts;
+  DBuf<unsigned char> stmp;
+  BinScratch bins;
 };
 
 __device__ __forceinline__ double sq3(double dx, double dy, double dz) {
@@ -218,8 +226,8 @@ static int contact_search(pd_ctx* c, const double4* pos) {
   const int64_t n = c->n;
   // bounding box of the search positions
   const int nblk = 148;
-  DBuf<double> part;
-  PD_CUDA_TRY(c, part.alloc(6 * nblk));
+  DBuf<double>& part = cs->part;
+  PD_CUDA_TRY(c, part.reserve(6 * nblk));
   k_bbox<<<nblk, 256, 0, c->stream>>>(n, pos, part.p);
   std::vector<double> hp(6 * nblk);
   PD_CUDA_TRY(c, cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -236,11 +244,12 @@ static int contact_search(pd_ctx* c, const double4* pos) {
     return PD_ERR_NONFINITE;
   }
   const Grid g = make_grid(n, lo, hi, cs->r_search);
-  DBuf<int32_t> idx_s;
-  DBuf<int64_t> cell_start, counts;
-  int rc = bin_points(c, pos, n, g, idx_s, cell_start);
+  DBuf<int32_t>& idx_s = cs->idx_s;
+  DBuf<int64_t>& cell_start = cs->cell_start;
+  DBuf<int64_t>& counts = cs->counts;
+  int rc = bin_points(c, pos, n, g, idx_s, cell_start, &cs->bins);
   if (rc != PD_OK) return rc;
-  PD_CUDA_TRY(c, counts.alloc(n + 1));
+  PD_CUDA_TRY(c, counts.reserve(n + 1));
   const unsigned gw = (unsigned)((n * 32 + 255) / 256);
   k_contact_search<false><<<gw, 256, 0, c->stream>>>(n, pos, g, cell_start.p, idx_s.p, cs->r_search, c->row.p,
                                                      c->col.p, counts.p, nullptr, nullptr);
@@ -249,8 +258,9 @@ static int contact_search(pd_ctx* c, const double4* pos) {
   PD_CUDA_TRY(c, cudaMemsetAsync(counts.p + n, 0, sizeof(int64_t), c->stream));
   size_t scan_bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts.p, cs->crow.p, (int)(n + 1), c->stream);
-  DBuf<unsigned char> stmp;
-  PD_CUDA_TRY(c, stmp.alloc(scan_bytes));
+  DBuf<unsigned char>& stmp = cs->stmp;
+  PD_CUDA_TRY(c, stmp.reserve(scan_bytes));
+  scan_bytes = stmp.count;
   PD_CUDA_TRY(c, cub::DeviceScan::ExclusiveSum(stmp.p, scan_bytes, counts.p, cs->crow.p, (int)(n + 1), c->stream));
   int64_t np = 0;
   PD_CUDA_TRY(c, cudaMemcpyAsync(&np, cs->crow.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));

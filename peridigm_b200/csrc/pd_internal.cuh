@@ -104,6 +104,12 @@ struct DBuf {
     count = 0;
   }
   size_t bytes() const { return count * sizeof(T); }
+  // At least n elements, reallocating (with a quarter's headroom) only when
+  // smaller: repeated work reuses its buffers instead of allocating each time.
+  cudaError_t reserve(size_t n) {
+    if (p && count >= n) return cudaSuccess;
+    return alloc(n + n / 4 + 16);
+  }
 };
 
 struct ContactState;
