@@ -625,11 +625,13 @@ __global__ void __launch_bounds__(kSplitBlock, WEIGHT ? 5 : PD_DIL_MINB) k_dilat
       // LPS: omega V_j |X| e; linear LPS: omega V_j X.du
       th = fmaf((own_ok && !brk) ? (LIN ? wv : wv * sb.zeta) : 0.0f, LIN ? sb.xu : sb.e, th);
     };
-    // neighbor records: slots 0-5 only (displacement, volume; the pass never
-    // reads a neighbor's A, B), two loads per record and fewer registers;
-    // the half-bond variant, whose extra tests keep the L1 busier, takes the
-    // whole record in one load (two loads per record double its L1 lookups)
-    constexpr int kRec = PAIR ? 0 : 2;
+    // neighbor records: the whole record in one 256-bit load although the
+    // pass reads slots 0-5 only (displacement, volume): two loads (16 + 8
+    // bytes) double the L1 lookups, and at 7 blocks per SM the registers for
+    // slots 6-7 are there (full-bond dilatation 0.1162 -> 0.1130 ms at the
+    // notched plate, 15.09 -> 14.68 ms at the 32,000,000-point plate with one
+    // material)
+    constexpr int kRec = 0;
     if constexpr (SELL)
       sell_walk<kRec>(i, lane, soff, col, dmg, bx3, ur, body);
     else
