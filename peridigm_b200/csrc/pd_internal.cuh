@@ -38,7 +38,7 @@ namespace pdb {
 // force density comes down chunk by chunk while the later chunks compute. The
 // transfers that cannot overlap (the first chunks up, the last one down)
 // shrink with the chunk: 32 chunks against 16 took the 32,000,000-point step
-// from 32.4 to 31.8 ms.
+// from 32.4 to 31.8 ms; 64 were slower again (32.2 against 31.9 ms).
 constexpr int kHostChunks = 32;
 
 // One 32-byte record per point, fetched with a single 256-bit load.
