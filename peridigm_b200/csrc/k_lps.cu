@@ -463,7 +463,10 @@ __global__ void k_pack_owner(int64_t n, const double4* __restrict__ pt, const do
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 p = pt[i];  // (m, K, mu, rho)
-  own[i] = make_float4((float)(3.0 / p.x), (float)((3.0 * p.y - 5.0 * p.z) / p.x), (float)(15.0 * p.z / p.x),
+  // a point with no bonds (m = 0) keeps theta = 0 and no force terms, as the
+  // reference's loops over its empty family leave them
+  const double im = p.x > 0.0 ? 1.0 / p.x : 0.0;
+  own[i] = make_float4((float)(3.0 * im), (float)((3.0 * p.y - 5.0 * p.z) * im), (float)(15.0 * p.z * im),
                        (float)sc[i]);
 }
 
@@ -1107,9 +1110,12 @@ __global__ void __launch_bounds__(kSplitBlock, PD_F64S_DIL_MINB) k_dilatation_f6
   broken = group_sum<4>(broken);
   if (valid && lane == 0) {
     const double4 p = pt[i];  // (m, K, mu, rho)
-    const double theta = 3.0 * th / p.x;
-    const double alpha = 15.0 * p.z / p.x;
-    const double q = 3.0 * p.y / p.x - alpha / 3.0;
+    // (a point with no own bonds, m = 0: theta = 0 and no force terms, as the
+    // reference's loops over an empty family leave them)
+    const bool fam = p.x > 0.0;
+    const double theta = fam ? 3.0 * th / p.x : 0.0;
+    const double alpha = fam ? 15.0 * p.z / p.x : 0.0;
+    const double q = fam ? 3.0 * p.y / p.x - alpha / 3.0 : 0.0;
     ab64[i] = make_double4(theta * q, alpha, theta, 0.0);
     theta_out[i] = theta;
     node_damage[i] = len > 0 ? (double)broken / (double)len : 0.0;

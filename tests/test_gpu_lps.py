@@ -330,3 +330,31 @@ def test_split_refuses_weighted_influence_across_horizons():
                 else:
                     ctx.compute_force(y)  # FP64 handles both horizons (omega_j with h_j)
     assert rel_l2(f["split"], f["fp64"]) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split", "fp64_sliced"])
+def test_point_without_bonds(precision):
+    """A point outside every horizon has an empty family (weighted volume 0):
+    the reference's loops over it leave its dilatation 0 and its force 0
+    (material_utilities.cxx:235-289, elastic.cxx:55-146), and the other
+    points match the oracle."""
+    x, vol, y, h = make_cloud(seed=4)
+    far = x.reshape(-1, 3).max(axis=0) + 10.0 * h
+    x2 = np.concatenate([x, far])
+    vol2 = np.concatenate([vol, vol[:1]])
+    y2 = np.concatenate([y, far + 1.0e-6])
+    row, col = O.neighbor_search(x2, h)
+    assert row[-1] == row[-2]  # the last point has no bonds
+    ev = O.eval_model(x2, y2, vol2, row, col, 130e9, 78e9, h)
+    with Context(precision=precision) as ctx:
+        ctx.set_points(x2, vol2)
+        ctx.set_horizons([h])
+        ctx.build_bonds([])
+        ctx.material(130e9, 78e9, 7800.0)
+        f = ctx.compute_force(y2)
+        th = ctx.field("Dilatation")
+    assert th[-1] == 0.0 and np.all(f[-3:] == 0.0)
+    assert np.all(np.isfinite(th)) and np.all(np.isfinite(f))
+    tol = 1e-6 if precision == "split" else 1e-11
+    assert rel_l2(f, ev["force"]) < tol
+    assert rel_l2(th, ev["theta"]) < tol
